@@ -1,0 +1,132 @@
+/* natsel_gpu.h -- C ABI of the B200 rigid-body step (libnatsel_gpu.so).
+ *
+ * The library is a drop-in for the reference engine's per-step rigid-body solve
+ * (reference: src/simulation/solver_integration.rs:807 World::step and the
+ * stages it calls: collide_pass.rs:164 collide, constraint_graph.rs:113
+ * add_contact_to_graph, solver_prepare.rs:269 prepare_all_contacts,
+ * solver_stages.rs:543 solve_constraint_stages, solver_integration.rs:435
+ * finalize_bodies, plus the broadphase pair update contact_creation.rs:901).
+ * Scene construction mirrors the reference World API so a host engine builds
+ * the same bodies/shapes/joints in the same order and gets the same ids.
+ *
+ * Plain C types only. Every call returns an int status (NS_OK == 0) unless
+ * documented otherwise; ns_last_error() gives a message. Calls on one world
+ * must be serialised by the caller (the reference World is Send, not Sync);
+ * distinct worlds may be used from distinct threads.
+ */
+#ifndef NATSEL_GPU_H
+#define NATSEL_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  NS_OK = 0,
+  NS_ERR_INVALID = 1,     /* bad argument or call order */
+  NS_ERR_CUDA = 2,        /* CUDA runtime error (message in ns_last_error) */
+  NS_ERR_CAPACITY = 3,    /* a device capacity (contacts, pairs) was exceeded */
+  NS_ERR_TIMEOUT = 4,     /* a bounded grid barrier gave up; the step result is invalid */
+  NS_ERR_NONFINITE = 5,   /* a body state became NaN/Inf */
+  NS_ERR_UNSUPPORTED = 6  /* feature outside the implemented path (e.g. sleeping) */
+};
+
+enum { NS_STATIC_BODY = 0, NS_KINEMATIC_BODY = 1, NS_DYNAMIC_BODY = 2 };
+
+typedef struct ns_world ns_world;
+
+/* World settings. Defaults follow the reference World::new (world_runtime.rs:1243-1272). */
+typedef struct {
+  float gravity[3];            /* (0,-10,0) */
+  int enable_sleep;            /* must be 0: sleeping islands are outside this path */
+  int enable_continuous;       /* fast bodies are only flagged (continuous.rs is outside this path) */
+  int enable_warm_starting;    /* 1 */
+  float contact_hertz;         /* 30 */
+  float contact_damping_ratio; /* 10 */
+  float contact_speed;         /* 3 m/s */
+  float max_linear_speed;      /* 400 m/s */
+  float restitution_threshold; /* 1 m/s */
+  int restitution_iterations;  /* 2 */
+  float joint_hertz;           /* 60 (JointDef default, joint_defs.rs:44) */
+  float joint_damping_ratio;   /* 2 */
+  int contact_capacity;        /* 0 = automatic (8 per shape + 4096) */
+  int solver_blocks;           /* 0 = automatic persistent grid size */
+  int device;                  /* CUDA device ordinal */
+} ns_world_def;
+
+/* Body definition (types/body_def.rs BodyDef). */
+typedef struct {
+  int type;                    /* NS_STATIC_BODY or NS_DYNAMIC_BODY */
+  double position[3];
+  float rotation[4];           /* x, y, z, s */
+  float linear_velocity[3];
+  float angular_velocity[3];
+  float linear_damping, angular_damping, gravity_scale;
+  int enable_sleep;            /* stored as a body flag; sleeping itself is not simulated */
+} ns_body_def;
+
+/* Shape definition (types/shape_def.rs ShapeDef with one surface material). */
+typedef struct {
+  float density, friction, restitution, rolling_resistance;
+  uint64_t category_bits, mask_bits;
+  int group_index;
+} ns_shape_def;
+
+void ns_default_world_def(ns_world_def* def);
+/* Creates a world; returns NULL on failure (message via ns_last_error(NULL)). */
+ns_world* ns_world_create(const ns_world_def* def);
+void ns_world_destroy(ns_world* world);
+const char* ns_last_error(const ns_world* world);
+
+/* Scene construction (replaces World::create_body world_runtime.rs:1506,
+ * create_hull_shape(make_box_hull) shape_creation.rs:559 / hull.rs:853,
+ * create_sphere_shape :504, create_capsule_shape :522,
+ * create_revolute_joint revolute_joint.rs:162). Returns the new id (>= 0) or -1. */
+int ns_create_body(ns_world* world, const ns_body_def* def);
+int ns_create_box_shape(ns_world* world, int body, const ns_shape_def* def, float hx, float hy, float hz);
+int ns_create_sphere_shape(ns_world* world, int body, const ns_shape_def* def, const float center[3],
+                           float radius);
+int ns_create_capsule_shape(ns_world* world, int body, const ns_shape_def* def, const float center1[3],
+                            const float center2[3], float radius);
+/* frame = position xyz + rotation xyzs, local to each body's origin. */
+int ns_create_revolute_joint(ns_world* world, int body_a, int body_b, const float frame_a[7],
+                             const float frame_b[7], int enable_limit, float lower_angle,
+                             float upper_angle, int enable_spring, float hertz, float damping_ratio,
+                             float max_motor_torque, int collide_connected);
+
+/* Advance one step (replaces World::step solver_integration.rs:807). Asynchronous:
+ * the step is enqueued on the world's stream; the first call uploads the scene. */
+int ns_world_step(ns_world* world, float dt, int substeps);
+/* Wait for queued steps and report device-side errors (capacity, barrier timeout). */
+int ns_world_synchronize(ns_world* world);
+
+/* Readback (synchronises). Arrays are per body in id order:
+ * pos f64x3, rot f32x4 (x,y,z,s), lin f32x3, ang f32x3. Any pointer may be NULL. */
+int ns_world_get_bodies(ns_world* world, double* pos, float* rot, float* lin, float* ang);
+int ns_world_body_count(const ns_world* world);
+/* FNV-1a digest identical to the reference World::world_state_hash (body_queries.rs:432). */
+int ns_world_state_hash(ns_world* world, uint64_t* out_hash);
+/* Live contacts in id order (same layout as the parity oracle):
+ * ints[8] = id, shape a, shape b, color, point count, flags, sat cache type, manifold count;
+ * features[4]; floats[24] = normal xyz, then per point anchor_a xyz, separation, normal impulse.
+ * Returns the number written (<= capacity) or -1. */
+int ns_world_contact_capacity(ns_world* world);
+int ns_world_get_contacts(ns_world* world, int32_t* ints, uint32_t* features, float* floats, int capacity);
+/* counters[32]: [0] live contacts [1] touching [2..25] per-color constraint counts
+ * [26] fast-body flags seen [27] SAT calls (0 on device) [28] recycled contacts last step
+ * [29] overflow contacts [30] new pairs last step [31] state changes last step */
+int ns_world_counters(ns_world* world, int32_t* counters);
+
+/* Per-step timing of the device phases of the last step, in ms (CUDA events):
+ * [0] broadphase [1] collide [2] state pass + color lists + prepare [3] solve [4] finalize. */
+int ns_world_phase_times(ns_world* world, float* ms5);
+/* Raw CUDA stream (cudaStream_t) the world enqueues on, for callers that time with events. */
+void* ns_world_stream(ns_world* world);
+/* Solver roofline inputs of the last step: [0] awake bodies [1] substeps [2] colored manifolds
+ * [3] colored points [4] static sides [5] joints [6] overflow manifolds [7] restitution on. */
+int ns_world_solver_counts(ns_world* world, int64_t* counts8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,929 @@
+// libnatsel_gpu: host side of the B200 step behind the C ABI in include/natsel_gpu.h.
+//
+// Scene construction mirrors the reference World API (world_runtime.rs:1506 create_body,
+// shape_creation.rs:287 create_shape_internal, body_api.rs:642 update_body_mass_data,
+// joint.rs:164 create_joint) so ids, mass properties and initial graph colors match.
+// The first step uploads the scene; every step after that is one CUDA graph launch
+// with no host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/natsel_gpu.h"
+#include "nsd_solve.cuh"
+
+using namespace nsd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct HostBody {
+  int type = 0, set = 0, local = 0;
+  uint32_t flags = 0;
+  int joint_count = 0;
+  float mass = 0;
+  std::vector<int> shapes;  // creation order
+};
+
+struct HostShape {
+  DShape d;
+  Hull hull;
+  float density = 0;
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct ns_world {
+  ns_world_def def;
+  std::string err;
+  std::vector<HostBody> bodies;
+  std::vector<DSim> asims, ssims;
+  std::vector<DState> states;
+  std::vector<HostShape> shapes;
+  std::vector<AABB> fat;
+  std::vector<DJoint> joints;
+  std::vector<uint32_t> body_mask;
+  std::vector<std::vector<int>> joint_partners;  // per body: bodies a joint keeps from colliding
+
+  bool uploaded = false;
+  int device = 0, sm_count = 0;
+  cudaStream_t stream = nullptr;
+  DW dw;
+  JointRanges jr;
+  std::vector<void*> allocations;
+  void* cub_sort_tmp = nullptr;
+  size_t cub_sort_bytes = 0;
+  void* cub_scan_tmp = nullptr;
+  size_t cub_scan_bytes = 0;
+  int solver_blocks = 1;
+  bool state_shared = false;
+  size_t state_smem = 0;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  float graph_dt = -1.0f;
+  int graph_substeps = -1;
+  cudaEvent_t ev[6] = {};
+  int steps_done = 0;
+  int last_substeps = 0;
+  bool eager = false;
+};
+
+namespace {
+
+int fail(ns_world* w, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (w) w->err = buf; else g_create_error = buf;
+  return code;
+}
+
+#define NS_CUDA(w, call)                                                                   \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail((w), NS_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+  } while (0)
+
+DSim& sim_ref(ns_world* w, const HostBody& b) { return b.set == 2 ? w->asims[b.local] : w->ssims[b.local]; }
+
+int encode(const HostBody& b) { return b.set == 2 ? b.local : -(b.local + 2); }
+
+// world_runtime.rs:1479 sync_body_flags
+void sync_flags(ns_world* w, int bi) {
+  HostBody& b = w->bodies[bi];
+  DSim& s = sim_ref(w, b);
+  s.flags = (s.flags & (kIsFast | kHadToi)) | (b.flags & ~kTransient);
+  if (b.set == 2) w->states[b.local].flags = b.flags & ~kTransient;
+}
+
+struct MassData { float mass; V3 center; M3 inertia; };
+
+MassData shape_mass(const HostShape& hs) {
+  const DShape& s = hs.d;
+  MassData md;
+  if (s.type == kHull) {  // shape_runtime.rs:312 compute_hull_mass
+    md.mass = hs.density * hs.hull.volume;
+    md.center = hs.hull.center;
+    md.inertia = mul_sm(hs.density, hs.hull.central_inertia);
+  } else if (s.type == kSphere) {  // sphere.rs:13 compute_sphere_mass
+    float r = s.sphere.radius;
+    float volume = 4.0f / 3.0f * kPi * r * r * r;
+    float mass = volume * hs.density;
+    float ixx = 0.4f * mass * r * r;
+    md.mass = mass;
+    md.center = s.sphere.center;
+    md.inertia = diag(ixx, ixx, ixx);
+  } else {  // capsule.rs:27 compute_capsule_mass
+    V3 c1 = s.capsule.c1, c2 = s.capsule.c2;
+    float r = s.capsule.radius;
+    float h = distance(c1, c2);
+    float cyl_mass = kPi * r * r * h * hs.density;
+    float sph_mass = (4.0f / 3.0f) * kPi * r * r * r * hs.density;
+    // geometry_queries.rs cylinder_inertia / sphere_inertia
+    float lateral = cyl_mass * (3.0f * r * r + h * h) / 12.0f;
+    float axial = 0.5f * cyl_mass * r * r;
+    M3 inertia = add_mm(diag(lateral, axial, lateral),
+                        diag(0.4f * sph_mass * r * r, 0.4f * sph_mass * r * r, 0.4f * sph_mass * r * r));
+    float st = 0.125f * sph_mass * (3.0f * r + 2.0f * h) * h;
+    inertia.cx.x += st;
+    inertia.cz.z += st;
+    M3 rot = identity_m3();
+    if (h * h > 1000.0f * kMinPositive) rot = matrix_from_quat(quat_between_unit_vectors(v3(0, 1, 0), normalize(c2 - c1)));
+    md.mass = sph_mass + cyl_mass;
+    md.center = 0.5f * (c1 + c2);
+    md.inertia = mul_mm(rot, mul_mm(inertia, transpose(rot)));
+  }
+  return md;
+}
+
+void shape_extent(const HostShape& hs, V3 lc, float* min_e, V3* max_e) {  // shape_runtime.rs:499
+  const DShape& s = hs.d;
+  if (s.type == kCapsule) {
+    float r = s.capsule.radius;
+    *min_e = r;
+    *max_e = max3(abs3(s.capsule.c1 - lc), abs3(s.capsule.c2 - lc)) + v3(r, r, r);
+  } else if (s.type == kSphere) {
+    float r = s.sphere.radius;
+    *min_e = r;
+    *max_e = abs3(s.sphere.center - lc) + v3(r, r, r);
+  } else {  // hull_queries.rs:101
+    *min_e = hs.hull.inner_radius;
+    V3 m = v3(0, 0, 0);
+    for (int i = 0; i < kHullVertexCount; ++i) m = max3(m, abs3(hs.hull.points[i] - lc));
+    *max_e = m;
+  }
+}
+
+// body_api.rs:642 update_body_mass_data (+ :611 update_isotropic_inertia)
+void update_mass(ns_world* w, int bi) {
+  HostBody& b = w->bodies[bi];
+  b.flags &= ~kDirtyMass;
+  b.flags &= ~kGyroscopic;
+  sync_flags(w, bi);
+  b.mass = 0.0f;
+  DSim& s = sim_ref(w, b);
+  s.inertia = m3zero(); s.inv_mass = 0.0f;
+  s.inv_inertia_local = m3zero(); s.inv_inertia_world = m3zero();
+  s.local_center = v3(0, 0, 0);
+  s.min_extent = huge_value();
+  s.max_extent = v3(0, 0, 0);
+  if (b.shapes.empty()) return;
+  if (b.type != NS_DYNAMIC_BODY) {
+    s.cx = s.px; s.cy = s.py; s.cz = s.pz;
+    return;
+  }
+  std::vector<MassData> masses;
+  V3 lc = v3(0, 0, 0);
+  for (auto it = b.shapes.rbegin(); it != b.shapes.rend(); ++it) {  // head of list = newest
+    const HostShape& hs = w->shapes[*it];
+    if (hs.density == 0.0f) { MassData z = {0, v3(0, 0, 0), m3zero()}; masses.push_back(z); continue; }
+    MassData md = shape_mass(hs);
+    b.mass += md.mass;
+    lc = mul_add(lc, md.mass, md.center);
+    masses.push_back(md);
+  }
+  if (b.mass > 0.0f) {
+    s.inv_mass = 1.0f / b.mass;
+    lc = s.inv_mass * lc;
+  }
+  for (const MassData& md : masses) {
+    if (md.mass == 0.0f) continue;
+    s.inertia = add_mm(s.inertia, add_mm(md.inertia, steiner(md.mass, lc - md.center)));
+  }
+  Q q = s.q;
+  if (det(s.inertia) > 0.0f) {
+    s.inv_inertia_local = invert_t(s.inertia);
+    M3 R = matrix_from_quat(q);
+    s.inv_inertia_world = mul_mm(mul_mm(R, s.inv_inertia_local), transpose(R));
+  }
+  Pos old_center = {s.cx, s.cy, s.cz};
+  s.local_center = lc;
+  WXf t;
+  t.p.x = s.px; t.p.y = s.py; t.p.z = s.pz; t.q = q;
+  Pos c = world_point(t, lc);
+  s.cx = c.x; s.cy = c.y; s.cz = c.z;
+  DState& st = w->states[b.local];
+  st.v = st.v + cross(st.w, sub_pos(c, old_center));
+  for (auto it = b.shapes.rbegin(); it != b.shapes.rend(); ++it) {
+    float mn; V3 mx;
+    shape_extent(w->shapes[*it], lc, &mn, &mx);
+    s.min_extent = minf(s.min_extent, mn);
+    s.max_extent = max3(s.max_extent, mx);
+  }
+  if ((s.flags & (kLockAngX | kLockAngY | kLockAngZ)) == (kLockAngX | kLockAngY | kLockAngZ)) {
+    s.inertia = m3zero(); s.inv_inertia_local = m3zero(); s.inv_inertia_world = m3zero();
+  }
+  // body_api.rs:611 update_isotropic_inertia (tolerance 0.2, world_runtime.rs:1256)
+  M3 I = s.inertia;
+  float mean = (I.cx.x + I.cy.y + I.cz.z) / 3.0f;
+  float dx = I.cx.x - mean, dy = I.cy.y - mean, dz = I.cz.z - mean;
+  float off = I.cy.x * I.cy.x + I.cz.x * I.cz.x + I.cz.y * I.cz.y;
+  float dev = dx * dx + dy * dy + dz * dz + 2.0f * off;
+  float tol = 0.2f;
+  if (2.0f * dev > 3.0f * tol * tol * mean * mean) b.flags |= kGyroscopic;
+  else b.flags &= ~kGyroscopic;
+  sync_flags(w, bi);
+}
+
+AABB shape_local_aabb(const HostShape& hs, Q q) {  // shape_runtime.rs:405
+  Xf t = xf(v3(0, 0, 0), q);
+  const DShape& s = hs.d;
+  if (s.type == kHull) return aabb_transform(t, hs.hull.bounds);
+  if (s.type == kSphere) {
+    V3 c = xf_point(t, s.sphere.center);
+    float r = s.sphere.radius;
+    return aabb(c - v3(r, r, r), c + v3(r, r, r));
+  }
+  V3 c1 = xf_point(t, s.capsule.c1), c2 = xf_point(t, s.capsule.c2);
+  float r = s.capsule.radius;
+  return aabb(min3(c1, c2) - v3(r, r, r), max3(c1, c2) + v3(r, r, r));
+}
+
+int create_shape(ns_world* w, int bi, const ns_shape_def* def, HostShape hs) {
+  if (w->uploaded) return fail(w, -1, "scene changes after the first step are not supported"), -1;
+  if (bi < 0 || bi >= (int)w->bodies.size() || !def) return fail(w, -1, "invalid body or shape def"), -1;
+  int sid = (int)w->shapes.size();
+  HostBody& b = w->bodies[bi];
+  DShape& s = hs.d;
+  s.body = bi;
+  s.enc = encode(b);
+  s.is_static = b.type == NS_STATIC_BODY;
+  hs.density = def->density;
+  s.friction = def->friction;
+  s.restitution = def->restitution;
+  s.rolling = def->rolling_resistance;
+  s.category = def->category_bits;
+  s.mask = def->mask_bits;
+  s.group = def->group_index;
+  // shape_creation.rs:199 compute_shape_margin
+  float margin;
+  if (s.type == kSphere) margin = s.sphere.radius;
+  else if (s.type == kCapsule) margin = 0.5f * distance(s.capsule.c2, s.capsule.c1) + s.capsule.radius;
+  else {
+    float mx = 0.0f;
+    for (int i = 0; i < kHullVertexCount; ++i) mx = maxf(mx, distance_sq(hs.hull.points[i], hs.hull.center));
+    margin = sqrtf(mx);
+  }
+  s.aabb_margin = minf(max_aabb_margin(), kAabbMarginFraction * margin);
+  // shape_creation.rs:236 update_shape_aabbs
+  const DSim& sim = sim_ref(w, b);
+  float spec = speculative_distance();
+  Pos p = {sim.px, sim.py, sim.pz};
+  AABB a = offset_aabb(aabb_inflate(shape_local_aabb(hs, sim.q), spec), p);
+  w->fat.push_back(aabb_inflate(a, s.is_static ? spec : s.aabb_margin));
+  s.hull = s.type == kHull ? sid : -1;
+  w->shapes.push_back(hs);
+  b.shapes.push_back(sid);
+  update_mass(w, bi);
+  return sid;
+}
+
+template <class T>
+T* dalloc(ns_world* w, size_t n, int* status) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    *status = fail(w, NS_ERR_CUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    return nullptr;
+  }
+  cudaMemsetAsync(p, 0, bytes, w->stream);
+  w->allocations.push_back(p);
+  return (T*)p;
+}
+
+template <class T>
+int upload(ns_world* w, T* dst, const std::vector<T>& src) {
+  if (src.empty()) return NS_OK;
+  NS_CUDA(w, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, w->stream));
+  return NS_OK;
+}
+
+int upload_world(ns_world* w) {
+  if (w->def.enable_sleep) return fail(w, NS_ERR_UNSUPPORTED, "sleeping islands are not supported");
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  NS_CUDA(w, cudaDeviceGetAttribute(&w->sm_count, cudaDevAttrMultiProcessorCount, w->def.device));
+  NS_CUDA(w, cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 6; ++i) NS_CUDA(w, cudaEventCreate(&w->ev[i]));
+  int st = NS_OK;
+  DW& d = w->dw;
+  memset(&d, 0, sizeof(d));
+  int na = (int)w->asims.size(), ns = (int)w->ssims.size(), nsh = (int)w->shapes.size();
+  int nb = (int)w->bodies.size(), nj = (int)w->joints.size();
+  d.n_awake = na; d.n_static = ns; d.n_shapes = nsh; d.n_bodies = nb; d.n_joints = nj;
+  int cap = w->def.contact_capacity > 0 ? w->def.contact_capacity : 8 * nsh + 4096;
+  cap = (cap + 1023) & ~1023;
+  d.cap = cap;
+  int hs_size = 1;
+  while (hs_size < 4 * cap) hs_size <<= 1;
+  d.hs_mask = hs_size - 1;
+  d.n_words = (cap + 31) / 32;
+  d.cand_cap = cap;
+  d.n_color_blocks = cap / kColorBlock;
+
+  // body -> shape table for finalize (awake bodies)
+  std::vector<int> body_shapes;
+  for (int i = 0; i < nb; ++i) {
+    HostBody& b = w->bodies[i];
+    if (b.set != 2) continue;
+    DSim& s = w->asims[b.local];
+    s.shape_begin = (int)body_shapes.size();
+    for (auto it = b.shapes.rbegin(); it != b.shapes.rend(); ++it) body_shapes.push_back(*it);
+    s.shape_end = (int)body_shapes.size();
+  }
+  std::vector<DShape> dshapes(nsh);
+  std::vector<Hull> hulls(nsh);
+  std::vector<int> large;
+  for (int i = 0; i < nsh; ++i) {
+    dshapes[i] = w->shapes[i].d;
+    hulls[i] = w->shapes[i].hull;
+    if (dshapes[i].is_static && (w->fat[i].hi.x - w->fat[i].lo.x) > 8.0f) large.push_back(i);
+  }
+  d.n_large = (int)large.size();
+  d.n_small = nsh - d.n_large;
+  // joint partner CSR (joint.rs:164: joints without collide_connected disable the pair)
+  std::vector<int> joff(nb + 1, 0), jother;
+  for (int i = 0; i < nb; ++i) {
+    joff[i] = (int)jother.size();
+    if (i < (int)w->joint_partners.size())
+      for (int o : w->joint_partners[i]) jother.push_back(o);
+  }
+  joff[nb] = (int)jother.size();
+  // joints grouped by graph color
+  std::vector<int> jlist;
+  for (int c = 0; c < kGraphColorCount; ++c) {
+    w->jr.off[c] = (int)jlist.size();
+    for (int j = 0; j < nj; ++j)
+      if (w->joints[j].color == c) jlist.push_back(j);
+  }
+  w->jr.off[kGraphColorCount] = (int)jlist.size();
+
+#define ALLOC(field, T, n) do { d.field = dalloc<T>(w, (n), &st); if (!d.field) return st; } while (0)
+  ALLOC(asims, DSim, na); ALLOC(states, DState, na); ALLOC(ssims, DSim, ns);
+  ALLOC(shapes, DShape, nsh); ALLOC(hulls, Hull, nsh); ALLOC(fat, AABB, nsh); ALLOC(moved, int, nsh);
+  ALLOC(body_shapes, int, body_shapes.size()); ALLOC(body_mask, uint32_t, nb);
+  ALLOC(body_joint_off, int, nb + 1); ALLOC(body_joint_other, int, jother.size());
+  ALLOC(contacts, DContact, cap); ALLOC(free_stack, int, cap);
+  ALLOC(hs, unsigned long long, hs_size);
+  ALLOC(changed_bits, uint32_t, d.n_words); ALLOC(changed_list, int, cap); ALLOC(destroyed, int, cap);
+  ALLOC(overflow_list, int, cap); ALLOC(ovf, DOverflow, cap);
+  ALLOC(joints, DJoint, nj); ALLOC(joint_list, int, jlist.size());
+  ALLOC(bp_keys_in, uint32_t, nsh); ALLOC(bp_keys_out, uint32_t, nsh);
+  ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
+  ALLOC(large_list, int, large.size());
+  ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
+  ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
+  ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
+  ALLOC(ctl, Control, 1);
+  CPlanes& P = d.cp;
+  P.cap = cap;
+#define PALLOC(field, T, n) do { P.field = dalloc<T>(w, (n), &st); if (!P.field) return st; } while (0)
+  PALLOC(idx, int4, cap); PALLOC(mass, float4, cap); PALLOC(ia0, float4, cap); PALLOC(ia1, float4, cap);
+  PALLOC(ib1, float4, cap); PALLOC(n, float4, cap); PALLOC(t1, float4, cap); PALLOC(t2, float4, cap);
+  PALLOC(ca, float4, cap); PALLOC(cb, float4, cap); PALLOC(tm, float4, cap); PALLOC(fr, float4, cap);
+  PALLOC(roll, float4, cap); PALLOC(rm, float4, cap);
+  PALLOC(pra, float4, 4 * (size_t)cap); PALLOC(prb, float4, 4 * (size_t)cap);
+  PALLOC(pimp, float4, 4 * (size_t)cap); PALLOC(prest, float, 4 * (size_t)cap);
+#undef PALLOC
+#undef ALLOC
+  if ((st = upload(w, d.asims, w->asims))) return st;
+  if ((st = upload(w, d.states, w->states))) return st;
+  if ((st = upload(w, d.ssims, w->ssims))) return st;
+  if ((st = upload(w, d.shapes, dshapes))) return st;
+  if ((st = upload(w, d.hulls, hulls))) return st;
+  if ((st = upload(w, d.fat, w->fat))) return st;
+  if ((st = upload(w, d.body_shapes, body_shapes))) return st;
+  if ((st = upload(w, d.body_mask, w->body_mask))) return st;
+  if ((st = upload(w, d.body_joint_off, joff))) return st;
+  if ((st = upload(w, d.body_joint_other, jother))) return st;
+  if ((st = upload(w, d.large_list, large))) return st;
+  if ((st = upload(w, d.joint_list, jlist))) return st;
+  std::vector<DJoint> dj = w->joints;
+  if ((st = upload(w, d.joints, dj))) return st;
+  std::vector<int> moved(nsh, 1);
+  if ((st = upload(w, d.moved, moved))) return st;
+  NS_CUDA(w, cudaMemsetAsync(d.hs, 0xff, sizeof(unsigned long long) * (size_t)hs_size, w->stream));
+  Control c0;
+  memset(&c0, 0, sizeof(c0));
+  c0.moved_count = nsh;
+  NS_CUDA(w, cudaMemcpyAsync(d.ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, w->stream));
+  // CUB scratch (sizes depend only on the shape count)
+  NS_CUDA(w, cub::DeviceRadixSort::SortPairs(nullptr, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
+                                              d.bp_vals_in, d.bp_vals_out, nsh));
+  NS_CUDA(w, cub::DeviceScan::ExclusiveSum(nullptr, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh));
+  NS_CUDA(w, cudaMalloc(&w->cub_sort_tmp, std::max<size_t>(w->cub_sort_bytes, 16)));
+  w->allocations.push_back(w->cub_sort_tmp);
+  NS_CUDA(w, cudaMalloc(&w->cub_scan_tmp, std::max<size_t>(w->cub_scan_bytes, 16)));
+  w->allocations.push_back(w->cub_scan_tmp);
+  // state pass keeps every body's color mask in shared memory when it fits
+  int max_smem = 0;
+  NS_CUDA(w, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, w->def.device));
+  size_t need = (size_t)nb * sizeof(uint32_t);
+  w->state_shared = need + 16 * 1024 <= (size_t)max_smem;
+  w->state_smem = w->state_shared ? need : 0;
+  if (w->state_shared && need > 48 * 1024)
+    NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+  // persistent solver grid: every block must be resident (cooperative launch)
+  int per_sm = 0;
+  NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kSolveThreads, 0));
+  int max_blocks = per_sm * w->sm_count;
+  int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : std::max(1, std::min(w->sm_count, (na + kSolveThreads - 1) / kSolveThreads));
+  w->solver_blocks = std::max(1, std::min(want, max_blocks));
+  NS_CUDA(w, cudaStreamSynchronize(w->stream));
+  const char* eager = getenv("NATSEL_EAGER");
+  w->eager = eager && eager[0] == '1';
+  w->uploaded = true;
+  return NS_OK;
+}
+
+int enqueue_step(ns_world* w, float dt, int substeps) {
+  DW d = w->dw;
+  cudaStream_t s = w->stream;
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  p.dt = dt;
+  p.substeps = substeps < 1 ? 1 : substeps;
+  if (dt > 0.0f) {
+    p.inv_dt = 1.0f / dt;
+    p.h = dt / (float)p.substeps;
+    p.inv_h = (float)p.substeps * p.inv_dt;
+  }
+  float hz = minf(w->def.contact_hertz, 0.125f * p.inv_h);
+  p.contact_softness = make_soft(hz, w->def.contact_damping_ratio, p.h);
+  p.static_softness = make_soft(2.0f * hz, 0.5f * w->def.contact_damping_ratio, p.h);
+  p.contact_speed = w->def.contact_speed;
+  p.max_linear_speed = w->def.max_linear_speed;
+  p.restitution_threshold = w->def.restitution_threshold;
+  p.warm_start = w->def.enable_warm_starting ? 1.0f : 0.0f;
+  p.restitution_iterations = w->def.restitution_iterations;
+  p.enable_continuous = w->def.enable_continuous;
+  p.gravity = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
+  int nsh = d.n_shapes;
+  auto blocks = [](int n, int t) { return std::max(1, (n + t - 1) / t); };
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[0], s, cudaEventRecordExternal));
+  // pair update (contact_creation.rs:901)
+  NS_CUDA(w, cudaMemsetAsync(d.seg_count, 0, sizeof(int) * (size_t)nsh, s));
+  NS_CUDA(w, cudaMemsetAsync(d.seg_cursor, 0, sizeof(int) * (size_t)nsh, s));
+  k_hs_rebuild_clear<<<4 * w->sm_count, 256, 0, s>>>(d);
+  k_hs_rebuild_insert<<<4 * w->sm_count, 256, 0, s>>>(d);
+  k_bp_keys<<<blocks(nsh, 256), 256, 0, s>>>(d);
+  NS_CUDA(w, cub::DeviceRadixSort::SortPairs(w->cub_sort_tmp, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
+                                              d.bp_vals_in, d.bp_vals_out, nsh, 0, 32, s));
+  k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d);
+  k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d);
+  NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
+  k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d);
+  k_bp_segsort<<<blocks(nsh, 256), 256, 0, s>>>(d);
+  k_bp_create<<<4 * w->sm_count, 256, 0, s>>>(d);
+  k_bp_finish<<<1, 1, 0, s>>>(d);
+  NS_CUDA(w, cudaMemsetAsync(d.moved, 0, sizeof(int) * (size_t)nsh, s));
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, cudaEventRecordExternal));
+  // narrowphase (collide_pass.rs:164)
+  k_collide<<<blocks(d.cap, 128), 128, 0, s>>>(d);
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, cudaEventRecordExternal));
+  // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
+  k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0);
+  k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d);
+  k_color_scan<<<1, 32, 0, s>>>(d);
+  k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p);
+  k_prepare_overflow<<<8, 128, 0, s>>>(d, p);
+  if (d.n_joints > 0) k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, cudaEventRecordExternal));
+  // solver stages (solver_stages.rs:543)
+  NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
+  {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(w->solver_blocks);
+    cfg.blockDim = dim3(kSolveThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve, d, p, w->jr));
+  }
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, cudaEventRecordExternal));
+  // finalize (solver_integration.rs:435)
+  k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p);
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, cudaEventRecordExternal));
+  NS_CUDA(w, cudaGetLastError());
+  return NS_OK;
+}
+
+int read_control(ns_world* w, Control* c) {
+  NS_CUDA(w, cudaStreamSynchronize(w->stream));
+  NS_CUDA(w, cudaMemcpy(c, w->dw.ctl, sizeof(Control), cudaMemcpyDeviceToHost));
+  return NS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ns_default_world_def(ns_world_def* d) {
+  memset(d, 0, sizeof(*d));
+  d->gravity[1] = -10.0f;
+  d->enable_sleep = 0;
+  d->enable_continuous = 1;
+  d->enable_warm_starting = 1;
+  d->contact_hertz = 30.0f;
+  d->contact_damping_ratio = 10.0f;
+  d->contact_speed = 3.0f;
+  d->max_linear_speed = 400.0f;
+  d->restitution_threshold = 1.0f;
+  d->restitution_iterations = 2;
+  d->joint_hertz = 60.0f;
+  d->joint_damping_ratio = 2.0f;
+}
+
+ns_world* ns_world_create(const ns_world_def* def) {
+  if (!def) { g_create_error = "null world def"; return nullptr; }
+  if (def->enable_sleep) { g_create_error = "enable_sleep must be 0: sleeping islands are not supported"; return nullptr; }
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  if (def->device < 0 || def->device >= count) { g_create_error = "invalid device ordinal"; return nullptr; }
+  ns_world* w = new ns_world();
+  w->def = *def;
+  return w;
+}
+
+void ns_world_destroy(ns_world* w) {
+  if (!w) return;
+  if (w->uploaded) {
+    cudaSetDevice(w->def.device);
+    cudaStreamSynchronize(w->stream);
+    if (w->graph_exec) cudaGraphExecDestroy(w->graph_exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    for (void* p : w->allocations) cudaFree(p);
+    for (int i = 0; i < 6; ++i) if (w->ev[i]) cudaEventDestroy(w->ev[i]);
+    cudaStreamDestroy(w->stream);
+  }
+  delete w;
+}
+
+const char* ns_last_error(const ns_world* w) { return w ? w->err.c_str() : g_create_error.c_str(); }
+
+int ns_create_body(ns_world* w, const ns_body_def* d) {
+  if (!w || !d) return -1;
+  if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
+  if (d->type != NS_STATIC_BODY && d->type != NS_DYNAMIC_BODY) { w->err = "only static and dynamic bodies are supported"; return -1; }
+  int id = (int)w->bodies.size();
+  HostBody b;
+  b.type = d->type;
+  b.set = d->type == NS_STATIC_BODY ? 0 : 2;
+  DSim s;
+  memset(&s, 0, sizeof(s));
+  s.px = d->position[0]; s.py = d->position[1]; s.pz = d->position[2];
+  s.q = quat(v3(d->rotation[0], d->rotation[1], d->rotation[2]), d->rotation[3]);
+  s.cx = s.px; s.cy = s.py; s.cz = s.pz;
+  s.min_extent = huge_value();
+  s.linear_damping = d->linear_damping;
+  s.angular_damping = d->angular_damping;
+  s.gravity_scale = d->gravity_scale;
+  s.safety_factor = 0.5f;
+  s.body_id = id;
+  s.flags = 0;
+  if (d->type == NS_DYNAMIC_BODY) s.flags |= kDynamicFlag;
+  if (d->enable_sleep) s.flags |= kEnableSleepFlag;
+  s.flags |= kEnableRecycling;
+  b.flags = s.flags;
+  if (b.set == 2) {
+    b.local = (int)w->asims.size();
+    w->asims.push_back(s);
+    DState st;
+    memset(&st, 0, sizeof(st));
+    st.v = v3(d->linear_velocity[0], d->linear_velocity[1], d->linear_velocity[2]);
+    st.w = v3(d->angular_velocity[0], d->angular_velocity[1], d->angular_velocity[2]);
+    st.dq = qid();
+    st.flags = s.flags;
+    w->states.push_back(st);
+  } else {
+    b.local = (int)w->ssims.size();
+    w->ssims.push_back(s);
+  }
+  w->bodies.push_back(b);
+  w->body_mask.push_back(0u);
+  return id;
+}
+
+int ns_create_box_shape(ns_world* w, int body, const ns_shape_def* def, float hx, float hy, float hz) {
+  if (!w) return -1;
+  HostShape hs;
+  memset(&hs.d, 0, sizeof(hs.d));
+  hs.d.type = kHull;
+  hs.hull = make_box_hull(hx, hy, hz);
+  return create_shape(w, body, def, hs);
+}
+
+int ns_create_sphere_shape(ns_world* w, int body, const ns_shape_def* def, const float c[3], float r) {
+  if (!w || !c) return -1;
+  HostShape hs;
+  memset(&hs.d, 0, sizeof(hs.d));
+  memset(&hs.hull, 0, sizeof(hs.hull));
+  hs.d.type = kSphere;
+  hs.d.sphere.center = v3(c[0], c[1], c[2]);
+  hs.d.sphere.radius = r;
+  return create_shape(w, body, def, hs);
+}
+
+int ns_create_capsule_shape(ns_world* w, int body, const ns_shape_def* def, const float c1[3],
+                            const float c2[3], float r) {
+  if (!w || !c1 || !c2) return -1;
+  HostShape hs;
+  memset(&hs.d, 0, sizeof(hs.d));
+  memset(&hs.hull, 0, sizeof(hs.hull));
+  V3 a = v3(c1[0], c1[1], c1[2]), b = v3(c2[0], c2[1], c2[2]);
+  if (distance(a, b) < min_capsule_length()) {  // shape_creation.rs:522
+    hs.d.type = kSphere;
+    hs.d.sphere.center = 0.5f * (a + b);
+    hs.d.sphere.radius = r;
+  } else {
+    hs.d.type = kCapsule;
+    hs.d.capsule.c1 = a; hs.d.capsule.c2 = b; hs.d.capsule.radius = r;
+  }
+  return create_shape(w, body, def, hs);
+}
+
+int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa[7], const float fb[7],
+                             int enable_limit, float lower, float upper, int enable_spring, float hertz,
+                             float damping_ratio, float max_motor_torque, int collide_connected) {
+  if (!w || !fa || !fb) return -1;
+  if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
+  int nb = (int)w->bodies.size();
+  if (body_a < 0 || body_b < 0 || body_a >= nb || body_b >= nb || body_a == body_b) { w->err = "invalid joint bodies"; return -1; }
+  HostBody& ba = w->bodies[body_a];
+  HostBody& bb = w->bodies[body_b];
+  if (ba.type != NS_DYNAMIC_BODY && bb.type != NS_DYNAMIC_BODY) { w->err = "a joint needs a dynamic body"; return -1; }
+  DJoint j;
+  memset(&j, 0, sizeof(j));
+  j.body_a = body_a; j.body_b = body_b;
+  j.enc_a = encode(ba); j.enc_b = encode(bb);
+  j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
+  j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
+  j.constraint_hertz = w->def.joint_hertz;
+  j.constraint_damping_ratio = w->def.joint_damping_ratio;
+  j.constraint_softness.bias_rate = 0.0f; j.constraint_softness.mass_scale = 1.0f; j.constraint_softness.impulse_scale = 0.0f;
+  j.enable_limit = enable_limit != 0; j.lower_angle = lower; j.upper_angle = upper;
+  j.enable_spring = enable_spring != 0; j.hertz = hertz; j.damping_ratio = damping_ratio;
+  j.max_motor_torque = max_motor_torque; j.enable_motor = max_motor_torque > 0.0f;
+  // constraint_graph.rs:256 assign_joint_color
+  uint32_t& ma = w->body_mask[body_a];
+  uint32_t& mb = w->body_mask[body_b];
+  int color = kOverflowIndex;
+  if (ba.type == NS_DYNAMIC_BODY && bb.type == NS_DYNAMIC_BODY) {
+    uint32_t avail = ~(ma | mb) & ((1u << kDynamicColorCount) - 1u);
+    if (avail) { color = __builtin_ctz(avail); ma |= 1u << color; mb |= 1u << color; }
+  } else {
+    uint32_t& m = ba.type == NS_DYNAMIC_BODY ? ma : mb;
+    uint32_t avail = ~m & (((1u << kOverflowIndex) - 1u) & ~1u);
+    if (avail) { color = 31 - __builtin_clz(avail); m |= 1u << color; }
+  }
+  j.color = color;
+  ba.joint_count++;
+  bb.joint_count++;
+  if (!collide_connected) {
+    if ((int)w->joint_partners.size() < nb) w->joint_partners.resize(nb);
+    w->joint_partners[body_a].push_back(body_b);
+    w->joint_partners[body_b].push_back(body_a);
+  }
+  w->joints.push_back(j);
+  return (int)w->joints.size() - 1;
+}
+
+int ns_world_step(ns_world* w, float dt, int substeps) {
+  if (!w) return NS_ERR_INVALID;
+  if (!(dt > 0.0f)) return fail(w, NS_ERR_INVALID, "dt must be positive");
+  if (!w->uploaded) {
+    int st = upload_world(w);
+    if (st) return st;
+  }
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  if (w->asims.empty()) return NS_OK;
+  if (w->eager) {
+    int st = enqueue_step(w, dt, substeps);
+    if (st) return st;
+    w->steps_done++;
+    w->last_substeps = substeps;
+    return NS_OK;
+  }
+  if (!w->graph_exec || w->graph_dt != dt || w->graph_substeps != substeps) {
+    if (w->graph_exec) { cudaGraphExecDestroy(w->graph_exec); w->graph_exec = nullptr; }
+    if (w->graph) { cudaGraphDestroy(w->graph); w->graph = nullptr; }
+    NS_CUDA(w, cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue_step(w, dt, substeps);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(w->stream, &g);
+    cudaGetLastError();
+    bool ok = st == NS_OK && e == cudaSuccess && g != nullptr;
+    if (ok && cudaGraphInstantiate(&w->graph_exec, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      w->graph_exec = nullptr;
+      ok = false;
+    }
+    if (!ok) {
+      // The step runs without a graph when capture is refused (for example a driver that
+      // does not capture cooperative launches); results are identical, launches cost more.
+      if (g) cudaGraphDestroy(g);
+      w->eager = true;
+      w->err = "graph capture unavailable; stepping without a CUDA graph";
+      int st2 = enqueue_step(w, dt, substeps);
+      if (st2) return st2;
+      w->steps_done++;
+      w->last_substeps = substeps;
+      return NS_OK;
+    }
+    w->graph = g;
+    w->graph_dt = dt;
+    w->graph_substeps = substeps;
+  }
+  NS_CUDA(w, cudaGraphLaunch(w->graph_exec, w->stream));
+  w->steps_done++;
+  w->last_substeps = substeps;
+  return NS_OK;
+}
+
+int ns_world_synchronize(ns_world* w) {
+  if (!w) return NS_ERR_INVALID;
+  if (!w->uploaded) return NS_OK;
+  Control c;
+  int st = read_control(w, &c);
+  if (st) return st;
+  if (c.error == kErrCapacity) return fail(w, NS_ERR_CAPACITY, "device capacity exceeded (contacts or pairs)");
+  if (c.error == kErrTimeout) return fail(w, NS_ERR_TIMEOUT, "solver grid barrier timed out");
+  if (c.error) return fail(w, c.error, "device error %d", c.error);
+  return NS_OK;
+}
+
+int ns_world_body_count(const ns_world* w) { return w ? (int)w->bodies.size() : -1; }
+
+int ns_world_get_bodies(ns_world* w, double* pos, float* rot, float* lin, float* ang) {
+  if (!w) return NS_ERR_INVALID;
+  if (w->uploaded) {
+    int st = ns_world_synchronize(w);
+    if (st) return st;
+    if (!w->asims.empty()) {
+      NS_CUDA(w, cudaMemcpy(w->asims.data(), w->dw.asims, sizeof(DSim) * w->asims.size(), cudaMemcpyDeviceToHost));
+      NS_CUDA(w, cudaMemcpy(w->states.data(), w->dw.states, sizeof(DState) * w->states.size(), cudaMemcpyDeviceToHost));
+    }
+  }
+  for (size_t i = 0; i < w->bodies.size(); ++i) {
+    const HostBody& b = w->bodies[i];
+    const DSim& s = b.set == 2 ? w->asims[b.local] : w->ssims[b.local];
+    if (pos) { pos[3 * i] = s.px; pos[3 * i + 1] = s.py; pos[3 * i + 2] = s.pz; }
+    if (rot) { rot[4 * i] = s.q.v.x; rot[4 * i + 1] = s.q.v.y; rot[4 * i + 2] = s.q.v.z; rot[4 * i + 3] = s.q.s; }
+    V3 v = v3(0, 0, 0), wv = v3(0, 0, 0);
+    if (b.set == 2) { v = w->states[b.local].v; wv = w->states[b.local].w; }
+    if (lin) { lin[3 * i] = v.x; lin[3 * i + 1] = v.y; lin[3 * i + 2] = v.z; }
+    if (ang) { ang[3 * i] = wv.x; ang[3 * i + 1] = wv.y; ang[3 * i + 2] = wv.z; }
+  }
+  return NS_OK;
+}
+
+int ns_world_state_hash(ns_world* w, uint64_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  size_t n = w->bodies.size();
+  std::vector<double> pos(3 * n);
+  std::vector<float> rot(4 * n), lin(3 * n), ang(3 * n);
+  int st = ns_world_get_bodies(w, pos.data(), rot.data(), lin.data(), ang.data());
+  if (st) return st;
+  const uint64_t prime = 1099511628211ull;
+  uint64_t h = 14695981039346656037ull;
+  auto mixf = [&](float f) { uint32_t b; memcpy(&b, &f, 4); h = (h ^ (uint64_t)b) * prime; };
+  auto mixd = [&](double d) { uint64_t b; memcpy(&b, &d, 8); h = (h ^ b) * prime; };
+  for (size_t i = 0; i < n; ++i) {
+    mixd(pos[3 * i]); mixd(pos[3 * i + 1]); mixd(pos[3 * i + 2]);
+    mixf(rot[4 * i]); mixf(rot[4 * i + 1]); mixf(rot[4 * i + 2]); mixf(rot[4 * i + 3]);
+    if (w->bodies[i].set == 2) {
+      mixf(lin[3 * i]); mixf(lin[3 * i + 1]); mixf(lin[3 * i + 2]);
+      mixf(ang[3 * i]); mixf(ang[3 * i + 1]); mixf(ang[3 * i + 2]);
+    }
+  }
+  *out = h;
+  return NS_OK;
+}
+
+int ns_world_contact_capacity(ns_world* w) {
+  if (!w) return -1;
+  if (!w->uploaded) return 0;
+  return w->dw.cap;
+}
+
+int ns_world_get_contacts(ns_world* w, int32_t* ints, uint32_t* feats, float* fl, int capacity) {
+  if (!w || !ints || !feats || !fl) return -1;
+  if (!w->uploaded) return 0;
+  if (ns_world_synchronize(w)) return -1;
+  std::vector<DContact> cs(w->dw.cap);
+  if (cudaMemcpy(cs.data(), w->dw.contacts, sizeof(DContact) * cs.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  int n = 0;
+  for (size_t i = 0; i < cs.size() && n < capacity; ++i) {
+    const DContact& c = cs[i];
+    if (!c.alive) continue;
+    int32_t* I = ints + 8 * n;
+    uint32_t* F = feats + 4 * n;
+    float* D = fl + 24 * n;
+    int pc = c.manifold_count > 0 ? c.manifold.point_count : 0;
+    I[0] = (int32_t)i; I[1] = c.shape_a; I[2] = c.shape_b; I[3] = c.color; I[4] = pc;
+    I[5] = (int32_t)c.flags; I[6] = c.sat.type; I[7] = c.manifold_count;
+    for (int k = 0; k < 4; ++k) F[k] = k < pc ? c.manifold.points[k].feature_id : 0u;
+    for (int k = 0; k < 24; ++k) D[k] = 0.0f;
+    if (pc > 0) {
+      D[0] = c.manifold.normal.x; D[1] = c.manifold.normal.y; D[2] = c.manifold.normal.z;
+      for (int k = 0; k < pc; ++k) {
+        D[3 + 5 * k] = c.manifold.points[k].anchor_a.x;
+        D[4 + 5 * k] = c.manifold.points[k].anchor_a.y;
+        D[5 + 5 * k] = c.manifold.points[k].anchor_a.z;
+        D[6 + 5 * k] = c.manifold.points[k].separation;
+        D[7 + 5 * k] = c.manifold.points[k].normal_impulse;
+      }
+    }
+    n++;
+  }
+  return n;
+}
+
+int ns_world_counters(ns_world* w, int32_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  for (int i = 0; i < 32; ++i) out[i] = 0;
+  if (!w->uploaded) return NS_OK;
+  Control c;
+  int st = read_control(w, &c);
+  if (st) return st;
+  std::vector<DContact> cs(w->dw.cap);
+  NS_CUDA(w, cudaMemcpy(cs.data(), w->dw.contacts, sizeof(DContact) * cs.size(), cudaMemcpyDeviceToHost));
+  for (const DContact& ct : cs) {
+    if (!ct.alive) continue;
+    out[0]++;
+    if (ct.flags & cTouching) out[1]++;
+  }
+  for (int k = 0; k < kOverflowIndex; ++k) out[2 + k] = c.color_count[k] + 0;
+  for (int k = 0; k < kOverflowIndex; ++k) out[2 + k] = 0;
+  for (const DContact& ct : cs)
+    if (ct.alive && (ct.flags & cTouching) && ct.color >= 0) out[2 + ct.color]++;
+  out[26] = c.fast_flags;
+  out[27] = 0;
+  out[28] = c.recycled;
+  out[29] = c.overflow_count;
+  out[30] = c.new_pairs;
+  out[31] = c.changed_count;
+  return NS_OK;
+}
+
+int ns_world_phase_times(ns_world* w, float* ms) {
+  if (!w || !ms) return NS_ERR_INVALID;
+  if (!w->uploaded || w->steps_done == 0) { for (int i = 0; i < 5; ++i) ms[i] = 0; return NS_OK; }
+  NS_CUDA(w, cudaStreamSynchronize(w->stream));
+  for (int i = 0; i < 5; ++i) NS_CUDA(w, cudaEventElapsedTime(&ms[i], w->ev[i], w->ev[i + 1]));
+  return NS_OK;
+}
+
+void* ns_world_stream(ns_world* w) { return w ? (void*)w->stream : nullptr; }
+
+int ns_world_solver_counts(ns_world* w, int64_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  for (int i = 0; i < 8; ++i) out[i] = 0;
+  out[0] = (int64_t)w->asims.size();
+  out[1] = w->last_substeps;
+  out[5] = (int64_t)w->joints.size();
+  if (!w->uploaded) return NS_OK;
+  Control c;
+  int st = read_control(w, &c);
+  if (st) return st;
+  int total = c.color_offset[kOverflowIndex];
+  std::vector<int4> idx(std::max(total, 1));
+  if (total > 0)
+    NS_CUDA(w, cudaMemcpy(idx.data(), w->dw.cp.idx, sizeof(int4) * total, cudaMemcpyDeviceToHost));
+  int64_t points = 0, stat = 0;
+  for (int k = 0; k < total; ++k) {
+    points += idx[k].w & 255;
+    stat += (idx[k].x < 0) + (idx[k].y < 0);
+  }
+  out[2] = total;
+  out[3] = points;
+  out[4] = stat;
+  out[6] = c.overflow_count;
+  out[7] = c.any_restitution;
+  return NS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,892 @@
+// Step kernels. One world step is: pair update (sort-and-sweep) -> contact
+// creation -> collide -> ordered state pass (graph coloring) -> color
+// partition + constraint prepare -> persistent colored solver -> finalize.
+// Each kernel cites the reference stage it replaces; arithmetic keeps the
+// reference operand order so results match the reference bit for bit.
+#pragma once
+#include <cub/cub.cuh>
+#include "nsd_types.cuh"
+
+namespace nsd {
+
+constexpr int kStatePassThreads = 1024;
+constexpr int kColorBlock = 1024;
+constexpr int kSolveThreads = 256;
+constexpr unsigned long long kHsEmpty = ~0ull;
+constexpr unsigned long long kHsTomb = ~0ull - 1ull;
+
+// Error codes mirrored from natsel_gpu.h.
+constexpr int kErrCapacity = 3;
+constexpr int kErrTimeout = 4;
+
+struct DW {
+  DSim* asims; DState* states; int n_awake;
+  DSim* ssims; int n_static;
+  DShape* shapes; Hull* hulls; AABB* fat; int* moved; int n_shapes;
+  int* body_shapes;                 // shape ids grouped per awake body (DSim shape range)
+  uint32_t* body_mask; int n_bodies;
+  int* body_joint_off; int* body_joint_other;  // joint partners with collision disabled
+  DContact* contacts; int cap;
+  int* free_stack;
+  unsigned long long* hs; int hs_mask;
+  uint32_t* changed_bits; int* changed_list; int* destroyed; int n_words;
+  int* overflow_list;
+  CPlanes cp;
+  DOverflow* ovf;
+  DJoint* joints; int n_joints; int* joint_list;
+  // broadphase scratch
+  uint32_t* bp_keys_in; uint32_t* bp_keys_out; int* bp_vals_in; int* bp_vals_out;
+  int n_small; int* large_list; int n_large;
+  int* seg_count; int* seg_off; int* seg_cursor;
+  unsigned long long* cand; unsigned long long* sorted_keys; int cand_cap;
+  int* block_color;                 // per color-partition block x 24
+  int n_color_blocks;
+  Control* ctl;
+};
+
+struct JointRanges { int off[25]; };
+
+// ---------------------------------------------------------------------------
+// Small device helpers
+
+__device__ __forceinline__ uint32_t float_sort_key(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ void raise_error(Control* c, int code) { atomicCAS(&c->error, 0, code); }
+
+// hash_set.rs:25 shape_pair_key with child 0
+__device__ __forceinline__ unsigned long long pair_key(int s1, int s2) {
+  const unsigned long long mask = (1ull << 22) - 1ull;
+  unsigned long long a = mask & (unsigned long long)(long long)s1;
+  unsigned long long b = mask & (unsigned long long)(long long)s2;
+  if (s1 < s2) return (a << 42) | (b << 20);
+  return (b << 42) | (a << 20);
+}
+
+__device__ __forceinline__ uint32_t hs_hash(unsigned long long k) {
+  k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+  return (uint32_t)k;
+}
+__device__ bool hs_contains(const DW& w, unsigned long long k) {
+  uint32_t i = hs_hash(k) & (uint32_t)w.hs_mask;
+  for (int probe = 0; probe <= w.hs_mask; ++probe) {
+    unsigned long long v = w.hs[i];
+    if (v == k) return true;
+    if (v == kHsEmpty) return false;
+    i = (i + 1) & (uint32_t)w.hs_mask;
+  }
+  return false;
+}
+__device__ void hs_insert(const DW& w, unsigned long long k) {
+  uint32_t i = hs_hash(k) & (uint32_t)w.hs_mask;
+  for (int probe = 0; probe <= w.hs_mask; ++probe) {
+    unsigned long long v = w.hs[i];
+    if (v == kHsEmpty || v == kHsTomb) {
+      if (atomicCAS(&w.hs[i], v, k) == v) return;
+      continue;  // lost the race for this slot; re-read it
+    }
+    i = (i + 1) & (uint32_t)w.hs_mask;
+  }
+  raise_error(w.ctl, kErrCapacity);
+}
+__device__ void hs_erase(const DW& w, unsigned long long k) {
+  uint32_t i = hs_hash(k) & (uint32_t)w.hs_mask;
+  for (int probe = 0; probe <= w.hs_mask; ++probe) {
+    unsigned long long v = w.hs[i];
+    if (v == k) { w.hs[i] = kHsTomb; atomicAdd(&w.ctl->tombstones, 1); return; }
+    if (v == kHsEmpty) return;
+    i = (i + 1) & (uint32_t)w.hs_mask;
+  }
+}
+
+__device__ __forceinline__ const DSim& sim_of(const DW& w, int enc) {
+  return enc >= 0 ? w.asims[enc] : w.ssims[-enc - 2];
+}
+
+// ---------------------------------------------------------------------------
+// Pair update (contact_creation.rs:901 update_broad_phase_pairs). The reference's tree
+// traversal yields every overlapping fat-AABB pair with at least one moved proxy; keys are
+// sorted before contacts are created, so any search that finds the same set is equivalent.
+// Here: a sort-and-sweep along x over the small proxies plus a direct test against the few
+// large static proxies.
+
+__global__ void k_hs_rebuild_clear(DW w) {
+  if (w.ctl->hs_rebuild == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= w.hs_mask; i += gridDim.x * blockDim.x)
+    w.hs[i] = kHsEmpty;
+}
+__global__ void k_hs_rebuild_insert(DW w) {
+  if (w.ctl->hs_rebuild == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.cap; i += gridDim.x * blockDim.x) {
+    const DContact& c = w.contacts[i];
+    if (c.alive) hs_insert(w, pair_key(c.shape_a, c.shape_b));
+  }
+}
+
+__global__ void k_bp_keys(DW w) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n_shapes) return;
+  const DShape& s = w.shapes[i];
+  AABB f = w.fat[i];
+  float width = f.hi.x - f.lo.x;
+  bool large = s.is_static && width > 8.0f;
+  w.bp_keys_in[i] = large ? 0xffffffffu : float_sort_key(f.lo.x);
+  w.bp_vals_in[i] = i;
+  if (!large) atomicMax(&w.ctl->max_width_bits, __float_as_int(fmaxf(width, 0.0f)));
+}
+
+// contact_creation.rs:151 should_create_pair for the filters this path supports
+__device__ bool should_create_pair(const DW& w, int a, int b) {
+  const DShape& A = w.shapes[a];
+  const DShape& B = w.shapes[b];
+  if (A.body == B.body) return false;
+  if (A.group == B.group && A.group != 0) {
+    if (!(A.group > 0)) return false;
+  } else if (!((A.mask & B.category) != 0 && (A.category & B.mask) != 0)) {
+    return false;
+  }
+  if (A.is_static && B.is_static) return false;  // contact_creation.rs:113 should_bodies_collide
+  for (int j = w.body_joint_off[A.body]; j < w.body_joint_off[A.body + 1]; ++j)
+    if (w.body_joint_other[j] == B.body) return false;
+  return true;
+}
+
+__device__ void emit_pair(const DW& w, int a, int b) {
+  if (!aabb_overlaps(w.fat[a], w.fat[b])) return;
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  if (!should_create_pair(w, lo, hi)) return;
+  unsigned long long k = pair_key(lo, hi);
+  if (hs_contains(w, k)) return;
+  int slot = atomicAdd(&w.ctl->cand_count, 1);
+  if (slot >= w.cand_cap) { raise_error(w.ctl, kErrCapacity); return; }
+  w.cand[slot] = k;
+  atomicAdd(&w.seg_count[lo], 1);
+}
+
+__device__ int lower_bound_u32(const uint32_t* keys, int n, uint32_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (keys[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_bp_query(DW w) {
+  if (w.ctl->moved_count == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n_small) return;
+  int m = w.bp_vals_out[i];
+  if (!w.moved[m]) return;
+  AABB fm = w.fat[m];
+  float max_w = __int_as_float(w.ctl->max_width_bits);
+  // Conservative start: any proxy whose x-interval can reach fm.lo.x. The exact overlap
+  // test below decides, so a wider scan never changes the result.
+  float start_x = fm.lo.x - (max_w * 1.001f + 1e-3f);
+  int j = lower_bound_u32(w.bp_keys_out, w.n_small, float_sort_key(start_x));
+  uint32_t stop = float_sort_key(fm.hi.x);
+  for (; j < w.n_small; ++j) {
+    if (w.bp_keys_out[j] > stop) break;
+    int b = w.bp_vals_out[j];
+    if (b == m) continue;
+    if (w.moved[b] && b < m) continue;  // the smaller moved proxy of a pair reports it
+    if (w.shapes[m].is_static && w.shapes[b].is_static) continue;
+    emit_pair(w, m, b);
+  }
+}
+
+__global__ void k_bp_large(DW w) {
+  if (w.ctl->moved_count == 0 || w.n_large == 0) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= w.n_shapes) return;
+  const DShape& S = w.shapes[s];
+  if (S.is_static && (w.fat[s].hi.x - w.fat[s].lo.x) > 8.0f) return;  // large itself
+  if (S.is_static) return;                                             // static vs static
+  for (int k = 0; k < w.n_large; ++k) {
+    int L = w.large_list[k];
+    if (!w.moved[s] && !w.moved[L]) continue;
+    emit_pair(w, s, L);
+  }
+}
+
+__global__ void k_bp_scatter(DW w) {
+  int n = w.ctl->cand_count;
+  if (n > w.cand_cap) n = w.cand_cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long k = w.cand[i];
+    int lo = (int)((k >> 42) & ((1ull << 22) - 1ull));
+    int pos = w.seg_off[lo] + atomicAdd(&w.seg_cursor[lo], 1);
+    w.sorted_keys[pos] = k;
+  }
+}
+
+__global__ void k_bp_segsort(DW w) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= w.n_shapes) return;
+  int n = w.seg_count[s];
+  if (n < 2) return;
+  unsigned long long* a = w.sorted_keys + w.seg_off[s];
+  for (int i = 1; i < n; ++i) {
+    unsigned long long v = a[i];
+    int j = i - 1;
+    while (j >= 0 && a[j] > v) { a[j + 1] = a[j]; --j; }
+    a[j + 1] = v;
+  }
+}
+
+// contact_creation.rs:219 create_contact. Contact ids come from the LIFO id pool
+// (id_pool.rs): the k-th new pair in key order takes the k-th id popped.
+__global__ void k_bp_create(DW w) {
+  int n = w.ctl->cand_count;
+  if (n > w.cand_cap) n = w.cand_cap;
+  int F = w.ctl->pool_top, N0 = w.ctl->pool_next;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    int id = k < F ? w.free_stack[F - 1 - k] : N0 + (k - F);
+    if (id >= w.cap) { raise_error(w.ctl, kErrCapacity); continue; }
+    unsigned long long key = w.sorted_keys[k];
+    int sa = (int)((key >> 42) & ((1ull << 22) - 1ull));
+    int sb = (int)((key >> 20) & ((1ull << 22) - 1ull));
+    int ta = w.shapes[sa].type, tb = w.shapes[sb].type;
+    // contact_creation.rs:65 registers: capsule > sphere, hull > sphere, hull > capsule
+    bool primary = ta == tb || (ta == kCapsule && tb == kSphere) ||
+                   (ta == kHull && (tb == kSphere || tb == kCapsule));
+    if (!primary) { int t = sa; sa = sb; sb = t; }
+    const DShape& A = w.shapes[sa];
+    const DShape& B = w.shapes[sb];
+    DContact c;
+    memset(&c, 0, sizeof(c));
+    c.shape_a = sa; c.shape_b = sb;
+    c.body_a = A.body; c.body_b = B.body;
+    c.enc_a = A.enc; c.enc_b = B.enc;
+    c.color = -1; c.local = -1; c.alive = 1;
+    const DSim& simA = sim_of(w, A.enc);
+    const DSim& simB = sim_of(w, B.enc);
+    uint32_t flags = 0;
+    if (A.is_static || B.is_static) flags |= cStatic;
+    flags |= cSpeculative;
+    if ((simA.flags & kEnableRecycling) && (simB.flags & kEnableRecycling)) flags |= cRecycle;
+    c.flags = flags;
+    float ra = A.type == kSphere ? A.sphere.radius : (A.type == kCapsule ? A.capsule.radius : 0.0f);
+    float rb = B.type == kSphere ? B.sphere.radius : (B.type == kCapsule ? B.capsule.radius : 0.0f);
+    c.rolling = maxf(A.rolling, B.rolling) * maxf(ra, rb);
+    c.sat = SATCache();
+    c.simplex = SimplexCache();
+    w.contacts[id] = c;
+    hs_insert(w, key);
+  }
+}
+
+__global__ void k_bp_finish(DW w) {
+  Control* c = w.ctl;
+  int n = c->cand_count;
+  if (n > w.cand_cap) n = w.cand_cap;
+  int F = c->pool_top, N0 = c->pool_next;
+  c->pool_top = F > n ? F - n : 0;
+  c->pool_next = N0 + (n > F ? n - F : 0);
+  c->new_pairs = n;
+  c->cand_count = 0;
+  c->moved_count = 0;
+  c->max_width_bits = 0;
+  c->recycled = 0;
+  c->hs_rebuild = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Narrowphase (collide_pass.rs:541 collide_one_contact, contact_update.rs:43-468)
+
+__device__ bool update_contact(const DW& w, DContact& c, V3 lca, WXf xa, V3 lcb, WXf xb) {
+  const DShape& A = w.shapes[c.shape_a];
+  const DShape& B = w.shapes[c.shape_b];
+  LocalManifold lm;
+  Xf b2a = inv_mul_wxf(xa, xb);
+  if (A.type == kSphere) {
+    collide_spheres(&lm, A.sphere, B.sphere, b2a);
+  } else if (A.type == kCapsule) {
+    if (B.type == kSphere) collide_capsule_sphere(&lm, A.capsule, B.sphere, b2a);
+    else collide_capsules(&lm, A.capsule, B.capsule, b2a);
+  } else {
+    const Hull& ha = w.hulls[A.hull];
+    if (B.type == kSphere) collide_hull_sphere(&lm, ha, B.sphere, b2a, &c.simplex);
+    else if (B.type == kCapsule) collide_hull_capsule(&lm, ha, B.capsule, b2a, &c.simplex);
+    else collide_hulls(&lm, ha, w.hulls[B.hull], b2a, &c.sat, nullptr);
+  }
+  if (lm.point_count == 0) {
+    c.manifold_count = 0;
+    c.flags &= ~cSimTouching;
+    return false;
+  }
+  ManifoldPoint old_points[4];
+  int old_count = 0;
+  if (c.manifold_count == 0) {
+    memset(&c.manifold, 0, sizeof(Manifold));
+    c.manifold_count = 1;
+  } else {
+    old_count = c.manifold.point_count;
+    for (int i = 0; i < old_count; ++i) old_points[i] = c.manifold.points[i];
+  }
+  Manifold& m = c.manifold;
+  m.point_count = lm.point_count;
+  M3 ma = matrix_from_quat(xa.q);
+  m.normal = mul_mv(ma, lm.normal);
+  for (int i = 0; i < lm.point_count; ++i) {
+    ManifoldPoint t;
+    memset(&t, 0, sizeof(t));
+    t.anchor_a = mul_mv(ma, lm.points[i].point);
+    t.anchor_b = t.anchor_a + sub_pos(xa.p, xb.p);
+    t.separation = lm.points[i].separation;
+    t.feature_id = make_feature_id(lm.points[i].pair);
+    m.points[i] = t;
+  }
+  for (int i = 0; i < lm.point_count; ++i) {
+    ManifoldPoint p2 = m.points[i];
+    p2.total_normal_impulse = 0.0f;
+    p2.persisted = 0;
+    for (int j = 0; j < old_count; ++j) {
+      if (p2.feature_id == old_points[j].feature_id) {
+        p2.normal_impulse = old_points[j].normal_impulse;
+        p2.persisted = 1;
+        old_points[j].feature_id = 0xffffffffu;
+        break;
+      }
+    }
+    if (!p2.persisted) p2.normal_impulse = 0.0f;
+    m.points[i] = p2;
+  }
+  // world_runtime.rs:1305 mix_friction / mix_restitution
+  c.friction = sqrtf(A.friction * B.friction);
+  c.restitution = maxf(A.restitution, B.restitution);
+  if (A.rolling > 0.0f || B.rolling > 0.0f) {
+    float rA = A.type == kSphere ? A.sphere.radius
+               : (A.type == kCapsule ? A.capsule.radius : 0.25f * w.hulls[A.hull].inner_radius);
+    float rB = B.type == kSphere ? B.sphere.radius
+               : (B.type == kCapsule ? B.capsule.radius : 0.25f * w.hulls[B.hull].inner_radius);
+    c.rolling = maxf(A.rolling, B.rolling) * maxf(rA, rB);
+  } else {
+    c.rolling = 0.0f;
+  }
+  V3 tva = rotate(xa.q, v3(0, 0, 0));
+  V3 tvb = rotate(xb.q, v3(0, 0, 0));
+  c.tangent_velocity = tva - tvb;
+  V3 ca = rotate(xa.q, lca), cb = rotate(xb.q, lcb);
+  for (int j = 0; j < m.point_count; ++j) {
+    m.points[j].anchor_a = m.points[j].anchor_a - ca;
+    m.points[j].anchor_b = m.points[j].anchor_b - cb;
+  }
+  c.flags |= cSimTouching;
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_collide(DW w) {
+  for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
+    if (!w.contacts[cid].alive) continue;
+    DContact c = w.contacts[cid];
+    bool changed = false;
+    if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
+      c.flags |= cSimDisjoint;
+      c.flags &= ~cSimTouching;
+      w.contacts[cid].flags = c.flags;
+      atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+      continue;
+    }
+    const DSim& sa = sim_of(w, c.enc_a);
+    const DSim& sb = sim_of(w, c.enc_b);
+    bool was_touching = (c.flags & cSimTouching) != 0;
+    WXf xa, xb;
+    xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
+    xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
+    bool is_fast = ((sa.flags | sb.flags) & kIsFast) != 0;
+    float recycle = contact_recycle_distance();
+    float spec = speculative_distance();
+    float recycle_nt = minf(recycle, spec);
+    float tol = was_touching ? recycle : recycle_nt;
+    bool recycled = false;
+    if (!is_fast && recycle > 0.0f && (c.flags & cRelativeValid) && (c.flags & cRecycle)) {
+      // collide_pass.rs:606-687 contact recycling
+      float ang_a = dot_quat(xa.q, c.cached_rot_a);
+      float ang_b = dot_quat(xb.q, c.cached_rot_b);
+      float ang = minf(ang_a * ang_a, ang_b * ang_b);
+      Xf x = inv_mul_wxf(xa, xb);
+      Xf xc = c.cached_rel;
+      V3 mea = c.enc_a < -1 ? v3(0, 0, 0) : sa.max_extent;
+      V3 meb = c.enc_b < -1 ? v3(0, 0, 0) : sb.max_extent;
+      V3 me = max3(mea, meb);
+      float dsq = distance_sq(x.p, xc.p);
+      if (ang > kRecycleAngular && dsq < tol * tol) {
+        float dist = sqrtf(dsq);
+        float slack = tol - dist;
+        Q qr = inv_mul_quat(xc.q, x.q);
+        V3 arc = modified_cross(abs3(qr.v), me);
+        float arc_sq = 4.0f * length_sq(arc);
+        if (arc_sq < slack * slack) {
+          Q dqa = mul_quat(xa.q, conjugate(c.cached_rot_a));
+          Q dqb = mul_quat(xb.q, conjugate(c.cached_rot_b));
+          M3 ma = matrix_from_quat(dqa), mb = matrix_from_quat(dqb);
+          Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+          V3 dc = sub_pos(cb, ca);
+          if (c.manifold_count > 0) {
+            Manifold& m = c.manifold;
+            V3 n = m.normal;
+            for (int i = 0; i < m.point_count; ++i) {
+              V3 ra = mul_mv(ma, m.points[i].anchor_a);
+              V3 rb = mul_mv(mb, m.points[i].anchor_b);
+              V3 dp = dc + (rb - ra);
+              m.points[i].separation = m.points[i].base_separation + dot(dp, n);
+              m.points[i].normal_velocity = 0.0f;
+              m.points[i].persisted = 1;
+            }
+          }
+          recycled = true;
+          atomicAdd(&w.ctl->recycled, 1);
+        }
+      }
+    }
+    if (!recycled) {
+      c.cached_rot_a = xa.q;
+      c.cached_rot_b = xb.q;
+      c.cached_rel = inv_mul_wxf(xa, xb);
+      c.flags |= cRelativeValid;
+      bool touching = update_contact(w, c, sa.local_center, xa, sb.local_center, xb);
+      if (touching && !was_touching) { c.flags |= cSimStarted; changed = true; }
+      else if (!touching && was_touching) { c.flags |= cSimStopped; changed = true; }
+      if (touching && c.manifold_count > 0) {
+        for (int i = 0; i < c.manifold.point_count; ++i)
+          c.manifold.points[i].base_separation = c.manifold.points[i].separation;
+      }
+    }
+    w.contacts[cid] = c;
+    if (changed) atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ordered state pass (collide_pass.rs:386) with greedy coloring
+// (constraint_graph.rs:113/200). One block: the changed ids are compacted in id order,
+// then one thread applies the transitions in that order, keeping every body's color
+// membership as a 24-bit mask (bit c == the reference's colors[c].body_set bit).
+
+template <bool kShared>
+__device__ void state_serial(const DW& w, uint32_t* mask, int count) {
+  int ovf = w.ctl->overflow_count;
+  for (int i = 0; i < count; ++i) {
+    int cid = w.changed_list[i];
+    DContact& c = w.contacts[cid];
+    uint32_t f = c.flags;
+    int destroyed = 0;
+    auto remove = [&](int color, int local) {  // constraint_graph.rs:200
+      if (color != kOverflowIndex) {
+        mask[c.body_a] &= ~(1u << color);
+        mask[c.body_b] &= ~(1u << color);
+      } else {
+        int last = ovf - 1;
+        if (local != last) {
+          int moved = w.overflow_list[last];
+          w.overflow_list[local] = moved;
+          w.contacts[moved].local = local;
+        }
+        ovf = last;
+      }
+    };
+    if (f == 0) {
+    } else if (f & cSimDisjoint) {  // contact_creation.rs:428 destroy_contact
+      c.manifold_count = 0;
+      if (c.color != -1) remove(c.color, c.local);
+      c.alive = 0;
+      c.color = -1;
+      c.local = -1;
+      destroyed = 1;
+    } else if (f & cSimStarted) {   // constraint_graph.rs:113 add_contact_to_graph
+      c.flags = (f & ~cSimStarted) | cTouching;
+      bool dyn_a = c.enc_a >= 0, dyn_b = c.enc_b >= 0;
+      int color = kOverflowIndex;
+      if (dyn_a && dyn_b) {
+        uint32_t avail = ~(mask[c.body_a] | mask[c.body_b]) & ((1u << kDynamicColorCount) - 1u);
+        if (avail) {
+          color = __ffs(avail) - 1;
+          mask[c.body_a] |= 1u << color;
+          mask[c.body_b] |= 1u << color;
+        }
+      } else {
+        int d = dyn_a ? c.body_a : c.body_b;
+        uint32_t avail = ~mask[d] & (((1u << kOverflowIndex) - 1u) & ~1u);  // colors 22..1
+        if (avail) {
+          color = 31 - __clz(avail);
+          mask[d] |= 1u << color;
+        }
+      }
+      c.color = color;
+      if (color == kOverflowIndex) {
+        c.local = ovf;
+        w.overflow_list[ovf] = cid;
+        ovf++;
+      } else {
+        c.local = -1;
+      }
+    } else if (f & cSimStopped) {
+      c.flags = f & ~(cSimStopped | cTouching);
+      int color = c.color, local = c.local;
+      c.color = -1;
+      c.local = -1;
+      remove(color, local);
+    }
+    w.destroyed[i] = destroyed;
+  }
+  w.ctl->overflow_count = ovf;
+}
+
+__global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_shared) {
+  extern __shared__ uint32_t smask[];
+  typedef cub::BlockScan<int, kStatePassThreads> Scan;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ int total_s;
+  int t = threadIdx.x;
+  int per = (w.n_words + kStatePassThreads - 1) / kStatePassThreads;
+  int w0 = t * per, w1 = min(w0 + per, w.n_words);
+  int mine = 0;
+  for (int k = w0; k < w1; ++k) mine += __popc(w.changed_bits[k]);
+  int off, total;
+  Scan(scan_tmp).ExclusiveSum(mine, off, total);
+  for (int k = w0; k < w1; ++k) {
+    uint32_t bits = w.changed_bits[k];
+    while (bits) {
+      int b = __ffs(bits) - 1;
+      w.changed_list[off++] = (k << 5) + b;
+      bits &= bits - 1;
+    }
+    w.changed_bits[k] = 0;
+  }
+  if (t == 0) { total_s = total; w.ctl->changed_count = total; }
+  __syncthreads();
+  total = total_s;
+  if (total == 0) return;
+  if (use_shared) {
+    for (int b = t; b < w.n_bodies; b += kStatePassThreads) smask[b] = w.body_mask[b];
+    __syncthreads();
+    if (t == 0) state_serial<true>(w, smask, total);
+    __syncthreads();
+    for (int b = t; b < w.n_bodies; b += kStatePassThreads) w.body_mask[b] = smask[b];
+  } else {
+    if (t == 0) state_serial<false>(w, w.body_mask, total);
+  }
+  __syncthreads();
+  // Destroyed ids go back on the LIFO pool in id order (contact_creation.rs:543 free).
+  int nd = 0;
+  int per2 = (total + kStatePassThreads - 1) / kStatePassThreads;
+  int i0 = t * per2, i1 = min(i0 + per2, total);
+  for (int i = i0; i < i1; ++i) nd += w.destroyed[i];
+  int doff, dtotal;
+  __syncthreads();
+  Scan(scan_tmp).ExclusiveSum(nd, doff, dtotal);
+  int top = w.ctl->pool_top;
+  for (int i = i0; i < i1; ++i) {
+    if (!w.destroyed[i]) continue;
+    int cid = w.changed_list[i];
+    w.free_stack[top + doff] = cid;
+    doff++;
+    const DContact& c = w.contacts[cid];
+    hs_erase(w, pair_key(c.shape_a, c.shape_b));
+  }
+  __syncthreads();
+  if (t == 0) {
+    w.ctl->pool_top = top + dtotal;
+    w.ctl->hs_rebuild = w.ctl->tombstones > (w.hs_mask + 1) / 4 ? 1 : 0;
+    if (w.ctl->hs_rebuild) w.ctl->tombstones = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Color partition and constraint preparation (solver_prepare.rs:269/335,
+// contact_solver.rs:445 prepare_contact_constraint). Constraints of color c occupy
+// slots [color_offset[c], color_offset[c+1]); order inside a color does not change
+// results because a color's constraints share no dynamic body.
+
+__device__ __forceinline__ int colored_color(const DContact& c) {
+  return (c.alive && (c.flags & cTouching) && c.color >= 0 && c.color < kOverflowIndex) ? c.color : -1;
+}
+
+__global__ void __launch_bounds__(kColorBlock) k_color_count(DW w) {
+  __shared__ int wc[kColorBlock / 32][24];
+  int cid = blockIdx.x * kColorBlock + threadIdx.x;
+  int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < kOverflowIndex; ++k) {
+    unsigned m = __ballot_sync(0xffffffffu, col == k);
+    if (lane == 0) wc[warp][k] = __popc(m);
+  }
+  __syncthreads();
+  if (threadIdx.x < kOverflowIndex) {
+    int s = 0;
+    for (int q = 0; q < kColorBlock / 32; ++q) s += wc[q][threadIdx.x];
+    w.block_color[blockIdx.x * 24 + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_color_scan(DW w) {
+  int k = threadIdx.x;
+  __shared__ int totals[24];
+  if (k < kOverflowIndex) {
+    int run = 0;
+    for (int b = 0; b < w.n_color_blocks; ++b) {
+      int v = w.block_color[b * 24 + k];
+      w.block_color[b * 24 + k] = run;
+      run += v;
+    }
+    totals[k] = run;
+    w.ctl->color_count[k] = run;
+  }
+  __syncthreads();
+  if (k == 0) {
+    int run = 0;
+    for (int c = 0; c < kOverflowIndex; ++c) { w.ctl->color_offset[c] = run; run += totals[c]; }
+    w.ctl->color_offset[kOverflowIndex] = run;
+    w.ctl->color_offset[24] = run;
+    w.ctl->color_count[kOverflowIndex] = w.ctl->overflow_count;
+    w.ctl->any_restitution = 0;
+  }
+}
+
+__device__ __forceinline__ DState state_at(const DW& w, int i) {
+  if (i >= 0) return w.states[i];
+  DState s;
+  s.v = v3(0, 0, 0); s.w = v3(0, 0, 0); s.dp = v3(0, 0, 0); s.flags = 0; s.dq = qid();
+  s.pad1 = 0; s.pad2 = 0;
+  return s;
+}
+
+__device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, int slot) {
+  const DContact& ct = w.contacts[cid];
+  const CPlanes& P = w.cp;
+  float inv_tau = 1.0f / speculative_distance();
+  float ws = p.warm_start;
+  int ia = ct.enc_a >= 0 ? ct.enc_a : -1;
+  int ib = ct.enc_b >= 0 ? ct.enc_b : -1;
+  float ima = 0.0f, imb = 0.0f;
+  Sym sa = sym_zero(), sb = sym_zero();
+  if (ia >= 0) { ima = w.asims[ia].inv_mass; sa = sym_from(w.asims[ia].inv_inertia_world); }
+  if (ib >= 0) { imb = w.asims[ib].inv_mass; sb = sym_from(w.asims[ib].inv_inertia_world); }
+  bool is_static = (ct.flags & cStatic) != 0;
+  float rolling = ct.rolling;
+  Sym inv_iab = sym_add(sa, sb);
+  Sym rm = rolling > 0.0f ? sym_invert(inv_iab) : sym_zero();
+  const Manifold& man = ct.manifold;
+  V3 n = man.normal;
+  V3 t1 = perp(n);
+  V3 t2 = cross(t1, n);
+  float tv1 = dot(ct.tangent_velocity, t1), tv2 = dot(ct.tangent_velocity, t2);
+  float twist = ws * man.twist_impulse;
+  V3 rimp = rolling > 0.0f ? ws * man.rolling_impulse : v3(0, 0, 0);
+  V2 fi = v2(ws * dot(man.friction_impulse, t1), ws * dot(man.friction_impulse, t2));
+  V3 ca = v3(0, 0, 0), cb = v3(0, 0, 0);
+  float tw = 0.0f;
+  int pc = man.point_count;
+  V3 ra_[4], rb_[4];
+  for (int i = 0; i < pc; ++i) {
+    const ManifoldPoint& mp = man.points[i];
+    V3 ra = mp.anchor_a, rb = mp.anchor_b;
+    ra_[i] = ra; rb_[i] = rb;
+    float base_sep = mp.separation - dot(rb - ra, n);
+    float weight = clampf(2.0f - mp.separation * inv_tau, kMinFrictionWeight, 1.0f);
+    ca = ca + weight * ra;
+    cb = cb + weight * rb;
+    tw += weight;
+    V3 rna = cross(ra, n), rnb = cross(rb, n);
+    float k = ima + imb;
+    k += dot(rna, sym_mv(sa, rna));
+    k += dot(rnb, sym_mv(sb, rnb));
+    float nm = k > 0.0f ? 1.0f / k : 0.0f;
+    P.pra[i * P.cap + slot] = make_float4(ra.x, ra.y, ra.z, base_sep);
+    P.prb[i * P.cap + slot] = make_float4(rb.x, rb.y, rb.z, nm);
+  }
+  if (tw > 0.0f) {
+    ca = (1.0f / tw) * ca;
+    cb = (1.0f / tw) * cb;
+  } else {
+    ca = v3(0, 0, 0); cb = v3(0, 0, 0);
+  }
+  float rv[4] = {0, 0, 0, 0};
+  if (ct.restitution > 0.0f) {
+    DState s_a = state_at(w, ia), s_b = state_at(w, ib);
+    for (int i = 0; i < pc; ++i) {
+      V3 vra = s_a.v + cross(s_a.w, ra_[i]);
+      V3 vrb = s_b.v + cross(s_b.w, rb_[i]);
+      rv[i] = dot(n, vrb - vra);
+    }
+    atomicOr(&w.ctl->any_restitution, 1);
+  }
+  for (int i = 0; i < pc; ++i) {
+    V3 d = ra_[i] - ca;
+    float lever = sqrtf(dot(d, d));
+    P.pimp[i * P.cap + slot] = make_float4(ws * man.points[i].normal_impulse, 0.0f, lever, rv[i]);
+    P.prest[i * P.cap + slot] = 0.0f;
+  }
+  V3 rta1 = cross(ca, t1), rta2 = cross(ca, t2), rtb1 = cross(cb, t1), rtb2 = cross(cb, t2);
+  V3 ia1 = sym_mv(sa, rta1), ia2 = sym_mv(sa, rta2), ib1 = sym_mv(sb, rtb1), ib2 = sym_mv(sb, rtb2);
+  float msum = ima + imb;
+  float kxx = (msum + dot(rta1, ia1)) + dot(rtb1, ib1);
+  float kyy = (msum + dot(rta2, ia2)) + dot(rtb2, ib2);
+  float kxy = dot(rta1, ia2) + dot(rtb1, ib2);
+  float det2 = kxx * kyy - kxy * kxy;
+  bool valid = absf(det2) > 1000.0f * kMinPositive && tw > 0.0f;
+  float inv = valid ? 1.0f / det2 : 0.0f;
+  float ktw = dot(n, sym_mv(inv_iab, n));
+  float twist_mass = ktw > 0.0f ? 1.0f / ktw : 0.0f;
+  P.idx[slot] = make_int4(ia, ib, cid, pc | (is_static ? 256 : 0));
+  P.mass[slot] = make_float4(ima, imb, ct.friction, ct.restitution);
+  P.ia0[slot] = make_float4(sa.xx, sa.xy, sa.xz, sa.yy);
+  P.ia1[slot] = make_float4(sa.yz, sa.zz, sb.xx, sb.xy);
+  P.ib1[slot] = make_float4(sb.xz, sb.yy, sb.yz, sb.zz);
+  P.n[slot] = make_float4(n.x, n.y, n.z, rolling);
+  P.t1[slot] = make_float4(t1.x, t1.y, t1.z, tv1);
+  P.t2[slot] = make_float4(t2.x, t2.y, t2.z, tv2);
+  P.ca[slot] = make_float4(ca.x, ca.y, ca.z, twist_mass);
+  P.cb[slot] = make_float4(cb.x, cb.y, cb.z, twist);
+  P.tm[slot] = make_float4(inv * kyy, -(inv * kxy), -(inv * kxy), inv * kxx);
+  P.fr[slot] = make_float4(fi.x, fi.y, rm.xx, rm.xy);
+  P.roll[slot] = make_float4(rimp.x, rimp.y, rimp.z, rm.xz);
+  P.rm[slot] = make_float4(rm.yy, rm.yz, rm.zz, 0.0f);
+}
+
+__global__ void __launch_bounds__(kColorBlock) k_color_scatter_prepare(DW w, StepParams p) {
+  __shared__ int wc[kColorBlock / 32][24];
+  int cid = blockIdx.x * kColorBlock + threadIdx.x;
+  int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned my_mask = 0;
+  for (int k = 0; k < kOverflowIndex; ++k) {
+    unsigned m = __ballot_sync(0xffffffffu, col == k);
+    if (lane == 0) wc[warp][k] = __popc(m);
+    if (col == k) my_mask = m;
+  }
+  __syncthreads();
+  if (col < 0) return;
+  int before = 0;
+  for (int q = 0; q < warp; ++q) before += wc[q][col];
+  int rank = __popc(my_mask & ((1u << lane) - 1u));
+  int slot = w.ctl->color_offset[col] + w.block_color[blockIdx.x * 24 + col] + before + rank;
+  prepare_constraint(w, p, cid, slot);
+}
+
+// overflow_contact_solver.rs:92 prepare_overflow_contacts
+__global__ void k_prepare_overflow(DW w, StepParams p) {
+  int n = w.ctl->overflow_count;
+  float ws = p.warm_start;
+  float inv_tau = 1.0f / speculative_distance();
+  Softness soft = p.contact_softness, stat = p.static_softness;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int cid = w.overflow_list[i];
+    DContact& ct = w.contacts[cid];
+    DOverflow c;
+    memset(&c, 0, sizeof(c));
+    int ia = ct.enc_a >= 0 ? ct.enc_a : -1;
+    int ib = ct.enc_b >= 0 ? ct.enc_b : -1;
+    c.contact_id = cid; c.index_a = ia; c.index_b = ib;
+    c.inv_ia = m3zero(); c.inv_ib = m3zero();
+    if (ia >= 0) { c.inv_mass_a = w.asims[ia].inv_mass; c.inv_ia = w.asims[ia].inv_inertia_world; }
+    if (ib >= 0) { c.inv_mass_b = w.asims[ib].inv_mass; c.inv_ib = w.asims[ib].inv_inertia_world; }
+    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    M3 iA = c.inv_ia, iB = c.inv_ib;
+    c.rolling_mass = invert_matrix(add_mm(iA, iB));
+    c.softness = (ct.flags & cStatic) ? stat : soft;
+    c.friction = ct.friction; c.restitution = ct.restitution; c.rolling_resistance = ct.rolling;
+    bool sample = ct.restitution > 0.0f;
+    if (sample) atomicOr(&w.ctl->any_restitution, 1);
+    V3 va = v3(0, 0, 0), wa = v3(0, 0, 0), vb = v3(0, 0, 0), wb = v3(0, 0, 0);
+    if (sample) {
+      if (ia >= 0) { va = w.states[ia].v; wa = w.states[ia].w; }
+      if (ib >= 0) { vb = w.states[ib].v; wb = w.states[ib].w; }
+    }
+    c.manifold_count = ct.manifold_count;
+    if (ct.manifold_count > 0) {
+      Manifold& man = ct.manifold;
+      ManifoldConstraint& mc = c.m;
+      int pc = man.point_count;
+      V3 nn = man.normal, t1 = perp(nn), t2 = cross(t1, nn);
+      mc.point_count = pc; mc.normal = nn; mc.tangent1 = t1; mc.tangent2 = t2;
+      mc.tangent_velocity1 = dot(ct.tangent_velocity, t1);
+      mc.tangent_velocity2 = dot(ct.tangent_velocity, t2);
+      V3 ca = v3(0, 0, 0), cb = v3(0, 0, 0);
+      float tw = 0.0f;
+      for (int q = 0; q < pc; ++q) {
+        ConstraintPoint cp;
+        memset(&cp, 0, sizeof(cp));
+        const ManifoldPoint& mp = man.points[q];
+        cp.r_a = mp.anchor_a; cp.r_b = mp.anchor_b;
+        float s = mp.separation;
+        cp.base_separation = s - dot(cp.r_b - cp.r_a, nn);
+        cp.normal_impulse = ws * mp.normal_impulse;
+        V3 ra = cp.r_a, rb = cp.r_b;
+        V3 rna = cross(ra, nn), rnb = cross(rb, nn);
+        float k = mA + mB + dot(rna, mul_mv(iA, rna)) + dot(rnb, mul_mv(iB, rnb));
+        cp.normal_mass = k > 0.0f ? 1.0f / k : 0.0f;
+        if (sample) {
+          V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+          cp.relative_velocity = dot(nn, vrb - vra);
+        } else {
+          cp.relative_velocity = 0.0f;
+        }
+        man.points[q].normal_velocity = 0.0f;
+        float weight = clampf(2.0f - s * inv_tau, kMinFrictionWeight, 1.0f);
+        ca = mul_add(ca, weight, ra);
+        cb = mul_add(cb, weight, rb);
+        tw += weight;
+        mc.points[q] = cp;
+      }
+      float iw = 1.0f / tw;
+      ca = iw * ca; cb = iw * cb;
+      mc.center_a = ca; mc.center_b = cb;
+      for (int q = 0; q < pc; ++q) mc.points[q].lever_arm = distance(mc.points[q].r_a, ca);
+      V3 rta1 = cross(ca, t1), rta2 = cross(ca, t2), rtb1 = cross(cb, t1), rtb2 = cross(cb, t2);
+      M2 k;
+      k.cx.x = mA + mB + dot(rta1, mul_mv(iA, rta1)) + dot(rtb1, mul_mv(iB, rtb1));
+      k.cy.y = mA + mB + dot(rta2, mul_mv(iA, rta2)) + dot(rtb2, mul_mv(iB, rtb2));
+      k.cx.y = dot(rta1, mul_mv(iA, rta2)) + dot(rtb1, mul_mv(iB, rtb2));
+      k.cy.x = k.cx.y;
+      mc.tangent_mass = invert2(k);
+      mc.friction_impulse = v2(ws * dot(man.friction_impulse, t1), ws * dot(man.friction_impulse, t2));
+      float ktw = dot(nn, mul_mv(add_mm(iA, iB), nn));
+      mc.twist_mass = ktw > 0.0f ? 1.0f / ktw : 0.0f;
+      mc.twist_impulse = ws * man.twist_impulse;
+      mc.rolling_impulse = ws * man.rolling_impulse;
+    }
+    w.ovf[i] = c;
+  }
+}
+
+// distance_joint_solver.rs:74 prepare_joint + revolute_joint.rs:183 prepare_revolute_joint
+__global__ void k_prepare_joints(DW w, StepParams p) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n_joints) return;
+  DJoint j = w.joints[i];
+  float hz = minf(j.constraint_hertz, 0.25f * p.inv_h);
+  j.constraint_softness = make_soft(hz, j.constraint_damping_ratio, p.h);
+  const DSim& sa = sim_of(w, j.enc_a);
+  const DSim& sb = sim_of(w, j.enc_b);
+  j.index_a = j.enc_a >= 0 ? j.enc_a : -1;
+  j.index_b = j.enc_b >= 0 ? j.enc_b : -1;
+  j.inv_mass_a = sa.inv_mass; j.inv_mass_b = sb.inv_mass;
+  j.inv_ia = sa.inv_inertia_world; j.inv_ib = sb.inv_inertia_world;
+  M3 sum = add_mm(j.inv_ia, j.inv_ib);
+  j.fixed_rotation = det(sum) < 1000.0f * kMinPositive;
+  j.frame_a.q = mul_quat(sa.q, j.local_frame_a.q);
+  j.frame_a.p = rotate(sa.q, j.local_frame_a.p - sa.local_center);
+  j.frame_b.q = mul_quat(sb.q, j.local_frame_b.q);
+  j.frame_b.p = rotate(sb.q, j.local_frame_b.p - sb.local_center);
+  Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+  j.delta_center = sub_pos(cb, ca);
+  V3 axis = rotate(j.frame_a.q, v3(0, 0, 1));
+  float k = dot(axis, mul_mv(sum, axis));
+  j.axial_mass = k > 0.0f ? 1.0f / k : 0.0f;
+  j.rotation_axis_z = axis;
+  Q rq = inv_mul_quat(j.frame_a.q, j.frame_b.q);
+  j.perp_axis_x = 0.5f * rotate(j.frame_a.q, rq.s * v3(1, 0, 0) + cross(rq.v, v3(1, 0, 0)));
+  j.perp_axis_y = 0.5f * rotate(j.frame_a.q, rq.s * v3(0, 1, 0) + cross(rq.v, v3(0, 1, 0)));
+  j.spring_softness = make_soft(j.hertz, j.damping_ratio, p.h);
+  if (p.warm_start == 0.0f) {
+    j.linear_impulse = v3(0, 0, 0); j.perp_impulse = v2(0, 0);
+    j.motor_impulse = 0; j.spring_impulse = 0; j.lower_impulse = 0; j.upper_impulse = 0;
+  }
+  w.joints[i] = j;
+}
+
+}  // namespace nsd

@@ -1,0 +1,978 @@
+// Persistent colored solver (solver_stages.rs:543 solve_constraint_stages) and body
+// finalization (solver_integration.rs:587 finalize_body_range).
+//
+// One cooperative launch runs every substep: integrate velocities, then per stage
+// (warm start, push, relax) the overflow color on one thread followed by colors
+// 0..22, each color one grid-wide phase; then restitution and impulse storage.
+// Colors with no work are skipped by every block alike, so they cost no barrier.
+#pragma once
+#include "nsd_kernels.cuh"
+
+namespace nsd {
+
+// Bounded grid barrier. The arrival counter is zeroed before each launch; barrier k is
+// complete when it reaches (k + 1) * gridDim.x. A block that waits longer than the limit
+// raises NS_ERR_TIMEOUT and the whole kernel unwinds at its next barrier instead of hanging.
+__device__ __forceinline__ bool grid_barrier(Control* ctl, int& index) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int target = (index + 1) * (int)gridDim.x;
+    __threadfence();
+    atomicAdd(&ctl->barrier_count, 1);
+    int ok = 1;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    long long spins = 0;
+    for (;;) {
+      int v = *((volatile int*)&ctl->barrier_count);
+      if (v >= target) break;
+      if (*((volatile int*)&ctl->error) != 0) { ok = 0; break; }
+      if (++spins > (1ll << 26)) { ok = 0; break; }
+      if ((spins & 1023) == 0) {
+        unsigned long long t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        if (t1 - t0 > 2000000000ull) { ok = 0; break; }  // 2 s
+      }
+      __nanosleep(32);
+    }
+    if (!ok) atomicCAS(&ctl->error, 0, kErrTimeout);
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  index++;
+  return ok_s != 0;
+}
+
+__device__ __forceinline__ void store_state_vw(const DW& w, int i, const DState& s) {
+  if (i >= 0 && (s.flags & kDynamicFlag)) {
+    w.states[i].v = s.v;
+    w.states[i].w = s.w;
+  }
+}
+
+// solver_integration.rs:263 integrate_velocities_range
+__device__ void integrate_velocity(const DW& w, const StepParams& p, int i) {
+  const DSim& sim = w.asims[i];
+  DState& st = w.states[i];
+  float h = p.h;
+  V3 v = st.v, wv = st.w;
+  float ld = 1.0f / (1.0f + h * sim.linear_damping);
+  float ad = 1.0f / (1.0f + h * sim.angular_damping);
+  float gs = sim.inv_mass > 0.0f ? sim.gravity_scale : 0.0f;
+  V3 lvd = blend2(h * sim.inv_mass, sim.force, h * gs, p.gravity);
+  v = mul_add(lvd, ld, v);
+  V3 avd = h * mul_mv(sim.inv_inertia_world, sim.torque);
+  wv = mul_add(avd, ad, wv);
+  if (sim.flags & kGyroscopic) {
+    Q q = mul_quat(st.dq, sim.q);
+    V3 om1 = inv_rotate(q, wv);
+    V3 om2 = om1;
+    float i00 = sim.inertia.cx.x, i01 = sim.inertia.cy.x, i02 = sim.inertia.cz.x;
+    float i11 = sim.inertia.cy.y, i12 = sim.inertia.cz.y, i22 = sim.inertia.cz.z;
+    float w1 = om2.x, w2 = om2.y, w3 = om2.z;
+    float iw1 = i00 * w1 + i01 * w2 + i02 * w3;
+    float iw2 = i01 * w1 + i11 * w2 + i12 * w3;
+    float iw3 = i02 * w1 + i12 * w2 + i22 * w3;
+    V3 dw = om2 - om1;
+    V3 b = v3(i00 * dw.x + i01 * dw.y + i02 * dw.z + h * (w2 * iw3 - w3 * iw2),
+              i01 * dw.x + i11 * dw.y + i12 * dw.z + h * (w3 * iw1 - w1 * iw3),
+              i02 * dw.x + i12 * dw.y + i22 * dw.z + h * (w1 * iw2 - w2 * iw1));
+    M3 J = m3(v3(i00 + h * (w2 * i02 - w3 * i01), i01 + h * (w3 * i00 - w1 * i02 - iw3),
+                 i02 + h * (w1 * i01 - w2 * i00 + iw2)),
+              v3(i01 + h * (w2 * i12 - w3 * i11 + iw3), i11 + h * (w3 * i01 - w1 * i12),
+                 i12 + h * (w1 * i11 - w2 * i01 - iw1)),
+              v3(i02 + h * (w2 * i22 - w3 * i12 - iw2), i12 + h * (w3 * i02 - w1 * i22 + iw1),
+                 i22 + h * (w1 * i12 - w2 * i02)));
+    om2 = om2 - solve3(J, b);
+    wv = rotate(q, om2);
+  }
+  st.v = v;
+  st.w = wv;
+}
+
+// solver_integration.rs:377 integrate_positions_range
+__device__ void integrate_position(const DW& w, const StepParams& p, int i) {
+  DState st = w.states[i];
+  float maxl = p.max_linear_speed;
+  float maxa = kMaxRotation * p.inv_dt;
+  float maxl2 = maxl * maxl, maxa2 = maxa * maxa;
+  V3 v = st.v, wv = st.w;
+  v.x = (st.flags & kLockLinX) ? 0.0f : v.x;
+  v.y = (st.flags & kLockLinY) ? 0.0f : v.y;
+  v.z = (st.flags & kLockLinZ) ? 0.0f : v.z;
+  wv.x = (st.flags & kLockAngX) ? 0.0f : wv.x;
+  wv.y = (st.flags & kLockAngY) ? 0.0f : wv.y;
+  wv.z = (st.flags & kLockAngZ) ? 0.0f : wv.z;
+  if (dot(v, v) > maxl2) {
+    float ratio = maxl / length(v);
+    v = ratio * v;
+    st.flags |= kIsSpeedCapped;
+  }
+  if (dot(wv, wv) > maxa2 && (st.flags & kAllowFastRotation) == 0) {
+    float ratio = maxa / length(wv);
+    wv = ratio * wv;
+    st.flags |= kIsSpeedCapped;
+  }
+  st.v = v;
+  st.w = wv;
+  st.dp = mul_add(st.dp, p.h, v);
+  st.dq = integrate_rotation(st.dq, p.h * wv);
+  w.states[i] = st;
+}
+
+struct CLoad {
+  int ia, ib, pc;
+  bool is_static;
+  float ima, imb, friction, restitution, rolling;
+  Sym sa, sb;
+  V3 n;
+};
+__device__ __forceinline__ CLoad load_constraint(const CPlanes& P, int k) {
+  CLoad c;
+  int4 idx = P.idx[k];
+  float4 m = P.mass[k], a0 = P.ia0[k], a1 = P.ia1[k], b1 = P.ib1[k], nn = P.n[k];
+  c.ia = idx.x; c.ib = idx.y; c.pc = idx.w & 255; c.is_static = (idx.w & 256) != 0;
+  c.ima = m.x; c.imb = m.y; c.friction = m.z; c.restitution = m.w;
+  c.sa.xx = a0.x; c.sa.xy = a0.y; c.sa.xz = a0.z; c.sa.yy = a0.w; c.sa.yz = a1.x; c.sa.zz = a1.y;
+  c.sb.xx = a1.z; c.sb.xy = a1.w; c.sb.xz = b1.x; c.sb.yy = b1.y; c.sb.yz = b1.z; c.sb.zz = b1.w;
+  c.n = v3(nn.x, nn.y, nn.z);
+  c.rolling = nn.w;
+  return c;
+}
+
+// contact_solver.rs:697 warm_start_contacts_body
+__device__ void warm_start_constraint(const DW& w, int k) {
+  const CPlanes& P = w.cp;
+  CLoad c = load_constraint(P, k);
+  float4 t1f = P.t1[k], t2f = P.t2[k], caf = P.ca[k], cbf = P.cb[k], frf = P.fr[k];
+  V3 t1 = v3(t1f.x, t1f.y, t1f.z), t2 = v3(t2f.x, t2f.y, t2f.z);
+  V3 center_a = v3(caf.x, caf.y, caf.z), center_b = v3(cbf.x, cbf.y, cbf.z);
+  float twist = cbf.w;
+  V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
+  float tni = 0.0f;
+  V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
+  for (int p = 0; p < c.pc; ++p) {
+    float4 ra = P.pra[p * P.cap + k], rb = P.prb[p * P.cap + k];
+    float ni = P.pimp[p * P.cap + k].x;
+    tni += ni;
+    moa = mul_add(moa, ni, v3(ra.x, ra.y, ra.z));
+    mob = mul_add(mob, ni, v3(rb.x, rb.y, rb.z));
+  }
+  V3 n = c.n;
+  V3 fi = frf.x * t1;
+  fi = mul_add(fi, frf.y, t2);
+  V3 lin = mul_add(fi, tni, n);
+  V3 twi = twist * n;
+  V3 anga = cross(moa, n) + cross(center_a, fi) + twi;
+  V3 angb = cross(mob, n) + cross(center_b, fi) + twi;
+  if (c.rolling > 0.0f) {
+    float4 r = P.roll[k];
+    V3 ri = v3(r.x, r.y, r.z);
+    anga = anga + ri;
+    angb = angb + ri;
+  }
+  li = li + lin; aia = aia + anga; aib = aib + angb;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  ba.w = ba.w - sym_mv(c.sa, aia);
+  ba.v = ba.v - c.ima * li;
+  bb.w = bb.w + sym_mv(c.sb, aib);
+  bb.v = bb.v + c.imb * li;
+  store_state_vw(w, c.ia, ba);
+  store_state_vw(w, c.ib, bb);
+}
+
+// contact_solver.rs:796 push_contacts_body
+__device__ void push_constraint(const DW& w, const StepParams& p, int k) {
+  const CPlanes& P = w.cp;
+  CLoad c = load_constraint(P, k);
+  float inv_h = p.inv_h;
+  float cs = -p.contact_speed;
+  float br = c.is_static ? p.static_softness.mass_scale * p.static_softness.bias_rate
+                         : p.contact_softness.mass_scale * p.contact_softness.bias_rate;
+  float ms = c.is_static ? p.static_softness.mass_scale : p.contact_softness.mass_scale;
+  float is = c.is_static ? p.static_softness.impulse_scale : p.contact_softness.impulse_scale;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  V3 dp = bb.dp - ba.dp;
+  float im = c.ima + c.imb;
+  V3 n = c.n;
+  float ns = dot(n, dp);
+  V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
+  float lnv = dot(n, bb.v - ba.v);
+  float mi = 0.0f;
+  for (int q = 0; q < c.pc; ++q) {
+    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
+    float4 imp4 = P.pimp[q * P.cap + k];
+    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+    float base_sep = raf.w, nmass = rbf.w, nimp = imp4.x;
+    float s = (ns + (dot(nb, rb) - dot(na, ra))) + base_sep;
+    bool sep = s > 0.0f;
+    float spec_bias = s * inv_h;
+    float ovl = maxf(br * s, cs);
+    float vb = sep ? spec_bias : ovl;
+    float pms = sep ? 1.0f : ms;
+    float pis = sep ? 0.0f : is;
+    V3 ua = cross(ra, n), ub = cross(rb, n);
+    V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
+    float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+    float neg = nmass * (pms * vn + vb) + pis * nimp;
+    float impulse = maxf(-neg, -nimp);
+    imp4.x = nimp + impulse;
+    P.pimp[q * P.cap + k] = imp4;
+    lnv += im * impulse;
+    mi += impulse;
+    ba.w = ba.w - impulse * ga;
+    bb.w = bb.w + impulse * gb;
+  }
+  V3 Pv = mi * n;
+  ba.v = ba.v - c.ima * Pv;
+  bb.v = bb.v + c.imb * Pv;
+  store_state_vw(w, c.ia, ba);
+  store_state_vw(w, c.ib, bb);
+}
+
+// contact_solver.rs:927 solve_contacts_body (relax)
+__device__ void relax_constraint(const DW& w, const StepParams& p, int k) {
+  const CPlanes& P = w.cp;
+  CLoad c = load_constraint(P, k);
+  float inv_h = p.inv_h;
+  const float eps = kEps;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  bool any_rolling = c.rolling > 0.0f;
+  V3 dp = bb.dp - ba.dp;
+  float im = c.ima + c.imb;
+  V3 n = c.n;
+  float4 t1f = P.t1[k], t2f = P.t2[k];
+  V3 t1 = v3(t1f.x, t1f.y, t1f.z), t2 = v3(t2f.x, t2f.y, t2f.z);
+  float ns = dot(n, dp);
+  V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
+  V3 dv = bb.v - ba.v;
+  float lnv = dot(n, dv);
+  float lt1 = dot(t1, dv) - t1f.w;
+  float lt2 = dot(t2, dv) - t2f.w;
+  float mi = 0.0f, tni = 0.0f, ttl = 0.0f;
+  for (int q = 0; q < c.pc; ++q) {
+    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
+    float4 imp4 = P.pimp[q * P.cap + k];
+    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+    float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
+    float vb = maxf(0.0f, s * inv_h);
+    V3 ua = cross(ra, n), ub = cross(rb, n);
+    V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
+    float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+    float neg = rbf.w * (vn + vb);
+    float impulse = maxf(-neg, -imp4.x);
+    float ni = imp4.x + impulse;
+    imp4.x = ni;
+    imp4.y = imp4.y + ni;
+    P.pimp[q * P.cap + k] = imp4;
+    tni += ni;
+    ttl += imp4.z * ni;
+    lnv += im * impulse;
+    mi += impulse;
+    ba.w = ba.w - impulse * ga;
+    bb.w = bb.w + impulse * gb;
+  }
+  if (any_rolling) {
+    float4 fr = P.fr[k], ro = P.roll[k], rmv = P.rm[k];
+    Sym rm = {fr.z, fr.w, ro.w, rmv.x, rmv.y, rmv.z};
+    V3 di = sym_mv(rm, ba.w - bb.w);
+    V3 old = v3(ro.x, ro.y, ro.z);
+    V3 rimp = old + di;
+    float mx = c.rolling * tni;
+    float lsq = dot(rimp, rimp);
+    bool mask = lsq > eps + mx * mx;
+    float nrm = mx / (sqrtf(lsq) + eps);
+    float sc = mask ? nrm : 1.0f;
+    V3 scaled = sc * rimp;
+    if (c.rolling == 0.0f) scaled = v3(0, 0, 0);
+    rimp = scaled;
+    di = rimp - old;
+    ba.w = ba.w - sym_mv(c.sa, di);
+    bb.w = bb.w + sym_mv(c.sb, di);
+    P.roll[k] = make_float4(rimp.x, rimp.y, rimp.z, ro.w);
+  }
+  {
+    float4 caf = P.ca[k], cbf = P.cb[k];
+    float ts = dot(n, bb.w - ba.w);
+    float ml = c.friction * ttl;
+    float old = cbf.w;
+    float impulse = -(caf.w * ts);
+    impulse = maxf(-ml - old, minf(impulse, ml - old));
+    cbf.w = old + impulse;
+    P.cb[k] = cbf;
+    ba.w = ba.w - impulse * sym_mv(c.sa, n);
+    bb.w = bb.w + impulse * sym_mv(c.sb, n);
+    V3 ra = v3(caf.x, caf.y, caf.z), rb = v3(cbf.x, cbf.y, cbf.z);
+    float4 tmf = P.tm[k], fr = P.fr[k];
+    M2 tm;
+    tm.cx = v2(tmf.x, tmf.y);
+    tm.cy = v2(tmf.z, tmf.w);
+    V3 arv = cross(bb.w, rb) - cross(ba.w, ra);
+    V2 vt = v2(lt1 + dot(arv, t1), lt2 + dot(arv, t2));
+    V2 di = mul_mv2(tm, vt);
+    di = v2(-di.x, -di.y);
+    V2 ni = v2(fr.x + di.x, fr.y + di.y);
+    float mx = c.friction * tni;
+    float lsq = ni.x * ni.x + ni.y * ni.y;
+    bool mask = lsq > mx * mx;
+    float nrm = mx / (sqrtf(lsq) + eps);
+    float sc = mask ? nrm : 1.0f;
+    ni = v2(sc * ni.x, sc * ni.y);
+    di = v2(ni.x - fr.x, ni.y - fr.y);
+    fr.x = ni.x; fr.y = ni.y;
+    P.fr[k] = fr;
+    V3 Pv = di.x * t1;
+    Pv = Pv + di.y * t2;
+    ba.w = ba.w - sym_mv(c.sa, cross(ra, Pv));
+    bb.w = bb.w + sym_mv(c.sb, cross(rb, Pv));
+    Pv = Pv + mi * n;
+    ba.v = ba.v - c.ima * Pv;
+    bb.v = bb.v + c.imb * Pv;
+  }
+  store_state_vw(w, c.ia, ba);
+  store_state_vw(w, c.ib, bb);
+}
+
+// contact_solver.rs:1135 apply_restitution_body
+__device__ void restitution_constraint(const DW& w, const StepParams& p, int k) {
+  const CPlanes& P = w.cp;
+  CLoad c = load_constraint(P, k);
+  if (c.restitution == 0.0f) return;
+  float inv_h = p.inv_h;
+  float nrt = -p.restitution_threshold;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  bool rmask = c.restitution > 0.0f;
+  V3 dp = bb.dp - ba.dp;
+  V3 n = c.n;
+  float ns = dot(n, dp);
+  V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
+  for (int q = 0; q < c.pc; ++q) {
+    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
+    float4 imp4 = P.pimp[q * P.cap + k];
+    float rest_imp = P.prest[q * P.cap + k];
+    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+    float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
+    float nm = rmask ? rbf.w : 0.0f;
+    float comp = imp4.y - rest_imp;
+    bool armed = rmask && imp4.w < nrt && comp > 0.0f;
+    float sb = maxf(0.0f, s * inv_h);
+    float vb = armed ? c.restitution * imp4.w : sb;
+    V3 vra = ba.v + cross(ba.w, ra), vrb = bb.v + cross(bb.w, rb);
+    float vn = dot(vrb - vra, n);
+    float neg = nm * (vn + vb);
+    float ni = maxf(imp4.x - neg, 0.0f);
+    float impulse = ni - imp4.x;
+    float app = minf(maxf(-nm * vn, 0.0f), maxf(impulse, 0.0f));
+    float allow = c.restitution * (comp + app) - rest_imp;
+    float mx = app + maxf(allow, 0.0f);
+    impulse = armed ? minf(impulse, mx) : impulse;
+    imp4.x = imp4.x + impulse;
+    rest_imp = rest_imp + (impulse - app);
+    imp4.y = imp4.y + impulse;
+    P.pimp[q * P.cap + k] = imp4;
+    P.prest[q * P.cap + k] = rest_imp;
+    V3 Pv = impulse * n;
+    ba.w = ba.w - sym_mv(c.sa, cross(ra, Pv));
+    ba.v = ba.v - c.ima * Pv;
+    bb.w = bb.w + sym_mv(c.sb, cross(rb, Pv));
+    bb.v = bb.v + c.imb * Pv;
+  }
+  store_state_vw(w, c.ia, ba);
+  store_state_vw(w, c.ib, bb);
+}
+
+// contact_solver.rs:1258 store_impulses_body
+__device__ void store_constraint(const DW& w, int k) {
+  const CPlanes& P = w.cp;
+  int4 idx = P.idx[k];
+  DContact& ct = w.contacts[idx.z];
+  if (ct.manifold_count <= 0) return;
+  int pc = idx.w & 255;
+  Manifold& out = ct.manifold;
+  int cnt = min_i(out.point_count, pc);
+  for (int q = 0; q < cnt; ++q) {
+    float4 imp4 = P.pimp[q * P.cap + k];
+    out.points[q].normal_impulse = imp4.x;
+    out.points[q].total_normal_impulse = imp4.y;
+  }
+  float4 cbf = P.cb[k], t1f = P.t1[k], t2f = P.t2[k], fr = P.fr[k], ro = P.roll[k];
+  out.twist_impulse = cbf.w;
+  out.friction_impulse = fr.x * v3(t1f.x, t1f.y, t1f.z) + fr.y * v3(t2f.x, t2f.y, t2f.z);
+  out.rolling_impulse = v3(ro.x, ro.y, ro.z);
+}
+
+// overflow_contact_solver.rs:308-700 sequential overflow color
+__device__ void ovf_store_velocity(const DW& w, int i, uint32_t flags, V3 v, V3 wv) {
+  if (i >= 0 && (flags & kDynamicFlag)) { w.states[i].v = v; w.states[i].w = wv; }
+}
+__device__ void warm_start_overflow(const DW& w, int n) {
+  for (int i = 0; i < n; ++i) {
+    const DOverflow& c = w.ovf[i];
+    V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
+    for (int mi = 0; mi < c.manifold_count; ++mi) {
+      const ManifoldConstraint& mc = c.m;
+      V3 nn = mc.normal;
+      float tni = 0.0f;
+      V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
+      for (int j = 0; j < mc.point_count; ++j) {
+        const ConstraintPoint& cp = mc.points[j];
+        tni += cp.normal_impulse;
+        moa = mul_add(moa, cp.normal_impulse, cp.r_a);
+        mob = mul_add(mob, cp.normal_impulse, cp.r_b);
+      }
+      V3 fi = mc.friction_impulse.x * mc.tangent1;
+      fi = mul_add(fi, mc.friction_impulse.y, mc.tangent2);
+      li = li + mul_add(fi, tni, nn);
+      V3 twi = mc.twist_impulse * nn;
+      V3 anga = (cross(moa, nn) + cross(mc.center_a, fi)) + twi;
+      V3 angb = (cross(mob, nn) + cross(mc.center_b, fi)) + twi;
+      aia = aia + (anga + mc.rolling_impulse);
+      aib = aib + (angb + mc.rolling_impulse);
+    }
+    if (c.index_a >= 0 && (w.states[c.index_a].flags & kDynamicFlag)) {
+      DState& s = w.states[c.index_a];
+      s.v = mul_sub(s.v, c.inv_mass_a, li);
+      s.w = s.w - mul_mv(c.inv_ia, aia);
+    }
+    if (c.index_b >= 0 && (w.states[c.index_b].flags & kDynamicFlag)) {
+      DState& s = w.states[c.index_b];
+      s.v = mul_add(s.v, c.inv_mass_b, li);
+      s.w = s.w + mul_mv(c.inv_ib, aib);
+    }
+  }
+}
+__device__ void push_overflow(const DW& w, const StepParams& p, int n) {
+  float inv_h = p.inv_h;
+  float cs = p.contact_speed;
+  for (int i = 0; i < n; ++i) {
+    DOverflow& c = w.ovf[i];
+    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    M3 iA = c.inv_ia, iB = c.inv_ib;
+    DState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
+    V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
+    Q dqa = sa.dq, dqb = sb.dq;
+    V3 dp = sb.dp - sa.dp;
+    Softness soft = c.softness;
+    for (int mi = 0; mi < c.manifold_count; ++mi) {
+      ManifoldConstraint& mc = c.m;
+      V3 nn = mc.normal;
+      for (int q = 0; q < mc.point_count; ++q) {
+        ConstraintPoint& cp = mc.points[q];
+        V3 ra = cp.r_a, rb = cp.r_b;
+        V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
+        float s = dot(ds, nn) + cp.base_separation;
+        float vbias, mscale, iscale;
+        if (s > 0.0f) { vbias = s * inv_h; mscale = 1.0f; iscale = 0.0f; }
+        else {
+          vbias = maxf(soft.mass_scale * soft.bias_rate * s, -cs);
+          mscale = soft.mass_scale; iscale = soft.impulse_scale;
+        }
+        V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+        float vn = dot(vrb - vra, nn);
+        float ni0 = cp.normal_impulse;
+        float di = -cp.normal_mass * (mscale * vn + vbias) - iscale * ni0;
+        float ni = maxf(ni0 + di, 0.0f);
+        di = ni - ni0;
+        cp.normal_impulse = ni;
+        V3 Pv = di * nn;
+        va = mul_sub(va, mA, Pv);
+        wa = wa - mul_mv(iA, cross(ra, Pv));
+        vb = mul_add(vb, mB, Pv);
+        wb = wb + mul_mv(iB, cross(rb, Pv));
+      }
+    }
+    ovf_store_velocity(w, c.index_a, sa.flags, va, wa);
+    ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
+  }
+}
+__device__ void relax_overflow(const DW& w, const StepParams& p, int n) {
+  float inv_h = p.inv_h;
+  for (int i = 0; i < n; ++i) {
+    DOverflow& c = w.ovf[i];
+    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    M3 iA = c.inv_ia, iB = c.inv_ib;
+    DState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
+    V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
+    Q dqa = sa.dq, dqb = sb.dq;
+    V3 dp = sb.dp - sa.dp;
+    float fr = c.friction, rr = c.rolling_resistance;
+    for (int mi = 0; mi < c.manifold_count; ++mi) {
+      ManifoldConstraint& mc = c.m;
+      V3 nn = mc.normal;
+      float tni = 0.0f, ttl = 0.0f;
+      for (int q = 0; q < mc.point_count; ++q) {
+        ConstraintPoint& cp = mc.points[q];
+        V3 ra = cp.r_a, rb = cp.r_b;
+        V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
+        float s = dot(ds, nn) + cp.base_separation;
+        float vbias = s > 0.0f ? s * inv_h : 0.0f;
+        V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+        float vn = dot(vrb - vra, nn);
+        float ni0 = cp.normal_impulse;
+        float di = -cp.normal_mass * (vn + vbias);
+        float ni = maxf(ni0 + di, 0.0f);
+        di = ni - ni0;
+        cp.normal_impulse = ni;
+        cp.total_normal_impulse += ni;
+        tni += ni;
+        ttl += cp.lever_arm * ni;
+        V3 Pv = di * nn;
+        va = mul_sub(va, mA, Pv);
+        wa = wa - mul_mv(iA, cross(ra, Pv));
+        vb = mul_add(vb, mB, Pv);
+        wb = wb + mul_mv(iB, cross(rb, Pv));
+      }
+      {
+        float ts = dot(nn, wb - wa);
+        float mx = fr * ttl;
+        float di = -mc.twist_mass * ts;
+        float old = mc.twist_impulse;
+        mc.twist_impulse = clampf(old + di, -mx, mx);
+        di = mc.twist_impulse - old;
+        wa = wa - mul_mv(iA, di * nn);
+        wb = wb + mul_mv(iB, di * nn);
+      }
+      if (rr > 0.0f) {
+        V3 di = -mul_mv(c.rolling_mass, wb - wa);
+        V3 old = mc.rolling_impulse;
+        mc.rolling_impulse = old + di;
+        float mx = rr * tni;
+        float msq = dot(mc.rolling_impulse, mc.rolling_impulse);
+        if (msq > mx * mx + kEps) mc.rolling_impulse = (mx / sqrtf(msq)) * mc.rolling_impulse;
+        di = mc.rolling_impulse - old;
+        wa = wa - mul_mv(iA, di);
+        wb = wb + mul_mv(iB, di);
+      }
+      {
+        V3 t1 = mc.tangent1, t2 = mc.tangent2, ra = mc.center_a, rb = mc.center_b;
+        V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+        V3 vr = vrb - vra;
+        V2 vt = v2(dot(vr, t1) - mc.tangent_velocity1, dot(vr, t2) - mc.tangent_velocity2);
+        V2 tm = mul_mv2(mc.tangent_mass, vt);
+        V2 di = v2(-tm.x, -tm.y);
+        V2 ni = v2(mc.friction_impulse.x + di.x, mc.friction_impulse.y + di.y);
+        float mx = fr * tni;
+        float lsq = dot2(ni, ni);
+        if (lsq > mx * mx) {
+          float sc = mx / sqrtf(lsq);
+          ni.x *= sc; ni.y *= sc;
+        }
+        di = v2(ni.x - mc.friction_impulse.x, ni.y - mc.friction_impulse.y);
+        mc.friction_impulse = ni;
+        V3 Pv = blend2(di.x, t1, di.y, t2);
+        va = mul_sub(va, mA, Pv);
+        wa = wa - mul_mv(iA, cross(ra, Pv));
+        vb = mul_add(vb, mB, Pv);
+        wb = wb + mul_mv(iB, cross(rb, Pv));
+      }
+    }
+    ovf_store_velocity(w, c.index_a, sa.flags, va, wa);
+    ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
+  }
+}
+__device__ void restitution_overflow(const DW& w, const StepParams& p, int n) {
+  float thr = p.restitution_threshold;
+  float inv_h = p.inv_h;
+  for (int i = 0; i < n; ++i) {
+    DOverflow& c = w.ovf[i];
+    float rest = c.restitution;
+    if (rest == 0.0f) continue;
+    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    M3 iA = c.inv_ia, iB = c.inv_ib;
+    DState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
+    V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
+    Q dqa = sa.dq, dqb = sb.dq;
+    V3 dp = sb.dp - sa.dp;
+    for (int mi = 0; mi < c.manifold_count; ++mi) {
+      ManifoldConstraint& mc = c.m;
+      V3 nn = mc.normal;
+      for (int q = 0; q < mc.point_count; ++q) {
+        ConstraintPoint cp = mc.points[q];
+        V3 ra = cp.r_a, rb = cp.r_b;
+        float comp = cp.total_normal_impulse - cp.restitution_impulse;
+        bool armed = rest > 0.0f && cp.relative_velocity < -thr && comp > 0.0f;
+        float vbias;
+        if (armed) vbias = rest * cp.relative_velocity;
+        else {
+          V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
+          float s = dot(ds, nn) + cp.base_separation;
+          vbias = s > 0.0f ? s * inv_h : 0.0f;
+        }
+        V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+        float vn = dot(vrb - vra, nn);
+        float imp = -cp.normal_mass * (vn + vbias);
+        float ni = maxf(cp.normal_impulse + imp, 0.0f);
+        imp = ni - cp.normal_impulse;
+        float app = minf(maxf(-cp.normal_mass * vn, 0.0f), maxf(imp, 0.0f));
+        if (armed) {
+          float allow = rest * (comp + app) - cp.restitution_impulse;
+          imp = minf(imp, app + maxf(allow, 0.0f));
+        }
+        mc.points[q].normal_impulse += imp;
+        mc.points[q].restitution_impulse += imp - app;
+        mc.points[q].total_normal_impulse += imp;
+        V3 Pv = imp * nn;
+        va = mul_sub(va, mA, Pv);
+        wa = wa - mul_mv(iA, cross(ra, Pv));
+        vb = mul_add(vb, mB, Pv);
+        wb = wb + mul_mv(iB, cross(rb, Pv));
+      }
+    }
+    ovf_store_velocity(w, c.index_a, sa.flags, va, wa);
+    ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
+  }
+}
+__device__ void store_overflow(const DW& w, int n) {
+  for (int i = 0; i < n; ++i) {
+    const DOverflow& c = w.ovf[i];
+    if (c.manifold_count == 0) continue;
+    Manifold& m = w.contacts[c.contact_id].manifold;
+    const ManifoldConstraint& mc = c.m;
+    m.twist_impulse = mc.twist_impulse;
+    m.friction_impulse = blend2(mc.friction_impulse.x, mc.tangent1, mc.friction_impulse.y, mc.tangent2);
+    m.rolling_impulse = mc.rolling_impulse;
+    for (int q = 0; q < mc.point_count; ++q) {
+      m.points[q].normal_impulse = mc.points[q].normal_impulse;
+      m.points[q].total_normal_impulse = mc.points[q].total_normal_impulse;
+    }
+  }
+}
+
+// revolute_joint.rs:95 solve_point_constraint
+__device__ V3 solve_point_constraint(float ma, float mb, M3 ia, M3 ib, V3 ra, V3 rb, V3 rhs) {
+  float axy = ra.z * ia.cy.y - ra.y * ia.cz.y;
+  float axz = ra.z * ia.cy.z - ra.y * ia.cz.z;
+  V3 ay = ra.x * ia.cz - ra.z * ia.cx;
+  V3 az = ra.y * ia.cx - ra.x * ia.cy;
+  float bxy = rb.z * ib.cy.y - rb.y * ib.cz.y;
+  float bxz = rb.z * ib.cy.z - rb.y * ib.cz.z;
+  V3 by = rb.x * ib.cz - rb.z * ib.cx;
+  V3 bz = rb.y * ib.cx - rb.x * ib.cy;
+  float m = ma + mb;
+  float kxx = (axy * ra.z - axz * ra.y) + (bxy * rb.z - bxz * rb.y) + m;
+  float kyy = (ay.z * ra.x - ay.x * ra.z) + (by.z * rb.x - by.x * rb.z) + m;
+  float kzz = (az.x * ra.y - az.y * ra.x) + (bz.x * rb.y - bz.y * rb.x) + m;
+  float kxy = (ay.y * ra.z - ay.z * ra.y) + (by.y * rb.z - by.z * rb.y);
+  float kxz = (az.y * ra.z - az.z * ra.y) + (bz.y * rb.z - bz.z * rb.y);
+  float kyz = (az.z * ra.x - az.x * ra.z) + (bz.z * rb.x - bz.x * rb.z);
+  float cxx = kyy * kzz - kyz * kyz;
+  float cyy = kxx * kzz - kxz * kxz;
+  float czz = kxx * kyy - kxy * kxy;
+  float cxy = kxz * kyz - kxy * kzz;
+  float cxz = kxy * kyz - kyy * kxz;
+  float cyz = kxy * kxz - kxx * kyz;
+  float d = kxx * cxx + kxy * cxy + kxz * cxz;
+  if (absf(d) > 1000.0f * kMinPositive) {
+    float inv = 1.0f / d;
+    return v3(inv * (cxx * rhs.x + cxy * rhs.y + cxz * rhs.z),
+              inv * (cxy * rhs.x + cyy * rhs.y + cyz * rhs.z),
+              inv * (cxz * rhs.x + cyz * rhs.y + czz * rhs.z));
+  }
+  return v3(0, 0, 0);
+}
+
+// revolute_joint.rs:261 warm_start_revolute_joint
+__device__ void warm_start_joint(const DW& w, DJoint& j) {
+  float mA = j.inv_mass_a, mB = j.inv_mass_b;
+  DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+  V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
+  V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
+  float axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
+  V3 ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
+  ang = mul_add(ang, axial, j.rotation_axis_z);
+  va = va - mA * j.linear_impulse;
+  wa = wa - mul_mv(j.inv_ia, cross(ra, j.linear_impulse) + ang);
+  vb = vb + mB * j.linear_impulse;
+  wb = wb + mul_mv(j.inv_ib, cross(rb, j.linear_impulse) + ang);
+  if (sa.flags & kDynamicFlag) { sa.v = va; sa.w = wa; }
+  if (sb.flags & kDynamicFlag) { sb.v = vb; sb.w = wb; }
+  store_state_vw(w, j.index_a, sa);
+  store_state_vw(w, j.index_b, sb);
+}
+
+// revolute_joint.rs:316 solve_revolute_joint
+__device__ void solve_joint(const DW& w, const StepParams& p, DJoint& j, bool use_bias) {
+  float mA = j.inv_mass_a, mB = j.inv_mass_b;
+  M3 iA = j.inv_ia, iB = j.inv_ib;
+  DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+  V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
+  bool fixed = j.fixed_rotation != 0;
+  Q qa = mul_quat(sa.dq, j.frame_a.q);
+  Q qb = mul_quat(sb.dq, j.frame_b.q);
+  if (dot_quat(qa, qb) < 0.0f) qb = quat(v3(-qb.v.x, -qb.v.y, -qb.v.z), -qb.s);
+  Q rq = inv_mul_quat(qa, qb);
+  if (!fixed && (j.enable_spring || j.enable_motor || j.enable_limit)) {
+    V3 axis = j.rotation_axis_z;
+    V3 ga = mul_mv(iA, axis), gb = mul_mv(iB, axis);
+    float k = dot(axis, ga + gb);
+    float acd = dot(wb - wa, axis);
+    float ai = 0.0f;
+    if (j.enable_spring) {
+      float angle = get_twist_angle(rq);
+      float c = angle - j.target_angle;
+      float bias = j.spring_softness.bias_rate * c;
+      float ms = j.spring_softness.mass_scale, is = j.spring_softness.impulse_scale;
+      float di = -ms * j.axial_mass * (acd + bias) - is * j.spring_impulse;
+      j.spring_impulse += di;
+      acd += k * di;
+      ai += di;
+    }
+    if (j.enable_motor) {
+      float cdot = acd - j.motor_speed;
+      float old = j.motor_impulse;
+      float mx = j.max_motor_torque * p.h;
+      float di = clampf(-j.axial_mass * cdot, -mx - old, mx - old);
+      j.motor_impulse = old + di;
+      acd += k * di;
+      ai += di;
+    }
+    if (j.enable_limit) {
+      float angle = get_twist_angle(rq);
+      {
+        float c = angle - j.lower_angle;
+        float bias = 0.0f, ms = 1.0f, is = 0.0f;
+        if (c > 0.0f) bias = c * p.inv_h;
+        else if (use_bias) {
+          bias = j.constraint_softness.bias_rate * c;
+          ms = j.constraint_softness.mass_scale;
+          is = j.constraint_softness.impulse_scale;
+        }
+        float old = j.lower_impulse;
+        float di = maxf(-ms * j.axial_mass * (acd + bias) - is * old, -old);
+        j.lower_impulse = old + di;
+        acd += k * di;
+        ai += di;
+      }
+      {
+        float c = j.upper_angle - angle;
+        float bias = 0.0f, ms = 1.0f, is = 0.0f;
+        if (c > 0.0f) bias = c * p.inv_h;
+        else if (use_bias) {
+          bias = j.constraint_softness.bias_rate * c;
+          ms = j.constraint_softness.mass_scale;
+          is = j.constraint_softness.impulse_scale;
+        }
+        float cdot = -acd;
+        float old = j.upper_impulse;
+        float di = maxf(-ms * j.axial_mass * (cdot + bias) - is * old, -old);
+        j.upper_impulse = old + di;
+        ai -= di;
+      }
+    }
+    wa = wa - ai * ga;
+    wb = wb + ai * gb;
+  }
+  if (!fixed) {
+    V2 bias = v2(0, 0);
+    float ms = 1.0f, is = 0.0f;
+    if (use_bias) {
+      V2 c = v2(rq.v.x, rq.v.y);
+      bias = v2(j.constraint_softness.bias_rate * c.x, j.constraint_softness.bias_rate * c.y);
+      ms = j.constraint_softness.mass_scale;
+      is = j.constraint_softness.impulse_scale;
+    }
+    V3 px = 0.5f * rotate(qa, rq.s * v3(1, 0, 0) + cross(rq.v, v3(1, 0, 0)));
+    V3 py = 0.5f * rotate(qa, rq.s * v3(0, 1, 0) + cross(rq.v, v3(0, 1, 0)));
+    j.perp_axis_x = px;
+    j.perp_axis_y = py;
+    M3 sum = add_mm(iA, iB);
+    float kxx = dot(px, mul_mv(sum, px));
+    float kyy = dot(py, mul_mv(sum, py));
+    float kxy = dot(px, mul_mv(sum, py));
+    M2 K;
+    K.cx = v2(kxx, kxy);
+    K.cy = v2(kxy, kyy);
+    V3 wr = wb - wa;
+    V2 cdot = v2(dot(wr, px), dot(wr, py));
+    V2 old = j.perp_impulse;
+    V2 sol = solve2(K, v2(cdot.x + bias.x, cdot.y + bias.y));
+    V2 di = v2((-ms) * sol.x - is * old.x, (-ms) * sol.y - is * old.y);
+    j.perp_impulse = v2(j.perp_impulse.x + di.x, j.perp_impulse.y + di.y);
+    V3 ang = di.x * px + di.y * py;
+    wa = wa - mul_mv(iA, ang);
+    wb = wb + mul_mv(iB, ang);
+  }
+  {
+    V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
+    V3 cdot = (vb + cross(wb, rb)) - va - cross(wa, ra);
+    V3 bias = v3(0, 0, 0);
+    float ms = 1.0f, is = 0.0f;
+    if (use_bias) {
+      V3 sep = ((sb.dp - sa.dp) + (rb - ra)) + j.delta_center;
+      bias = j.constraint_softness.bias_rate * sep;
+      ms = j.constraint_softness.mass_scale;
+      is = j.constraint_softness.impulse_scale;
+    }
+    V3 b = solve_point_constraint(mA, mB, j.inv_ia, j.inv_ib, ra, rb, cdot + bias);
+    V3 imp = (-ms) * b - is * j.linear_impulse;
+    j.linear_impulse = j.linear_impulse + imp;
+    va = va - mA * imp;
+    wa = wa - mul_mv(iA, cross(ra, imp));
+    vb = vb + mB * imp;
+    wb = wb + mul_mv(iB, cross(rb, imp));
+  }
+  if (sa.flags & kDynamicFlag) { sa.v = va; sa.w = wa; }
+  if (sb.flags & kDynamicFlag) { sb.v = vb; sb.w = wb; }
+  store_state_vw(w, j.index_a, sa);
+  store_state_vw(w, j.index_b, sb);
+}
+
+enum Stage { kWarm = 0, kPush = 1, kRelax = 2, kRestitution = 3 };
+
+__device__ void run_color(const DW& w, const StepParams& p, const JointRanges& jr, const int* coff,
+                          int c, int stage) {
+  int nj = jr.off[c + 1] - jr.off[c];
+  int nc = coff[c + 1] - coff[c];
+  int total = (stage == kRestitution ? 0 : nj) + nc;
+  int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    if (stage != kRestitution && t < nj) {
+      DJoint& j = w.joints[w.joint_list[jr.off[c] + t]];
+      if (stage == kWarm) warm_start_joint(w, j);
+      else solve_joint(w, p, j, stage == kPush);
+    } else {
+      int k = coff[c] + (t - (stage == kRestitution ? 0 : nj));
+      if (stage == kWarm) warm_start_constraint(w, k);
+      else if (stage == kPush) push_constraint(w, p, k);
+      else if (stage == kRelax) relax_constraint(w, p, k);
+      else restitution_constraint(w, p, k);
+    }
+  }
+}
+
+__device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges& jr, int n_ovf, int stage) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (stage != kRestitution) {
+    for (int t = jr.off[kOverflowIndex]; t < jr.off[kOverflowIndex + 1]; ++t) {
+      DJoint& j = w.joints[w.joint_list[t]];
+      if (stage == kWarm) warm_start_joint(w, j);
+      else solve_joint(w, p, j, stage == kPush);
+    }
+  }
+  if (stage == kWarm) warm_start_overflow(w, n_ovf);
+  else if (stage == kPush) push_overflow(w, p, n_ovf);
+  else if (stage == kRelax) relax_overflow(w, p, n_ovf);
+  else restitution_overflow(w, p, n_ovf);
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_solve(DW w, StepParams p, JointRanges jr) {
+  __shared__ int coff[25];
+  __shared__ int n_ovf_s, any_rest_s;
+  if (threadIdx.x < 25) coff[threadIdx.x] = threadIdx.x < 24 ? w.ctl->color_offset[threadIdx.x] : w.ctl->color_offset[23];
+  if (threadIdx.x == 0) { n_ovf_s = w.ctl->overflow_count; any_rest_s = w.ctl->any_restitution; }
+  __syncthreads();
+  int n_ovf = n_ovf_s;
+  bool ovf_work = n_ovf > 0 || jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex];
+  int bar = 0;
+  int stride = gridDim.x * blockDim.x;
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int sub = 0; sub < p.substeps; ++sub) {
+    for (int i = g; i < w.n_awake; i += stride) integrate_velocity(w, p, i);
+    if (!grid_barrier(w.ctl, bar)) return;
+    for (int stage = kWarm; stage <= kRelax; ++stage) {
+      if (stage == kRelax) {
+        for (int i = g; i < w.n_awake; i += stride) integrate_position(w, p, i);
+        if (!grid_barrier(w.ctl, bar)) return;
+      }
+      if (ovf_work) {
+        run_overflow(w, p, jr, n_ovf, stage);
+        if (!grid_barrier(w.ctl, bar)) return;
+      }
+      for (int c = 0; c < kOverflowIndex; ++c) {
+        if (coff[c + 1] == coff[c] && jr.off[c + 1] == jr.off[c]) continue;
+        run_color(w, p, jr, coff, c, stage);
+        if (!grid_barrier(w.ctl, bar)) return;
+      }
+    }
+  }
+  if (any_rest_s && p.restitution_iterations > 0) {
+    for (int it = 0; it < p.restitution_iterations; ++it) {
+      if (n_ovf > 0) {
+        run_overflow(w, p, jr, n_ovf, kRestitution);
+        if (!grid_barrier(w.ctl, bar)) return;
+      }
+      for (int c = 0; c < kOverflowIndex; ++c) {
+        if (coff[c + 1] == coff[c]) continue;
+        run_color(w, p, jr, coff, c, kRestitution);
+        if (!grid_barrier(w.ctl, bar)) return;
+      }
+    }
+  }
+  // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
+  if (g == 0) store_overflow(w, n_ovf);
+  for (int k = g; k < coff[kOverflowIndex]; k += stride) store_constraint(w, k);
+}
+
+// solver_integration.rs:587 finalize_body_range (sleep disabled: bodies never sleep; a fast
+// body is flagged and keeps its previous broadphase bounds, as the reference leaves them
+// to the continuous pass)
+__global__ void k_finalize(DW w, StepParams p) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.n_awake) return;
+  DState st = w.states[i];
+  DSim sim = w.asims[i];
+  float dt = p.dt;
+  V3 v = st.v, wv = st.w;
+  V3 lom = inv_rotate(sim.q, wv);
+  V3 ldr = inv_rotate(sim.q, st.dq.v);
+  Pos center = {sim.cx, sim.cy, sim.cz};
+  center = offset_pos(center, st.dp);
+  sim.cx = center.x; sim.cy = center.y; sim.cz = center.z;
+  sim.q = normalize_quat(mul_quat(st.dq, sim.q));
+  V3 varc = modified_cross(abs3(lom), sim.max_extent);
+  float maxv = length(v) + length(varc);
+  V3 rarc = modified_cross(abs3(ldr), sim.max_extent);
+  float maxdp = length(st.dp) + 2.0f * length(rarc);
+  st.dp = v3(0, 0, 0);
+  st.dq = qid();
+  Pos tp = offset_pos(center, -rotate(sim.q, sim.local_center));
+  sim.px = tp.x; sim.py = tp.y; sim.pz = tp.z;
+  sim.force = v3(0, 0, 0);
+  sim.torque = v3(0, 0, 0);
+  sim.flags &= ~(kIsFast | kTransient);
+  st.flags &= ~kTransient;
+  float max_motion = maxf(maxdp, maxv * dt);
+  if (p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
+    sim.flags |= kIsFast;
+    atomicAdd(&w.ctl->fast_flags, 1);
+  }
+  M3 R = matrix_from_quat(sim.q);
+  sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
+  if ((sim.flags & kIsFast) == 0) {
+    WXf xf_;
+    xf_.p = tp; xf_.q = sim.q;
+    float spec = speculative_distance();
+    for (int k = sim.shape_begin; k < sim.shape_end; ++k) {
+      int sid = w.body_shapes[k];
+      const DShape& sh = w.shapes[sid];
+      // shape_runtime.rs:405-427 compute_fat_shape_aabb
+      Xf lt = xf(v3(0, 0, 0), xf_.q);
+      AABB a;
+      if (sh.type == kHull) {
+        a = aabb_transform(lt, w.hulls[sh.hull].bounds);
+      } else if (sh.type == kSphere) {
+        V3 c = xf_point(lt, sh.sphere.center);
+        float r = sh.sphere.radius;
+        V3 e = v3(r, r, r);
+        a = aabb(c - e, c + e);
+      } else {
+        V3 c1 = xf_point(lt, sh.capsule.c1), c2 = xf_point(lt, sh.capsule.c2);
+        float r = sh.capsule.radius;
+        V3 e = v3(r, r, r);
+        a = aabb(min3(c1, c2) - e, max3(c1, c2) + e);
+      }
+      a = offset_aabb(aabb_inflate(a, spec), xf_.p);
+      if (!aabb_contains(w.fat[sid], a)) {
+        w.fat[sid] = aabb_inflate(a, sh.aabb_margin);
+        w.moved[sid] = 1;
+        atomicAdd(&w.ctl->moved_count, 1);
+      }
+    }
+  }
+  w.states[i] = st;
+  w.asims[i] = sim;
+}
+
+}  // namespace nsd

@@ -1,0 +1,189 @@
+"""Seeded synthetic scenes for the rigid-body step.
+
+Every builder takes a world object exposing ``create_body``, ``create_box``,
+``create_sphere``, ``create_capsule`` and ``create_revolute`` and returns a
+dict describing the scene. Values are generated as float32 (positions
+widened to float64 exactly) so the same call sequence builds bit-identical
+scenes in any world implementation with this interface.
+
+- :func:`large_pyramid`, :func:`many_pyramids`: the reference benchmark scenes
+  (src/bin/benchmarks/scenes.rs:105 and :170), used with the reference's
+  golden state hashes.
+- :func:`box_pyramid`: a 20-wide pyramid of 1 m cubes (210 bodies).
+- :func:`large_pile`: 10 000 mixed boxes/spheres/capsules dropped onto a
+  ground box.
+- :func:`jointed_chains`: capsule chains linked by limited revolute joints
+  with loose boxes falling onto them.
+"""
+import numpy as np
+
+STATIC = 0
+DYNAMIC = 2
+F = np.float32
+
+
+def _f(x):
+    return float(np.float32(x))
+
+
+def large_pyramid(world, base_count=100):
+    """scenes.rs:105 create_large_pyramid (default world: gravity -10)."""
+    g = world.create_body(type=STATIC, position=(0.0, -1.0, 0.0))
+    world.create_box(g, 400.0, 1.0, 400.0)
+    h = F(0.5)
+    shift = h
+    n = 0
+    for i in range(base_count):
+        y = (F(2.0) * F(i) + F(1.0)) * shift
+        for j in range(i, base_count):
+            x = (F(i) + F(1.0)) * shift + F(2.0) * F(j - i) * shift - h * F(base_count)
+            b = world.create_body(type=DYNAMIC, position=(float(x), float(y), 0.0))
+            world.create_box(b, float(h), float(h), float(h), density=100.0)
+            n += 1
+    return {"name": "large_pyramid", "dynamic_bodies": n}
+
+
+def many_pyramids(world, base_count=10, rows=14, cols=14):
+    """scenes.rs:170 create_many_pyramids."""
+    extent = F(0.5)
+    ground_extent = extent * F(cols) * (F(base_count) + F(1.0))
+    g = world.create_body(type=STATIC, position=(0.0, -1.0, 0.0))
+    world.create_box(g, float(ground_extent), 1.0, float(ground_extent))
+    base_width = F(2.0) * extent * F(base_count)
+    base_z = -ground_extent + F(2.0) * extent
+    delta_z = F(2.0) * (ground_extent - F(2.0) * extent) / F(rows - 1)
+    z = base_z
+    n = 0
+    for _ in range(rows):
+        for j in range(cols):
+            cx = -ground_extent + F(j) * (base_width + F(2.0) * extent) + F(2.0) * extent
+            for i in range(base_count):
+                y = (F(2.0) * F(i) + F(1.0)) * extent
+                for k in range(i, base_count):
+                    x = (F(i) + F(1.0)) * extent + F(2.0) * F(k - i) * extent + cx - F(0.5)
+                    b = world.create_body(type=DYNAMIC, position=(float(x), float(y), float(z)), enable_sleep=False)
+                    world.create_box(b, float(extent), float(extent), float(extent), density=100.0)
+                    n += 1
+        z = z + delta_z
+    return {"name": "many_pyramids", "dynamic_bodies": n}
+
+
+def box_pyramid(world, base=20, seed=1):
+    """20-wide pyramid of 1 m cubes (base 20 -> 210 cubes), 1.05 m spacing with x/z jitter."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
+    world.create_box(g, 50.0, 0.5, 50.0, friction=0.6)
+    n = 0
+    for i in range(base):
+        count = base - i
+        for j in range(count):
+            jx, jz = rng.uniform(-0.01, 0.01, 2).astype(np.float32)
+            x = F((F(j) - F(0.5) * F(count - 1)) * F(1.05)) + jx
+            y = F(0.5) + F(1.0) * F(i)
+            b = world.create_body(type=DYNAMIC, position=(float(x), float(y), float(jz)))
+            world.create_box(b, 0.5, 0.5, 0.5, density=1000.0, friction=0.6, restitution=0.0)
+            n += 1
+    return {"name": "box_pyramid", "dynamic_bodies": n}
+
+
+def _random_quats(rng, n):
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return q.astype(np.float32)
+
+
+def large_pile(world, n=10000, seed=2, ground_half=50.0):
+    """10 000 dynamic bodies (60% boxes, 25% spheres, 15% capsules) dropped from a 40x60x40 m volume."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
+    world.create_box(g, ground_half, 0.5, ground_half, friction=0.6)
+    n_box = int(round(0.6 * n))
+    n_sph = int(round(0.25 * n))
+    kinds = np.array([0] * n_box + [1] * n_sph + [2] * (n - n_box - n_sph))
+    rng.shuffle(kinds)
+    pos = np.stack([rng.uniform(-20.0, 20.0, n), rng.uniform(1.0, 61.0, n), rng.uniform(-20.0, 20.0, n)], 1).astype(np.float32)
+    quats = _random_quats(rng, n)
+    box_h = rng.uniform(0.25, 0.75, (n, 3)).astype(np.float32)
+    sph_r = rng.uniform(0.2, 0.6, n).astype(np.float32)
+    cap_r = rng.uniform(0.15, 0.4, n).astype(np.float32)
+    cap_hh = rng.uniform(0.2, 0.8, n).astype(np.float32)
+    density = rng.uniform(500.0, 2000.0, n).astype(np.float32)
+    friction = rng.uniform(0.3, 0.9, n).astype(np.float32)
+    for i in range(n):
+        b = world.create_body(type=DYNAMIC, position=tuple(float(v) for v in pos[i]),
+                              rotation=tuple(float(v) for v in quats[i]))
+        mat = dict(density=float(density[i]), friction=float(friction[i]), restitution=0.0)
+        if kinds[i] == 0:
+            world.create_box(b, float(box_h[i, 0]), float(box_h[i, 1]), float(box_h[i, 2]), **mat)
+        elif kinds[i] == 1:
+            world.create_sphere(b, float(sph_r[i]), **mat)
+        else:
+            hh = float(cap_hh[i])
+            world.create_capsule(b, (0.0, -hh, 0.0), (0.0, hh, 0.0), float(cap_r[i]), **mat)
+    return {"name": "large_pile", "dynamic_bodies": n, "boxes": n_box, "spheres": n_sph,
+            "capsules": n - n_box - n_sph}
+
+
+def _axis_angle_quat(axis, angle):
+    s, c = np.sin(0.5 * angle), np.cos(0.5 * angle)
+    return (float(F(axis[0] * s)), float(F(axis[1] * s)), float(F(axis[2] * s)), float(F(c)))
+
+
+def jointed_chains(world, chains=2000, links=24, boxes=4000, seed=3, grid=45, spacing=2.0, height=30.0):
+    """Capsule chains (r 0.1, half-height 0.25) on revolute joints limited to +-60 degrees,
+    plus loose boxes (half-extent 0.3) falling onto them."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
+    world.create_box(g, 100.0, 0.5, 100.0, friction=0.6)
+    r, hh = 0.1, 0.25
+    link = 2.0 * hh
+    limit = float(F(np.pi / 3.0))
+    n_joints = 0
+    half = 0.5 * (grid - 1) * spacing
+    for c in range(chains):
+        gx, gz = c % grid, c // grid
+        ax, az = gx * spacing - half, gz * spacing - half
+        anchor = world.create_body(type=STATIC, position=(float(F(ax)), float(F(height)), float(F(az))))
+        prev = anchor
+        prev_frame = (0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0)
+        angles = rng.uniform(-0.3, 0.3, links).astype(np.float32)
+        for k in range(links):
+            y = height - (k + 0.5) * link
+            b = world.create_body(type=DYNAMIC, position=(float(F(ax)), float(F(y)), float(F(az))))
+            world.create_capsule(b, (0.0, -hh, 0.0), (0.0, hh, 0.0), r, density=1000.0, friction=0.6)
+            q = _axis_angle_quat((0.0, 0.0, 1.0), float(angles[k]))
+            frame_b = (0.0, hh, 0.0) + q
+            world.create_revolute(prev, b, prev_frame, frame_b, enable_limit=True, lower=-limit, upper=limit)
+            n_joints += 1
+            prev = b
+            prev_frame = (0.0, -hh, 0.0, 0.0, 0.0, 0.0, 1.0)
+    pos = np.stack([rng.uniform(-half, half, boxes), rng.uniform(height + 2.0, height + 22.0, boxes),
+                    rng.uniform(-half, half, boxes)], 1).astype(np.float32)
+    quats = _random_quats(rng, boxes)
+    for i in range(boxes):
+        b = world.create_body(type=DYNAMIC, position=tuple(float(v) for v in pos[i]),
+                              rotation=tuple(float(v) for v in quats[i]))
+        world.create_box(b, 0.3, 0.3, 0.3, density=1000.0, friction=0.6)
+    return {"name": "jointed_chains", "dynamic_bodies": chains * links + boxes, "joints": n_joints}
+
+
+WORLD_SETTINGS = {
+    # gravity per scene: the reference scenes use the World default (-10); the synthetic
+    # configurations use -9.81. Parity runs keep continuous collision off (fast bodies are
+    # only flagged; the continuous pass itself is outside this path).
+    "large_pyramid": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
+    "many_pyramids": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
+    "box_pyramid": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
+    "large_pile": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
+    "jointed_chains": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
+}
+
+SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8}
+
+BUILDERS = {
+    "large_pyramid": large_pyramid,
+    "many_pyramids": many_pyramids,
+    "box_pyramid": box_pyramid,
+    "large_pile": large_pile,
+    "jointed_chains": jointed_chains,
+}

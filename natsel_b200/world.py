@@ -1,0 +1,265 @@
+"""Python view of libnatsel_gpu.so, mirroring the reference World API.
+
+The reference engine exposes ``World::create_body``, ``create_hull_shape``
+(boxes via ``make_box_hull``), ``create_sphere_shape``,
+``create_capsule_shape``, ``create_revolute_joint`` and ``step(dt, substeps)``
+(src/simulation/world_runtime.rs:1506, shape_creation.rs:504-569,
+revolute_joint.rs:162, solver_integration.rs:807). :class:`World` offers the
+same calls over the C ABI declared in ``include/natsel_gpu.h``; there is no
+CPU fallback: constructing a World without the CUDA library or a GPU raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnatsel_gpu.so")
+
+STATIC_BODY = 0
+DYNAMIC_BODY = 2
+
+
+class NsError(RuntimeError):
+    """A natsel_gpu call returned a non-zero status."""
+
+    def __init__(self, code, message):
+        super().__init__(f"natsel_gpu error {code}: {message}")
+        self.code = code
+
+
+class WorldDef(ctypes.Structure):
+    _fields_ = [
+        ("gravity", ctypes.c_float * 3),
+        ("enable_sleep", ctypes.c_int),
+        ("enable_continuous", ctypes.c_int),
+        ("enable_warm_starting", ctypes.c_int),
+        ("contact_hertz", ctypes.c_float),
+        ("contact_damping_ratio", ctypes.c_float),
+        ("contact_speed", ctypes.c_float),
+        ("max_linear_speed", ctypes.c_float),
+        ("restitution_threshold", ctypes.c_float),
+        ("restitution_iterations", ctypes.c_int),
+        ("joint_hertz", ctypes.c_float),
+        ("joint_damping_ratio", ctypes.c_float),
+        ("contact_capacity", ctypes.c_int),
+        ("solver_blocks", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+class BodyDef(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("position", ctypes.c_double * 3),
+        ("rotation", ctypes.c_float * 4),
+        ("linear_velocity", ctypes.c_float * 3),
+        ("angular_velocity", ctypes.c_float * 3),
+        ("linear_damping", ctypes.c_float),
+        ("angular_damping", ctypes.c_float),
+        ("gravity_scale", ctypes.c_float),
+        ("enable_sleep", ctypes.c_int),
+    ]
+
+
+class ShapeDef(ctypes.Structure):
+    _fields_ = [
+        ("density", ctypes.c_float),
+        ("friction", ctypes.c_float),
+        ("restitution", ctypes.c_float),
+        ("rolling_resistance", ctypes.c_float),
+        ("category_bits", ctypes.c_uint64),
+        ("mask_bits", ctypes.c_uint64),
+        ("group_index", ctypes.c_int),
+    ]
+
+
+_F3 = ctypes.c_float * 3
+_F7 = ctypes.c_float * 7
+_lib = None
+
+EXPORTED = [
+    "ns_default_world_def", "ns_world_create", "ns_world_destroy", "ns_last_error",
+    "ns_create_body", "ns_create_box_shape", "ns_create_sphere_shape", "ns_create_capsule_shape",
+    "ns_create_revolute_joint", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
+    "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
+    "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
+]
+
+
+def load_library(path=LIB_PATH):
+    """Load libnatsel_gpu.so and declare its signatures. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with natsel_b200._build.build()")
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    lib.ns_default_world_def.argtypes = [ctypes.POINTER(WorldDef)]
+    lib.ns_world_create.argtypes = [ctypes.POINTER(WorldDef)]
+    lib.ns_world_create.restype = P
+    lib.ns_world_destroy.argtypes = [P]
+    lib.ns_last_error.argtypes = [P]
+    lib.ns_last_error.restype = ctypes.c_char_p
+    lib.ns_create_body.argtypes = [P, ctypes.POINTER(BodyDef)]
+    lib.ns_create_box_shape.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef)] + [ctypes.c_float] * 3
+    lib.ns_create_sphere_shape.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef), _F3, ctypes.c_float]
+    lib.ns_create_capsule_shape.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef), _F3, _F3, ctypes.c_float]
+    lib.ns_create_revolute_joint.argtypes = [P, ctypes.c_int, ctypes.c_int, _F7, _F7, ctypes.c_int,
+                                             ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
+                                             ctypes.c_float, ctypes.c_float, ctypes.c_int]
+    lib.ns_world_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
+    lib.ns_world_synchronize.argtypes = [P]
+    lib.ns_world_get_bodies.argtypes = [P, P, P, P, P]
+    lib.ns_world_body_count.argtypes = [P]
+    lib.ns_world_state_hash.argtypes = [P, ctypes.POINTER(ctypes.c_uint64)]
+    lib.ns_world_contact_capacity.argtypes = [P]
+    lib.ns_world_get_contacts.argtypes = [P, P, P, P, ctypes.c_int]
+    lib.ns_world_counters.argtypes = [P, P]
+    lib.ns_world_phase_times.argtypes = [P, P]
+    lib.ns_world_stream.argtypes = [P]
+    lib.ns_world_stream.restype = P
+    lib.ns_world_solver_counts.argtypes = [P, P]
+    _lib = lib
+    return lib
+
+
+def default_world_def(**overrides):
+    lib = load_library()
+    d = WorldDef()
+    lib.ns_default_world_def(ctypes.byref(d))
+    for k, v in overrides.items():
+        if k == "gravity":
+            d.gravity = (ctypes.c_float * 3)(*v)
+        else:
+            setattr(d, k, v)
+    return d
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class World:
+    """A device-resident world. Methods follow the reference World API."""
+
+    def __init__(self, world_def=None, **overrides):
+        self._lib = load_library()
+        d = world_def if world_def is not None else default_world_def(**overrides)
+        self._w = self._lib.ns_world_create(ctypes.byref(d))
+        if not self._w:
+            raise NsError(1, self._lib.ns_last_error(None).decode())
+        self.body_types = []
+
+    def close(self):
+        if getattr(self, "_w", None):
+            self._lib.ns_world_destroy(self._w)
+            self._w = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, status):
+        if status != 0:
+            raise NsError(status, self._lib.ns_last_error(self._w).decode())
+
+    def _id(self, value):
+        if value < 0:
+            raise NsError(1, self._lib.ns_last_error(self._w).decode())
+        return value
+
+    # scene construction -------------------------------------------------
+    def create_body(self, type=DYNAMIC_BODY, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0),
+                    linear_velocity=(0.0, 0.0, 0.0), angular_velocity=(0.0, 0.0, 0.0),
+                    linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, enable_sleep=True):
+        b = BodyDef()
+        b.type = type
+        b.position = (ctypes.c_double * 3)(*position)
+        b.rotation = (ctypes.c_float * 4)(*rotation)
+        b.linear_velocity = (ctypes.c_float * 3)(*linear_velocity)
+        b.angular_velocity = (ctypes.c_float * 3)(*angular_velocity)
+        b.linear_damping, b.angular_damping, b.gravity_scale = linear_damping, angular_damping, gravity_scale
+        b.enable_sleep = 1 if enable_sleep else 0
+        self.body_types.append(type)
+        return self._id(self._lib.ns_create_body(self._w, ctypes.byref(b)))
+
+    @staticmethod
+    def shape_def(density=1000.0, friction=0.6, restitution=0.0, rolling_resistance=0.0,
+                  category_bits=1, mask_bits=0xFFFFFFFFFFFFFFFF, group_index=0):
+        s = ShapeDef()
+        s.density, s.friction, s.restitution, s.rolling_resistance = density, friction, restitution, rolling_resistance
+        s.category_bits, s.mask_bits, s.group_index = category_bits, mask_bits, group_index
+        return s
+
+    def create_box(self, body, hx, hy, hz, **shape):
+        return self._id(self._lib.ns_create_box_shape(self._w, body, ctypes.byref(self.shape_def(**shape)), hx, hy, hz))
+
+    def create_sphere(self, body, radius, center=(0.0, 0.0, 0.0), **shape):
+        return self._id(self._lib.ns_create_sphere_shape(self._w, body, ctypes.byref(self.shape_def(**shape)),
+                                                         _F3(*center), radius))
+
+    def create_capsule(self, body, center1, center2, radius, **shape):
+        return self._id(self._lib.ns_create_capsule_shape(self._w, body, ctypes.byref(self.shape_def(**shape)),
+                                                          _F3(*center1), _F3(*center2), radius))
+
+    def create_revolute(self, body_a, body_b, frame_a, frame_b, enable_limit=False, lower=0.0, upper=0.0,
+                        enable_spring=False, hertz=0.0, damping_ratio=0.0, max_motor_torque=0.0,
+                        collide_connected=False):
+        return self._id(self._lib.ns_create_revolute_joint(
+            self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b), int(enable_limit), lower, upper,
+            int(enable_spring), hertz, damping_ratio, max_motor_torque, int(collide_connected)))
+
+    # stepping and readback ----------------------------------------------
+    def step(self, dt=1.0 / 60.0, substeps=4):
+        self._check(self._lib.ns_world_step(self._w, dt, substeps))
+
+    def synchronize(self):
+        self._check(self._lib.ns_world_synchronize(self._w))
+
+    @property
+    def body_count(self):
+        return self._lib.ns_world_body_count(self._w)
+
+    def bodies(self):
+        n = self.body_count
+        pos = np.zeros((n, 3), np.float64)
+        rot = np.zeros((n, 4), np.float32)
+        lin = np.zeros((n, 3), np.float32)
+        ang = np.zeros((n, 3), np.float32)
+        self._check(self._lib.ns_world_get_bodies(self._w, _ptr(pos), _ptr(rot), _ptr(lin), _ptr(ang)))
+        return pos, rot, lin, ang
+
+    def state_hash(self):
+        out = ctypes.c_uint64(0)
+        self._check(self._lib.ns_world_state_hash(self._w, ctypes.byref(out)))
+        return out.value
+
+    def contacts(self):
+        cap = self._lib.ns_world_contact_capacity(self._w)
+        cap = max(cap, 1)
+        ints = np.zeros((cap, 8), np.int32)
+        feats = np.zeros((cap, 4), np.uint32)
+        fl = np.zeros((cap, 24), np.float32)
+        n = self._lib.ns_world_get_contacts(self._w, _ptr(ints), _ptr(feats), _ptr(fl), cap)
+        if n < 0:
+            raise NsError(2, self._lib.ns_last_error(self._w).decode())
+        return ints[:n], feats[:n], fl[:n]
+
+    def counters(self):
+        out = np.zeros(32, np.int32)
+        self._check(self._lib.ns_world_counters(self._w, _ptr(out)))
+        return out
+
+    def phase_times(self):
+        out = np.zeros(5, np.float32)
+        self._check(self._lib.ns_world_phase_times(self._w, _ptr(out)))
+        return out
+
+    def solver_counts(self):
+        out = np.zeros(8, np.int64)
+        self._check(self._lib.ns_world_solver_counts(self._w, _ptr(out)))
+        return out
+
+    def stream(self):
+        return self._lib.ns_world_stream(self._w)

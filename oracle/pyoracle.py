@@ -1,0 +1,209 @@
+"""ctypes wrapper of the oracle (libns_oracle.so).
+
+TEST INFRASTRUCTURE ONLY. The oracle is the CPU restatement of the
+reference's scalar world step; tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use it as the parity checker. The product package never
+imports this module. The method names match natsel_b200.world.World so one
+scene builder drives both.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libns_oracle.so")
+SOURCES = ["ns_world.cpp", "ns_math.hpp", "ns_collide.hpp", "ns_joint.hpp", "ns_oracle.h"]
+
+STATIC_BODY = 0
+DYNAMIC_BODY = 2
+
+
+def build(force=False):
+    """Compile libns_oracle.so with g++ (IEEE f32, no contraction)."""
+    if not force and os.path.exists(LIB_PATH):
+        t = os.path.getmtime(LIB_PATH)
+        if all(os.path.getmtime(os.path.join(HERE, s)) <= t for s in SOURCES):
+            return LIB_PATH
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+class WorldDef(ctypes.Structure):
+    _fields_ = [
+        ("gravity", ctypes.c_float * 3),
+        ("enable_sleep", ctypes.c_int),
+        ("enable_continuous", ctypes.c_int),
+        ("enable_warm_starting", ctypes.c_int),
+        ("contact_hertz", ctypes.c_float),
+        ("contact_damping_ratio", ctypes.c_float),
+        ("contact_speed", ctypes.c_float),
+        ("max_linear_speed", ctypes.c_float),
+        ("restitution_threshold", ctypes.c_float),
+        ("restitution_iterations", ctypes.c_int),
+        ("joint_hertz", ctypes.c_float),
+        ("joint_damping_ratio", ctypes.c_float),
+    ]
+
+
+class BodyDef(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("position", ctypes.c_double * 3),
+        ("rotation", ctypes.c_float * 4),
+        ("linear_velocity", ctypes.c_float * 3),
+        ("angular_velocity", ctypes.c_float * 3),
+        ("linear_damping", ctypes.c_float),
+        ("angular_damping", ctypes.c_float),
+        ("gravity_scale", ctypes.c_float),
+        ("enable_sleep", ctypes.c_int),
+    ]
+
+
+class ShapeDef(ctypes.Structure):
+    _fields_ = [
+        ("density", ctypes.c_float),
+        ("friction", ctypes.c_float),
+        ("restitution", ctypes.c_float),
+        ("rolling_resistance", ctypes.c_float),
+        ("category_bits", ctypes.c_uint64),
+        ("mask_bits", ctypes.c_uint64),
+        ("group_index", ctypes.c_int),
+    ]
+
+
+_F3 = ctypes.c_float * 3
+_F7 = ctypes.c_float * 7
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    build()
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    lib.nso_default_world_def.argtypes = [ctypes.POINTER(WorldDef)]
+    lib.nso_create.argtypes = [ctypes.POINTER(WorldDef)]
+    lib.nso_create.restype = P
+    lib.nso_destroy.argtypes = [P]
+    lib.nso_create_body.argtypes = [P, ctypes.POINTER(BodyDef)]
+    lib.nso_create_box.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef)] + [ctypes.c_float] * 3
+    lib.nso_create_sphere.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef), _F3, ctypes.c_float]
+    lib.nso_create_capsule.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef), _F3, _F3, ctypes.c_float]
+    lib.nso_create_revolute.argtypes = [P, ctypes.c_int, ctypes.c_int, _F7, _F7, ctypes.c_int, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_int]
+    lib.nso_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
+    lib.nso_state_hash.argtypes = [P]
+    lib.nso_state_hash.restype = ctypes.c_uint64
+    lib.nso_body_count.argtypes = [P]
+    lib.nso_get_bodies.argtypes = [P, P, P, P, P]
+    lib.nso_contact_capacity.argtypes = [P]
+    lib.nso_get_contacts.argtypes = [P, P, P, P]
+    lib.nso_counters.argtypes = [P, P]
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class OracleWorld:
+    """CPU oracle world with the same scene-building calls as natsel_b200.World."""
+
+    def __init__(self, gravity=(0.0, -10.0, 0.0), enable_continuous=True, enable_warm_starting=True,
+                 **overrides):
+        self._lib = load()
+        d = WorldDef()
+        self._lib.nso_default_world_def(ctypes.byref(d))
+        d.gravity = (ctypes.c_float * 3)(*gravity)
+        d.enable_continuous = int(enable_continuous)
+        d.enable_warm_starting = int(enable_warm_starting)
+        for k, v in overrides.items():
+            if hasattr(d, k):
+                setattr(d, k, v)
+        self._w = self._lib.nso_create(ctypes.byref(d))
+        self.body_types = []
+
+    def close(self):
+        if getattr(self, "_w", None):
+            self._lib.nso_destroy(self._w)
+            self._w = None
+
+    def __del__(self):
+        self.close()
+
+    def create_body(self, type=DYNAMIC_BODY, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0),
+                    linear_velocity=(0.0, 0.0, 0.0), angular_velocity=(0.0, 0.0, 0.0),
+                    linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, enable_sleep=True):
+        b = BodyDef()
+        b.type = type
+        b.position = (ctypes.c_double * 3)(*position)
+        b.rotation = (ctypes.c_float * 4)(*rotation)
+        b.linear_velocity = (ctypes.c_float * 3)(*linear_velocity)
+        b.angular_velocity = (ctypes.c_float * 3)(*angular_velocity)
+        b.linear_damping, b.angular_damping, b.gravity_scale = linear_damping, angular_damping, gravity_scale
+        b.enable_sleep = 1 if enable_sleep else 0
+        self.body_types.append(type)
+        return self._lib.nso_create_body(self._w, ctypes.byref(b))
+
+    @staticmethod
+    def shape_def(density=1000.0, friction=0.6, restitution=0.0, rolling_resistance=0.0,
+                  category_bits=1, mask_bits=0xFFFFFFFFFFFFFFFF, group_index=0):
+        s = ShapeDef()
+        s.density, s.friction, s.restitution, s.rolling_resistance = density, friction, restitution, rolling_resistance
+        s.category_bits, s.mask_bits, s.group_index = category_bits, mask_bits, group_index
+        return s
+
+    def create_box(self, body, hx, hy, hz, **shape):
+        return self._lib.nso_create_box(self._w, body, ctypes.byref(self.shape_def(**shape)), hx, hy, hz)
+
+    def create_sphere(self, body, radius, center=(0.0, 0.0, 0.0), **shape):
+        return self._lib.nso_create_sphere(self._w, body, ctypes.byref(self.shape_def(**shape)), _F3(*center), radius)
+
+    def create_capsule(self, body, center1, center2, radius, **shape):
+        return self._lib.nso_create_capsule(self._w, body, ctypes.byref(self.shape_def(**shape)),
+                                            _F3(*center1), _F3(*center2), radius)
+
+    def create_revolute(self, body_a, body_b, frame_a, frame_b, enable_limit=False, lower=0.0, upper=0.0,
+                        enable_spring=False, hertz=0.0, damping_ratio=0.0, max_motor_torque=0.0,
+                        collide_connected=False):
+        return self._lib.nso_create_revolute(self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b),
+                                             int(enable_limit), lower, upper, int(enable_spring), hertz,
+                                             damping_ratio, max_motor_torque, int(collide_connected))
+
+    def step(self, dt=1.0 / 60.0, substeps=4):
+        self._lib.nso_step(self._w, dt, substeps)
+
+    @property
+    def body_count(self):
+        return self._lib.nso_body_count(self._w)
+
+    def bodies(self):
+        n = self.body_count
+        pos = np.zeros((n, 3), np.float64)
+        rot = np.zeros((n, 4), np.float32)
+        lin = np.zeros((n, 3), np.float32)
+        ang = np.zeros((n, 3), np.float32)
+        self._lib.nso_get_bodies(self._w, _ptr(pos), _ptr(rot), _ptr(lin), _ptr(ang))
+        return pos, rot, lin, ang
+
+    def state_hash(self):
+        return self._lib.nso_state_hash(self._w)
+
+    def contacts(self):
+        cap = max(self._lib.nso_contact_capacity(self._w), 1)
+        ints = np.zeros((cap, 8), np.int32)
+        feats = np.zeros((cap, 4), np.uint32)
+        fl = np.zeros((cap, 24), np.float32)
+        n = self._lib.nso_get_contacts(self._w, _ptr(ints), _ptr(feats), _ptr(fl))
+        return ints[:n], feats[:n], fl[:n]
+
+    def counters(self):
+        out = np.zeros(32, np.int32)
+        self._lib.nso_counters(self._w, _ptr(out))
+        return out
