@@ -126,6 +126,31 @@ void* ns_world_stream(ns_world* world);
  * [3] colored points [4] static sides [5] joints [6] overflow manifolds [7] restitution on. */
 int ns_world_solver_counts(ns_world* world, int64_t* counts8);
 
+/* Batch narrowphase (replaces the per-pair routines collide_hulls_with_scratch
+ * convex_manifold.rs:1445, collide_spheres / collide_capsule_and_sphere /
+ * collide_capsules / collide_hull_and_sphere / collide_hull_and_capsule
+ * convex_manifold_shapes.rs:21-643). Types: 0 capsule, 3 box hull, 5 sphere; A is
+ * the primary type (capsule > sphere, hull > sphere/capsule). geom: box hx,hy,hz;
+ * sphere cx,cy,cz,r; capsule c1 xyz, c2 xyz, r. xf = B in A's frame (p xyz, q xyzs).
+ * The SAT/simplex caches are read and written back. Runs one device thread per pair. */
+typedef struct {
+  int32_t type_a, type_b;
+  float geom_a[7], geom_b[7];
+  float xf[7];
+  float sat_separation;
+  int32_t sat_type, sat_index_a, sat_index_b, sat_hit;
+  float simplex_metric;
+  int32_t simplex_count, simplex_ia[4], simplex_ib[4];
+} ns_pair_job;
+typedef struct {
+  float normal[3];
+  int32_t point_count;
+  float points[4][4]; /* x, y, z, separation in frame A */
+  uint32_t feature_ids[4];
+} ns_pair_result;
+/* Synchronous; host arrays; device 0 unless ns_world-independent device selection is added. */
+int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count);
+
 #ifdef __cplusplus
 }
 #endif

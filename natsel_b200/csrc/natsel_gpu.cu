@@ -315,9 +315,37 @@ int upload(ns_world* w, T* dst, const std::vector<T>& src) {
   return NS_OK;
 }
 
+// The narrowphase keeps the reference's 64-vertex clip buffers on the thread stack (about
+// 2.5 KB). The default per-thread stack limit is 1 KB, so the limit is raised to the largest
+// local-memory size of the step kernels before anything runs.
+int ensure_stack(ns_world* w) {
+  size_t need = 0;
+  cudaFuncAttributes a;
+  const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_jobs, (const void*)k_solve,
+                           (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
+                           (const void*)k_finalize, (const void*)k_state_pass};
+  for (const void* k : kernels) {
+    cudaError_t e = cudaFuncGetAttributes(&a, k);
+    if (e != cudaSuccess) return fail(w, NS_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
+    if (a.localSizeBytes > need) need = a.localSizeBytes;
+  }
+  need = ((need + 1023) / 1024) * 1024 + 1024;
+  size_t cur = 0;
+  cudaDeviceGetLimit(&cur, cudaLimitStackSize);
+  if (cur < need) {
+    cudaError_t e = cudaDeviceSetLimit(cudaLimitStackSize, need);
+    if (e != cudaSuccess) return fail(w, NS_ERR_CUDA, "cudaDeviceSetLimit(stack %zu): %s", need, cudaGetErrorString(e));
+  }
+  return NS_OK;
+}
+
 int upload_world(ns_world* w) {
   if (w->def.enable_sleep) return fail(w, NS_ERR_UNSUPPORTED, "sleeping islands are not supported");
   NS_CUDA(w, cudaSetDevice(w->def.device));
+  {
+    int st0 = ensure_stack(w);
+    if (st0) return st0;
+  }
   NS_CUDA(w, cudaDeviceGetAttribute(&w->sm_count, cudaDevAttrMultiProcessorCount, w->def.device));
   NS_CUDA(w, cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
   for (int i = 0; i < 6; ++i) NS_CUDA(w, cudaEventCreate(&w->ev[i]));
@@ -923,6 +951,32 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   out[4] = stat;
   out[6] = c.overflow_count;
   out[7] = c.any_restitution;
+  return NS_OK;
+}
+
+int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count) {
+  static_assert(sizeof(ns_pair_job) == sizeof(PairJob), "pair job layout");
+  static_assert(sizeof(ns_pair_result) == sizeof(PairResult), "pair result layout");
+  if (count < 0 || (count > 0 && (!jobs || !results))) return fail(nullptr, NS_ERR_INVALID, "invalid pair batch");
+  if (count == 0) return NS_OK;
+  {
+    int st0 = ensure_stack(nullptr);
+    if (st0) return st0;
+  }
+  PairJob* dj = nullptr;
+  PairResult* dr = nullptr;
+  cudaError_t e = cudaMalloc(&dj, sizeof(PairJob) * (size_t)count);
+  if (e == cudaSuccess) e = cudaMalloc(&dr, sizeof(PairResult) * (size_t)count);
+  if (e == cudaSuccess) e = cudaMemcpy(dj, jobs, sizeof(PairJob) * (size_t)count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_collide_jobs<<<(count + 127) / 128, 128>>>(dj, dr, count);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(jobs, dj, sizeof(PairJob) * (size_t)count, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(results, dr, sizeof(PairResult) * (size_t)count, cudaMemcpyDeviceToHost);
+  if (dj) cudaFree(dj);
+  if (dr) cudaFree(dr);
+  if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs: %s", cudaGetErrorString(e));
   return NS_OK;
 }
 

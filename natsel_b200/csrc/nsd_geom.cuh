@@ -1024,35 +1024,49 @@ NSD_HD V3 closest_on_simplex(const Simplex& s) {                                
   return v3(0, 0, 0);
 }
 
-// distance.rs:543 shape_distance with use_radii = false (the only form used here)
+// distance.rs:543 shape_distance with use_radii = false (the only form used here).
+// The reference restores the previous simplex by value when an iteration does not make
+// progress; here the loop instead records which of the two simplices is final and the
+// epilogue reads that one. Same result, but the restore never becomes a whole-struct
+// copy (ptxas -O3 dropped the barycentric weights of such a restore in this loop).
+NSD_HD void simplex_vertex(SVert* v, const V3* pa, const V3* pb, int i1, int i2, const M3& m, V3 p) {
+  V3 w1 = pa[i1];
+  V3 w2 = mul_mv(m, pb[i2]) + p;
+  v->ia = i1; v->ib = i2; v->wa = w1; v->wb = w2; v->w = w2 - w1; v->a = 0.0f;
+}
 NSD_HD DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, SimplexCache* cache) {
   M3 m = matrix_from_quat(x.q);
   M3 mt = transpose(m);
-  Simplex s;
-  s.count = cache->count;
-  for (int i = 0; i < cache->count; ++i) {
-    int i1 = cache->ia[i], i2 = cache->ib[i];
-    V3 w1 = pa[i1];
-    V3 w2 = mul_mv(m, pb[i2]) + x.p;
-    s.v[i].ia = i1; s.v[i].ib = i2; s.v[i].wa = w1; s.v[i].wb = w2; s.v[i].w = w2 - w1; s.v[i].a = 0.0f;
+  Simplex sx[2];
+  for (int k = 0; k < 2; ++k)
+    for (int i = 0; i < 4; ++i) {
+      sx[k].v[i].wa = sx[k].v[i].wb = sx[k].v[i].w = v3(0, 0, 0);
+      sx[k].v[i].a = 0.0f; sx[k].v[i].ia = sx[k].v[i].ib = 0;
+    }
+  int cur = 0;  // sx[cur] is the working simplex, sx[cur ^ 1] the last accepted one
+  {
+    Simplex& s = sx[0];
+    s.count = cache->count;
+    for (int i = 0; i < cache->count; ++i) simplex_vertex(&s.v[i], pa, pb, cache->ia[i], cache->ib[i], m, x.p);
+    if (s.count > 0) {
+      float m1 = cache->metric, m2 = simplex_metric(s);
+      if (2.0f * m1 < m2 || m2 < 0.5f * m1 || m2 < kEps) s.count = 0;
+    }
+    if (s.count == 0) {
+      s.count = 1;
+      simplex_vertex(&s.v[0], pa, pb, 0, 0, m, x.p);
+    }
   }
-  if (s.count > 0) {
-    float m1 = cache->metric, m2 = simplex_metric(s);
-    if (2.0f * m1 < m2 || m2 < 0.5f * m1 || m2 < kEps) s.count = 0;
-  }
-  if (s.count == 0) {
-    V3 w1 = pa[0], w2 = mul_mv(m, pb[0]) + x.p;
-    s.count = 1;
-    s.v[0].ia = 0; s.v[0].ib = 0; s.v[0].wa = w1; s.v[0].wb = w2; s.v[0].w = w2 - w1; s.v[0].a = 0.0f;
-  }
-  Simplex backup;
+  sx[1].count = 0;
   DistOut out;
   out.pa = out.pb = out.normal = v3(0, 0, 0);
   out.distance = 0;
   float dsq = kFltMax;
   V3 normal = v3(0, 0, 0);
   int it = 0;
+  int fin = -1;  // which simplex the loop ended on
   while (it < 32) {
+    Simplex& s = sx[cur];
     bool solved;
     switch (s.count) {
       case 1: s.v[0].a = 1.0f; solved = true; break;
@@ -1060,7 +1074,7 @@ NSD_HD DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
       case 3: solved = solve3(s); break;
       default: solved = solve4(s); break;
     }
-    if (!solved) { s = backup; break; }
+    if (!solved) { fin = cur ^ 1; break; }
     if (s.count == 4) {
       witness(s, &out.pa, &out.pb);
       out.normal = v3(0, 0, 0);
@@ -1070,7 +1084,7 @@ NSD_HD DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
     float old = dsq;
     V3 cp = closest_on_simplex(s);
     dsq = dot(cp, cp);
-    if (dsq >= old) { s = backup; break; }
+    if (dsq >= old) { fin = cur ^ 1; break; }
     V3 sd;
     if (s.count == 1) {
       sd = -s.v[0].w;
@@ -1094,16 +1108,21 @@ NSD_HD DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
     V3 sd2 = mul_mv(mt, sd);
     int ib = point_support(pb, nb, sd2);
     V3 sb = mul_mv(m, pb[ib]) + x.p;
-    backup = s;
     bool dup = false;
     for (int i = 0; i < s.count; ++i)
       if (s.v[i].ia == ia && s.v[i].ib == ib) { dup = true; break; }
-    if (dup) break;
+    if (dup) { fin = cur; break; }
+    // accept s: it becomes the fallback, the extended copy becomes the working simplex
+    Simplex& t = sx[cur ^ 1];
+    t.count = s.count + 1;
+    for (int i = 0; i < s.count; ++i) t.v[i] = s.v[i];
     int k = s.count;
-    s.v[k].ia = ia; s.v[k].ib = ib; s.v[k].wa = sa; s.v[k].wb = sb; s.v[k].w = sb - sa;
-    s.count += 1;
+    t.v[k].ia = ia; t.v[k].ib = ib; t.v[k].wa = sa; t.v[k].wb = sb; t.v[k].w = sb - sa; t.v[k].a = 0.0f;
+    cur ^= 1;
     it++;
   }
+  if (fin < 0) fin = cur;
+  const Simplex& s = sx[fin];
   witness(s, &out.pa, &out.pb);
   normal = normalize(normal);
   if (!is_normalized(normal)) {

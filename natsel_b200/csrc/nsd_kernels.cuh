@@ -889,4 +889,68 @@ __global__ void k_prepare_joints(DW w, StepParams p) {
   w.joints[i] = j;
 }
 
+// Batch narrowphase over explicit pair jobs (the same routines k_collide calls).
+struct PairJob {
+  int32_t type_a, type_b;
+  float geom_a[7], geom_b[7];
+  float xf[7];
+  float sat_separation;
+  int32_t sat_type, sat_index_a, sat_index_b, sat_hit;
+  float simplex_metric;
+  int32_t simplex_count, simplex_ia[4], simplex_ib[4];
+};
+struct PairResult {
+  float normal[3];
+  int32_t point_count;
+  float points[4][4];
+  uint32_t feature_ids[4];
+};
+
+__global__ void __launch_bounds__(128) k_collide_jobs(PairJob* jobs, PairResult* results, int count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  PairJob j = jobs[i];
+  PairResult r;
+  memset(&r, 0, sizeof(r));
+  Xf x = xf(v3(j.xf[0], j.xf[1], j.xf[2]), quat(v3(j.xf[3], j.xf[4], j.xf[5]), j.xf[6]));
+  LocalManifold lm;
+  Sphere sa = {v3(j.geom_a[0], j.geom_a[1], j.geom_a[2]), j.geom_a[3]};
+  Sphere sb = {v3(j.geom_b[0], j.geom_b[1], j.geom_b[2]), j.geom_b[3]};
+  Capsule ca = {v3(j.geom_a[0], j.geom_a[1], j.geom_a[2]), v3(j.geom_a[3], j.geom_a[4], j.geom_a[5]), j.geom_a[6]};
+  Capsule cb = {v3(j.geom_b[0], j.geom_b[1], j.geom_b[2]), v3(j.geom_b[3], j.geom_b[4], j.geom_b[5]), j.geom_b[6]};
+  SATCache sat;
+  sat.separation = j.sat_separation; sat.type = (uint8_t)j.sat_type;
+  sat.index_a = (uint8_t)j.sat_index_a; sat.index_b = (uint8_t)j.sat_index_b; sat.hit = (uint8_t)j.sat_hit;
+  SimplexCache sc;
+  sc.metric = j.simplex_metric; sc.count = (uint16_t)j.simplex_count;
+  for (int k = 0; k < 4; ++k) { sc.ia[k] = (uint8_t)j.simplex_ia[k]; sc.ib[k] = (uint8_t)j.simplex_ib[k]; }
+  if (j.type_a == kSphere) {
+    collide_spheres(&lm, sa, sb, x);
+  } else if (j.type_a == kCapsule) {
+    if (j.type_b == kSphere) collide_capsule_sphere(&lm, ca, sb, x);
+    else collide_capsules(&lm, ca, cb, x);
+  } else {
+    Hull ha = make_box_hull(j.geom_a[0], j.geom_a[1], j.geom_a[2]);
+    if (j.type_b == kSphere) collide_hull_sphere(&lm, ha, sb, x, &sc);
+    else if (j.type_b == kCapsule) collide_hull_capsule(&lm, ha, cb, x, &sc);
+    else {
+      Hull hb = make_box_hull(j.geom_b[0], j.geom_b[1], j.geom_b[2]);
+      collide_hulls(&lm, ha, hb, x, &sat, nullptr);
+    }
+  }
+  j.sat_separation = sat.separation; j.sat_type = sat.type; j.sat_index_a = sat.index_a;
+  j.sat_index_b = sat.index_b; j.sat_hit = sat.hit;
+  j.simplex_metric = sc.metric; j.simplex_count = sc.count;
+  for (int k = 0; k < 4; ++k) { j.simplex_ia[k] = sc.ia[k]; j.simplex_ib[k] = sc.ib[k]; }
+  r.normal[0] = lm.normal.x; r.normal[1] = lm.normal.y; r.normal[2] = lm.normal.z;
+  r.point_count = lm.point_count;
+  for (int k = 0; k < lm.point_count && k < 4; ++k) {
+    r.points[k][0] = lm.points[k].point.x; r.points[k][1] = lm.points[k].point.y;
+    r.points[k][2] = lm.points[k].point.z; r.points[k][3] = lm.points[k].separation;
+    r.feature_ids[k] = make_feature_id(lm.points[k].pair);
+  }
+  jobs[i] = j;
+  results[i] = r;
+}
+
 }  // namespace nsd

@@ -71,6 +71,27 @@ int nso_get_contacts(const nso_world* w, int32_t* ints /* cap*8 */, uint32_t* fe
  * [27]=sat calls [28]=recycled last step */
 void nso_counters(const nso_world* w, int32_t* out /* 32 */);
 
+/* One narrowphase pair (collision/convex_manifold*.rs entry points). Types: 0 capsule,
+ * 3 box hull, 5 sphere; A must be the primary type (capsule>sphere, hull>sphere/capsule).
+ * geom: box hx,hy,hz; sphere cx,cy,cz,r; capsule c1 xyz, c2 xyz, r. xf = B in A's frame
+ * (p xyz, q xyzs). The caches are read and written back. */
+typedef struct {
+  int32_t type_a, type_b;
+  float geom_a[7], geom_b[7];
+  float xf[7];
+  float sat_separation;
+  int32_t sat_type, sat_index_a, sat_index_b, sat_hit;
+  float simplex_metric;
+  int32_t simplex_count, simplex_ia[4], simplex_ib[4];
+} nso_pair_job;
+typedef struct {
+  float normal[3];
+  int32_t point_count;
+  float points[4][4]; /* x, y, z, separation (frame A) */
+  uint32_t feature_ids[4];
+} nso_pair_result;
+void nso_collide_pairs(nso_pair_job* jobs, nso_pair_result* results, int count);
+
 #ifdef __cplusplus
 }
 #endif

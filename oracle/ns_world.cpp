@@ -1939,4 +1939,47 @@ void nso_counters(const nso_world* w, int32_t* out) {
   out[28] = w->recycled;
 }
 
+void nso_collide_pairs(nso_pair_job* jobs, nso_pair_result* results, int count) {
+  for (int i = 0; i < count; ++i) {
+    nso_pair_job& j = jobs[i];
+    nso_pair_result& r = results[i];
+    std::memset(&r, 0, sizeof(r));
+    Xf x = xf(v3(j.xf[0], j.xf[1], j.xf[2]), quat(v3(j.xf[3], j.xf[4], j.xf[5]), j.xf[6]));
+    LocalManifold lm;
+    auto sphere = [](const float* g) { Sphere s; s.center = v3(g[0], g[1], g[2]); s.radius = g[3]; return s; };
+    auto capsule = [](const float* g) { Capsule c; c.c1 = v3(g[0], g[1], g[2]); c.c2 = v3(g[3], g[4], g[5]); c.radius = g[6]; return c; };
+    SATCache sat;
+    sat.separation = j.sat_separation; sat.type = (uint8_t)j.sat_type;
+    sat.index_a = (uint8_t)j.sat_index_a; sat.index_b = (uint8_t)j.sat_index_b; sat.hit = (uint8_t)j.sat_hit;
+    SimplexCache sc;
+    sc.metric = j.simplex_metric; sc.count = (uint16_t)j.simplex_count;
+    for (int k = 0; k < 4; ++k) { sc.ia[k] = (uint8_t)j.simplex_ia[k]; sc.ib[k] = (uint8_t)j.simplex_ib[k]; }
+    if (j.type_a == kSphere) {
+      collide_spheres(&lm, sphere(j.geom_a), sphere(j.geom_b), x);
+    } else if (j.type_a == kCapsule) {
+      if (j.type_b == kSphere) collide_capsule_sphere(&lm, capsule(j.geom_a), sphere(j.geom_b), x);
+      else collide_capsules(&lm, capsule(j.geom_a), capsule(j.geom_b), x);
+    } else {
+      Hull ha = make_box_hull(j.geom_a[0], j.geom_a[1], j.geom_a[2]);
+      if (j.type_b == kSphere) collide_hull_sphere(&lm, ha, sphere(j.geom_b), x, &sc);
+      else if (j.type_b == kCapsule) collide_hull_capsule(&lm, ha, capsule(j.geom_b), x, &sc);
+      else {
+        Hull hb = make_box_hull(j.geom_b[0], j.geom_b[1], j.geom_b[2]);
+        collide_hulls(&lm, ha, hb, x, &sat, nullptr);
+      }
+    }
+    j.sat_separation = sat.separation; j.sat_type = sat.type; j.sat_index_a = sat.index_a;
+    j.sat_index_b = sat.index_b; j.sat_hit = sat.hit;
+    j.simplex_metric = sc.metric; j.simplex_count = sc.count;
+    for (int k = 0; k < 4; ++k) { j.simplex_ia[k] = sc.ia[k]; j.simplex_ib[k] = sc.ib[k]; }
+    r.normal[0] = lm.normal.x; r.normal[1] = lm.normal.y; r.normal[2] = lm.normal.z;
+    r.point_count = lm.point_count;
+    for (int k = 0; k < lm.point_count; ++k) {
+      r.points[k][0] = lm.points[k].point.x; r.points[k][1] = lm.points[k].point.y;
+      r.points[k][2] = lm.points[k].point.z; r.points[k][3] = lm.points[k].separation;
+      r.feature_ids[k] = make_feature_id(lm.points[k].pair);
+    }
+  }
+}
+
 }  // extern "C"
