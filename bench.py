@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Throughput of the plain rigid-body step (body-substeps per second) on one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl natsel|reference]
+
+Workload (default): the 10 000-body pile, i.e. 6 000 boxes, 2 500 spheres and 1 500 capsules
+dropped from a 40 x 60 x 40 m volume onto a ground box, stepped at 60 Hz with 4 substeps in
+FP32 (scene builder ``natsel_b200.scenes.large_pile``; seeded synthetic data). A step is one
+``World::step`` (solver_integration.rs:807 in the reference): broadphase pair update,
+narrowphase, colouring, prepare, the substep solve and finalize. The timed steps are
+W+1 .. W+K of the drop.
+
+natsel arm (default): one world per GPU (replicas, weak scaling; no collective on the data
+path). ``value`` is the device time of the K steps measured with CUDA events on the world's
+stream, with the L2 flushed between steps outside the events (the working set fits in L2);
+``e2e`` repeats the run through the public C ABI with per-step host inputs (external forces,
+copied host->device) and the full body state read back to pinned host memory every step.
+``roofline`` is for the persistent solver kernel (k_solve): algorithmic bytes per launch from
+the per-step solver counts divided by its CUDA-event duration. ``cpu_baseline`` times the CPU
+oracle (a scalar C++ restatement of the reference step) on a bounded sample of the same drop.
+
+reference arm (``--impl reference``): the reference engine is Rust and cannot be built on
+this image, so its CPU step is timed through the oracle port, one replica world per host
+core, on a bounded sample of the same workload; under torchrun only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 1.0 / 60.0
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+METRIC = "body-substeps/s"
+
+WORKLOADS = {
+    "large_pile": ("large_pile", {}, "10 000 dynamic bodies (6 000 boxes h U(0.25,0.75), 2 500 spheres r U(0.2,0.6), "
+                                     "1 500 capsules r U(0.15,0.4) hh U(0.2,0.8)) dropped from a 40x60x40 m volume "
+                                     "onto a ground box; 60 Hz, 4 substeps, FP32"),
+    "box_pyramid": ("box_pyramid", {}, "pyramid of 210 unit cubes (base 20) on a ground box; 60 Hz, 4 substeps, FP32"),
+    "jointed_chains": ("jointed_chains", {}, "2 000 chains of 24 capsules on limited revolute joints + 4 000 boxes; "
+                                             "60 Hz, 8 substeps, FP32"),
+}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=3, help=">= 1 (the first step uploads the scene)")
+    ap.add_argument("--impl", choices=["natsel", "reference"], default="natsel")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="large_pile")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--reference-seconds", type=float, default=60.0, help="budget of the reference arm's timed sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic bytes of one k_solve launch (the solver stages of one step, all substeps)
+
+def solve_launch_bytes(counts, substeps, restitution_iterations=2):
+    """Bytes the solver stages must move for one step, compact FP32 SoA accounting:
+    per awake body and substep 116 B integrate-velocity (+40 B when gyroscopic) and 104 B
+    integrate-position; per manifold and substep with P points 756 + 120 P B over warm start,
+    push and relax, minus 200 B per static side (its body is never read or written); per
+    revolute joint and substep 680 B; once per step the impulse store (40 + 16 P B per
+    manifold) and, when any contact has restitution, that many push-like passes
+    (220 + 40 P B per manifold, minus 76 B per static side)."""
+    c = [int(x) for x in counts]
+    n_awake, manifolds, points, static_sides, joints = c[0], c[2], c[3], c[4], c[5]
+    overflow, gyro, o_points, o_static = c[6], c[8], c[9], c[10]
+    m_all, p_all, s_all = manifolds + overflow, points + o_points, static_sides + o_static
+    per_substep = n_awake * (116 + 104) + 40 * gyro + 756 * m_all + 120 * p_all - 200 * s_all + 680 * joints
+    per_step = 40 * m_all + 16 * p_all
+    if c[7]:
+        per_step += restitution_iterations * (220 * m_all + 40 * p_all - 76 * s_all)
+    return substeps * per_substep + per_step
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of k_solve from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "k_solve_large_pile.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    QUERY = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, uuids):
+        self.uuids = [u.lower().replace("gpu-", "") for u in uuids]
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.seek(0)
+        sm, smax, reasons, power = [], [], set(), []
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            uuid = parts[0].lower().replace("gpu-", "")
+            if self.uuids and uuid not in self.uuids:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, val in zip(self.REASONS, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        self.file.close()
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU side (oracle): single-thread baseline and the reference arm's replica workers
+
+def oracle_run(scene, kw, warmup, max_steps, budget_s, barrier=None):
+    from natsel_b200 import scenes
+    from oracle import pyoracle
+    w = pyoracle.OracleWorld(**scenes.WORLD_SETTINGS[scene])
+    info = scenes.BUILDERS[scene](w, **kw)
+    sub = scenes.SUBSTEPS[scene]
+    for _ in range(warmup):
+        w.step(DT, sub)
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps:
+        w.step(DT, sub)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    return {"steps": steps, "seconds": time.perf_counter() - t0, "bodies": info["dynamic_bodies"], "substeps": sub}
+
+
+def _replica_worker(scene, kw, warmup, max_steps, budget_s, barrier, queue):
+    try:
+        queue.put(oracle_run(scene, kw, warmup, max_steps, budget_s, barrier))
+    except Exception as e:  # report instead of hanging the parent
+        queue.put({"error": repr(e)})
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args):
+    import multiprocessing as mp
+    from oracle import pyoracle
+    pyoracle.build()
+    scene, kw, desc = WORKLOADS[args.workload]
+    n = min(host_cores(), 128)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(n)
+    queue = ctx.Queue()
+    procs = [ctx.Process(target=_replica_worker, args=(scene, kw, args.warmup, args.steps, args.reference_seconds,
+                                                        barrier, queue)) for _ in range(n)]
+    for p in procs:
+        p.start()
+    results = [queue.get(timeout=args.reference_seconds + 600) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    errors = [r["error"] for r in results if "error" in r]
+    if errors:
+        raise RuntimeError("reference replica failed: %s" % errors[0])
+    seconds = max(r["seconds"] for r in results)
+    units = sum(r["steps"] * r["bodies"] * r["substeps"] for r in results)
+    value = units / seconds
+    steps = min(r["steps"] for r in results)
+    ms_per_step = 1000.0 * statistics.mean(r["seconds"] / r["steps"] for r in results)
+    sample = ("%d replica worlds (one per host core, %s), each timing steps %d..%d of the drop "
+              "(bounded to %.0f s)" % (n, cpu_model(), args.warmup + 1, args.warmup + steps, args.reference_seconds))
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene builder, no dataset)",
+        "config": config_block(args, desc), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": n, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timed_steps_per_replica": steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, desc):
+    return {"workload": "%s: %s" % (args.workload, desc), "first_timed_step": args.warmup + 1,
+            "timed_steps": args.steps, "l2": "flushed between steps (256 MiB write outside the timed events)",
+            "parallelism": "replicas: one independent world per GPU (%d)" % args.gpus}
+
+
+# ---------------------------------------------------------------------------------------------
+# natsel arm
+
+def build_gpu_world(args, device):
+    from natsel_b200 import scenes
+    from natsel_b200.world import World, default_world_def
+    scene, kw, _ = WORKLOADS[args.workload]
+    s = scenes.WORLD_SETTINGS[scene]
+    w = World(default_world_def(gravity=s["gravity"], enable_continuous=int(s["enable_continuous"]), device=device))
+    info = scenes.BUILDERS[scene](w, **kw)
+    return w, info, scenes.SUBSTEPS[scene]
+
+
+def run_natsel_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from natsel_b200 import _build
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: the natsel arm needs a CUDA device")
+    if not os.path.exists(_build.LIB):
+        raise SystemExit("bench.py: libnatsel_gpu.so is missing; run __graft_entry__.build()")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world_size > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world_size > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x, op):
+        if world_size == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    uuids = [str(torch.cuda.get_device_properties(local_rank).uuid)]
+    if world_size > 1:
+        gathered = [None] * world_size
+        dist.all_gather_object(gathered, uuids[0])
+        uuids = gathered
+
+    scene, kw, desc = WORKLOADS[args.workload]
+    world, info, sub = build_gpu_world(args, local_rank)
+    bodies = info["dynamic_bodies"]
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        world.step(DT, sub)
+    world.synchronize()
+    stream = torch.cuda.ExternalStream(world.stream(), device=dev)  # created by the first step
+    launches0 = int(world.solver_counts()[12])
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    phase = np.zeros((args.steps, 5), np.float64)
+    solve_bytes = np.zeros(args.steps, np.float64)
+    barrier()
+    sampler = ClockSampler(uuids) if rank == 0 else None
+    wall0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            world.step(DT, sub)
+            ends[k].record(stream)
+            ends[k].synchronize()
+            phase[k] = world.phase_times()
+            solve_bytes[k] = solve_launch_bytes(world.solver_counts(), sub)
+    world.synchronize()
+    barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop() if sampler else None
+    launches = int(world.solver_counts()[12]) - launches0
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    total_ms = reduce(float(step_ms.sum()), dist.ReduceOp.MAX if world_size > 1 else None)
+    launches = int(reduce(float(launches), dist.ReduceOp.SUM if world_size > 1 else None))
+    value = world_size * bodies * sub * args.steps / (total_ms / 1000.0)
+
+    solve_ms = phase[:, 3]
+    achieved = solve_bytes.sum() / (solve_ms.sum() / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic()
+    roofline = {"kernel": "k_solve", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": float(solve_bytes.mean()),
+                "launch_ms": float(solve_ms.mean())}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, local_rank, dev, barrier, reduce, world_size)
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        r = oracle_run(scene, kw, args.warmup, args.steps, args.cpu_seconds)
+        cpu = {"value": r["steps"] * r["bodies"] * r["substeps"] / r["seconds"], "unit": METRIC, "cores": 1,
+               "kind": "port",
+               "sample": "CPU oracle (scalar C++ restatement of the reference step, 1 thread, %s) timing steps "
+                         "%d..%d of the same drop (bounded to %.0f s)" % (cpu_model(), args.warmup + 1,
+                                                                          args.warmup + r["steps"], args.cpu_seconds)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene builder, no dataset)", "config": config_block(args, desc),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
+            "wall_s": wall,
+            "phase_ms_mean": {k: float(v) for k, v in zip(["broadphase", "collide", "state_color_prepare", "solve",
+                                                          "finalize"], phase.mean(0))},
+        }
+        print(json.dumps(line), flush=True)
+    world.close()
+    if world_size > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(args, local_rank, dev, barrier, reduce, world_size):
+    """The same workload through the public API with host buffers: every step uploads that
+    step's external forces and torques (24 B per body, host->device) and reads the whole body
+    state back into pinned host memory (64 B per body)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    world, info, sub = build_gpu_world(args, local_rank)
+    n = world.body_count
+    rng = np.random.Generator(np.random.PCG64(17))
+    forces = [rng.normal(0.0, 1.0, (n, 3)).astype(np.float32) for _ in range(8)]
+    torques = [rng.normal(0.0, 0.1, (n, 3)).astype(np.float32) for _ in range(8)]
+    pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    rot = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    lin = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    ang = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+
+    def one(k):
+        world.apply_forces(forces[k % 8], torques[k % 8])
+        world.step(DT, sub)
+        world.get_bodies_into(pos, rot, lin, ang)
+
+    for k in range(args.warmup):
+        one(k)
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        one(k)
+    barrier()
+    seconds = reduce(time.perf_counter() - t0, dist.ReduceOp.MAX if world_size > 1 else None)
+    world.close()
+    return {"value": world_size * info["dynamic_bodies"] * sub * args.steps / seconds, "unit": METRIC,
+            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 64 * n, "ms_per_step": 1000.0 * seconds / args.steps,
+            "timing": "host wall clock around the K steps, synchronised by each step's readback"}
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.warmup < 1 or args.steps < 1:
+        raise SystemExit("bench.py: need --steps >= 1 and --warmup >= 1")
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return  # the CPU reference runs once, on rank 0
+        run_reference_arm(args)
+    else:
+        run_natsel_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -95,13 +95,22 @@ int ns_create_revolute_joint(ns_world* world, int body_a, int body_b, const floa
                              float max_motor_torque, int collide_connected);
 
 /* Advance one step (replaces World::step solver_integration.rs:807). Asynchronous:
- * the step is enqueued on the world's stream; the first call uploads the scene. */
+ * the step is enqueued on the world's stream; the first call uploads the scene. dt == 0
+ * updates the broadphase pairs only, as the reference does; dt < 0 is NS_ERR_INVALID. */
 int ns_world_step(ns_world* world, float dt, int substeps);
+/* Adds per-body external force and torque (each n_bodies x 3 floats in body id order, either
+ * may be NULL) to the awake bodies for the next step; finalize clears them, as the reference
+ * does (replaces apply_body_force_to_center body_api.rs:351 and apply_body_torque :366 for
+ * every body at once). The arrays are copied before the call returns. */
+int ns_world_apply_forces(ns_world* world, const float* force, const float* torque);
 /* Wait for queued steps and report device-side errors (capacity, barrier timeout). */
 int ns_world_synchronize(ns_world* world);
 
 /* Readback (synchronises). Arrays are per body in id order:
- * pos f64x3, rot f32x4 (x,y,z,s), lin f32x3, ang f32x3. Any pointer may be NULL. */
+ * pos f64x3, rot f32x4 (x,y,z,s), lin f32x3, ang f32x3. Any pointer may be NULL. One device
+ * gather packs the state, then each requested array is one copy (pinned host memory makes
+ * the copies asynchronous DMA). Reports device errors of the queued steps, like
+ * ns_world_synchronize. */
 int ns_world_get_bodies(ns_world* world, double* pos, float* rot, float* lin, float* ang);
 int ns_world_body_count(const ns_world* world);
 /* FNV-1a digest identical to the reference World::world_state_hash (body_queries.rs:432). */
@@ -122,9 +131,12 @@ int ns_world_counters(ns_world* world, int32_t* counters);
 int ns_world_phase_times(ns_world* world, float* ms5);
 /* Raw CUDA stream (cudaStream_t) the world enqueues on, for callers that time with events. */
 void* ns_world_stream(ns_world* world);
-/* Solver roofline inputs of the last step: [0] awake bodies [1] substeps [2] colored manifolds
- * [3] colored points [4] static sides [5] joints [6] overflow manifolds [7] restitution on. */
-int ns_world_solver_counts(ns_world* world, int64_t* counts8);
+/* Solver roofline inputs of the last step (synchronises): [0] awake bodies [1] substeps
+ * [2] colored manifolds [3] colored points [4] colored static sides [5] joints
+ * [6] overflow contacts [7] restitution on [8] gyroscopic bodies [9] overflow points
+ * [10] overflow static sides [11] library kernel launches per step [12] library kernel
+ * launches since creation; [13..15] zero. */
+int ns_world_solver_counts(ns_world* world, int64_t* counts16);
 
 /* Batch narrowphase (replaces the per-pair routines collide_hulls_with_scratch
  * convex_manifold.rs:1445, collide_spheres / collide_capsule_and_sphere /
@@ -148,8 +160,14 @@ typedef struct {
   float points[4][4]; /* x, y, z, separation in frame A */
   uint32_t feature_ids[4];
 } ns_pair_result;
-/* Synchronous; host arrays; device 0 unless ns_world-independent device selection is added. */
+/* Synchronous; host arrays; runs on the calling thread's current CUDA device. */
 int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count);
+
+/* Diagnostics (no counterpart in the reference): launches the solver's bounded grid barrier
+ * waiting for one arrival that never comes, so every block gives up after timeout_ms
+ * (1..2000). Returns NS_ERR_TIMEOUT when the wait expired and was reported as designed; the
+ * CUDA context stays usable afterwards. */
+int ns_selftest_barrier_timeout(int device, int timeout_ms);
 
 #ifdef __cplusplus
 }

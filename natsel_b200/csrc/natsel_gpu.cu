@@ -79,6 +79,18 @@ struct ns_world {
   int steps_done = 0;
   int last_substeps = 0;
   bool eager = false;
+  // readback: body id -> awake index (>= 0) or -(static index + 1); packed output staging
+  int* body_loc = nullptr;
+  char* out_stage = nullptr;
+  Control* host_ctl = nullptr;  // pinned
+  // per-step external forces: pinned host staging -> device staging (force xyz | torque xyz)
+  float* host_in = nullptr;     // pinned, 6 floats per body
+  float* in_stage = nullptr;
+  cudaEvent_t in_done = nullptr;
+  // accounting
+  int pair_kernels = 0, step_kernels = 0;  // own kernel launches per pair update / full step
+  int64_t kernel_launches = 0;
+  int64_t n_gyroscopic = 0;
 };
 
 namespace {
@@ -473,10 +485,54 @@ int upload_world(ns_world* w) {
   int max_blocks = per_sm * w->sm_count;
   int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : std::max(1, std::min(w->sm_count, (na + kSolveThreads - 1) / kSolveThreads));
   w->solver_blocks = std::max(1, std::min(want, max_blocks));
+  // readback staging (64 B per body) and the body location table
+  {
+    std::vector<int> loc(nb);
+    for (int i = 0; i < nb; ++i) loc[i] = w->bodies[i].set == 2 ? w->bodies[i].local : -(w->bodies[i].local + 1);
+    w->body_loc = dalloc<int>(w, nb, &st);
+    if (!w->body_loc) return st;
+    if ((st = upload(w, w->body_loc, loc))) return st;
+    w->out_stage = dalloc<char>(w, (size_t)std::max(nb, 1) * 64, &st);
+    if (!w->out_stage) return st;
+    NS_CUDA(w, cudaHostAlloc((void**)&w->host_ctl, sizeof(Control), cudaHostAllocDefault));
+    NS_CUDA(w, cudaHostAlloc((void**)&w->host_in, sizeof(float) * 6 * (size_t)std::max(nb, 1), cudaHostAllocDefault));
+    w->in_stage = dalloc<float>(w, 6 * (size_t)std::max(nb, 1), &st);
+    if (!w->in_stage) return st;
+    NS_CUDA(w, cudaEventCreateWithFlags(&w->in_done, cudaEventDisableTiming));
+    w->n_gyroscopic = 0;
+    for (const DSim& a : w->asims) w->n_gyroscopic += (a.flags & kGyroscopic) ? 1 : 0;
+  }
   NS_CUDA(w, cudaStreamSynchronize(w->stream));
   const char* eager = getenv("NATSEL_EAGER");
   w->eager = eager && eager[0] == '1';
   w->uploaded = true;
+  return NS_OK;
+}
+
+// Broadphase pair update (contact_creation.rs:901 update_broad_phase_pairs): new pairs of
+// overlapping fat AABBs with a moved proxy become contacts, in pair-key order.
+int enqueue_pair_update(ns_world* w) {
+  DW d = w->dw;
+  cudaStream_t s = w->stream;
+  int nsh = d.n_shapes;
+  auto blocks = [](int n, int t) { return std::max(1, (n + t - 1) / t); };
+  int nk = 0;
+  NS_CUDA(w, cudaMemsetAsync(d.seg_count, 0, sizeof(int) * (size_t)nsh, s));
+  NS_CUDA(w, cudaMemsetAsync(d.seg_cursor, 0, sizeof(int) * (size_t)nsh, s));
+  k_hs_rebuild_clear<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  k_hs_rebuild_insert<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  k_bp_keys<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cub::DeviceRadixSort::SortPairs(w->cub_sort_tmp, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
+                                              d.bp_vals_in, d.bp_vals_out, nsh, 0, 32, s));
+  k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d); ++nk;
+  k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
+  k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  k_bp_segsort<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
+  k_bp_create<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  k_bp_finish<<<1, 1, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cudaMemsetAsync(d.moved, 0, sizeof(int) * (size_t)nsh, s));
+  w->pair_kernels = nk;
   return NS_OK;
 }
 
@@ -502,36 +558,27 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   p.restitution_iterations = w->def.restitution_iterations;
   p.enable_continuous = w->def.enable_continuous;
   p.gravity = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
-  int nsh = d.n_shapes;
   auto blocks = [](int n, int t) { return std::max(1, (n + t - 1) / t); };
+  int nk = 0;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[0], s, cudaEventRecordExternal));
-  // pair update (contact_creation.rs:901)
-  NS_CUDA(w, cudaMemsetAsync(d.seg_count, 0, sizeof(int) * (size_t)nsh, s));
-  NS_CUDA(w, cudaMemsetAsync(d.seg_cursor, 0, sizeof(int) * (size_t)nsh, s));
-  k_hs_rebuild_clear<<<4 * w->sm_count, 256, 0, s>>>(d);
-  k_hs_rebuild_insert<<<4 * w->sm_count, 256, 0, s>>>(d);
-  k_bp_keys<<<blocks(nsh, 256), 256, 0, s>>>(d);
-  NS_CUDA(w, cub::DeviceRadixSort::SortPairs(w->cub_sort_tmp, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
-                                              d.bp_vals_in, d.bp_vals_out, nsh, 0, 32, s));
-  k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d);
-  k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d);
-  NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
-  k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d);
-  k_bp_segsort<<<blocks(nsh, 256), 256, 0, s>>>(d);
-  k_bp_create<<<4 * w->sm_count, 256, 0, s>>>(d);
-  k_bp_finish<<<1, 1, 0, s>>>(d);
-  NS_CUDA(w, cudaMemsetAsync(d.moved, 0, sizeof(int) * (size_t)nsh, s));
+  {
+    int st = enqueue_pair_update(w);
+    if (st) return st;
+  }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, cudaEventRecordExternal));
   // narrowphase (collide_pass.rs:164)
-  k_collide<<<blocks(d.cap, 128), 128, 0, s>>>(d);
+  k_collide<<<blocks(d.cap, 128), 128, 0, s>>>(d); ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, cudaEventRecordExternal));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
-  k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0);
-  k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d);
-  k_color_scan<<<1, 32, 0, s>>>(d);
-  k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p);
-  k_prepare_overflow<<<8, 128, 0, s>>>(d, p);
-  if (d.n_joints > 0) k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
+  k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0); ++nk;
+  k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
+  k_color_scan<<<1, 32, 0, s>>>(d); ++nk;
+  k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p); ++nk;
+  k_prepare_overflow<<<8, 128, 0, s>>>(d, p); ++nk;
+  if (d.n_joints > 0) {
+    k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
+    ++nk;
+  }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, cudaEventRecordExternal));
   // solver stages (solver_stages.rs:543)
   NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
@@ -546,12 +593,48 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve, d, p, w->jr));
+    ++nk;
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, cudaEventRecordExternal));
   // finalize (solver_integration.rs:435)
-  k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p);
+  k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p); ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, cudaEventRecordExternal));
   NS_CUDA(w, cudaGetLastError());
+  w->step_kernels = w->pair_kernels + nk;
+  return NS_OK;
+}
+
+// body_api.rs:351 apply_body_force_to_center and :366 apply_body_torque for every body at
+// once: awake bodies accumulate force and torque until finalize clears them.
+__global__ void k_apply_forces(DW d, const int* body_loc, int nb, const float* force, const float* torque) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    int loc = body_loc[i];
+    if (loc < 0) continue;
+    DSim& s = d.asims[loc];
+    if (force) s.force = s.force + v3(force[3 * i], force[3 * i + 1], force[3 * i + 2]);
+    if (torque) s.torque = s.torque + v3(torque[3 * i], torque[3 * i + 1], torque[3 * i + 2]);
+  }
+}
+
+// Packs the body state in id order for readback: pos f64x3 | rot f32x4 | lin f32x3 | ang f32x3.
+__global__ void k_gather_bodies(DW d, const int* body_loc, int nb, double* pos, float* rot, float* lin,
+                                float* ang) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    int loc = body_loc[i];
+    const DSim& s = loc >= 0 ? d.asims[loc] : d.ssims[-loc - 1];
+    pos[3 * i] = s.px; pos[3 * i + 1] = s.py; pos[3 * i + 2] = s.pz;
+    rot[4 * i] = s.q.v.x; rot[4 * i + 1] = s.q.v.y; rot[4 * i + 2] = s.q.v.z; rot[4 * i + 3] = s.q.s;
+    V3 v = v3(0, 0, 0), wv = v3(0, 0, 0);
+    if (loc >= 0) { v = d.states[loc].v; wv = d.states[loc].w; }
+    lin[3 * i] = v.x; lin[3 * i + 1] = v.y; lin[3 * i + 2] = v.z;
+    ang[3 * i] = wv.x; ang[3 * i + 1] = wv.y; ang[3 * i + 2] = wv.z;
+  }
+}
+
+int control_status(ns_world* w, const Control& c) {
+  if (c.error == kErrCapacity) return fail(w, NS_ERR_CAPACITY, "device capacity exceeded (contacts or pairs)");
+  if (c.error == kErrTimeout) return fail(w, NS_ERR_TIMEOUT, "solver grid barrier timed out");
+  if (c.error) return fail(w, c.error, "device error %d", c.error);
   return NS_OK;
 }
 
@@ -604,6 +687,9 @@ void ns_world_destroy(ns_world* w) {
     if (w->graph_exec) cudaGraphExecDestroy(w->graph_exec);
     if (w->graph) cudaGraphDestroy(w->graph);
     for (void* p : w->allocations) cudaFree(p);
+    if (w->host_ctl) cudaFreeHost(w->host_ctl);
+    if (w->host_in) cudaFreeHost(w->host_in);
+    if (w->in_done) cudaEventDestroy(w->in_done);
     for (int i = 0; i < 6; ++i) if (w->ev[i]) cudaEventDestroy(w->ev[i]);
     cudaStreamDestroy(w->stream);
   }
@@ -741,18 +827,27 @@ int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa
 
 int ns_world_step(ns_world* w, float dt, int substeps) {
   if (!w) return NS_ERR_INVALID;
-  if (!(dt > 0.0f)) return fail(w, NS_ERR_INVALID, "dt must be positive");
+  if (!(dt >= 0.0f)) return fail(w, NS_ERR_INVALID, "dt must be >= 0");
   if (!w->uploaded) {
     int st = upload_world(w);
     if (st) return st;
   }
   NS_CUDA(w, cudaSetDevice(w->def.device));
   if (w->asims.empty()) return NS_OK;
+  if (dt == 0.0f) {
+    // solver_integration.rs:807 with a zero time step: pairs are updated, nothing else runs
+    int st = enqueue_pair_update(w);
+    if (st) return st;
+    NS_CUDA(w, cudaGetLastError());
+    w->kernel_launches += w->pair_kernels;
+    return NS_OK;
+  }
   if (w->eager) {
     int st = enqueue_step(w, dt, substeps);
     if (st) return st;
     w->steps_done++;
     w->last_substeps = substeps;
+    w->kernel_launches += w->step_kernels;
     return NS_OK;
   }
   if (!w->graph_exec || w->graph_dt != dt || w->graph_substeps != substeps) {
@@ -779,6 +874,7 @@ int ns_world_step(ns_world* w, float dt, int substeps) {
       if (st2) return st2;
       w->steps_done++;
       w->last_substeps = substeps;
+      w->kernel_launches += w->step_kernels;
       return NS_OK;
     }
     w->graph = g;
@@ -788,6 +884,7 @@ int ns_world_step(ns_world* w, float dt, int substeps) {
   NS_CUDA(w, cudaGraphLaunch(w->graph_exec, w->stream));
   w->steps_done++;
   w->last_substeps = substeps;
+  w->kernel_launches += w->step_kernels;
   return NS_OK;
 }
 
@@ -797,25 +894,65 @@ int ns_world_synchronize(ns_world* w) {
   Control c;
   int st = read_control(w, &c);
   if (st) return st;
-  if (c.error == kErrCapacity) return fail(w, NS_ERR_CAPACITY, "device capacity exceeded (contacts or pairs)");
-  if (c.error == kErrTimeout) return fail(w, NS_ERR_TIMEOUT, "solver grid barrier timed out");
-  if (c.error) return fail(w, c.error, "device error %d", c.error);
-  return NS_OK;
+  return control_status(w, c);
 }
 
 int ns_world_body_count(const ns_world* w) { return w ? (int)w->bodies.size() : -1; }
 
+int ns_world_apply_forces(ns_world* w, const float* force, const float* torque) {
+  if (!w) return NS_ERR_INVALID;
+  int nb = (int)w->bodies.size();
+  if (nb == 0 || (!force && !torque)) return NS_OK;
+  if (!w->uploaded) {
+    for (int i = 0; i < nb; ++i) {
+      const HostBody& b = w->bodies[i];
+      if (b.set != 2) continue;
+      DSim& s = w->asims[b.local];
+      if (force) s.force = s.force + v3(force[3 * i], force[3 * i + 1], force[3 * i + 2]);
+      if (torque) s.torque = s.torque + v3(torque[3 * i], torque[3 * i + 1], torque[3 * i + 2]);
+    }
+    return NS_OK;
+  }
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  // the pinned staging buffer is reused: wait for the previous upload from it to finish
+  NS_CUDA(w, cudaEventSynchronize(w->in_done));
+  size_t n3 = 3 * (size_t)nb;
+  if (force) memcpy(w->host_in, force, sizeof(float) * n3);
+  if (torque) memcpy(w->host_in + n3, torque, sizeof(float) * n3);
+  size_t off = force ? 0 : n3, len = (force && torque) ? 2 * n3 : n3;
+  NS_CUDA(w, cudaMemcpyAsync(w->in_stage + off, w->host_in + off, sizeof(float) * len, cudaMemcpyHostToDevice,
+                             w->stream));
+  NS_CUDA(w, cudaEventRecord(w->in_done, w->stream));
+  k_apply_forces<<<std::min(4 * w->sm_count, (nb + 255) / 256), 256, 0, w->stream>>>(
+      w->dw, w->body_loc, nb, force ? w->in_stage : nullptr, torque ? w->in_stage + n3 : nullptr);
+  w->kernel_launches++;
+  NS_CUDA(w, cudaGetLastError());
+  return NS_OK;
+}
+
 int ns_world_get_bodies(ns_world* w, double* pos, float* rot, float* lin, float* ang) {
   if (!w) return NS_ERR_INVALID;
-  if (w->uploaded) {
-    int st = ns_world_synchronize(w);
-    if (st) return st;
-    if (!w->asims.empty()) {
-      NS_CUDA(w, cudaMemcpy(w->asims.data(), w->dw.asims, sizeof(DSim) * w->asims.size(), cudaMemcpyDeviceToHost));
-      NS_CUDA(w, cudaMemcpy(w->states.data(), w->dw.states, sizeof(DState) * w->states.size(), cudaMemcpyDeviceToHost));
-    }
+  int nb = (int)w->bodies.size();
+  if (w->uploaded && nb > 0) {
+    // one gather kernel packs the state, then one copy per requested array and one sync
+    NS_CUDA(w, cudaSetDevice(w->def.device));
+    double* dpos = (double*)w->out_stage;
+    float* drot = (float*)(dpos + 3 * (size_t)nb);
+    float* dlin = drot + 4 * (size_t)nb;
+    float* dang = dlin + 3 * (size_t)nb;
+    k_gather_bodies<<<std::min(4 * w->sm_count, (nb + 255) / 256), 256, 0, w->stream>>>(w->dw, w->body_loc, nb, dpos,
+                                                                                        drot, dlin, dang);
+    w->kernel_launches++;
+    NS_CUDA(w, cudaGetLastError());
+    if (pos) NS_CUDA(w, cudaMemcpyAsync(pos, dpos, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, w->stream));
+    if (rot) NS_CUDA(w, cudaMemcpyAsync(rot, drot, sizeof(float) * 4 * nb, cudaMemcpyDeviceToHost, w->stream));
+    if (lin) NS_CUDA(w, cudaMemcpyAsync(lin, dlin, sizeof(float) * 3 * nb, cudaMemcpyDeviceToHost, w->stream));
+    if (ang) NS_CUDA(w, cudaMemcpyAsync(ang, dang, sizeof(float) * 3 * nb, cudaMemcpyDeviceToHost, w->stream));
+    NS_CUDA(w, cudaMemcpyAsync(w->host_ctl, w->dw.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+    NS_CUDA(w, cudaStreamSynchronize(w->stream));
+    return control_status(w, *w->host_ctl);
   }
-  for (size_t i = 0; i < w->bodies.size(); ++i) {
+  for (int i = 0; i < nb; ++i) {
     const HostBody& b = w->bodies[i];
     const DSim& s = b.set == 2 ? w->asims[b.local] : w->ssims[b.local];
     if (pos) { pos[3 * i] = s.px; pos[3 * i + 1] = s.py; pos[3 * i + 2] = s.pz; }
@@ -929,10 +1066,13 @@ void* ns_world_stream(ns_world* w) { return w ? (void*)w->stream : nullptr; }
 
 int ns_world_solver_counts(ns_world* w, int64_t* out) {
   if (!w || !out) return NS_ERR_INVALID;
-  for (int i = 0; i < 8; ++i) out[i] = 0;
+  for (int i = 0; i < 16; ++i) out[i] = 0;
   out[0] = (int64_t)w->asims.size();
   out[1] = w->last_substeps;
   out[5] = (int64_t)w->joints.size();
+  out[8] = w->n_gyroscopic;
+  out[11] = w->step_kernels;
+  out[12] = w->kernel_launches;
   if (!w->uploaded) return NS_OK;
   Control c;
   int st = read_control(w, &c);
@@ -951,6 +1091,14 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   out[4] = stat;
   out[6] = c.overflow_count;
   out[7] = c.any_restitution;
+  if (c.overflow_count > 0) {
+    std::vector<DOverflow> ov(c.overflow_count);
+    NS_CUDA(w, cudaMemcpy(ov.data(), w->dw.ovf, sizeof(DOverflow) * ov.size(), cudaMemcpyDeviceToHost));
+    for (const DOverflow& o : ov) {
+      out[9] += o.manifold_count > 0 ? o.m.point_count : 0;
+      out[10] += (o.index_a < 0) + (o.index_b < 0);
+    }
+  }
   return NS_OK;
 }
 
@@ -978,6 +1126,26 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count) {
   if (dr) cudaFree(dr);
   if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs: %s", cudaGetErrorString(e));
   return NS_OK;
+}
+
+int ns_selftest_barrier_timeout(int device, int timeout_ms) {
+  if (timeout_ms <= 0 || timeout_ms > 2000) return fail(nullptr, NS_ERR_INVALID, "timeout_ms must be in 1..2000");
+  cudaError_t e = cudaSetDevice(device);
+  Control* ctl = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&ctl, sizeof(Control));
+  if (e == cudaSuccess) e = cudaMemset(ctl, 0, sizeof(Control));
+  if (e == cudaSuccess) {
+    k_barrier_selftest<<<2, 32>>>(ctl, (unsigned long long)timeout_ms * 1000000ull);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  Control c;
+  memset(&c, 0, sizeof(c));
+  if (e == cudaSuccess) e = cudaMemcpy(&c, ctl, sizeof(Control), cudaMemcpyDeviceToHost);
+  if (ctl) cudaFree(ctl);
+  if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "barrier self-test: %s", cudaGetErrorString(e));
+  if (c.error == kErrTimeout) return fail(nullptr, NS_ERR_TIMEOUT, "grid barrier gave up after %d ms as designed", timeout_ms);
+  return fail(nullptr, NS_ERR_INVALID, "barrier self-test did not time out (error %d)", c.error);
 }
 
 }  // extern "C"

@@ -11,13 +11,16 @@
 namespace nsd {
 
 // Bounded grid barrier. The arrival counter is zeroed before each launch; barrier k is
-// complete when it reaches (k + 1) * gridDim.x. A block that waits longer than the limit
-// raises NS_ERR_TIMEOUT and the whole kernel unwinds at its next barrier instead of hanging.
-__device__ __forceinline__ bool grid_barrier(Control* ctl, int& index) {
+// complete when it reaches (k + 1) * gridDim.x (+ ``missing``, which only the barrier
+// self-test sets, to wait for arrivals that never come). A block that waits longer than
+// ``limit_ns`` raises NS_ERR_TIMEOUT and the whole kernel unwinds at its next barrier
+// instead of hanging.
+__device__ __forceinline__ bool grid_barrier(Control* ctl, int& index, int missing = 0,
+                                             unsigned long long limit_ns = 2000000000ull) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
-    int target = (index + 1) * (int)gridDim.x;
+    int target = (index + 1) * (int)gridDim.x + missing;
     __threadfence();
     atomicAdd(&ctl->barrier_count, 1);
     int ok = 1;
@@ -32,7 +35,7 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, int& index) {
       if ((spins & 1023) == 0) {
         unsigned long long t1;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 2000000000ull) { ok = 0; break; }  // 2 s
+        if (t1 - t0 > limit_ns) { ok = 0; break; }
       }
       __nanosleep(32);
     }
@@ -43,6 +46,14 @@ __device__ __forceinline__ bool grid_barrier(Control* ctl, int& index) {
   __syncthreads();
   index++;
   return ok_s != 0;
+}
+
+// Self-test of the bounded wait: every block arrives, but the barrier also waits for one
+// arrival that nothing makes, so each block gives up after ``limit_ns`` and the kernel
+// returns with ctl->error = kErrTimeout.
+__global__ void k_barrier_selftest(Control* ctl, unsigned long long limit_ns) {
+  int bar = 0;
+  grid_barrier(ctl, bar, 1, limit_ns);
 }
 
 __device__ __forceinline__ void store_state_vw(const DW& w, int i, const DState& s) {

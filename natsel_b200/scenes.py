@@ -14,6 +14,9 @@ scenes in any world implementation with this interface.
   ground box.
 - :func:`jointed_chains`: capsule chains linked by limited revolute joints
   with loose boxes falling onto them.
+- :func:`overflow_pile`, :func:`restitution_ball`: the reference's own test
+  scenes for the overflow colour (tests/simulation/overflow_color_tests.rs:15)
+  and restitution (tests/simulation/restitution_phase_tests.rs:36-70).
 """
 import numpy as np
 
@@ -92,11 +95,18 @@ def _random_quats(rng, n):
     return q.astype(np.float32)
 
 
-def large_pile(world, n=10000, seed=2, ground_half=50.0):
-    """10 000 dynamic bodies (60% boxes, 25% spheres, 15% capsules) dropped from a 40x60x40 m volume."""
+GROUND_HALF_HEIGHT = 5.0
+
+
+def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0):
+    """10 000 dynamic bodies (60% boxes, 25% spheres, 15% capsules) dropped from a 40x60x40 m volume.
+    ``restitution`` > 0 gives every shape that coefficient (exercises the restitution stage).
+    The ground box is 100 x 10 x 100 m with its top at y = 0: bodies dropped from 61 m arrive
+    at up to 35 m/s (0.58 m per step) and, with continuous collision outside this path, a
+    1 m slab would let the smallest of them pass through in one step."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
-    world.create_box(g, ground_half, 0.5, ground_half, friction=0.6)
+    g = world.create_body(type=STATIC, position=(0.0, -GROUND_HALF_HEIGHT, 0.0))
+    world.create_box(g, ground_half, GROUND_HALF_HEIGHT, ground_half, friction=0.6)
     n_box = int(round(0.6 * n))
     n_sph = int(round(0.25 * n))
     kinds = np.array([0] * n_box + [1] * n_sph + [2] * (n - n_box - n_sph))
@@ -112,7 +122,7 @@ def large_pile(world, n=10000, seed=2, ground_half=50.0):
     for i in range(n):
         b = world.create_body(type=DYNAMIC, position=tuple(float(v) for v in pos[i]),
                               rotation=tuple(float(v) for v in quats[i]))
-        mat = dict(density=float(density[i]), friction=float(friction[i]), restitution=0.0)
+        mat = dict(density=float(density[i]), friction=float(friction[i]), restitution=float(restitution))
         if kinds[i] == 0:
             world.create_box(b, float(box_h[i, 0]), float(box_h[i, 1]), float(box_h[i, 2]), **mat)
         elif kinds[i] == 1:
@@ -131,10 +141,11 @@ def _axis_angle_quat(axis, angle):
 
 def jointed_chains(world, chains=2000, links=24, boxes=4000, seed=3, grid=45, spacing=2.0, height=30.0):
     """Capsule chains (r 0.1, half-height 0.25) on revolute joints limited to +-60 degrees,
-    plus loose boxes (half-extent 0.3) falling onto them."""
+    plus loose boxes (half-extent 0.3) falling onto them. The ground is 10 m thick (top at
+    y = 0) for the same reason as in :func:`large_pile`."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
-    world.create_box(g, 100.0, 0.5, 100.0, friction=0.6)
+    g = world.create_body(type=STATIC, position=(0.0, -GROUND_HALF_HEIGHT, 0.0))
+    world.create_box(g, 100.0, GROUND_HALF_HEIGHT, 100.0, friction=0.6)
     r, hh = 0.1, 0.25
     link = 2.0 * hh
     limit = float(F(np.pi / 3.0))
@@ -167,6 +178,90 @@ def jointed_chains(world, chains=2000, links=24, boxes=4000, seed=3, grid=45, sp
     return {"name": "jointed_chains", "dynamic_bodies": chains * links + boxes, "joints": n_joints}
 
 
+PI = F(3.14159265359)  # base/constants.rs:6
+
+
+def unwind_angle(radians):
+    """math/functions.rs:134 unwind_angle: IEEE remainder by 2*pi, computed exactly in float64."""
+    x = float(F(radians))
+    period = float(F(2.0) * PI)
+    n = float(np.round(x / period))  # numpy rounds half to even
+    r = x - n * period
+    if r > 0.5 * period:
+        n += 1.0
+        r = x - n * period
+    elif r < -0.5 * period:
+        n -= 1.0
+        r = x - n * period
+    return F(r)
+
+
+def compute_cos_sin(radians):
+    """math/functions.rs:101 compute_cos_sin (rational approximation, float32 throughout)."""
+    x = unwind_angle(radians)
+    pi2 = PI * PI
+    if x < F(-0.5) * PI:
+        y = x + PI
+        y2 = y * y
+        c = -(pi2 - F(4.0) * y2) / (pi2 + y2)
+    elif x > F(0.5) * PI:
+        y = x - PI
+        y2 = y * y
+        c = -(pi2 - F(4.0) * y2) / (pi2 + y2)
+    else:
+        y2 = x * x
+        c = (pi2 - F(4.0) * y2) / (pi2 + y2)
+    if x < F(0.0):
+        y = x + PI
+        s = F(-16.0) * y * (PI - y) / (F(5.0) * pi2 - F(4.0) * y * (PI - y))
+    else:
+        s = F(16.0) * x * (PI - x) / (F(5.0) * pi2 - F(4.0) * x * (PI - x))
+    mag = np.sqrt(s * s + c * c)
+    inv = F(1.0) / mag if mag > F(0.0) else F(0.0)
+    return F(c * inv), F(s * inv)
+
+
+def quat_from_axis_angle(axis, radians):
+    """math/functions.rs:461 make_quat_from_axis_angle, as (x, y, z, s)."""
+    c, s = compute_cos_sin(F(0.5) * F(radians))
+    return (float(F(s * F(axis[0]))), float(F(s * F(axis[1]))), float(F(s * F(axis[2]))), float(c))
+
+
+def overflow_pile(world, ring_count=5, per_ring=5):
+    """overflow_color_tests.rs:15 create_overflow_color_pile: a tall hub box ringed by 25 small
+    boxes in 5 staggered layers, enough dynamic neighbours to populate the overflow colour."""
+    g = world.create_body(type=STATIC, position=(0.0, -1.0, 0.0))
+    world.create_box(g, 20.0, 1.0, 20.0)
+    hub = world.create_body(type=DYNAMIC, position=(0.0, 2.5, 0.0))
+    world.create_box(hub, 0.5, 2.5, 0.5, density=50.0)
+    half = F(0.2)
+    ring_radius = F(0.5) + half - F(0.03)
+    base_y = half + F(0.05)
+    n = 0
+    for ring in range(ring_count):
+        y = base_y + F(0.5) * F(ring)
+        offset = PI / F(per_ring) if ring & 1 else F(0.0)
+        for slot in range(per_ring):
+            theta = offset + (F(2.0) * PI * F(slot)) / F(per_ring)
+            c, s = compute_cos_sin(theta)
+            b = world.create_body(type=DYNAMIC, position=(float(F(ring_radius * c)), float(y), float(F(ring_radius * s))))
+            world.create_box(b, float(half), float(half), float(half))
+            n += 1
+    return {"name": "overflow_pile", "dynamic_bodies": n + 1}
+
+
+def restitution_ball(world, restitution=0.5, gap=0.0, speed=5.0):
+    """restitution_phase_tests.rs:36-70: a frictionless ball of radius 0.5 driven at ``speed``
+    into a frictionless static ground (top at y = 0) from ``gap`` above contact; run with
+    gravity 0. Returns the ball's body id."""
+    g = world.create_body(type=STATIC, position=(0.0, -1.0, 0.0))
+    world.create_box(g, 40.0, 1.0, 40.0, friction=0.0, restitution=float(restitution))
+    ball = world.create_body(type=DYNAMIC, position=(0.0, float(F(F(0.5) + F(gap))), 0.0),
+                             linear_velocity=(0.0, -float(speed), 0.0))
+    world.create_sphere(ball, 0.5, friction=0.0, restitution=float(restitution))
+    return {"name": "restitution_ball", "dynamic_bodies": 1, "ball": ball}
+
+
 WORLD_SETTINGS = {
     # gravity per scene: the reference scenes use the World default (-10); the synthetic
     # configurations use -9.81. Parity runs keep continuous collision off (fast bodies are
@@ -176,9 +271,12 @@ WORLD_SETTINGS = {
     "box_pyramid": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "large_pile": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "jointed_chains": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
+    "overflow_pile": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
+    "restitution_ball": dict(gravity=(0.0, 0.0, 0.0), enable_continuous=True),
 }
 
-SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8}
+SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8,
+            "overflow_pile": 4, "restitution_ball": 4}
 
 BUILDERS = {
     "large_pyramid": large_pyramid,
@@ -186,4 +284,6 @@ BUILDERS = {
     "box_pyramid": box_pyramid,
     "large_pile": large_pile,
     "jointed_chains": jointed_chains,
+    "overflow_pile": overflow_pile,
+    "restitution_ball": restitution_ball,
 }

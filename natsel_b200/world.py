@@ -84,6 +84,7 @@ EXPORTED = [
     "ns_create_revolute_joint", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
     "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
+    "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces",
 ]
 
 
@@ -121,6 +122,9 @@ def load_library(path=LIB_PATH):
     lib.ns_world_stream.argtypes = [P]
     lib.ns_world_stream.restype = P
     lib.ns_world_solver_counts.argtypes = [P, P]
+    lib.ns_collide_pairs.argtypes = [P, P, ctypes.c_int]
+    lib.ns_selftest_barrier_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.ns_world_apply_forces.argtypes = [P, P, P]
     _lib = lib
     return lib
 
@@ -214,6 +218,23 @@ class World:
     def step(self, dt=1.0 / 60.0, substeps=4):
         self._check(self._lib.ns_world_step(self._w, dt, substeps))
 
+    def apply_forces(self, force=None, torque=None):
+        """Add per-body force / torque (float32 arrays, n_bodies x 3) for the next step."""
+        f = None if force is None else np.ascontiguousarray(force, np.float32)
+        t = None if torque is None else np.ascontiguousarray(torque, np.float32)
+        for a in (f, t):
+            if a is not None and a.shape != (self.body_count, 3):
+                raise ValueError("force/torque must be n_bodies x 3")
+        self._check(self._lib.ns_world_apply_forces(self._w, _ptr(f), _ptr(t)))
+
+    def get_bodies_into(self, pos, rot, lin, ang):
+        """Readback into caller-owned arrays (for example pinned host buffers); any may be None."""
+        def addr(a):
+            if a is None:
+                return None
+            return ctypes.c_void_p(a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data)
+        self._check(self._lib.ns_world_get_bodies(self._w, addr(pos), addr(rot), addr(lin), addr(ang)))
+
     def synchronize(self):
         self._check(self._lib.ns_world_synchronize(self._w))
 
@@ -257,7 +278,7 @@ class World:
         return out
 
     def solver_counts(self):
-        out = np.zeros(8, np.int64)
+        out = np.zeros(16, np.int64)
         self._check(self._lib.ns_world_solver_counts(self._w, _ptr(out)))
         return out
 

@@ -1939,6 +1939,17 @@ void nso_counters(const nso_world* w, int32_t* out) {
   out[28] = w->recycled;
 }
 
+// body_api.rs:351 apply_body_force_to_center and :366 apply_body_torque, every body in id order
+void nso_apply_forces(nso_world* w, const float* force, const float* torque) {
+  for (size_t i = 0; i < w->bodies.size(); ++i) {
+    const Body& b = w->bodies[i];
+    if (b.set_index != 2) continue;
+    BodySim& s = w->awake_sims[b.local_index];
+    if (force) s.force = s.force + v3(force[3 * i], force[3 * i + 1], force[3 * i + 2]);
+    if (torque) s.torque = s.torque + v3(torque[3 * i], torque[3 * i + 1], torque[3 * i + 2]);
+  }
+}
+
 void nso_collide_pairs(nso_pair_job* jobs, nso_pair_result* results, int count) {
   for (int i = 0; i < count; ++i) {
     nso_pair_job& j = jobs[i];

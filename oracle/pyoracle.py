@@ -104,6 +104,8 @@ def load():
     lib.nso_contact_capacity.argtypes = [P]
     lib.nso_get_contacts.argtypes = [P, P, P, P]
     lib.nso_counters.argtypes = [P, P]
+    lib.nso_collide_pairs.argtypes = [P, P, ctypes.c_int]
+    lib.nso_apply_forces.argtypes = [P, P, P]
     _lib = lib
     return lib
 
@@ -179,6 +181,11 @@ class OracleWorld:
     def step(self, dt=1.0 / 60.0, substeps=4):
         self._lib.nso_step(self._w, dt, substeps)
 
+    def apply_forces(self, force=None, torque=None):
+        f = None if force is None else np.ascontiguousarray(force, np.float32)
+        t = None if torque is None else np.ascontiguousarray(torque, np.float32)
+        self._lib.nso_apply_forces(self._w, None if f is None else _ptr(f), None if t is None else _ptr(t))
+
     @property
     def body_count(self):
         return self._lib.nso_body_count(self._w)
@@ -207,3 +214,27 @@ class OracleWorld:
         out = np.zeros(32, np.int32)
         self._lib.nso_counters(self._w, _ptr(out))
         return out
+
+
+# One narrowphase pair per row, laid out like nso_pair_job / nso_pair_result (ns_oracle.h).
+PAIR_JOB_DTYPE = np.dtype([
+    ("type_a", "<i4"), ("type_b", "<i4"),
+    ("geom_a", "<f4", 7), ("geom_b", "<f4", 7),
+    ("xf", "<f4", 7),
+    ("sat_separation", "<f4"), ("sat_type", "<i4"), ("sat_index_a", "<i4"), ("sat_index_b", "<i4"),
+    ("sat_hit", "<i4"),
+    ("simplex_metric", "<f4"), ("simplex_count", "<i4"), ("simplex_ia", "<i4", 4), ("simplex_ib", "<i4", 4),
+])
+PAIR_RESULT_DTYPE = np.dtype([
+    ("normal", "<f4", 3), ("point_count", "<i4"), ("points", "<f4", (4, 4)), ("feature_ids", "<u4", 4),
+])
+
+
+def collide_pairs(jobs):
+    """Oracle narrowphase for each job (caches in ``jobs`` are updated in place)."""
+    assert jobs.dtype == PAIR_JOB_DTYPE and jobs.flags.c_contiguous
+    lib = load()
+    results = np.zeros(len(jobs), PAIR_RESULT_DTYPE)
+    if len(jobs):
+        lib.nso_collide_pairs(_ptr(jobs), _ptr(results), len(jobs))
+    return results
