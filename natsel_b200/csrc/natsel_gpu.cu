@@ -68,7 +68,7 @@ struct ns_world {
   size_t cub_sort_bytes = 0;
   void* cub_scan_tmp = nullptr;
   size_t cub_scan_bytes = 0;
-  int solver_blocks = 1;
+  int solver_blocks = 1;           // CTAs in the solver cluster
   bool state_shared = false;
   size_t state_smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
@@ -270,6 +270,8 @@ AABB shape_local_aabb(const HostShape& hs, Q q) {  // shape_runtime.rs:405
 int create_shape(ns_world* w, int bi, const ns_shape_def* def, HostShape hs) {
   if (w->uploaded) return fail(w, -1, "scene changes after the first step are not supported"), -1;
   if (bi < 0 || bi >= (int)w->bodies.size() || !def) return fail(w, -1, "invalid body or shape def"), -1;
+  // pair keys hold two 22-bit shape ids
+  if (w->shapes.size() >= (1u << 22) - 1) return fail(w, -1, "at most 4194303 shapes per world"), -1;
   int sid = (int)w->shapes.size();
   HostBody& b = w->bodies[bi];
   DShape& s = hs.d;
@@ -426,6 +428,7 @@ int upload_world(ns_world* w) {
   ALLOC(joints, DJoint, nj); ALLOC(joint_list, int, jlist.size());
   ALLOC(bp_keys_in, uint32_t, nsh); ALLOC(bp_keys_out, uint32_t, nsh);
   ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
+  ALLOC(bp_xy, float4, nsh); ALLOC(bp_z, float2, nsh); ALLOC(bp_meta, int, nsh);
   ALLOC(large_list, int, large.size());
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
@@ -471,20 +474,45 @@ int upload_world(ns_world* w) {
   w->allocations.push_back(w->cub_sort_tmp);
   NS_CUDA(w, cudaMalloc(&w->cub_scan_tmp, std::max<size_t>(w->cub_scan_bytes, 16)));
   w->allocations.push_back(w->cub_scan_tmp);
-  // state pass keeps every body's color mask in shared memory when it fits
+  // state pass: staged change chunks always live in shared memory; every body's color
+  // mask joins them there when it fits
   int max_smem = 0;
   NS_CUDA(w, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, w->def.device));
-  size_t need = (size_t)nb * sizeof(uint32_t);
+  size_t stage_bytes = (size_t)kStateChunk * 5 * sizeof(int);
+  size_t need = stage_bytes + (size_t)nb * sizeof(uint32_t);
   w->state_shared = need + 16 * 1024 <= (size_t)max_smem;
-  w->state_smem = w->state_shared ? need : 0;
-  if (w->state_shared && need > 48 * 1024)
-    NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-  // persistent solver grid: every block must be resident (cooperative launch)
-  int per_sm = 0;
-  NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, kSolveThreads, 0));
-  int max_blocks = per_sm * w->sm_count;
-  int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : std::max(1, std::min(w->sm_count, (na + kSolveThreads - 1) / kSolveThreads));
-  w->solver_blocks = std::max(1, std::min(want, max_blocks));
+  w->state_smem = w->state_shared ? need : stage_bytes;
+  if (w->state_smem > 48 * 1024)
+    NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
+  // solver: one thread-block cluster (non-portable sizes up to 16 CTAs where the device
+  // offers them); all of its CTAs are co-scheduled by the hardware. Each CTA carries two
+  // shared-memory constraint slots per thread for the prefetch pipeline.
+  {
+    NS_CUDA(w, cudaFuncSetAttribute(k_solve, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    NS_CUDA(w, cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem));
+    int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : kMaxSolveCluster;
+    want = std::max(1, std::min(want, kMaxSolveCluster));
+    int best = 0;
+    for (int cs = want; cs >= 1; --cs) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.blockDim = dim3(kSolveThreads);
+      cfg.gridDim = dim3(cs);
+      cfg.dynamicSmemBytes = kSolveSmem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, k_solve, &cfg);
+      if (e == cudaSuccess && clusters >= 1) { best = cs; break; }
+      cudaGetLastError();
+    }
+    if (best == 0) return fail(w, NS_ERR_CUDA, "the solver cluster does not fit on this device");
+    w->solver_blocks = best;
+  }
   // readback staging (64 B per body) and the body location table
   {
     std::vector<int> loc(nb);
@@ -524,6 +552,7 @@ int enqueue_pair_update(ns_world* w) {
   k_bp_keys<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   NS_CUDA(w, cub::DeviceRadixSort::SortPairs(w->cub_sort_tmp, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
                                               d.bp_vals_in, d.bp_vals_out, nsh, 0, 32, s));
+  k_bp_gather<<<blocks(d.n_small, 256), 256, 0, s>>>(d); ++nk;
   k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d); ++nk;
   k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
@@ -581,15 +610,17 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, cudaEventRecordExternal));
   // solver stages (solver_stages.rs:543)
-  NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
   {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(w->solver_blocks);
     cfg.blockDim = dim3(kSolveThreads);
+    cfg.dynamicSmemBytes = kSolveSmem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = w->solver_blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve, d, p, w->jr));
@@ -1073,6 +1104,7 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   out[8] = w->n_gyroscopic;
   out[11] = w->step_kernels;
   out[12] = w->kernel_launches;
+  out[13] = w->solver_blocks;
   if (!w->uploaded) return NS_OK;
   Control c;
   int st = read_control(w, &c);

@@ -11,7 +11,8 @@ namespace nsd {
 
 constexpr int kStatePassThreads = 1024;
 constexpr int kColorBlock = 1024;
-constexpr int kSolveThreads = 256;
+constexpr int kSolveThreads = 256;   // per CTA of the solver cluster
+constexpr int kMaxSolveCluster = 16;
 constexpr unsigned long long kHsEmpty = ~0ull;
 constexpr unsigned long long kHsTomb = ~0ull - 1ull;
 
@@ -36,6 +37,8 @@ struct DW {
   DJoint* joints; int n_joints; int* joint_list;
   // broadphase scratch
   uint32_t* bp_keys_in; uint32_t* bp_keys_out; int* bp_vals_in; int* bp_vals_out;
+  // small proxies in sorted lo.x order: (lo.x, hi.x, lo.y, hi.y), (lo.z, hi.z), shape id | flags
+  float4* bp_xy; float2* bp_z; int* bp_meta;
   int n_small; int* large_list; int n_large;
   int* seg_count; int* seg_off; int* seg_cursor;
   unsigned long long* cand; unsigned long long* sorted_keys; int cand_cap;
@@ -153,8 +156,9 @@ __device__ bool should_create_pair(const DW& w, int a, int b) {
   return true;
 }
 
-__device__ void emit_pair(const DW& w, int a, int b) {
-  if (!aabb_overlaps(w.fat[a], w.fat[b])) return;
+// Appends the pair {a, b} (fat AABBs known to overlap) when the filters accept it and it is
+// not already a contact.
+__device__ void emit_overlapping_pair(const DW& w, int a, int b) {
   int lo = a < b ? a : b, hi = a < b ? b : a;
   if (!should_create_pair(w, lo, hi)) return;
   unsigned long long k = pair_key(lo, hi);
@@ -165,35 +169,62 @@ __device__ void emit_pair(const DW& w, int a, int b) {
   atomicAdd(&w.seg_count[lo], 1);
 }
 
-__device__ int lower_bound_u32(const uint32_t* keys, int n, uint32_t v) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (keys[mid] < v) lo = mid + 1; else hi = mid;
-  }
-  return lo;
+__device__ void emit_pair(const DW& w, int a, int b) {
+  if (!aabb_overlaps(w.fat[a], w.fat[b])) return;
+  emit_overlapping_pair(w, a, b);
 }
 
+constexpr int kMetaMoved = 1 << 30;
+constexpr int kMetaStatic = 1 << 29;
+constexpr int kMetaId = (1 << 29) - 1;
+
+// Sorted small proxies as contiguous arrays, so the sweep below reads neighbouring memory.
+__global__ void k_bp_gather(DW w) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= w.n_small) return;
+  int b = w.bp_vals_out[j];
+  AABB f = w.fat[b];
+  w.bp_xy[j] = make_float4(f.lo.x, f.hi.x, f.lo.y, f.hi.y);
+  w.bp_z[j] = make_float2(f.lo.z, f.hi.z);
+  w.bp_meta[j] = b | (w.moved[b] ? kMetaMoved : 0) | (w.shapes[b].is_static ? kMetaStatic : 0);
+}
+
+// dynamic_tree.rs query of each moved proxy (contact_creation.rs:1000 find_pairs), as a
+// sort-and-sweep over lo.x: every proxy whose fat AABB can overlap proxy m in x lies in the
+// sorted window [lo.x(m) - widest proxy, hi.x(m)], walked outwards from m's own slot.
+// Each overlapping pair with at least one moved proxy is reported once (by the smaller
+// moved shape id when both moved).
 __global__ void k_bp_query(DW w) {
   if (w.ctl->moved_count == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n_small) return;
-  int m = w.bp_vals_out[i];
-  if (!w.moved[m]) return;
-  AABB fm = w.fat[m];
+  int mm = w.bp_meta[i];
+  if (!(mm & kMetaMoved)) return;
+  int m = mm & kMetaId;
+  bool m_static = (mm & kMetaStatic) != 0;
+  float4 A = w.bp_xy[i];
+  float2 Az = w.bp_z[i];
   float max_w = __int_as_float(w.ctl->max_width_bits);
-  // Conservative start: any proxy whose x-interval can reach fm.lo.x. The exact overlap
-  // test below decides, so a wider scan never changes the result.
-  float start_x = fm.lo.x - (max_w * 1.001f + 1e-3f);
-  int j = lower_bound_u32(w.bp_keys_out, w.n_small, float_sort_key(start_x));
-  uint32_t stop = float_sort_key(fm.hi.x);
-  for (; j < w.n_small; ++j) {
-    if (w.bp_keys_out[j] > stop) break;
-    int b = w.bp_vals_out[j];
-    if (b == m) continue;
-    if (w.moved[b] && b < m) continue;  // the smaller moved proxy of a pair reports it
-    if (w.shapes[m].is_static && w.shapes[b].is_static) continue;
-    emit_pair(w, m, b);
+  float start_x = A.x - (max_w * 1.001f + 1e-3f);
+  auto visit = [&](int j) {
+    int bm = w.bp_meta[j];
+    int b = bm & kMetaId;
+    if ((bm & kMetaMoved) && b < m) return;  // the smaller moved proxy of a pair reports it
+    if (m_static && (bm & kMetaStatic)) return;
+    float4 B = w.bp_xy[j];
+    if (A.y < B.x || A.x > B.y) return;  // aabb_overlaps (collision/aabb.rs:903), axis by axis
+    if (A.w < B.z || A.z > B.w) return;
+    float2 Bz = w.bp_z[j];
+    if (Az.y < Bz.x || Az.x > Bz.y) return;
+    emit_overlapping_pair(w, m, b);
+  };
+  for (int j = i + 1; j < w.n_small; ++j) {
+    if (w.bp_xy[j].x > A.y) break;
+    visit(j);
+  }
+  for (int j = i - 1; j >= 0; --j) {
+    if (w.bp_xy[j].x < start_x) break;
+    visit(j);
   }
 }
 
@@ -466,19 +497,33 @@ __global__ void __launch_bounds__(128) k_collide(DW w) {
 // then one thread applies the transitions in that order, keeping every body's color
 // membership as a 24-bit mask (bit c == the reference's colors[c].body_set bit).
 
-template <bool kShared>
-__device__ void state_serial(const DW& w, uint32_t* mask, int count) {
-  int ovf = w.ctl->overflow_count;
-  for (int i = 0; i < count; ++i) {
-    int cid = w.changed_list[i];
-    DContact& c = w.contacts[cid];
-    uint32_t f = c.flags;
-    int destroyed = 0;
-    auto remove = [&](int color, int local) {  // constraint_graph.rs:200
+// collide_pass.rs:386-430: contact state changes in contact-id order. Begin-touch adds the
+// contact to the constraint graph (constraint_graph.rs:113 greedy color from the bodies'
+// color masks), end-touch removes it (:200), disjoint contacts are destroyed
+// (contact_creation.rs:428). The coloring is order dependent, so one thread walks the
+// changes; the contact fields it needs are staged in shared memory by the whole block
+// chunk by chunk, and the results are written back by the whole block.
+constexpr int kStateChunk = 2048;
+struct StateStage {
+  int* cid; uint32_t* flags; int* info; int* ba; int* bb;
+};
+// info: bits 0..7 color + 1 (0 = none), bit 8 dynamic A, bit 9 dynamic B; after the walk
+// bits 16..23 hold the new color + 1 and bit 24 marks a destroyed contact.
+template <typename MaskT>
+__device__ int state_walk(const DW& w, MaskT mask, const StateStage& st, int n, int ovf) {
+  for (int i = 0; i < n; ++i) {
+    uint32_t f = st.flags[i];
+    int info = st.info[i];
+    int old_color = (info & 255) - 1;
+    int a = st.ba[i], b = st.bb[i];
+    int cid = st.cid[i];
+    int new_color = old_color, destroyed = 0;
+    auto remove = [&](int color) {  // constraint_graph.rs:200
       if (color != kOverflowIndex) {
-        mask[c.body_a] &= ~(1u << color);
-        mask[c.body_b] &= ~(1u << color);
+        mask[a] &= ~(1u << color);
+        mask[b] &= ~(1u << color);
       } else {
+        int local = w.contacts[cid].local;
         int last = ovf - 1;
         if (local != last) {
           int moved = w.overflow_list[last];
@@ -489,57 +534,48 @@ __device__ void state_serial(const DW& w, uint32_t* mask, int count) {
       }
     };
     if (f == 0) {
-    } else if (f & cSimDisjoint) {  // contact_creation.rs:428 destroy_contact
-      c.manifold_count = 0;
-      if (c.color != -1) remove(c.color, c.local);
-      c.alive = 0;
-      c.color = -1;
-      c.local = -1;
+    } else if (f & cSimDisjoint) {
+      if (old_color != -1) remove(old_color);
+      new_color = -1;
       destroyed = 1;
-    } else if (f & cSimStarted) {   // constraint_graph.rs:113 add_contact_to_graph
-      c.flags = (f & ~cSimStarted) | cTouching;
-      bool dyn_a = c.enc_a >= 0, dyn_b = c.enc_b >= 0;
+    } else if (f & cSimStarted) {
+      bool dyn_a = (info >> 8) & 1, dyn_b = (info >> 9) & 1;
       int color = kOverflowIndex;
       if (dyn_a && dyn_b) {
-        uint32_t avail = ~(mask[c.body_a] | mask[c.body_b]) & ((1u << kDynamicColorCount) - 1u);
+        uint32_t avail = ~(mask[a] | mask[b]) & ((1u << kDynamicColorCount) - 1u);
         if (avail) {
           color = __ffs(avail) - 1;
-          mask[c.body_a] |= 1u << color;
-          mask[c.body_b] |= 1u << color;
+          mask[a] |= 1u << color;
+          mask[b] |= 1u << color;
         }
       } else {
-        int d = dyn_a ? c.body_a : c.body_b;
+        int d = dyn_a ? a : b;
         uint32_t avail = ~mask[d] & (((1u << kOverflowIndex) - 1u) & ~1u);  // colors 22..1
         if (avail) {
           color = 31 - __clz(avail);
           mask[d] |= 1u << color;
         }
       }
-      c.color = color;
+      new_color = color;
       if (color == kOverflowIndex) {
-        c.local = ovf;
+        w.contacts[cid].local = ovf;
         w.overflow_list[ovf] = cid;
         ovf++;
-      } else {
-        c.local = -1;
       }
     } else if (f & cSimStopped) {
-      c.flags = f & ~(cSimStopped | cTouching);
-      int color = c.color, local = c.local;
-      c.color = -1;
-      c.local = -1;
-      remove(color, local);
+      remove(old_color);
+      new_color = -1;
     }
-    w.destroyed[i] = destroyed;
+    st.info[i] = (info & 0xffff) | ((new_color + 1) << 16) | (destroyed << 24);
   }
-  w.ctl->overflow_count = ovf;
+  return ovf;
 }
 
 __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_shared) {
-  extern __shared__ uint32_t smask[];
+  extern __shared__ uint32_t dyn_smem[];
   typedef cub::BlockScan<int, kStatePassThreads> Scan;
   __shared__ typename Scan::TempStorage scan_tmp;
-  __shared__ int total_s;
+  __shared__ int total_s, ovf_s;
   int t = threadIdx.x;
   int per = (w.n_words + kStatePassThreads - 1) / kStatePassThreads;
   int w0 = t * per, w1 = min(w0 + per, w.n_words);
@@ -556,19 +592,63 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
     }
     w.changed_bits[k] = 0;
   }
-  if (t == 0) { total_s = total; w.ctl->changed_count = total; }
+  if (t == 0) { total_s = total; w.ctl->changed_count = total; ovf_s = w.ctl->overflow_count; }
   __syncthreads();
   total = total_s;
   if (total == 0) return;
+  StateStage st;
+  st.cid = (int*)dyn_smem;
+  st.flags = (uint32_t*)(st.cid + kStateChunk);
+  st.info = (int*)(st.flags + kStateChunk);
+  st.ba = st.info + kStateChunk;
+  st.bb = st.ba + kStateChunk;
+  uint32_t* smask = (uint32_t*)(st.bb + kStateChunk);
   if (use_shared) {
     for (int b = t; b < w.n_bodies; b += kStatePassThreads) smask[b] = w.body_mask[b];
-    __syncthreads();
-    if (t == 0) state_serial<true>(w, smask, total);
-    __syncthreads();
-    for (int b = t; b < w.n_bodies; b += kStatePassThreads) w.body_mask[b] = smask[b];
-  } else {
-    if (t == 0) state_serial<false>(w, w.body_mask, total);
   }
+  for (int base = 0; base < total; base += kStateChunk) {
+    int n = min(kStateChunk, total - base);
+    for (int i = t; i < n; i += kStatePassThreads) {
+      int cid = w.changed_list[base + i];
+      const DContact& c = w.contacts[cid];
+      st.cid[i] = cid;
+      st.flags[i] = c.flags;
+      st.ba[i] = c.body_a;
+      st.bb[i] = c.body_b;
+      st.info[i] = (c.color + 1) | ((c.enc_a >= 0) << 8) | ((c.enc_b >= 0) << 9);
+    }
+    __syncthreads();
+    if (t == 0) ovf_s = use_shared ? state_walk(w, smask, st, n, ovf_s) : state_walk(w, w.body_mask, st, n, ovf_s);
+    __syncthreads();
+    for (int i = t; i < n; i += kStatePassThreads) {
+      DContact& c = w.contacts[st.cid[i]];
+      uint32_t f = st.flags[i];
+      int info = st.info[i];
+      int color = ((info >> 16) & 255) - 1;
+      int destroyed = (info >> 24) & 1;
+      if (f == 0) {
+      } else if (f & cSimDisjoint) {
+        c.manifold_count = 0;
+        c.alive = 0;
+        c.color = -1;
+        c.local = -1;
+      } else if (f & cSimStarted) {
+        c.flags = (f & ~cSimStarted) | cTouching;
+        c.color = color;
+        if (color != kOverflowIndex) c.local = -1;
+      } else if (f & cSimStopped) {
+        c.flags = f & ~(cSimStopped | cTouching);
+        c.color = -1;
+        c.local = -1;
+      }
+      w.destroyed[base + i] = destroyed;
+    }
+    __syncthreads();
+  }
+  if (use_shared) {
+    for (int b = t; b < w.n_bodies; b += kStatePassThreads) w.body_mask[b] = smask[b];
+  }
+  if (t == 0) w.ctl->overflow_count = ovf_s;
   __syncthreads();
   // Destroyed ids go back on the LIFO pool in id order (contact_creation.rs:543 free).
   int nd = 0;
@@ -646,8 +726,9 @@ __global__ void k_color_scan(DW w) {
   }
 }
 
+__device__ __forceinline__ DState* state_ptr(const DW& w, int i) { return &w.states[i]; }
 __device__ __forceinline__ DState state_at(const DW& w, int i) {
-  if (i >= 0) return w.states[i];
+  if (i >= 0) return *state_ptr(w, i);
   DState s;
   s.v = v3(0, 0, 0); s.w = v3(0, 0, 0); s.dp = v3(0, 0, 0); s.flags = 0; s.dq = qid();
   s.pad1 = 0; s.pad2 = 0;

@@ -1,10 +1,12 @@
 // Persistent colored solver (solver_stages.rs:543 solve_constraint_stages) and body
 // finalization (solver_integration.rs:587 finalize_body_range).
 //
-// One cooperative launch runs every substep: integrate velocities, then per stage
+// One thread-block cluster runs every substep: integrate velocities, then per stage
 // (warm start, push, relax) the overflow color on one thread followed by colors
-// 0..22, each color one grid-wide phase; then restitution and impulse storage.
-// Colors with no work are skipped by every block alike, so they cost no barrier.
+// 0..22, each color one cluster-wide phase separated by the hardware cluster barrier;
+// then restitution and impulse storage. Every CTA takes the same path through the
+// phases (the loop bounds are read identically by all of them), so every CTA reaches
+// every barrier; colors with no work are skipped by all CTAs alike.
 #pragma once
 #include "nsd_kernels.cuh"
 
@@ -56,6 +58,12 @@ __global__ void k_barrier_selftest(Control* ctl, unsigned long long limit_ns) {
   grid_barrier(ctl, bar, 1, limit_ns);
 }
 
+// barrier.cluster with release/acquire semantics: global-memory writes of every thread of
+// the cluster before the barrier are visible to every thread of the cluster after it.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ void store_state_vw(const DW& w, int i, const DState& s) {
   if (i >= 0 && (s.flags & kDynamicFlag)) {
     w.states[i].v = s.v;
@@ -63,21 +71,44 @@ __device__ __forceinline__ void store_state_vw(const DW& w, int i, const DState&
   }
 }
 
-// solver_integration.rs:263 integrate_velocities_range
-__device__ void integrate_velocity(const DW& w, const StepParams& p, int i) {
+// solver_integration.rs:263 integrate_velocities_range. Split into a load and an update so
+// a thread can issue the loads of all its bodies before the first update.
+struct IVIn {
+  float lin_damp, ang_damp, inv_mass, grav_scale;
+  V3 force, torque;
+  M3 iiw;
+  uint32_t flags;
+  Q q;
+  M3 inertia;
+  V3 v, w;
+  Q dq;
+};
+__device__ __forceinline__ IVIn load_iv(const DW& w, int i) {
   const DSim& sim = w.asims[i];
-  DState& st = w.states[i];
+  const DState& st = w.states[i];
+  IVIn r;
+  r.lin_damp = sim.linear_damping; r.ang_damp = sim.angular_damping;
+  r.inv_mass = sim.inv_mass; r.grav_scale = sim.gravity_scale;
+  r.force = sim.force; r.torque = sim.torque;
+  r.iiw = sim.inv_inertia_world;
+  r.flags = sim.flags;
+  r.q = sim.q;
+  r.inertia = sim.inertia;
+  r.v = st.v; r.w = st.w; r.dq = st.dq;
+  return r;
+}
+__device__ __forceinline__ void apply_iv(const DW& w, const StepParams& p, int i, const IVIn& sim) {
   float h = p.h;
-  V3 v = st.v, wv = st.w;
-  float ld = 1.0f / (1.0f + h * sim.linear_damping);
-  float ad = 1.0f / (1.0f + h * sim.angular_damping);
-  float gs = sim.inv_mass > 0.0f ? sim.gravity_scale : 0.0f;
+  V3 v = sim.v, wv = sim.w;
+  float ld = 1.0f / (1.0f + h * sim.lin_damp);
+  float ad = 1.0f / (1.0f + h * sim.ang_damp);
+  float gs = sim.inv_mass > 0.0f ? sim.grav_scale : 0.0f;
   V3 lvd = blend2(h * sim.inv_mass, sim.force, h * gs, p.gravity);
   v = mul_add(lvd, ld, v);
-  V3 avd = h * mul_mv(sim.inv_inertia_world, sim.torque);
+  V3 avd = h * mul_mv(sim.iiw, sim.torque);
   wv = mul_add(avd, ad, wv);
   if (sim.flags & kGyroscopic) {
-    Q q = mul_quat(st.dq, sim.q);
+    Q q = mul_quat(sim.dq, sim.q);
     V3 om1 = inv_rotate(q, wv);
     V3 om2 = om1;
     float i00 = sim.inertia.cx.x, i01 = sim.inertia.cy.x, i02 = sim.inertia.cz.x;
@@ -99,13 +130,13 @@ __device__ void integrate_velocity(const DW& w, const StepParams& p, int i) {
     om2 = om2 - solve3(J, b);
     wv = rotate(q, om2);
   }
+  DState& st = w.states[i];
   st.v = v;
   st.w = wv;
 }
 
-// solver_integration.rs:377 integrate_positions_range
-__device__ void integrate_position(const DW& w, const StepParams& p, int i) {
-  DState st = w.states[i];
+// solver_integration.rs:377 integrate_positions_range (the state row is the only input)
+__device__ __forceinline__ void apply_ip(const DW& w, const StepParams& p, int i, DState st) {
   float maxl = p.max_linear_speed;
   float maxa = kMaxRotation * p.inv_dt;
   float maxl2 = maxl * maxl, maxa2 = maxa * maxa;
@@ -133,6 +164,12 @@ __device__ void integrate_position(const DW& w, const StepParams& p, int i) {
   w.states[i] = st;
 }
 
+// Contact constraint data in registers. load_direct issues every load of a constraint
+// before the first store and before the dependent body-state loads, so one L2 round trip
+// brings all the planes instead of one per point behind each impulse store. Read-only
+// planes (written by prepare, never by the solver) go through the non-coherent path;
+// impulse planes are read and written only by the thread that processes the constraint in
+// a phase, with phase barriers in between.
 struct CLoad {
   int ia, ib, pc;
   bool is_static;
@@ -140,10 +177,8 @@ struct CLoad {
   Sym sa, sb;
   V3 n;
 };
-__device__ __forceinline__ CLoad load_constraint(const CPlanes& P, int k) {
+__device__ __forceinline__ CLoad unpack_constraint(int4 idx, float4 m, float4 a0, float4 a1, float4 b1, float4 nn) {
   CLoad c;
-  int4 idx = P.idx[k];
-  float4 m = P.mass[k], a0 = P.ia0[k], a1 = P.ia1[k], b1 = P.ib1[k], nn = P.n[k];
   c.ia = idx.x; c.ib = idx.y; c.pc = idx.w & 255; c.is_static = (idx.w & 256) != 0;
   c.ima = m.x; c.imb = m.y; c.friction = m.z; c.restitution = m.w;
   c.sa.xx = a0.x; c.sa.xy = a0.y; c.sa.xz = a0.z; c.sa.yy = a0.w; c.sa.yz = a1.x; c.sa.zz = a1.y;
@@ -153,39 +188,66 @@ __device__ __forceinline__ CLoad load_constraint(const CPlanes& P, int k) {
   return c;
 }
 
+enum Stage { kWarm = 0, kPush = 1, kRelax = 2, kRestitution = 3 };
+
+struct CData {
+  CLoad c;
+  float4 t1, t2, ca, cb, fr, roll, rm, tm;
+  float4 pra[4], prb[4], pimp[4];
+  float prest[4];
+};
+
+__device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d) {
+  d.c = unpack_constraint(__ldg(&P.idx[k]), __ldg(&P.mass[k]), __ldg(&P.ia0[k]), __ldg(&P.ia1[k]),
+                          __ldg(&P.ib1[k]), __ldg(&P.n[k]));
+  if (stage == kWarm || stage == kRelax) {
+    d.t1 = __ldg(&P.t1[k]); d.t2 = __ldg(&P.t2[k]); d.ca = __ldg(&P.ca[k]);
+    d.cb = P.cb[k]; d.fr = P.fr[k]; d.roll = P.roll[k];
+  }
+  if (stage == kRelax) { d.rm = __ldg(&P.rm[k]); d.tm = __ldg(&P.tm[k]); }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q < d.c.pc) {
+      d.pra[q] = __ldg(&P.pra[q * P.cap + k]);
+      d.prb[q] = __ldg(&P.prb[q * P.cap + k]);
+      d.pimp[q] = P.pimp[q * P.cap + k];
+      if (stage == kRestitution) d.prest[q] = P.prest[q * P.cap + k];
+    }
+  }
+}
+
 // contact_solver.rs:697 warm_start_contacts_body
-__device__ void warm_start_constraint(const DW& w, int k) {
-  const CPlanes& P = w.cp;
-  CLoad c = load_constraint(P, k);
-  float4 t1f = P.t1[k], t2f = P.t2[k], caf = P.ca[k], cbf = P.cb[k], frf = P.fr[k];
-  V3 t1 = v3(t1f.x, t1f.y, t1f.z), t2 = v3(t2f.x, t2f.y, t2f.z);
-  V3 center_a = v3(caf.x, caf.y, caf.z), center_b = v3(cbf.x, cbf.y, cbf.z);
-  float twist = cbf.w;
+__device__ void warm_start_constraint(const DW& w, const CData& d) {
+  const CLoad& c = d.c;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  V3 t1 = v3(d.t1.x, d.t1.y, d.t1.z), t2 = v3(d.t2.x, d.t2.y, d.t2.z);
+  V3 center_a = v3(d.ca.x, d.ca.y, d.ca.z), center_b = v3(d.cb.x, d.cb.y, d.cb.z);
+  float twist = d.cb.w;
   V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
   float tni = 0.0f;
   V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
-  for (int p = 0; p < c.pc; ++p) {
-    float4 ra = P.pra[p * P.cap + k], rb = P.prb[p * P.cap + k];
-    float ni = P.pimp[p * P.cap + k].x;
-    tni += ni;
-    moa = mul_add(moa, ni, v3(ra.x, ra.y, ra.z));
-    mob = mul_add(mob, ni, v3(rb.x, rb.y, rb.z));
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q < c.pc) {
+      float ni = d.pimp[q].x;
+      tni += ni;
+      moa = mul_add(moa, ni, v3(d.pra[q].x, d.pra[q].y, d.pra[q].z));
+      mob = mul_add(mob, ni, v3(d.prb[q].x, d.prb[q].y, d.prb[q].z));
+    }
   }
   V3 n = c.n;
-  V3 fi = frf.x * t1;
-  fi = mul_add(fi, frf.y, t2);
+  V3 fi = d.fr.x * t1;
+  fi = mul_add(fi, d.fr.y, t2);
   V3 lin = mul_add(fi, tni, n);
   V3 twi = twist * n;
   V3 anga = cross(moa, n) + cross(center_a, fi) + twi;
   V3 angb = cross(mob, n) + cross(center_b, fi) + twi;
   if (c.rolling > 0.0f) {
-    float4 r = P.roll[k];
-    V3 ri = v3(r.x, r.y, r.z);
+    V3 ri = v3(d.roll.x, d.roll.y, d.roll.z);
     anga = anga + ri;
     angb = angb + ri;
   }
   li = li + lin; aia = aia + anga; aib = aib + angb;
-  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
   ba.w = ba.w - sym_mv(c.sa, aia);
   ba.v = ba.v - c.ima * li;
   bb.w = bb.w + sym_mv(c.sb, aib);
@@ -195,16 +257,16 @@ __device__ void warm_start_constraint(const DW& w, int k) {
 }
 
 // contact_solver.rs:796 push_contacts_body
-__device__ void push_constraint(const DW& w, const StepParams& p, int k) {
+__device__ void push_constraint(const DW& w, const StepParams& p, int k, const CData& d) {
   const CPlanes& P = w.cp;
-  CLoad c = load_constraint(P, k);
+  const CLoad& c = d.c;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
   float inv_h = p.inv_h;
   float cs = -p.contact_speed;
   float br = c.is_static ? p.static_softness.mass_scale * p.static_softness.bias_rate
                          : p.contact_softness.mass_scale * p.contact_softness.bias_rate;
   float ms = c.is_static ? p.static_softness.mass_scale : p.contact_softness.mass_scale;
   float is = c.is_static ? p.static_softness.impulse_scale : p.contact_softness.impulse_scale;
-  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
   V3 dp = bb.dp - ba.dp;
   float im = c.ima + c.imb;
   V3 n = c.n;
@@ -212,29 +274,32 @@ __device__ void push_constraint(const DW& w, const StepParams& p, int k) {
   V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
   float lnv = dot(n, bb.v - ba.v);
   float mi = 0.0f;
-  for (int q = 0; q < c.pc; ++q) {
-    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
-    float4 imp4 = P.pimp[q * P.cap + k];
-    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
-    float base_sep = raf.w, nmass = rbf.w, nimp = imp4.x;
-    float s = (ns + (dot(nb, rb) - dot(na, ra))) + base_sep;
-    bool sep = s > 0.0f;
-    float spec_bias = s * inv_h;
-    float ovl = maxf(br * s, cs);
-    float vb = sep ? spec_bias : ovl;
-    float pms = sep ? 1.0f : ms;
-    float pis = sep ? 0.0f : is;
-    V3 ua = cross(ra, n), ub = cross(rb, n);
-    V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
-    float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
-    float neg = nmass * (pms * vn + vb) + pis * nimp;
-    float impulse = maxf(-neg, -nimp);
-    imp4.x = nimp + impulse;
-    P.pimp[q * P.cap + k] = imp4;
-    lnv += im * impulse;
-    mi += impulse;
-    ba.w = ba.w - impulse * ga;
-    bb.w = bb.w + impulse * gb;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q < c.pc) {
+      float4 raf = d.pra[q], rbf = d.prb[q];
+      float4 imp4 = d.pimp[q];
+      V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+      float base_sep = raf.w, nmass = rbf.w, nimp = imp4.x;
+      float s = (ns + (dot(nb, rb) - dot(na, ra))) + base_sep;
+      bool sep = s > 0.0f;
+      float spec_bias = s * inv_h;
+      float ovl = maxf(br * s, cs);
+      float vb = sep ? spec_bias : ovl;
+      float pms = sep ? 1.0f : ms;
+      float pis = sep ? 0.0f : is;
+      V3 ua = cross(ra, n), ub = cross(rb, n);
+      V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
+      float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+      float neg = nmass * (pms * vn + vb) + pis * nimp;
+      float impulse = maxf(-neg, -nimp);
+      imp4.x = nimp + impulse;
+      P.pimp[q * P.cap + k] = imp4;
+      lnv += im * impulse;
+      mi += impulse;
+      ba.w = ba.w - impulse * ga;
+      bb.w = bb.w + impulse * gb;
+    }
   }
   V3 Pv = mi * n;
   ba.v = ba.v - c.ima * Pv;
@@ -244,49 +309,51 @@ __device__ void push_constraint(const DW& w, const StepParams& p, int k) {
 }
 
 // contact_solver.rs:927 solve_contacts_body (relax)
-__device__ void relax_constraint(const DW& w, const StepParams& p, int k) {
+__device__ void relax_constraint(const DW& w, const StepParams& p, int k, const CData& d) {
   const CPlanes& P = w.cp;
-  CLoad c = load_constraint(P, k);
+  const CLoad& c = d.c;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
+  float4 cbf = d.cb, fr = d.fr, ro = d.roll, rmv = d.rm, caf = d.ca, tmf = d.tm;
+  bool any_rolling = c.rolling > 0.0f;
   float inv_h = p.inv_h;
   const float eps = kEps;
-  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
-  bool any_rolling = c.rolling > 0.0f;
   V3 dp = bb.dp - ba.dp;
   float im = c.ima + c.imb;
   V3 n = c.n;
-  float4 t1f = P.t1[k], t2f = P.t2[k];
-  V3 t1 = v3(t1f.x, t1f.y, t1f.z), t2 = v3(t2f.x, t2f.y, t2f.z);
+  V3 t1 = v3(d.t1.x, d.t1.y, d.t1.z), t2 = v3(d.t2.x, d.t2.y, d.t2.z);
   float ns = dot(n, dp);
   V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
   V3 dv = bb.v - ba.v;
   float lnv = dot(n, dv);
-  float lt1 = dot(t1, dv) - t1f.w;
-  float lt2 = dot(t2, dv) - t2f.w;
+  float lt1 = dot(t1, dv) - d.t1.w;
+  float lt2 = dot(t2, dv) - d.t2.w;
   float mi = 0.0f, tni = 0.0f, ttl = 0.0f;
-  for (int q = 0; q < c.pc; ++q) {
-    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
-    float4 imp4 = P.pimp[q * P.cap + k];
-    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
-    float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
-    float vb = maxf(0.0f, s * inv_h);
-    V3 ua = cross(ra, n), ub = cross(rb, n);
-    V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
-    float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
-    float neg = rbf.w * (vn + vb);
-    float impulse = maxf(-neg, -imp4.x);
-    float ni = imp4.x + impulse;
-    imp4.x = ni;
-    imp4.y = imp4.y + ni;
-    P.pimp[q * P.cap + k] = imp4;
-    tni += ni;
-    ttl += imp4.z * ni;
-    lnv += im * impulse;
-    mi += impulse;
-    ba.w = ba.w - impulse * ga;
-    bb.w = bb.w + impulse * gb;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q < c.pc) {
+      float4 raf = d.pra[q], rbf = d.prb[q];
+      float4 imp4 = d.pimp[q];
+      V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+      float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
+      float vb = maxf(0.0f, s * inv_h);
+      V3 ua = cross(ra, n), ub = cross(rb, n);
+      V3 ga = sym_mv(c.sa, ua), gb = sym_mv(c.sb, ub);
+      float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+      float neg = rbf.w * (vn + vb);
+      float impulse = maxf(-neg, -imp4.x);
+      float ni = imp4.x + impulse;
+      imp4.x = ni;
+      imp4.y = imp4.y + ni;
+      P.pimp[q * P.cap + k] = imp4;
+      tni += ni;
+      ttl += imp4.z * ni;
+      lnv += im * impulse;
+      mi += impulse;
+      ba.w = ba.w - impulse * ga;
+      bb.w = bb.w + impulse * gb;
+    }
   }
   if (any_rolling) {
-    float4 fr = P.fr[k], ro = P.roll[k], rmv = P.rm[k];
     Sym rm = {fr.z, fr.w, ro.w, rmv.x, rmv.y, rmv.z};
     V3 di = sym_mv(rm, ba.w - bb.w);
     V3 old = v3(ro.x, ro.y, ro.z);
@@ -305,7 +372,6 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k) {
     P.roll[k] = make_float4(rimp.x, rimp.y, rimp.z, ro.w);
   }
   {
-    float4 caf = P.ca[k], cbf = P.cb[k];
     float ts = dot(n, bb.w - ba.w);
     float ml = c.friction * ttl;
     float old = cbf.w;
@@ -316,7 +382,6 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k) {
     ba.w = ba.w - impulse * sym_mv(c.sa, n);
     bb.w = bb.w + impulse * sym_mv(c.sb, n);
     V3 ra = v3(caf.x, caf.y, caf.z), rb = v3(cbf.x, cbf.y, cbf.z);
-    float4 tmf = P.tm[k], fr = P.fr[k];
     M2 tm;
     tm.cx = v2(tmf.x, tmf.y);
     tm.cy = v2(tmf.z, tmf.w);
@@ -347,51 +412,61 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k) {
 }
 
 // contact_solver.rs:1135 apply_restitution_body
-__device__ void restitution_constraint(const DW& w, const StepParams& p, int k) {
+__device__ void restitution_constraint(const DW& w, const StepParams& p, int k, const CData& d) {
   const CPlanes& P = w.cp;
-  CLoad c = load_constraint(P, k);
+  const CLoad& c = d.c;
   if (c.restitution == 0.0f) return;
+  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
   float inv_h = p.inv_h;
   float nrt = -p.restitution_threshold;
-  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
   bool rmask = c.restitution > 0.0f;
   V3 dp = bb.dp - ba.dp;
   V3 n = c.n;
   float ns = dot(n, dp);
   V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
-  for (int q = 0; q < c.pc; ++q) {
-    float4 raf = P.pra[q * P.cap + k], rbf = P.prb[q * P.cap + k];
-    float4 imp4 = P.pimp[q * P.cap + k];
-    float rest_imp = P.prest[q * P.cap + k];
-    V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
-    float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
-    float nm = rmask ? rbf.w : 0.0f;
-    float comp = imp4.y - rest_imp;
-    bool armed = rmask && imp4.w < nrt && comp > 0.0f;
-    float sb = maxf(0.0f, s * inv_h);
-    float vb = armed ? c.restitution * imp4.w : sb;
-    V3 vra = ba.v + cross(ba.w, ra), vrb = bb.v + cross(bb.w, rb);
-    float vn = dot(vrb - vra, n);
-    float neg = nm * (vn + vb);
-    float ni = maxf(imp4.x - neg, 0.0f);
-    float impulse = ni - imp4.x;
-    float app = minf(maxf(-nm * vn, 0.0f), maxf(impulse, 0.0f));
-    float allow = c.restitution * (comp + app) - rest_imp;
-    float mx = app + maxf(allow, 0.0f);
-    impulse = armed ? minf(impulse, mx) : impulse;
-    imp4.x = imp4.x + impulse;
-    rest_imp = rest_imp + (impulse - app);
-    imp4.y = imp4.y + impulse;
-    P.pimp[q * P.cap + k] = imp4;
-    P.prest[q * P.cap + k] = rest_imp;
-    V3 Pv = impulse * n;
-    ba.w = ba.w - sym_mv(c.sa, cross(ra, Pv));
-    ba.v = ba.v - c.ima * Pv;
-    bb.w = bb.w + sym_mv(c.sb, cross(rb, Pv));
-    bb.v = bb.v + c.imb * Pv;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q < c.pc) {
+      float4 raf = d.pra[q], rbf = d.prb[q];
+      float4 imp4 = d.pimp[q];
+      float rest_imp = d.prest[q];
+      V3 ra = v3(raf.x, raf.y, raf.z), rb = v3(rbf.x, rbf.y, rbf.z);
+      float s = (ns + (dot(nb, rb) - dot(na, ra))) + raf.w;
+      float nm = rmask ? rbf.w : 0.0f;
+      float comp = imp4.y - rest_imp;
+      bool armed = rmask && imp4.w < nrt && comp > 0.0f;
+      float sb = maxf(0.0f, s * inv_h);
+      float vb = armed ? c.restitution * imp4.w : sb;
+      V3 vra = ba.v + cross(ba.w, ra), vrb = bb.v + cross(bb.w, rb);
+      float vn = dot(vrb - vra, n);
+      float neg = nm * (vn + vb);
+      float ni = maxf(imp4.x - neg, 0.0f);
+      float impulse = ni - imp4.x;
+      float app = minf(maxf(-nm * vn, 0.0f), maxf(impulse, 0.0f));
+      float allow = c.restitution * (comp + app) - rest_imp;
+      float mx = app + maxf(allow, 0.0f);
+      impulse = armed ? minf(impulse, mx) : impulse;
+      imp4.x = imp4.x + impulse;
+      rest_imp = rest_imp + (impulse - app);
+      imp4.y = imp4.y + impulse;
+      P.pimp[q * P.cap + k] = imp4;
+      P.prest[q * P.cap + k] = rest_imp;
+      V3 Pv = impulse * n;
+      ba.w = ba.w - sym_mv(c.sa, cross(ra, Pv));
+      ba.v = ba.v - c.ima * Pv;
+      bb.w = bb.w + sym_mv(c.sb, cross(rb, Pv));
+      bb.v = bb.v + c.imb * Pv;
+    }
   }
   store_state_vw(w, c.ia, ba);
   store_state_vw(w, c.ib, bb);
+}
+
+__device__ __forceinline__ void run_contact(const DW& w, const StepParams& p, int k, int stage, const CData& d) {
+  if (stage == kWarm) warm_start_constraint(w, d);
+  else if (stage == kPush) push_constraint(w, p, k, d);
+  else if (stage == kRelax) relax_constraint(w, p, k, d);
+  else restitution_constraint(w, p, k, d);
 }
 
 // contact_solver.rs:1258 store_impulses_body
@@ -416,7 +491,7 @@ __device__ void store_constraint(const DW& w, int k) {
 
 // overflow_contact_solver.rs:308-700 sequential overflow color
 __device__ void ovf_store_velocity(const DW& w, int i, uint32_t flags, V3 v, V3 wv) {
-  if (i >= 0 && (flags & kDynamicFlag)) { w.states[i].v = v; w.states[i].w = wv; }
+  if (i >= 0 && (flags & kDynamicFlag)) { DState* d = state_ptr(w, i); d->v = v; d->w = wv; }
 }
 __device__ void warm_start_overflow(const DW& w, int n) {
   for (int i = 0; i < n; ++i) {
@@ -442,13 +517,13 @@ __device__ void warm_start_overflow(const DW& w, int n) {
       aia = aia + (anga + mc.rolling_impulse);
       aib = aib + (angb + mc.rolling_impulse);
     }
-    if (c.index_a >= 0 && (w.states[c.index_a].flags & kDynamicFlag)) {
-      DState& s = w.states[c.index_a];
+    if (c.index_a >= 0 && (state_ptr(w, c.index_a)->flags & kDynamicFlag)) {
+      DState& s = *state_ptr(w, c.index_a);
       s.v = mul_sub(s.v, c.inv_mass_a, li);
       s.w = s.w - mul_mv(c.inv_ia, aia);
     }
-    if (c.index_b >= 0 && (w.states[c.index_b].flags & kDynamicFlag)) {
-      DState& s = w.states[c.index_b];
+    if (c.index_b >= 0 && (state_ptr(w, c.index_b)->flags & kDynamicFlag)) {
+      DState& s = *state_ptr(w, c.index_b);
       s.v = mul_add(s.v, c.inv_mass_b, li);
       s.w = s.w + mul_mv(c.inv_ib, aib);
     }
@@ -685,7 +760,7 @@ __device__ V3 solve_point_constraint(float ma, float mb, M3 ia, M3 ib, V3 ra, V3
 }
 
 // revolute_joint.rs:261 warm_start_revolute_joint
-__device__ void warm_start_joint(const DW& w, DJoint& j) {
+__device__ __noinline__ void warm_start_joint(const DW& w, DJoint& j) {
   float mA = j.inv_mass_a, mB = j.inv_mass_b;
   DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
   V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
@@ -704,7 +779,7 @@ __device__ void warm_start_joint(const DW& w, DJoint& j) {
 }
 
 // revolute_joint.rs:316 solve_revolute_joint
-__device__ void solve_joint(const DW& w, const StepParams& p, DJoint& j, bool use_bias) {
+__device__ __noinline__ void solve_joint(const DW& w, const StepParams& p, DJoint& j, bool use_bias) {
   float mA = j.inv_mass_a, mB = j.inv_mass_b;
   M3 iA = j.inv_ia, iB = j.inv_ib;
   DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
@@ -830,29 +905,6 @@ __device__ void solve_joint(const DW& w, const StepParams& p, DJoint& j, bool us
   store_state_vw(w, j.index_b, sb);
 }
 
-enum Stage { kWarm = 0, kPush = 1, kRelax = 2, kRestitution = 3 };
-
-__device__ void run_color(const DW& w, const StepParams& p, const JointRanges& jr, const int* coff,
-                          int c, int stage) {
-  int nj = jr.off[c + 1] - jr.off[c];
-  int nc = coff[c + 1] - coff[c];
-  int total = (stage == kRestitution ? 0 : nj) + nc;
-  int stride = gridDim.x * blockDim.x;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
-    if (stage != kRestitution && t < nj) {
-      DJoint& j = w.joints[w.joint_list[jr.off[c] + t]];
-      if (stage == kWarm) warm_start_joint(w, j);
-      else solve_joint(w, p, j, stage == kPush);
-    } else {
-      int k = coff[c] + (t - (stage == kRestitution ? 0 : nj));
-      if (stage == kWarm) warm_start_constraint(w, k);
-      else if (stage == kPush) push_constraint(w, p, k);
-      else if (stage == kRelax) relax_constraint(w, p, k);
-      else restitution_constraint(w, p, k);
-    }
-  }
-}
-
 __device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges& jr, int n_ovf, int stage) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   if (stage != kRestitution) {
@@ -868,48 +920,71 @@ __device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges
   else restitution_overflow(w, p, n_ovf);
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_solve(DW w, StepParams p, JointRanges jr) {
+// Phase codes: contact phases stage * 32 + color; the rest as below.
+constexpr int kPhaseIntegrateVelocity = 1000, kPhaseIntegratePosition = 1001, kPhaseOverflow = 2000;
+constexpr size_t kSolveSmem = 0;
+
+__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, JointRanges jr) {
   __shared__ int coff[25];
-  __shared__ int n_ovf_s, any_rest_s;
+  __shared__ int phases[3 * 25 + 2];  // one substep
+  __shared__ int rphases[25];         // one restitution iteration
+  __shared__ int n_ph_s, n_rph_s, n_ovf_s;
   if (threadIdx.x < 25) coff[threadIdx.x] = threadIdx.x < 24 ? w.ctl->color_offset[threadIdx.x] : w.ctl->color_offset[23];
-  if (threadIdx.x == 0) { n_ovf_s = w.ctl->overflow_count; any_rest_s = w.ctl->any_restitution; }
   __syncthreads();
-  int n_ovf = n_ovf_s;
-  bool ovf_work = n_ovf > 0 || jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex];
-  int bar = 0;
-  int stride = gridDim.x * blockDim.x;
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int sub = 0; sub < p.substeps; ++sub) {
-    for (int i = g; i < w.n_awake; i += stride) integrate_velocity(w, p, i);
-    if (!grid_barrier(w.ctl, bar)) return;
+  if (threadIdx.x == 0) {
+    int n_ovf = w.ctl->overflow_count;
+    bool ovf_work = n_ovf > 0 || jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex];
+    int n = 0;
+    phases[n++] = kPhaseIntegrateVelocity;
     for (int stage = kWarm; stage <= kRelax; ++stage) {
-      if (stage == kRelax) {
-        for (int i = g; i < w.n_awake; i += stride) integrate_position(w, p, i);
-        if (!grid_barrier(w.ctl, bar)) return;
-      }
-      if (ovf_work) {
-        run_overflow(w, p, jr, n_ovf, stage);
-        if (!grid_barrier(w.ctl, bar)) return;
-      }
-      for (int c = 0; c < kOverflowIndex; ++c) {
-        if (coff[c + 1] == coff[c] && jr.off[c + 1] == jr.off[c]) continue;
-        run_color(w, p, jr, coff, c, stage);
-        if (!grid_barrier(w.ctl, bar)) return;
-      }
+      if (stage == kRelax) phases[n++] = kPhaseIntegratePosition;
+      if (ovf_work) phases[n++] = kPhaseOverflow + stage;
+      for (int c = 0; c < kOverflowIndex; ++c)
+        if (coff[c + 1] != coff[c] || jr.off[c + 1] != jr.off[c]) phases[n++] = stage * 32 + c;
     }
+    int m = 0;
+    if (w.ctl->any_restitution && p.restitution_iterations > 0) {
+      if (n_ovf > 0) rphases[m++] = kPhaseOverflow + kRestitution;
+      for (int c = 0; c < kOverflowIndex; ++c)
+        if (coff[c + 1] != coff[c]) rphases[m++] = kRestitution * 32 + c;
+    }
+    n_ph_s = n;
+    n_rph_s = m;
+    n_ovf_s = n_ovf;
   }
-  if (any_rest_s && p.restitution_iterations > 0) {
-    for (int it = 0; it < p.restitution_iterations; ++it) {
-      if (n_ovf > 0) {
-        run_overflow(w, p, jr, n_ovf, kRestitution);
-        if (!grid_barrier(w.ctl, bar)) return;
-      }
-      for (int c = 0; c < kOverflowIndex; ++c) {
-        if (coff[c + 1] == coff[c]) continue;
-        run_color(w, p, jr, coff, c, kRestitution);
-        if (!grid_barrier(w.ctl, bar)) return;
+  __syncthreads();
+  const int n_ph = n_ph_s, n_rph = n_rph_s, n_ovf = n_ovf_s;
+  const int main_phases = p.substeps * n_ph;
+  const int total_phases = main_phases + (n_rph > 0 ? p.restitution_iterations * n_rph : 0);
+  auto phase_at = [&](int s) { return s < main_phases ? phases[s % n_ph] : rphases[(s - main_phases) % n_rph]; };
+  const int stride = gridDim.x * blockDim.x;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int s = 0; s < total_phases; ++s) {
+    int ph = phase_at(s);
+    if (ph == kPhaseIntegrateVelocity) {
+      for (int i = g; i < w.n_awake; i += stride) apply_iv(w, p, i, load_iv(w, i));
+    } else if (ph == kPhaseIntegratePosition) {
+      for (int i = g; i < w.n_awake; i += stride) apply_ip(w, p, i, w.states[i]);
+    } else if (ph >= kPhaseOverflow) {
+      run_overflow(w, p, jr, n_ovf, ph - kPhaseOverflow);
+    } else {
+      int stage = ph >> 5, c = ph & 31;
+      int nj = stage == kRestitution ? 0 : jr.off[c + 1] - jr.off[c];
+      int total = nj + (coff[c + 1] - coff[c]);
+      for (int t = g; t < total; t += stride) {
+        if (t < nj) {
+          DJoint& j = w.joints[w.joint_list[jr.off[c] + t]];
+          if (stage == kWarm) warm_start_joint(w, j);
+          else solve_joint(w, p, j, stage == kPush);
+        } else {
+          int k = coff[c] + (t - nj);
+          CData d;
+          load_direct(w.cp, k, stage, d);
+          run_contact(w, p, k, stage, d);
+        }
       }
     }
+    cluster_sync_all();
   }
   // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
   if (g == 0) store_overflow(w, n_ovf);
