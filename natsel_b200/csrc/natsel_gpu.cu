@@ -589,15 +589,19 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   p.gravity = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
   auto blocks = [](int n, int t) { return std::max(1, (n + t - 1) / t); };
   int nk = 0;
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[0], s, cudaEventRecordExternal));
+  // phase events: graph nodes that record externally when captured, plain records otherwise
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  NS_CUDA(w, cudaStreamIsCapturing(s, &capturing));
+  unsigned ev_flags = capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[0], s, ev_flags));
   {
     int st = enqueue_pair_update(w);
     if (st) return st;
   }
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, cudaEventRecordExternal));
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, ev_flags));
   // narrowphase (collide_pass.rs:164)
-  k_collide<<<blocks(d.cap, 128), 128, 0, s>>>(d); ++nk;
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, cudaEventRecordExternal));
+  k_collide<<<blocks(d.cap, kCollideThreads), kCollideThreads, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
   k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0); ++nk;
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
@@ -608,7 +612,7 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
     ++nk;
   }
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, cudaEventRecordExternal));
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, ev_flags));
   // solver stages (solver_stages.rs:543)
   {
     cudaLaunchConfig_t cfg = {};
@@ -626,10 +630,10 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve, d, p, w->jr));
     ++nk;
   }
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, cudaEventRecordExternal));
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, ev_flags));
   // finalize (solver_integration.rs:435)
   k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p); ++nk;
-  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, cudaEventRecordExternal));
+  NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, ev_flags));
   NS_CUDA(w, cudaGetLastError());
   w->step_kernels = w->pair_kernels + nk;
   return NS_OK;

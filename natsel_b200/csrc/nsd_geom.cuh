@@ -11,7 +11,11 @@ namespace nsd {
 // Clip buffers hold 64 vertices like the reference (manifold.rs:9 MAX_CLIP_POINTS);
 // writes past the end are dropped instead of corrupting memory (the reference
 // would abort there).
-constexpr int kClipCap = 64;
+// Clip buffer capacity. The reference sizes its buffers for 64 points (manifold.rs:10);
+// a box face clipped by the four side planes of another box face has at most 8 vertices
+// (Sutherland-Hodgman adds at most one vertex per plane to a convex polygon), so 16 keeps
+// twice that as headroom; every write is bounds-guarded.
+constexpr int kClipCap = 16;
 
 NSD_HD uint32_t fbits(float f) {
 #ifdef __CUDA_ARCH__

@@ -160,9 +160,10 @@ __device__ bool should_create_pair(const DW& w, int a, int b) {
 // not already a contact.
 __device__ void emit_overlapping_pair(const DW& w, int a, int b) {
   int lo = a < b ? a : b, hi = a < b ? b : a;
-  if (!should_create_pair(w, lo, hi)) return;
+  // most overlapping pairs are existing contacts: test the pair set before the filters
   unsigned long long k = pair_key(lo, hi);
   if (hs_contains(w, k)) return;
+  if (!should_create_pair(w, lo, hi)) return;
   int slot = atomicAdd(&w.ctl->cand_count, 1);
   if (slot >= w.cand_cap) { raise_error(w.ctl, kErrCapacity); return; }
   w.cand[slot] = k;
@@ -267,6 +268,15 @@ __global__ void k_bp_segsort(DW w) {
   }
 }
 
+// Six pair kinds, A being the primary shape: sphere-sphere, capsule-sphere, capsule-capsule,
+// hull-sphere, hull-capsule, hull-hull.
+constexpr int kPairKinds = 6;
+__device__ __forceinline__ int pair_kind(int ta, int tb) {
+  if (ta == kSphere) return 0;
+  if (ta == kCapsule) return tb == kSphere ? 1 : 2;
+  return tb == kSphere ? 3 : (tb == kCapsule ? 4 : 5);
+}
+
 // contact_creation.rs:219 create_contact. Contact ids come from the LIFO id pool
 // (id_pool.rs): the k-th new pair in key order takes the k-th id popped.
 __global__ void k_bp_create(DW w) {
@@ -292,6 +302,7 @@ __global__ void k_bp_create(DW w) {
     c.body_a = A.body; c.body_b = B.body;
     c.enc_a = A.enc; c.enc_b = B.enc;
     c.color = -1; c.local = -1; c.alive = 1;
+    c.kind = pair_kind(A.type, B.type);
     const DSim& simA = sim_of(w, A.enc);
     const DSim& simB = sim_of(w, B.enc);
     uint32_t flags = 0;
@@ -409,85 +420,109 @@ __device__ bool update_contact(const DW& w, DContact& c, V3 lca, WXf xa, V3 lcb,
   return true;
 }
 
-__global__ void __launch_bounds__(128) k_collide(DW w) {
-  for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
-    if (!w.contacts[cid].alive) continue;
-    DContact c = w.contacts[cid];
-    bool changed = false;
-    if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
-      c.flags |= cSimDisjoint;
-      c.flags &= ~cSimTouching;
-      w.contacts[cid].flags = c.flags;
-      atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
-      continue;
-    }
-    const DSim& sa = sim_of(w, c.enc_a);
-    const DSim& sb = sim_of(w, c.enc_b);
-    bool was_touching = (c.flags & cSimTouching) != 0;
-    WXf xa, xb;
-    xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
-    xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
-    bool is_fast = ((sa.flags | sb.flags) & kIsFast) != 0;
-    float recycle = contact_recycle_distance();
-    float spec = speculative_distance();
-    float recycle_nt = minf(recycle, spec);
-    float tol = was_touching ? recycle : recycle_nt;
-    bool recycled = false;
-    if (!is_fast && recycle > 0.0f && (c.flags & cRelativeValid) && (c.flags & cRecycle)) {
-      // collide_pass.rs:606-687 contact recycling
-      float ang_a = dot_quat(xa.q, c.cached_rot_a);
-      float ang_b = dot_quat(xb.q, c.cached_rot_b);
-      float ang = minf(ang_a * ang_a, ang_b * ang_b);
-      Xf x = inv_mul_wxf(xa, xb);
-      Xf xc = c.cached_rel;
-      V3 mea = c.enc_a < -1 ? v3(0, 0, 0) : sa.max_extent;
-      V3 meb = c.enc_b < -1 ? v3(0, 0, 0) : sb.max_extent;
-      V3 me = max3(mea, meb);
-      float dsq = distance_sq(x.p, xc.p);
-      if (ang > kRecycleAngular && dsq < tol * tol) {
-        float dist = sqrtf(dsq);
-        float slack = tol - dist;
-        Q qr = inv_mul_quat(xc.q, x.q);
-        V3 arc = modified_cross(abs3(qr.v), me);
-        float arc_sq = 4.0f * length_sq(arc);
-        if (arc_sq < slack * slack) {
-          Q dqa = mul_quat(xa.q, conjugate(c.cached_rot_a));
-          Q dqb = mul_quat(xb.q, conjugate(c.cached_rot_b));
-          M3 ma = matrix_from_quat(dqa), mb = matrix_from_quat(dqb);
-          Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
-          V3 dc = sub_pos(cb, ca);
-          if (c.manifold_count > 0) {
-            Manifold& m = c.manifold;
-            V3 n = m.normal;
-            for (int i = 0; i < m.point_count; ++i) {
-              V3 ra = mul_mv(ma, m.points[i].anchor_a);
-              V3 rb = mul_mv(mb, m.points[i].anchor_b);
-              V3 dp = dc + (rb - ra);
-              m.points[i].separation = m.points[i].base_separation + dot(dp, n);
-              m.points[i].normal_velocity = 0.0f;
-              m.points[i].persisted = 1;
-            }
+// collide_pass.rs:541 collide_one_contact for one live contact, updated in place.
+__device__ void collide_one(const DW& w, int cid) {
+  DContact& c = w.contacts[cid];
+  if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
+    c.flags = (c.flags | cSimDisjoint) & ~cSimTouching;
+    atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+    return;
+  }
+  bool changed = false;
+  const DSim& sa = sim_of(w, c.enc_a);
+  const DSim& sb = sim_of(w, c.enc_b);
+  bool was_touching = (c.flags & cSimTouching) != 0;
+  WXf xa, xb;
+  xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
+  xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
+  bool is_fast = ((sa.flags | sb.flags) & kIsFast) != 0;
+  float recycle = contact_recycle_distance();
+  float spec = speculative_distance();
+  float recycle_nt = minf(recycle, spec);
+  float tol = was_touching ? recycle : recycle_nt;
+  bool recycled = false;
+  if (!is_fast && recycle > 0.0f && (c.flags & cRelativeValid) && (c.flags & cRecycle)) {
+    // collide_pass.rs:606-687 contact recycling
+    float ang_a = dot_quat(xa.q, c.cached_rot_a);
+    float ang_b = dot_quat(xb.q, c.cached_rot_b);
+    float ang = minf(ang_a * ang_a, ang_b * ang_b);
+    Xf x = inv_mul_wxf(xa, xb);
+    Xf xc = c.cached_rel;
+    V3 mea = c.enc_a < -1 ? v3(0, 0, 0) : sa.max_extent;
+    V3 meb = c.enc_b < -1 ? v3(0, 0, 0) : sb.max_extent;
+    V3 me = max3(mea, meb);
+    float dsq = distance_sq(x.p, xc.p);
+    if (ang > kRecycleAngular && dsq < tol * tol) {
+      float dist = sqrtf(dsq);
+      float slack = tol - dist;
+      Q qr = inv_mul_quat(xc.q, x.q);
+      V3 arc = modified_cross(abs3(qr.v), me);
+      float arc_sq = 4.0f * length_sq(arc);
+      if (arc_sq < slack * slack) {
+        Q dqa = mul_quat(xa.q, conjugate(c.cached_rot_a));
+        Q dqb = mul_quat(xb.q, conjugate(c.cached_rot_b));
+        M3 ma = matrix_from_quat(dqa), mb = matrix_from_quat(dqb);
+        Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+        V3 dc = sub_pos(cb, ca);
+        if (c.manifold_count > 0) {
+          Manifold& m = c.manifold;
+          V3 n = m.normal;
+          for (int i = 0; i < m.point_count; ++i) {
+            V3 ra = mul_mv(ma, m.points[i].anchor_a);
+            V3 rb = mul_mv(mb, m.points[i].anchor_b);
+            V3 dp = dc + (rb - ra);
+            m.points[i].separation = m.points[i].base_separation + dot(dp, n);
+            m.points[i].normal_velocity = 0.0f;
+            m.points[i].persisted = 1;
           }
-          recycled = true;
-          atomicAdd(&w.ctl->recycled, 1);
         }
+        recycled = true;
+        atomicAdd(&w.ctl->recycled, 1);
       }
     }
-    if (!recycled) {
-      c.cached_rot_a = xa.q;
-      c.cached_rot_b = xb.q;
-      c.cached_rel = inv_mul_wxf(xa, xb);
-      c.flags |= cRelativeValid;
-      bool touching = update_contact(w, c, sa.local_center, xa, sb.local_center, xb);
-      if (touching && !was_touching) { c.flags |= cSimStarted; changed = true; }
-      else if (!touching && was_touching) { c.flags |= cSimStopped; changed = true; }
-      if (touching && c.manifold_count > 0) {
-        for (int i = 0; i < c.manifold.point_count; ++i)
-          c.manifold.points[i].base_separation = c.manifold.points[i].separation;
-      }
+  }
+  if (!recycled) {
+    c.cached_rot_a = xa.q;
+    c.cached_rot_b = xb.q;
+    c.cached_rel = inv_mul_wxf(xa, xb);
+    c.flags |= cRelativeValid;
+    bool touching = update_contact(w, c, sa.local_center, xa, sb.local_center, xb);
+    if (touching && !was_touching) { c.flags |= cSimStarted; changed = true; }
+    else if (!touching && was_touching) { c.flags |= cSimStopped; changed = true; }
+    if (touching && c.manifold_count > 0) {
+      for (int i = 0; i < c.manifold.point_count; ++i)
+        c.manifold.points[i].base_separation = c.manifold.points[i].separation;
     }
-    w.contacts[cid] = c;
-    if (changed) atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+  }
+  if (changed) atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+}
+
+// Narrowphase over all contact slots. Each block takes a tile of slots, orders its live
+// contacts by pair kind in shared memory (a counting sort), and runs them in that order so
+// a warp mostly executes one shape combination. Contacts are independent here: the order
+// only changes which warp runs what.
+constexpr int kCollideThreads = 256;
+__global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
+  __shared__ int order[kCollideThreads];
+  __shared__ int bucket[kPairKinds + 1];
+  for (int base = blockIdx.x * kCollideThreads; base < w.cap; base += gridDim.x * kCollideThreads) {
+    int cid = base + threadIdx.x;
+    int kind = -1;
+    if (cid < w.cap && w.contacts[cid].alive) kind = w.contacts[cid].kind;
+    if (threadIdx.x <= kPairKinds) bucket[threadIdx.x] = 0;
+    __syncthreads();
+    int slot = kind >= 0 ? atomicAdd(&bucket[kind], 1) : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int k = 0; k < kPairKinds; ++k) { int n = bucket[k]; bucket[k] = acc; acc += n; }
+      bucket[kPairKinds] = acc;
+    }
+    __syncthreads();
+    if (kind >= 0) order[bucket[kind] + slot] = cid;
+    __syncthreads();
+    if (threadIdx.x < bucket[kPairKinds]) collide_one(w, order[threadIdx.x]);
+    __syncthreads();
   }
 }
 

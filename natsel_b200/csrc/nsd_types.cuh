@@ -84,6 +84,7 @@ struct alignas(16) DContact {
   int local;           // position in the overflow list (overflow color only)
   int manifold_count;
   int alive;
+  int kind;            // pair kind (shape type combination), fixed at creation
   float friction, restitution, rolling;
   V3 tangent_velocity;
   Q cached_rot_a, cached_rot_b;

@@ -234,6 +234,13 @@ def test_applied_forces_match_oracle():
         assert g.state_hash() == o.state_hash()
 
 
+def test_eager_path_matches_oracle(monkeypatch):
+    """Without a CUDA graph (the fallback when stream capture is refused) the step is the same."""
+    monkeypatch.setenv("NATSEL_EAGER", "1")
+    g, o = _both(lambda w: scenes.box_pyramid(w, base=8), steps=20)
+    assert g.phase_times().sum() > 0
+
+
 def test_contact_capacity_exceeded_is_reported():
     w = World(default_world_def(contact_capacity=1024))
     scenes.large_pyramid(w)  # about 15 000 contacts on the first step
