@@ -163,6 +163,21 @@ typedef struct {
 /* Synchronous; host arrays; runs on the calling thread's current CUDA device. */
 int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count);
 
+/* ns_collide_pairs for callers that must not allocate device memory (no counterpart in the
+ * reference). Some hosts cannot call cudaMalloc/cudaFree while they run: an engine whose device
+ * memory is fully reserved by its own pool allocator, or a frame loop that may not take the
+ * device-wide synchronisation those calls imply. This variant works in a fixed scratch area
+ * compiled into the library (about 1 MiB, held on every GPU that loads the library until the
+ * process exits) and so handles at most 4096 pairs per call; larger batches are rejected with
+ * NS_ERR_CAPACITY before any GPU work (split them into calls of 4096 or fewer). Inputs and
+ * outputs are the caller's host arrays, as for ns_collide_pairs, with identical results. The
+ * first call on a device looks up the scratch address there and makes the kernel's first
+ * launch on that device: make that first call before any stream capture. All calls on a device
+ * share the one scratch area, so calls that overlap on the GPU (from several host threads, for
+ * example) race; serialise them. Runs on the calling thread's current device and returns when
+ * the results are in the host arrays. */
+int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int count);
+
 /* Diagnostics (no counterpart in the reference): launches the solver's bounded grid barrier
  * waiting for one arrival that never comes, so every block gives up after timeout_ms
  * (1..2000). Returns NS_ERR_TIMEOUT when the wait expired and was reported as designed; the

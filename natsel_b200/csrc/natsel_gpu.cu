@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -681,6 +682,20 @@ int read_control(ns_world* w, Control* c) {
 
 }  // namespace
 
+// Fixed device scratch of ns_collide_pairs_noalloc: the device copies of one call's jobs
+// (first kNoAllocPairs * sizeof(PairJob) bytes) and results (the rest). Every GPU that loads
+// the library holds it until the process exits; all calls on a device share it.
+constexpr int kNoAllocPairs = 4096;
+constexpr size_t kNoAllocJobBytes = (size_t)kNoAllocPairs * sizeof(nsd::PairJob);
+static_assert(kNoAllocJobBytes % 256 == 0, "results must start 256-byte aligned");
+static __device__ __align__(256) unsigned char g_pair_scratch[kNoAllocJobBytes + (size_t)kNoAllocPairs * sizeof(nsd::PairResult)];
+
+// Device address of g_pair_scratch per device, looked up once with that device current (in
+// host code the symbol is only a host-side stand-in, never a device address).
+constexpr int kNoAllocMaxDevices = 64;
+static unsigned char* g_pair_scratch_addr[kNoAllocMaxDevices];
+static std::mutex g_pair_scratch_mutex;
+
 extern "C" {
 
 void ns_default_world_def(ns_world_def* d) {
@@ -1161,6 +1176,47 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count) {
   if (dj) cudaFree(dj);
   if (dr) cudaFree(dr);
   if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs: %s", cudaGetErrorString(e));
+  return NS_OK;
+}
+
+// See natsel_gpu.h: the batch narrowphase without any device allocation. The first call on a
+// device resolves the scratch address for that device (and is the first launch of the kernel
+// there); everything after that is two copies in, one launch and two copies out, all on the
+// legacy default stream, so each call has finished when it returns.
+int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int count) {
+  if (count < 0 || (count > 0 && (!jobs || !results))) return fail(nullptr, NS_ERR_INVALID, "invalid pair batch");
+  if (count > kNoAllocPairs)
+    return fail(nullptr, NS_ERR_CAPACITY, "ns_collide_pairs_noalloc: %d pairs exceed its fixed scratch of %d pairs",
+                count, kNoAllocPairs);
+  if (count == 0) return NS_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, NS_ERR_INVALID, "device %d out of range", dev);
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pair_scratch_mutex);
+    if (!g_pair_scratch_addr[dev]) {
+      e = cudaGetSymbolAddress((void**)&g_pair_scratch_addr[dev], g_pair_scratch);
+      if (e != cudaSuccess) {
+        g_pair_scratch_addr[dev] = nullptr;
+        return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc scratch address: %s", cudaGetErrorString(e));
+      }
+    }
+    base = g_pair_scratch_addr[dev];
+  }
+  // every slot below count is overwritten (jobs by the copy, results by the kernel), so nothing
+  // left from an earlier call is read
+  PairJob* dj = reinterpret_cast<PairJob*>(base);
+  PairResult* dr = reinterpret_cast<PairResult*>(base + kNoAllocJobBytes);
+  e = cudaMemcpy(dj, jobs, sizeof(PairJob) * (size_t)count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_collide_jobs<<<(count + 127) / 128, 128>>>(dj, dr, count);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(jobs, dj, sizeof(PairJob) * (size_t)count, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(results, dr, sizeof(PairResult) * (size_t)count, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc: %s", cudaGetErrorString(e));
   return NS_OK;
 }
 

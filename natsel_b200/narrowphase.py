@@ -47,3 +47,21 @@ def collide_pairs(jobs):
     if status != 0:
         raise NsError(status, lib.ns_last_error(None).decode())
     return results
+
+
+NOALLOC_MAX_PAIRS = 4096
+
+
+def collide_pairs_noalloc(jobs):
+    """Same as :func:`collide_pairs` through ``ns_collide_pairs_noalloc``, which allocates no
+    device memory (it works in a fixed scratch area inside the library) and therefore takes at
+    most NOALLOC_MAX_PAIRS jobs per call. For hosts that cannot call cudaMalloc while running."""
+    if jobs.dtype != PAIR_JOB_DTYPE or not jobs.flags.c_contiguous:
+        raise ValueError("jobs must be a C-contiguous PAIR_JOB_DTYPE array")
+    lib = load_library()
+    results = np.zeros(len(jobs), PAIR_RESULT_DTYPE)
+    status = lib.ns_collide_pairs_noalloc(jobs.ctypes.data_as(ctypes.c_void_p),
+                                          results.ctypes.data_as(ctypes.c_void_p), len(jobs))
+    if status != 0:
+        raise NsError(status, lib.ns_last_error(None).decode())
+    return results

@@ -84,7 +84,7 @@ EXPORTED = [
     "ns_create_revolute_joint", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
     "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
-    "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces",
+    "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
 ]
 
 
@@ -123,6 +123,7 @@ def load_library(path=LIB_PATH):
     lib.ns_world_stream.restype = P
     lib.ns_world_solver_counts.argtypes = [P, P]
     lib.ns_collide_pairs.argtypes = [P, P, ctypes.c_int]
+    lib.ns_collide_pairs_noalloc.argtypes = [P, P, ctypes.c_int]
     lib.ns_selftest_barrier_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.ns_world_apply_forces.argtypes = [P, P, P]
     _lib = lib
