@@ -44,6 +44,8 @@ WORKLOADS = {
                                      "1 500 capsules r U(0.15,0.4) hh U(0.2,0.8)) dropped from a 40x60x40 m volume "
                                      "onto a ground box; 60 Hz, 4 substeps, FP32"),
     "box_pyramid": ("box_pyramid", {}, "pyramid of 210 unit cubes (base 20) on a ground box; 60 Hz, 4 substeps, FP32"),
+    "large_pyramid": ("large_pyramid", {}, "the reference's large_pyramid benchmark scene (5 050 boxes resting from the "
+                                           "first step, scenes.rs:105); 60 Hz, 4 substeps, FP32"),
     "jointed_chains": ("jointed_chains", {}, "2 000 chains of 24 capsules on limited revolute joints + 4 000 boxes; "
                                              "60 Hz, 8 substeps, FP32"),
 }
@@ -94,16 +96,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of k_solve from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "k_solve_large_pile.md")
+def profiled_traffic(algorithmic_bytes):
+    """DRAM bytes per k_solve launch from the committed ncu capture (profiles/k_solve_large_pyramid.md,
+    a smaller contact-rich case), scaled to this run by algorithmic bytes; None without it."""
+    path = os.path.join(ROOT, "profiles", "k_solve_large_pyramid.md")
+    found = {}
     try:
         for line in open(path):
-            if line.strip().startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+            key, _, val = line.partition(":")
+            if key.strip() in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch") and val.strip():
+                found[key.strip()] = float(val.split()[0])
     except OSError:
-        pass
-    return None
+        return None
+    if len(found) < 2 or found["algorithmic_bytes_per_launch"] <= 0:
+        return None
+    return found["traffic_bytes_per_launch"] / found["algorithmic_bytes_per_launch"] * algorithmic_bytes
 
 
 # ---------------------------------------------------------------------------------------------
@@ -337,10 +344,12 @@ def run_natsel_arm(args):
     solve_ms = phase[:, 3]
     achieved = solve_bytes.sum() / (solve_ms.sum() / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(float(solve_bytes.mean()))
     roofline = {"kernel": "k_solve", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic, "algorithmic_bytes_per_launch": float(solve_bytes.mean()),
+                "traffic": traffic,
+                "traffic_source": "ncu capture of k_solve on large_pyramid (profiles/), scaled by algorithmic bytes",
+                "algorithmic_bytes_per_launch": float(solve_bytes.mean()),
                 "launch_ms": float(solve_ms.mean())}
 
     e2e = None
