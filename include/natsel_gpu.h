@@ -50,7 +50,9 @@ typedef struct {
   float joint_hertz;           /* 60 (JointDef default, joint_defs.rs:44) */
   float joint_damping_ratio;   /* 2 */
   int contact_capacity;        /* 0 = automatic (8 per shape + 4096) */
-  int solver_blocks;           /* CTAs in the solver's thread-block cluster, 0 = automatic (16 where available) */
+  int solver_blocks;           /* solver launch: 0 = automatic (one 16-CTA cluster on B200); 1..16 =
+                                  one thread-block cluster of that many CTAs; > 16 = cooperative grid
+                                  of that many blocks (capped at what fits co-resident) */
   int device;                  /* CUDA device ordinal */
 } ns_world_def;
 
@@ -135,7 +137,8 @@ void* ns_world_stream(ns_world* world);
  * [2] colored manifolds [3] colored points [4] colored static sides [5] joints
  * [6] overflow contacts [7] restitution on [8] gyroscopic bodies [9] overflow points
  * [10] overflow static sides [11] library kernel launches per step [12] library kernel
- * launches since creation; [13] CTAs in the solver cluster; [14..15] zero. */
+ * launches since creation; [13] blocks of the solver launch [14] 1 when that launch is a
+ * cooperative grid, 0 when it is one thread-block cluster; [15] zero. */
 int ns_world_solver_counts(ns_world* world, int64_t* counts16);
 
 /* Batch narrowphase (replaces the per-pair routines collide_hulls_with_scratch

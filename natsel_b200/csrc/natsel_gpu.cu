@@ -37,6 +37,7 @@ struct HostShape {
   DShape d;
   Hull hull;
   float density = 0;
+  float bound_radius = 0;  // radius about the shape's origin holding its local box in any rotation
 };
 
 template <class T>
@@ -69,7 +70,9 @@ struct ns_world {
   size_t cub_sort_bytes = 0;
   void* cub_scan_tmp = nullptr;
   size_t cub_scan_bytes = 0;
-  int solver_blocks = 1;           // CTAs in the solver cluster
+  int solver_blocks = 1;           // blocks of the solver launch
+  bool solver_grid = true;         // cooperative grid (true) or one thread-block cluster
+  int sort_bits = 32;              // key bits of the broadphase sort (bucket index + large flag)
   bool state_shared = false;
   size_t state_smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
@@ -296,6 +299,14 @@ int create_shape(ns_world* w, int bi, const ns_shape_def* def, HostShape hs) {
     margin = sqrtf(mx);
   }
   s.aabb_margin = minf(max_aabb_margin(), kAabbMarginFraction * margin);
+  if (s.type == kHull) {
+    // the tight box rotates the hull's local bounds about the shape origin
+    V3 lo = hs.hull.bounds.lo, hi = hs.hull.bounds.hi;
+    V3 far_corner = v3(maxf(absf(lo.x), absf(hi.x)), maxf(absf(lo.y), absf(hi.y)), maxf(absf(lo.z), absf(hi.z)));
+    hs.bound_radius = length(far_corner);
+  } else {
+    hs.bound_radius = margin;
+  }
   // shape_creation.rs:236 update_shape_aabbs
   const DSim& sim = sim_ref(w, b);
   float spec = speculative_distance();
@@ -336,7 +347,8 @@ int upload(ns_world* w, T* dst, const std::vector<T>& src) {
 int ensure_stack(ns_world* w) {
   size_t need = 0;
   cudaFuncAttributes a;
-  const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_jobs, (const void*)k_solve,
+  const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_jobs, (const void*)k_solve<true>,
+                           (const void*)k_solve<false>,
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
                            (const void*)k_finalize, (const void*)k_state_pass};
   for (const void* k : kernels) {
@@ -400,6 +412,32 @@ int upload_world(ns_world* w) {
   }
   d.n_large = (int)large.size();
   d.n_small = nsh - d.n_large;
+  // grid cell edge: a bound on every small proxy's fat-AABB extent on any axis. A moving shape's
+  // tight box lies within twice its bounding radius (the shape margin of
+  // shape_creation.rs:199), and finalize grows it by the speculative distance and the shape's
+  // AABB margin on each side; a static shape keeps its creation-time box.
+  {
+    float ext = 1e-3f;
+    for (int i = 0; i < nsh; ++i) {
+      const HostShape& h = w->shapes[i];
+      if (std::find(large.begin(), large.end(), i) != large.end()) continue;
+      float e;
+      if (h.d.is_static) {
+        const AABB& f = w->fat[i];
+        e = maxf(f.hi.x - f.lo.x, maxf(f.hi.y - f.lo.y, f.hi.z - f.lo.z));
+      } else {
+        e = 2.0f * h.bound_radius + 2.0f * (speculative_distance() + h.d.aabb_margin);
+      }
+      ext = maxf(ext, e);
+    }
+    d.cell = ext * 1.001f + 1e-3f;
+    d.inv_cell = 1.0f / d.cell;
+    int buckets = 1024;
+    while (buckets < 4 * std::max(d.n_small, 1)) buckets <<= 1;
+    d.cell_mask = buckets - 1;
+    w->sort_bits = 1;
+    while ((1u << w->sort_bits) <= (unsigned)buckets) ++w->sort_bits;
+  }
   // joint partner CSR (joint.rs:164: joints without collide_connected disable the pair)
   std::vector<int> joff(nb + 1, 0), jother;
   for (int i = 0; i < nb; ++i) {
@@ -430,6 +468,7 @@ int upload_world(ns_world* w) {
   ALLOC(bp_keys_in, uint32_t, nsh); ALLOC(bp_keys_out, uint32_t, nsh);
   ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
   ALLOC(bp_xy, float4, nsh); ALLOC(bp_z, float2, nsh); ALLOC(bp_meta, int, nsh);
+  ALLOC(cells, int2, (size_t)d.cell_mask + 1);
   ALLOC(large_list, int, large.size());
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
@@ -485,34 +524,44 @@ int upload_world(ns_world* w) {
   w->state_smem = w->state_shared ? need : stage_bytes;
   if (w->state_smem > 48 * 1024)
     NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
-  // solver: one thread-block cluster (non-portable sizes up to 16 CTAs where the device
-  // offers them); all of its CTAs are co-scheduled by the hardware. Each CTA carries two
-  // shared-memory constraint slots per thread for the prefetch pipeline.
+  // solver launch shape. solver_blocks 0: one cluster of the largest size that fits (16 CTAs on
+  // B200); 1..16: one thread-block cluster of that many CTAs (non-portable sizes above 8); above
+  // 16: a cooperative grid of that many blocks, capped at what fits co-resident. On the
+  // 10 000-body pile the 16-CTA cluster is about 4 % faster than grids of 32 to 148 blocks: a
+  // colour phase is bounded by one thread's latency chain, not by the number of SMs.
   {
-    NS_CUDA(w, cudaFuncSetAttribute(k_solve, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    NS_CUDA(w, cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem));
     int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : kMaxSolveCluster;
-    want = std::max(1, std::min(want, kMaxSolveCluster));
-    int best = 0;
-    for (int cs = want; cs >= 1; --cs) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.blockDim = dim3(kSolveThreads);
-      cfg.gridDim = dim3(cs);
-      cfg.dynamicSmemBytes = kSolveSmem;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = cs;
-      attr[0].val.clusterDim.y = 1;
-      attr[0].val.clusterDim.z = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      int clusters = 0;
-      cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, k_solve, &cfg);
-      if (e == cudaSuccess && clusters >= 1) { best = cs; break; }
-      cudaGetLastError();
+    if (want >= 1 && want <= kMaxSolveCluster) {
+      NS_CUDA(w, cudaFuncSetAttribute(k_solve<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      int best = 0;
+      for (int cs = want; cs >= 1; --cs) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.blockDim = dim3(kSolveThreads);
+        cfg.gridDim = dim3(cs);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, k_solve<false>, &cfg);
+        if (e == cudaSuccess && clusters >= 1) { best = cs; break; }
+        cudaGetLastError();
+      }
+      if (best == 0) return fail(w, NS_ERR_CUDA, "the solver cluster does not fit on this device");
+      w->solver_blocks = best;
+      w->solver_grid = false;
+    } else {
+      int per_sm = 0;
+      NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true>, kSolveThreads, 0));
+      int max_blocks = per_sm * w->sm_count;
+      if (max_blocks < 1) return fail(w, NS_ERR_CUDA, "the solver block does not fit on this device");
+      int blocks_ = std::min(want, max_blocks);
+      w->solver_blocks = blocks_;
+      w->solver_grid = true;
     }
-    if (best == 0) return fail(w, NS_ERR_CUDA, "the solver cluster does not fit on this device");
-    w->solver_blocks = best;
   }
   // readback staging (64 B per body) and the body location table
   {
@@ -552,7 +601,8 @@ int enqueue_pair_update(ns_world* w) {
   k_hs_rebuild_insert<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
   k_bp_keys<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   NS_CUDA(w, cub::DeviceRadixSort::SortPairs(w->cub_sort_tmp, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
-                                              d.bp_vals_in, d.bp_vals_out, nsh, 0, 32, s));
+                                              d.bp_vals_in, d.bp_vals_out, nsh, 0, w->sort_bits, s));
+  NS_CUDA(w, cudaMemsetAsync(d.cells, 0, sizeof(int2) * ((size_t)d.cell_mask + 1), s));
   k_bp_gather<<<blocks(d.n_small, 256), 256, 0, s>>>(d); ++nk;
   k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d); ++nk;
   k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
@@ -619,16 +669,22 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(w->solver_blocks);
     cfg.blockDim = dim3(kSolveThreads);
-    cfg.dynamicSmemBytes = kSolveSmem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = w->solver_blocks;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
+    if (w->solver_grid) {
+      NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+    } else {
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = w->solver_blocks;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+    }
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve, d, p, w->jr));
+    if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<true>, d, p, w->jr));
+    else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<false>, d, p, w->jr));
     ++nk;
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, ev_flags));
@@ -1124,6 +1180,7 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   out[11] = w->step_kernels;
   out[12] = w->kernel_launches;
   out[13] = w->solver_blocks;
+  out[14] = w->solver_grid ? 1 : 0;
   if (!w->uploaded) return NS_OK;
   Control c;
   int st = read_control(w, &c);

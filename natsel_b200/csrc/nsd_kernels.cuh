@@ -37,8 +37,11 @@ struct DW {
   DJoint* joints; int n_joints; int* joint_list;
   // broadphase scratch
   uint32_t* bp_keys_in; uint32_t* bp_keys_out; int* bp_vals_in; int* bp_vals_out;
-  // small proxies in sorted lo.x order: (lo.x, hi.x, lo.y, hi.y), (lo.z, hi.z), shape id | flags
+  // small proxies sorted by grid cell: (lo.x, hi.x, lo.y, hi.y), (lo.z, hi.z), shape id | flags
   float4* bp_xy; float2* bp_z; int* bp_meta;
+  // uniform grid over small proxies: cell edge >= every small proxy's extent; cells hashed into
+  // cell_mask + 1 buckets holding [first, end) ranges of the sorted proxies
+  float cell, inv_cell; int cell_mask; int2* cells;
   int n_small; int* large_list; int n_large;
   int* seg_count; int* seg_off; int* seg_cursor;
   unsigned long long* cand; unsigned long long* sorted_keys; int cand_cap;
@@ -128,6 +131,14 @@ __global__ void k_hs_rebuild_insert(DW w) {
   }
 }
 
+// Grid cell of a coordinate (monotone in x, so order-preserving comparisons stay valid).
+__device__ __forceinline__ int grid_coord(float x, float inv_cell) { return __float2int_rd(x * inv_cell); }
+__device__ __forceinline__ uint32_t cell_hash(int cx, int cy, int cz) {
+  return ((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^ ((uint32_t)cz * 83492791u);
+}
+
+// Sort keys: the hashed grid cell of each small proxy's lower corner; large static proxies
+// (the ground) sort after all of them and are paired by k_bp_large.
 __global__ void k_bp_keys(DW w) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n_shapes) return;
@@ -135,9 +146,12 @@ __global__ void k_bp_keys(DW w) {
   AABB f = w.fat[i];
   float width = f.hi.x - f.lo.x;
   bool large = s.is_static && width > 8.0f;
-  w.bp_keys_in[i] = large ? 0xffffffffu : float_sort_key(f.lo.x);
+  uint32_t key = (uint32_t)w.cell_mask + 1u;
+  if (!large)
+    key = cell_hash(grid_coord(f.lo.x, w.inv_cell), grid_coord(f.lo.y, w.inv_cell), grid_coord(f.lo.z, w.inv_cell)) &
+          (uint32_t)w.cell_mask;
+  w.bp_keys_in[i] = key;
   w.bp_vals_in[i] = i;
-  if (!large) atomicMax(&w.ctl->max_width_bits, __float_as_int(fmaxf(width, 0.0f)));
 }
 
 // contact_creation.rs:151 should_create_pair for the filters this path supports
@@ -179,7 +193,8 @@ constexpr int kMetaMoved = 1 << 30;
 constexpr int kMetaStatic = 1 << 29;
 constexpr int kMetaId = (1 << 29) - 1;
 
-// Sorted small proxies as contiguous arrays, so the sweep below reads neighbouring memory.
+// Sorted small proxies as contiguous arrays, and each occupied bucket's [first, end) range
+// (the bucket table is zeroed before this kernel).
 __global__ void k_bp_gather(DW w) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= w.n_small) return;
@@ -188,13 +203,28 @@ __global__ void k_bp_gather(DW w) {
   w.bp_xy[j] = make_float4(f.lo.x, f.hi.x, f.lo.y, f.hi.y);
   w.bp_z[j] = make_float2(f.lo.z, f.hi.z);
   w.bp_meta[j] = b | (w.moved[b] ? kMetaMoved : 0) | (w.shapes[b].is_static ? kMetaStatic : 0);
+  uint32_t key = w.bp_keys_out[j];
+  if (j == 0 || w.bp_keys_out[j - 1] != key) w.cells[key].x = j;
+  if (j == w.n_small - 1 || w.bp_keys_out[j + 1] != key) w.cells[key].y = j + 1;
 }
 
-// dynamic_tree.rs query of each moved proxy (contact_creation.rs:1000 find_pairs), as a
-// sort-and-sweep over lo.x: every proxy whose fat AABB can overlap proxy m in x lies in the
-// sorted window [lo.x(m) - widest proxy, hi.x(m)], walked outwards from m's own slot.
-// Each overlapping pair with at least one moved proxy is reported once (by the smaller
-// moved shape id when both moved).
+// Cell range [lo, hi] of one axis, at most three cells: every proxy that can overlap a box
+// with bounds [lo, hi] has its own lower bound in [lo - extent, hi], and extents stay below
+// cell / 1.001, so rounding lo - cell cannot exclude one. Non-finite bounds give a clamped
+// range instead of a runaway loop.
+__device__ __forceinline__ void axis_cells(float lo, float hi, const DW& w, int* c0, int* c1) {
+  int a = grid_coord(lo - w.cell, w.inv_cell);
+  int b = grid_coord(hi, w.inv_cell);
+  if (b - a > 2 || b < a) b = a + 2;
+  *c0 = a;
+  *c1 = b;
+}
+
+// contact_creation.rs:1000 find_pairs for each moved proxy (the reference queries its dynamic
+// trees; the set of pairs is the same): every small proxy whose fat AABB overlaps the moved
+// proxy's lies in the grid cells around it. Each overlapping pair with at least one moved
+// proxy is reported once (by the smaller moved shape id when both moved); a proxy met again
+// through a hash collision is skipped by checking its own cell.
 __global__ void k_bp_query(DW w) {
   if (w.ctl->moved_count == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -205,28 +235,31 @@ __global__ void k_bp_query(DW w) {
   bool m_static = (mm & kMetaStatic) != 0;
   float4 A = w.bp_xy[i];
   float2 Az = w.bp_z[i];
-  float max_w = __int_as_float(w.ctl->max_width_bits);
-  float start_x = A.x - (max_w * 1.001f + 1e-3f);
-  auto visit = [&](int j) {
-    int bm = w.bp_meta[j];
-    int b = bm & kMetaId;
-    if ((bm & kMetaMoved) && b < m) return;  // the smaller moved proxy of a pair reports it
-    if (m_static && (bm & kMetaStatic)) return;
-    float4 B = w.bp_xy[j];
-    if (A.y < B.x || A.x > B.y) return;  // aabb_overlaps (collision/aabb.rs:903), axis by axis
-    if (A.w < B.z || A.z > B.w) return;
-    float2 Bz = w.bp_z[j];
-    if (Az.y < Bz.x || Az.x > Bz.y) return;
-    emit_overlapping_pair(w, m, b);
-  };
-  for (int j = i + 1; j < w.n_small; ++j) {
-    if (w.bp_xy[j].x > A.y) break;
-    visit(j);
-  }
-  for (int j = i - 1; j >= 0; --j) {
-    if (w.bp_xy[j].x < start_x) break;
-    visit(j);
-  }
+  int x0, x1, y0, y1, z0, z1;
+  axis_cells(A.x, A.y, w, &x0, &x1);
+  axis_cells(A.z, A.w, w, &y0, &y1);
+  axis_cells(Az.x, Az.y, w, &z0, &z1);
+  for (int cx = x0; cx <= x1; ++cx)
+    for (int cy = y0; cy <= y1; ++cy)
+      for (int cz = z0; cz <= z1; ++cz) {
+        int2 r = w.cells[cell_hash(cx, cy, cz) & (uint32_t)w.cell_mask];
+        for (int j = r.x; j < r.y; ++j) {
+          if (j == i) continue;
+          int bm = w.bp_meta[j];
+          int b = bm & kMetaId;
+          if ((bm & kMetaMoved) && b < m) continue;  // the smaller moved proxy of a pair reports it
+          if (m_static && (bm & kMetaStatic)) continue;
+          float4 B = w.bp_xy[j];
+          if (A.y < B.x || A.x > B.y) continue;  // aabb_overlaps (collision/aabb.rs:903), axis by axis
+          if (A.w < B.z || A.z > B.w) continue;
+          float2 Bz = w.bp_z[j];
+          if (Az.y < Bz.x || Az.x > Bz.y) continue;
+          if (grid_coord(B.x, w.inv_cell) != cx || grid_coord(B.z, w.inv_cell) != cy ||
+              grid_coord(Bz.x, w.inv_cell) != cz)
+            continue;
+          emit_overlapping_pair(w, m, b);
+        }
+      }
 }
 
 __global__ void k_bp_large(DW w) {

@@ -1,12 +1,13 @@
 // Persistent colored solver (solver_stages.rs:543 solve_constraint_stages) and body
 // finalization (solver_integration.rs:587 finalize_body_range).
 //
-// One thread-block cluster runs every substep: integrate velocities, then per stage
-// (warm start, push, relax) the overflow color on one thread followed by colors
-// 0..22, each color one cluster-wide phase separated by the hardware cluster barrier;
-// then restitution and impulse storage. Every CTA takes the same path through the
-// phases (the loop bounds are read identically by all of them), so every CTA reaches
-// every barrier; colors with no work are skipped by all CTAs alike.
+// One persistent launch runs every substep: integrate velocities, then per stage (warm
+// start, push, relax) the overflow color on one thread followed by colors 0..22, each color
+// one phase separated by a barrier over the whole launch (a grid-wide barrier for a
+// cooperative launch over the GPU, or the hardware barrier of one thread-block cluster);
+// then restitution and impulse storage. Every block takes the same path through the phases
+// (the loop bounds are read identically by all of them), so every block reaches every
+// barrier; colors with no work are skipped by all blocks alike.
 #pragma once
 #include "nsd_kernels.cuh"
 
@@ -62,6 +63,47 @@ __global__ void k_barrier_selftest(Control* ctl, unsigned long long limit_ns) {
 // the cluster before the barrier are visible to every thread of the cluster after it.
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Grid-wide barrier of the cooperative solver launch: thread 0 of each block adds its arrival
+// with release semantics and polls the counter with acquire loads; the block's other threads
+// are ordered by __syncthreads on both sides. Barrier k completes at (k + 1) * gridDim.x
+// arrivals (the counter is zeroed before each launch). The wait is bounded: after 2 s, 2^26
+// polls or another block's error it raises NS_ERR_TIMEOUT and returns false, and every block
+// then leaves the kernel at its next barrier.
+__device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int target = (index + 1) * (int)gridDim.x;
+    int* cnt = &ctl->barrier_count;
+    asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(cnt) : "memory");
+    int ok = 1;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (long long spins = 1;; ++spins) {
+      int v;
+      asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+      if (v >= target) break;
+      if ((spins & 255) == 0) {
+        unsigned long long t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        if (*((volatile int*)&ctl->error) != 0 || t1 - t0 > 2000000000ull || spins > (1ll << 26)) { ok = 0; break; }
+      }
+    }
+    if (!ok) atomicCAS(&ctl->error, 0, kErrTimeout);
+    ok_s = ok;
+  }
+  __syncthreads();
+  index++;
+  return ok_s != 0;
+}
+
+template <bool kGrid>
+__device__ __forceinline__ bool phase_sync(Control* ctl, int& index) {
+  if (kGrid) return grid_sync_acq_rel(ctl, index);
+  cluster_sync_all();
+  return true;
 }
 
 __device__ __forceinline__ void store_state_vw(const DW& w, int i, const DState& s) {
@@ -922,8 +964,10 @@ __device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges
 
 // Phase codes: contact phases stage * 32 + color; the rest as below.
 constexpr int kPhaseIntegrateVelocity = 1000, kPhaseIntegratePosition = 1001, kPhaseOverflow = 2000;
-constexpr size_t kSolveSmem = 0;
 
+// Persistent solver. kGrid: one cooperative launch over the whole GPU, phases separated by
+// grid_sync_acq_rel; otherwise one thread-block cluster separated by barrier.cluster.
+template <bool kGrid>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, JointRanges jr) {
   __shared__ int coff[25];
   __shared__ int phases[3 * 25 + 2];  // one substep
@@ -959,6 +1003,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
   auto phase_at = [&](int s) { return s < main_phases ? phases[s % n_ph] : rphases[(s - main_phases) % n_rph]; };
   const int stride = gridDim.x * blockDim.x;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
     if (ph == kPhaseIntegrateVelocity) {
@@ -984,7 +1029,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
         }
       }
     }
-    cluster_sync_all();
+    if (!phase_sync<kGrid>(w.ctl, bar)) return;
   }
   // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
   if (g == 0) store_overflow(w, n_ovf);

@@ -234,6 +234,18 @@ def test_applied_forces_match_oracle():
         assert g.state_hash() == o.state_hash()
 
 
+@pytest.mark.parametrize("solver_blocks", [64, 4])
+def test_solver_launch_shapes_match_oracle(solver_blocks):
+    """A cooperative grid of 64 blocks and a cluster of 4 CTAs give the same bits as the default."""
+    g, _ = gpu_world("large_pile", world_kw={"solver_blocks": solver_blocks}, n=3000, seed=4)
+    o, _ = oracle_world("large_pile", n=3000, seed=4)
+    for _ in range(40):
+        g.step(DT, 4)
+        o.step(DT, 4)
+    assert g.state_hash() == o.state_hash()
+    assert g.solver_counts()[14] == (1 if solver_blocks > 16 else 0)
+
+
 def test_eager_path_matches_oracle(monkeypatch):
     """Without a CUDA graph (the fallback when stream capture is refused) the step is the same."""
     monkeypatch.setenv("NATSEL_EAGER", "1")
