@@ -50,7 +50,8 @@ typedef struct {
   float joint_hertz;           /* 60 (JointDef default, joint_defs.rs:44) */
   float joint_damping_ratio;   /* 2 */
   int contact_capacity;        /* 0 = automatic (8 per shape + 4096) */
-  int solver_blocks;           /* solver launch: 0 = automatic (one 16-CTA cluster on B200); 1..16 =
+  int solver_blocks;           /* solver launch: 0 = automatic (one 16-CTA cluster on B200 for one
+                                  world, a grid over every SM for sub-worlds); 1..16 =
                                   one thread-block cluster of that many CTAs; > 16 = cooperative grid
                                   of that many blocks (capped at what fits co-resident) */
   int device;                  /* CUDA device ordinal */
@@ -95,6 +96,21 @@ int ns_create_revolute_joint(ns_world* world, int body_a, int body_b, const floa
                              const float frame_b[7], int enable_limit, float lower_angle,
                              float upper_angle, int enable_spring, float hertz, float damping_ratio,
                              float max_motor_torque, int collide_connected);
+
+/* Batched worlds (no counterpart in the reference, which steps one world at a time): a world
+ * can hold several independent sub-worlds that are stepped together by every ns_world_step.
+ * Sub-world 0 exists from creation; ns_world_begin_subworld starts the next one and returns
+ * its index (-1 after the first step). Bodies created afterwards belong to it, and shapes and
+ * joints can only be added to bodies of the newest sub-world, so each sub-world's bodies,
+ * shapes and joints have contiguous ids. Bodies of different sub-worlds never collide. Each
+ * sub-world keeps its own contact ids, colouring and overflow list, so its result is bit for
+ * bit the result of stepping it as a world of its own. */
+int ns_world_begin_subworld(ns_world* world);
+int ns_world_subworld_count(const ns_world* world);
+/* first_body[count + 1]: the first body id of each sub-world, then the total body count. */
+int ns_world_subworld_bodies(const ns_world* world, int* first_body);
+/* out[count]: world_state_hash of each sub-world's bodies (synchronises). */
+int ns_world_subworld_hashes(ns_world* world, uint64_t* out);
 
 /* Advance one step (replaces World::step solver_integration.rs:807). Asynchronous:
  * the step is enqueued on the world's stream; the first call uploads the scene. dt == 0

@@ -27,6 +27,7 @@ thread_local std::string g_create_error;
 
 struct HostBody {
   int type = 0, set = 0, local = 0;
+  int world = 0;            // sub-world
   uint32_t flags = 0;
   int joint_count = 0;
   float mass = 0;
@@ -95,6 +96,9 @@ struct ns_world {
   int pair_kernels = 0, step_kernels = 0;  // own kernel launches per pair update / full step
   int64_t kernel_launches = 0;
   int64_t n_gyroscopic = 0;
+  // sub-worlds: the first body and shape of each (bodies, shapes and joints are added to the
+  // newest sub-world only, so each sub-world's ids are contiguous)
+  std::vector<int> sub_body_begin = {0}, sub_shape_begin = {0};
 };
 
 namespace {
@@ -278,8 +282,11 @@ int create_shape(ns_world* w, int bi, const ns_shape_def* def, HostShape hs) {
   if (w->shapes.size() >= (1u << 22) - 1) return fail(w, -1, "at most 4194303 shapes per world"), -1;
   int sid = (int)w->shapes.size();
   HostBody& b = w->bodies[bi];
+  if (b.world != (int)w->sub_body_begin.size() - 1)
+    return fail(w, -1, "shapes can only be added to bodies of the newest sub-world"), -1;
   DShape& s = hs.d;
   s.body = bi;
+  s.world = b.world;
   s.enc = encode(b);
   s.is_static = b.type == NS_STATIC_BODY;
   hs.density = def->density;
@@ -382,9 +389,27 @@ int upload_world(ns_world* w) {
   int na = (int)w->asims.size(), ns = (int)w->ssims.size(), nsh = (int)w->shapes.size();
   int nb = (int)w->bodies.size(), nj = (int)w->joints.size();
   d.n_awake = na; d.n_static = ns; d.n_shapes = nsh; d.n_bodies = nb; d.n_joints = nj;
-  int cap = w->def.contact_capacity > 0 ? w->def.contact_capacity : 8 * nsh + 4096;
-  cap = (cap + 1023) & ~1023;
+  // contact id ranges: one world keeps the reference-sized capacity; each sub-world of a batch
+  // gets 12 contacts per shape + 64 (or contact_capacity), a multiple of 32 so its changed
+  // bits fill whole words; the last range is padded to a multiple of 1024
+  int n_worlds = (int)w->sub_body_begin.size();
+  std::vector<int> world_shape(w->sub_shape_begin), world_cbase(n_worlds + 1, 0);
+  world_shape.push_back(nsh);
+  int cap;
+  if (n_worlds == 1) {
+    cap = w->def.contact_capacity > 0 ? w->def.contact_capacity : 8 * nsh + 4096;
+    cap = (cap + 1023) & ~1023;
+  } else {
+    for (int k = 0; k < n_worlds; ++k) {
+      int ns_k = world_shape[k + 1] - world_shape[k];
+      int c = w->def.contact_capacity > 0 ? w->def.contact_capacity : 12 * ns_k + 64;
+      world_cbase[k + 1] = world_cbase[k] + ((c + 31) & ~31);
+    }
+    cap = (world_cbase[n_worlds] + 1023) & ~1023;
+  }
+  world_cbase[n_worlds] = cap;
   d.cap = cap;
+  d.n_worlds = n_worlds;
   int hs_size = 1;
   while (hs_size < 4 * cap) hs_size <<= 1;
   d.hs_mask = hs_size - 1;
@@ -412,6 +437,9 @@ int upload_world(ns_world* w) {
   }
   d.n_large = (int)large.size();
   d.n_small = nsh - d.n_large;
+  std::vector<int> large_off(n_worlds + 1, 0);
+  for (int i : large) large_off[dshapes[i].world + 1]++;
+  for (int k = 0; k < n_worlds; ++k) large_off[k + 1] += large_off[k];
   // grid cell edge: a bound on every small proxy's fat-AABB extent on any axis. A moving shape's
   // tight box lies within twice its bounding radius (the shape margin of
   // shape_creation.rs:199), and finalize grows it by the speculative distance and the shape's
@@ -468,7 +496,10 @@ int upload_world(ns_world* w) {
   ALLOC(bp_keys_in, uint32_t, nsh); ALLOC(bp_keys_out, uint32_t, nsh);
   ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
   ALLOC(bp_xy, float4, nsh); ALLOC(bp_z, float2, nsh); ALLOC(bp_meta, int, nsh);
-  ALLOC(cells, int2, (size_t)d.cell_mask + 1);
+  ALLOC(cells, int2, (size_t)d.cell_mask + 1); ALLOC(bp_world, int, nsh);
+  ALLOC(world_cbase, int, n_worlds + 1); ALLOC(world_shape, int, n_worlds + 1);
+  ALLOC(pool_top, int, n_worlds); ALLOC(pool_next, int, n_worlds); ALLOC(ovf_count, int, n_worlds);
+  ALLOC(large_off, int, n_worlds + 1);
   ALLOC(large_list, int, large.size());
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
@@ -496,6 +527,15 @@ int upload_world(ns_world* w) {
   if ((st = upload(w, d.body_joint_off, joff))) return st;
   if ((st = upload(w, d.body_joint_other, jother))) return st;
   if ((st = upload(w, d.large_list, large))) return st;
+  if ((st = upload(w, d.world_cbase, world_cbase))) return st;
+  if ((st = upload(w, d.world_shape, world_shape))) return st;
+  if ((st = upload(w, d.large_off, large_off))) return st;
+  {
+    std::vector<int> zeros(n_worlds, 0);
+    if ((st = upload(w, d.pool_top, zeros))) return st;
+    if ((st = upload(w, d.pool_next, zeros))) return st;
+    if ((st = upload(w, d.ovf_count, zeros))) return st;
+  }
   if ((st = upload(w, d.joint_list, jlist))) return st;
   std::vector<DJoint> dj = w->joints;
   if ((st = upload(w, d.joints, dj))) return st;
@@ -525,12 +565,14 @@ int upload_world(ns_world* w) {
   if (w->state_smem > 48 * 1024)
     NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
   // solver launch shape. solver_blocks 0: one cluster of the largest size that fits (16 CTAs on
-  // B200); 1..16: one thread-block cluster of that many CTAs (non-portable sizes above 8); above
+  // B200) for a single world, a cooperative grid over every SM for a batch of sub-worlds; 1..16: one thread-block cluster of that many CTAs (non-portable sizes above 8); above
   // 16: a cooperative grid of that many blocks, capped at what fits co-resident. On the
   // 10 000-body pile the 16-CTA cluster is about 4 % faster than grids of 32 to 148 blocks: a
   // colour phase is bounded by one thread's latency chain, not by the number of SMs.
   {
-    int want = w->def.solver_blocks > 0 ? w->def.solver_blocks : kMaxSolveCluster;
+    // a batch of sub-worlds has many constraints per colour phase: spread it over every SM
+    int want = w->def.solver_blocks > 0 ? w->def.solver_blocks
+               : (n_worlds > 1 ? std::max(w->sm_count, kMaxSolveCluster + 1) : kMaxSolveCluster);
     if (want >= 1 && want <= kMaxSolveCluster) {
       NS_CUDA(w, cudaFuncSetAttribute(k_solve<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
       int best = 0;
@@ -610,6 +652,7 @@ int enqueue_pair_update(ns_world* w) {
   k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
   k_bp_segsort<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   k_bp_create<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  k_bp_pools<<<blocks(d.n_worlds, 256), 256, 0, s>>>(d); ++nk;
   k_bp_finish<<<1, 1, 0, s>>>(d); ++nk;
   NS_CUDA(w, cudaMemsetAsync(d.moved, 0, sizeof(int) * (size_t)nsh, s));
   w->pair_kernels = nk;
@@ -654,11 +697,18 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   k_collide<<<blocks(d.cap, kCollideThreads), kCollideThreads, 0, s>>>(d); ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
-  k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0); ++nk;
+  if (d.n_worlds == 1) {
+    k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0); ++nk;
+  } else {
+    NS_CUDA(w, cudaMemsetAsync(&d.ctl->changed_count, 0, sizeof(int), s));
+    NS_CUDA(w, cudaMemsetAsync(&d.ctl->overflow_count, 0, sizeof(int), s));
+    k_state_worlds<<<blocks(d.n_worlds, 128), 128, 0, s>>>(d); ++nk;
+    k_state_finish<<<1, 1, 0, s>>>(d); ++nk;
+  }
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
   k_color_scan<<<1, 32, 0, s>>>(d); ++nk;
   k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p); ++nk;
-  k_prepare_overflow<<<8, 128, 0, s>>>(d, p); ++nk;
+  k_prepare_overflow<<<std::min(std::max(d.n_worlds, 8), 4096), 128, 0, s>>>(d, p); ++nk;
   if (d.n_joints > 0) {
     k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
     ++nk;
@@ -842,6 +892,7 @@ int ns_create_body(ns_world* w, const ns_body_def* d) {
     b.local = (int)w->ssims.size();
     w->ssims.push_back(s);
   }
+  b.world = (int)w->sub_body_begin.size() - 1;
   w->bodies.push_back(b);
   w->body_mask.push_back(0u);
   return id;
@@ -895,9 +946,14 @@ int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa
   HostBody& ba = w->bodies[body_a];
   HostBody& bb = w->bodies[body_b];
   if (ba.type != NS_DYNAMIC_BODY && bb.type != NS_DYNAMIC_BODY) { w->err = "a joint needs a dynamic body"; return -1; }
+  if (ba.world != bb.world || ba.world != (int)w->sub_body_begin.size() - 1) {
+    w->err = "joint bodies must belong to the newest sub-world";
+    return -1;
+  }
   DJoint j;
   memset(&j, 0, sizeof(j));
   j.body_a = body_a; j.body_b = body_b;
+  j.world = ba.world;
   j.enc_a = encode(ba); j.enc_b = encode(bb);
   j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
   j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
@@ -1071,18 +1127,14 @@ int ns_world_get_bodies(ns_world* w, double* pos, float* rot, float* lin, float*
   return NS_OK;
 }
 
-int ns_world_state_hash(ns_world* w, uint64_t* out) {
-  if (!w || !out) return NS_ERR_INVALID;
-  size_t n = w->bodies.size();
-  std::vector<double> pos(3 * n);
-  std::vector<float> rot(4 * n), lin(3 * n), ang(3 * n);
-  int st = ns_world_get_bodies(w, pos.data(), rot.data(), lin.data(), ang.data());
-  if (st) return st;
+// body_queries.rs:432 world_state_hash over the bodies [b0, b1) of host arrays
+static uint64_t state_hash_range(const ns_world* w, const double* pos, const float* rot, const float* lin,
+                                 const float* ang, size_t b0, size_t b1) {
   const uint64_t prime = 1099511628211ull;
   uint64_t h = 14695981039346656037ull;
   auto mixf = [&](float f) { uint32_t b; memcpy(&b, &f, 4); h = (h ^ (uint64_t)b) * prime; };
   auto mixd = [&](double d) { uint64_t b; memcpy(&b, &d, 8); h = (h ^ b) * prime; };
-  for (size_t i = 0; i < n; ++i) {
+  for (size_t i = b0; i < b1; ++i) {
     mixd(pos[3 * i]); mixd(pos[3 * i + 1]); mixd(pos[3 * i + 2]);
     mixf(rot[4 * i]); mixf(rot[4 * i + 1]); mixf(rot[4 * i + 2]); mixf(rot[4 * i + 3]);
     if (w->bodies[i].set == 2) {
@@ -1090,7 +1142,49 @@ int ns_world_state_hash(ns_world* w, uint64_t* out) {
       mixf(ang[3 * i]); mixf(ang[3 * i + 1]); mixf(ang[3 * i + 2]);
     }
   }
-  *out = h;
+  return h;
+}
+
+int ns_world_state_hash(ns_world* w, uint64_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  size_t n = w->bodies.size();
+  std::vector<double> pos(3 * n);
+  std::vector<float> rot(4 * n), lin(3 * n), ang(3 * n);
+  int st = ns_world_get_bodies(w, pos.data(), rot.data(), lin.data(), ang.data());
+  if (st) return st;
+  *out = state_hash_range(w, pos.data(), rot.data(), lin.data(), ang.data(), 0, n);
+  return NS_OK;
+}
+
+int ns_world_begin_subworld(ns_world* w) {
+  if (!w) return -1;
+  if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
+  w->sub_body_begin.push_back((int)w->bodies.size());
+  w->sub_shape_begin.push_back((int)w->shapes.size());
+  return (int)w->sub_body_begin.size() - 1;
+}
+
+int ns_world_subworld_count(const ns_world* w) { return w ? (int)w->sub_body_begin.size() : -1; }
+
+int ns_world_subworld_bodies(const ns_world* w, int* first_body) {
+  if (!w || !first_body) return NS_ERR_INVALID;
+  for (size_t k = 0; k < w->sub_body_begin.size(); ++k) first_body[k] = w->sub_body_begin[k];
+  first_body[w->sub_body_begin.size()] = (int)w->bodies.size();
+  return NS_OK;
+}
+
+int ns_world_subworld_hashes(ns_world* w, uint64_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  size_t n = w->bodies.size();
+  std::vector<double> pos(3 * n);
+  std::vector<float> rot(4 * n), lin(3 * n), ang(3 * n);
+  int st = ns_world_get_bodies(w, pos.data(), rot.data(), lin.data(), ang.data());
+  if (st) return st;
+  size_t nw = w->sub_body_begin.size();
+  for (size_t k = 0; k < nw; ++k) {
+    size_t b1 = k + 1 < nw ? (size_t)w->sub_body_begin[k + 1] : n;
+    out[k] = state_hash_range(w, pos.data(), rot.data(), lin.data(), ang.data(), (size_t)w->sub_body_begin[k], b1);
+  }
   return NS_OK;
 }
 
@@ -1200,11 +1294,18 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   out[6] = c.overflow_count;
   out[7] = c.any_restitution;
   if (c.overflow_count > 0) {
-    std::vector<DOverflow> ov(c.overflow_count);
-    NS_CUDA(w, cudaMemcpy(ov.data(), w->dw.ovf, sizeof(DOverflow) * ov.size(), cudaMemcpyDeviceToHost));
-    for (const DOverflow& o : ov) {
-      out[9] += o.manifold_count > 0 ? o.m.point_count : 0;
-      out[10] += (o.index_a < 0) + (o.index_b < 0);
+    int nw = w->dw.n_worlds;
+    std::vector<int> cnt(nw), base(nw + 1);
+    NS_CUDA(w, cudaMemcpy(cnt.data(), w->dw.ovf_count, sizeof(int) * nw, cudaMemcpyDeviceToHost));
+    NS_CUDA(w, cudaMemcpy(base.data(), w->dw.world_cbase, sizeof(int) * (nw + 1), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nw; ++k) {
+      if (cnt[k] == 0) continue;
+      std::vector<DOverflow> ov(cnt[k]);
+      NS_CUDA(w, cudaMemcpy(ov.data(), w->dw.ovf + base[k], sizeof(DOverflow) * ov.size(), cudaMemcpyDeviceToHost));
+      for (const DOverflow& o : ov) {
+        out[9] += o.manifold_count > 0 ? o.m.point_count : 0;
+        out[10] += (o.index_a < 0) + (o.index_b < 0);
+      }
     }
   }
   return NS_OK;

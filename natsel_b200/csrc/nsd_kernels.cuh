@@ -48,6 +48,15 @@ struct DW {
   int* block_color;                 // per color-partition block x 24
   int n_color_blocks;
   Control* ctl;
+  // Sub-worlds (independent worlds stepped together; one for a plain world). World w owns the
+  // shapes [world_shape[w], world_shape[w+1]), the contact ids [world_cbase[w],
+  // world_cbase[w+1]) (multiples of 32), a LIFO id pool on free_stack at world_cbase[w] with
+  // pool_top[w] free ids and pool_next[w] the next never-used local id, an overflow list at
+  // overflow_list + world_cbase[w] with ovf_count[w] entries, and the large static proxies
+  // large_list[large_off[w] .. large_off[w+1]).
+  int n_worlds;
+  int* world_cbase; int* world_shape; int* pool_top; int* pool_next; int* ovf_count; int* large_off;
+  int* bp_world;  // sub-world of each sorted small proxy
 };
 
 struct JointRanges { int off[25]; };
@@ -133,8 +142,9 @@ __global__ void k_hs_rebuild_insert(DW w) {
 
 // Grid cell of a coordinate (monotone in x, so order-preserving comparisons stay valid).
 __device__ __forceinline__ int grid_coord(float x, float inv_cell) { return __float2int_rd(x * inv_cell); }
-__device__ __forceinline__ uint32_t cell_hash(int cx, int cy, int cz) {
-  return ((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^ ((uint32_t)cz * 83492791u);
+__device__ __forceinline__ uint32_t cell_hash(int world, int cx, int cy, int cz) {
+  return ((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^ ((uint32_t)cz * 83492791u) ^
+         ((uint32_t)world * 2654435761u);
 }
 
 // Sort keys: the hashed grid cell of each small proxy's lower corner; large static proxies
@@ -148,8 +158,8 @@ __global__ void k_bp_keys(DW w) {
   bool large = s.is_static && width > 8.0f;
   uint32_t key = (uint32_t)w.cell_mask + 1u;
   if (!large)
-    key = cell_hash(grid_coord(f.lo.x, w.inv_cell), grid_coord(f.lo.y, w.inv_cell), grid_coord(f.lo.z, w.inv_cell)) &
-          (uint32_t)w.cell_mask;
+    key = cell_hash(s.world, grid_coord(f.lo.x, w.inv_cell), grid_coord(f.lo.y, w.inv_cell),
+                    grid_coord(f.lo.z, w.inv_cell)) & (uint32_t)w.cell_mask;
   w.bp_keys_in[i] = key;
   w.bp_vals_in[i] = i;
 }
@@ -203,6 +213,7 @@ __global__ void k_bp_gather(DW w) {
   w.bp_xy[j] = make_float4(f.lo.x, f.hi.x, f.lo.y, f.hi.y);
   w.bp_z[j] = make_float2(f.lo.z, f.hi.z);
   w.bp_meta[j] = b | (w.moved[b] ? kMetaMoved : 0) | (w.shapes[b].is_static ? kMetaStatic : 0);
+  w.bp_world[j] = w.shapes[b].world;
   uint32_t key = w.bp_keys_out[j];
   if (j == 0 || w.bp_keys_out[j - 1] != key) w.cells[key].x = j;
   if (j == w.n_small - 1 || w.bp_keys_out[j + 1] != key) w.cells[key].y = j + 1;
@@ -224,7 +235,8 @@ __device__ __forceinline__ void axis_cells(float lo, float hi, const DW& w, int*
 // trees; the set of pairs is the same): every small proxy whose fat AABB overlaps the moved
 // proxy's lies in the grid cells around it. Each overlapping pair with at least one moved
 // proxy is reported once (by the smaller moved shape id when both moved); a proxy met again
-// through a hash collision is skipped by checking its own cell.
+// through a hash collision is skipped by checking its own cell and sub-world (proxies of
+// different sub-worlds never pair).
 __global__ void k_bp_query(DW w) {
   if (w.ctl->moved_count == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -233,6 +245,7 @@ __global__ void k_bp_query(DW w) {
   if (!(mm & kMetaMoved)) return;
   int m = mm & kMetaId;
   bool m_static = (mm & kMetaStatic) != 0;
+  int mw = w.bp_world[i];
   float4 A = w.bp_xy[i];
   float2 Az = w.bp_z[i];
   int x0, x1, y0, y1, z0, z1;
@@ -242,7 +255,7 @@ __global__ void k_bp_query(DW w) {
   for (int cx = x0; cx <= x1; ++cx)
     for (int cy = y0; cy <= y1; ++cy)
       for (int cz = z0; cz <= z1; ++cz) {
-        int2 r = w.cells[cell_hash(cx, cy, cz) & (uint32_t)w.cell_mask];
+        int2 r = w.cells[cell_hash(mw, cx, cy, cz) & (uint32_t)w.cell_mask];
         for (int j = r.x; j < r.y; ++j) {
           if (j == i) continue;
           int bm = w.bp_meta[j];
@@ -255,7 +268,7 @@ __global__ void k_bp_query(DW w) {
           float2 Bz = w.bp_z[j];
           if (Az.y < Bz.x || Az.x > Bz.y) continue;
           if (grid_coord(B.x, w.inv_cell) != cx || grid_coord(B.z, w.inv_cell) != cy ||
-              grid_coord(Bz.x, w.inv_cell) != cz)
+              grid_coord(Bz.x, w.inv_cell) != cz || w.bp_world[j] != mw)
             continue;
           emit_overlapping_pair(w, m, b);
         }
@@ -269,7 +282,7 @@ __global__ void k_bp_large(DW w) {
   const DShape& S = w.shapes[s];
   if (S.is_static && (w.fat[s].hi.x - w.fat[s].lo.x) > 8.0f) return;  // large itself
   if (S.is_static) return;                                             // static vs static
-  for (int k = 0; k < w.n_large; ++k) {
+  for (int k = w.large_off[S.world]; k < w.large_off[S.world + 1]; ++k) {
     int L = w.large_list[k];
     if (!w.moved[s] && !w.moved[L]) continue;
     emit_pair(w, s, L);
@@ -312,14 +325,30 @@ __device__ __forceinline__ int pair_kind(int ta, int tb) {
 
 // contact_creation.rs:219 create_contact. Contact ids come from the LIFO id pool
 // (id_pool.rs): the k-th new pair in key order takes the k-th id popped.
+// First sorted candidate whose smaller shape is >= shape (candidate keys sort by that shape).
+__device__ int first_candidate_of_shape(const DW& w, int n, int shape) {
+  unsigned long long v = (unsigned long long)shape << 42;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (w.sorted_keys[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
 __global__ void k_bp_create(DW w) {
   int n = w.ctl->cand_count;
   if (n > w.cand_cap) n = w.cand_cap;
-  int F = w.ctl->pool_top, N0 = w.ctl->pool_next;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    int id = k < F ? w.free_stack[F - 1 - k] : N0 + (k - F);
-    if (id >= w.cap) { raise_error(w.ctl, kErrCapacity); continue; }
     unsigned long long key = w.sorted_keys[k];
+    int wi = w.shapes[(int)((key >> 42) & ((1ull << 22) - 1ull))].world;
+    // the pair's rank among its sub-world's new pairs decides which id it pops
+    int rank = k - first_candidate_of_shape(w, n, w.world_shape[wi]);
+    int base = w.world_cbase[wi];
+    int F = w.pool_top[wi], N0 = w.pool_next[wi];
+    int local = rank < F ? -1 : N0 + (rank - F);
+    if (local >= w.world_cbase[wi + 1] - base) { raise_error(w.ctl, kErrCapacity); continue; }
+    int id = rank < F ? w.free_stack[base + F - 1 - rank] : base + local;
     int sa = (int)((key >> 42) & ((1ull << 22) - 1ull));
     int sb = (int)((key >> 20) & ((1ull << 22) - 1ull));
     int ta = w.shapes[sa].type, tb = w.shapes[sb].type;
@@ -353,13 +382,22 @@ __global__ void k_bp_create(DW w) {
   }
 }
 
+// Per sub-world pool update for the pairs k_bp_create just made.
+__global__ void k_bp_pools(DW w) {
+  int wi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (wi >= w.n_worlds) return;
+  int n = w.ctl->cand_count;
+  if (n > w.cand_cap) n = w.cand_cap;
+  int nw = first_candidate_of_shape(w, n, w.world_shape[wi + 1]) - first_candidate_of_shape(w, n, w.world_shape[wi]);
+  int F = w.pool_top[wi], N0 = w.pool_next[wi];
+  w.pool_top[wi] = F > nw ? F - nw : 0;
+  w.pool_next[wi] = N0 + (nw > F ? nw - F : 0);
+}
+
 __global__ void k_bp_finish(DW w) {
   Control* c = w.ctl;
   int n = c->cand_count;
   if (n > w.cand_cap) n = w.cand_cap;
-  int F = c->pool_top, N0 = c->pool_next;
-  c->pool_top = F > n ? F - n : 0;
-  c->pool_next = N0 + (n > F ? n - F : 0);
   c->new_pairs = n;
   c->cand_count = 0;
   c->moved_count = 0;
@@ -660,7 +698,7 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
     }
     w.changed_bits[k] = 0;
   }
-  if (t == 0) { total_s = total; w.ctl->changed_count = total; ovf_s = w.ctl->overflow_count; }
+  if (t == 0) { total_s = total; w.ctl->changed_count = total; ovf_s = w.ovf_count[0]; }
   __syncthreads();
   total = total_s;
   if (total == 0) return;
@@ -716,7 +754,7 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
   if (use_shared) {
     for (int b = t; b < w.n_bodies; b += kStatePassThreads) w.body_mask[b] = smask[b];
   }
-  if (t == 0) w.ctl->overflow_count = ovf_s;
+  if (t == 0) { w.ovf_count[0] = ovf_s; w.ctl->overflow_count = ovf_s; }
   __syncthreads();
   // Destroyed ids go back on the LIFO pool in id order (contact_creation.rs:543 free).
   int nd = 0;
@@ -726,7 +764,7 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
   int doff, dtotal;
   __syncthreads();
   Scan(scan_tmp).ExclusiveSum(nd, doff, dtotal);
-  int top = w.ctl->pool_top;
+  int top = w.pool_top[0];
   for (int i = i0; i < i1; ++i) {
     if (!w.destroyed[i]) continue;
     int cid = w.changed_list[i];
@@ -737,10 +775,100 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
   }
   __syncthreads();
   if (t == 0) {
-    w.ctl->pool_top = top + dtotal;
+    w.pool_top[0] = top + dtotal;
     w.ctl->hs_rebuild = w.ctl->tombstones > (w.hs_mask + 1) / 4 ? 1 : 0;
     if (w.ctl->hs_rebuild) w.ctl->tombstones = 0;
   }
+}
+
+// The ordered state pass for several sub-worlds: one thread per sub-world walks the changed
+// contacts of its own id range in id order (its bitmap words), with the same transitions as
+// k_state_pass, its own overflow list and its own id pool. Sub-worlds share no bodies, so
+// their walks are independent. ctl->changed_count and ctl->overflow_count are zeroed before.
+__global__ void k_state_worlds(DW w) {
+  int wi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (wi >= w.n_worlds) return;
+  int base = w.world_cbase[wi], end = w.world_cbase[wi + 1];
+  int ovf = w.ovf_count[wi], top = w.pool_top[wi], changes = 0;
+  int* olist = w.overflow_list + base;
+  for (int word = base >> 5; word < (end >> 5); ++word) {
+    uint32_t bits = w.changed_bits[word];
+    if (!bits) continue;
+    w.changed_bits[word] = 0;
+    while (bits) {
+      int cid = (word << 5) + __ffs(bits) - 1;
+      bits &= bits - 1;
+      ++changes;
+      DContact& c = w.contacts[cid];
+      uint32_t f = c.flags;
+      auto remove = [&](int color) {  // constraint_graph.rs:200
+        if (color != kOverflowIndex) {
+          w.body_mask[c.body_a] &= ~(1u << color);
+          w.body_mask[c.body_b] &= ~(1u << color);
+        } else {
+          int local = c.local, last = ovf - 1;
+          if (local != last) {
+            int moved = olist[last];
+            olist[local] = moved;
+            w.contacts[moved].local = local;
+          }
+          ovf = last;
+        }
+      };
+      if (f == 0) {
+      } else if (f & cSimDisjoint) {  // contact_creation.rs:428 destroy_contact
+        if (c.color != -1) remove(c.color);
+        c.manifold_count = 0;
+        c.alive = 0;
+        c.color = -1;
+        c.local = -1;
+        w.free_stack[base + top++] = cid;  // contact_creation.rs:543: ids go back in id order
+        hs_erase(w, pair_key(c.shape_a, c.shape_b));
+      } else if (f & cSimStarted) {   // constraint_graph.rs:113 add_contact_to_graph
+        c.flags = (f & ~cSimStarted) | cTouching;
+        bool dyn_a = c.enc_a >= 0, dyn_b = c.enc_b >= 0;
+        int color = kOverflowIndex;
+        if (dyn_a && dyn_b) {
+          uint32_t avail = ~(w.body_mask[c.body_a] | w.body_mask[c.body_b]) & ((1u << kDynamicColorCount) - 1u);
+          if (avail) {
+            color = __ffs(avail) - 1;
+            w.body_mask[c.body_a] |= 1u << color;
+            w.body_mask[c.body_b] |= 1u << color;
+          }
+        } else {
+          int d = dyn_a ? c.body_a : c.body_b;
+          uint32_t avail = ~w.body_mask[d] & (((1u << kOverflowIndex) - 1u) & ~1u);  // colors 22..1
+          if (avail) {
+            color = 31 - __clz(avail);
+            w.body_mask[d] |= 1u << color;
+          }
+        }
+        c.color = color;
+        if (color == kOverflowIndex) {
+          c.local = ovf;
+          olist[ovf++] = cid;
+        } else {
+          c.local = -1;
+        }
+      } else if (f & cSimStopped) {
+        c.flags = f & ~(cSimStopped | cTouching);
+        int color = c.color;
+        remove(color);
+        c.color = -1;
+        c.local = -1;
+      }
+    }
+  }
+  w.ovf_count[wi] = ovf;
+  w.pool_top[wi] = top;
+  if (changes) atomicAdd(&w.ctl->changed_count, changes);
+  if (ovf) atomicAdd(&w.ctl->overflow_count, ovf);
+}
+
+// After k_state_worlds: rebuild the pair set when erased slots pass a quarter.
+__global__ void k_state_finish(DW w) {
+  w.ctl->hs_rebuild = w.ctl->tombstones > (w.hs_mask + 1) / 4 ? 1 : 0;
+  if (w.ctl->hs_rebuild) w.ctl->tombstones = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -918,11 +1046,11 @@ __global__ void __launch_bounds__(kColorBlock) k_color_scatter_prepare(DW w, Ste
 
 // overflow_contact_solver.rs:92 prepare_overflow_contacts
 __global__ void k_prepare_overflow(DW w, StepParams p) {
-  int n = w.ctl->overflow_count;
   float ws = p.warm_start;
   float inv_tau = 1.0f / speculative_distance();
   Softness soft = p.contact_softness, stat = p.static_softness;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int wi = blockIdx.x; wi < w.n_worlds; wi += gridDim.x)
+  for (int i = w.world_cbase[wi] + threadIdx.x; i < w.world_cbase[wi] + w.ovf_count[wi]; i += blockDim.x) {
     int cid = w.overflow_list[i];
     DContact& ct = w.contacts[cid];
     DOverflow c;

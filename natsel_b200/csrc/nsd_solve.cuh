@@ -535,8 +535,8 @@ __device__ void store_constraint(const DW& w, int k) {
 __device__ void ovf_store_velocity(const DW& w, int i, uint32_t flags, V3 v, V3 wv) {
   if (i >= 0 && (flags & kDynamicFlag)) { DState* d = state_ptr(w, i); d->v = v; d->w = wv; }
 }
-__device__ void warm_start_overflow(const DW& w, int n) {
-  for (int i = 0; i < n; ++i) {
+__device__ void warm_start_overflow(const DW& w, int base, int n) {
+  for (int i = base; i < base + n; ++i) {
     const DOverflow& c = w.ovf[i];
     V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
     for (int mi = 0; mi < c.manifold_count; ++mi) {
@@ -571,10 +571,10 @@ __device__ void warm_start_overflow(const DW& w, int n) {
     }
   }
 }
-__device__ void push_overflow(const DW& w, const StepParams& p, int n) {
+__device__ void push_overflow(const DW& w, const StepParams& p, int base, int n) {
   float inv_h = p.inv_h;
   float cs = p.contact_speed;
-  for (int i = 0; i < n; ++i) {
+  for (int i = base; i < base + n; ++i) {
     DOverflow& c = w.ovf[i];
     float mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
@@ -615,9 +615,9 @@ __device__ void push_overflow(const DW& w, const StepParams& p, int n) {
     ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
   }
 }
-__device__ void relax_overflow(const DW& w, const StepParams& p, int n) {
+__device__ void relax_overflow(const DW& w, const StepParams& p, int base, int n) {
   float inv_h = p.inv_h;
-  for (int i = 0; i < n; ++i) {
+  for (int i = base; i < base + n; ++i) {
     DOverflow& c = w.ovf[i];
     float mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
@@ -700,10 +700,10 @@ __device__ void relax_overflow(const DW& w, const StepParams& p, int n) {
     ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
   }
 }
-__device__ void restitution_overflow(const DW& w, const StepParams& p, int n) {
+__device__ void restitution_overflow(const DW& w, const StepParams& p, int base, int n) {
   float thr = p.restitution_threshold;
   float inv_h = p.inv_h;
-  for (int i = 0; i < n; ++i) {
+  for (int i = base; i < base + n; ++i) {
     DOverflow& c = w.ovf[i];
     float rest = c.restitution;
     if (rest == 0.0f) continue;
@@ -752,8 +752,8 @@ __device__ void restitution_overflow(const DW& w, const StepParams& p, int n) {
     ovf_store_velocity(w, c.index_b, sb.flags, vb, wb);
   }
 }
-__device__ void store_overflow(const DW& w, int n) {
-  for (int i = 0; i < n; ++i) {
+__device__ void store_overflow(const DW& w, int base, int n) {
+  for (int i = base; i < base + n; ++i) {
     const DOverflow& c = w.ovf[i];
     if (c.manifold_count == 0) continue;
     Manifold& m = w.contacts[c.contact_id].manifold;
@@ -947,19 +947,37 @@ __device__ __noinline__ void solve_joint(const DW& w, const StepParams& p, DJoin
   store_state_vw(w, j.index_b, sb);
 }
 
-__device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges& jr, int n_ovf, int stage) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  if (stage != kRestitution) {
-    for (int t = jr.off[kOverflowIndex]; t < jr.off[kOverflowIndex + 1]; ++t) {
-      DJoint& j = w.joints[w.joint_list[t]];
-      if (stage == kWarm) warm_start_joint(w, j);
-      else solve_joint(w, p, j, stage == kPush);
-    }
+// First position in [lo, hi) of joint_list whose joint belongs to sub-world >= wi (the list of
+// one color is in joint id order, and joint ids are grouped by sub-world).
+__device__ int first_joint_of_world(const DW& w, int lo, int hi, int wi) {
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (w.joints[w.joint_list[mid]].world < wi) lo = mid + 1; else hi = mid;
   }
-  if (stage == kWarm) warm_start_overflow(w, n_ovf);
-  else if (stage == kPush) push_overflow(w, p, n_ovf);
-  else if (stage == kRelax) relax_overflow(w, p, n_ovf);
-  else restitution_overflow(w, p, n_ovf);
+  return lo;
+}
+
+// The overflow color: in each sub-world, one thread runs its overflow joints then its overflow
+// contacts in list order (overflow_contact_solver.rs:41); sub-worlds run side by side.
+__device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges& jr, int stage) {
+  int stride = gridDim.x * blockDim.x;
+  for (int wi = blockIdx.x * blockDim.x + threadIdx.x; wi < w.n_worlds; wi += stride) {
+    if (stage != kRestitution && jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex]) {
+      int j0 = first_joint_of_world(w, jr.off[kOverflowIndex], jr.off[kOverflowIndex + 1], wi);
+      int j1 = first_joint_of_world(w, j0, jr.off[kOverflowIndex + 1], wi + 1);
+      for (int t = j0; t < j1; ++t) {
+        DJoint& j = w.joints[w.joint_list[t]];
+        if (stage == kWarm) warm_start_joint(w, j);
+        else solve_joint(w, p, j, stage == kPush);
+      }
+    }
+    int base = w.world_cbase[wi], n = w.ovf_count[wi];
+    if (n == 0) continue;
+    if (stage == kWarm) warm_start_overflow(w, base, n);
+    else if (stage == kPush) push_overflow(w, p, base, n);
+    else if (stage == kRelax) relax_overflow(w, p, base, n);
+    else restitution_overflow(w, p, base, n);
+  }
 }
 
 // Phase codes: contact phases stage * 32 + color; the rest as below.
@@ -997,7 +1015,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
     n_ovf_s = n_ovf;
   }
   __syncthreads();
-  const int n_ph = n_ph_s, n_rph = n_rph_s, n_ovf = n_ovf_s;
+  const int n_ph = n_ph_s, n_rph = n_rph_s;
   const int main_phases = p.substeps * n_ph;
   const int total_phases = main_phases + (n_rph > 0 ? p.restitution_iterations * n_rph : 0);
   auto phase_at = [&](int s) { return s < main_phases ? phases[s % n_ph] : rphases[(s - main_phases) % n_rph]; };
@@ -1011,7 +1029,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
     } else if (ph == kPhaseIntegratePosition) {
       for (int i = g; i < w.n_awake; i += stride) apply_ip(w, p, i, w.states[i]);
     } else if (ph >= kPhaseOverflow) {
-      run_overflow(w, p, jr, n_ovf, ph - kPhaseOverflow);
+      run_overflow(w, p, jr, ph - kPhaseOverflow);
     } else {
       int stage = ph >> 5, c = ph & 31;
       int nj = stage == kRestitution ? 0 : jr.off[c + 1] - jr.off[c];
@@ -1032,7 +1050,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
     if (!phase_sync<kGrid>(w.ctl, bar)) return;
   }
   // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
-  if (g == 0) store_overflow(w, n_ovf);
+  for (int wi = g; wi < w.n_worlds; wi += stride) store_overflow(w, w.world_cbase[wi], w.ovf_count[wi]);
   for (int k = g; k < coff[kOverflowIndex]; k += stride) store_constraint(w, k);
 }
 

@@ -58,6 +58,7 @@ struct DShape {
   float aabb_margin, friction, restitution, rolling;
   uint64_t category, mask;
   int group, hull;
+  int world;           // sub-world of the shape (0 for a single world)
   Sphere sphere;
   Capsule capsule;
 };
@@ -196,6 +197,7 @@ struct DOverflow {
 // Revolute joint rows (revolute_joint.rs:28 RevoluteJointSim + JointSim base fields).
 struct DJoint {
   int body_a, body_b, color, enc_a, enc_b, index_a, index_b;
+  int world;           // sub-world of both bodies
   int enable_spring, enable_motor, enable_limit, fixed_rotation;
   Xf local_frame_a, local_frame_b;
   float constraint_hertz, constraint_damping_ratio;
@@ -229,13 +231,13 @@ struct Control {
   int error;              // NS_ERR_* raised on the device
   int barrier_count;      // grid barrier arrivals
   int barrier_gen;        // grid barrier generation
-  int pool_top;           // free contact ids on the stack
-  int pool_next;          // next never-used contact id
+  int pool_top;           // unused (per sub-world pools live in DW)
+  int pool_next;          // unused
   int moved_count;        // proxies enlarged since the last pair update
   int new_pairs;          // pairs found by the last pair update
   int cand_count;         // candidate slots used by the last pair update
   int changed_count;      // contact state changes in the last collide
-  int overflow_count;     // contacts in the overflow color
+  int overflow_count;     // contacts in the overflow color, all sub-worlds
   int recycled;           // contacts recycled in the last collide
   int fast_flags;         // fast-body flags raised by finalize
   int any_restitution;    // a prepared contact has restitution

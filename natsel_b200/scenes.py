@@ -98,7 +98,7 @@ def _random_quats(rng, n):
 GROUND_HALF_HEIGHT = 5.0
 
 
-def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0):
+def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0, spread=20.0, drop=(1.0, 61.0)):
     """10 000 dynamic bodies (60% boxes, 25% spheres, 15% capsules) dropped from a 40x60x40 m volume.
     ``restitution`` > 0 gives every shape that coefficient (exercises the restitution stage).
     The ground box is 100 x 10 x 100 m with its top at y = 0: bodies dropped from 61 m arrive
@@ -111,7 +111,8 @@ def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0):
     n_sph = int(round(0.25 * n))
     kinds = np.array([0] * n_box + [1] * n_sph + [2] * (n - n_box - n_sph))
     rng.shuffle(kinds)
-    pos = np.stack([rng.uniform(-20.0, 20.0, n), rng.uniform(1.0, 61.0, n), rng.uniform(-20.0, 20.0, n)], 1).astype(np.float32)
+    pos = np.stack([rng.uniform(-spread, spread, n), rng.uniform(drop[0], drop[1], n), rng.uniform(-spread, spread, n)],
+                   1).astype(np.float32)
     quats = _random_quats(rng, n)
     box_h = rng.uniform(0.25, 0.75, (n, 3)).astype(np.float32)
     sph_r = rng.uniform(0.2, 0.6, n).astype(np.float32)
@@ -176,6 +177,38 @@ def jointed_chains(world, chains=2000, links=24, boxes=4000, seed=3, grid=45, sp
                               rotation=tuple(float(v) for v in quats[i]))
         world.create_box(b, 0.3, 0.3, 0.3, density=1000.0, friction=0.6)
     return {"name": "jointed_chains", "dynamic_bodies": chains * links + boxes, "joints": n_joints}
+
+
+def batch_world(world, index, seed=4):
+    """One world of the batched-worlds workload: N ~ log-uniform(32, 512) bodies, either a box
+    pyramid of about N cubes or a random drop of N bodies with the 10 000-body pile's shape mix
+    and parameter ranges (dropped from its volume scaled to N at the same density), seeded by
+    (seed, index)."""
+    rng = np.random.Generator(np.random.PCG64([seed, index]))
+    n = int(np.exp(rng.uniform(np.log(32.0), np.log(512.0))))
+    if rng.uniform() < 0.5:
+        base = max(2, int((np.sqrt(8 * n + 1) - 1) / 2))
+        info = box_pyramid(world, base=base, seed=int(rng.integers(1 << 30)))
+        return {"kind": "pyramid", "dynamic_bodies": info["dynamic_bodies"]}
+    # the 10 000-body pile's 40 x 60 x 40 m volume scaled to N at the same initial density
+    scale = (n / 10000.0) ** (1.0 / 3.0)
+    spread = float(np.float32(20.0 * scale))
+    height = float(np.float32(60.0 * scale))
+    info = large_pile(world, n=n, seed=int(rng.integers(1 << 30)), ground_half=max(10.0, 2.5 * spread),
+                      spread=spread, drop=(1.0, 1.0 + height))
+    return {"kind": "drop", "dynamic_bodies": info["dynamic_bodies"]}
+
+
+def batched_worlds(world, count=4096, seed=4):
+    """``count`` independent worlds (batch_world) in one world object, one sub-world each."""
+    total, kinds = 0, []
+    for k in range(count):
+        if k > 0:
+            world.begin_subworld()
+        info = batch_world(world, k, seed)
+        total += info["dynamic_bodies"]
+        kinds.append(info["kind"])
+    return {"name": "batched_worlds", "worlds": count, "dynamic_bodies": total, "kinds": kinds}
 
 
 PI = F(3.14159265359)  # base/constants.rs:6
@@ -272,11 +305,12 @@ WORLD_SETTINGS = {
     "large_pile": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "jointed_chains": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "overflow_pile": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
+    "batched_worlds": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "restitution_ball": dict(gravity=(0.0, 0.0, 0.0), enable_continuous=True),
 }
 
 SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8,
-            "overflow_pile": 4, "restitution_ball": 4}
+            "overflow_pile": 4, "restitution_ball": 4, "batched_worlds": 4}
 
 BUILDERS = {
     "large_pyramid": large_pyramid,
@@ -286,4 +320,5 @@ BUILDERS = {
     "jointed_chains": jointed_chains,
     "overflow_pile": overflow_pile,
     "restitution_ball": restitution_ball,
+    "batched_worlds": batched_worlds,
 }

@@ -85,6 +85,7 @@ EXPORTED = [
     "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
+    "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
 ]
 
 
@@ -126,6 +127,10 @@ def load_library(path=LIB_PATH):
     lib.ns_collide_pairs_noalloc.argtypes = [P, P, ctypes.c_int]
     lib.ns_selftest_barrier_timeout.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.ns_world_apply_forces.argtypes = [P, P, P]
+    lib.ns_world_begin_subworld.argtypes = [P]
+    lib.ns_world_subworld_count.argtypes = [P]
+    lib.ns_world_subworld_bodies.argtypes = [P, P]
+    lib.ns_world_subworld_hashes.argtypes = [P, P]
     _lib = lib
     return lib
 
@@ -218,6 +223,26 @@ class World:
     # stepping and readback ----------------------------------------------
     def step(self, dt=1.0 / 60.0, substeps=4):
         self._check(self._lib.ns_world_step(self._w, dt, substeps))
+
+    # batched worlds ------------------------------------------------------
+    def begin_subworld(self):
+        """Start the next independent sub-world; later bodies, shapes and joints belong to it."""
+        return self._id(self._lib.ns_world_begin_subworld(self._w))
+
+    @property
+    def subworld_count(self):
+        return self._lib.ns_world_subworld_count(self._w)
+
+    def subworld_bodies(self):
+        """First body id of each sub-world followed by the total body count."""
+        out = np.zeros(self.subworld_count + 1, np.int32)
+        self._check(self._lib.ns_world_subworld_bodies(self._w, _ptr(out)))
+        return out
+
+    def subworld_hashes(self):
+        out = np.zeros(self.subworld_count, np.uint64)
+        self._check(self._lib.ns_world_subworld_hashes(self._w, _ptr(out)))
+        return out
 
     def apply_forces(self, force=None, torque=None):
         """Add per-body force / torque (float32 arrays, n_bodies x 3) for the next step."""

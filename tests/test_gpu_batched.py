@@ -1,0 +1,74 @@
+"""Batched worlds: independent sub-worlds stepped together in one world object must each give
+the bits of the same world stepped on its own (per-sub-world world_state_hash equal to the
+oracle's), including their overflow colours, joints and restitution."""
+import numpy as np
+import pytest
+
+from natsel_b200 import scenes
+from natsel_b200.world import World, default_world_def
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+DT = 1.0 / 60.0
+SETTINGS = dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False)
+
+MIXED = [
+    ("overflow_pile", {}),
+    ("box_pyramid", {"base": 6}),
+    ("jointed_chains", {"chains": 6, "boxes": 12, "grid": 3, "height": 8.0}),
+    ("large_pile", {"n": 300, "seed": 9, "restitution": 0.4, "spread": 4.0, "drop": (1.0, 9.0), "ground_half": 15.0}),
+    ("box_pyramid", {"base": 3}),
+]
+
+
+def oracle_hash(build, steps, substeps):
+    o = pyoracle.OracleWorld(**SETTINGS)
+    build(o)
+    for _ in range(steps):
+        o.step(DT, substeps)
+    return o.state_hash()
+
+
+def test_mixed_batch_matches_each_world_alone():
+    g = World(default_world_def(gravity=SETTINGS["gravity"], enable_continuous=0))
+    for k, (name, kw) in enumerate(MIXED):
+        if k:
+            g.begin_subworld()
+        scenes.BUILDERS[name](g, **kw)
+    assert g.subworld_count == len(MIXED)
+    for _ in range(40):
+        g.step(DT, 4)
+    got = g.subworld_hashes()
+    for k, (name, kw) in enumerate(MIXED):
+        want = oracle_hash(lambda w: scenes.BUILDERS[name](w, **kw), 40, 4)
+        assert int(got[k]) == want, "sub-world %d (%s) differs" % (k, name)
+    c = g.counters()
+    assert c[2 + 23] > 0  # the overflow pile's overflow colour is populated inside the batch
+
+
+def test_batched_worlds_workload_sample_matches():
+    """The 4096-world workload (log-uniform 32..512 bodies each): after 12 steps a sample of
+    sub-worlds equals the same worlds stepped alone."""
+    g = World(default_world_def(gravity=SETTINGS["gravity"], enable_continuous=0))
+    info = scenes.batched_worlds(g, count=4096, seed=4)
+    assert g.subworld_count == 4096 and info["dynamic_bodies"] > 500000
+    for _ in range(12):
+        g.step(DT, 4)
+    got = g.subworld_hashes()
+    for k in [0, 1, 2, 3, 511, 1024, 2047, 3000, 4095]:
+        want = oracle_hash(lambda w: scenes.batch_world(w, k, 4), 12, 4)
+        assert int(got[k]) == want, "sub-world %d differs" % k
+
+
+def test_subworld_rules():
+    g = World(default_world_def())
+    b0 = g.create_body(type=2)
+    assert g.begin_subworld() == 1
+    b1 = g.create_body(type=2, position=(0.0, 2.0, 0.0))
+    from natsel_b200.world import NsError
+    with pytest.raises(NsError):
+        g.create_box(b0, 0.5, 0.5, 0.5)  # a body of an earlier sub-world
+    with pytest.raises(NsError):
+        g.create_revolute(b0, b1, (0,) * 6 + (1,), (0,) * 6 + (1,))
+    g.create_box(b1, 0.5, 0.5, 0.5)
+    assert list(g.subworld_bodies()) == [0, 1, 2]
