@@ -46,6 +46,9 @@ WORKLOADS = {
     "box_pyramid": ("box_pyramid", {}, "pyramid of 210 unit cubes (base 20) on a ground box; 60 Hz, 4 substeps, FP32"),
     "large_pyramid": ("large_pyramid", {}, "the reference's large_pyramid benchmark scene (5 050 boxes resting from the "
                                            "first step, scenes.rs:105); 60 Hz, 4 substeps, FP32"),
+    "batched_worlds": ("batched_worlds", {"count": 4096, "seed": 4},
+                       "4 096 independent worlds, each a box pyramid or a random drop (shape mix and ranges of the "
+                       "10 000-body pile) of N ~ log-uniform(32, 512) bodies, stepped together; 60 Hz, 4 substeps, FP32"),
     "jointed_chains": ("jointed_chains", {}, "2 000 chains of 24 capsules on limited revolute joints + 4 000 boxes; "
                                              "60 Hz, 8 substeps, FP32"),
 }
@@ -167,12 +170,33 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 # CPU side (oracle): single-thread baseline and the reference arm's replica workers
 
-def oracle_run(scene, kw, warmup, max_steps, budget_s, barrier=None):
+def oracle_run(scene, kw, warmup, max_steps, budget_s, barrier=None, first_world=0, world_step=1):
+    """Time the oracle on the workload. A batch of worlds is timed world by world (the oracle is
+    one world): worlds first_world, first_world + world_step, ... each run warmup + max_steps
+    steps, until the budget is spent."""
     from natsel_b200 import scenes
     from oracle import pyoracle
+    sub = scenes.SUBSTEPS[scene]
+    if scene == "batched_worlds":
+        if barrier is not None:
+            barrier.wait()
+        units, seconds, steps, k = 0, 0.0, 0, first_world
+        while seconds < budget_s and k < kw["count"]:
+            w = pyoracle.OracleWorld(**scenes.WORLD_SETTINGS[scene])
+            info = scenes.batch_world(w, k, kw["seed"])
+            for _ in range(warmup):
+                w.step(DT, sub)
+            t0 = time.perf_counter()
+            for _ in range(max_steps):
+                w.step(DT, sub)
+            seconds += time.perf_counter() - t0
+            units += info["dynamic_bodies"] * sub * max_steps
+            steps += max_steps
+            k += world_step
+        return {"steps": steps, "seconds": seconds, "bodies": units / max(steps, 1) / sub, "substeps": sub,
+                "worlds": (k - first_world) // world_step}
     w = pyoracle.OracleWorld(**scenes.WORLD_SETTINGS[scene])
     info = scenes.BUILDERS[scene](w, **kw)
-    sub = scenes.SUBSTEPS[scene]
     for _ in range(warmup):
         w.step(DT, sub)
     if barrier is not None:
@@ -187,9 +211,9 @@ def oracle_run(scene, kw, warmup, max_steps, budget_s, barrier=None):
     return {"steps": steps, "seconds": time.perf_counter() - t0, "bodies": info["dynamic_bodies"], "substeps": sub}
 
 
-def _replica_worker(scene, kw, warmup, max_steps, budget_s, barrier, queue):
+def _replica_worker(scene, kw, warmup, max_steps, budget_s, barrier, queue, first_world=0, world_step=1):
     try:
-        queue.put(oracle_run(scene, kw, warmup, max_steps, budget_s, barrier))
+        queue.put(oracle_run(scene, kw, warmup, max_steps, budget_s, barrier, first_world, world_step))
     except Exception as e:  # report instead of hanging the parent
         queue.put({"error": repr(e)})
 
@@ -221,7 +245,7 @@ def run_reference_arm(args):
     barrier = ctx.Barrier(n)
     queue = ctx.Queue()
     procs = [ctx.Process(target=_replica_worker, args=(scene, kw, args.warmup, args.steps, args.reference_seconds,
-                                                        barrier, queue)) for _ in range(n)]
+                                                        barrier, queue, r, n)) for r in range(n)]
     for p in procs:
         p.start()
     results = [queue.get(timeout=args.reference_seconds + 600) for _ in procs]
@@ -235,8 +259,14 @@ def run_reference_arm(args):
     value = units / seconds
     steps = min(r["steps"] for r in results)
     ms_per_step = 1000.0 * statistics.mean(r["seconds"] / r["steps"] for r in results)
-    sample = ("%d replica worlds (one per host core, %s), each timing steps %d..%d of the drop "
-              "(bounded to %.0f s)" % (n, cpu_model(), args.warmup + 1, args.warmup + steps, args.reference_seconds))
+    if scene == "batched_worlds":
+        sample = ("%d processes (one per host core, %s) stepping the batch's worlds one after another, "
+                  "%d worlds, steps %d..%d of each (bounded to %.0f s)" % (
+                      n, cpu_model(), sum(r.get("worlds", 0) for r in results), args.warmup + 1,
+                      args.warmup + args.steps, args.reference_seconds))
+    else:
+        sample = ("%d replica worlds (one per host core, %s), each timing steps %d..%d of the drop "
+                  "(bounded to %.0f s)" % (n, cpu_model(), args.warmup + 1, args.warmup + steps, args.reference_seconds))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -359,11 +389,16 @@ def run_natsel_arm(args):
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         r = oracle_run(scene, kw, args.warmup, args.steps, args.cpu_seconds)
+        what = ("%d of the batch's worlds one after another, steps %d..%d of each" % (
+            r.get("worlds", 0), args.warmup + 1, args.warmup + args.steps)) if scene == "batched_worlds" else (
+            "steps %d..%d of the same drop" % (args.warmup + 1, args.warmup + r["steps"]))
         cpu = {"value": r["steps"] * r["bodies"] * r["substeps"] / r["seconds"], "unit": METRIC, "cores": 1,
                "kind": "port",
-               "sample": "CPU oracle (scalar C++ restatement of the reference step, 1 thread, %s) timing steps "
-                         "%d..%d of the same drop (bounded to %.0f s)" % (cpu_model(), args.warmup + 1,
-                                                                          args.warmup + r["steps"], args.cpu_seconds)}
+               "sample": "CPU oracle (scalar C++ restatement of the reference step, 1 thread, %s) timing %s "
+                         "(bounded to %.0f s)" % (cpu_model(), what, args.cpu_seconds)}
+    one_at_a_time = None
+    if rank == 0 and scene == "batched_worlds":
+        one_at_a_time = run_one_world_at_a_time(args, local_rank, kw)
 
     if rank == 0:
         line = {
@@ -372,6 +407,7 @@ def run_natsel_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene builder, no dataset)", "config": config_block(args, desc),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
+            "one_world_at_a_time": one_at_a_time,
             "wall_s": wall,
             "phase_ms_mean": {k: float(v) for k, v in zip(["broadphase", "collide", "state_color_prepare", "solve",
                                                           "finalize"], phase.mean(0))},
@@ -381,6 +417,36 @@ def run_natsel_arm(args):
     if world_size > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_one_world_at_a_time(args, local_rank, kw, sample=64, steps=100):
+    """The batch's alternative on the same GPU: each world as a world of its own, stepped one
+    at a time through the plain path. Times ``steps`` steps (after the warm-up) of ``sample``
+    worlds spread over the batch with CUDA events and reports their aggregate throughput."""
+    import torch
+    from natsel_b200 import scenes
+    from natsel_b200.world import World, default_world_def
+    s = scenes.WORLD_SETTINGS["batched_worlds"]
+    units, ms = 0, 0.0
+    picks = [int(k * kw["count"] / sample) for k in range(sample)]
+    for k in picks:
+        w = World(default_world_def(gravity=s["gravity"], enable_continuous=int(s["enable_continuous"]), device=local_rank))
+        info = scenes.batch_world(w, k, kw["seed"])
+        for _ in range(args.warmup):
+            w.step(DT, 4)
+        w.synchronize()
+        stream = torch.cuda.ExternalStream(w.stream(), device=torch.device("cuda", local_rank))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            w.step(DT, 4)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        units += info["dynamic_bodies"] * 4 * steps
+        w.close()
+    return {"value": units / (ms / 1000.0), "unit": METRIC, "sample_worlds": sample, "steps_each": steps,
+            "timing": "CUDA events around each world's steps, worlds run one after another"}
 
 
 def run_e2e(args, local_rank, dev, barrier, reduce, world_size):
