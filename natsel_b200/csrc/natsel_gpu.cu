@@ -354,7 +354,8 @@ int upload(ns_world* w, T* dst, const std::vector<T>& src) {
 int ensure_stack(ns_world* w) {
   size_t need = 0;
   cudaFuncAttributes a;
-  const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_jobs, (const void*)k_solve<true>,
+  const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_update, (const void*)k_collide_jobs,
+                           (const void*)k_solve<true>,
                            (const void*)k_solve<false>,
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
                            (const void*)k_finalize, (const void*)k_state_pass};
@@ -497,6 +498,7 @@ int upload_world(ns_world* w) {
   ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
   ALLOC(bp_xy, float4, nsh); ALLOC(bp_z, float2, nsh); ALLOC(bp_meta, int, nsh);
   ALLOC(cells, int2, (size_t)d.cell_mask + 1); ALLOC(bp_world, int, nsh);
+  ALLOC(collide_list, int, (size_t)kPairKinds * cap);
   ALLOC(world_cbase, int, n_worlds + 1); ALLOC(world_shape, int, n_worlds + 1);
   ALLOC(pool_top, int, n_worlds); ALLOC(pool_next, int, n_worlds); ALLOC(ovf_count, int, n_worlds);
   ALLOC(large_off, int, n_worlds + 1);
@@ -694,7 +696,9 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, ev_flags));
   // narrowphase (collide_pass.rs:164)
-  k_collide<<<blocks(d.cap, kCollideThreads), kCollideThreads, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cudaMemsetAsync(d.ctl->collide_count, 0, sizeof(d.ctl->collide_count), s));
+  k_collide<<<std::min(blocks(d.cap, kCollideThreads), 16 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
+  k_collide_update<<<std::min(blocks(d.cap, kCollideThreads), 8 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
   if (d.n_worlds == 1) {

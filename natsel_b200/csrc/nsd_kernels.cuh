@@ -57,6 +57,7 @@ struct DW {
   int n_worlds;
   int* world_cbase; int* world_shape; int* pool_top; int* pool_next; int* ovf_count; int* large_off;
   int* bp_world;  // sub-world of each sorted small proxy
+  int* collide_list;  // per pair kind k: ids at collide_list + k * cap needing a full update
 };
 
 struct JointRanges { int off[25]; };
@@ -491,15 +492,16 @@ __device__ bool update_contact(const DW& w, DContact& c, V3 lca, WXf xa, V3 lcb,
   return true;
 }
 
-// collide_pass.rs:541 collide_one_contact for one live contact, updated in place.
-__device__ void collide_one(const DW& w, int cid) {
+// collide_pass.rs:541 collide_one_contact, first half, for one live contact: the AABB
+// re-check and the recycling test (collide_pass.rs:606-687). Returns true when the contact
+// needs a full manifold update (collide_full).
+__device__ bool collide_recycle(const DW& w, int cid) {
   DContact& c = w.contacts[cid];
   if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
     c.flags = (c.flags | cSimDisjoint) & ~cSimTouching;
     atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
-    return;
+    return false;
   }
-  bool changed = false;
   const DSim& sa = sim_of(w, c.enc_a);
   const DSim& sb = sim_of(w, c.enc_b);
   bool was_touching = (c.flags & cSimTouching) != 0;
@@ -552,7 +554,21 @@ __device__ void collide_one(const DW& w, int cid) {
       }
     }
   }
-  if (!recycled) {
+  return !recycled;
+}
+
+// collide_pass.rs:541 collide_one_contact, second half: a new manifold from the narrowphase
+// routines and the touch transition.
+__device__ void collide_full(const DW& w, int cid) {
+  DContact& c = w.contacts[cid];
+  const DSim& sa = sim_of(w, c.enc_a);
+  const DSim& sb = sim_of(w, c.enc_b);
+  bool was_touching = (c.flags & cSimTouching) != 0;
+  WXf xa, xb;
+  xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
+  xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
+  bool changed = false;
+  {
     c.cached_rot_a = xa.q;
     c.cached_rot_b = xb.q;
     c.cached_rel = inv_mul_wxf(xa, xb);
@@ -568,32 +584,34 @@ __device__ void collide_one(const DW& w, int cid) {
   if (changed) atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
 }
 
-// Narrowphase over all contact slots. Each block takes a tile of slots, orders its live
-// contacts by pair kind in shared memory (a counting sort), and runs them in that order so
-// a warp mostly executes one shape combination. Contacts are independent here: the order
-// only changes which warp runs what.
+// Narrowphase, first pass over all contact slots: recycle what can be recycled and queue the
+// rest by pair kind.
 constexpr int kCollideThreads = 256;
 __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
-  __shared__ int order[kCollideThreads];
-  __shared__ int bucket[kPairKinds + 1];
-  for (int base = blockIdx.x * kCollideThreads; base < w.cap; base += gridDim.x * kCollideThreads) {
-    int cid = base + threadIdx.x;
-    int kind = -1;
-    if (cid < w.cap && w.contacts[cid].alive) kind = w.contacts[cid].kind;
-    if (threadIdx.x <= kPairKinds) bucket[threadIdx.x] = 0;
-    __syncthreads();
-    int slot = kind >= 0 ? atomicAdd(&bucket[kind], 1) : 0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int k = 0; k < kPairKinds; ++k) { int n = bucket[k]; bucket[k] = acc; acc += n; }
-      bucket[kPairKinds] = acc;
+  for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
+    if (!w.contacts[cid].alive) continue;
+    if (collide_recycle(w, cid)) {
+      int kind = w.contacts[cid].kind;
+      int slot = atomicAdd(&w.ctl->collide_count[kind], 1);
+      w.collide_list[(size_t)kind * w.cap + slot] = cid;
     }
-    __syncthreads();
-    if (kind >= 0) order[bucket[kind] + slot] = cid;
-    __syncthreads();
-    if (threadIdx.x < bucket[kPairKinds]) collide_one(w, order[threadIdx.x]);
-    __syncthreads();
+  }
+}
+
+// Narrowphase, second pass: full updates, kind by kind, so a warp runs one shape
+// combination. Contacts are independent here: the order only changes which warp runs what.
+__global__ void __launch_bounds__(kCollideThreads) k_collide_update(DW w) {
+  __shared__ int start[kPairKinds + 1];
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int k = 0; k < kPairKinds; ++k) { start[k] = acc; acc += w.ctl->collide_count[k]; }
+    start[kPairKinds] = acc;
+  }
+  __syncthreads();
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < start[kPairKinds]; t += gridDim.x * blockDim.x) {
+    int k = 0;
+    while (t >= start[k + 1]) ++k;
+    collide_full(w, w.collide_list[(size_t)k * w.cap + (t - start[k])]);
   }
 }
 

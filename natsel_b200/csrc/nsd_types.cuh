@@ -247,6 +247,7 @@ struct Control {
   int color_count[24];    // constraints per color (colors 0..22)
   int color_offset[25];
   int live_contacts;
+  int collide_count[6];   // contacts per pair kind queued for a full manifold update
 };
 
 }  // namespace nsd
