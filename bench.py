@@ -298,6 +298,28 @@ def build_gpu_world(args, device):
     return w, info, scenes.SUBSTEPS[scene]
 
 
+def make_reducer(world_size, device):
+    """reduce(x, "max" | "sum") over the ranks of the default process group (identity alone)."""
+    import torch
+    import torch.distributed as dist
+
+    def reduce(x, op):
+        if world_size == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+    return reduce
+
+
+def job_throughput(bodies, substeps, steps, elapsed_ms, reduce):
+    """Whole-job body-substeps/s: the bodies of every rank over the slowest rank's time.
+    Returns (value, max elapsed ms)."""
+    total_ms = reduce(float(elapsed_ms), "max")
+    units = reduce(float(bodies), "sum") * substeps * steps
+    return units / (total_ms / 1000.0), total_ms
+
+
 def run_natsel_arm(args):
     import numpy as np
     import torch
@@ -322,12 +344,7 @@ def run_natsel_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def reduce(x, op):
-        if world_size == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=op)
-        return float(t.item())
+    reduce = make_reducer(world_size, dev)
 
     uuids = [str(torch.cuda.get_device_properties(local_rank).uuid)]
     if world_size > 1:
@@ -367,9 +384,8 @@ def run_natsel_arm(args):
     clocks = sampler.stop() if sampler else None
     launches = int(world.solver_counts()[12]) - launches0
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
-    total_ms = reduce(float(step_ms.sum()), dist.ReduceOp.MAX if world_size > 1 else None)
-    launches = int(reduce(float(launches), dist.ReduceOp.SUM if world_size > 1 else None))
-    value = world_size * bodies * sub * args.steps / (total_ms / 1000.0)
+    value, total_ms = job_throughput(bodies, sub, args.steps, float(step_ms.sum()), reduce)
+    launches = int(reduce(float(launches), "sum"))
 
     solve_ms = phase[:, 3]
     achieved = solve_bytes.sum() / (solve_ms.sum() / 1000.0) / 1e9
@@ -478,9 +494,10 @@ def run_e2e(args, local_rank, dev, barrier, reduce, world_size):
     for k in range(args.steps):
         one(k)
     barrier()
-    seconds = reduce(time.perf_counter() - t0, dist.ReduceOp.MAX if world_size > 1 else None)
+    value, ms = job_throughput(info["dynamic_bodies"], sub, args.steps, 1000.0 * (time.perf_counter() - t0), reduce)
+    seconds = ms / 1000.0
     world.close()
-    return {"value": world_size * info["dynamic_bodies"] * sub * args.steps / seconds, "unit": METRIC,
+    return {"value": value, "unit": METRIC,
             "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 64 * n, "ms_per_step": 1000.0 * seconds / args.steps,
             "timing": "host wall clock around the K steps, synchronised by each step's readback"}
 
