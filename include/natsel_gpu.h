@@ -197,8 +197,9 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count);
  * the results are in the host arrays. */
 int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int count);
 
-/* Diagnostics (no counterpart in the reference): launches the solver's bounded grid barrier
- * waiting for one arrival that never comes, so every block gives up after timeout_ms
+/* Diagnostics (no counterpart in the reference): launches the bounded grid barrier of the
+ * cooperative solver launch (solver_blocks > 16, or sub-worlds) waiting for one arrival that
+ * never comes, so every block gives up after timeout_ms
  * (1..2000). Returns NS_ERR_TIMEOUT when the wait expired and was reported as designed; the
  * CUDA context stays usable afterwards. */
 int ns_selftest_barrier_timeout(int device, int timeout_ms);

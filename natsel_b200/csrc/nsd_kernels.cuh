@@ -402,7 +402,6 @@ __global__ void k_bp_finish(DW w) {
   c->new_pairs = n;
   c->cand_count = 0;
   c->moved_count = 0;
-  c->max_width_bits = 0;
   c->recycled = 0;
   c->hs_rebuild = 0;
 }

@@ -13,52 +13,6 @@
 
 namespace nsd {
 
-// Bounded grid barrier. The arrival counter is zeroed before each launch; barrier k is
-// complete when it reaches (k + 1) * gridDim.x (+ ``missing``, which only the barrier
-// self-test sets, to wait for arrivals that never come). A block that waits longer than
-// ``limit_ns`` raises NS_ERR_TIMEOUT and the whole kernel unwinds at its next barrier
-// instead of hanging.
-__device__ __forceinline__ bool grid_barrier(Control* ctl, int& index, int missing = 0,
-                                             unsigned long long limit_ns = 2000000000ull) {
-  __shared__ int ok_s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int target = (index + 1) * (int)gridDim.x + missing;
-    __threadfence();
-    atomicAdd(&ctl->barrier_count, 1);
-    int ok = 1;
-    unsigned long long t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    long long spins = 0;
-    for (;;) {
-      int v = *((volatile int*)&ctl->barrier_count);
-      if (v >= target) break;
-      if (*((volatile int*)&ctl->error) != 0) { ok = 0; break; }
-      if (++spins > (1ll << 26)) { ok = 0; break; }
-      if ((spins & 1023) == 0) {
-        unsigned long long t1;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > limit_ns) { ok = 0; break; }
-      }
-      __nanosleep(32);
-    }
-    if (!ok) atomicCAS(&ctl->error, 0, kErrTimeout);
-    __threadfence();
-    ok_s = ok;
-  }
-  __syncthreads();
-  index++;
-  return ok_s != 0;
-}
-
-// Self-test of the bounded wait: every block arrives, but the barrier also waits for one
-// arrival that nothing makes, so each block gives up after ``limit_ns`` and the kernel
-// returns with ctl->error = kErrTimeout.
-__global__ void k_barrier_selftest(Control* ctl, unsigned long long limit_ns) {
-  int bar = 0;
-  grid_barrier(ctl, bar, 1, limit_ns);
-}
-
 // barrier.cluster with release/acquire semantics: global-memory writes of every thread of
 // the cluster before the barrier are visible to every thread of the cluster after it.
 __device__ __forceinline__ void cluster_sync_all() {
@@ -68,14 +22,16 @@ __device__ __forceinline__ void cluster_sync_all() {
 // Grid-wide barrier of the cooperative solver launch: thread 0 of each block adds its arrival
 // with release semantics and polls the counter with acquire loads; the block's other threads
 // are ordered by __syncthreads on both sides. Barrier k completes at (k + 1) * gridDim.x
-// arrivals (the counter is zeroed before each launch). The wait is bounded: after 2 s, 2^26
-// polls or another block's error it raises NS_ERR_TIMEOUT and returns false, and every block
-// then leaves the kernel at its next barrier.
-__device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index) {
+// arrivals (the counter is zeroed before each launch; ``missing`` is only set by the barrier
+// self-test, to wait for arrivals that never come). The wait is bounded: after limit_ns (2 s),
+// 2^26 polls or another block's error it raises NS_ERR_TIMEOUT and returns false, and every
+// block then leaves the kernel at its next barrier.
+__device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index, int missing = 0,
+                                                  unsigned long long limit_ns = 2000000000ull) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
-    int target = (index + 1) * (int)gridDim.x;
+    int target = (index + 1) * (int)gridDim.x + missing;
     int* cnt = &ctl->barrier_count;
     asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(cnt) : "memory");
     int ok = 1;
@@ -88,7 +44,7 @@ __device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index) {
       if ((spins & 255) == 0) {
         unsigned long long t1;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (*((volatile int*)&ctl->error) != 0 || t1 - t0 > 2000000000ull || spins > (1ll << 26)) { ok = 0; break; }
+        if (*((volatile int*)&ctl->error) != 0 || t1 - t0 > limit_ns || spins > (1ll << 26)) { ok = 0; break; }
       }
     }
     if (!ok) atomicCAS(&ctl->error, 0, kErrTimeout);
@@ -97,6 +53,14 @@ __device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index) {
   __syncthreads();
   index++;
   return ok_s != 0;
+}
+
+// Self-test of the solver's bounded grid barrier: every block arrives, but the barrier also
+// waits for one arrival that nothing makes, so each block gives up after ``limit_ns`` and the
+// kernel returns with ctl->error = kErrTimeout.
+__global__ void k_barrier_selftest(Control* ctl, unsigned long long limit_ns) {
+  int bar = 0;
+  grid_sync_acq_rel(ctl, bar, 1, limit_ns);
 }
 
 template <bool kGrid>

@@ -230,9 +230,6 @@ struct StepParams {
 struct Control {
   int error;              // NS_ERR_* raised on the device
   int barrier_count;      // grid barrier arrivals
-  int barrier_gen;        // grid barrier generation
-  int pool_top;           // unused (per sub-world pools live in DW)
-  int pool_next;          // unused
   int moved_count;        // proxies enlarged since the last pair update
   int new_pairs;          // pairs found by the last pair update
   int cand_count;         // candidate slots used by the last pair update
@@ -241,7 +238,6 @@ struct Control {
   int recycled;           // contacts recycled in the last collide
   int fast_flags;         // fast-body flags raised by finalize
   int any_restitution;    // a prepared contact has restitution
-  int max_width_bits;     // widest small proxy (x extent, float bits)
   int tombstones;         // erased pair-set slots since the last rebuild
   int hs_rebuild;         // rebuild the pair set this step
   int color_count[24];    // constraints per color (colors 0..22)
