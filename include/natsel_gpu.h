@@ -204,6 +204,49 @@ int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int cou
  * CUDA context stays usable afterwards. */
 int ns_selftest_barrier_timeout(int device, int timeout_ms);
 
+/* ---- Adjoint: vector-Jacobian product of a recorded rollout --------------------------------
+ * No counterpart in the reference, which has no differentiation; these calls are the
+ * differentiable form of World::step (solver_integration.rs:807) built on the same step.
+ *
+ * ns_world_tape_begin starts recording: every later ns_world_step is logged, and the world's
+ * device state is copied to a checkpoint at the start and whenever checkpoint_substeps
+ * substeps have passed since the last checkpoint (steps are whole, so a checkpoint falls on
+ * the first step boundary at or after that count). While recording, dt must be > 0 and
+ * ns_world_apply_forces is refused. Scope: one world (no sub-worlds) of box bodies with the
+ * centre of mass at the body origin, no joints, restitution, rolling resistance or continuous
+ * collision (NS_ERR_UNSUPPORTED otherwise); steps that put contacts in the overflow colour are
+ * reported by ns_world_vjp as NS_ERR_UNSUPPORTED. */
+int ns_world_tape_begin(ns_world* w, int checkpoint_substeps);
+/* Stops recording; the tape stays for ns_world_vjp. */
+int ns_world_tape_end(ns_world* w);
+/* Releases the tape and its checkpoints. */
+int ns_world_tape_free(ns_world* w);
+/* out[6]: recorded steps, checkpoints, narrowphase replays that did not reproduce the
+ * recorded manifold (their pose derivatives are left out), VJP calls, recording (0/1),
+ * checkpoint interval in substeps. */
+int ns_world_tape_info(ns_world* w, int64_t* out);
+/* Cotangents of the world's state after the last recorded step, in body id order (rows as
+ * ns_world_get_bodies: position xyz, rotation xyzw, linear and angular velocity; any may be
+ * NULL for zero), are pulled back to the state and parameters at ns_world_tape_begin:
+ * initial linear and angular velocity (3 per body), body mass (the density scale: inverse
+ * mass and inverse inertia scale as 1/m, inertia as m), the friction of the body's shape, initial position
+ * (3) and rotation (4). Any output may be NULL; static bodies get zeros. The recorded steps
+ * are replayed from the checkpoints (bit-identical to the recorded run) to rebuild the
+ * intermediate state, and the world is left in its state after the last recorded step.
+ * Gradients are exact for the branch the rollout took (contact sets, clamps and friction
+ * cones are held). Synchronous. */
+int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
+                 float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0);
+
+/* Diagnostics (no counterpart in the reference): an f64 check, on the host without a GPU, of
+ * one local derivative the adjoint uses (which: 0 warm start, 1 push, 2 relax, 3 prepare,
+ * 4 integrate velocities, 5 integrate positions, 6 finalize rotation, 7 inverse world inertia,
+ * 8 recycled separations, 9..11 box-box manifolds: face, any axis, edge pair) at seeded random
+ * inputs. worst[0] = the largest relative difference between the dual-number vector-Jacobian
+ * product and central differences over all input directions; worst[1] = the separating-axis
+ * kind of the box cases (-1 otherwise). */
+int ns_adjoint_selfcheck(int which, int seed, double* worst);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
@@ -18,6 +19,7 @@
 
 #include "../../include/natsel_gpu.h"
 #include "nsd_solve.cuh"
+#include "nsd_adjoint.cuh"
 
 using namespace nsd;
 
@@ -67,6 +69,8 @@ struct ns_world {
   DW dw;
   JointRanges jr;
   std::vector<void*> allocations;
+  std::vector<size_t> allocation_bytes;
+  struct AdTape* tape = nullptr;   // rollout record for the adjoint (ns_world_tape_begin)
   void* cub_sort_tmp = nullptr;
   size_t cub_sort_bytes = 0;
   void* cub_scan_tmp = nullptr;
@@ -338,6 +342,7 @@ T* dalloc(ns_world* w, size_t n, int* status) {
   }
   cudaMemsetAsync(p, 0, bytes, w->stream);
   w->allocations.push_back(p);
+  w->allocation_bytes.push_back(bytes);
   return (T*)p;
 }
 
@@ -355,10 +360,14 @@ int ensure_stack(ns_world* w) {
   size_t need = 0;
   cudaFuncAttributes a;
   const void* kernels[] = {(const void*)k_collide, (const void*)k_collide_update, (const void*)k_collide_jobs,
-                           (const void*)k_solve<true>,
-                           (const void*)k_solve<false>,
+                           (const void*)k_solve<true, false>,
+                           (const void*)k_solve<false, false>,
+                           (const void*)k_solve<true, true>,
+                           (const void*)k_solve<false, true>,
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
-                           (const void*)k_finalize, (const void*)k_state_pass};
+                           (const void*)k_finalize, (const void*)k_state_pass,
+                           (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
+                           (const void*)k_adj_narrow, (const void*)k_adj_prepare};
   for (const void* k : kernels) {
     cudaError_t e = cudaFuncGetAttributes(&a, k);
     if (e != cudaSuccess) return fail(w, NS_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
@@ -554,8 +563,10 @@ int upload_world(ns_world* w) {
   NS_CUDA(w, cub::DeviceScan::ExclusiveSum(nullptr, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh));
   NS_CUDA(w, cudaMalloc(&w->cub_sort_tmp, std::max<size_t>(w->cub_sort_bytes, 16)));
   w->allocations.push_back(w->cub_sort_tmp);
+  w->allocation_bytes.push_back(std::max<size_t>(w->cub_sort_bytes, 16));
   NS_CUDA(w, cudaMalloc(&w->cub_scan_tmp, std::max<size_t>(w->cub_scan_bytes, 16)));
   w->allocations.push_back(w->cub_scan_tmp);
+  w->allocation_bytes.push_back(std::max<size_t>(w->cub_scan_bytes, 16));
   // state pass: staged change chunks always live in shared memory; every body's color
   // mask joins them there when it fits
   int max_smem = 0;
@@ -576,7 +587,8 @@ int upload_world(ns_world* w) {
     int want = w->def.solver_blocks > 0 ? w->def.solver_blocks
                : (n_worlds > 1 ? std::max(w->sm_count, kMaxSolveCluster + 1) : kMaxSolveCluster);
     if (want >= 1 && want <= kMaxSolveCluster) {
-      NS_CUDA(w, cudaFuncSetAttribute(k_solve<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
       int best = 0;
       for (int cs = want; cs >= 1; --cs) {
         cudaLaunchConfig_t cfg = {};
@@ -590,7 +602,7 @@ int upload_world(ns_world* w) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, k_solve<false>, &cfg);
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, k_solve<false, false>, &cfg);
         if (e == cudaSuccess && clusters >= 1) { best = cs; break; }
         cudaGetLastError();
       }
@@ -599,7 +611,7 @@ int upload_world(ns_world* w) {
       w->solver_grid = false;
     } else {
       int per_sm = 0;
-      NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true>, kSolveThreads, 0));
+      NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true, false>, kSolveThreads, 0));
       int max_blocks = per_sm * w->sm_count;
       if (max_blocks < 1) return fail(w, NS_ERR_CUDA, "the solver block does not fit on this device");
       int blocks_ = std::min(want, max_blocks);
@@ -661,9 +673,7 @@ int enqueue_pair_update(ns_world* w) {
   return NS_OK;
 }
 
-int enqueue_step(ns_world* w, float dt, int substeps) {
-  DW d = w->dw;
-  cudaStream_t s = w->stream;
+StepParams make_step_params(const ns_world* w, float dt, int substeps) {
   StepParams p;
   memset(&p, 0, sizeof(p));
   p.dt = dt;
@@ -683,8 +693,31 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
   p.restitution_iterations = w->def.restitution_iterations;
   p.enable_continuous = w->def.enable_continuous;
   p.gravity = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
+  return p;
+}
+
+// Device copies of one step's inputs that the adjoint replays (nsd_adjoint.cuh StepTape).
+struct HostStepTape {
+  StepTape dev;
+  SolveTape solve;
+  CopyOp* plane_ops = nullptr;  // device table: the prepared planes -> dev.planes
+  int n_plane_ops = 0;
+};
+
+// One step. With a tape the narrowphase outcomes, the contacts before the narrowphase and
+// after the state pass, the prepared planes and the solver's inputs are recorded as well
+// (the arithmetic is unchanged).
+int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape = nullptr) {
+  DW d = w->dw;
+  cudaStream_t s = w->stream;
+  StepParams p = make_step_params(w, dt, substeps);
   auto blocks = [](int n, int t) { return std::max(1, (n + t - 1) / t); };
   int nk = 0;
+  if (tape) {
+    d.np_mode = tape->dev.mode;
+    NS_CUDA(w, cudaMemsetAsync(tape->dev.mode, 0, (size_t)d.cap, s));
+    NS_CUDA(w, cudaMemcpyAsync(tape->dev.sims, d.asims, sizeof(DSim) * (size_t)d.n_awake, cudaMemcpyDeviceToDevice, s));
+  }
   // phase events: graph nodes that record externally when captured, plain records otherwise
   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   NS_CUDA(w, cudaStreamIsCapturing(s, &capturing));
@@ -695,6 +728,8 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     if (st) return st;
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[1], s, ev_flags));
+  if (tape)
+    NS_CUDA(w, cudaMemcpyAsync(tape->dev.pre, d.contacts, sizeof(DContact) * (size_t)d.cap, cudaMemcpyDeviceToDevice, s));
   // narrowphase (collide_pass.rs:164)
   NS_CUDA(w, cudaMemsetAsync(d.ctl->collide_count, 0, sizeof(d.ctl->collide_count), s));
   k_collide<<<std::min(blocks(d.cap, kCollideThreads), 16 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
@@ -709,6 +744,8 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     k_state_worlds<<<blocks(d.n_worlds, 128), 128, 0, s>>>(d); ++nk;
     k_state_finish<<<1, 1, 0, s>>>(d); ++nk;
   }
+  if (tape)
+    NS_CUDA(w, cudaMemcpyAsync(tape->dev.post, d.contacts, sizeof(DContact) * (size_t)d.cap, cudaMemcpyDeviceToDevice, s));
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
   k_color_scan<<<1, 32, 0, s>>>(d); ++nk;
   k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p); ++nk;
@@ -718,6 +755,10 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     ++nk;
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, ev_flags));
+  if (tape) {
+    k_multi_copy<<<4 * w->sm_count, 256, 0, s>>>(tape->plane_ops, tape->n_plane_ops);
+    NS_CUDA(w, cudaMemcpyAsync(tape->dev.ctl, d.ctl, sizeof(Control), cudaMemcpyDeviceToDevice, s));
+  }
   // solver stages (solver_stages.rs:543)
   {
     cudaLaunchConfig_t cfg = {};
@@ -737,8 +778,13 @@ int enqueue_step(ns_world* w, float dt, int substeps) {
     }
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<true>, d, p, w->jr));
-    else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<false>, d, p, w->jr));
+    SolveTape tp;
+    memset(&tp, 0, sizeof(tp));
+    if (tape) tp = tape->solve;
+    if (tape && w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<true, true>, d, p, w->jr, tp));
+    else if (tape) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<false, true>, d, p, w->jr, tp));
+    else if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<true, false>, d, p, w->jr, tp));
+    else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_solve<false, false>, d, p, w->jr, tp));
     ++nk;
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, ev_flags));
@@ -790,6 +836,457 @@ int read_control(ns_world* w, Control* c) {
   return NS_OK;
 }
 
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Rollout tape and adjoint (ns_world_tape_begin / ns_world_vjp).
+//
+// While a tape records, every step is logged and the world's device buffers are copied to a
+// checkpoint whenever `every` substeps have passed since the last one. The vector-Jacobian
+// product walks the checkpoint segments backwards: it restores a checkpoint, replays the
+// segment's steps with the solver tape on (bit-identical to the recorded steps: same kernels,
+// same inputs), and runs the reverse kernels step by step from the segment's end. The world is
+// put back in its final state afterwards.
+struct AdStepRec { float dt; int substeps; };
+struct AdCheckpoint {
+  char* data = nullptr;      // snapshot bytes followed by the two copy tables
+  CopyOp* save = nullptr;
+  CopyOp* load = nullptr;
+};
+struct AdTape {
+  int every = 8;
+  bool recording = false;
+  std::vector<AdStepRec> steps;
+  std::vector<int> ckpt_at;           // index of the first step after each checkpoint
+  std::vector<AdCheckpoint> ckpt;
+  int since = 0;
+  int64_t replay_mismatch = 0;        // narrowphase replays that missed the recorded manifold
+  int64_t vjp_calls = 0;
+};
+
+namespace {
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int take_checkpoint(ns_world* w, AdCheckpoint* ck) {
+  if (w->allocation_bytes.size() != w->allocations.size())
+    return fail(w, NS_ERR_INVALID, "device allocation table is inconsistent");
+  size_t n = w->allocations.size(), bytes = 0;
+  std::vector<size_t> off(n);
+  for (size_t i = 0; i < n; ++i) { off[i] = bytes; bytes += align256(w->allocation_bytes[i]); }
+  size_t table = align256(n * sizeof(CopyOp));
+  if (!ck->data) {
+    NS_CUDA(w, cudaMalloc(&ck->data, bytes + 2 * table));
+    std::vector<CopyOp> save(n), load(n);
+    for (size_t i = 0; i < n; ++i) {
+      save[i] = {(const char*)w->allocations[i], ck->data + off[i], w->allocation_bytes[i]};
+      load[i] = {ck->data + off[i], (char*)w->allocations[i], w->allocation_bytes[i]};
+    }
+    ck->save = (CopyOp*)(ck->data + bytes);
+    ck->load = (CopyOp*)(ck->data + bytes + table);
+    NS_CUDA(w, cudaMemcpy(ck->save, save.data(), n * sizeof(CopyOp), cudaMemcpyHostToDevice));
+    NS_CUDA(w, cudaMemcpy(ck->load, load.data(), n * sizeof(CopyOp), cudaMemcpyHostToDevice));
+  }
+  k_multi_copy<<<4 * w->sm_count, 256, 0, w->stream>>>(ck->save, (int)n);
+  NS_CUDA(w, cudaGetLastError());
+  return NS_OK;
+}
+
+int restore_checkpoint(ns_world* w, const AdCheckpoint& ck) {
+  k_multi_copy<<<4 * w->sm_count, 256, 0, w->stream>>>(ck.load, (int)w->allocations.size());
+  NS_CUDA(w, cudaGetLastError());
+  return NS_OK;
+}
+
+void free_tape(ns_world* w) {
+  if (!w->tape) return;
+  cudaStreamSynchronize(w->stream);
+  for (AdCheckpoint& c : w->tape->ckpt) cudaFree(c.data);
+  delete w->tape;
+  w->tape = nullptr;
+}
+
+int tape_after_step(ns_world* w, float dt, int substeps) {
+  AdTape* t = w->tape;
+  t->steps.push_back({dt, substeps});
+  t->since += substeps;
+  if (t->since >= t->every) {
+    t->ckpt.emplace_back();
+    int st = take_checkpoint(w, &t->ckpt.back());
+    if (st) return st;
+    t->ckpt_at.push_back((int)t->steps.size());
+    t->since = 0;
+  }
+  return NS_OK;
+}
+
+// The adjoint covers one world of boxes without joints, restitution, rolling resistance or
+// continuous collision.
+int check_adjoint_scope(ns_world* w) {
+  if (w->sub_body_begin.size() > 1) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint takes a single world");
+  if (!w->joints.empty()) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover joints");
+  if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
+  for (const HostShape& hs : w->shapes) {
+    if (hs.d.type != kHull) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint covers box shapes only");
+    if (hs.d.restitution != 0.0f || hs.d.rolling != 0.0f)
+      return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover restitution or rolling resistance");
+  }
+  for (const DSim& a : w->asims) {
+    if (a.local_center.x != 0.0f || a.local_center.y != 0.0f || a.local_center.z != 0.0f)
+      return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs each body's centre of mass at its origin");
+  }
+  return NS_OK;
+}
+
+// Device storage of the step tapes of one segment.
+struct TapeSet {
+  char* data = nullptr;
+  std::vector<HostStepTape> steps;
+};
+
+int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
+  const DW& d = w->dw;
+  size_t cap = (size_t)d.cap, n = (size_t)std::max(d.n_awake, 1);
+  std::vector<std::pair<size_t*, size_t>> parts;
+  size_t per = 0;
+  auto take = [&](size_t b) { size_t o = per; per += align256(b); return o; };
+  size_t o_sims = take(sizeof(DSim) * n), o_pre = take(sizeof(DContact) * cap), o_post = take(sizeof(DContact) * cap);
+  size_t o_ctl = take(sizeof(Control));
+  size_t o_pl = take(sizeof(int4) * cap + 13 * sizeof(float4) * cap + 3 * 4 * sizeof(float4) * cap + 4 * sizeof(float) * cap + 16 * 20);
+  size_t o_body = take(sizeof(DState) * 3 * n * max_substeps);
+  size_t o_push = take(sizeof(float4) * 4 * cap * max_substeps);
+  size_t o_relax = take(sizeof(float4) * 5 * cap * max_substeps);
+  size_t o_fin = take(sizeof(float4) * cap), o_mode = take(cap), o_ops = take(sizeof(CopyOp) * 20);
+  NS_CUDA(w, cudaMalloc(&ts->data, per * (size_t)count));
+  ts->steps.resize(count);
+  for (int j = 0; j < count; ++j) {
+    char* b = ts->data + per * (size_t)j;
+    HostStepTape& h = ts->steps[j];
+    StepTape& t = h.dev;
+    t.sims = (DSim*)(b + o_sims); t.pre = (DContact*)(b + o_pre); t.post = (DContact*)(b + o_post);
+    t.ctl = (Control*)(b + o_ctl);
+    char* pl = b + o_pl;
+    auto carve = [&](size_t bytes) { char* r = pl; pl += (bytes + 15) & ~(size_t)15; return r; };
+    CPlanes& P = t.planes;
+    const CPlanes& L = d.cp;
+    P.cap = L.cap;
+    P.idx = (int4*)carve(sizeof(int4) * cap);
+    float4** f4[] = {&P.mass, &P.ia0, &P.ia1, &P.ib1, &P.n, &P.t1, &P.t2, &P.ca, &P.cb, &P.tm, &P.fr, &P.roll, &P.rm};
+    for (float4** f : f4) *f = (float4*)carve(sizeof(float4) * cap);
+    P.pra = (float4*)carve(sizeof(float4) * 4 * cap);
+    P.prb = (float4*)carve(sizeof(float4) * 4 * cap);
+    P.pimp = (float4*)carve(sizeof(float4) * 4 * cap);
+    P.prest = (float*)carve(sizeof(float) * 4 * cap);
+    std::vector<CopyOp> ops;
+    ops.push_back({(const char*)L.idx, (char*)P.idx, sizeof(int4) * cap});
+    float4* const* lf4[] = {&L.mass, &L.ia0, &L.ia1, &L.ib1, &L.n, &L.t1, &L.t2, &L.ca, &L.cb, &L.tm, &L.fr, &L.roll, &L.rm};
+    for (int i = 0; i < 13; ++i) ops.push_back({(const char*)*lf4[i], (char*)*f4[i], sizeof(float4) * cap});
+    ops.push_back({(const char*)L.pra, (char*)P.pra, sizeof(float4) * 4 * cap});
+    ops.push_back({(const char*)L.prb, (char*)P.prb, sizeof(float4) * 4 * cap});
+    ops.push_back({(const char*)L.pimp, (char*)P.pimp, sizeof(float4) * 4 * cap});
+    t.body = (DState*)(b + o_body);
+    t.push = (float4*)(b + o_push);
+    t.relax = (float4*)(b + o_relax);
+    t.fin = (float4*)(b + o_fin);
+    t.mode = (uint8_t*)(b + o_mode);
+    t.substeps = 0;
+    h.solve.body = t.body; h.solve.push = t.push; h.solve.relax = t.relax; h.solve.fin = t.fin;
+    h.plane_ops = (CopyOp*)(b + o_ops);
+    h.n_plane_ops = (int)ops.size();
+    NS_CUDA(w, cudaMemcpy(h.plane_ops, ops.data(), ops.size() * sizeof(CopyOp), cudaMemcpyHostToDevice));
+  }
+  return NS_OK;
+}
+
+int launch_adj_solve(ns_world* w, const StepTape& t, const AdjBufs& a, const StepParams& p) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(kAdjThreads);
+  cfg.stream = w->stream;
+  cudaLaunchAttribute attr[1];
+  int blocks = w->solver_blocks;
+  if (w->solver_grid) {
+    int per_sm = 0;
+    NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve<true>, kAdjThreads, 0));
+    blocks = std::max(1, std::min(blocks, per_sm * w->sm_count));
+    NS_CUDA(w, cudaMemsetAsync(&w->dw.ctl->barrier_count, 0, sizeof(int), w->stream));
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+  } else {
+    NS_CUDA(w, cudaFuncSetAttribute(k_adj_solve<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = blocks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+  }
+  cfg.gridDim = dim3(blocks);
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<true>, t, a, p, w->dw.ctl));
+  else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<false>, t, a, p, w->dw.ctl));
+  return NS_OK;
+}
+
+// Host check of the adjoint's local derivatives in f64: for each input direction i the
+// dual-number VJP component sum_j ybar_j dy_j/dx_i is compared with the central difference of
+// the same function evaluated in plain f64.
+struct Rng64 {
+  uint64_t s;
+  double next() {  // uniform in [0, 1)
+    s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+    return (double)(s >> 11) * (1.0 / 9007199254740992.0);
+  }
+  double range(double a, double b) { return a + (b - a) * next(); }
+};
+
+template <class Fn>
+double vjp_fd_error(const std::vector<double>& x0, int ny, Fn fn, Rng64& rng, int n_dirs = -1) {
+  const int nx = (int)x0.size();
+  std::vector<double> ybar(ny);
+  for (double& v : ybar) v = rng.range(-1.0, 1.0);
+  std::vector<ad::Dual<double, 1>> yd(ny);
+  std::vector<double> yp(ny), ym(ny), xp(x0), xm(x0);
+  double worst = 0.0;
+  for (int i = 0; i < (n_dirs < 0 ? nx : n_dirs); ++i) {
+    ad::SeedIn<double, 1> in;
+    in.x = x0.data();
+    in.dir[0] = i;
+    fn(in, yd.data());
+    double g = 0.0;
+    for (int j = 0; j < ny; ++j) g += ybar[j] * yd[j].d[0];
+    const double h = 1e-6 * std::max(1.0, std::fabs(x0[i]));
+    xp = x0; xm = x0;
+    xp[i] += h; xm[i] -= h;
+    ad::PlainIn<double> ip{xp.data()}, im{xm.data()};
+    fn(ip, yp.data());
+    fn(im, ym.data());
+    double fd = 0.0;
+    for (int j = 0; j < ny; ++j) fd += ybar[j] * (yp[j] - ym[j]) / (2.0 * h);
+    double err = std::fabs(g - fd) / std::max(1.0, std::fabs(fd));
+    worst = std::max(worst, err);
+  }
+  return worst;
+}
+
+void random_unit(Rng64& r, double* v, int n) {
+  double l = 0.0;
+  for (int i = 0; i < n; ++i) { v[i] = r.range(-1.0, 1.0); l += v[i] * v[i]; }
+  l = std::sqrt(l);
+  for (int i = 0; i < n; ++i) v[i] /= l;
+}
+void random_spd(Rng64& r, double* s /* xx xy xz yy yz zz */) {
+  s[0] = r.range(0.5, 2.0); s[3] = r.range(0.5, 2.0); s[5] = r.range(0.5, 2.0);
+  s[1] = r.range(-0.1, 0.1); s[2] = r.range(-0.1, 0.1); s[4] = r.range(-0.1, 0.1);
+}
+void random_constraint(Rng64& r, std::vector<double>& x) {
+  using namespace ad;
+  x.assign(kCV, 0.0);
+  for (int i = 0; i < 12; ++i) x[i] = r.range(-1.0, 1.0);
+  for (int i = 0; i < 3; ++i) { x[cvDpA + i] = r.range(-0.01, 0.01); x[cvDpB + i] = r.range(-0.01, 0.01); }
+  for (int b = 0; b < 2; ++b) {
+    double* q = &x[b ? cvDqB : cvDqA];
+    q[0] = r.range(-0.02, 0.02); q[1] = r.range(-0.02, 0.02); q[2] = r.range(-0.02, 0.02);
+    q[3] = std::sqrt(1.0 - q[0] * q[0] - q[1] * q[1] - q[2] * q[2]);
+  }
+  for (int q = 0; q < 4; ++q) x[cvLam + q] = r.range(0.05, 1.0);
+  x[cvFr] = r.range(-0.1, 0.1); x[cvFr + 1] = r.range(-0.1, 0.1); x[cvTwist] = r.range(-0.01, 0.01);
+  x[cvIma] = r.range(0.5, 2.0); x[cvImb] = r.range(0.5, 2.0);
+  random_spd(r, &x[cvSa]); random_spd(r, &x[cvSb]);
+  random_unit(r, &x[cvN], 3);
+  for (int i = 0; i < 3; ++i) { x[cvCa + i] = r.range(-0.5, 0.5); x[cvCb + i] = r.range(-0.5, 0.5); }
+  x[cvTwistMass] = r.range(0.3, 1.0);
+  x[cvTm] = r.range(0.5, 1.0); x[cvTm + 1] = r.range(-0.1, 0.1); x[cvTm + 2] = x[cvTm + 1]; x[cvTm + 3] = r.range(0.5, 1.0);
+  x[cvFriction] = r.range(0.3, 0.9);
+  {
+    // tangents from the normal, as prepare builds them
+    ad::PlainIn<double> in{&x[cvN]};
+    ad::TV3<double> n = ad::in3<double>(in, 0);
+    ad::TV3<double> t1 = ad::perp(n), t2 = ad::cross(t1, n);
+    x[cvT1] = t1.x; x[cvT1 + 1] = t1.y; x[cvT1 + 2] = t1.z;
+    x[cvT2] = t2.x; x[cvT2 + 1] = t2.y; x[cvT2 + 2] = t2.z;
+  }
+  for (int q = 0; q < 4; ++q) {
+    for (int f = 0; f < 6; ++f) x[cv_point(q, f)] = r.range(-0.5, 0.5);
+    x[cv_point(q, 6)] = r.range(-0.02, 0.01);
+    x[cv_point(q, 7)] = r.range(0.3, 1.0);
+    x[cv_point(q, 8)] = r.range(0.05, 0.7);
+  }
+}
+
+}  // namespace
+
+extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
+  using namespace ad;
+  if (!worst) return NS_ERR_INVALID;
+  Rng64 r{0x9E3779B97F4A7C15ull ^ ((uint64_t)seed * 0xD1B54A32D192ED03ull + 1)};
+  CParams cp;
+  cp.pc = 4; cp.is_static = seed & 1;
+  float h = 1.0f / 240.0f;
+  cp.inv_h = 240.0f; cp.contact_speed = 3.0f;
+  cp.contact_softness = make_soft(30.0f, 10.0f, h);
+  cp.static_softness = make_soft(60.0f, 5.0f, h);
+  std::vector<double> x;
+  double e = -1.0;
+  switch (which) {
+    case 0:  // warm start
+      random_constraint(r, x);
+      e = vjp_fd_error(x, kWarmOut, [&](const auto& in, auto* y) { warm_fn(in, cp, y); }, r);
+      break;
+    case 1:  // push
+      random_constraint(r, x);
+      e = vjp_fd_error(x, kPushOut, [&](const auto& in, auto* y) { push_fn(in, cp, y); }, r);
+      break;
+    case 2:  // relax
+      random_constraint(r, x);
+      e = vjp_fd_error(x, kRelaxOut, [&](const auto& in, auto* y) { relax_fn(in, cp, y); }, r);
+      break;
+    case 3: {  // prepare
+      x.assign(kPI, 0.0);
+      random_unit(r, &x[piN], 3);
+      for (int q = 0; q < 4; ++q) {
+        for (int f = 0; f < 6; ++f) x[pi_point(q, f)] = r.range(-0.5, 0.5);
+        x[pi_point(q, 6)] = r.range(-0.02, 0.015);
+        x[pi_point(q, 7)] = r.range(0.0, 1.0);
+      }
+      for (int f = 0; f < 3; ++f) x[piFrictionImpulse + f] = r.range(-0.2, 0.2);
+      x[piTwist] = r.range(-0.05, 0.05);
+      x[piIma] = r.range(0.5, 2.0); x[piImb] = r.range(0.5, 2.0);
+      random_spd(r, &x[piSa]); random_spd(r, &x[piSb]);
+      x[piFriction] = r.range(0.3, 0.9);
+      PParams pp = {4, 0, 1.0f};
+      e = vjp_fd_error(x, kCVOwn, [&](const auto& in, auto* y) { prepare_fn(in, pp, y); }, r);
+      break;
+    }
+    case 4: {  // integrate velocities
+      x.assign(kIVIn, 0.0);
+      for (int i = 0; i < 6; ++i) x[i] = r.range(-2.0, 2.0);
+      x[6] = r.range(0.5, 2.0);
+      for (int i = 0; i < 9; ++i) x[7 + i] = r.range(-0.2, 0.2) + ((i % 4) == 0 ? 1.0 : 0.0);
+      for (int i = 16; i < 22; ++i) x[i] = r.range(-5.0, 5.0);
+      random_unit(r, &x[22], 4);
+      x[26] = r.range(-0.02, 0.02); x[27] = r.range(-0.02, 0.02); x[28] = r.range(-0.02, 0.02); x[29] = 1.0;
+      {
+        double s6[6];
+        random_spd(r, s6);
+        const int at[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int i = 0; i < 9; ++i) x[30 + i] = s6[at[i]];
+      }
+      BParams bp = {};
+      bp.h = h; bp.lin_damp = 0.1f; bp.ang_damp = 0.05f; bp.grav_scale = 1.0f; bp.gravity = v3(0, -9.81f, 0);
+      bp.flags = (seed & 1) ? kGyroscopic : 0u;  // odd seeds take the gyroscopic step
+      e = vjp_fd_error(x, kIVOut, [&](const auto& in, auto* y) { iv_fn(in, bp, y); }, r);
+      break;
+    }
+    case 5: {  // integrate positions
+      x.assign(kIP, 0.0);
+      for (int i = 0; i < 6; ++i) x[i] = r.range(-3.0, 3.0);
+      for (int i = 6; i < 9; ++i) x[i] = r.range(-0.05, 0.05);
+      random_unit(r, &x[9], 4);
+      BParams bp = {};
+      bp.h = h; bp.inv_dt = 60.0f; bp.max_linear_speed = (seed & 1) ? 1.0f : 400.0f;  // odd seeds cap the speed
+      e = vjp_fd_error(x, kIP, [&](const auto& in, auto* y) { ip_fn(in, bp, y); }, r);
+      break;
+    }
+    case 6: {  // finalize rotation
+      x.assign(8, 0.0);
+      random_unit(r, &x[0], 4);
+      x[4] = r.range(-0.02, 0.02); x[5] = r.range(-0.02, 0.02); x[6] = r.range(-0.02, 0.02); x[7] = 1.0;
+      e = vjp_fd_error(x, 4, [&](const auto& in, auto* y) { final_rot_fn(in, y); }, r);
+      break;
+    }
+    case 7: {  // inverse world inertia
+      x.assign(13, 0.0);
+      random_unit(r, &x[0], 4);
+      for (int i = 0; i < 9; ++i) x[4 + i] = r.range(-0.1, 0.1) + ((i % 4) == 0 ? 1.0 : 0.0);
+      e = vjp_fd_error(x, 9, [&](const auto& in, auto* y) { inv_inertia_fn(in, y); }, r);
+      break;
+    }
+    case 8: {  // recycled separations
+      x.assign(kRI, 0.0);
+      for (int i = 0; i < 6; ++i) x[i] = 0.0;
+      for (int b = 0; b < 4; ++b) random_unit(r, &x[riQa + 4 * b], 4);
+      random_unit(r, &x[riN], 3);
+      for (int q = 0; q < 4; ++q) {
+        for (int f = 0; f < 6; ++f) x[ri_point(q, f)] = r.range(-0.5, 0.5);
+        x[ri_point(q, 6)] = r.range(-0.02, 0.02);
+      }
+      Pos ca = {r.range(-5, 5), r.range(0, 5), r.range(-5, 5)};
+      Pos cb = {ca.x + r.range(-1, 1), ca.y + r.range(-1, 1), ca.z + r.range(-1, 1)};
+      e = vjp_fd_error(x, 4, [&](const auto& in, auto* y) { recycle_fn(in, ca, cb, 4, y); }, r);
+      break;
+    }
+    case 9: case 10: case 11: {  // box-box narrowphase replay: face contact (9), any axis (10), edges (11)
+      Hull ha = make_box_hull(2.0f, 0.5f, 2.0f), hb = make_box_hull(0.5f, 0.4f, 0.3f);
+      x.assign(kFI, 0.0);
+      Pos ca = {0.0, 0.0, 0.0};
+      double tilt = which == 9 ? 0.05 : 0.6;
+      double qa[4], qb[4];
+      qa[0] = r.range(-0.02, 0.02); qa[1] = r.range(-0.02, 0.02); qa[2] = r.range(-0.02, 0.02);
+      qa[3] = std::sqrt(1 - qa[0] * qa[0] - qa[1] * qa[1] - qa[2] * qa[2]);
+      qb[0] = r.range(-tilt, tilt); qb[1] = r.range(-tilt, tilt); qb[2] = r.range(-tilt, tilt);
+      double l = std::sqrt(qb[0] * qb[0] + qb[1] * qb[1] + qb[2] * qb[2] + 1.0);
+      for (int i = 0; i < 3; ++i) qb[i] /= l;
+      qb[3] = 1.0 / l;
+      for (int i = 0; i < 4; ++i) { x[fiQa + i] = qa[i]; x[fiQb + i] = qb[i]; }
+      // place B just touching the top face of A
+      Q qbf = {v3((float)qb[0], (float)qb[1], (float)qb[2]), (float)qb[3]};
+      float low = 1e30f;
+      for (int v = 0; v < 8; ++v) low = std::min(low, nsd::rotate(qbf, hb.points[v]).y);
+      Pos cb = {r.range(-0.5, 0.5), 0.5 - (double)low - 0.005, r.range(-0.5, 0.5)};
+      if (which == 11) {
+        // B turned 45 degrees about x, then -25 degrees about z: its edge along the turned x
+        // axis, sloping down towards +x, is placed across A's top edge (x = 2, y = 0.5) with a
+        // gap of 3 mm along the edge pair's normal, so the separating axis is an edge pair.
+        double th = -25.0 * M_PI / 180.0 * 0.5, ph = 45.0 * M_PI / 180.0 * 0.5;
+        double qz[4] = {0, 0, std::sin(th), std::cos(th)}, qx[4] = {std::sin(ph), 0, 0, std::cos(ph)};
+        qb[0] = qz[3] * qx[0] + qz[0] * qx[3] + qz[1] * qx[2] - qz[2] * qx[1];
+        qb[1] = qz[3] * qx[1] - qz[0] * qx[2] + qz[1] * qx[3] + qz[2] * qx[0];
+        qb[2] = qz[3] * qx[2] + qz[0] * qx[1] - qz[1] * qx[0] + qz[2] * qx[3];
+        qb[3] = qz[3] * qx[3] - qz[0] * qx[0] - qz[1] * qx[1] - qz[2] * qx[2];
+        qb[0] += r.range(-0.005, 0.005); qb[1] += r.range(-0.005, 0.005);
+        double lq = std::sqrt(qb[0] * qb[0] + qb[1] * qb[1] + qb[2] * qb[2] + qb[3] * qb[3]);
+        for (int i = 0; i < 4; ++i) { qb[i] /= lq; x[fiQb + i] = qb[i]; }
+        qbf = Q{v3((float)qb[0], (float)qb[1], (float)qb[2]), (float)qb[3]};
+        double a25 = 25.0 * M_PI / 180.0;
+        V3 nrm = v3((float)std::sin(a25), (float)std::cos(a25), 0.0f);
+        float best = -1e30f;
+        for (int v = 0; v < 8; ++v) best = std::max(best, -nsd::dot(nsd::rotate(qbf, hb.points[v]), nrm));
+        V3 mid = v3(0, 0, 0);
+        int cnt = 0;
+        for (int v = 0; v < 8; ++v) {
+          V3 pv = nsd::rotate(qbf, hb.points[v]);
+          if (-nsd::dot(pv, nrm) > best - 1e-3f) { mid = mid + pv; ++cnt; }
+        }
+        mid = (1.0f / (float)cnt) * mid;
+        double gap = 0.003;
+        cb = {2.0 + gap * nrm.x - mid.x, 0.5 + gap * nrm.y - mid.y, r.range(-0.5, 0.5) - mid.z};
+      }
+      WXf xa = {ca, Q{v3((float)qa[0], (float)qa[1], (float)qa[2]), (float)qa[3]}}, xbw = {cb, qbf};
+      Xf b2a = inv_mul_wxf(xa, xbw);
+      LocalManifold lm;
+      SATCache cache;
+      collide_hulls(&lm, ha, hb, b2a, &cache, nullptr);
+      if (lm.point_count == 0) { e = 0.0; break; }
+      NarrowCase nc = {cache.type, cache.index_a, cache.index_b, cache.hit};
+      worst[1] = (double)cache.type;
+      int pc = -1;
+      {
+        ad::PlainIn<double> in{x.data()};
+        double y[kFO];
+        pc = narrow_box_fn(in, ca, cb, ha, hb, nc, y);
+      }
+      if (pc < 1) return fail(nullptr, NS_ERR_INVALID, "narrowphase replay found no manifold");
+      e = vjp_fd_error(x, 3 + 7 * pc,
+                       [&](const auto& in, auto* y) { narrow_box_fn(in, ca, cb, ha, hb, nc, y); }, r);
+      break;
+    }
+    default:
+      return fail(nullptr, NS_ERR_INVALID, "unknown check %d", which);
+  }
+  *worst = e;
+  return NS_OK;
+}
+
+namespace {
 }  // namespace
 
 // Fixed device scratch of ns_collide_pairs_noalloc: the device copies of one call's jobs
@@ -846,6 +1343,7 @@ void ns_world_destroy(ns_world* w) {
     cudaStreamSynchronize(w->stream);
     if (w->graph_exec) cudaGraphExecDestroy(w->graph_exec);
     if (w->graph) cudaGraphDestroy(w->graph);
+    free_tape(w);
     for (void* p : w->allocations) cudaFree(p);
     if (w->host_ctl) cudaFreeHost(w->host_ctl);
     if (w->host_in) cudaFreeHost(w->host_in);
@@ -991,8 +1489,18 @@ int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa
   return (int)w->joints.size() - 1;
 }
 
+static int world_step(ns_world* w, float dt, int substeps);
+
 int ns_world_step(ns_world* w, float dt, int substeps) {
   if (!w) return NS_ERR_INVALID;
+  bool rec = w->tape && w->tape->recording;
+  if (rec && !(dt > 0.0f)) return fail(w, NS_ERR_UNSUPPORTED, "a recording tape needs dt > 0");
+  int st = world_step(w, dt, substeps);
+  if (st || !rec) return st;
+  return tape_after_step(w, dt, substeps < 1 ? 1 : substeps);
+}
+
+static int world_step(ns_world* w, float dt, int substeps) {
   if (!(dt >= 0.0f)) return fail(w, NS_ERR_INVALID, "dt must be >= 0");
   if (!w->uploaded) {
     int st = upload_world(w);
@@ -1066,6 +1574,8 @@ int ns_world_synchronize(ns_world* w) {
 int ns_world_body_count(const ns_world* w) { return w ? (int)w->bodies.size() : -1; }
 
 int ns_world_apply_forces(ns_world* w, const float* force, const float* torque) {
+  if (w && w->tape && w->tape->recording)
+    return fail(w, NS_ERR_UNSUPPORTED, "forces cannot be applied while a tape records");
   if (!w) return NS_ERR_INVALID;
   int nb = (int)w->bodies.size();
   if (nb == 0 || (!force && !torque)) return NS_OK;
@@ -1400,6 +1910,182 @@ int ns_selftest_barrier_timeout(int device, int timeout_ms) {
   if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "barrier self-test: %s", cudaGetErrorString(e));
   if (c.error == kErrTimeout) return fail(nullptr, NS_ERR_TIMEOUT, "grid barrier gave up after %d ms as designed", timeout_ms);
   return fail(nullptr, NS_ERR_INVALID, "barrier self-test did not time out (error %d)", c.error);
+}
+
+
+int ns_world_tape_begin(ns_world* w, int checkpoint_substeps) {
+  if (!w) return NS_ERR_INVALID;
+  if (checkpoint_substeps < 1) return fail(w, NS_ERR_INVALID, "checkpoint_substeps must be >= 1");
+  if (!w->uploaded) {
+    int st = upload_world(w);
+    if (st) return st;
+  }
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  int st = check_adjoint_scope(w);
+  if (st) return st;
+  free_tape(w);
+  w->tape = new AdTape();
+  w->tape->every = checkpoint_substeps;
+  w->tape->ckpt.emplace_back();
+  st = take_checkpoint(w, &w->tape->ckpt.back());
+  if (st) { free_tape(w); return st; }
+  w->tape->ckpt_at.push_back(0);
+  w->tape->recording = true;
+  return NS_OK;
+}
+
+int ns_world_tape_end(ns_world* w) {
+  if (!w) return NS_ERR_INVALID;
+  if (!w->tape) return fail(w, NS_ERR_INVALID, "no tape");
+  w->tape->recording = false;
+  return NS_OK;
+}
+
+int ns_world_tape_free(ns_world* w) {
+  if (!w) return NS_ERR_INVALID;
+  free_tape(w);
+  return NS_OK;
+}
+
+int ns_world_tape_info(ns_world* w, int64_t* out) {
+  if (!w || !out) return NS_ERR_INVALID;
+  for (int i = 0; i < 6; ++i) out[i] = 0;
+  if (!w->tape) return NS_OK;
+  const AdTape* t = w->tape;
+  out[0] = (int64_t)t->steps.size();
+  out[1] = (int64_t)t->ckpt.size();
+  out[2] = t->replay_mismatch;
+  out[3] = t->vjp_calls;
+  out[4] = t->recording ? 1 : 0;
+  out[5] = t->every;
+  return NS_OK;
+}
+
+int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
+                 float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0) {
+  if (!w) return NS_ERR_INVALID;
+  if (!w->tape || w->tape->steps.empty()) return fail(w, NS_ERR_INVALID, "no recorded steps");
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  AdTape* tp = w->tape;
+  tp->recording = false;
+  tp->vjp_calls++;
+  const DW& d = w->dw;
+  const int nb = (int)w->bodies.size(), n = d.n_awake, cap = d.cap;
+  auto blocks = [](int count, int t) { return std::max(1, (count + t - 1) / t); };
+  static bool dirs_ready[64] = {};
+  if (w->def.device >= 0 && w->def.device < 64 && !dirs_ready[w->def.device]) {
+    StageDirs sd = make_stage_dirs();
+    NS_CUDA(w, cudaMemcpyToSymbol(c_dirs, &sd, sizeof(sd)));
+    dirs_ready[w->def.device] = true;
+  }
+  // segments between checkpoints
+  std::vector<std::pair<int, int>> segs;
+  for (size_t c = 0; c < tp->ckpt_at.size(); ++c) {
+    int a = tp->ckpt_at[c];
+    int b = c + 1 < tp->ckpt_at.size() ? tp->ckpt_at[c + 1] : (int)tp->steps.size();
+    segs.push_back({a, b});
+  }
+  int max_len = 0, max_sub = 1;
+  for (auto& sg : segs) max_len = std::max(max_len, sg.second - sg.first);
+  for (const AdStepRec& r : tp->steps) max_sub = std::max(max_sub, r.substeps);
+  AdCheckpoint final_state;
+  TapeSet ts;
+  char* buf = nullptr;
+  int st = NS_OK;
+  std::vector<float> host_out((size_t)16 * std::max(nb, 1));
+  do {
+    if ((st = take_checkpoint(w, &final_state))) break;
+    if ((st = alloc_tapes(w, std::max(max_len, 1), max_sub, &ts))) break;
+    // cotangent buffers and staging
+    size_t o = 0;
+    auto take = [&](size_t b) { size_t r = o; o += align256(b); return r; };
+    size_t o_bb = take(sizeof(float) * 16 * (size_t)n), o_cq = take(sizeof(float) * 8 * (size_t)n);
+    size_t o_pb = take(sizeof(float) * kPB * (size_t)n), o_kb = take(sizeof(float) * ad::kCVOwn * (size_t)cap);
+    size_t o_mb = take(sizeof(float) * kMB * (size_t)cap), o_mis = take(sizeof(int));
+    size_t o_seed = take(sizeof(float) * 13 * (size_t)nb), o_out = take(sizeof(float) * 16 * (size_t)nb);
+    if (cudaMalloc(&buf, o) != cudaSuccess) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
+    NS_CUDA(w, cudaMemsetAsync(buf, 0, o, w->stream));
+    AdjBufs a;
+    a.bb = (float*)(buf + o_bb); a.cq = (float*)(buf + o_cq); a.pb = (float*)(buf + o_pb);
+    a.kb = (float*)(buf + o_kb); a.mb = (float*)(buf + o_mb); a.mismatch = (int*)(buf + o_mis);
+    a.cap = cap; a.n_awake = n;
+    float* seed = (float*)(buf + o_seed);
+    float* dev_out = (float*)(buf + o_out);
+    const float* src[4] = {dpos, drot, dlin, dang};
+    const int width[4] = {3, 4, 3, 3};
+    float* dst[4] = {seed, seed + 3 * (size_t)nb, seed + 7 * (size_t)nb, seed + 10 * (size_t)nb};
+    for (int i = 0; i < 4; ++i)
+      if (src[i]) NS_CUDA(w, cudaMemcpyAsync(dst[i], src[i], sizeof(float) * width[i] * (size_t)nb, cudaMemcpyHostToDevice, w->stream));
+    k_adj_seed<<<blocks(nb, 256), 256, 0, w->stream>>>(a, w->body_loc, nb, src[0] ? dst[0] : nullptr,
+                                                        src[1] ? dst[1] : nullptr, src[2] ? dst[2] : nullptr,
+                                                        src[3] ? dst[3] : nullptr);
+    for (int sgi = (int)segs.size() - 1; sgi >= 0 && st == NS_OK; --sgi) {
+      int s0 = segs[sgi].first, s1 = segs[sgi].second;
+      if (s1 <= s0) continue;
+      if ((st = restore_checkpoint(w, tp->ckpt[sgi]))) break;
+      for (int j = s0; j < s1 && st == NS_OK; ++j) {
+        HostStepTape& h = ts.steps[j - s0];
+        h.dev.substeps = tp->steps[j].substeps;
+        st = enqueue_step(w, tp->steps[j].dt, tp->steps[j].substeps, &h);
+      }
+      if (st) break;
+      // the recorded steps must stay inside the adjoint's scope
+      std::vector<Control> ctl(s1 - s0);
+      for (int j = s0; j < s1; ++j)
+        NS_CUDA(w, cudaMemcpyAsync(&ctl[j - s0], ts.steps[j - s0].dev.ctl, sizeof(Control), cudaMemcpyDeviceToHost, w->stream));
+      NS_CUDA(w, cudaStreamSynchronize(w->stream));
+      for (int j = s0; j < s1 && st == NS_OK; ++j) {
+        const Control& c = ctl[j - s0];
+        if (c.error) st = control_status(w, c);
+        else if (c.overflow_count > 0) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has overflow constraints; the adjoint does not cover them", j);
+        else if (c.any_restitution) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has restitution", j);
+      }
+      for (int j = s1 - 1; j >= s0 && st == NS_OK; --j) {
+        const StepTape& t = ts.steps[j - s0].dev;
+        StepParams p = make_step_params(w, tp->steps[j].dt, tp->steps[j].substeps);
+        int n_slots = ctl[j - s0].color_offset[kOverflowIndex];
+        if (n > 0) k_adj_finalize<<<blocks(n, 128), 128, 0, w->stream>>>(t, a, n);
+        if (n_slots > 0) k_adj_store<<<blocks(n_slots, 128), 128, 0, w->stream>>>(t, a, n_slots);
+        if ((st = launch_adj_solve(w, t, a, p))) break;
+        if (n_slots > 0) k_adj_prepare<<<blocks(n_slots, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d, p, n_slots);
+        if (n > 0) k_adj_inertia<<<blocks(n, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a);
+        k_adj_narrow<<<blocks(cap, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d);
+        NS_CUDA(w, cudaGetLastError());
+      }
+    }
+    if (st) break;
+    k_adj_result<<<blocks(nb, 256), 256, 0, w->stream>>>(a, d, w->body_loc, nb, dev_out);
+    NS_CUDA(w, cudaMemcpyAsync(host_out.data(), dev_out, sizeof(float) * 16 * (size_t)nb, cudaMemcpyDeviceToHost, w->stream));
+    int mismatch = 0;
+    NS_CUDA(w, cudaMemcpyAsync(&mismatch, a.mismatch, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+    if ((st = restore_checkpoint(w, final_state))) break;
+    NS_CUDA(w, cudaStreamSynchronize(w->stream));
+    tp->replay_mismatch += mismatch;
+    Control c;
+    if ((st = read_control(w, &c))) break;
+    if ((st = control_status(w, c))) break;
+  } while (0);
+  if (st) {
+    // put the world back even when the reverse pass failed
+    if (final_state.data) { restore_checkpoint(w, final_state); cudaStreamSynchronize(w->stream); }
+  }
+  cudaStreamSynchronize(w->stream);
+  if (final_state.data) cudaFree(final_state.data);
+  if (ts.data) cudaFree(ts.data);
+  if (buf) cudaFree(buf);
+  if (st) return st;
+  for (int i = 0; i < nb; ++i) {
+    const float* o = &host_out[(size_t)16 * i];
+    for (int f = 0; f < 3; ++f) {
+      if (dlin0) dlin0[3 * i + f] = o[f];
+      if (dang0) dang0[3 * i + f] = o[3 + f];
+      if (dpos0) dpos0[3 * i + f] = o[8 + f];
+    }
+    for (int f = 0; f < 4; ++f) if (drot0) drot0[4 * i + f] = o[11 + f];
+    if (dmass) dmass[i] = o[6];
+    if (dfriction) dfriction[i] = o[7];
+  }
+  return NS_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,1005 @@
+// Differentiable restatement of the step's local functions, for the vector-Jacobian product
+// of a rollout (the adjoint).
+//
+// Every function here is a template over its scalar type T and repeats, operation for
+// operation, the f32 code of the forward kernels it mirrors (the functions named beside each
+// one). Instantiated with a dual number Dual<R, K> it carries K directional derivatives next
+// to the value: its value part performs the same IEEE operations in the same order as the
+// forward kernel, so for R = float every comparison takes the branch the forward step took,
+// and the derivative parts are the exact derivatives of that branch. The adjoint kernels seed
+// one input direction per warp lane, evaluate a local function once, and contract the output
+// derivatives with the incoming cotangent, which yields one component of the local
+// vector-Jacobian product per direction. With R = double the same code is the FP64 check.
+#pragma once
+#include "nsd_types.cuh"
+
+namespace nsd {
+namespace ad {
+
+NSD_HD float rsqrt_(float a) { return sqrtf(a); }
+NSD_HD double rsqrt_(double a) { return sqrt(a); }
+
+// ---------------------------------------------------------------------------------------------
+// Dual numbers: value v and K tangents d.
+template <class R, int K>
+struct Dual {
+  R v;
+  R d[K];
+  NSD_HD Dual() {}
+  NSD_HD Dual(R x) : v(x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) d[k] = R(0);
+  }
+  friend NSD_HD Dual operator+(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] + b.d[k];
+    return r;
+  }
+  friend NSD_HD Dual operator-(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] - b.d[k];
+    return r;
+  }
+  friend NSD_HD Dual operator-(const Dual& a) {
+    Dual r;
+    r.v = -a.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = -a.d[k];
+    return r;
+  }
+  friend NSD_HD Dual operator*(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+    return r;
+  }
+  friend NSD_HD Dual operator/(const Dual& a, const Dual& b) {
+    Dual r;
+    r.v = a.v / b.v;
+    R ib = R(1) / b.v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * ib;
+    return r;
+  }
+  friend NSD_HD bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+  friend NSD_HD bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+  friend NSD_HD bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
+  friend NSD_HD bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
+  friend NSD_HD bool operator==(const Dual& a, const Dual& b) { return a.v == b.v; }
+  friend NSD_HD Dual tsqrt(const Dual& a) {
+    Dual r;
+    r.v = rsqrt_(a.v);
+    R s = r.v > R(0) ? R(0.5) / r.v : R(0);
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = a.d[k] * s;
+    return r;
+  }
+  friend NSD_HD R val(const Dual& a) { return a.v; }
+};
+
+NSD_HD float tsqrt(float a) { return sqrtf(a); }
+NSD_HD double tsqrt(double a) { return sqrt(a); }
+NSD_HD float val(float a) { return a; }
+NSD_HD double val(double a) { return a; }
+
+// functions.rs:16-60 semantics: ties return the second operand.
+template <class T> NSD_HD T tmin(const T& a, const T& b) { return a < b ? a : b; }
+template <class T> NSD_HD T tmax(const T& a, const T& b) { return a > b ? a : b; }
+template <class T> NSD_HD T tabs(const T& a) { return a < T(0.0f) ? -a : a; }
+template <class T> NSD_HD T tclamp(const T& a, const T& lo, const T& hi) { return a < lo ? lo : (hi < a ? hi : a); }
+
+// ---------------------------------------------------------------------------------------------
+// Vectors, quaternions and matrices over T (nsd_math.cuh, same association order).
+template <class T> struct TV2 { T x, y; };
+template <class T> struct TV3 { T x, y, z; };
+template <class T> struct TQ { TV3<T> v; T s; };
+template <class T> struct TM3 { TV3<T> cx, cy, cz; };
+template <class T> struct TM2 { TV2<T> cx, cy; };
+template <class T> struct TSym { T xx, xy, xz, yy, yz, zz; };
+template <class T> struct TXf { TV3<T> p; TQ<T> q; };
+template <class T> struct TPlane { TV3<T> n; T off; };
+
+template <class T> NSD_HD TV3<T> tv3(const T& x, const T& y, const T& z) { TV3<T> r = {x, y, z}; return r; }
+template <class T> NSD_HD TV3<T> tv3(V3 a) { return tv3<T>(T(a.x), T(a.y), T(a.z)); }
+template <class T> NSD_HD TV3<T> tzero3() { return tv3<T>(T(0.0f), T(0.0f), T(0.0f)); }
+template <class T> NSD_HD TQ<T> tquat(TV3<T> v, const T& s) { TQ<T> r = {v, s}; return r; }
+template <class T> NSD_HD TQ<T> tqid() { return tquat<T>(tzero3<T>(), T(1.0f)); }
+template <class T> NSD_HD TM3<T> tm3(TV3<T> a, TV3<T> b, TV3<T> c) { TM3<T> r = {a, b, c}; return r; }
+template <class T> NSD_HD TM3<T> tm3(const M3& m) { return tm3<T>(tv3<T>(m.cx), tv3<T>(m.cy), tv3<T>(m.cz)); }
+template <class T> NSD_HD TPlane<T> tplane(const Plane& p) { TPlane<T> r = {tv3<T>(p.n), T(p.off)}; return r; }
+
+template <class T> NSD_HD TV3<T> operator+(const TV3<T>& a, const TV3<T>& b) { return tv3<T>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class T> NSD_HD TV3<T> operator-(const TV3<T>& a, const TV3<T>& b) { return tv3<T>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class T> NSD_HD TV3<T> operator-(const TV3<T>& a) { return tv3<T>(-a.x, -a.y, -a.z); }
+template <class T> NSD_HD TV3<T> operator*(const T& s, const TV3<T>& a) { return tv3<T>(s * a.x, s * a.y, s * a.z); }
+
+template <class T> NSD_HD T dot(const TV3<T>& a, const TV3<T>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> NSD_HD T length(const TV3<T>& v) { return tsqrt(dot(v, v)); }
+template <class T> NSD_HD T length_sq(const TV3<T>& a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+template <class T> NSD_HD TV3<T> normalize(const TV3<T>& a) {
+  T ls = a.x * a.x + a.y * a.y + a.z * a.z;
+  if (ls > T(1000.0f * kMinPositive)) {
+    T s = T(1.0f) / tsqrt(ls);
+    return tv3<T>(s * a.x, s * a.y, s * a.z);
+  }
+  return tzero3<T>();
+}
+template <class T> NSD_HD TV3<T> perp(const TV3<T>& a) {
+  TV3<T> p = (a.x < T(-0.5f) || T(0.5f) < a.x) ? tv3<T>(a.y, -a.x, T(0.0f)) : tv3<T>(T(0.0f), a.z, -a.y);
+  return normalize(p);
+}
+template <class T> NSD_HD TV3<T> mul_add(const TV3<T>& a, const T& s, const TV3<T>& b) {
+  return tv3<T>(a.x + s * b.x, a.y + s * b.y, a.z + s * b.z);
+}
+template <class T> NSD_HD TV3<T> mul_sub(const TV3<T>& a, const T& s, const TV3<T>& b) {
+  return tv3<T>(a.x - s * b.x, a.y - s * b.y, a.z - s * b.z);
+}
+template <class T> NSD_HD TV3<T> cross(const TV3<T>& a, const TV3<T>& b) {
+  return tv3<T>(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <class T> NSD_HD TV3<T> lerp(const TV3<T>& a, const TV3<T>& b, const T& t) {
+  return tv3<T>((T(1.0f) - t) * a.x + t * b.x, (T(1.0f) - t) * a.y + t * b.y, (T(1.0f) - t) * a.z + t * b.z);
+}
+template <class T> NSD_HD TV3<T> blend2(const T& s, const TV3<T>& a, const T& t, const TV3<T>& b) {
+  return tv3<T>(s * a.x + t * b.x, s * a.y + t * b.y, s * a.z + t * b.z);
+}
+template <class T> NSD_HD TV3<T> rotate(const TQ<T>& q, const TV3<T>& v) {
+  TV3<T> t1 = cross(q.v, v);
+  TV3<T> t2 = mul_add(t1, q.s, v);
+  TV3<T> t3 = cross(q.v, t2);
+  return mul_add(v, T(2.0f), t3);
+}
+template <class T> NSD_HD TV3<T> inv_rotate(const TQ<T>& q, const TV3<T>& v) {
+  TV3<T> t1 = cross(q.v, v);
+  TV3<T> t2 = mul_sub(t1, q.s, v);
+  TV3<T> t3 = cross(q.v, t2);
+  return mul_add(v, T(2.0f), t3);
+}
+// nsd_types.cuh inv_rotate_wide (contact_solver.rs:291)
+template <class T> NSD_HD TV3<T> inv_rotate_wide(const TQ<T>& q, const TV3<T>& a) {
+  TV3<T> t0 = cross(q.v, a);
+  TV3<T> t = tv3<T>(t0.x + t0.x, t0.y + t0.y, t0.z + t0.z);
+  TV3<T> u = cross(q.v, t);
+  return tv3<T>((a.x - q.s * t.x) + u.x, (a.y - q.s * t.y) + u.y, (a.z - q.s * t.z) + u.z);
+}
+template <class T> NSD_HD T dot_quat(const TQ<T>& a, const TQ<T>& b) {
+  return a.v.x * b.v.x + a.v.y * b.v.y + a.v.z * b.v.z + a.s * b.s;
+}
+template <class T> NSD_HD TQ<T> mul_quat(const TQ<T>& q1, const TQ<T>& q2) {
+  TV3<T> t1 = cross(q1.v, q2.v);
+  TV3<T> t2 = mul_add(t1, q1.s, q2.v);
+  TV3<T> t3 = mul_add(t2, q2.s, q1.v);
+  return tquat<T>(t3, q1.s * q2.s - dot(q1.v, q2.v));
+}
+template <class T> NSD_HD TQ<T> inv_mul_quat(const TQ<T>& q1, const TQ<T>& q2) {
+  TV3<T> t1 = cross(q2.v, q1.v);
+  TV3<T> t2 = mul_add(t1, q1.s, q2.v);
+  TV3<T> t3 = mul_sub(t2, q2.s, q1.v);
+  return tquat<T>(t3, q1.s * q2.s + dot(q1.v, q2.v));
+}
+template <class T> NSD_HD TQ<T> conjugate(const TQ<T>& q) { return tquat<T>(tv3<T>(-q.v.x, -q.v.y, -q.v.z), q.s); }
+template <class T> NSD_HD TQ<T> normalize_quat(const TQ<T>& q) {
+  T ls = dot_quat(q, q);
+  if (ls > T(1000.0f * kMinPositive)) {
+    T s = T(1.0f) / tsqrt(ls);
+    return tquat<T>(tv3<T>(s * q.v.x, s * q.v.y, s * q.v.z), s * q.s);
+  }
+  return tqid<T>();
+}
+template <class T> NSD_HD TQ<T> integrate_rotation(const TQ<T>& q1, const TV3<T>& dr) {
+  TQ<T> qd = mul_quat(tquat<T>(T(0.5f) * dr, T(0.0f)), q1);
+  return normalize_quat(tquat<T>(q1.v + qd.v, qd.s + q1.s));
+}
+template <class T> NSD_HD TXf<T> invert_xf(const TXf<T>& t) {
+  TXf<T> r = {inv_rotate(t.q, -t.p), conjugate(t.q)};
+  return r;
+}
+template <class T> NSD_HD TV3<T> xf_point(const TXf<T>& t, const TV3<T>& v) { return rotate(t.q, v) + t.p; }
+template <class T> NSD_HD TM3<T> matrix_from_quat(const TQ<T>& q) {
+  T xx = q.v.x * q.v.x, yy = q.v.y * q.v.y, zz = q.v.z * q.v.z;
+  T xy = q.v.x * q.v.y, xz = q.v.x * q.v.z, xw = q.v.x * q.s;
+  T yz = q.v.y * q.v.z, yw = q.v.y * q.s, zw = q.v.z * q.s;
+  const T one(1.0f), two(2.0f);
+  return tm3<T>(tv3<T>(one - two * (yy + zz), two * (xy + zw), two * (xz - yw)),
+                tv3<T>(two * (xy - zw), one - two * (xx + zz), two * (yz + xw)),
+                tv3<T>(two * (xz + yw), two * (yz - xw), one - two * (xx + yy)));
+}
+template <class T> NSD_HD TV3<T> mul_mv(const TM3<T>& m, const TV3<T>& a) {
+  return tv3<T>(m.cx.x * a.x + m.cy.x * a.y + m.cz.x * a.z,
+                m.cx.y * a.x + m.cy.y * a.y + m.cz.y * a.z,
+                m.cx.z * a.x + m.cy.z * a.y + m.cz.z * a.z);
+}
+template <class T> NSD_HD TM3<T> mul_mm(const TM3<T>& a, const TM3<T>& b) {
+  return tm3<T>(mul_mv(a, b.cx), mul_mv(a, b.cy), mul_mv(a, b.cz));
+}
+template <class T> NSD_HD TM3<T> transpose(const TM3<T>& m) {
+  return tm3<T>(tv3<T>(m.cx.x, m.cy.x, m.cz.x), tv3<T>(m.cx.y, m.cy.y, m.cz.y), tv3<T>(m.cx.z, m.cy.z, m.cz.z));
+}
+template <class T> NSD_HD TV3<T> sym_mv(const TSym<T>& s, const TV3<T>& a) {
+  return tv3<T>(s.xx * a.x + (s.xy * a.y + s.xz * a.z), s.xy * a.x + (s.yy * a.y + s.yz * a.z),
+                s.xz * a.x + (s.yz * a.y + s.zz * a.z));
+}
+template <class T> NSD_HD TSym<T> sym_add(const TSym<T>& a, const TSym<T>& b) {
+  TSym<T> s = {a.xx + b.xx, a.xy + b.xy, a.xz + b.xz, a.yy + b.yy, a.yz + b.yz, a.zz + b.zz};
+  return s;
+}
+template <class T> NSD_HD TV2<T> mul_mv2(const TM2<T>& m, const TV2<T>& a) {
+  TV2<T> r = {m.cx.x * a.x + m.cy.x * a.y, m.cx.y * a.x + m.cy.y * a.y};
+  return r;
+}
+template <class T> NSD_HD T plane_sep(const TPlane<T>& p, const TV3<T>& x) { return dot(p.n, x) - p.off; }
+
+// A world-space difference of f64 centres, rounded to f32 like sub_pos, plus the difference of
+// the two centres' offsets ta - tb. The adjoint passes zero offsets (the value stays sub_pos's
+// bits) whose tangents carry the centres' perturbations.
+template <class T> NSD_HD TV3<T> sub_pos_t(const Pos& a, const Pos& b, const TV3<T>& ta, const TV3<T>& tb) {
+  V3 r = sub_pos(a, b);
+  TV3<T> t = ta - tb;
+  return tv3<T>(t.x + T(r.x), t.y + T(r.y), t.z + T(r.z));
+}
+
+template <class T> NSD_HD V3 real3(const TV3<T>& a) { return v3((float)val(a.x), (float)val(a.y), (float)val(a.z)); }
+
+// ---------------------------------------------------------------------------------------------
+// Input access: a local function reads input i as in(i). Plain evaluation returns the stored
+// value; a seeded evaluation returns a dual number whose tangent k is 1 when i is the k-th
+// direction of this lane.
+template <class R>
+struct PlainIn {
+  const R* x;
+  NSD_HD R operator()(int i) const { return x[i]; }
+};
+template <class R, int K>
+struct SeedIn {
+  const R* x;
+  int dir[K];
+  NSD_HD Dual<R, K> operator()(int i) const {
+    Dual<R, K> r(x[i]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) r.d[k] = dir[k] == i ? R(1) : R(0);
+    return r;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Constraint vector layout (one contact constraint; shared by warm start, push, relax and the
+// output of prepare). Indices below 26 are the two bodies' solver state.
+enum CV : int {
+  cvVA = 0, cvWA = 3, cvVB = 6, cvWB = 9, cvDpA = 12, cvDpB = 15, cvDqA = 18, cvDqB = 22,
+  cvLam = 26, cvFr = 30, cvTwist = 32,
+  cvIma = 33, cvImb = 34, cvSa = 35, cvSb = 41, cvN = 47, cvT1 = 50, cvT2 = 53, cvTv1 = 56, cvTv2 = 57,
+  cvCa = 58, cvCb = 61, cvTwistMass = 64, cvTm = 65, cvFriction = 69,
+  cvPoint = 70,  // + 9 q: ra 0..2, rb 3..5, base separation 6, normal mass 7, lever 8
+  kCV = 106,
+  kCVOwn = kCV - cvLam,  // the constraint's own entries (impulses and constants)
+};
+NSD_HD int cv_point(int q, int f) { return cvPoint + 9 * q + f; }
+
+template <class T, class In> NSD_HD TV3<T> in3(const In& x, int i) { return tv3<T>(x(i), x(i + 1), x(i + 2)); }
+template <class T, class In> NSD_HD TQ<T> in4(const In& x, int i) { return tquat<T>(tv3<T>(x(i), x(i + 1), x(i + 2)), x(i + 3)); }
+template <class T, class In> NSD_HD TSym<T> in_sym(const In& x, int i) {
+  TSym<T> s = {x(i), x(i + 1), x(i + 2), x(i + 3), x(i + 4), x(i + 5)};
+  return s;
+}
+template <class T> NSD_HD void out3(T* y, int i, const TV3<T>& a) { y[i] = a.x; y[i + 1] = a.y; y[i + 2] = a.z; }
+template <class T> NSD_HD void out4(T* y, int i, const TQ<T>& a) { y[i] = a.v.x; y[i + 1] = a.v.y; y[i + 2] = a.v.z; y[i + 3] = a.s; }
+
+// Parameters of one constraint that are not differentiated.
+struct CParams {
+  int pc;          // manifold points
+  int is_static;   // softness of a static contact
+  float inv_h, contact_speed;
+  Softness contact_softness, static_softness;
+};
+
+// Outputs of warm start: vA wA vB wB (12).
+constexpr int kWarmOut = 12;
+// nsd_solve.cuh warm_start_constraint (contact_solver.rs:697), rolling resistance zero.
+template <class T, class In>
+NSD_HD void warm_fn(const In& x, const CParams& cp, T* y) {
+  TV3<T> t1 = in3<T>(x, cvT1), t2 = in3<T>(x, cvT2);
+  TV3<T> center_a = in3<T>(x, cvCa), center_b = in3<T>(x, cvCb);
+  T twist = x(cvTwist);
+  TV3<T> li = tzero3<T>(), aia = tzero3<T>(), aib = tzero3<T>();
+  T tni = T(0.0f);
+  TV3<T> moa = tzero3<T>(), mob = tzero3<T>();
+  for (int q = 0; q < cp.pc; ++q) {
+    T ni = x(cvLam + q);
+    tni = tni + ni;
+    moa = mul_add(moa, ni, in3<T>(x, cv_point(q, 0)));
+    mob = mul_add(mob, ni, in3<T>(x, cv_point(q, 3)));
+  }
+  TV3<T> n = in3<T>(x, cvN);
+  TV3<T> fi = x(cvFr) * t1;
+  fi = mul_add(fi, x(cvFr + 1), t2);
+  TV3<T> lin = mul_add(fi, tni, n);
+  TV3<T> twi = twist * n;
+  TV3<T> anga = cross(moa, n) + cross(center_a, fi) + twi;
+  TV3<T> angb = cross(mob, n) + cross(center_b, fi) + twi;
+  li = li + lin; aia = aia + anga; aib = aib + angb;
+  TSym<T> sa = in_sym<T>(x, cvSa), sb = in_sym<T>(x, cvSb);
+  T ima = x(cvIma), imb = x(cvImb);
+  out3(y, 3, in3<T>(x, cvWA) - sym_mv(sa, aia));
+  out3(y, 0, in3<T>(x, cvVA) - ima * li);
+  out3(y, 9, in3<T>(x, cvWB) + sym_mv(sb, aib));
+  out3(y, 6, in3<T>(x, cvVB) + imb * li);
+}
+
+// Outputs of push: vA wA vB wB (12), normal impulses (4).
+constexpr int kPushOut = 16;
+// nsd_solve.cuh push_constraint (contact_solver.rs:796)
+template <class T, class In>
+NSD_HD void push_fn(const In& x, const CParams& cp, T* y) {
+  T inv_h = T(cp.inv_h);
+  T cs = T(-cp.contact_speed);
+  const Softness& so = cp.is_static ? cp.static_softness : cp.contact_softness;
+  T br = T(so.mass_scale * so.bias_rate);
+  T ms = T(so.mass_scale);
+  T is = T(so.impulse_scale);
+  TV3<T> va = in3<T>(x, cvVA), wa = in3<T>(x, cvWA), vb = in3<T>(x, cvVB), wb = in3<T>(x, cvWB);
+  TQ<T> dqa = in4<T>(x, cvDqA), dqb = in4<T>(x, cvDqB);
+  TV3<T> dp = in3<T>(x, cvDpB) - in3<T>(x, cvDpA);
+  T ima = x(cvIma), imb = x(cvImb);
+  TSym<T> sa = in_sym<T>(x, cvSa), sb = in_sym<T>(x, cvSb);
+  T im = ima + imb;
+  TV3<T> n = in3<T>(x, cvN);
+  T ns = dot(n, dp);
+  TV3<T> na = inv_rotate_wide(dqa, n), nb = inv_rotate_wide(dqb, n);
+  T lnv = dot(n, vb - va);
+  T mi = T(0.0f);
+  for (int q = 0; q < 4; ++q) y[12 + q] = x(cvLam + q);
+  for (int q = 0; q < cp.pc; ++q) {
+    TV3<T> ra = in3<T>(x, cv_point(q, 0)), rb = in3<T>(x, cv_point(q, 3));
+    T base_sep = x(cv_point(q, 6)), nmass = x(cv_point(q, 7)), nimp = x(cvLam + q);
+    T s = (ns + (dot(nb, rb) - dot(na, ra))) + base_sep;
+    bool sep = s > T(0.0f);
+    T spec_bias = s * inv_h;
+    T ovl = tmax(br * s, cs);
+    T vbias = sep ? spec_bias : ovl;
+    T pms = sep ? T(1.0f) : ms;
+    T pis = sep ? T(0.0f) : is;
+    TV3<T> ua = cross(ra, n), ub = cross(rb, n);
+    TV3<T> ga = sym_mv(sa, ua), gb = sym_mv(sb, ub);
+    T vn = lnv + (dot(ub, wb) - dot(ua, wa));
+    T neg = nmass * (pms * vn + vbias) + pis * nimp;
+    T impulse = tmax(-neg, -nimp);
+    y[12 + q] = nimp + impulse;
+    lnv = lnv + im * impulse;
+    mi = mi + impulse;
+    wa = wa - impulse * ga;
+    wb = wb + impulse * gb;
+  }
+  TV3<T> Pv = mi * n;
+  va = va - ima * Pv;
+  vb = vb + imb * Pv;
+  out3(y, 0, va); out3(y, 3, wa); out3(y, 6, vb); out3(y, 9, wb);
+}
+
+// Outputs of relax: vA wA vB wB (12), normal impulses (4), friction impulse (2), twist (1).
+constexpr int kRelaxOut = 19;
+// nsd_solve.cuh relax_constraint (contact_solver.rs:927), rolling resistance zero.
+template <class T, class In>
+NSD_HD void relax_fn(const In& x, const CParams& cp, T* y) {
+  T inv_h = T(cp.inv_h);
+  const T eps(kEps);
+  TV3<T> va = in3<T>(x, cvVA), wa = in3<T>(x, cvWA), vb = in3<T>(x, cvVB), wb = in3<T>(x, cvWB);
+  TQ<T> dqa = in4<T>(x, cvDqA), dqb = in4<T>(x, cvDqB);
+  TV3<T> dp = in3<T>(x, cvDpB) - in3<T>(x, cvDpA);
+  T ima = x(cvIma), imb = x(cvImb);
+  TSym<T> sa = in_sym<T>(x, cvSa), sb = in_sym<T>(x, cvSb);
+  T im = ima + imb;
+  TV3<T> n = in3<T>(x, cvN);
+  TV3<T> t1 = in3<T>(x, cvT1), t2 = in3<T>(x, cvT2);
+  T ns = dot(n, dp);
+  TV3<T> na = inv_rotate_wide(dqa, n), nb = inv_rotate_wide(dqb, n);
+  TV3<T> dv = vb - va;
+  T lnv = dot(n, dv);
+  T lt1 = dot(t1, dv) - x(cvTv1);
+  T lt2 = dot(t2, dv) - x(cvTv2);
+  T mi = T(0.0f), tni = T(0.0f), ttl = T(0.0f);
+  for (int q = 0; q < 4; ++q) y[12 + q] = x(cvLam + q);
+  for (int q = 0; q < cp.pc; ++q) {
+    TV3<T> ra = in3<T>(x, cv_point(q, 0)), rb = in3<T>(x, cv_point(q, 3));
+    T s = (ns + (dot(nb, rb) - dot(na, ra))) + x(cv_point(q, 6));
+    T vbias = tmax(T(0.0f), s * inv_h);
+    TV3<T> ua = cross(ra, n), ub = cross(rb, n);
+    TV3<T> ga = sym_mv(sa, ua), gb = sym_mv(sb, ub);
+    T vn = lnv + (dot(ub, wb) - dot(ua, wa));
+    T neg = x(cv_point(q, 7)) * (vn + vbias);
+    T old = x(cvLam + q);
+    T impulse = tmax(-neg, -old);
+    T ni = old + impulse;
+    y[12 + q] = ni;
+    tni = tni + ni;
+    ttl = ttl + x(cv_point(q, 8)) * ni;
+    lnv = lnv + im * impulse;
+    mi = mi + impulse;
+    wa = wa - impulse * ga;
+    wb = wb + impulse * gb;
+  }
+  T twist_out, frx, fry;
+  {
+    T ts = dot(n, wb - wa);
+    T ml = x(cvFriction) * ttl;
+    T old = x(cvTwist);
+    T impulse = -(x(cvTwistMass) * ts);
+    impulse = tmax(-ml - old, tmin(impulse, ml - old));
+    twist_out = old + impulse;
+    wa = wa - impulse * sym_mv(sa, n);
+    wb = wb + impulse * sym_mv(sb, n);
+    TV3<T> ra = in3<T>(x, cvCa), rb = in3<T>(x, cvCb);
+    TM2<T> tm;
+    tm.cx.x = x(cvTm); tm.cx.y = x(cvTm + 1);
+    tm.cy.x = x(cvTm + 2); tm.cy.y = x(cvTm + 3);
+    TV3<T> arv = cross(wb, rb) - cross(wa, ra);
+    TV2<T> vt = {lt1 + dot(arv, t1), lt2 + dot(arv, t2)};
+    TV2<T> di = mul_mv2(tm, vt);
+    di.x = -di.x; di.y = -di.y;
+    T fx = x(cvFr), fy = x(cvFr + 1);
+    TV2<T> ni = {fx + di.x, fy + di.y};
+    T mx = x(cvFriction) * tni;
+    T lsq = ni.x * ni.x + ni.y * ni.y;
+    bool mask = lsq > mx * mx;
+    T nrm = mx / (tsqrt(lsq) + eps);
+    T sc = mask ? nrm : T(1.0f);
+    ni.x = sc * ni.x; ni.y = sc * ni.y;
+    di.x = ni.x - fx; di.y = ni.y - fy;
+    frx = ni.x; fry = ni.y;
+    TV3<T> Pv = di.x * t1;
+    Pv = Pv + di.y * t2;
+    wa = wa - sym_mv(sa, cross(ra, Pv));
+    wb = wb + sym_mv(sb, cross(rb, Pv));
+    Pv = Pv + mi * n;
+    va = va - ima * Pv;
+    vb = vb + imb * Pv;
+  }
+  out3(y, 0, va); out3(y, 3, wa); out3(y, 6, vb); out3(y, 9, wb);
+  y[16] = frx; y[17] = fry; y[18] = twist_out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Prepare (nsd_kernels.cuh prepare_constraint; contact_solver.rs:445): manifold and body mass
+// data -> the constraint's own entries of the constraint vector (outputs cvLam..kCV-1).
+enum PI : int {
+  piN = 0, piPoint = 3,  // + 8 q: anchor_a 0..2, anchor_b 3..5, separation 6, normal impulse 7
+  piFrictionImpulse = 35, piTwist = 38, piIma = 39, piImb = 40, piSa = 41, piSb = 47, piFriction = 53,
+  kPI = 54,
+};
+NSD_HD int pi_point(int q, int f) { return piPoint + 8 * q + f; }
+struct PParams {
+  int pc, is_static;
+  float warm_start;
+};
+template <class T, class In>
+NSD_HD void prepare_fn(const In& x, const PParams& pp, T* y /* kCVOwn, index - cvLam */) {
+  auto Y = [&](int cv) -> T& { return y[cv - cvLam]; };
+  auto Y3 = [&](int cv, const TV3<T>& a) { Y(cv) = a.x; Y(cv + 1) = a.y; Y(cv + 2) = a.z; };
+  const T inv_tau = T(1.0f / speculative_distance());
+  const T ws = T(pp.warm_start);
+  T ima = x(piIma), imb = x(piImb);
+  TSym<T> sa = in_sym<T>(x, piSa), sb = in_sym<T>(x, piSb);
+  TSym<T> inv_iab = sym_add(sa, sb);
+  TV3<T> n = in3<T>(x, piN);
+  TV3<T> t1 = perp(n);
+  TV3<T> t2 = cross(t1, n);
+  TV3<T> tvel = tzero3<T>();
+  T tv1 = dot(tvel, t1), tv2 = dot(tvel, t2);
+  T twist = ws * x(piTwist);
+  TV3<T> fimp = in3<T>(x, piFrictionImpulse);
+  T fix = ws * dot(fimp, t1), fiy = ws * dot(fimp, t2);
+  TV3<T> ca = tzero3<T>(), cb = tzero3<T>();
+  T tw = T(0.0f);
+  TV3<T> ra_[4];
+  for (int i = 0; i < 4; ++i) {
+    for (int f = 0; f < 9; ++f) Y(cv_point(i, f)) = T(0.0f);
+    Y(cvLam + i) = T(0.0f);
+  }
+  for (int i = 0; i < pp.pc; ++i) {
+    TV3<T> ra = in3<T>(x, pi_point(i, 0)), rb = in3<T>(x, pi_point(i, 3));
+    T sep = x(pi_point(i, 6));
+    ra_[i] = ra;
+    T base_sep = sep - dot(rb - ra, n);
+    T weight = tclamp(T(2.0f) - sep * inv_tau, T(kMinFrictionWeight), T(1.0f));
+    ca = ca + weight * ra;
+    cb = cb + weight * rb;
+    tw = tw + weight;
+    TV3<T> rna = cross(ra, n), rnb = cross(rb, n);
+    T k = ima + imb;
+    k = k + dot(rna, sym_mv(sa, rna));
+    k = k + dot(rnb, sym_mv(sb, rnb));
+    T nm = k > T(0.0f) ? T(1.0f) / k : T(0.0f);
+    Y3(cv_point(i, 0), ra);
+    Y(cv_point(i, 6)) = base_sep;
+    Y3(cv_point(i, 3), rb);
+    Y(cv_point(i, 7)) = nm;
+  }
+  if (tw > T(0.0f)) {
+    ca = (T(1.0f) / tw) * ca;
+    cb = (T(1.0f) / tw) * cb;
+  } else {
+    ca = tzero3<T>(); cb = tzero3<T>();
+  }
+  for (int i = 0; i < pp.pc; ++i) {
+    TV3<T> d = ra_[i] - ca;
+    Y(cv_point(i, 8)) = tsqrt(dot(d, d));
+    Y(cvLam + i) = ws * x(pi_point(i, 7));
+  }
+  TV3<T> rta1 = cross(ca, t1), rta2 = cross(ca, t2), rtb1 = cross(cb, t1), rtb2 = cross(cb, t2);
+  TV3<T> ia1 = sym_mv(sa, rta1), ia2 = sym_mv(sa, rta2), ib1 = sym_mv(sb, rtb1), ib2 = sym_mv(sb, rtb2);
+  T msum = ima + imb;
+  T kxx = (msum + dot(rta1, ia1)) + dot(rtb1, ib1);
+  T kyy = (msum + dot(rta2, ia2)) + dot(rtb2, ib2);
+  T kxy = dot(rta1, ia2) + dot(rtb1, ib2);
+  T det2 = kxx * kyy - kxy * kxy;
+  bool valid = tabs(det2) > T(1000.0f * kMinPositive) && tw > T(0.0f);
+  T inv = valid ? T(1.0f) / det2 : T(0.0f);
+  T ktw = dot(n, sym_mv(inv_iab, n));
+  T twist_mass = ktw > T(0.0f) ? T(1.0f) / ktw : T(0.0f);
+  Y(cvIma) = ima; Y(cvImb) = imb;
+  Y(cvSa) = sa.xx; Y(cvSa + 1) = sa.xy; Y(cvSa + 2) = sa.xz; Y(cvSa + 3) = sa.yy; Y(cvSa + 4) = sa.yz; Y(cvSa + 5) = sa.zz;
+  Y(cvSb) = sb.xx; Y(cvSb + 1) = sb.xy; Y(cvSb + 2) = sb.xz; Y(cvSb + 3) = sb.yy; Y(cvSb + 4) = sb.yz; Y(cvSb + 5) = sb.zz;
+  Y(cvFriction) = x(piFriction);
+  Y3(cvN, n);
+  Y3(cvT1, t1); Y(cvTv1) = tv1;
+  Y3(cvT2, t2); Y(cvTv2) = tv2;
+  Y3(cvCa, ca); Y(cvTwistMass) = twist_mass;
+  Y3(cvCb, cb); Y(cvTwist) = twist;
+  Y(cvTm) = inv * kyy; Y(cvTm + 1) = -(inv * kxy); Y(cvTm + 2) = -(inv * kxy); Y(cvTm + 3) = inv * kxx;
+  Y(cvFr) = fix; Y(cvFr + 1) = fiy;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Body stages.
+struct BParams {
+  float h, inv_dt, max_linear_speed;
+  float lin_damp, ang_damp, grav_scale;
+  uint32_t flags;
+  V3 gravity;
+};
+template <class T> NSD_HD T det(const TM3<T>& m) { return dot(m.cx, cross(m.cy, m.cz)); }
+template <class T> NSD_HD TV3<T> solve3(const TM3<T>& m, const TV3<T>& a) {
+  T d = det(m);
+  if (tabs(d) > T(1000.0f * kMinPositive)) {
+    T inv_d = T(1.0f) / d;
+    TV3<T> sx = cross(m.cy, m.cz), sy = cross(m.cz, m.cx), sz = cross(m.cx, m.cy);
+    return tv3<T>(inv_d * dot(sx, a), inv_d * dot(sy, a), inv_d * dot(sz, a));
+  }
+  return tzero3<T>();
+}
+
+// integrate velocities (nsd_solve.cuh apply_iv, solver_integration.rs:263) with the implicit
+// gyroscopic step of bodies flagged kGyroscopic.
+// Inputs: v 0..2, w 3..5, inv_mass 6, inverse world inertia 7..15 (cx, cy, cz), force 16..18,
+// torque 19..21, rotation 22..25, substep rotation dq 26..29, local inertia 30..38 (cx, cy, cz).
+// Outputs: v, w.
+constexpr int kIVIn = 39, kIVOut = 6;
+template <class T, class In>
+NSD_HD void iv_fn(const In& x, const BParams& bp, T* y) {
+  T h = T(bp.h);
+  TV3<T> v = in3<T>(x, 0), wv = in3<T>(x, 3);
+  T inv_mass = x(6);
+  TM3<T> iiw = tm3<T>(in3<T>(x, 7), in3<T>(x, 10), in3<T>(x, 13));
+  TV3<T> force = in3<T>(x, 16), torque = in3<T>(x, 19);
+  T ld = T(1.0f) / (T(1.0f) + h * T(bp.lin_damp));
+  T ad = T(1.0f) / (T(1.0f) + h * T(bp.ang_damp));
+  T gs = inv_mass > T(0.0f) ? T(bp.grav_scale) : T(0.0f);
+  TV3<T> lvd = blend2(h * inv_mass, force, h * gs, tv3<T>(bp.gravity));
+  v = mul_add(lvd, ld, v);
+  TV3<T> avd = h * mul_mv(iiw, torque);
+  wv = mul_add(avd, ad, wv);
+  if (bp.flags & kGyroscopic) {
+    TQ<T> q = mul_quat(in4<T>(x, 26), in4<T>(x, 22));
+    TV3<T> om1 = inv_rotate(q, wv);
+    TV3<T> om2 = om1;
+    T i00 = x(30), i01 = x(33), i02 = x(36);
+    T i11 = x(34), i12 = x(37), i22 = x(38);
+    T w1 = om2.x, w2 = om2.y, w3 = om2.z;
+    T iw1 = i00 * w1 + i01 * w2 + i02 * w3;
+    T iw2 = i01 * w1 + i11 * w2 + i12 * w3;
+    T iw3 = i02 * w1 + i12 * w2 + i22 * w3;
+    TV3<T> dw = om2 - om1;
+    TV3<T> b = tv3<T>(i00 * dw.x + i01 * dw.y + i02 * dw.z + h * (w2 * iw3 - w3 * iw2),
+                      i01 * dw.x + i11 * dw.y + i12 * dw.z + h * (w3 * iw1 - w1 * iw3),
+                      i02 * dw.x + i12 * dw.y + i22 * dw.z + h * (w1 * iw2 - w2 * iw1));
+    TM3<T> J = tm3<T>(tv3<T>(i00 + h * (w2 * i02 - w3 * i01), i01 + h * (w3 * i00 - w1 * i02 - iw3),
+                             i02 + h * (w1 * i01 - w2 * i00 + iw2)),
+                      tv3<T>(i01 + h * (w2 * i12 - w3 * i11 + iw3), i11 + h * (w3 * i01 - w1 * i12),
+                             i12 + h * (w1 * i11 - w2 * i01 - iw1)),
+                      tv3<T>(i02 + h * (w2 * i22 - w3 * i12 - iw2), i12 + h * (w3 * i02 - w1 * i22 + iw1),
+                             i22 + h * (w1 * i12 - w2 * i02)));
+    om2 = om2 - solve3(J, b);
+    wv = rotate(q, om2);
+  }
+  out3(y, 0, v); out3(y, 3, wv);
+}
+// integrate positions (nsd_solve.cuh apply_ip, solver_integration.rs:377).
+// Inputs and outputs: v 0..2, w 3..5, dp 6..8, dq 9..12.
+constexpr int kIP = 13;
+template <class T, class In>
+NSD_HD void ip_fn(const In& x, const BParams& bp, T* y) {
+  uint32_t flags = bp.flags;
+  T maxl = T(bp.max_linear_speed);
+  T maxa = T(kMaxRotation * bp.inv_dt);
+  T maxl2 = maxl * maxl, maxa2 = maxa * maxa;
+  TV3<T> v = in3<T>(x, 0), wv = in3<T>(x, 3);
+  v.x = (flags & kLockLinX) ? T(0.0f) : v.x;
+  v.y = (flags & kLockLinY) ? T(0.0f) : v.y;
+  v.z = (flags & kLockLinZ) ? T(0.0f) : v.z;
+  wv.x = (flags & kLockAngX) ? T(0.0f) : wv.x;
+  wv.y = (flags & kLockAngY) ? T(0.0f) : wv.y;
+  wv.z = (flags & kLockAngZ) ? T(0.0f) : wv.z;
+  if (dot(v, v) > maxl2) {
+    T ratio = maxl / length(v);
+    v = ratio * v;
+  }
+  if (dot(wv, wv) > maxa2 && (flags & kAllowFastRotation) == 0) {
+    T ratio = maxa / length(wv);
+    wv = ratio * wv;
+  }
+  TV3<T> dp = mul_add(in3<T>(x, 6), T(bp.h), v);
+  TQ<T> dq = integrate_rotation(in4<T>(x, 9), T(bp.h) * wv);
+  out3(y, 0, v); out3(y, 3, wv); out3(y, 6, dp); out4(y, 9, dq);
+}
+// finalize rotation (nsd_solve.cuh k_finalize, solver_integration.rs:587): q' = normalize(dq q).
+// Inputs: q 0..3, dq 4..7. Outputs: q'.
+template <class T, class In>
+NSD_HD void final_rot_fn(const In& x, T* y) {
+  out4(y, 0, normalize_quat(mul_quat(in4<T>(x, 4), in4<T>(x, 0))));
+}
+// inverse world inertia R I^-1 R^T of finalize. Inputs: q 0..3, local inverse inertia 4..12
+// (cx, cy, cz). Outputs: the world matrix (cx, cy, cz).
+template <class T, class In>
+NSD_HD void inv_inertia_fn(const In& x, T* y) {
+  TM3<T> R = matrix_from_quat(in4<T>(x, 0));
+  TM3<T> il = tm3<T>(in3<T>(x, 4), in3<T>(x, 7), in3<T>(x, 10));
+  TM3<T> m = mul_mm(mul_mm(R, il), transpose(R));
+  out3(y, 0, m.cx); out3(y, 3, m.cy); out3(y, 6, m.cz);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Contact recycling (nsd_kernels.cuh collide_recycle; collide_pass.rs:606-687): the new
+// separations of a recycled manifold. Inputs: tangents of centre A 0..2 and B 3..5 (the
+// centres' values are f64 and passed apart), qa 6..9, qb 10..13, cached rotation A 14..17 and
+// B 18..21, normal 22..24, per point q: 25 + 7 q + {anchor_a 0..2, anchor_b 3..5, base
+// separation 6}. Outputs: the separations (point_count).
+enum RI : int { riCa = 0, riCb = 3, riQa = 6, riQb = 10, riRotA = 14, riRotB = 18, riN = 22, riPoint = 25, kRI = 53 };
+NSD_HD int ri_point(int q, int f) { return riPoint + 7 * q + f; }
+template <class T, class In>
+NSD_HD void recycle_fn(const In& x, const Pos& ca, const Pos& cb, int pc, T* y) {
+  TQ<T> qa = in4<T>(x, riQa), qb = in4<T>(x, riQb);
+  TQ<T> dqa = mul_quat(qa, conjugate(in4<T>(x, riRotA)));
+  TQ<T> dqb = mul_quat(qb, conjugate(in4<T>(x, riRotB)));
+  TM3<T> ma = matrix_from_quat(dqa), mb = matrix_from_quat(dqb);
+  TV3<T> dc = sub_pos_t(cb, ca, in3<T>(x, riCb), in3<T>(x, riCa));
+  TV3<T> n = in3<T>(x, riN);
+  for (int i = 0; i < pc; ++i) {
+    TV3<T> ra = mul_mv(ma, in3<T>(x, ri_point(i, 0)));
+    TV3<T> rb = mul_mv(mb, in3<T>(x, ri_point(i, 3)));
+    TV3<T> dp = dc + (rb - ra);
+    y[i] = x(ri_point(i, 6)) + dot(dp, n);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Box-box manifolds (nsd_geom.cuh collide_hulls and its builders, convex_manifold.rs), replayed
+// along the branch the forward step took: the SAT cache after the narrowphase names the axis
+// kind and features, and every comparison inside the builders is taken on the value parts.
+template <class T> struct TClipVertex { TV3<T> position; T separation; FeaturePair pair; };
+template <class T> struct TLocalPoint { TV3<T> point; T separation; FeaturePair pair; };
+template <class T> struct TLocalManifold { TV3<T> normal; TLocalPoint<T> points[4]; int point_count; };
+
+template <class T>
+NSD_HD int t_build_polygon(TClipVertex<T>* out, const TXf<T>& t, const Hull& h, int inc_face, const TPlane<T>& ref) {
+  int ei = box_face_edge(inc_face);
+  int n = 0;
+  TM3<T> m = matrix_from_quat(t.q);
+  for (;;) {
+    HalfEdge e = box_edge(ei);
+    int ni = e.next;
+    HalfEdge nx = box_edge(ni);
+    TClipVertex<T> v;
+    v.position = mul_mv(m, tv3<T>(h.points[nx.origin])) + t.p;
+    v.separation = plane_sep(ref, v.position);
+    v.pair = make_feature_pair(1, ei, 1, ni);
+    out[n++] = v;
+    ei = ni;
+    if (ei == box_face_edge(inc_face) || n >= kClipCap) break;
+  }
+  return n;
+}
+template <class T>
+NSD_HD int t_clip_polygon(TClipVertex<T>* out, const TClipVertex<T>* poly, int count, const TPlane<T>& clip, int edge,
+                          const TPlane<T>& ref) {
+  TClipVertex<T> v1 = poly[count - 1];
+  T d1 = plane_sep(clip, v1.position);
+  int n = 0;
+  for (int i = 0; i < count; ++i) {
+    TClipVertex<T> v2 = poly[i];
+    T d2 = plane_sep(clip, v2.position);
+    if (d1 <= T(0.0f) && d2 <= T(0.0f)) {
+      if (n < kClipCap) out[n] = v2;
+      n++;
+    } else if (d1 <= T(0.0f) && d2 > T(0.0f)) {
+      T f = d1 / (d1 - d2);
+      TV3<T> pos = mul_add(v1.position, f, v2.position - v1.position);
+      TClipVertex<T> v;
+      v.position = pos; v.separation = plane_sep(ref, pos); v.pair = v2.pair;
+      v.pair.owner2 = 0; v.pair.index2 = (uint8_t)edge;
+      if (n < kClipCap) out[n] = v;
+      n++;
+    } else if (d2 <= T(0.0f) && d1 > T(0.0f)) {
+      T f = d1 / (d1 - d2);
+      TV3<T> pos = mul_add(v1.position, f, v2.position - v1.position);
+      TClipVertex<T> v;
+      v.position = pos; v.separation = plane_sep(ref, pos); v.pair = v1.pair;
+      v.pair.owner1 = 0; v.pair.index1 = (uint8_t)edge;
+      if (n < kClipCap) out[n] = v;
+      n++;
+      if (n < kClipCap) out[n] = v2;
+      n++;
+    }
+    v1 = v2; d1 = d2;
+  }
+  return n < kClipCap ? n : kClipCap;
+}
+template <class T>
+NSD_HD void t_reduce_manifold_points(TLocalManifold<T>* m, TLocalPoint<T>* pts, int count) {
+  if (count <= 4) {
+    for (int i = 0; i < count; ++i) m->points[i] = pts[i];
+    m->point_count = count;
+    return;
+  }
+  TV3<T> normal = m->normal;
+  T spec = T(speculative_distance());
+  T tol_sqr = spec * spec;
+  const T bias(0.95f);
+  int best = kNull;
+  T best_score = T(-kFltMax);
+  // the normal is the reference face's plane normal, a constant of the hull
+  TV3<T> sd = tv3<T>(arbitrary_perp(real3(normal)));
+  for (int i = 0; i < count; ++i) {
+    if (pts[i].separation > spec) continue;
+    T score = -pts[i].separation + dot(sd, pts[i].point);
+    if (bias * score > best_score) { best = i; best_score = score; }
+  }
+  if (best == kNull) { m->point_count = 0; return; }
+  m->points[0] = pts[best];
+  m->point_count = 1;
+  pts[best] = pts[count - 1];
+  count--;
+  TV3<T> a = m->points[0].point;
+  best_score = T(0.0f); best = kNull;
+  for (int i = 0; i < count; ++i) {
+    TV3<T> d = pts[i].point - a;
+    TV3<T> v = mul_sub(d, dot(d, normal), normal);
+    T dsq = length_sq(v);
+    T sep = tmax(T(0.0f), -pts[i].separation);
+    T score = dsq + T(4.0f) * sep * sep;
+    if (bias * score > best_score) { best_score = score; best = i; }
+  }
+  if (best_score < tol_sqr) return;
+  m->points[1] = pts[best];
+  m->point_count = 2;
+  pts[best] = pts[count - 1];
+  count--;
+  TV3<T> b = m->points[1].point;
+  best_score = tol_sqr; best = kNull;
+  T best_signed = T(0.0f);
+  TV3<T> ba = b - a;
+  for (int i = 0; i < count; ++i) {
+    TV3<T> p = pts[i].point;
+    T signed_area = dot(normal, cross(ba, p - a));
+    T score = tabs(signed_area);
+    if (bias * score >= best_score) { best_score = score; best = i; best_signed = signed_area; }
+  }
+  if (best == kNull) return;
+  m->points[2] = pts[best];
+  m->point_count = 3;
+  pts[best] = pts[count - 1];
+  count--;
+  TV3<T> c = m->points[2].point;
+  best_score = tol_sqr; best = kNull;
+  T sign = best_signed < T(0.0f) ? T(-1.0f) : T(1.0f);
+  for (int i = 0; i < count; ++i) {
+    TV3<T> p = pts[i].point;
+    T u1 = sign * dot(normal, cross(p - a, ba));
+    T u2 = sign * dot(normal, cross(p - b, c - b));
+    T u3 = sign * dot(normal, cross(p - c, a - c));
+    T score = tmax(u1, tmax(u2, u3));
+    if (bias * score > best_score) { best_score = score; best = i; }
+  }
+  if (best != kNull) {
+    m->points[m->point_count] = pts[best];
+    m->point_count += 1;
+  }
+}
+// convex_manifold.rs:1150 build_face_a_contact; returns false when the forward step found no
+// contact on this axis.
+template <class T>
+NSD_HD bool t_build_face_a(TLocalManifold<T>* m, const Hull& ha, const Hull& hb, const TXf<T>& xb, int ref_face,
+                           int vertex) {
+  TClipVertex<T> poly1[kClipCap], poly2[kClipCap];
+  TLocalPoint<T> pts[kClipCap];
+  TPlane<T> rp = tplane<T>(ha.planes[ref_face]);
+  TV3<T> ref_n_in_b = inv_rotate(xb.q, rp.n);
+  int inc = find_incident_face(hb, real3(ref_n_in_b), vertex);
+  int count = t_build_polygon(poly1, xb, hb, inc, rp);
+  int ei = box_face_edge(ref_face);
+  bool use1 = true;
+  for (;;) {
+    HalfEdge e = box_edge(ei);
+    int ni = e.next;
+    HalfEdge nx = box_edge(ni);
+    V3 p1 = ha.points[e.origin], p2 = ha.points[nx.origin];
+    V3 tangent = nsd::normalize(p2 - p1);
+    V3 binormal = nsd::cross(tangent, ha.planes[ref_face].n);
+    TPlane<T> cp = tplane<T>(plane_from_normal_point(binormal, p1));
+    if (use1) count = t_clip_polygon(poly2, poly1, count, cp, ei, rp);
+    else count = t_clip_polygon(poly1, poly2, count, cp, ei, rp);
+    use1 = !use1;
+    if (count < 3) return false;
+    ei = ni;
+    if (ei == box_face_edge(ref_face)) break;
+  }
+  count = count < kClipCap ? count : kClipCap;
+  m->normal = rp.n;
+  const TClipVertex<T>* src = use1 ? poly1 : poly2;
+  T min_sep = T(kFltMax);
+  for (int i = 0; i < count; ++i) {
+    TLocalPoint<T> p;
+    p.point = mul_sub(src[i].position, T(0.5f) * src[i].separation, rp.n);
+    p.separation = src[i].separation;
+    p.pair = src[i].pair;
+    min_sep = tmin(min_sep, src[i].separation);
+    pts[i] = p;
+  }
+  if (min_sep >= T(speculative_distance())) return false;
+  t_reduce_manifold_points(m, pts, count);
+  return true;
+}
+template <class T>
+NSD_HD bool t_build_face_b(TLocalManifold<T>* m, const Hull& ha, const Hull& hb, const TXf<T>& xb, int vertex,
+                           int ref_face_b) {
+  TXf<T> xa = invert_xf(xb);
+  if (!t_build_face_a(m, hb, ha, xa, ref_face_b, vertex)) return false;
+  TM3<T> mat = matrix_from_quat(xb.q);
+  m->normal = -mul_mv(mat, m->normal);
+  for (int i = 0; i < m->point_count; ++i) {
+    m->points[i].point = mul_mv(mat, m->points[i].point) + xb.p;
+    m->points[i].pair = flip_pair(m->points[i].pair);
+  }
+  return true;
+}
+template <class T>
+NSD_HD bool t_build_edge(TLocalManifold<T>* m, const Hull& ha, const Hull& hb, const TXf<T>& xb, const TV3<T>& normal,
+                         int index_a, int index_b) {
+  HalfEdge ea = box_edge(index_a);
+  HalfEdge ta = box_edge(ea.twin);
+  TV3<T> pa = tv3<T>(ha.points[ea.origin]), qa = tv3<T>(ha.points[ta.origin]);
+  TV3<T> e_a = qa - pa;
+  HalfEdge eb = box_edge(index_b);
+  HalfEdge tb = box_edge(eb.twin);
+  TV3<T> pb = xf_point(xb, tv3<T>(hb.points[eb.origin]));
+  TV3<T> qb = xf_point(xb, tv3<T>(hb.points[tb.origin]));
+  TV3<T> e_b = qb - pb;
+  // nsd_math.cuh line_distance
+  T a11 = dot(e_a, e_a), a12 = -dot(e_a, e_b), a21 = dot(e_b, e_a), a22 = -dot(e_b, e_b);
+  TV3<T> wv = pa - pb;
+  T b1 = -dot(e_a, wv), b2 = -dot(e_b, wv);
+  T d = a11 * a22 - a12 * a21;
+  TV3<T> p1, p2;
+  T f1, f2;
+  if (d * d < T(1000.0f * kMinPositive)) {
+    T s1 = dot(pb - pa, e_a) / dot(e_a, e_a);
+    p1 = mul_add(pa, s1, e_a); f1 = s1; p2 = pb; f2 = T(0.0f);
+  } else {
+    T s1 = (a22 * b1 - a12 * b2) / d;
+    T s2 = (a11 * b2 - a21 * b1) / d;
+    p1 = mul_add(pa, s1, e_a); f1 = s1; p2 = mul_add(pb, s2, e_b); f2 = s2;
+  }
+  if (!((T(0.0f) <= f1 && f1 <= T(1.0f)) && (T(0.0f) <= f2 && f2 <= T(1.0f)))) return false;
+  m->normal = normal;
+  m->point_count = 1;
+  m->points[0].point = T(0.5f) * (p1 + p2);
+  m->points[0].separation = dot(normal, p2 - p1);
+  m->points[0].pair = make_feature_pair(0, index_a, 1, index_b);
+  return true;
+}
+// The edge-pair axis as the cached fast path computes it (nsd_geom.cuh collide_hulls).
+template <class T>
+NSD_HD TV3<T> t_edge_axis_cached(const Hull& ha, const Hull& hb, const TXf<T>& xb, int ia, int ib) {
+  HalfEdge e1 = box_edge(ia), t1 = box_edge(ia + 1);
+  TV3<T> e_a = tv3<T>(ha.points[t1.origin]) - tv3<T>(ha.points[e1.origin]);
+  HalfEdge e2 = box_edge(ib), t2 = box_edge(ib + 1);
+  TV3<T> ub = rotate(xb.q, tv3<T>(hb.planes[e2.face].n));
+  TV3<T> vb = rotate(xb.q, tv3<T>(hb.planes[t2.face].n));
+  T cba = dot(ub, e_a), dba = dot(vb, e_a);
+  T t = cba / (cba - dba);
+  return -normalize(lerp(ub, vb, t));
+}
+// The edge-pair axis as the full separating-axis search computes it (nsd_geom.cuh
+// compute_separating_axis).
+template <class T>
+NSD_HD TV3<T> t_edge_axis_sat(const Hull& ha, const Hull& hb, const TXf<T>& xb, int ia, int ib) {
+  TM3<T> r = matrix_from_quat(xb.q);
+  TV3<T> r0 = tv3<T>(r.cx.x, r.cy.x, r.cz.x), r1 = tv3<T>(r.cx.y, r.cy.y, r.cz.y), r2 = tv3<T>(r.cx.z, r.cy.z, r.cz.z);
+  HalfEdge e = box_edge(ib), tw = box_edge(ib + 1);
+  auto bface = [&](int f) {
+    TV3<T> v = tv3<T>(v3(hb.nx[f], hb.ny[f], hb.nz[f]));
+    TV3<T> o = tv3<T>(dot(r0, v), dot(r1, v), dot(r2, v));
+    return tv3<T>(-o.x, -o.y, -o.z);
+  };
+  TV3<T> c = bface(e.face), dn = bface(tw.face);
+  HalfEdge ea = box_edge(ia), ta = box_edge(ia + 1);
+  int v0 = ea.origin, v1 = ta.origin;
+  TV3<T> d = tv3<T>(v3(ha.vx[v1] - ha.vx[v0], ha.vy[v1] - ha.vy[v0], ha.vz[v1] - ha.vz[v0]));
+  T cba = dot(c, d), dba = dot(dn, d);
+  T t = -cba / (dba - cba);
+  TV3<T> n = mul_add(c, t, dn - c);
+  T len2 = dot(n, n);
+  T inv = T(1.0f) / tsqrt(len2);
+  return inv * n;
+}
+
+// Narrowphase of a box pair followed by the world transform of update_contact
+// (nsd_kernels.cuh update_contact, contact_update.rs:43). Inputs: tangents of centre A 0..2,
+// qa 3..6, tangents of centre B 7..9, qb 10..13. Outputs: normal 0..2, per point q:
+// 3 + 7 q + {anchor_a 0..2, anchor_b 3..5, separation 6}. Returns the point count, or -1
+// when the replay does not reproduce a manifold.
+enum FI : int { fiCa = 0, fiQa = 3, fiCb = 7, fiQb = 10, kFI = 14 };
+constexpr int kFO = 31;
+struct NarrowCase {
+  uint8_t type, index_a, index_b, hit;  // SAT cache after the forward narrowphase
+};
+template <class T, class In>
+NSD_HD int narrow_box_fn(const In& x, const Pos& ca, const Pos& cb, const Hull& ha, const Hull& hb, NarrowCase nc,
+                         T* y, uint32_t* ids = nullptr) {
+  TQ<T> qa = in4<T>(x, fiQa), qb = in4<T>(x, fiQb);
+  // inv_mul_wxf(xa, xb): the position of B in A's frame, and the relative rotation
+  TV3<T> d = sub_pos_t(cb, ca, in3<T>(x, fiCb), in3<T>(x, fiCa));
+  TXf<T> xb;
+  xb.p = inv_rotate(qa, d);
+  xb.q = inv_mul_quat(qa, qb);
+  TLocalManifold<T> lm;
+  lm.point_count = 0;
+  bool ok = false;
+  if (nc.type == kFaceAxisA) {
+    int vi = nc.index_b;
+    if (nc.hit) {
+      V3 sd = -nsd::inv_rotate(Q{real3(xb.q.v), (float)val(xb.q.s)}, ha.planes[nc.index_a].n);
+      vi = find_hull_support_vertex(hb, sd);
+    }
+    ok = t_build_face_a(&lm, ha, hb, xb, nc.index_a, vi);
+  } else if (nc.type == kFaceAxisB) {
+    int vi = nc.index_a;
+    if (nc.hit) {
+      V3 sd = -nsd::rotate(Q{real3(xb.q.v), (float)val(xb.q.s)}, hb.planes[nc.index_b].n);
+      vi = find_hull_support_vertex(ha, sd);
+    }
+    ok = t_build_face_b(&lm, ha, hb, xb, vi, nc.index_b);
+  } else if (nc.type == kEdgePairAxis) {
+    TV3<T> nrm = nc.hit ? t_edge_axis_cached(ha, hb, xb, nc.index_a, nc.index_b)
+                        : t_edge_axis_sat(ha, hb, xb, nc.index_a, nc.index_b);
+    ok = t_build_edge(&lm, ha, hb, xb, nrm, nc.index_a, nc.index_b);
+  }
+  if (!ok || lm.point_count == 0) return -1;
+  TM3<T> ma = matrix_from_quat(qa);
+  TV3<T> dab = sub_pos_t(ca, cb, in3<T>(x, fiCa), in3<T>(x, fiCb));
+  out3(y, 0, mul_mv(ma, lm.normal));
+  for (int i = 0; i < lm.point_count; ++i) {
+    TV3<T> aa = mul_mv(ma, lm.points[i].point);
+    out3(y, 3 + 7 * i, aa);
+    out3(y, 3 + 7 * i + 3, aa + dab);
+    y[3 + 7 * i + 6] = lm.points[i].separation;
+    if (ids) ids[i] = make_feature_id(lm.points[i].pair);
+  }
+  return lm.point_count;
+}
+
+}  // namespace ad
+}  // namespace nsd

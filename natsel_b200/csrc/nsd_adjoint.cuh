@@ -1,0 +1,717 @@
+// Adjoint of the step (vector-Jacobian product of a rollout) on the device.
+//
+// The forward step is replayed from a checkpoint with a tape: the body state at the start of
+// the step, the contacts before the narrowphase and after the state pass, the prepared
+// constraint planes, per substep three body rows (before integrate-velocities, before and
+// after integrate-positions) and the inputs of every push and relax update. The reverse pass
+// then walks the step backwards: finalize, impulse store, the substeps (relax colours 22..0,
+// integrate positions, push colours 22..0, warm start colours 22..0, integrate velocities),
+// prepare, the inverse world inertia and the narrowphase. Each local function's
+// vector-Jacobian product is formed by one warp: lane l seeds input directions l, l + 32, ...
+// of the dual-number restatement (nsd_ad.cuh), evaluates it once and contracts the output
+// tangents with the incoming cotangents. Colours keep the forward's independence: inside a
+// colour no two constraints share a dynamic body, so their body cotangents are written
+// without atomics.
+//
+// Scope of the adjoint: one world of box bodies (hull shapes) without joints, restitution,
+// rolling resistance, continuous collision or overflow constraints; the host rejects other
+// worlds.
+#pragma once
+#include "nsd_solve.cuh"
+#include "nsd_ad.cuh"
+
+namespace nsd {
+
+// Device tape of one step.
+struct StepTape {
+  DSim* sims;        // [n_awake] at the start of the step
+  DContact* pre;     // [cap] before the narrowphase (after the pair update)
+  DContact* post;    // [cap] after the state pass
+  Control* ctl;      // after prepare (colour offsets)
+  CPlanes planes;    // after prepare
+  DState* body;      // [substep][3][n_awake]: before IV, before IP, after IP
+  float4* push;      // [substep][4][cap]: vA|l0, wA|l1, vB|l2, wB|l3 before push
+  float4* relax;     // [substep][5][cap]: the same before relax, then fr.x, fr.y, twist
+  float4* fin;       // [cap]: friction impulse x, y and twist after the solve
+  uint8_t* mode;     // [cap]: narrowphase 0 none/disjoint, 1 recycled, 2 new manifold, 3 no points
+  int substeps;
+};
+
+// Cotangent buffers of the reverse pass.
+enum : int {
+  pbInvMass = 0, pbIiw = 1, pbIinv = 10, pbFriction = 19, pbInertia = 20, kPB = 29,
+  // contact manifold cotangent: normal, per point 9 (anchor_a, anchor_b, separation,
+  // base separation, normal impulse), friction impulse, twist, cached rotations
+  mbN = 0, mbPoint = 3, mbFrictionImpulse = 39, mbTwist = 42, mbRotA = 43, mbRotB = 47, kMB = 51,
+};
+__host__ __device__ __forceinline__ int mb_point(int q, int f) { return mbPoint + 9 * q + f; }
+struct AdjBufs {
+  float* bb;   // [n_awake][16]: v|-, w|-, dp|-, dq (cotangents of the solver state)
+  float* cq;   // [n_awake][8]: centre|-, rotation (cotangents at the current step boundary)
+  float* pb;   // [n_awake][kPB]: parameters
+  float* kb;   // [kCVOwn][cap]: constraint entries cvLam.. of each slot
+  float* mb;   // [kMB][cap]: manifold state of each contact id
+  int* mismatch;  // narrowphase replays that did not reproduce the forward manifold
+  int cap, n_awake;
+};
+
+constexpr int kAdjThreads = 256;
+
+__device__ __forceinline__ float& BB(const AdjBufs& a, int i, int f) { return a.bb[(size_t)i * 16 + f]; }
+__device__ __forceinline__ float& CQ(const AdjBufs& a, int i, int f) { return a.cq[(size_t)i * 8 + f]; }
+__device__ __forceinline__ float& PB(const AdjBufs& a, int i, int f) { return a.pb[(size_t)i * kPB + f]; }
+__device__ __forceinline__ float& KB(const AdjBufs& a, int k, int cv) { return a.kb[(size_t)(cv - ad::cvLam) * a.cap + k]; }
+__device__ __forceinline__ float& MB(const AdjBufs& a, int c, int f) { return a.mb[(size_t)f * a.cap + c]; }
+
+// One warp: x̄[dir] = sum_j ȳ_j dy_j/dx_dir for the directions of this lane.
+template <int K, int NY, class Fn>
+__device__ __forceinline__ void warp_vjp(const float* xs, const float* ys, const int16_t* dirs, int ndirs, Fn fn,
+                                         float* xbar, int* dir) {
+  int lane = threadIdx.x & 31;
+  ad::SeedIn<float, K> in;
+  in.x = xs;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    int d = lane + 32 * k;
+    in.dir[k] = d < ndirs ? dirs[d] : -1;
+  }
+  ad::Dual<float, K> y[NY];
+  fn(in, y);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < NY; ++j) acc += ys[j] * y[j].d[k];
+    xbar[k] = acc;
+    dir[k] = in.dir[k];
+  }
+}
+
+// Direction lists (constraint vector indices) of the three contact stages.
+struct StageDirs { int16_t warm[64], push[96], relax[128]; int n_warm, n_push, n_relax; };
+__constant__ StageDirs c_dirs;
+
+inline StageDirs make_stage_dirs() {
+  using namespace ad;
+  StageDirs s = {};
+  auto add = [](int16_t* l, int& n, int a, int b) { for (int i = a; i < b; ++i) l[n++] = (int16_t)i; };
+  // warm start is affine in the velocities (identity Jacobian): only its constants and impulses
+  add(s.warm, s.n_warm, cvLam, cvT2 + 3);
+  add(s.warm, s.n_warm, cvCa, cvCb + 3);
+  for (int q = 0; q < 4; ++q) add(s.warm, s.n_warm, cv_point(q, 0), cv_point(q, 6));
+  add(s.push, s.n_push, 0, cvLam + 4);
+  add(s.push, s.n_push, cvIma, cvN + 3);
+  for (int q = 0; q < 4; ++q) add(s.push, s.n_push, cv_point(q, 0), cv_point(q, 8));
+  add(s.relax, s.n_relax, 0, cvTv1);
+  add(s.relax, s.n_relax, cvCa, kCV);
+  return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Finalize (k_finalize): centre' = centre + dp, q' = normalize(dq q).
+__global__ void k_adj_finalize(StepTape t, AdjBufs a, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DSim& s = t.sims[i];
+  const DState& last = t.body[((size_t)(t.substeps - 1) * 3 + 2) * n + i];
+  float xs[8] = {s.q.v.x, s.q.v.y, s.q.v.z, s.q.s, last.dq.v.x, last.dq.v.y, last.dq.v.z, last.dq.s};
+  ad::SeedIn<float, 8> in;
+  in.x = xs;
+  for (int k = 0; k < 8; ++k) in.dir[k] = k;
+  ad::Dual<float, 8> y[4];
+  ad::final_rot_fn<ad::Dual<float, 8>>(in, y);
+  float qbar[4] = {CQ(a, i, 4), CQ(a, i, 5), CQ(a, i, 6), CQ(a, i, 7)};
+  float xb[8];
+  for (int k = 0; k < 8; ++k) {
+    float acc = 0.0f;
+    for (int j = 0; j < 4; ++j) acc += qbar[j] * y[j].d[k];
+    xb[k] = acc;
+  }
+  for (int f = 0; f < 3; ++f) BB(a, i, 8 + f) = CQ(a, i, f);   // dp̄ = centre cotangent
+  for (int f = 0; f < 4; ++f) BB(a, i, 12 + f) = xb[4 + f];     // dq̄
+  for (int f = 0; f < 4; ++f) CQ(a, i, 4 + f) = xb[f];          // q̄ at the step start
+}
+
+// Impulse store (store_constraint): the manifold's impulses after the step are the solver's
+// final impulses; their cotangents seed the constraint's own entries.
+__global__ void k_adj_store(StepTape t, AdjBufs a, int n_slots) {
+  using namespace ad;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_slots) return;
+  int4 idx = t.planes.idx[k];
+  int cid = idx.z, pc = idx.w & 255;
+  for (int cv = cvLam; cv < kCV; ++cv) KB(a, k, cv) = 0.0f;
+  for (int q = 0; q < pc; ++q) {
+    KB(a, k, cvLam + q) = MB(a, cid, mb_point(q, 8));
+    MB(a, cid, mb_point(q, 8)) = 0.0f;
+  }
+  V3 F = v3(MB(a, cid, mbFrictionImpulse), MB(a, cid, mbFrictionImpulse + 1), MB(a, cid, mbFrictionImpulse + 2));
+  float twist = MB(a, cid, mbTwist);
+  for (int f = 0; f < 3; ++f) MB(a, cid, mbFrictionImpulse + f) = 0.0f;
+  MB(a, cid, mbTwist) = 0.0f;
+  float4 fin = t.fin[k], t1 = t.planes.t1[k], t2 = t.planes.t2[k];
+  KB(a, k, cvFr) = F.x * t1.x + F.y * t1.y + F.z * t1.z;
+  KB(a, k, cvFr + 1) = F.x * t2.x + F.y * t2.y + F.z * t2.z;
+  KB(a, k, cvTwist) = twist;
+  KB(a, k, cvT1) = fin.x * F.x; KB(a, k, cvT1 + 1) = fin.x * F.y; KB(a, k, cvT1 + 2) = fin.x * F.z;
+  KB(a, k, cvT2) = fin.y * F.x; KB(a, k, cvT2 + 1) = fin.y * F.y; KB(a, k, cvT2 + 2) = fin.y * F.z;
+}
+
+// The constraint vector of slot k in stage `stage` of substep `sub` (values of the forward),
+// gathered by the lanes of one warp into xs.
+__device__ void gather_cv(const StepTape& t, int n, int cap, int k, int sub, int stage, float* xs) {
+  using namespace ad;
+  const CPlanes& P = t.planes;
+  int lane = threadIdx.x & 31;
+  int4 idx = P.idx[k];
+  int ia = idx.x, ib = idx.y;
+  auto put4 = [&](int at, float4 v, int cnt) {
+    xs[at] = v.x; if (cnt > 1) xs[at + 1] = v.y; if (cnt > 2) xs[at + 2] = v.z; if (cnt > 3) xs[at + 3] = v.w;
+  };
+  const float4* rows = stage == kPush ? t.push + (size_t)sub * 4 * cap : t.relax + (size_t)sub * 5 * cap;
+  if (stage == kWarm) rows = t.push + (size_t)sub * 4 * cap;
+  int row_sel = stage == kRelax ? 2 : 0;  // dp, dq seen by the stage
+  switch (lane) {
+    case 0: case 1: case 2: case 3: {
+      float4 r = rows[(size_t)lane * cap + k];
+      if (stage == kWarm) { r.x = 0.0f; r.y = 0.0f; r.z = 0.0f; }  // unused by warm start
+      put4(3 * lane, r, 3);
+      xs[cvLam + lane] = r.w;
+      break;
+    }
+    case 4: {
+      float4 r = t.relax[((size_t)sub * 5 + 4) * cap + k];
+      xs[cvFr] = r.x; xs[cvFr + 1] = r.y; xs[cvTwist] = r.z;
+      break;
+    }
+    case 5: case 6: {
+      int b = lane == 5 ? ia : ib;
+      float4 dp = make_float4(0, 0, 0, 0), dq = make_float4(0, 0, 0, 1);
+      if (b >= 0) {
+        const DState& st = t.body[((size_t)sub * 3 + row_sel) * n + b];
+        dp = make_float4(st.dp.x, st.dp.y, st.dp.z, 0.0f);
+        dq = make_float4(st.dq.v.x, st.dq.v.y, st.dq.v.z, st.dq.s);
+      }
+      put4(lane == 5 ? cvDpA : cvDpB, dp, 3);
+      put4(lane == 5 ? cvDqA : cvDqB, dq, 4);
+      break;
+    }
+    case 7: { float4 m = P.mass[k]; xs[cvIma] = m.x; xs[cvImb] = m.y; xs[cvFriction] = m.z; break; }
+    case 8: put4(cvSa, P.ia0[k], 4); break;
+    case 9: { float4 v = P.ia1[k]; xs[cvSa + 4] = v.x; xs[cvSa + 5] = v.y; xs[cvSb] = v.z; xs[cvSb + 1] = v.w; break; }
+    case 10: put4(cvSb + 2, P.ib1[k], 4); break;
+    case 11: put4(cvN, P.n[k], 3); break;
+    case 12: { float4 v = P.t1[k]; put4(cvT1, v, 3); xs[cvTv1] = v.w; break; }  // t1 | tangent velocity 1
+    case 13: { float4 v = P.t2[k]; put4(cvT2, v, 3); xs[cvTv2] = v.w; break; }
+    case 14: { float4 v = P.ca[k]; put4(cvCa, v, 3); xs[cvTwistMass] = v.w; break; }
+    case 15: put4(cvCb, P.cb[k], 3); break;
+    case 16: put4(cvTm, P.tm[k], 4); break;
+    default: {
+      int g = lane - 17;  // 0..11: pra, prb, pimp of the four points
+      if (g < 12) {
+        int q = g % 4, kind = g / 4;
+        float4 v = kind == 0 ? P.pra[(size_t)q * cap + k] : kind == 1 ? P.prb[(size_t)q * cap + k] : P.pimp[(size_t)q * cap + k];
+        if (kind == 0) { put4(cv_point(q, 0), v, 3); xs[cv_point(q, 6)] = v.w; }
+        else if (kind == 1) { put4(cv_point(q, 3), v, 3); xs[cv_point(q, 7)] = v.w; }
+        else xs[cv_point(q, 8)] = v.z;
+      }
+      break;
+    }
+  }
+}
+
+// Reverse of one contact stage for slot k, by one warp.
+template <int Stage>
+__device__ void adj_contact(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int k, int sub, float* xs,
+                            float* ys) {
+  using namespace ad;
+  int lane = threadIdx.x & 31;
+  int4 idx = t.planes.idx[k];
+  int ia = idx.x, ib = idx.y;
+  CParams cp;
+  cp.pc = idx.w & 255;
+  cp.is_static = (idx.w & 256) != 0;
+  cp.inv_h = p.inv_h;
+  cp.contact_speed = p.contact_speed;
+  cp.contact_softness = p.contact_softness;
+  cp.static_softness = p.static_softness;
+  gather_cv(t, n, a.cap, k, sub, Stage, xs);
+  // incoming cotangents of the outputs
+  constexpr int NY = Stage == kWarm ? kWarmOut : Stage == kPush ? kPushOut : kRelaxOut;
+  if (lane < 12) {
+    int b = lane < 6 ? ia : ib;
+    int f = lane % 6;
+    ys[lane] = b >= 0 ? BB(a, b, f < 3 ? f : f + 1) : 0.0f;
+  } else if (lane < NY) {
+    int j = lane - 12;  // impulses, then friction and twist (relax)
+    int cv = j < 4 ? cvLam + j : (j == 4 ? cvFr : j == 5 ? cvFr + 1 : cvTwist);
+    ys[lane] = KB(a, k, cv);
+  }
+  __syncwarp();
+  float xb[4];
+  int dir[4];
+  if (Stage == kWarm) {
+    warp_vjp<2, kWarmOut>(xs, ys, c_dirs.warm, c_dirs.n_warm,
+                          [&](const SeedIn<float, 2>& in, Dual<float, 2>* y) { warm_fn(in, cp, y); }, xb, dir);
+  } else if (Stage == kPush) {
+    warp_vjp<3, kPushOut>(xs, ys, c_dirs.push, c_dirs.n_push,
+                          [&](const SeedIn<float, 3>& in, Dual<float, 3>* y) { push_fn(in, cp, y); }, xb, dir);
+  } else {
+    warp_vjp<4, kRelaxOut>(xs, ys, c_dirs.relax, c_dirs.n_relax,
+                           [&](const SeedIn<float, 4>& in, Dual<float, 4>* y) { relax_fn(in, cp, y); }, xb, dir);
+  }
+  __syncwarp();
+  constexpr int KD = Stage == kWarm ? 2 : Stage == kPush ? 3 : 4;
+#pragma unroll
+  for (int kk = 0; kk < KD; ++kk) {
+    int d = dir[kk];
+    if (d < 0) continue;
+    float v = xb[kk];
+    if (d < cvDpA) {  // velocities: the input's cotangent replaces the output's
+      int b = d < 6 ? ia : ib;
+      int f = d % 6;
+      if (b >= 0) BB(a, b, f < 3 ? f : f + 1) = v;
+    } else if (d < cvLam) {  // dp, dq: inputs only
+      int b = (d < cvDpB || (d >= cvDqA && d < cvDqB)) ? ia : ib;
+      int f = d < cvDqA ? 8 + (d - cvDpA) % 3 : 12 + (d - cvDqA) % 4;
+      if (b >= 0) BB(a, b, f) += v;
+    } else if (d < cvIma) {  // impulses: replaced when the stage updates them
+      bool updated = Stage == kRelax || (Stage == kPush && d < cvFr);
+      if (updated) KB(a, k, d) = v; else KB(a, k, d) += v;
+    } else {
+      KB(a, k, d) += v;
+    }
+  }
+}
+
+// Reverse of integrate positions for body i (one warp, lanes 0..12).
+__device__ void adj_ip(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub, float* xs,
+                       float* ys) {
+  using namespace ad;
+  int lane = threadIdx.x & 31;
+  const DState& st = t.body[((size_t)sub * 3 + 1) * n + i];
+  if (lane == 0) {
+    xs[0] = st.v.x; xs[1] = st.v.y; xs[2] = st.v.z; xs[3] = st.w.x; xs[4] = st.w.y; xs[5] = st.w.z;
+    xs[6] = st.dp.x; xs[7] = st.dp.y; xs[8] = st.dp.z;
+    xs[9] = st.dq.v.x; xs[10] = st.dq.v.y; xs[11] = st.dq.v.z; xs[12] = st.dq.s;
+  }
+  const int map[13] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14, 15};
+  if (lane < kIP) ys[lane] = BB(a, i, map[lane]);
+  __syncwarp();
+  BParams bp = {};
+  bp.h = p.h; bp.inv_dt = p.inv_dt; bp.max_linear_speed = p.max_linear_speed; bp.flags = st.flags;
+  SeedIn<float, 1> in;
+  in.x = xs;
+  in.dir[0] = lane < kIP ? lane : -1;
+  Dual<float, 1> y[kIP];
+  ip_fn(in, bp, y);
+  float acc = 0.0f;
+  for (int j = 0; j < kIP; ++j) acc += ys[j] * y[j].d[0];
+  __syncwarp();
+  if (lane < kIP) BB(a, i, map[lane]) = acc;
+}
+
+// Reverse of integrate velocities for body i (one warp, two directions per lane).
+__device__ void adj_iv(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub, float* xs,
+                       float* ys) {
+  using namespace ad;
+  int lane = threadIdx.x & 31;
+  const DState& st = t.body[((size_t)sub * 3 + 0) * n + i];
+  const DSim& s = t.sims[i];
+  if (lane == 0) {
+    xs[0] = st.v.x; xs[1] = st.v.y; xs[2] = st.v.z; xs[3] = st.w.x; xs[4] = st.w.y; xs[5] = st.w.z;
+    xs[6] = s.inv_mass;
+    const float* m = &s.inv_inertia_world.cx.x;
+    for (int f = 0; f < 9; ++f) xs[7 + f] = m[f];
+    xs[16] = s.force.x; xs[17] = s.force.y; xs[18] = s.force.z;
+    xs[19] = s.torque.x; xs[20] = s.torque.y; xs[21] = s.torque.z;
+    xs[22] = s.q.v.x; xs[23] = s.q.v.y; xs[24] = s.q.v.z; xs[25] = s.q.s;
+    xs[26] = st.dq.v.x; xs[27] = st.dq.v.y; xs[28] = st.dq.v.z; xs[29] = st.dq.s;
+    const float* in = &s.inertia.cx.x;
+    for (int f = 0; f < 9; ++f) xs[30 + f] = in[f];
+  }
+  const int map[6] = {0, 1, 2, 4, 5, 6};
+  if (lane < kIVOut) ys[lane] = BB(a, i, map[lane]);
+  __syncwarp();
+  BParams bp = {};
+  bp.h = p.h; bp.lin_damp = s.linear_damping; bp.ang_damp = s.angular_damping; bp.grav_scale = s.gravity_scale;
+  bp.gravity = p.gravity;
+  bp.flags = s.flags;
+  SeedIn<float, 2> in;
+  in.x = xs;
+  in.dir[0] = lane;
+  in.dir[1] = lane + 32 < kIVIn ? lane + 32 : -1;
+  Dual<float, 2> y[kIVOut];
+  iv_fn(in, bp, y);
+  float acc[2];
+  for (int kk = 0; kk < 2; ++kk) {
+    acc[kk] = 0.0f;
+    for (int j = 0; j < kIVOut; ++j) acc[kk] += ys[j] * y[j].d[kk];
+  }
+  __syncwarp();
+  for (int kk = 0; kk < 2; ++kk) {
+    int d = in.dir[kk];
+    float v = acc[kk];
+    if (d < 0) continue;
+    if (d < 6) BB(a, i, map[d]) = v;                       // velocities: replaced
+    else if (d == 6) PB(a, i, pbInvMass) += v;
+    else if (d < 16) PB(a, i, pbIiw + d - 7) += v;
+    else if (d < 22) continue;                             // applied force and torque
+    else if (d < 26) CQ(a, i, 4 + d - 22) += v;            // rotation at the step start
+    else if (d < 30) BB(a, i, 12 + d - 26) += v;           // substep rotation dq
+    else PB(a, i, pbInertia + d - 30) += v;                // local inertia
+  }
+}
+
+// Reverse of the solver stages of one step: a persistent launch over the same barriers as the
+// forward solver, phases in reverse order.
+template <bool kGrid>
+__global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBufs a, StepParams p, Control* ctl) {
+  __shared__ int coff[25];
+  __shared__ float xs_s[kAdjThreads / 32][ad::kCV + 2];
+  __shared__ float ys_s[kAdjThreads / 32][32];
+  if (threadIdx.x < 24) coff[threadIdx.x] = t.ctl->color_offset[threadIdx.x];
+  if (threadIdx.x == 24) coff[24] = t.ctl->color_offset[23];
+  __syncthreads();
+  const int n = a.n_awake;
+  const int warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * (kAdjThreads / 32) + warp;
+  const int nw = gridDim.x * (kAdjThreads / 32);
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  int bar = 0;
+  auto contacts = [&](auto stage_tag, int sub) -> bool {
+    constexpr int Stage = decltype(stage_tag)::value;
+    for (int c = kOverflowIndex - 1; c >= 0; --c) {
+      if (coff[c + 1] == coff[c]) continue;
+      for (int k = coff[c] + gw; k < coff[c + 1]; k += nw) adj_contact<Stage>(t, a, p, n, k, sub, xs, ys);
+      if (!phase_sync<kGrid>(ctl, bar)) return false;
+    }
+    return true;
+  };
+  for (int sub = t.substeps - 1; sub >= 0; --sub) {
+    if (!contacts(std::integral_constant<int, kRelax>(), sub)) return;
+    for (int i = gw; i < n; i += nw) adj_ip(t, a, p, n, i, sub, xs, ys);
+    if (!phase_sync<kGrid>(ctl, bar)) return;
+    if (!contacts(std::integral_constant<int, kPush>(), sub)) return;
+    if (!contacts(std::integral_constant<int, kWarm>(), sub)) return;
+    for (int i = gw; i < n; i += nw) adj_iv(t, a, p, n, i, sub, xs, ys);
+    if (!phase_sync<kGrid>(ctl, bar)) return;
+  }
+}
+
+// Reverse of prepare for slot k (one warp): constraint cotangents -> manifold, masses,
+// inverse inertia and friction.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_prepare(StepTape t, AdjBufs a, DW w, StepParams p, int n_slots) {
+  using namespace ad;
+  __shared__ float xs_s[kAdjThreads / 32][kPI + 2];
+  __shared__ float ys_s[kAdjThreads / 32][kCVOwn];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int k = blockIdx.x * (kAdjThreads / 32) + warp;
+  if (k >= n_slots) return;
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  int4 idx = t.planes.idx[k];
+  int ia = idx.x, ib = idx.y, cid = idx.z;
+  const DContact& c = t.post[cid];
+  PParams pp;
+  pp.pc = idx.w & 255;
+  pp.is_static = (idx.w & 256) != 0;
+  pp.warm_start = p.warm_start;
+  if (lane == 0) {
+    const Manifold& m = c.manifold;
+    xs[piN] = m.normal.x; xs[piN + 1] = m.normal.y; xs[piN + 2] = m.normal.z;
+    for (int q = 0; q < 4; ++q) {
+      const ManifoldPoint& mp = m.points[q];
+      xs[pi_point(q, 0)] = mp.anchor_a.x; xs[pi_point(q, 1)] = mp.anchor_a.y; xs[pi_point(q, 2)] = mp.anchor_a.z;
+      xs[pi_point(q, 3)] = mp.anchor_b.x; xs[pi_point(q, 4)] = mp.anchor_b.y; xs[pi_point(q, 5)] = mp.anchor_b.z;
+      xs[pi_point(q, 6)] = mp.separation; xs[pi_point(q, 7)] = mp.normal_impulse;
+    }
+    xs[piFrictionImpulse] = m.friction_impulse.x; xs[piFrictionImpulse + 1] = m.friction_impulse.y;
+    xs[piFrictionImpulse + 2] = m.friction_impulse.z;
+    xs[piTwist] = m.twist_impulse;
+    xs[piFriction] = c.friction;
+  }
+  if (lane == 1 || lane == 2) {
+    int b = lane == 1 ? ia : ib;
+    float im = 0.0f;
+    Sym s = sym_zero();
+    if (b >= 0) { im = t.sims[b].inv_mass; s = sym_from(t.sims[b].inv_inertia_world); }
+    int at = lane == 1 ? piSa : piSb;
+    xs[lane == 1 ? piIma : piImb] = im;
+    xs[at] = s.xx; xs[at + 1] = s.xy; xs[at + 2] = s.xz; xs[at + 3] = s.yy; xs[at + 4] = s.yz; xs[at + 5] = s.zz;
+  }
+  for (int j = lane; j < kCVOwn; j += 32) ys[j] = a.kb[(size_t)j * a.cap + k];
+  __syncwarp();
+  SeedIn<float, 2> in;
+  in.x = xs;
+  in.dir[0] = lane;
+  in.dir[1] = lane + 32 < kPI ? lane + 32 : -1;
+  Dual<float, 2> y[kCVOwn];
+  prepare_fn(in, pp, y);
+  float xb[2];
+  for (int kk = 0; kk < 2; ++kk) {
+    float acc = 0.0f;
+    for (int j = 0; j < kCVOwn; ++j) acc += ys[j] * y[j].d[kk];
+    xb[kk] = acc;
+  }
+  const int sym_to_m3[6] = {0, 1, 2, 4, 5, 8};
+  for (int kk = 0; kk < 2; ++kk) {
+    int d = in.dir[kk];
+    if (d < 0) continue;
+    float v = xb[kk];
+    if (d < piPoint) MB(a, cid, mbN + d) += v;
+    else if (d < piFrictionImpulse) {
+      int q = (d - piPoint) / 8, f = (d - piPoint) % 8;
+      int mf = f < 7 ? f : 8;  // anchor_a, anchor_b, separation; normal impulse
+      MB(a, cid, mb_point(q, mf)) += v;
+    } else if (d < piTwist) MB(a, cid, mbFrictionImpulse + d - piFrictionImpulse) += v;
+    else if (d == piTwist) MB(a, cid, mbTwist) += v;
+    else if (d == piIma) { if (ia >= 0) atomicAdd(&PB(a, ia, pbInvMass), v); }
+    else if (d == piImb) { if (ib >= 0) atomicAdd(&PB(a, ib, pbInvMass), v); }
+    else if (d < piSb) { if (ia >= 0) atomicAdd(&PB(a, ia, pbIiw + sym_to_m3[d - piSa]), v); }
+    else if (d < piFriction) { if (ib >= 0) atomicAdd(&PB(a, ib, pbIiw + sym_to_m3[d - piSb]), v); }
+    else {
+      // friction = sqrt(fa fb) (world_runtime.rs:1305 mix_friction)
+      float fa = w.shapes[c.shape_a].friction, fb = w.shapes[c.shape_b].friction;
+      if (c.friction > 0.0f) {
+        if (ia >= 0) atomicAdd(&PB(a, ia, pbFriction), v * 0.5f * fb / c.friction);
+        if (ib >= 0) atomicAdd(&PB(a, ib, pbFriction), v * 0.5f * fa / c.friction);
+      }
+    }
+  }
+}
+
+// Reverse of the inverse world inertia of finalize (one warp per body, lanes 0..12).
+__global__ void __launch_bounds__(kAdjThreads) k_adj_inertia(StepTape t, AdjBufs a) {
+  using namespace ad;
+  __shared__ float xs_s[kAdjThreads / 32][14];
+  __shared__ float ys_s[kAdjThreads / 32][9];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int i = blockIdx.x * (kAdjThreads / 32) + warp;
+  if (i >= a.n_awake) return;
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  const DSim& s = t.sims[i];
+  if (lane == 0) {
+    xs[0] = s.q.v.x; xs[1] = s.q.v.y; xs[2] = s.q.v.z; xs[3] = s.q.s;
+    const float* m = &s.inv_inertia_local.cx.x;
+    for (int f = 0; f < 9; ++f) xs[4 + f] = m[f];
+  }
+  if (lane < 9) ys[lane] = PB(a, i, pbIiw + lane);
+  __syncwarp();
+  SeedIn<float, 1> in;
+  in.x = xs;
+  in.dir[0] = lane < 13 ? lane : -1;
+  Dual<float, 1> y[9];
+  inv_inertia_fn(in, y);
+  float acc = 0.0f;
+  for (int j = 0; j < 9; ++j) acc += ys[j] * y[j].d[0];
+  __syncwarp();
+  if (lane < 4) CQ(a, i, 4 + lane) += acc;
+  else if (lane < 13) PB(a, i, pbIinv + lane - 4) += acc;
+  if (lane < 9) PB(a, i, pbIiw + lane) = 0.0f;
+}
+
+__device__ __forceinline__ const DSim& sim_at(const StepTape& t, const DW& w, int enc) {
+  return enc >= 0 ? t.sims[enc] : w.ssims[-enc - 2];
+}
+
+// Reverse of the narrowphase for contact cid (one warp): the manifold's cotangent flows to the
+// two bodies' poses at the start of the step and to the manifold state the step started from.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_narrow(StepTape t, AdjBufs a, DW w) {
+  using namespace ad;
+  __shared__ float xs_s[kAdjThreads / 32][kRI + 3];
+  __shared__ float ys_s[kAdjThreads / 32][kMB + 1];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int cid = blockIdx.x * (kAdjThreads / 32) + warp;
+  if (cid >= a.cap) return;
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  int mode = t.mode[cid];
+  if (mode != 1 && mode != 2) {
+    for (int f = lane; f < kMB; f += 32) MB(a, cid, f) = 0.0f;
+    return;
+  }
+  const DContact& post = t.post[cid];
+  const DContact& pre = t.pre[cid];
+  int ea = post.enc_a, eb = post.enc_b;
+  const DSim& sa = sim_at(t, w, ea);
+  const DSim& sb = sim_at(t, w, eb);
+  int pc = post.manifold.point_count;
+  for (int f = lane; f < kMB; f += 32) ys[f] = MB(a, cid, f);
+  __syncwarp();
+  auto body_bar = [&](int enc, int f, float v) {  // f: centre 0..2, rotation 4..7
+    if (enc >= 0) atomicAdd(&CQ(a, enc, f), v);
+  };
+  if (mode == 2) {
+    const DShape& A = w.shapes[post.shape_a];
+    const DShape& B = w.shapes[post.shape_b];
+    Pos pa = {sa.px, sa.py, sa.pz}, pb = {sb.px, sb.py, sb.pz};
+    if (lane == 0) {
+      for (int f = 0; f < 3; ++f) { xs[fiCa + f] = 0.0f; xs[fiCb + f] = 0.0f; }
+      xs[fiQa] = sa.q.v.x; xs[fiQa + 1] = sa.q.v.y; xs[fiQa + 2] = sa.q.v.z; xs[fiQa + 3] = sa.q.s;
+      xs[fiQb] = sb.q.v.x; xs[fiQb + 1] = sb.q.v.y; xs[fiQb + 2] = sb.q.v.z; xs[fiQb + 3] = sb.q.s;
+    }
+    __syncwarp();
+    NarrowCase nc = {post.sat.type, post.sat.index_a, post.sat.index_b, post.sat.hit};
+    SeedIn<float, 1> in;
+    in.x = xs;
+    in.dir[0] = lane < kFI ? lane : -1;
+    Dual<float, 1> y[kFO];
+    uint32_t ids[4];
+    int got = narrow_box_fn(in, pa, pb, w.hulls[A.hull], w.hulls[B.hull], nc, y, ids);
+    bool same = got == pc;
+    for (int q = 0; same && q < pc; ++q) same = ids[q] == post.manifold.points[q].feature_id;
+    if (!same) {
+      if (lane == 0) atomicAdd(a.mismatch, 1);
+    } else {
+      float acc = 0.0f;
+      for (int j = 0; j < 3; ++j) acc += ys[mbN + j] * y[j].d[0];
+      for (int q = 0; q < pc; ++q) {
+        for (int f = 0; f < 6; ++f) acc += ys[mb_point(q, f)] * y[3 + 7 * q + f].d[0];
+        acc += (ys[mb_point(q, 6)] + ys[mb_point(q, 7)]) * y[3 + 7 * q + 6].d[0];
+      }
+      if (lane < 3) body_bar(ea, lane, acc);
+      else if (lane < 7) body_bar(ea, 4 + lane - 3, acc + ys[mbRotA + lane - 3]);
+      else if (lane < 10) body_bar(eb, lane - 7, acc);
+      else if (lane < 14) body_bar(eb, 4 + lane - 10, acc + ys[mbRotB + lane - 10]);
+    }
+    __syncwarp();
+    // the state before the step: matched normal impulses, and the friction and twist
+    // impulses a persisting manifold keeps
+    if (lane == 0) {
+      float out[kMB];
+      for (int f = 0; f < kMB; ++f) out[f] = 0.0f;
+      int old_count = pre.manifold_count > 0 ? pre.manifold.point_count : 0;
+      if (old_count > 0) {
+        bool used[4] = {false, false, false, false};
+        for (int i = 0; i < pc; ++i) {
+          uint32_t fid = post.manifold.points[i].feature_id;
+          for (int j = 0; j < old_count; ++j) {
+            if (!used[j] && pre.manifold.points[j].feature_id == fid) {
+              out[mb_point(j, 8)] += ys[mb_point(i, 8)];
+              used[j] = true;
+              break;
+            }
+          }
+        }
+        for (int f = 0; f < 3; ++f) out[mbFrictionImpulse + f] = ys[mbFrictionImpulse + f];
+        out[mbTwist] = ys[mbTwist];
+      }
+      for (int f = 0; f < kMB; ++f) MB(a, cid, f) = out[f];
+    }
+  } else {
+    // recycled: separations recomputed from the poses and the cached manifold
+    Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+    if (lane == 0) {
+      for (int f = 0; f < 6; ++f) xs[riCa + f] = 0.0f;
+      xs[riQa] = sa.q.v.x; xs[riQa + 1] = sa.q.v.y; xs[riQa + 2] = sa.q.v.z; xs[riQa + 3] = sa.q.s;
+      xs[riQb] = sb.q.v.x; xs[riQb + 1] = sb.q.v.y; xs[riQb + 2] = sb.q.v.z; xs[riQb + 3] = sb.q.s;
+      Q ra = post.cached_rot_a, rb = post.cached_rot_b;
+      xs[riRotA] = ra.v.x; xs[riRotA + 1] = ra.v.y; xs[riRotA + 2] = ra.v.z; xs[riRotA + 3] = ra.s;
+      xs[riRotB] = rb.v.x; xs[riRotB + 1] = rb.v.y; xs[riRotB + 2] = rb.v.z; xs[riRotB + 3] = rb.s;
+      const Manifold& m = post.manifold;
+      xs[riN] = m.normal.x; xs[riN + 1] = m.normal.y; xs[riN + 2] = m.normal.z;
+      for (int q = 0; q < 4; ++q) {
+        const ManifoldPoint& mp = m.points[q];
+        xs[ri_point(q, 0)] = mp.anchor_a.x; xs[ri_point(q, 1)] = mp.anchor_a.y; xs[ri_point(q, 2)] = mp.anchor_a.z;
+        xs[ri_point(q, 3)] = mp.anchor_b.x; xs[ri_point(q, 4)] = mp.anchor_b.y; xs[ri_point(q, 5)] = mp.anchor_b.z;
+        xs[ri_point(q, 6)] = mp.base_separation;
+      }
+    }
+    __syncwarp();
+    SeedIn<float, 2> in;
+    in.x = xs;
+    in.dir[0] = lane;
+    in.dir[1] = lane + 32 < kRI ? lane + 32 : -1;
+    Dual<float, 2> y[4];
+    recycle_fn(in, ca, cb, pc, y);
+    float xb[2];
+    for (int kk = 0; kk < 2; ++kk) {
+      float acc = 0.0f;
+      for (int q = 0; q < pc; ++q) acc += ys[mb_point(q, 6)] * y[q].d[kk];
+      xb[kk] = acc;
+    }
+    __syncwarp();
+    // the state before the step is the manifold itself, except the overwritten separations
+    for (int f = lane; f < kMB; f += 32) {
+      bool is_sep = f >= mbPoint && f < mbFrictionImpulse && (f - mbPoint) % 9 == 6;
+      MB(a, cid, f) = is_sep ? 0.0f : ys[f];
+    }
+    __syncwarp();
+    for (int kk = 0; kk < 2; ++kk) {
+      int d = in.dir[kk];
+      if (d < 0) continue;
+      float v = xb[kk];
+      if (d < riCb) body_bar(ea, d - riCa, v);
+      else if (d < riQa) body_bar(eb, d - riCb, v);
+      else if (d < riQb) body_bar(ea, 4 + d - riQa, v);
+      else if (d < riRotA) body_bar(eb, 4 + d - riQb, v);
+      else if (d < riRotB) MB(a, cid, mbRotA + d - riRotA) += v;
+      else if (d < riN) MB(a, cid, mbRotB + d - riRotB) += v;
+      else if (d < riPoint) MB(a, cid, mbN + d - riN) += v;
+      else {
+        int q = (d - riPoint) / 7, f = (d - riPoint) % 7;
+        MB(a, cid, mb_point(q, f < 6 ? f : 7)) += v;  // anchors; base separation
+      }
+    }
+  }
+}
+
+// Seeds (cotangents of the final state, body id order) and results.
+__global__ void k_adj_seed(AdjBufs a, const int* body_loc, int nb, const float* dpos, const float* drot,
+                           const float* dlin, const float* dang) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    int loc = body_loc[i];
+    if (loc < 0) continue;
+    for (int f = 0; f < 3; ++f) {
+      CQ(a, loc, f) = dpos ? dpos[3 * i + f] : 0.0f;
+      BB(a, loc, f) = dlin ? dlin[3 * i + f] : 0.0f;
+      BB(a, loc, 4 + f) = dang ? dang[3 * i + f] : 0.0f;
+    }
+    for (int f = 0; f < 4; ++f) CQ(a, loc, 4 + f) = drot ? drot[4 * i + f] : 0.0f;
+  }
+}
+// out per body id: lin 3 | ang 3 | mass | friction | pos 3 | rot 4  (16 floats)
+__global__ void k_adj_result(AdjBufs a, const DW w, const int* body_loc, int nb, float* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+    float* o = out + (size_t)16 * i;
+    int loc = body_loc[i];
+    if (loc < 0) {
+      for (int f = 0; f < 16; ++f) o[f] = 0.0f;
+      continue;
+    }
+    for (int f = 0; f < 3; ++f) { o[f] = BB(a, loc, f); o[3 + f] = BB(a, loc, 4 + f); o[8 + f] = CQ(a, loc, f); }
+    for (int f = 0; f < 4; ++f) o[11 + f] = CQ(a, loc, 4 + f);
+    // inv_mass = 1/m and the local inverse inertia scale as 1/m
+    const DSim& s = w.asims[loc];
+    float im = s.inv_mass;
+    const float* il = &s.inv_inertia_local.cx.x;
+    float dot_ii = 0.0f;
+    for (int f = 0; f < 9; ++f) dot_ii += PB(a, loc, pbIinv + f) * il[f];
+    // the local inertia (gyroscopic step) scales as m
+    const float* ii = &s.inertia.cx.x;
+    float dot_i = 0.0f;
+    for (int f = 0; f < 9; ++f) dot_i += PB(a, loc, pbInertia + f) * ii[f];
+    o[6] = -PB(a, loc, pbInvMass) * im * im - dot_ii * im + dot_i * im;
+    o[7] = PB(a, loc, pbFriction);
+    o[15] = 0.0f;
+  }
+}
+
+// Snapshot copies of device buffers: dst[i] <- src[i] for each listed buffer.
+struct CopyOp { const char* src; char* dst; size_t bytes; };
+__global__ void k_multi_copy(const CopyOp* ops, int n_ops) {
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  for (int o = 0; o < n_ops; ++o) {
+    CopyOp op = ops[o];
+    size_t n16 = op.bytes / 16;
+    const float4* s = (const float4*)op.src;
+    float4* d = (float4*)op.dst;
+    for (size_t i = tid; i < n16; i += stride) d[i] = s[i];
+    for (size_t i = n16 * 16 + tid; i < op.bytes; i += stride) op.dst[i] = op.src[i];
+  }
+}
+
+}  // namespace nsd

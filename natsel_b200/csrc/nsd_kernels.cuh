@@ -58,6 +58,9 @@ struct DW {
   int* world_cbase; int* world_shape; int* pool_top; int* pool_next; int* ovf_count; int* large_off;
   int* bp_world;  // sub-world of each sorted small proxy
   int* collide_list;  // per pair kind k: ids at collide_list + k * cap needing a full update
+  // Optional record of each contact's narrowphase outcome (0 none or disjoint, 1 recycled,
+  // 2 new manifold, 3 no points), written only while the adjoint replays a step.
+  uint8_t* np_mode;
 };
 
 struct JointRanges { int off[25]; };
@@ -499,6 +502,7 @@ __device__ bool collide_recycle(const DW& w, int cid) {
   if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
     c.flags = (c.flags | cSimDisjoint) & ~cSimTouching;
     atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
+    if (w.np_mode) w.np_mode[cid] = 0;
     return false;
   }
   const DSim& sa = sim_of(w, c.enc_a);
@@ -550,6 +554,7 @@ __device__ bool collide_recycle(const DW& w, int cid) {
         }
         recycled = true;
         atomicAdd(&w.ctl->recycled, 1);
+        if (w.np_mode) w.np_mode[cid] = 1;
       }
     }
   }
@@ -573,6 +578,7 @@ __device__ void collide_full(const DW& w, int cid) {
     c.cached_rel = inv_mul_wxf(xa, xb);
     c.flags |= cRelativeValid;
     bool touching = update_contact(w, c, sa.local_center, xa, sb.local_center, xb);
+    if (w.np_mode) w.np_mode[cid] = touching ? 2 : 3;
     if (touching && !was_touching) { c.flags |= cSimStarted; changed = true; }
     else if (!touching && was_touching) { c.flags |= cSimStopped; changed = true; }
     if (touching && c.manifold_count > 0) {

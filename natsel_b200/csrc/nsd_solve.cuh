@@ -947,10 +947,36 @@ __device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges
 // Phase codes: contact phases stage * 32 + color; the rest as below.
 constexpr int kPhaseIntegrateVelocity = 1000, kPhaseIntegratePosition = 1001, kPhaseOverflow = 2000;
 
+// Record of the solver's inputs kept while the adjoint replays a step (kTape): per substep
+// three body rows (before integrate-velocities, before and after integrate-positions), the
+// velocities and normal impulses each push and relax update reads, the friction and twist
+// impulses each relax update reads, and the final friction and twist impulses.
+struct SolveTape {
+  DState* body;    // [substep][3][n_awake]
+  float4* push;    // [substep][4][cap]: vA|l0, wA|l1, vB|l2, wB|l3
+  float4* relax;   // [substep][5][cap]: the same, then fr.x, fr.y, twist
+  float4* fin;     // [cap]
+};
+
+__device__ __forceinline__ void tape_contact(const DW& w, const SolveTape& tp, int sub, int stage, int k,
+                                             const CData& d) {
+  const int cap = w.cp.cap;
+  DState ba = state_at(w, d.c.ia), bb = state_at(w, d.c.ib);
+  float l[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) l[q] = q < d.c.pc ? d.pimp[q].x : 0.0f;
+  float4* rows = stage == kPush ? tp.push + (size_t)sub * 4 * cap : tp.relax + (size_t)sub * 5 * cap;
+  rows[k] = make_float4(ba.v.x, ba.v.y, ba.v.z, l[0]);
+  rows[(size_t)cap + k] = make_float4(ba.w.x, ba.w.y, ba.w.z, l[1]);
+  rows[2 * (size_t)cap + k] = make_float4(bb.v.x, bb.v.y, bb.v.z, l[2]);
+  rows[3 * (size_t)cap + k] = make_float4(bb.w.x, bb.w.y, bb.w.z, l[3]);
+  if (stage == kRelax) rows[4 * (size_t)cap + k] = make_float4(d.fr.x, d.fr.y, d.cb.w, 0.0f);
+}
+
 // Persistent solver. kGrid: one cooperative launch over the whole GPU, phases separated by
 // grid_sync_acq_rel; otherwise one thread-block cluster separated by barrier.cluster.
-template <bool kGrid>
-__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, JointRanges jr) {
+template <bool kGrid, bool kTape>
+__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, JointRanges jr, SolveTape tp) {
   __shared__ int coff[25];
   __shared__ int phases[3 * 25 + 2];  // one substep
   __shared__ int rphases[25];         // one restitution iteration
@@ -988,10 +1014,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
   int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
+    const int sub = s / n_ph;
     if (ph == kPhaseIntegrateVelocity) {
-      for (int i = g; i < w.n_awake; i += stride) apply_iv(w, p, i, load_iv(w, i));
+      for (int i = g; i < w.n_awake; i += stride) {
+        if (kTape) tp.body[((size_t)sub * 3) * w.n_awake + i] = w.states[i];
+        apply_iv(w, p, i, load_iv(w, i));
+      }
     } else if (ph == kPhaseIntegratePosition) {
-      for (int i = g; i < w.n_awake; i += stride) apply_ip(w, p, i, w.states[i]);
+      for (int i = g; i < w.n_awake; i += stride) {
+        DState st = w.states[i];
+        if (kTape) tp.body[((size_t)sub * 3 + 1) * w.n_awake + i] = st;
+        apply_ip(w, p, i, st);
+        if (kTape) tp.body[((size_t)sub * 3 + 2) * w.n_awake + i] = w.states[i];
+      }
     } else if (ph >= kPhaseOverflow) {
       run_overflow(w, p, jr, ph - kPhaseOverflow);
     } else {
@@ -1007,6 +1042,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
           int k = coff[c] + (t - nj);
           CData d;
           load_direct(w.cp, k, stage, d);
+          if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
           run_contact(w, p, k, stage, d);
         }
       }
@@ -1015,7 +1051,10 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
   }
   // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
   for (int wi = g; wi < w.n_worlds; wi += stride) store_overflow(w, w.world_cbase[wi], w.ovf_count[wi]);
-  for (int k = g; k < coff[kOverflowIndex]; k += stride) store_constraint(w, k);
+  for (int k = g; k < coff[kOverflowIndex]; k += stride) {
+    if (kTape) tp.fin[k] = make_float4(w.cp.fr[k].x, w.cp.fr[k].y, w.cp.cb[k].w, 0.0f);
+    store_constraint(w, k);
+  }
 }
 
 // solver_integration.rs:587 finalize_body_range (sleep disabled: bodies never sleep; a fast

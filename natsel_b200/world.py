@@ -86,6 +86,8 @@ EXPORTED = [
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
+    "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
+    "ns_adjoint_selfcheck",
 ]
 
 
@@ -131,6 +133,12 @@ def load_library(path=LIB_PATH):
     lib.ns_world_subworld_count.argtypes = [P]
     lib.ns_world_subworld_bodies.argtypes = [P, P]
     lib.ns_world_subworld_hashes.argtypes = [P, P]
+    lib.ns_world_tape_begin.argtypes = [P, ctypes.c_int]
+    lib.ns_world_tape_end.argtypes = [P]
+    lib.ns_world_tape_free.argtypes = [P]
+    lib.ns_world_tape_info.argtypes = [P, P]
+    lib.ns_world_vjp.argtypes = [P] * 11
+    lib.ns_adjoint_selfcheck.argtypes = [ctypes.c_int, ctypes.c_int, P]
     _lib = lib
     return lib
 
@@ -310,3 +318,58 @@ class World:
 
     def stream(self):
         return self._lib.ns_world_stream(self._w)
+
+    # ---- adjoint ---------------------------------------------------------------------------
+    def tape_begin(self, checkpoint_substeps=8):
+        """Record the following steps for vjp(), with a checkpoint every checkpoint_substeps."""
+        self._check(self._lib.ns_world_tape_begin(self._w, int(checkpoint_substeps)))
+
+    def tape_end(self):
+        self._check(self._lib.ns_world_tape_end(self._w))
+
+    def tape_free(self):
+        self._check(self._lib.ns_world_tape_free(self._w))
+
+    def tape_info(self):
+        """steps, checkpoints, replay mismatches, vjp calls, recording, checkpoint interval."""
+        out = np.zeros(6, np.int64)
+        self._check(self._lib.ns_world_tape_info(self._w, _ptr(out)))
+        return out
+
+    def vjp(self, dpos=None, drot=None, dlin=None, dang=None):
+        """Pull cotangents of the final state (body id order) back to the tape's start.
+
+        Returns a dict of float32 arrays: lin0, ang0 (n x 3), mass, friction (n), pos0 (n x 3),
+        rot0 (n x 4)."""
+        n = self.body_count
+        def arr(a, w):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.float32)
+            if a.shape != (n, w):
+                raise ValueError(f"cotangent must be n_bodies x {w}")
+            return a
+        ins = [arr(dpos, 3), arr(drot, 4), arr(dlin, 3), arr(dang, 3)]
+        out = dict(lin0=np.zeros((n, 3), np.float32), ang0=np.zeros((n, 3), np.float32),
+                   mass=np.zeros(n, np.float32), friction=np.zeros(n, np.float32),
+                   pos0=np.zeros((n, 3), np.float32), rot0=np.zeros((n, 4), np.float32))
+        self._check(self._lib.ns_world_vjp(self._w, *[_ptr(a) for a in ins], _ptr(out["lin0"]), _ptr(out["ang0"]),
+                                           _ptr(out["mass"]), _ptr(out["friction"]), _ptr(out["pos0"]),
+                                           _ptr(out["rot0"])))
+        return out
+
+
+ADJOINT_CHECKS = ["warm_start", "push", "relax", "prepare", "integrate_velocities", "integrate_positions",
+                  "finalize_rotation", "inverse_inertia", "recycle", "box_face", "box_any", "box_edge"]
+
+
+def adjoint_selfcheck(which, seed):
+    """f64 check of one local derivative of the adjoint on the host (no GPU): returns the
+    worst relative difference between the dual-number VJP and central differences, and the
+    separating-axis kind of the box cases (-1 otherwise)."""
+    lib = load_library()
+    out = np.array([-1.0, -1.0])
+    st = lib.ns_adjoint_selfcheck(int(which), int(seed), _ptr(out))
+    if st != 0:
+        raise NsError(st, lib.ns_last_error(None).decode())
+    return float(out[0]), int(out[1])

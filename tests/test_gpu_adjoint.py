@@ -1,0 +1,219 @@
+"""The adjoint (ns_world_vjp) on the GPU: gradients of a rollout's loss against central finite
+differences of the forward step, and the tape's bookkeeping.
+
+The scenes keep one contact set over the horizon (boxes sliding and spinning on the ground, a
+box running into a lighter one, a box sliding on another). Contact solves still have kinks (an
+impulse meeting its clamp at zero, a corner point unloading); where one falls inside the
+difference interval the central difference does not converge, and below h ~ 1e-3 the f32
+rounding of the trajectory dominates it. So each entry is differenced at h and 2 h, and the
+entries of at least 5 % of their kind's largest whose two differences agree to 0.2 % are
+checked: they must match the adjoint to 1e-3 relative plus twice that spread. Each scene must
+yield a minimum number of checked entries of every kind it exercises.
+"""
+import numpy as np
+import pytest
+
+from natsel_b200.world import DYNAMIC_BODY, STATIC_BODY, NsError, World
+
+pytestmark = pytest.mark.gpu
+
+DT, SUBSTEPS, STEPS = 1.0 / 60.0, 4, 8
+WORLD = dict(gravity=(0.0, -9.81, 0.0), enable_sleep=0, enable_continuous=0)
+
+# (position, half extents, linear velocity, angular velocity, density, friction); resting boxes
+# start 2 mm into their support, inside the push's penetration branch
+SLIDERS = [
+    ((0.0, 0.498, 0.0), (0.5, 0.5, 0.5), (2.0, 0.0, 0.5), (0.0, 0.8, 0.0), 1000.0, 0.6),
+    ((4.0, 0.298, 1.0), (0.4, 0.3, 0.5), (-1.5, 0.0, 0.3), (0.0, -0.5, 0.0), 800.0, 0.5),
+    ((-3.0, 0.498, -2.0), (0.5, 0.5, 0.5), (0.5, 0.0, 1.8), (0.0, 0.3, 0.0), 1200.0, 0.7),
+]
+# a box sliding on slippery ground runs into a lighter one (momentum exchange: the masses matter)
+COLLIDE = [
+    ((-1.2, 0.498, 0.0), (0.5, 0.5, 0.5), (3.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1000.0, 0.5),
+    ((0.0, 0.398, 0.05), (0.4, 0.4, 0.4), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 500.0, 0.5),
+]
+STACK = [
+    ((0.0, 0.498, 0.0), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1000.0, 0.8),
+    ((0.05, 1.394, 0.02), (0.4, 0.4, 0.4), (1.2, 0.0, 0.2), (0.0, 0.4, 0.0), 600.0, 0.4),
+]
+
+
+def build(bodies, checkpoint=None, ground_friction=0.6):
+    w = World(**WORLD)
+    g = w.create_body(type=STATIC_BODY, position=(0.0, -0.5, 0.0))
+    w.create_box(g, 20.0, 0.5, 20.0, friction=ground_friction)
+    for pos, he, v, om, rho, mu in bodies:
+        b = w.create_body(type=DYNAMIC_BODY, position=pos, linear_velocity=v, angular_velocity=om, enable_sleep=False)
+        w.create_box(b, *he, density=rho, friction=mu)
+    if checkpoint is not None:
+        w.tape_begin(checkpoint)
+    return w
+
+
+def targets(bodies):
+    return np.array([[p[0] + 1.0, p[1], p[2] - 0.5] for p, *_ in bodies])
+
+
+def loss(bodies, steps=STEPS, ground_friction=0.6):
+    w = build(bodies, None, ground_friction)
+    for _ in range(steps):
+        w.step(DT, SUBSTEPS)
+    pos = w.bodies()[0][1:]
+    w.close()
+    return float(np.sum((pos - targets(bodies)) ** 2))
+
+
+def adjoint(bodies, checkpoint=8, steps=STEPS, ground_friction=0.6):
+    w = build(bodies, checkpoint, ground_friction)
+    for _ in range(steps):
+        w.step(DT, SUBSTEPS)
+    pos = w.bodies()[0]
+    dpos = np.zeros_like(pos, dtype=np.float32)
+    dpos[1:] = 2.0 * (pos[1:] - targets(bodies))
+    h0 = w.state_hash()
+    g = w.vjp(dpos=dpos)
+    info = w.tape_info()
+    h1 = w.state_hash()
+    w.close()
+    return g, info, h0, h1
+
+
+def perturbed(bodies, i, field, comp, delta):
+    """bodies with one input moved by delta; returns them and the input's new value (the
+    velocities are float32 in the body definition, so the step taken is the rounded one)."""
+    rows = [list(b) for b in bodies]
+    if field in (2, 3):
+        vec = list(rows[i][field])
+        vec[comp] = float(np.float32(vec[comp] + delta))
+        rows[i][field] = tuple(vec)
+        value = vec[comp]
+    else:
+        rows[i][field] = rows[i][field] + delta
+        value = rows[i][field]
+    return [tuple(r) for r in rows], value
+
+
+def fd(bodies, i, field, comp, h, ground_friction=0.6):
+    up, a = perturbed(bodies, i, field, comp, h)
+    dn, b = perturbed(bodies, i, field, comp, -h)
+    return (loss(up, STEPS, ground_friction) - loss(dn, STEPS, ground_friction)) / (a - b)
+
+
+def check(bodies, ground_friction=0.6):
+    g, info, h0, h1 = adjoint(bodies, ground_friction=ground_friction)
+    assert info[2] == 0, "narrowphase replay did not reproduce a recorded manifold"
+    assert h0 == h1, "the adjoint must leave the world in its final state"
+    rows = []  # kind, adjoint, fd(h), fd(2 h)
+    for i, (pos, he, v, om, rho, mu) in enumerate(bodies):
+        vol = 8.0 * he[0] * he[1] * he[2]
+        entries = [("velocity", g["lin0"][i + 1, c], 2, c, 1e-3) for c in range(3)]
+        entries += [("velocity", g["ang0"][i + 1, c], 3, c, 1e-3) for c in range(3)]
+        entries += [("mass", g["mass"][i + 1] * vol, 4, 0, 1e-3 * rho), ("friction", g["friction"][i + 1], 5, 0, 1e-3)]
+        for kind, a, field, c, h in entries:
+            rows.append((kind, float(a), fd(bodies, i, field, c, h, ground_friction),
+                         fd(bodies, i, field, c, 2 * h, ground_friction)))
+    scale = {}
+    for k, a, f1, f2 in rows:
+        scale[k] = max(scale.get(k, 0.0), abs(f1))
+    checked, bad = [], []
+    for k, a, f1, f2 in rows:
+        spread = abs(f1 - f2)
+        print(f"{k:9s} adjoint {a: .6e}  fd(h) {f1: .6e}  fd(2h) {f2: .6e}")
+        if abs(f1) < 0.05 * scale[k] or spread > 2e-3 * abs(f1):
+            continue  # under the differences' resolution, or a kink inside the interval
+        checked.append((k, a, f1))
+        if abs(a - f1) > 1e-3 * abs(f1) + 2.0 * spread:
+            bad.append((k, a, f1, f2))
+    assert not bad, bad
+    return rows, checked
+
+
+def checked_count(checked, kind):
+    return sum(1 for k, a, f in checked if k == kind)
+
+
+def test_sliding_boxes_gradients_match_finite_differences():
+    rows, checked = check(SLIDERS)
+    assert checked_count(checked, "velocity") >= 4
+    assert checked_count(checked, "friction") >= 2
+
+
+def test_colliding_boxes_gradients_match_finite_differences():
+    rows, checked = check(COLLIDE, ground_friction=0.05)
+    assert checked_count(checked, "velocity") >= 2
+    assert checked_count(checked, "mass") >= 1
+
+
+def test_box_on_box_gradients_match_finite_differences():
+    rows, checked = check(STACK)
+    assert checked_count(checked, "velocity") >= 2
+
+
+def test_spinning_box_rotation_gradient_matches_finite_differences():
+    # twist friction slows a box spinning on the ground: loss on the final rotation
+    body = [((0.0, 0.498, 0.0), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0), (0.0, 2.0, 0.0), 1000.0, 0.6)]
+    q_target = np.array([0.0, 0.3, 0.0, 0.954], np.float64)
+
+    def spin_loss(b):
+        w = build(b)
+        for _ in range(STEPS):
+            w.step(DT, SUBSTEPS)
+        q = w.bodies()[1][1].astype(np.float64)
+        w.close()
+        return float(np.sum((q - q_target) ** 2))
+
+    w = build(body, 8)
+    for _ in range(STEPS):
+        w.step(DT, SUBSTEPS)
+    rot = w.bodies()[1]
+    drot = np.zeros_like(rot)
+    drot[1] = 2.0 * (rot[1] - q_target)
+    g = w.vjp(drot=drot)
+    w.close()
+    for field, comp, a in ((3, 1, g["ang0"][1, 1]), (5, 0, g["friction"][1])):
+        up, hi = perturbed(body, 0, field, comp, 1e-3)
+        dn, lo = perturbed(body, 0, field, comp, -1e-3)
+        f = (spin_loss(up) - spin_loss(dn)) / (hi - lo)
+        assert abs(a - f) <= 1e-3 * abs(f), (field, a, f)
+
+
+def test_checkpoint_interval_does_not_change_gradients():
+    g1 = adjoint(SLIDERS, checkpoint=4)[0]
+    g2 = adjoint(SLIDERS, checkpoint=1000)[0]
+    for k in g1:
+        np.testing.assert_allclose(g1[k], g2[k], rtol=1e-5, atol=1e-6)
+
+
+def test_vjp_of_velocity_cotangent_is_identity_without_contacts():
+    # a free box in flight: final velocity = initial velocity + g t, so dL/dv0 = dL/dv
+    w = World(**WORLD)
+    b = w.create_body(type=DYNAMIC_BODY, position=(0.0, 10.0, 0.0), linear_velocity=(1.0, 2.0, 3.0),
+                      angular_velocity=(0.1, 0.2, 0.3), enable_sleep=False)
+    w.create_box(b, 0.5, 0.5, 0.5)
+    w.tape_begin(8)
+    for _ in range(5):
+        w.step(DT, SUBSTEPS)
+    dlin = np.array([[0.3, -0.2, 0.7]], np.float32)
+    g = w.vjp(dlin=dlin)
+    np.testing.assert_allclose(g["lin0"], dlin, rtol=1e-6)
+    # position after T: p0 + v0 T + ..., so dL/dv0 from a position cotangent is T per unit
+    g = w.vjp(dpos=np.array([[1.0, 0.0, 0.0]], np.float32))
+    np.testing.assert_allclose(g["lin0"][0, 0], 5 * DT, rtol=1e-5)
+    np.testing.assert_allclose(g["pos0"][0], [1.0, 0.0, 0.0], rtol=1e-6)
+    w.close()
+
+
+def test_adjoint_scope_is_enforced():
+    w = World(**WORLD)
+    b = w.create_body(type=DYNAMIC_BODY, position=(0.0, 1.0, 0.0), enable_sleep=False)
+    w.create_sphere(b, 0.5)
+    with pytest.raises(NsError) as e:
+        w.tape_begin(8)
+    assert e.value.code == 6
+    w.close()
+    w = build(SLIDERS, checkpoint=8)
+    with pytest.raises(NsError):
+        w.apply_forces(force=np.zeros((4, 3), np.float32))
+    with pytest.raises(NsError):
+        w.step(0.0, SUBSTEPS)
+    w.close()
