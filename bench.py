@@ -51,7 +51,13 @@ WORKLOADS = {
                        "10 000-body pile) of N ~ log-uniform(32, 512) bodies, stepped together; 60 Hz, 4 substeps, FP32"),
     "jointed_chains": ("jointed_chains", {}, "2 000 chains of 24 capsules on limited revolute joints + 4 000 boxes; "
                                              "60 Hz, 8 substeps, FP32"),
+    "differentiable_rollout": ("differentiable_rollout", {},
+                               "1 024 unit cubes on a ground box with v0 ~ N(0, 2^2) m/s and w0 ~ N(0, 1) rad/s, "
+                               "64 steps at 60 Hz with 4 substeps, loss sum |x_final - x_target|^2, gradients "
+                               "w.r.t. initial velocities, masses and frictions by the adjoint (ns_world_vjp) "
+                               "with checkpoints every 8 substeps; FP32"),
 }
+ROLLOUT_STEPS, ROLLOUT_CHECKPOINT = 64, 8
 
 
 def parse_args(argv=None):
@@ -353,6 +359,12 @@ def run_natsel_arm(args):
         uuids = gathered
 
     scene, kw, desc = WORKLOADS[args.workload]
+    if scene == "differentiable_rollout":
+        run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uuids, desc)
+        if world_size > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     world, info, sub = build_gpu_world(args, local_rank)
     bodies = info["dynamic_bodies"]
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -433,6 +445,183 @@ def run_natsel_arm(args):
     if world_size > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def rollout_fd_check(args, local_rank, g, n_entries=12, seed=11):
+    """Central differences of the rollout's loss for a seeded sample of gradient entries
+    (initial velocity components, masses, frictions), each at h and 2 h; entries whose two
+    differences agree to 0.2 % are compared with the adjoint (the rest straddle a contact
+    kink: a clamp, a corner unloading or a contact beginning inside the interval)."""
+    import numpy as np
+    from natsel_b200 import scenes
+    from natsel_b200.world import World, default_world_def
+    s = scenes.WORLD_SETTINGS["differentiable_rollout"]
+
+    def loss(what, body, comp, delta):
+        w = World(default_world_def(gravity=s["gravity"], enable_continuous=0, device=local_rank))
+        info = scenes.differentiable_rollout(w, perturb=(what, body, comp, delta))
+        for _ in range(ROLLOUT_STEPS):
+            w.step(DT, 4)
+        pos = w.bodies()[0][1:]
+        w.close()
+        return float(np.sum((pos - info["targets"]) ** 2)), info["perturbed_value"]
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rows = []
+    for e in range(n_entries):
+        body = int(rng.integers(0, 1024))
+        kind = ("velocity", "velocity", "mass", "friction")[e % 4]
+        comp = int(rng.integers(0, 3))
+        if kind == "velocity":
+            what, hs, adj = "v0", 1e-3, float(g["lin0"][body + 1, comp])
+        elif kind == "mass":
+            # a unit cube: mass = density * 1 m^3, so d/d(density) = d/d(mass)
+            what, hs, adj, comp = "density", 1.0, float(g["mass"][body + 1]), 0
+        else:
+            what, hs, adj, comp = "friction", 1e-3, float(g["friction"][body + 1]), 0
+        fds = []
+        for h in (hs, 2 * hs):
+            lu, vu = loss(what, body, comp, h)
+            ld, vd = loss(what, body, comp, -h)
+            fds.append((lu - ld) / (vu - vd))
+        rows.append({"entry": kind, "body": body, "component": comp, "adjoint": adj, "fd_h": fds[0],
+                     "fd_2h": fds[1]})
+    clean = [r for r in rows if abs(r["fd_h"] - r["fd_2h"]) <= 2e-3 * abs(r["fd_h"]) and r["fd_h"] != 0.0]
+    rel = [abs(r["adjoint"] - r["fd_h"]) / abs(r["fd_h"]) for r in clean]
+    return {"entries": len(rows), "smooth_entries": len(clean),
+            "max_rel_err_smooth": max(rel) if rel else None,
+            "median_rel_err_smooth": statistics.median(rel) if rel else None,
+            "within_1e-3_plus_spread": sum(1 for r in clean if abs(r["adjoint"] - r["fd_h"]) <= 1e-3 * abs(r["fd_h"]) +
+                                           2 * abs(r["fd_h"] - r["fd_2h"])),
+            "rows": rows}
+
+
+def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uuids, desc):
+    """The differentiable rollout: per timed repetition, the plain forward rollout (64 steps, no
+    tape), the same rollout recorded on a tape (checkpoint copies every 8 substeps) and its
+    vector-Jacobian product, each timed with CUDA events on the world's stream. The headline
+    value is body-substeps/s through the recorded forward plus the adjoint; the adjoint's cost
+    is reported against the plain forward's."""
+    import numpy as np
+    import torch
+    from natsel_b200 import scenes
+    from natsel_b200.world import World, default_world_def
+    s = scenes.WORLD_SETTINGS["differentiable_rollout"]
+
+    def fresh():
+        w = World(default_world_def(gravity=s["gravity"], enable_continuous=0, device=local_rank))
+        info = scenes.differentiable_rollout(w)
+        return w, info
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    plain_ms, taped_ms, vjp_ms, e2e_ms, launches = [], [], [], [], []
+    phase = np.zeros(5)
+    sampler = None
+    grads = None
+    for rep in range(args.warmup + args.steps):
+        timed = rep >= args.warmup
+        if timed and sampler is None and rank == 0:
+            barrier()
+            sampler = ClockSampler(uuids)
+        # plain forward: one untimed step uploads the scene, then 64 timed steps
+        w, info = fresh()
+        w.step(DT, 4)
+        w.synchronize()
+        st = torch.cuda.ExternalStream(w.stream(), device=dev)
+        c0 = int(w.solver_counts()[12])
+        e0, e1 = events()
+        e0.record(st)
+        ph = np.zeros(5)
+        for _ in range(ROLLOUT_STEPS):
+            w.step(DT, 4)
+        e1.record(st)
+        e1.synchronize()
+        ph += w.phase_times()
+        fwd_launches = int(w.solver_counts()[12]) - c0
+        w.close()
+        # recorded forward and its adjoint (tape_begin uploads the scene and takes checkpoint 0)
+        w, info = fresh()
+        w.tape_begin(ROLLOUT_CHECKPOINT)
+        w.synchronize()
+        st = torch.cuda.ExternalStream(w.stream(), device=dev)
+        t0, t1 = events()
+        a0, a1 = events()
+        wall0 = time.perf_counter()
+        t0.record(st)
+        for _ in range(ROLLOUT_STEPS):
+            w.step(DT, 4)
+        t1.record(st)
+        pos = w.bodies()[0]
+        dpos = np.zeros_like(pos, dtype=np.float32)
+        dpos[1:] = 2.0 * (pos[1:] - info["targets"])
+        a0.record(st)
+        g = w.vjp(dpos=dpos)
+        a1.record(st)
+        a1.synchronize()
+        wall = time.perf_counter() - wall0
+        tinfo = w.tape_info()
+        if tinfo[2]:
+            raise SystemExit("bench.py: the adjoint's narrowphase replay missed %d manifolds" % tinfo[2])
+        w.close()
+        if timed:
+            plain_ms.append(e0.elapsed_time(e1))
+            taped_ms.append(t0.elapsed_time(t1))
+            vjp_ms.append(a0.elapsed_time(a1))
+            e2e_ms.append(1000.0 * wall)
+            launches.append(fwd_launches + ROLLOUT_STEPS * 0 + int(tinfo[6]))
+            phase += ph
+            grads = g
+    clocks = sampler.stop() if sampler else None
+    n = 1024
+    units = n * 4 * ROLLOUT_STEPS
+    k = len(plain_ms)
+    plain = reduce(float(np.mean(plain_ms)), "max")
+    taped = reduce(float(np.mean(taped_ms)), "max")
+    vjp = reduce(float(np.mean(vjp_ms)), "max")
+    e2e = reduce(float(np.mean(e2e_ms)), "max")
+    value = world_size * units / ((taped + vjp) / 1000.0)
+    fd = rollout_fd_check(args, local_rank, grads) if (rank == 0 and not args.no_cpu_baseline) else None
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        r = oracle_run("differentiable_rollout", {}, 1, ROLLOUT_STEPS, args.cpu_seconds)
+        cpu = {"value": r["steps"] * r["bodies"] * r["substeps"] / r["seconds"], "unit": METRIC, "cores": 1,
+               "kind": "port",
+               "sample": "CPU oracle forward rollout only (the reference has no adjoint), %d steps, 1 thread, %s"
+                         % (r["steps"], cpu_model())}
+    solve_ms = phase[3] / max(k, 1) / ROLLOUT_STEPS
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (taped + vjp) / ROLLOUT_STEPS, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene builder, no dataset)",
+            "config": {"workload": "%s: %s" % (args.workload, desc),
+                       "timed_steps": "%d rollouts of %d steps" % (args.steps, ROLLOUT_STEPS),
+                       "l2": "working set (~40 MB of world and tape) stays in L2 between rollouts; not flushed",
+                       "parallelism": "replicas: one independent world per GPU (%d)" % args.gpus},
+            "adjoint": {"forward_ms_per_step": plain / ROLLOUT_STEPS,
+                        "recorded_forward_ms_per_step": taped / ROLLOUT_STEPS,
+                        "adjoint_ms_per_step": vjp / ROLLOUT_STEPS,
+                        "adjoint_over_forward": vjp / plain,
+                        "recorded_forward_plus_adjoint_over_forward": (taped + vjp) / plain,
+                        "checkpoint_substeps": ROLLOUT_CHECKPOINT,
+                        "fd_check": fd},
+            "roofline": {"kernel": "k_solve (forward rollout)", "bound": "hbm", "achieved": None,
+                         "peak": measured_peak()[0], "unit": "GB/s", "frac": None, "traffic": None,
+                         "launch_ms": solve_ms,
+                         "note": "this workload is measured for the adjoint's cost; the solver's roofline is "
+                                 "reported on the large_pile line"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world_size * units / (e2e / 1000.0), "unit": METRIC,
+                    "h2d_bytes_per_step": 12 * (n + 1) / ROLLOUT_STEPS,
+                    "d2h_bytes_per_step": (52 + 64) * (n + 1) / ROLLOUT_STEPS,
+                    "timing": "host wall clock around the recorded rollout, the final-state readback and the "
+                              "VJP (cotangents host->device, gradients device->host)"},
+            "clocks": clocks, "gpu_launches": int(np.mean(launches)) if launches else 0,
+        }
+        print(json.dumps(line), flush=True)
 
 
 def run_one_world_at_a_time(args, local_rank, kw, sample=64, steps=100):

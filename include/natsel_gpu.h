@@ -221,9 +221,9 @@ int ns_world_tape_begin(ns_world* w, int checkpoint_substeps);
 int ns_world_tape_end(ns_world* w);
 /* Releases the tape and its checkpoints. */
 int ns_world_tape_free(ns_world* w);
-/* out[6]: recorded steps, checkpoints, narrowphase replays that did not reproduce the
+/* out[8]: recorded steps, checkpoints, narrowphase replays that did not reproduce the
  * recorded manifold (their pose derivatives are left out), VJP calls, recording (0/1),
- * checkpoint interval in substeps. */
+ * checkpoint interval in substeps, own kernel launches of the last VJP, 0. */
 int ns_world_tape_info(ns_world* w, int64_t* out);
 /* Cotangents of the world's state after the last recorded step, in body id order (rows as
  * ns_world_get_bodies: position xyz, rotation xyzw, linear and angular velocity; any may be

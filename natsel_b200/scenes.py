@@ -295,6 +295,45 @@ def restitution_ball(world, restitution=0.5, gap=0.0, speed=5.0):
     return {"name": "restitution_ball", "dynamic_bodies": 1, "ball": ball}
 
 
+def differentiable_rollout(world, count=1024, seed=5, spacing=1.25, perturb=None):
+    """1024 unit cubes (half-extent 0.5 m) on a 32 x 32 grid, resting 2 mm into a ground box,
+    with initial linear velocities N(0, 2^2) m/s and angular velocities N(0, 1) rad/s per
+    component; density 1000, friction 0.6. Returns the seeded target positions of the
+    rollout's loss sum |x_final - x_target|^2 (the initial positions plus N(0, 0.5^2) m).
+    ``perturb`` = (what, body, component, delta) moves one input ("v0", "density" or
+    "friction") for finite differences; the value applied (f32 where the API takes f32) is
+    returned as ``perturbed_value``."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = world.create_body(type=STATIC, position=(0.0, -0.5, 0.0))
+    world.create_box(g, 40.0, 0.5, 40.0, friction=0.6)
+    side = int(round(count ** 0.5))
+    pos = np.zeros((count, 3))
+    v0 = rng.normal(0.0, 2.0, (count, 3)).astype(np.float32)
+    w0 = rng.normal(0.0, 1.0, (count, 3)).astype(np.float32)
+    density = np.full(count, 1000.0)
+    friction = np.full(count, 0.6)
+    value = None
+    if perturb is not None:
+        what, body, comp, delta = perturb
+        if what == "v0":
+            v0[body, comp] = np.float32(float(v0[body, comp]) + delta)
+            value = float(v0[body, comp])
+        elif what == "density":
+            density[body] += delta
+            value = float(np.float32(density[body]))
+        else:
+            friction[body] += delta
+            value = float(np.float32(friction[body]))
+    for k in range(count):
+        i, j = divmod(k, side)
+        pos[k] = ((i - 0.5 * (side - 1)) * spacing, 0.498, (j - 0.5 * (side - 1)) * spacing)
+        b = world.create_body(type=DYNAMIC, position=tuple(pos[k]), linear_velocity=tuple(map(float, v0[k])),
+                              angular_velocity=tuple(map(float, w0[k])), enable_sleep=False)
+        world.create_box(b, 0.5, 0.5, 0.5, density=float(density[k]), friction=float(friction[k]))
+    targets = pos + rng.normal(0.0, 0.5, (count, 3))
+    return {"name": "differentiable_rollout", "dynamic_bodies": count, "targets": targets, "perturbed_value": value}
+
+
 WORLD_SETTINGS = {
     # gravity per scene: the reference scenes use the World default (-10); the synthetic
     # configurations use -9.81. Parity runs keep continuous collision off (fast bodies are
@@ -307,10 +346,11 @@ WORLD_SETTINGS = {
     "overflow_pile": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
     "batched_worlds": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "restitution_ball": dict(gravity=(0.0, 0.0, 0.0), enable_continuous=True),
+    "differentiable_rollout": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
 }
 
 SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8,
-            "overflow_pile": 4, "restitution_ball": 4, "batched_worlds": 4}
+            "overflow_pile": 4, "restitution_ball": 4, "batched_worlds": 4, "differentiable_rollout": 4}
 
 BUILDERS = {
     "large_pyramid": large_pyramid,
@@ -321,4 +361,5 @@ BUILDERS = {
     "overflow_pile": overflow_pile,
     "restitution_ball": restitution_ball,
     "batched_worlds": batched_worlds,
+    "differentiable_rollout": differentiable_rollout,
 }

@@ -331,8 +331,9 @@ class World:
         self._check(self._lib.ns_world_tape_free(self._w))
 
     def tape_info(self):
-        """steps, checkpoints, replay mismatches, vjp calls, recording, checkpoint interval."""
-        out = np.zeros(6, np.int64)
+        """steps, checkpoints, replay mismatches, vjp calls, recording, checkpoint interval,
+        kernel launches of the last vjp, 0."""
+        out = np.zeros(8, np.int64)
         self._check(self._lib.ns_world_tape_info(self._w, _ptr(out)))
         return out
 

@@ -187,6 +187,18 @@ def _both(build, steps=5, dt=DT, substeps=4):
     return g, o
 
 
+def test_rollout_scene_matches_oracle():
+    # 1024 cubes with random velocities on the ground (the adjoint's rollout scene); this body
+    # count also needs the state pass's shared-memory limit raised above the 48 KB default
+    g, _ = gpu_world("differentiable_rollout")
+    o, _ = oracle_world("differentiable_rollout")
+    for _ in range(10):
+        g.step(DT, 4)
+        o.step(DT, 4)
+        assert g.state_hash() == o.state_hash()
+    g.close()
+
+
 def test_empty_world():
     _both(lambda w: None)
 
