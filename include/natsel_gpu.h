@@ -244,7 +244,10 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
  * 8 recycled separations, 9..11 box-box manifolds: face, any axis, edge pair) at seeded random
  * inputs. worst[0] = the largest relative difference between the dual-number vector-Jacobian
  * product and central differences over all input directions; worst[1] = the separating-axis
- * kind of the box cases (-1 otherwise). */
+ * kind of the box cases (-1 otherwise). which 12..16 instead compare the hand-written reverse
+ * sweeps the GPU runs for warm start, push, relax (also their state-and-impulse-only form),
+ * integrate positions and integrate velocities (without the gyroscopic step) with the
+ * dual-number products. */
 int ns_adjoint_selfcheck(int which, int seed, double* worst);
 
 #ifdef __cplusplus

@@ -367,7 +367,7 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
                            (const void*)k_finalize, (const void*)k_state_pass,
                            (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
-                           (const void*)k_adj_narrow, (const void*)k_adj_prepare};
+                           (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
   for (const void* k : kernels) {
     cudaError_t e = cudaFuncGetAttributes(&a, k);
     if (e != cudaSuccess) return fail(w, NS_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
@@ -515,6 +515,7 @@ int upload_world(ns_world* w) {
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
   ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
+  ALLOC(long_segment, int, kLongSegmentCap);
   ALLOC(ctl, Control, 1);
   CPlanes& P = d.cp;
   P.cap = cap;
@@ -557,6 +558,8 @@ int upload_world(ns_world* w) {
   memset(&c0, 0, sizeof(c0));
   c0.moved_count = nsh;
   NS_CUDA(w, cudaMemcpyAsync(d.ctl, &c0, sizeof(Control), cudaMemcpyHostToDevice, w->stream));
+  NS_CUDA(w, cudaFuncSetAttribute(k_bp_segsort_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kLongSegmentKeys * sizeof(unsigned long long))));
   // CUB scratch (sizes depend only on the shape count)
   NS_CUDA(w, cub::DeviceRadixSort::SortPairs(nullptr, w->cub_sort_bytes, d.bp_keys_in, d.bp_keys_out,
                                               d.bp_vals_in, d.bp_vals_out, nsh));
@@ -665,7 +668,9 @@ int enqueue_pair_update(ns_world* w) {
   k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
   k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
+  NS_CUDA(w, cudaMemsetAsync(&d.ctl->long_segments, 0, sizeof(int), s));
   k_bp_segsort<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
+  k_bp_segsort_long<<<32, 1024, kLongSegmentKeys * sizeof(unsigned long long), s>>>(d); ++nk;
   k_bp_create<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;
   k_bp_pools<<<blocks(d.n_worlds, 256), 256, 0, s>>>(d); ++nk;
   k_bp_finish<<<1, 1, 0, s>>>(d); ++nk;
@@ -1282,6 +1287,72 @@ extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
       if (pc < 1) return fail(nullptr, NS_ERR_INVALID, "narrowphase replay found no manifold");
       e = vjp_fd_error(x, 3 + 7 * pc,
                        [&](const auto& in, auto* y) { narrow_box_fn(in, ca, cb, ha, hb, nc, y); }, r);
+      break;
+    }
+    case 12: case 13: case 14: {  // hand-written reverse sweeps against the dual numbers
+      random_constraint(r, x);
+      if (seed % 3 == 1) for (int q = 0; q < 4; ++q) x[cv_point(q, 6)] = r.range(0.0005, 0.01);  // speculative
+      if (seed % 4 == 2) cp.pc = 1 + seed % 3;
+      const int ny = which == 12 ? kWarmOut : which == 13 ? kPushOut : kRelaxOut;
+      std::vector<double> yb(ny), hand(kCV, 0.0), crit(kCV, 0.0);
+      for (double& v : yb) v = r.range(-1.0, 1.0);
+      if (which == 12) { warm_vjp(x.data(), cp, yb.data(), hand.data()); warm_vjp<double, false>(x.data(), cp, yb.data(), crit.data()); }
+      else if (which == 13) { push_vjp(x.data(), cp, yb.data(), hand.data()); push_vjp<double, false>(x.data(), cp, yb.data(), crit.data()); }
+      else { relax_vjp(x.data(), cp, yb.data(), hand.data()); relax_vjp<double, false>(x.data(), cp, yb.data(), crit.data()); }
+      std::vector<Dual<double, 1>> y(ny);
+      e = 0.0;
+      for (int i = 0; i < kCV; ++i) {
+        SeedIn<double, 1> in;
+        in.x = x.data();
+        in.dir[0] = i;
+        if (which == 12) warm_fn(in, cp, y.data());
+        else if (which == 13) push_fn(in, cp, y.data());
+        else relax_fn(in, cp, y.data());
+        double g = 0.0;
+        for (int j = 0; j < ny; ++j) g += yb[j] * y[j].d[0];
+        e = std::max(e, std::fabs(g - hand[i]) / std::max(1.0, std::fabs(g)));
+        // the critical-path variant keeps exactly the state and impulse entries
+        double c = i < cvIma ? g : 0.0;
+        e = std::max(e, std::fabs(c - crit[i]) / std::max(1.0, std::fabs(c)));
+      }
+      break;
+    }
+    case 15: case 16: {  // hand-written reverse of integrate positions / velocities
+      const int nx = which == 15 ? kIP : kIVIn, ny = which == 15 ? kIP : kIVOut;
+      x.assign(nx, 0.0);
+      BParams bp = {};
+      bp.h = h; bp.inv_dt = 60.0f; bp.lin_damp = 0.1f; bp.ang_damp = 0.05f; bp.grav_scale = 1.0f;
+      bp.gravity = v3(0, -9.81f, 0);
+      if (which == 15) {
+        for (int i = 0; i < 6; ++i) x[i] = r.range(-3.0, 3.0);
+        for (int i = 6; i < 9; ++i) x[i] = r.range(-0.05, 0.05);
+        random_unit(r, &x[9], 4);
+        bp.max_linear_speed = (seed & 1) ? 1.0f : 400.0f;
+        if (seed % 3 == 2) { bp.flags = kLockAngX | kLockLinZ; for (int i = 3; i < 6; ++i) x[i] *= 300.0; }
+      } else {
+        for (int i = 0; i < 6; ++i) x[i] = r.range(-2.0, 2.0);
+        x[6] = r.range(0.5, 2.0);
+        for (int i = 0; i < 9; ++i) x[7 + i] = r.range(-0.2, 0.2) + ((i % 4) == 0 ? 1.0 : 0.0);
+        for (int i = 16; i < 22; ++i) x[i] = r.range(-5.0, 5.0);
+        random_unit(r, &x[22], 4);
+        x[29] = 1.0;
+      }
+      std::vector<double> yb(ny), hand(nx, 0.0);
+      for (double& v : yb) v = r.range(-1.0, 1.0);
+      if (which == 15) ip_vjp(x.data(), bp, yb.data(), hand.data());
+      else iv_vjp_plain(x.data(), bp, yb.data(), hand.data());
+      std::vector<Dual<double, 1>> y(ny);
+      e = 0.0;
+      for (int i = 0; i < nx; ++i) {
+        if (which == 16 && i >= 16) continue;  // force, torque (not returned); rotation, inertia (gyroscopic only)
+        SeedIn<double, 1> in;
+        in.x = x.data();
+        in.dir[0] = i;
+        if (which == 15) ip_fn(in, bp, y.data()); else iv_fn(in, bp, y.data());
+        double g = 0.0;
+        for (int j = 0; j < ny; ++j) g += yb[j] * y[j].d[0];
+        e = std::max(e, std::fabs(g - hand[i]) / std::max(1.0, std::fabs(g)));
+      }
       break;
     }
     default:
@@ -1978,12 +2049,6 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
   const DW& d = w->dw;
   const int nb = (int)w->bodies.size(), n = d.n_awake, cap = d.cap;
   auto blocks = [](int count, int t) { return std::max(1, (count + t - 1) / t); };
-  static bool dirs_ready[64] = {};
-  if (w->def.device >= 0 && w->def.device < 64 && !dirs_ready[w->def.device]) {
-    StageDirs sd = make_stage_dirs();
-    NS_CUDA(w, cudaMemcpyToSymbol(c_dirs, &sd, sizeof(sd)));
-    dirs_ready[w->def.device] = true;
-  }
   // segments between checkpoints
   std::vector<std::pair<int, int>> segs;
   for (size_t c = 0; c < tp->ckpt_at.size(); ++c) {
@@ -2008,12 +2073,14 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
     size_t o_bb = take(sizeof(float) * 16 * (size_t)n), o_cq = take(sizeof(float) * 8 * (size_t)n);
     size_t o_pb = take(sizeof(float) * kPB * (size_t)n), o_kb = take(sizeof(float) * ad::kCVOwn * (size_t)cap);
     size_t o_mb = take(sizeof(float) * kMB * (size_t)cap), o_mis = take(sizeof(int));
+    size_t o_yrec = take(sizeof(float) * 3 * ad::kRelaxOut * (size_t)cap * max_sub);
     size_t o_seed = take(sizeof(float) * 13 * (size_t)nb), o_out = take(sizeof(float) * 16 * (size_t)nb);
     if (cudaMalloc(&buf, o) != cudaSuccess) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
     NS_CUDA(w, cudaMemsetAsync(buf, 0, o, w->stream));
     AdjBufs a;
     a.bb = (float*)(buf + o_bb); a.cq = (float*)(buf + o_cq); a.pb = (float*)(buf + o_pb);
     a.kb = (float*)(buf + o_kb); a.mb = (float*)(buf + o_mb); a.mismatch = (int*)(buf + o_mis);
+    a.yrec = (float*)(buf + o_yrec);
     a.cap = cap; a.n_awake = n;
     float* seed = (float*)(buf + o_seed);
     float* dev_out = (float*)(buf + o_out);
@@ -2056,11 +2123,12 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
         if (n > 0) k_adj_finalize<<<blocks(n, 128), 128, 0, w->stream>>>(t, a, n);
         if (n_slots > 0) k_adj_store<<<blocks(n_slots, 128), 128, 0, w->stream>>>(t, a, n_slots);
         if ((st = launch_adj_solve(w, t, a, p))) break;
+        if (n_slots > 0) k_adj_consts<<<blocks(n_slots, 64), 64, 0, w->stream>>>(t, a, p, n_slots);
         if (n_slots > 0) k_adj_prepare<<<blocks(n_slots, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d, p, n_slots);
         if (n > 0) k_adj_inertia<<<blocks(n, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a);
         k_adj_narrow<<<blocks(cap, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d);
         NS_CUDA(w, cudaGetLastError());
-        launches += 2 + (n > 0 ? 2 : 0) + (n_slots > 0 ? 2 : 0);  // solve, narrowphase, per-body, per-slot
+        launches += 2 + (n > 0 ? 2 : 0) + (n_slots > 0 ? 3 : 0);  // solve, narrowphase, per-body, per-slot
       }
     }
     if (st) break;

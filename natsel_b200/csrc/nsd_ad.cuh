@@ -463,6 +463,417 @@ NSD_HD void relax_fn(const In& x, const CParams& cp, T* y) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Hand-derived reverse sweeps of warm start, push and relax (one thread per constraint). Each
+// takes the stage's inputs x (constraint vector layout) and the cotangents ybar of its outputs
+// and adds the vector-Jacobian product into xbar (kCV entries, zeroed by the caller). They are
+// the reverse-mode counterparts of warm_fn, push_fn and relax_fn above, which remain the
+// reference they are checked against (ns_adjoint_selfcheck).
+
+// Where a reverse sweep adds its cotangents: all of them, or (kAll false) only the two bodies'
+// solver state and the constraint's impulses (entries below cvIma) -- what the next phase of
+// the reverse solve needs; the constant entries' terms are then dead code.
+template <class R, bool kAll>
+struct Sink {
+  R* p;
+  NSD_HD void add(int i, R v) {
+    if (kAll || i < cvIma) p[i] += v;
+  }
+};
+
+// d(S a) for a symmetric S stored as xx xy xz yy yz zz: Sbar += ybar a^T (symmetrised by
+// storage), abar += S ybar.
+template <class R, class S>
+NSD_HD void sym_mv_vjp(const TSym<R>& s, const TV3<R>& a, const TV3<R>& yb, S& xs, int at, TV3<R>& abar) {
+  xs.add(at, yb.x * a.x);
+  xs.add(at + 1, yb.x * a.y + yb.y * a.x);
+  xs.add(at + 2, yb.x * a.z + yb.z * a.x);
+  xs.add(at + 3, yb.y * a.y);
+  xs.add(at + 4, yb.y * a.z + yb.z * a.y);
+  xs.add(at + 5, yb.z * a.z);
+  abar = abar + sym_mv(s, yb);
+}
+// c = a x b: abar += b x cbar, bbar += cbar x a
+template <class R> NSD_HD void cross_vjp(const TV3<R>& a, const TV3<R>& b, const TV3<R>& cb, TV3<R>& abar, TV3<R>& bbar) {
+  abar = abar + cross(b, cb);
+  bbar = bbar + cross(cb, a);
+}
+// inv_rotate_wide(q, a) (nsd_types.cuh): out = (a - q.s t) + q.v x t, t = 2 q.v x a
+template <class R, class S>
+NSD_HD void irw_vjp(const TQ<R>& q, const TV3<R>& a, const TV3<R>& ob, S& xs, int at, TV3<R>& abar) {
+  TV3<R> t0 = cross(q.v, a);
+  TV3<R> t = tv3<R>(t0.x + t0.x, t0.y + t0.y, t0.z + t0.z);
+  abar = abar + ob;
+  xs.add(at + 3, -dot(t, ob));
+  TV3<R> tb = R(-1) * (q.s * ob);
+  TV3<R> qvb = tzero3<R>();
+  cross_vjp(q.v, t, ob, qvb, tb);
+  TV3<R> t0b = tb + tb;
+  cross_vjp(q.v, a, t0b, qvb, abar);
+  xs.add(at, qvb.x); xs.add(at + 1, qvb.y); xs.add(at + 2, qvb.z);
+}
+template <class R, class S> NSD_HD void add3(S& xs, int i, const TV3<R>& v) { xs.add(i, v.x); xs.add(i + 1, v.y); xs.add(i + 2, v.z); }
+template <class R> NSD_HD TV3<R> ld3(const R* x, int i) { return tv3<R>(x[i], x[i + 1], x[i + 2]); }
+template <class R> NSD_HD TSym<R> ldsym(const R* x, int i) {
+  TSym<R> s = {x[i], x[i + 1], x[i + 2], x[i + 3], x[i + 4], x[i + 5]};
+  return s;
+}
+
+template <class R, bool kAll = true>
+NSD_HD void warm_vjp(const R* x, const CParams& cp, const R* yb, R* xbar_) {
+  Sink<R, kAll> xbar{xbar_};
+  TV3<R> t1 = ld3(x, cvT1), t2 = ld3(x, cvT2), ca = ld3(x, cvCa), cb = ld3(x, cvCb), n = ld3(x, cvN);
+  R twist = x[cvTwist], fx = x[cvFr], fy = x[cvFr + 1], ima = x[cvIma], imb = x[cvImb];
+  TSym<R> sa = ldsym(x, cvSa), sb = ldsym(x, cvSb);
+  R tni = R(0);
+  TV3<R> moa = tzero3<R>(), mob = tzero3<R>();
+  for (int q = 0; q < cp.pc; ++q) {
+    R ni = x[cvLam + q];
+    tni = tni + ni;
+    moa = mul_add(moa, ni, ld3(x, cv_point(q, 0)));
+    mob = mul_add(mob, ni, ld3(x, cv_point(q, 3)));
+  }
+  TV3<R> fi = mul_add(fx * t1, fy, t2);
+  TV3<R> lin = mul_add(fi, tni, n);
+  TV3<R> twi = twist * n;
+  TV3<R> anga = cross(moa, n) + cross(ca, fi) + twi;
+  TV3<R> angb = cross(mob, n) + cross(cb, fi) + twi;
+  // reverse (the velocities pass through)
+  TV3<R> vab = ld3(yb, 0), wab = ld3(yb, 3), vbb = ld3(yb, 6), wbb = ld3(yb, 9);
+  add3(xbar, cvVA, vab); add3(xbar, cvWA, wab); add3(xbar, cvVB, vbb); add3(xbar, cvWB, wbb);
+  TV3<R> lib = R(-1) * (ima * vab) + imb * vbb;
+  xbar.add(cvIma, -dot(lin, vab));
+  xbar.add(cvImb, dot(lin, vbb));
+  TV3<R> aiab = tzero3<R>(), aibb = tzero3<R>();
+  sym_mv_vjp(sa, anga, R(-1) * wab, xbar, cvSa, aiab);
+  sym_mv_vjp(sb, angb, wbb, xbar, cvSb, aibb);
+  TV3<R> moab = tzero3<R>(), mobb = tzero3<R>(), nb = tzero3<R>(), cab = tzero3<R>(), cbb = tzero3<R>();
+  TV3<R> fib = lib, twib = aiab + aibb;
+  cross_vjp(moa, n, aiab, moab, nb);
+  cross_vjp(ca, fi, aiab, cab, fib);
+  cross_vjp(mob, n, aibb, mobb, nb);
+  cross_vjp(cb, fi, aibb, cbb, fib);
+  xbar.add(cvTwist, dot(n, twib));
+  nb = nb + twist * twib;
+  R tnib = dot(n, lib);
+  nb = nb + tni * lib;
+  xbar.add(cvFr, dot(t1, fib));
+  xbar.add(cvFr + 1, dot(t2, fib));
+  add3(xbar, cvT1, fx * fib);
+  add3(xbar, cvT2, fy * fib);
+  for (int q = 0; q < cp.pc; ++q) {
+    R ni = x[cvLam + q];
+    xbar.add(cvLam + q, dot(ld3(x, cv_point(q, 0)), moab) + dot(ld3(x, cv_point(q, 3)), mobb) + tnib);
+    add3(xbar, cv_point(q, 0), ni * moab);
+    add3(xbar, cv_point(q, 3), ni * mobb);
+  }
+  add3(xbar, cvN, nb); add3(xbar, cvCa, cab); add3(xbar, cvCb, cbb);
+}
+
+// Shared tail of push and relax: the reverse of the setup (the normal's rotation by the
+// substep rotations, the relative displacement).
+template <class R, class S>
+NSD_HD void contact_setup_vjp(const R* x, const TV3<R>& n, R nsb, const TV3<R>& nab, const TV3<R>& nbb, S& xbar,
+                              TV3<R>& nbar) {
+  TQ<R> dqa = tquat<R>(ld3(x, cvDqA), x[cvDqA + 3]), dqb = tquat<R>(ld3(x, cvDqB), x[cvDqB + 3]);
+  irw_vjp(dqa, n, nab, xbar, cvDqA, nbar);
+  irw_vjp(dqb, n, nbb, xbar, cvDqB, nbar);
+  TV3<R> dp = ld3(x, cvDpB) - ld3(x, cvDpA);
+  nbar = nbar + nsb * dp;
+  add3(xbar, cvDpB, nsb * n);
+  add3(xbar, cvDpA, R(-1) * (nsb * n));
+}
+
+template <class R, bool kAll = true>
+NSD_HD void push_vjp(const R* x, const CParams& cp, const R* yb, R* xbar_) {
+  Sink<R, kAll> xbar{xbar_};
+  const R inv_h = R(cp.inv_h), cs = R(-cp.contact_speed);
+  const Softness& so = cp.is_static ? cp.static_softness : cp.contact_softness;
+  const R br = R(so.mass_scale * so.bias_rate), ms = R(so.mass_scale), is = R(so.impulse_scale);
+  TV3<R> va = ld3(x, cvVA), vb = ld3(x, cvVB), n = ld3(x, cvN);
+  TQ<R> dqa = tquat<R>(ld3(x, cvDqA), x[cvDqA + 3]), dqb = tquat<R>(ld3(x, cvDqB), x[cvDqB + 3]);
+  R ima = x[cvIma], imb = x[cvImb], im = ima + imb;
+  TSym<R> sa = ldsym(x, cvSa), sb = ldsym(x, cvSb);
+  TV3<R> dp = ld3(x, cvDpB) - ld3(x, cvDpA);
+  R ns = dot(n, dp);
+  TV3<R> na = inv_rotate_wide(dqa, n), nbv = inv_rotate_wide(dqb, n);
+  // forward, keeping each point's values
+  R lnv = dot(n, vb - va), mi = R(0);
+  TV3<R> wa = ld3(x, cvWA), wb = ld3(x, cvWB);
+  TV3<R> wa_q[4], wb_q[4], ua[4], ub[4], ga[4], gb[4];
+  R imp[4], vn[4], vbias[4], pms[4], pis[4];
+  bool sepq[4], selq[4], ovlq[4];
+  for (int q = 0; q < cp.pc; ++q) {
+    TV3<R> ra = ld3(x, cv_point(q, 0)), rb = ld3(x, cv_point(q, 3));
+    R nimp = x[cvLam + q];
+    R s = (ns + (dot(nbv, rb) - dot(na, ra))) + x[cv_point(q, 6)];
+    bool sep = s > R(0);
+    R ovl = tmax(br * s, cs);
+    ovlq[q] = br * s > cs;
+    vbias[q] = sep ? s * inv_h : ovl;
+    pms[q] = sep ? R(1) : ms;
+    pis[q] = sep ? R(0) : is;
+    ua[q] = cross(ra, n); ub[q] = cross(rb, n);
+    ga[q] = sym_mv(sa, ua[q]); gb[q] = sym_mv(sb, ub[q]);
+    wa_q[q] = wa; wb_q[q] = wb;
+    vn[q] = lnv + (dot(ub[q], wb) - dot(ua[q], wa));
+    R neg = x[cv_point(q, 7)] * (pms[q] * vn[q] + vbias[q]) + pis[q] * nimp;
+    selq[q] = -neg > -nimp;
+    imp[q] = tmax(-neg, -nimp);
+    lnv = lnv + im * imp[q];
+    mi = mi + imp[q];
+    wa = wa - imp[q] * ga[q];
+    wb = wb + imp[q] * gb[q];
+    sepq[q] = sep;
+  }
+  TV3<R> Pv = mi * n;
+  // reverse
+  TV3<R> vab = ld3(yb, 0), wab = ld3(yb, 3), vbb = ld3(yb, 6), wbb = ld3(yb, 9);
+  add3(xbar, cvVA, vab); add3(xbar, cvVB, vbb);
+  TV3<R> Pvb = R(-1) * (ima * vab) + imb * vbb;
+  xbar.add(cvIma, -dot(Pv, vab));
+  xbar.add(cvImb, dot(Pv, vbb));
+  R mib = dot(n, Pvb);
+  TV3<R> nbar = mi * Pvb;
+  R lnvb = R(0), imb_ = R(0), nsb = R(0);
+  TV3<R> nab = tzero3<R>(), nbb = tzero3<R>();
+  for (int q = cp.pc - 1; q >= 0; --q) {
+    TV3<R> ra = ld3(x, cv_point(q, 0)), rb = ld3(x, cv_point(q, 3));
+    R nm = x[cv_point(q, 7)];
+    R impb = -dot(ga[q], wab) + dot(gb[q], wbb) + mib + im * lnvb;
+    TV3<R> gab = R(-1) * (imp[q] * wab), gbb = imp[q] * wbb;
+    imb_ = imb_ + imp[q] * lnvb;
+    R lamb = yb[12 + q];
+    impb = impb + lamb;
+    R nimpb = lamb;
+    R negb = R(0);
+    if (selq[q]) negb = -impb; else nimpb = nimpb - impb;
+    xbar.add(cv_point(q, 7), (pms[q] * vn[q] + vbias[q]) * negb);
+    R vnb = nm * pms[q] * negb, vbiasb = nm * negb;
+    nimpb = nimpb + pis[q] * negb;
+    R sb_ = R(0);
+    if (sepq[q]) sb_ = inv_h * vbiasb; else if (ovlq[q]) sb_ = br * vbiasb;
+    lnvb = lnvb + vnb;
+    TV3<R> uab = R(-1) * (vnb * wa_q[q]), ubb = vnb * wb_q[q];
+    wab = wab - vnb * ua[q];
+    wbb = wbb + vnb * ub[q];
+    sym_mv_vjp(sa, ua[q], gab, xbar, cvSa, uab);
+    sym_mv_vjp(sb, ub[q], gbb, xbar, cvSb, ubb);
+    TV3<R> rab = tzero3<R>(), rbb = tzero3<R>();
+    cross_vjp(ra, n, uab, rab, nbar);
+    cross_vjp(rb, n, ubb, rbb, nbar);
+    nsb = nsb + sb_;
+    nbb = nbb + sb_ * rb;
+    rbb = rbb + sb_ * nbv;
+    nab = nab - sb_ * ra;
+    rab = rab - sb_ * na;
+    xbar.add(cv_point(q, 6), sb_);
+    add3(xbar, cv_point(q, 0), rab);
+    add3(xbar, cv_point(q, 3), rbb);
+    xbar.add(cvLam + q, nimpb);
+  }
+  for (int q = cp.pc; q < 4; ++q) xbar.add(cvLam + q, yb[12 + q]);
+  add3(xbar, cvWA, wab); add3(xbar, cvWB, wbb);
+  xbar.add(cvIma, imb_); xbar.add(cvImb, imb_);
+  nbar = nbar + lnvb * (vb - va);
+  add3(xbar, cvVB, lnvb * n);
+  add3(xbar, cvVA, R(-1) * (lnvb * n));
+  contact_setup_vjp(x, n, nsb, nab, nbb, xbar, nbar);
+  add3(xbar, cvN, nbar);
+}
+
+template <class R, bool kAll = true>
+NSD_HD void relax_vjp(const R* x, const CParams& cp, const R* yb, R* xbar_) {
+  Sink<R, kAll> xbar{xbar_};
+  const R inv_h = R(cp.inv_h), eps = R(kEps);
+  TV3<R> va = ld3(x, cvVA), vb = ld3(x, cvVB), n = ld3(x, cvN), t1 = ld3(x, cvT1), t2 = ld3(x, cvT2);
+  TV3<R> ca = ld3(x, cvCa), cb = ld3(x, cvCb);
+  TQ<R> dqa = tquat<R>(ld3(x, cvDqA), x[cvDqA + 3]), dqb = tquat<R>(ld3(x, cvDqB), x[cvDqB + 3]);
+  R ima = x[cvIma], imb = x[cvImb], im = ima + imb, mu = x[cvFriction];
+  TSym<R> sa = ldsym(x, cvSa), sb = ldsym(x, cvSb);
+  TV3<R> dp = ld3(x, cvDpB) - ld3(x, cvDpA);
+  R ns = dot(n, dp);
+  TV3<R> na = inv_rotate_wide(dqa, n), nbv = inv_rotate_wide(dqb, n);
+  TV3<R> dv = vb - va;
+  R lnv = dot(n, dv);
+  R lt1 = dot(t1, dv) - x[cvTv1], lt2 = dot(t2, dv) - x[cvTv2];
+  R mi = R(0), tni = R(0), ttl = R(0);
+  TV3<R> wa = ld3(x, cvWA), wb = ld3(x, cvWB);
+  TV3<R> wa_q[4], wb_q[4], ua[4], ub[4], ga[4], gb[4];
+  R imp[4], vn[4], vbias[4], ni[4];
+  bool selq[4], actq[4];
+  for (int q = 0; q < cp.pc; ++q) {
+    TV3<R> ra = ld3(x, cv_point(q, 0)), rb = ld3(x, cv_point(q, 3));
+    R s = (ns + (dot(nbv, rb) - dot(na, ra))) + x[cv_point(q, 6)];
+    actq[q] = !(R(0) > s * inv_h);
+    vbias[q] = tmax(R(0), s * inv_h);
+    ua[q] = cross(ra, n); ub[q] = cross(rb, n);
+    ga[q] = sym_mv(sa, ua[q]); gb[q] = sym_mv(sb, ub[q]);
+    wa_q[q] = wa; wb_q[q] = wb;
+    vn[q] = lnv + (dot(ub[q], wb) - dot(ua[q], wa));
+    R neg = x[cv_point(q, 7)] * (vn[q] + vbias[q]);
+    R old = x[cvLam + q];
+    selq[q] = -neg > -old;
+    imp[q] = tmax(-neg, -old);
+    ni[q] = old + imp[q];
+    tni = tni + ni[q];
+    ttl = ttl + x[cv_point(q, 8)] * ni[q];
+    lnv = lnv + im * imp[q];
+    mi = mi + imp[q];
+    wa = wa - imp[q] * ga[q];
+    wb = wb + imp[q] * gb[q];
+  }
+  // twist
+  TV3<R> wa_p = wa, wb_p = wb;
+  R ts = dot(n, wb - wa);
+  R ml = mu * ttl, oldt = x[cvTwist], tmw = x[cvTwistMass];
+  R it0 = -(tmw * ts);
+  bool sel_in = it0 < ml - oldt;
+  R inner = sel_in ? it0 : ml - oldt;
+  bool sel_out = -ml - oldt > inner;
+  R it = sel_out ? -ml - oldt : inner;
+  TV3<R> gna = sym_mv(sa, n), gnb = sym_mv(sb, n);
+  TV3<R> wa_t = wa_p - it * gna, wb_t = wb_p + it * gnb;
+  // friction
+  R cxx = x[cvTm], cxy = x[cvTm + 1], cyx = x[cvTm + 2], cyy = x[cvTm + 3];
+  TV3<R> arv = cross(wb_t, cb) - cross(wa_t, ca);
+  R vtx = lt1 + dot(arv, t1), vty = lt2 + dot(arv, t2);
+  R d0x = cxx * vtx + cyx * vty, d0y = cxy * vtx + cyy * vty;
+  R fx = x[cvFr], fy = x[cvFr + 1];
+  R nx = fx + (-d0x), ny = fy + (-d0y);
+  R mx = mu * tni;
+  R lsq = nx * nx + ny * ny;
+  bool mask = lsq > mx * mx;
+  R root = tsqrt(lsq);
+  R den = root + eps;
+  R nrm = mx / den;
+  R sc = mask ? nrm : R(1);
+  R nxs = sc * nx, nys = sc * ny;
+  R dix = nxs - fx, diy = nys - fy;
+  TV3<R> Pv = dix * t1 + diy * t2;
+  TV3<R> Pv2 = Pv + mi * n;
+  // ---- reverse
+  TV3<R> vab = ld3(yb, 0), wab = ld3(yb, 3), vbb = ld3(yb, 6), wbb = ld3(yb, 9);
+  R frxb = yb[16], fryb = yb[17], twb = yb[18];
+  TV3<R> nbar = tzero3<R>(), t1b = tzero3<R>(), t2b = tzero3<R>(), cab = tzero3<R>(), cbb = tzero3<R>();
+  add3(xbar, cvVA, vab); add3(xbar, cvVB, vbb);
+  TV3<R> Pv2b = R(-1) * (ima * vab) + imb * vbb;
+  xbar.add(cvIma, -dot(Pv2, vab));
+  xbar.add(cvImb, dot(Pv2, vbb));
+  TV3<R> Pvb = Pv2b;
+  R mib = dot(n, Pv2b);
+  nbar = nbar + mi * Pv2b;
+  {  // wB_F = wB_T + Sb (cb x Pv), wA_F = wA_T - Sa (ca x Pv)
+    TV3<R> u = cross(cb, Pv), ubar = tzero3<R>();
+    sym_mv_vjp(sb, u, wbb, xbar, cvSb, ubar);
+    cross_vjp(cb, Pv, ubar, cbb, Pvb);
+    TV3<R> u2 = cross(ca, Pv), u2bar = tzero3<R>();
+    sym_mv_vjp(sa, u2, R(-1) * wab, xbar, cvSa, u2bar);
+    cross_vjp(ca, Pv, u2bar, cab, Pvb);
+  }
+  R dixb = dot(t1, Pvb), diyb = dot(t2, Pvb);
+  t1b = t1b + dix * Pvb;
+  t2b = t2b + diy * Pvb;
+  R nxsb = frxb + dixb, nysb = fryb + diyb;
+  R fxb = -dixb, fyb = -diyb;
+  R scb = nx * nxsb + ny * nysb;
+  R nxb = sc * nxsb, nyb = sc * nysb;
+  R mxb = R(0), tnib = R(0), ttlb = R(0);
+  if (mask) {
+    R nrmb = scb;
+    mxb = mxb + nrmb / den;
+    R denb = -nrmb * mx / (den * den);
+    R lsqb = root > R(0) ? denb * R(0.5) / root : R(0);
+    nxb = nxb + R(2) * nx * lsqb;
+    nyb = nyb + R(2) * ny * lsqb;
+  }
+  xbar.add(cvFriction, tni * mxb);
+  tnib = tnib + mu * mxb;
+  fxb = fxb + nxb; fyb = fyb + nyb;
+  R d0xb = -nxb, d0yb = -nyb;
+  xbar.add(cvTm, d0xb * vtx); xbar.add(cvTm + 2, d0xb * vty);
+  xbar.add(cvTm + 1, d0yb * vtx); xbar.add(cvTm + 3, d0yb * vty);
+  R vtxb = cxx * d0xb + cxy * d0yb, vtyb = cyx * d0xb + cyy * d0yb;
+  R lt1b = vtxb, lt2b = vtyb;
+  TV3<R> arvb = vtxb * t1 + vtyb * t2;
+  t1b = t1b + vtxb * arv;
+  t2b = t2b + vtyb * arv;
+  TV3<R> wbtb = wbb, watb = wab;
+  cross_vjp(wb_t, cb, arvb, wbtb, cbb);
+  cross_vjp(wa_t, ca, R(-1) * arvb, watb, cab);
+  // twist: wA_T = wA_P - it gna, wB_T = wB_P + it gnb
+  R itb = -dot(gna, watb) + dot(gnb, wbtb) + twb;
+  TV3<R> gnab = R(-1) * (it * watb), gnbb = it * wbtb;
+  sym_mv_vjp(sa, n, gnab, xbar, cvSa, nbar);
+  sym_mv_vjp(sb, n, gnbb, xbar, cvSb, nbar);
+  R oldtb = twb, mlb = R(0), innerb = R(0);
+  if (sel_out) { mlb = mlb - itb; oldtb = oldtb - itb; } else innerb = itb;
+  R it0b = R(0);
+  if (sel_in) it0b = innerb; else { mlb = mlb + innerb; oldtb = oldtb - innerb; }
+  xbar.add(cvTwistMass, -ts * it0b);
+  R tsb = -tmw * it0b;
+  xbar.add(cvFriction, ttl * mlb);
+  ttlb = ttlb + mu * mlb;
+  xbar.add(cvTwist, oldtb);
+  nbar = nbar + tsb * (wb_p - wa_p);
+  wbb = wbtb + tsb * n;
+  wab = watb - tsb * n;
+  // points, last to first
+  R lnvb = R(0), imb_ = R(0), nsb = R(0);
+  TV3<R> nab = tzero3<R>(), nbb = tzero3<R>();
+  for (int q = cp.pc - 1; q >= 0; --q) {
+    TV3<R> ra = ld3(x, cv_point(q, 0)), rb = ld3(x, cv_point(q, 3));
+    R nm = x[cv_point(q, 7)], lev = x[cv_point(q, 8)];
+    R impb = -dot(ga[q], wab) + dot(gb[q], wbb) + mib + im * lnvb;
+    TV3<R> gab = R(-1) * (imp[q] * wab), gbb = imp[q] * wbb;
+    imb_ = imb_ + imp[q] * lnvb;
+    xbar.add(cv_point(q, 8), ni[q] * ttlb);
+    R nib = lev * ttlb + tnib + yb[12 + q];
+    R oldb = nib;
+    impb = impb + nib;
+    R negb = R(0);
+    if (selq[q]) negb = -impb; else oldb = oldb - impb;
+    xbar.add(cv_point(q, 7), (vn[q] + vbias[q]) * negb);
+    R vnb = nm * negb, vbiasb = nm * negb;
+    R sb_ = actq[q] ? inv_h * vbiasb : R(0);
+    lnvb = lnvb + vnb;
+    TV3<R> uab = R(-1) * (vnb * wa_q[q]), ubb = vnb * wb_q[q];
+    wab = wab - vnb * ua[q];
+    wbb = wbb + vnb * ub[q];
+    sym_mv_vjp(sa, ua[q], gab, xbar, cvSa, uab);
+    sym_mv_vjp(sb, ub[q], gbb, xbar, cvSb, ubb);
+    TV3<R> rab = tzero3<R>(), rbb = tzero3<R>();
+    cross_vjp(ra, n, uab, rab, nbar);
+    cross_vjp(rb, n, ubb, rbb, nbar);
+    nsb = nsb + sb_;
+    nbb = nbb + sb_ * rb;
+    rbb = rbb + sb_ * nbv;
+    nab = nab - sb_ * ra;
+    rab = rab - sb_ * na;
+    xbar.add(cv_point(q, 6), sb_);
+    add3(xbar, cv_point(q, 0), rab);
+    add3(xbar, cv_point(q, 3), rbb);
+    xbar.add(cvLam + q, oldb);
+  }
+  for (int q = cp.pc; q < 4; ++q) xbar.add(cvLam + q, yb[12 + q]);
+  add3(xbar, cvWA, wab); add3(xbar, cvWB, wbb);
+  xbar.add(cvIma, imb_); xbar.add(cvImb, imb_);
+  xbar.add(cvFr, fxb); xbar.add(cvFr + 1, fyb);
+  // setup: lnv = n . dv, lt = t . dv - tv, dv = vB - vA
+  TV3<R> dvb = lnvb * n + lt1b * t1 + lt2b * t2;
+  nbar = nbar + lnvb * dv;
+  t1b = t1b + lt1b * dv;
+  t2b = t2b + lt2b * dv;
+  xbar.add(cvTv1, -lt1b);
+  xbar.add(cvTv2, -lt2b);
+  add3(xbar, cvVB, dvb);
+  add3(xbar, cvVA, R(-1) * dvb);
+  contact_setup_vjp(x, n, nsb, nab, nbb, xbar, nbar);
+  add3(xbar, cvN, nbar);
+  add3(xbar, cvT1, t1b); add3(xbar, cvT2, t2b);
+  add3(xbar, cvCa, cab); add3(xbar, cvCb, cbb);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Prepare (nsd_kernels.cuh prepare_constraint; contact_solver.rs:445): manifold and body mass
 // data -> the constraint's own entries of the constraint vector (outputs cvLam..kCV-1).
 enum PI : int {
@@ -659,6 +1070,81 @@ NSD_HD void inv_inertia_fn(const In& x, T* y) {
   TM3<T> il = tm3<T>(in3<T>(x, 4), in3<T>(x, 7), in3<T>(x, 10));
   TM3<T> m = mul_mm(mul_mm(R, il), transpose(R));
   out3(y, 0, m.cx); out3(y, 3, m.cy); out3(y, 6, m.cz);
+}
+
+// Hand-derived reverse of integrate positions (ip_fn): x, ybar and xbar in its 13-entry layout.
+template <class R>
+NSD_HD void ip_vjp(const R* x, const BParams& bp, const R* yb, R* xbar_) {
+  Sink<R, true> xbar{xbar_};
+  uint32_t flags = bp.flags;
+  const R h = R(bp.h), maxl = R(bp.max_linear_speed), maxa = R(kMaxRotation * bp.inv_dt);
+  TV3<R> v = ld3(x, 0), wv = ld3(x, 3);
+  v.x = (flags & kLockLinX) ? R(0) : v.x;
+  v.y = (flags & kLockLinY) ? R(0) : v.y;
+  v.z = (flags & kLockLinZ) ? R(0) : v.z;
+  wv.x = (flags & kLockAngX) ? R(0) : wv.x;
+  wv.y = (flags & kLockAngY) ? R(0) : wv.y;
+  wv.z = (flags & kLockAngZ) ? R(0) : wv.z;
+  bool capv = dot(v, v) > maxl * maxl;
+  R lv = length(v);
+  bool capw = dot(wv, wv) > maxa * maxa && (flags & kAllowFastRotation) == 0;
+  R lw = length(wv);
+  TV3<R> wc = capw ? (maxa / lw) * wv : wv;
+  TQ<R> q1 = tquat<R>(ld3(x, 9), x[12]);
+  TV3<R> pv = R(0.5) * (h * wc);
+  TQ<R> qd = mul_quat(tquat<R>(pv, R(0)), q1);
+  TQ<R> qs = tquat<R>(q1.v + qd.v, qd.s + q1.s);
+  // dq' = normalize(qs)
+  TQ<R> qsb = tquat<R>(tzero3<R>(), R(0));
+  R ls = dot_quat(qs, qs);
+  TQ<R> qob = tquat<R>(ld3(yb, 9), yb[12]);
+  if (ls > R(1000.0f * kMinPositive)) {
+    R inv = R(1) / tsqrt(ls);
+    TQ<R> qh = tquat<R>(inv * qs.v, inv * qs.s);
+    R d = dot_quat(qh, qob);
+    qsb = tquat<R>(inv * (qob.v - d * qh.v), inv * (qob.s - d * qh.s));
+  }
+  // qd = p (x) q1 with p = (pv, 0): v = pv x q1.v + q1.s pv, s = -pv . q1.v
+  TV3<R> pvb = cross(q1.v, qsb.v) + q1.s * qsb.v - qsb.s * q1.v;
+  TV3<R> q1vb = qsb.v + cross(qsb.v, pv) - qsb.s * pv;
+  R q1sb = qsb.s + dot(pv, qsb.v);
+  TV3<R> wcb = ld3(yb, 3) + (R(0.5) * h) * pvb;
+  TV3<R> vcb = ld3(yb, 0) + h * ld3(yb, 6);
+  add3(xbar, 6, ld3(yb, 6));
+  xbar.add(9, q1vb.x); xbar.add(10, q1vb.y); xbar.add(11, q1vb.z); xbar.add(12, q1sb);
+  if (capv) {
+    TV3<R> vh = (R(1) / lv) * v;
+    vcb = (maxl / lv) * (vcb - dot(vh, vcb) * vh);
+  }
+  if (capw) {
+    TV3<R> wh = (R(1) / lw) * wv;
+    wcb = (maxa / lw) * (wcb - dot(wh, wcb) * wh);
+  }
+  xbar.add(0, (flags & kLockLinX) ? R(0) : vcb.x);
+  xbar.add(1, (flags & kLockLinY) ? R(0) : vcb.y);
+  xbar.add(2, (flags & kLockLinZ) ? R(0) : vcb.z);
+  xbar.add(3, (flags & kLockAngX) ? R(0) : wcb.x);
+  xbar.add(4, (flags & kLockAngY) ? R(0) : wcb.y);
+  xbar.add(5, (flags & kLockAngZ) ? R(0) : wcb.z);
+}
+// Hand-derived reverse of integrate velocities without the gyroscopic step (iv_fn):
+// v' = (h m^-1 F + h gs g) + ld v, w' = h (I^-1 tau) + ad w.
+template <class R>
+NSD_HD void iv_vjp_plain(const R* x, const BParams& bp, const R* yb, R* xbar_) {
+  Sink<R, true> xbar{xbar_};
+  const R h = R(bp.h);
+  R ld = R(1) / (R(1) + h * R(bp.lin_damp));
+  R ad = R(1) / (R(1) + h * R(bp.ang_damp));
+  TV3<R> vb = ld3(yb, 0), wb = ld3(yb, 3);
+  add3(xbar, 0, ld * vb);
+  add3(xbar, 3, ad * wb);
+  xbar.add(6, h * dot(ld3(x, 16), vb));
+  for (int c = 0; c < 3; ++c) {
+    R tau = x[19 + c];
+    xbar.add(7 + 3 * c, h * wb.x * tau);
+    xbar.add(7 + 3 * c + 1, h * wb.y * tau);
+    xbar.add(7 + 3 * c + 2, h * wb.z * tau);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------

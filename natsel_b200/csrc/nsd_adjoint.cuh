@@ -6,12 +6,15 @@
 // after integrate-positions) and the inputs of every push and relax update. The reverse pass
 // then walks the step backwards: finalize, impulse store, the substeps (relax colours 22..0,
 // integrate positions, push colours 22..0, warm start colours 22..0, integrate velocities),
-// prepare, the inverse world inertia and the narrowphase. Each local function's
-// vector-Jacobian product is formed by one warp: lane l seeds input directions l, l + 32, ...
-// of the dual-number restatement (nsd_ad.cuh), evaluates it once and contracts the output
-// tangents with the incoming cotangents. Colours keep the forward's independence: inside a
-// colour no two constraints share a dynamic body, so their body cotangents are written
-// without atomics.
+// prepare, the inverse world inertia and the narrowphase. The solver stages run one thread per
+// constraint or body through hand-derived reverse sweeps (nsd_ad.cuh); the barrier-separated
+// sweep carries only the bodies' and impulses' cotangents, and the constant planes'
+// cotangents of every update are added afterwards by one parallel pass (k_adj_consts).
+// Prepare, the inertia and the narrowphase form their vector-Jacobian products with one warp
+// each: lane l seeds input directions l, l + 32, ... of the dual-number restatement, evaluates
+// it once and contracts the output tangents with the incoming cotangents. Colours keep the
+// forward's independence: inside a colour no two constraints share a dynamic body, so their
+// body cotangents are written without atomics.
 //
 // Scope of the adjoint: one world of box bodies (hull shapes) without joints, restitution,
 // rolling resistance, continuous collision or overflow constraints; the host rejects other
@@ -51,6 +54,7 @@ struct AdjBufs {
   float* pb;   // [n_awake][kPB]: parameters
   float* kb;   // [kCVOwn][cap]: constraint entries cvLam.. of each slot
   float* mb;   // [kMB][cap]: manifold state of each contact id
+  float* yrec; // [substep][stage][kRelaxOut][cap]: output cotangents each contact update received
   int* mismatch;  // narrowphase replays that did not reproduce the forward manifold
   int cap, n_awake;
 };
@@ -62,50 +66,6 @@ __device__ __forceinline__ float& CQ(const AdjBufs& a, int i, int f) { return a.
 __device__ __forceinline__ float& PB(const AdjBufs& a, int i, int f) { return a.pb[(size_t)i * kPB + f]; }
 __device__ __forceinline__ float& KB(const AdjBufs& a, int k, int cv) { return a.kb[(size_t)(cv - ad::cvLam) * a.cap + k]; }
 __device__ __forceinline__ float& MB(const AdjBufs& a, int c, int f) { return a.mb[(size_t)f * a.cap + c]; }
-
-// One warp: x̄[dir] = sum_j ȳ_j dy_j/dx_dir for the directions of this lane.
-template <int K, int NY, class Fn>
-__device__ __forceinline__ void warp_vjp(const float* xs, const float* ys, const int16_t* dirs, int ndirs, Fn fn,
-                                         float* xbar, int* dir) {
-  int lane = threadIdx.x & 31;
-  ad::SeedIn<float, K> in;
-  in.x = xs;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    int d = lane + 32 * k;
-    in.dir[k] = d < ndirs ? dirs[d] : -1;
-  }
-  ad::Dual<float, K> y[NY];
-  fn(in, y);
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    float acc = 0.0f;
-#pragma unroll
-    for (int j = 0; j < NY; ++j) acc += ys[j] * y[j].d[k];
-    xbar[k] = acc;
-    dir[k] = in.dir[k];
-  }
-}
-
-// Direction lists (constraint vector indices) of the three contact stages.
-struct StageDirs { int16_t warm[64], push[96], relax[128]; int n_warm, n_push, n_relax; };
-__constant__ StageDirs c_dirs;
-
-inline StageDirs make_stage_dirs() {
-  using namespace ad;
-  StageDirs s = {};
-  auto add = [](int16_t* l, int& n, int a, int b) { for (int i = a; i < b; ++i) l[n++] = (int16_t)i; };
-  // warm start is affine in the velocities (identity Jacobian): only its constants and impulses
-  add(s.warm, s.n_warm, cvLam, cvT2 + 3);
-  add(s.warm, s.n_warm, cvCa, cvCb + 3);
-  for (int q = 0; q < 4; ++q) add(s.warm, s.n_warm, cv_point(q, 0), cv_point(q, 6));
-  add(s.push, s.n_push, 0, cvLam + 4);
-  add(s.push, s.n_push, cvIma, cvN + 3);
-  for (int q = 0; q < 4; ++q) add(s.push, s.n_push, cv_point(q, 0), cv_point(q, 8));
-  add(s.relax, s.n_relax, 0, cvTv1);
-  add(s.relax, s.n_relax, cvCa, kCV);
-  return s;
-}
 
 // ---------------------------------------------------------------------------------------------
 // Finalize (k_finalize): centre' = centre + dp, q' = normalize(dq q).
@@ -157,245 +117,242 @@ __global__ void k_adj_store(StepTape t, AdjBufs a, int n_slots) {
   KB(a, k, cvT2) = fin.y * F.x; KB(a, k, cvT2 + 1) = fin.y * F.y; KB(a, k, cvT2 + 2) = fin.y * F.z;
 }
 
-// The constraint vector of slot k in stage `stage` of substep `sub` (values of the forward),
-// gathered by the lanes of one warp into xs.
-__device__ void gather_cv(const StepTape& t, int n, int cap, int k, int sub, int stage, float* xs) {
+// The constraint vector of slot k in stage `stage` of substep `sub`: the values the forward
+// update read (body velocities and impulses from the solver tape, dp and dq from the body rows,
+// the constants from the prepared planes).
+__device__ void gather_cv(const StepTape& t, int n, int cap, int k, int sub, int stage, float* x) {
   using namespace ad;
   const CPlanes& P = t.planes;
-  int lane = threadIdx.x & 31;
   int4 idx = P.idx[k];
   int ia = idx.x, ib = idx.y;
-  auto put4 = [&](int at, float4 v, int cnt) {
-    xs[at] = v.x; if (cnt > 1) xs[at + 1] = v.y; if (cnt > 2) xs[at + 2] = v.z; if (cnt > 3) xs[at + 3] = v.w;
+  auto put = [&](int at, float4 v, int cnt) {
+    x[at] = v.x; if (cnt > 1) x[at + 1] = v.y; if (cnt > 2) x[at + 2] = v.z; if (cnt > 3) x[at + 3] = v.w;
   };
-  const float4* rows = stage == kPush ? t.push + (size_t)sub * 4 * cap : t.relax + (size_t)sub * 5 * cap;
-  if (stage == kWarm) rows = t.push + (size_t)sub * 4 * cap;
-  int row_sel = stage == kRelax ? 2 : 0;  // dp, dq seen by the stage
-  switch (lane) {
-    case 0: case 1: case 2: case 3: {
-      float4 r = rows[(size_t)lane * cap + k];
-      if (stage == kWarm) { r.x = 0.0f; r.y = 0.0f; r.z = 0.0f; }  // unused by warm start
-      put4(3 * lane, r, 3);
-      xs[cvLam + lane] = r.w;
-      break;
+  const float4* rows = stage == kRelax ? t.relax + (size_t)sub * 5 * cap : t.push + (size_t)sub * 4 * cap;
+  for (int r = 0; r < 4; ++r) {
+    float4 v = rows[(size_t)r * cap + k];
+    if (stage == kWarm) { v.x = 0.0f; v.y = 0.0f; v.z = 0.0f; }  // warm start is affine in them
+    put(3 * r, v, 3);
+    x[cvLam + r] = v.w;
+  }
+  {
+    float4 v = t.relax[((size_t)sub * 5 + 4) * cap + k];
+    x[cvFr] = v.x; x[cvFr + 1] = v.y; x[cvTwist] = v.z;
+  }
+  int row_sel = stage == kRelax ? 2 : 0;  // the dp, dq the stage sees
+  for (int s = 0; s < 2; ++s) {
+    int b = s == 0 ? ia : ib;
+    float4 dp = make_float4(0, 0, 0, 0), dq = make_float4(0, 0, 0, 1);
+    if (b >= 0) {
+      const DState& st = t.body[((size_t)sub * 3 + row_sel) * n + b];
+      dp = make_float4(st.dp.x, st.dp.y, st.dp.z, 0.0f);
+      dq = make_float4(st.dq.v.x, st.dq.v.y, st.dq.v.z, st.dq.s);
     }
-    case 4: {
-      float4 r = t.relax[((size_t)sub * 5 + 4) * cap + k];
-      xs[cvFr] = r.x; xs[cvFr + 1] = r.y; xs[cvTwist] = r.z;
-      break;
-    }
-    case 5: case 6: {
-      int b = lane == 5 ? ia : ib;
-      float4 dp = make_float4(0, 0, 0, 0), dq = make_float4(0, 0, 0, 1);
-      if (b >= 0) {
-        const DState& st = t.body[((size_t)sub * 3 + row_sel) * n + b];
-        dp = make_float4(st.dp.x, st.dp.y, st.dp.z, 0.0f);
-        dq = make_float4(st.dq.v.x, st.dq.v.y, st.dq.v.z, st.dq.s);
-      }
-      put4(lane == 5 ? cvDpA : cvDpB, dp, 3);
-      put4(lane == 5 ? cvDqA : cvDqB, dq, 4);
-      break;
-    }
-    case 7: { float4 m = P.mass[k]; xs[cvIma] = m.x; xs[cvImb] = m.y; xs[cvFriction] = m.z; break; }
-    case 8: put4(cvSa, P.ia0[k], 4); break;
-    case 9: { float4 v = P.ia1[k]; xs[cvSa + 4] = v.x; xs[cvSa + 5] = v.y; xs[cvSb] = v.z; xs[cvSb + 1] = v.w; break; }
-    case 10: put4(cvSb + 2, P.ib1[k], 4); break;
-    case 11: put4(cvN, P.n[k], 3); break;
-    case 12: { float4 v = P.t1[k]; put4(cvT1, v, 3); xs[cvTv1] = v.w; break; }  // t1 | tangent velocity 1
-    case 13: { float4 v = P.t2[k]; put4(cvT2, v, 3); xs[cvTv2] = v.w; break; }
-    case 14: { float4 v = P.ca[k]; put4(cvCa, v, 3); xs[cvTwistMass] = v.w; break; }
-    case 15: put4(cvCb, P.cb[k], 3); break;
-    case 16: put4(cvTm, P.tm[k], 4); break;
-    default: {
-      int g = lane - 17;  // 0..11: pra, prb, pimp of the four points
-      if (g < 12) {
-        int q = g % 4, kind = g / 4;
-        float4 v = kind == 0 ? P.pra[(size_t)q * cap + k] : kind == 1 ? P.prb[(size_t)q * cap + k] : P.pimp[(size_t)q * cap + k];
-        if (kind == 0) { put4(cv_point(q, 0), v, 3); xs[cv_point(q, 6)] = v.w; }
-        else if (kind == 1) { put4(cv_point(q, 3), v, 3); xs[cv_point(q, 7)] = v.w; }
-        else xs[cv_point(q, 8)] = v.z;
-      }
-      break;
-    }
+    put(s == 0 ? cvDpA : cvDpB, dp, 3);
+    put(s == 0 ? cvDqA : cvDqB, dq, 4);
+  }
+  float4 m = P.mass[k];
+  x[cvIma] = m.x; x[cvImb] = m.y; x[cvFriction] = m.z;
+  put(cvSa, P.ia0[k], 4);
+  float4 v1 = P.ia1[k];
+  x[cvSa + 4] = v1.x; x[cvSa + 5] = v1.y; x[cvSb] = v1.z; x[cvSb + 1] = v1.w;
+  put(cvSb + 2, P.ib1[k], 4);
+  put(cvN, P.n[k], 3);
+  float4 t1 = P.t1[k], t2 = P.t2[k], ca = P.ca[k];
+  put(cvT1, t1, 3); x[cvTv1] = t1.w;
+  put(cvT2, t2, 3); x[cvTv2] = t2.w;
+  put(cvCa, ca, 3); x[cvTwistMass] = ca.w;
+  put(cvCb, P.cb[k], 3);
+  put(cvTm, P.tm[k], 4);
+  for (int q = 0; q < 4; ++q) {
+    float4 ra = P.pra[(size_t)q * cap + k], rb = P.prb[(size_t)q * cap + k], im = P.pimp[(size_t)q * cap + k];
+    put(cv_point(q, 0), ra, 3); x[cv_point(q, 6)] = ra.w;
+    put(cv_point(q, 3), rb, 3); x[cv_point(q, 7)] = rb.w;
+    x[cv_point(q, 8)] = im.z;
   }
 }
 
-// Reverse of one contact stage for slot k, by one warp.
-template <int Stage>
-__device__ void adj_contact(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int k, int sub, float* xs,
-                            float* ys) {
-  using namespace ad;
-  int lane = threadIdx.x & 31;
-  int4 idx = t.planes.idx[k];
-  int ia = idx.x, ib = idx.y;
-  CParams cp;
+__device__ __forceinline__ ad::CParams contact_params(int4 idx, const StepParams& p) {
+  ad::CParams cp;
   cp.pc = idx.w & 255;
   cp.is_static = (idx.w & 256) != 0;
   cp.inv_h = p.inv_h;
   cp.contact_speed = p.contact_speed;
   cp.contact_softness = p.contact_softness;
   cp.static_softness = p.static_softness;
-  gather_cv(t, n, a.cap, k, sub, Stage, xs);
-  // incoming cotangents of the outputs
+  return cp;
+}
+
+// Reverse of one contact stage for slot k (one thread), on the reverse solve's critical path:
+// the hand-derived reverse sweep of the stage (nsd_ad.cuh) restricted to the two bodies' state
+// and the impulses, written back (velocities replace the outputs' for push and relax, dp and
+// dq accumulate, impulses replace where the stage updates them and accumulate where it only
+// reads them). The output cotangents are recorded for k_adj_consts, which adds the constant
+// entries' cotangents of every update afterwards, off the critical path.
+template <int Stage>
+__device__ void adj_contact(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int k, int sub) {
+  using namespace ad;
+  int4 idx = t.planes.idx[k];
+  int ia = idx.x, ib = idx.y;
+  CParams cp = contact_params(idx, p);
+  float x[kCV], xb[cvIma], yb[kRelaxOut];
+  gather_cv(t, n, a.cap, k, sub, Stage, x);
+  for (int f = 0; f < 12; ++f) {
+    int b = f < 6 ? ia : ib;
+    int g = f % 6;
+    yb[f] = b >= 0 ? BB(a, b, g < 3 ? g : g + 1) : 0.0f;
+  }
+  for (int q = 0; q < 4; ++q) yb[12 + q] = KB(a, k, cvLam + q);
+  yb[16] = KB(a, k, cvFr); yb[17] = KB(a, k, cvFr + 1); yb[18] = KB(a, k, cvTwist);
+  for (int i = 0; i < cvIma; ++i) xb[i] = 0.0f;
+  if (Stage == kWarm) warm_vjp<float, false>(x, cp, yb, xb);
+  else if (Stage == kPush) push_vjp<float, false>(x, cp, yb, xb);
+  else relax_vjp<float, false>(x, cp, yb, xb);
   constexpr int NY = Stage == kWarm ? kWarmOut : Stage == kPush ? kPushOut : kRelaxOut;
-  if (lane < 12) {
-    int b = lane < 6 ? ia : ib;
-    int f = lane % 6;
-    ys[lane] = b >= 0 ? BB(a, b, f < 3 ? f : f + 1) : 0.0f;
-  } else if (lane < NY) {
-    int j = lane - 12;  // impulses, then friction and twist (relax)
-    int cv = j < 4 ? cvLam + j : (j == 4 ? cvFr : j == 5 ? cvFr + 1 : cvTwist);
-    ys[lane] = KB(a, k, cv);
-  }
-  __syncwarp();
-  float xb[4];
-  int dir[4];
-  if (Stage == kWarm) {
-    warp_vjp<2, kWarmOut>(xs, ys, c_dirs.warm, c_dirs.n_warm,
-                          [&](const SeedIn<float, 2>& in, Dual<float, 2>* y) { warm_fn(in, cp, y); }, xb, dir);
-  } else if (Stage == kPush) {
-    warp_vjp<3, kPushOut>(xs, ys, c_dirs.push, c_dirs.n_push,
-                          [&](const SeedIn<float, 3>& in, Dual<float, 3>* y) { push_fn(in, cp, y); }, xb, dir);
-  } else {
-    warp_vjp<4, kRelaxOut>(xs, ys, c_dirs.relax, c_dirs.n_relax,
-                           [&](const SeedIn<float, 4>& in, Dual<float, 4>* y) { relax_fn(in, cp, y); }, xb, dir);
-  }
-  __syncwarp();
-  constexpr int KD = Stage == kWarm ? 2 : Stage == kPush ? 3 : 4;
-#pragma unroll
-  for (int kk = 0; kk < KD; ++kk) {
-    int d = dir[kk];
-    if (d < 0) continue;
-    float v = xb[kk];
-    if (d < cvDpA) {  // velocities: the input's cotangent replaces the output's
-      int b = d < 6 ? ia : ib;
-      int f = d % 6;
-      if (b >= 0) BB(a, b, f < 3 ? f : f + 1) = v;
-    } else if (d < cvLam) {  // dp, dq: inputs only
-      int b = (d < cvDpB || (d >= cvDqA && d < cvDqB)) ? ia : ib;
-      int f = d < cvDqA ? 8 + (d - cvDpA) % 3 : 12 + (d - cvDqA) % 4;
-      if (b >= 0) BB(a, b, f) += v;
-    } else if (d < cvIma) {  // impulses: replaced when the stage updates them
-      bool updated = Stage == kRelax || (Stage == kPush && d < cvFr);
-      if (updated) KB(a, k, d) = v; else KB(a, k, d) += v;
-    } else {
-      KB(a, k, d) += v;
+  float* rec = a.yrec + ((size_t)(sub * 3 + Stage) * kRelaxOut) * a.cap + k;
+  for (int j = 0; j < NY; ++j) rec[(size_t)j * a.cap] = yb[j];
+  if (Stage != kWarm) {
+    for (int f = 0; f < 12; ++f) {
+      int b = f < 6 ? ia : ib;
+      int g = f % 6;
+      if (b >= 0) BB(a, b, g < 3 ? g : g + 1) = xb[f];
+    }
+    for (int f = 0; f < 3; ++f) {
+      if (ia >= 0) BB(a, ia, 8 + f) += xb[cvDpA + f];
+      if (ib >= 0) BB(a, ib, 8 + f) += xb[cvDpB + f];
+    }
+    for (int f = 0; f < 4; ++f) {
+      if (ia >= 0) BB(a, ia, 12 + f) += xb[cvDqA + f];
+      if (ib >= 0) BB(a, ib, 12 + f) += xb[cvDqB + f];
     }
   }
+  for (int cv = cvLam; cv < cvIma; ++cv) {
+    bool updated = Stage == kRelax || (Stage == kPush && cv < cvFr);
+    if (updated) KB(a, k, cv) = xb[cv];
+    else if (Stage == kWarm) KB(a, k, cv) += xb[cv];
+  }
 }
 
-// Reverse of integrate positions for body i (one warp, lanes 0..12).
-__device__ void adj_ip(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub, float* xs,
-                       float* ys) {
+// The constant entries' cotangents of every contact update of the step (all substeps and
+// stages of slot k, one thread), from the inputs on the tape and the recorded output
+// cotangents; summed into the slot's constraint cotangents.
+__global__ void k_adj_consts(StepTape t, AdjBufs a, StepParams p, int n_slots) {
   using namespace ad;
-  int lane = threadIdx.x & 31;
-  const DState& st = t.body[((size_t)sub * 3 + 1) * n + i];
-  if (lane == 0) {
-    xs[0] = st.v.x; xs[1] = st.v.y; xs[2] = st.v.z; xs[3] = st.w.x; xs[4] = st.w.y; xs[5] = st.w.z;
-    xs[6] = st.dp.x; xs[7] = st.dp.y; xs[8] = st.dp.z;
-    xs[9] = st.dq.v.x; xs[10] = st.dq.v.y; xs[11] = st.dq.v.z; xs[12] = st.dq.s;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_slots) return;
+  CParams cp = contact_params(t.planes.idx[k], p);
+  float sum[kCV - cvIma];
+  for (int i = 0; i < kCV - cvIma; ++i) sum[i] = 0.0f;
+  float x[kCV], xb[kCV], yb[kRelaxOut];
+  for (int sub = 0; sub < t.substeps; ++sub) {
+    for (int stage = kWarm; stage <= kRelax; ++stage) {
+      gather_cv(t, a.n_awake, a.cap, k, sub, stage, x);
+      const float* rec = a.yrec + ((size_t)(sub * 3 + stage) * kRelaxOut) * a.cap + k;
+      int ny = stage == kWarm ? kWarmOut : stage == kPush ? kPushOut : kRelaxOut;
+      for (int j = 0; j < kRelaxOut; ++j) yb[j] = j < ny ? rec[(size_t)j * a.cap] : 0.0f;
+      for (int i = 0; i < kCV; ++i) xb[i] = 0.0f;
+      if (stage == kWarm) warm_vjp(x, cp, yb, xb);
+      else if (stage == kPush) push_vjp(x, cp, yb, xb);
+      else relax_vjp(x, cp, yb, xb);
+      for (int i = 0; i < kCV - cvIma; ++i) sum[i] += xb[cvIma + i];
+    }
   }
-  const int map[13] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14, 15};
-  if (lane < kIP) ys[lane] = BB(a, i, map[lane]);
-  __syncwarp();
+  for (int i = 0; i < kCV - cvIma; ++i) KB(a, k, cvIma + i) += sum[i];
+}
+
+// Reverse of integrate positions for body i (one thread).
+__device__ void adj_ip(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub) {
+  using namespace ad;
+  const DState& st = t.body[((size_t)sub * 3 + 1) * n + i];
+  float x[kIP] = {st.v.x, st.v.y, st.v.z, st.w.x, st.w.y, st.w.z, st.dp.x, st.dp.y, st.dp.z,
+                  st.dq.v.x, st.dq.v.y, st.dq.v.z, st.dq.s};
+  const int map[kIP] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14, 15};
+  float yb[kIP], xb[kIP];
+  for (int f = 0; f < kIP; ++f) { yb[f] = BB(a, i, map[f]); xb[f] = 0.0f; }
   BParams bp = {};
   bp.h = p.h; bp.inv_dt = p.inv_dt; bp.max_linear_speed = p.max_linear_speed; bp.flags = st.flags;
-  SeedIn<float, 1> in;
-  in.x = xs;
-  in.dir[0] = lane < kIP ? lane : -1;
-  Dual<float, 1> y[kIP];
-  ip_fn(in, bp, y);
-  float acc = 0.0f;
-  for (int j = 0; j < kIP; ++j) acc += ys[j] * y[j].d[0];
-  __syncwarp();
-  if (lane < kIP) BB(a, i, map[lane]) = acc;
+  ip_vjp(x, bp, yb, xb);
+  for (int f = 0; f < kIP; ++f) BB(a, i, map[f]) = xb[f];
 }
 
-// Reverse of integrate velocities for body i (one warp, two directions per lane).
-__device__ void adj_iv(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub, float* xs,
-                       float* ys) {
+// Reverse of integrate velocities for body i (one thread): the hand-derived sweep, or for a
+// gyroscopic body the dual-number product one input direction at a time.
+__device__ void adj_iv(const StepTape& t, const AdjBufs& a, const StepParams& p, int n, int i, int sub) {
   using namespace ad;
-  int lane = threadIdx.x & 31;
   const DState& st = t.body[((size_t)sub * 3 + 0) * n + i];
   const DSim& s = t.sims[i];
-  if (lane == 0) {
-    xs[0] = st.v.x; xs[1] = st.v.y; xs[2] = st.v.z; xs[3] = st.w.x; xs[4] = st.w.y; xs[5] = st.w.z;
-    xs[6] = s.inv_mass;
-    const float* m = &s.inv_inertia_world.cx.x;
-    for (int f = 0; f < 9; ++f) xs[7 + f] = m[f];
-    xs[16] = s.force.x; xs[17] = s.force.y; xs[18] = s.force.z;
-    xs[19] = s.torque.x; xs[20] = s.torque.y; xs[21] = s.torque.z;
-    xs[22] = s.q.v.x; xs[23] = s.q.v.y; xs[24] = s.q.v.z; xs[25] = s.q.s;
-    xs[26] = st.dq.v.x; xs[27] = st.dq.v.y; xs[28] = st.dq.v.z; xs[29] = st.dq.s;
-    const float* in = &s.inertia.cx.x;
-    for (int f = 0; f < 9; ++f) xs[30 + f] = in[f];
-  }
+  float x[kIVIn];
+  x[0] = st.v.x; x[1] = st.v.y; x[2] = st.v.z; x[3] = st.w.x; x[4] = st.w.y; x[5] = st.w.z;
+  x[6] = s.inv_mass;
+  const float* m = &s.inv_inertia_world.cx.x;
+  for (int f = 0; f < 9; ++f) x[7 + f] = m[f];
+  x[16] = s.force.x; x[17] = s.force.y; x[18] = s.force.z;
+  x[19] = s.torque.x; x[20] = s.torque.y; x[21] = s.torque.z;
+  x[22] = s.q.v.x; x[23] = s.q.v.y; x[24] = s.q.v.z; x[25] = s.q.s;
+  x[26] = st.dq.v.x; x[27] = st.dq.v.y; x[28] = st.dq.v.z; x[29] = st.dq.s;
+  const float* in = &s.inertia.cx.x;
+  for (int f = 0; f < 9; ++f) x[30 + f] = in[f];
   const int map[6] = {0, 1, 2, 4, 5, 6};
-  if (lane < kIVOut) ys[lane] = BB(a, i, map[lane]);
-  __syncwarp();
+  float yb[kIVOut], xb[kIVIn];
+  for (int f = 0; f < kIVOut; ++f) yb[f] = BB(a, i, map[f]);
+  for (int f = 0; f < kIVIn; ++f) xb[f] = 0.0f;
   BParams bp = {};
   bp.h = p.h; bp.lin_damp = s.linear_damping; bp.ang_damp = s.angular_damping; bp.grav_scale = s.gravity_scale;
   bp.gravity = p.gravity;
   bp.flags = s.flags;
-  SeedIn<float, 2> in;
-  in.x = xs;
-  in.dir[0] = lane;
-  in.dir[1] = lane + 32 < kIVIn ? lane + 32 : -1;
-  Dual<float, 2> y[kIVOut];
-  iv_fn(in, bp, y);
-  float acc[2];
-  for (int kk = 0; kk < 2; ++kk) {
-    acc[kk] = 0.0f;
-    for (int j = 0; j < kIVOut; ++j) acc[kk] += ys[j] * y[j].d[kk];
+  if (s.flags & kGyroscopic) {
+    for (int d = 0; d < kIVIn; ++d) {
+      if (d >= 16 && d < 22) continue;  // applied force and torque: not returned
+      SeedIn<float, 1> sin;
+      sin.x = x;
+      sin.dir[0] = d;
+      Dual<float, 1> y[kIVOut];
+      iv_fn(sin, bp, y);
+      float acc = 0.0f;
+      for (int j = 0; j < kIVOut; ++j) acc += yb[j] * y[j].d[0];
+      xb[d] = acc;
+    }
+  } else {
+    iv_vjp_plain(x, bp, yb, xb);
   }
-  __syncwarp();
-  for (int kk = 0; kk < 2; ++kk) {
-    int d = in.dir[kk];
-    float v = acc[kk];
-    if (d < 0) continue;
-    if (d < 6) BB(a, i, map[d]) = v;                       // velocities: replaced
-    else if (d == 6) PB(a, i, pbInvMass) += v;
-    else if (d < 16) PB(a, i, pbIiw + d - 7) += v;
-    else if (d < 22) continue;                             // applied force and torque
-    else if (d < 26) CQ(a, i, 4 + d - 22) += v;            // rotation at the step start
-    else if (d < 30) BB(a, i, 12 + d - 26) += v;           // substep rotation dq
-    else PB(a, i, pbInertia + d - 30) += v;                // local inertia
+  for (int f = 0; f < 6; ++f) BB(a, i, map[f]) = xb[f];
+  PB(a, i, pbInvMass) += xb[6];
+  for (int f = 0; f < 9; ++f) PB(a, i, pbIiw + f) += xb[7 + f];
+  if (s.flags & kGyroscopic) {
+    for (int f = 0; f < 4; ++f) CQ(a, i, 4 + f) += xb[22 + f];      // rotation at the step start
+    for (int f = 0; f < 4; ++f) BB(a, i, 12 + f) += xb[26 + f];     // substep rotation dq
+    for (int f = 0; f < 9; ++f) PB(a, i, pbInertia + f) += xb[30 + f];
   }
 }
 
 // Reverse of the solver stages of one step: a persistent launch over the same barriers as the
-// forward solver, phases in reverse order.
+// forward solver, phases in reverse order, one thread per constraint or body.
 template <bool kGrid>
 __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBufs a, StepParams p, Control* ctl) {
   __shared__ int coff[25];
-  __shared__ float xs_s[kAdjThreads / 32][ad::kCV + 2];
-  __shared__ float ys_s[kAdjThreads / 32][32];
   if (threadIdx.x < 24) coff[threadIdx.x] = t.ctl->color_offset[threadIdx.x];
   if (threadIdx.x == 24) coff[24] = t.ctl->color_offset[23];
   __syncthreads();
   const int n = a.n_awake;
-  const int warp = threadIdx.x >> 5;
-  const int gw = blockIdx.x * (kAdjThreads / 32) + warp;
-  const int nw = gridDim.x * (kAdjThreads / 32);
-  float* xs = xs_s[warp];
-  float* ys = ys_s[warp];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
   int bar = 0;
   auto contacts = [&](auto stage_tag, int sub) -> bool {
     constexpr int Stage = decltype(stage_tag)::value;
     for (int c = kOverflowIndex - 1; c >= 0; --c) {
       if (coff[c + 1] == coff[c]) continue;
-      for (int k = coff[c] + gw; k < coff[c + 1]; k += nw) adj_contact<Stage>(t, a, p, n, k, sub, xs, ys);
+      for (int k = coff[c] + g; k < coff[c + 1]; k += stride) adj_contact<Stage>(t, a, p, n, k, sub);
       if (!phase_sync<kGrid>(ctl, bar)) return false;
     }
     return true;
   };
   for (int sub = t.substeps - 1; sub >= 0; --sub) {
     if (!contacts(std::integral_constant<int, kRelax>(), sub)) return;
-    for (int i = gw; i < n; i += nw) adj_ip(t, a, p, n, i, sub, xs, ys);
+    for (int i = g; i < n; i += stride) adj_ip(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
     if (!contacts(std::integral_constant<int, kPush>(), sub)) return;
     if (!contacts(std::integral_constant<int, kWarm>(), sub)) return;
-    for (int i = gw; i < n; i += nw) adj_iv(t, a, p, n, i, sub, xs, ys);
+    for (int i = g; i < n; i += stride) adj_iv(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
   }
 }

@@ -61,6 +61,7 @@ struct DW {
   // Optional record of each contact's narrowphase outcome (0 none or disjoint, 1 recycled,
   // 2 new manifold, 3 no points), written only while the adjoint replays a step.
   uint8_t* np_mode;
+  int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
 };
 
 struct JointRanges { int off[25]; };
@@ -304,17 +305,64 @@ __global__ void k_bp_scatter(DW w) {
   }
 }
 
-__global__ void k_bp_segsort(DW w) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= w.n_shapes) return;
-  int n = w.seg_count[s];
-  if (n < 2) return;
-  unsigned long long* a = w.sorted_keys + w.seg_off[s];
+// Each shape's candidate segment is sorted by its pair keys. Short segments (most of them) are
+// sorted by one thread; longer ones (a large shape meeting many new partners at once, such as
+// a ground box on the first step) are listed for k_bp_segsort_long, which sorts each with one
+// block in shared memory.
+constexpr int kShortSegment = 32, kLongSegmentCap = 256, kLongSegmentKeys = 8192;
+
+__device__ void insertion_sort_keys(unsigned long long* a, int n) {
   for (int i = 1; i < n; ++i) {
     unsigned long long v = a[i];
     int j = i - 1;
     while (j >= 0 && a[j] > v) { a[j + 1] = a[j]; --j; }
     a[j + 1] = v;
+  }
+}
+
+__global__ void k_bp_segsort(DW w) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= w.n_shapes) return;
+  int n = w.seg_count[s];
+  if (n < 2) return;
+  if (n > kShortSegment && n <= kLongSegmentKeys) {
+    int slot = atomicAdd(&w.ctl->long_segments, 1);
+    if (slot < kLongSegmentCap) {
+      w.long_segment[slot] = s;
+      return;
+    }
+  }
+  insertion_sort_keys(w.sorted_keys + w.seg_off[s], n);
+}
+
+// Bitonic sort of one long segment per block (keys padded to a power of two with the largest
+// key; equal keys are equal values, so the result is the segment's sorted order).
+__global__ void __launch_bounds__(1024) k_bp_segsort_long(DW w) {
+  extern __shared__ unsigned long long keys[];
+  int count = min(w.ctl->long_segments, kLongSegmentCap);
+  for (int li = blockIdx.x; li < count; li += gridDim.x) {
+    int s = w.long_segment[li];
+    int n = w.seg_count[s];
+    unsigned long long* a = w.sorted_keys + w.seg_off[s];
+    int p2 = 1;
+    while (p2 < n) p2 <<= 1;
+    for (int i = threadIdx.x; i < p2; i += blockDim.x) keys[i] = i < n ? a[i] : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= p2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+          int ixj = i ^ j;
+          if (ixj > i) {
+            unsigned long long x = keys[i], y = keys[ixj];
+            bool up = (i & k) == 0;
+            if ((x > y) == up) { keys[i] = y; keys[ixj] = x; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = keys[i];
+    __syncthreads();
   }
 }
 

@@ -244,6 +244,7 @@ struct Control {
   int color_offset[25];
   int live_contacts;
   int collide_count[6];   // contacts per pair kind queued for a full manifold update
+  int long_segments;      // candidate segments handed to the block sort this pair update
 };
 
 }  // namespace nsd

@@ -361,7 +361,9 @@ class World:
 
 
 ADJOINT_CHECKS = ["warm_start", "push", "relax", "prepare", "integrate_velocities", "integrate_positions",
-                  "finalize_rotation", "inverse_inertia", "recycle", "box_face", "box_any", "box_edge"]
+                  "finalize_rotation", "inverse_inertia", "recycle", "box_face", "box_any", "box_edge",
+                  "warm_start_reverse_sweep", "push_reverse_sweep", "relax_reverse_sweep",
+                  "integrate_positions_reverse_sweep", "integrate_velocities_reverse_sweep"]
 
 
 def adjoint_selfcheck(which, seed):

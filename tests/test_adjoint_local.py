@@ -1,10 +1,12 @@
 """The adjoint's local derivatives, checked in f64 on the host (no GPU).
 
-Every reverse stage of ns_world_vjp contracts the tangents of a dual-number restatement of one
-forward function (warm start, push, relax, prepare, the body stages, recycled separations and
-box-box manifolds). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random
-inputs and compares the dual-number vector-Jacobian product, direction by direction, with
-central differences of the same function.
+The reverse stages of ns_world_vjp rest on a dual-number restatement of each forward function
+(warm start, push, relax, prepare, the body stages, recycled separations and box-box
+manifolds). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random inputs and
+compares its vector-Jacobian product, direction by direction, with central differences of the
+same function; and it compares the hand-derived reverse sweeps the solver stages run on the
+GPU (warm start, push, relax, integrate positions and velocities) with the dual-number
+products, which they must reproduce to rounding.
 """
 import pytest
 
@@ -20,7 +22,7 @@ def test_local_vjp_matches_central_differences(which):
         assert 0.0 <= worst < 1e-6, (ADJOINT_CHECKS[which], seed, worst)
 
 
-@pytest.mark.parametrize("which", [9, 10, 11], ids=ADJOINT_CHECKS[9:])
+@pytest.mark.parametrize("which", [9, 10, 11], ids=ADJOINT_CHECKS[9:12])
 def test_box_manifold_vjp_matches_central_differences(which):
     kinds = set()
     for seed in range(16):
@@ -31,3 +33,10 @@ def test_box_manifold_vjp_matches_central_differences(which):
         assert K_FACE_A in kinds
     if which == 11:
         assert K_EDGE in kinds, kinds  # the edge-pair manifold is exercised
+
+
+@pytest.mark.parametrize("which", range(12, 17), ids=ADJOINT_CHECKS[12:17])
+def test_reverse_sweeps_match_dual_numbers(which):
+    for seed in range(16):
+        worst, _ = adjoint_selfcheck(which, seed)
+        assert 0.0 <= worst < 1e-12, (ADJOINT_CHECKS[which], seed, worst)
