@@ -57,7 +57,7 @@ WORKLOADS = {
                                "w.r.t. initial velocities, masses and frictions by the adjoint (ns_world_vjp) "
                                "with checkpoints every 8 substeps; FP32"),
 }
-ROLLOUT_STEPS, ROLLOUT_CHECKPOINT = 64, 8
+ROLLOUT_CHECKPOINT = 8
 
 
 def parse_args(argv=None):
@@ -71,6 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--reference-seconds", type=float, default=60.0, help="budget of the reference arm's timed sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rollout-steps", type=int, default=64,
+                    help="steps of each differentiable rollout (64 in the workload; fewer for profiling)")
     return ap.parse_args(argv)
 
 
@@ -460,7 +462,7 @@ def rollout_fd_check(args, local_rank, g, n_entries=12, seed=11):
     def loss(what, body, comp, delta):
         w = World(default_world_def(gravity=s["gravity"], enable_continuous=0, device=local_rank))
         info = scenes.differentiable_rollout(w, perturb=(what, body, comp, delta))
-        for _ in range(ROLLOUT_STEPS):
+        for _ in range(args.rollout_steps):
             w.step(DT, 4)
         pos = w.bodies()[0][1:]
         w.close()
@@ -534,7 +536,7 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
         e0, e1 = events()
         e0.record(st)
         ph = np.zeros(5)
-        for _ in range(ROLLOUT_STEPS):
+        for _ in range(args.rollout_steps):
             w.step(DT, 4)
         e1.record(st)
         e1.synchronize()
@@ -550,7 +552,7 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
         a0, a1 = events()
         wall0 = time.perf_counter()
         t0.record(st)
-        for _ in range(ROLLOUT_STEPS):
+        for _ in range(args.rollout_steps):
             w.step(DT, 4)
         t1.record(st)
         pos = w.bodies()[0]
@@ -570,12 +572,12 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
             taped_ms.append(t0.elapsed_time(t1))
             vjp_ms.append(a0.elapsed_time(a1))
             e2e_ms.append(1000.0 * wall)
-            launches.append(fwd_launches + ROLLOUT_STEPS * 0 + int(tinfo[6]))
+            launches.append(fwd_launches + int(tinfo[6]))
             phase += ph
             grads = g
     clocks = sampler.stop() if sampler else None
     n = 1024
-    units = n * 4 * ROLLOUT_STEPS
+    units = n * 4 * args.rollout_steps
     k = len(plain_ms)
     plain = reduce(float(np.mean(plain_ms)), "max")
     taped = reduce(float(np.mean(taped_ms)), "max")
@@ -585,25 +587,25 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
     fd = rollout_fd_check(args, local_rank, grads) if (rank == 0 and not args.no_cpu_baseline) else None
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        r = oracle_run("differentiable_rollout", {}, 1, ROLLOUT_STEPS, args.cpu_seconds)
+        r = oracle_run("differentiable_rollout", {}, 1, args.rollout_steps, args.cpu_seconds)
         cpu = {"value": r["steps"] * r["bodies"] * r["substeps"] / r["seconds"], "unit": METRIC, "cores": 1,
                "kind": "port",
                "sample": "CPU oracle forward rollout only (the reference has no adjoint), %d steps, 1 thread, %s"
                          % (r["steps"], cpu_model())}
-    solve_ms = phase[3] / max(k, 1) / ROLLOUT_STEPS
+    solve_ms = phase[3] / max(k, 1) / args.rollout_steps
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": (taped + vjp) / ROLLOUT_STEPS, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": (taped + vjp) / args.rollout_steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded scene builder, no dataset)",
             "config": {"workload": "%s: %s" % (args.workload, desc),
-                       "timed_steps": "%d rollouts of %d steps" % (args.steps, ROLLOUT_STEPS),
+                       "timed_steps": "%d rollouts of %d steps" % (args.steps, args.rollout_steps),
                        "l2": "working set (~40 MB of world and tape) stays in L2 between rollouts; not flushed",
                        "parallelism": "replicas: one independent world per GPU (%d)" % args.gpus},
-            "adjoint": {"forward_ms_per_step": plain / ROLLOUT_STEPS,
-                        "recorded_forward_ms_per_step": taped / ROLLOUT_STEPS,
-                        "adjoint_ms_per_step": vjp / ROLLOUT_STEPS,
+            "adjoint": {"forward_ms_per_step": plain / args.rollout_steps,
+                        "recorded_forward_ms_per_step": taped / args.rollout_steps,
+                        "adjoint_ms_per_step": vjp / args.rollout_steps,
                         "adjoint_over_forward": vjp / plain,
                         "recorded_forward_plus_adjoint_over_forward": (taped + vjp) / plain,
                         "checkpoint_substeps": ROLLOUT_CHECKPOINT,
@@ -615,8 +617,8 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
                                  "reported on the large_pile line"},
             "cpu_baseline": cpu,
             "e2e": {"value": world_size * units / (e2e / 1000.0), "unit": METRIC,
-                    "h2d_bytes_per_step": 12 * (n + 1) / ROLLOUT_STEPS,
-                    "d2h_bytes_per_step": (52 + 64) * (n + 1) / ROLLOUT_STEPS,
+                    "h2d_bytes_per_step": 12 * (n + 1) / args.rollout_steps,
+                    "d2h_bytes_per_step": (52 + 64) * (n + 1) / args.rollout_steps,
                     "timing": "host wall clock around the recorded rollout, the final-state readback and the "
                               "VJP (cotangents host->device, gradients device->host)"},
             "clocks": clocks, "gpu_launches": int(np.mean(launches)) if launches else 0,
