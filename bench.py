@@ -20,8 +20,10 @@ the per-step solver counts divided by its CUDA-event duration. ``cpu_baseline`` 
 oracle (a scalar C++ restatement of the reference step) on a bounded sample of the same drop.
 
 reference arm (``--impl reference``): the reference engine is Rust and cannot be built on
-this image, so its CPU step is timed through the oracle port, one replica world per host
-core, on a bounded sample of the same workload; under torchrun only rank 0 runs it.
+this image, so its CPU step is timed through the oracle port on a bounded sample of the same
+workload: one world colour-parallel on every host core, as the reference parallelises a world
+(``--reference-mode replicas``: one replica world per core instead; batched worlds always run
+one world per core); under torchrun only rank 0 runs it.
 """
 import argparse
 import json
@@ -70,6 +72,9 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--reference-seconds", type=float, default=60.0, help="budget of the reference arm's timed sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-mode", choices=["colour-parallel", "replicas"], default="colour-parallel",
+                    help="reference arm for a single world: the oracle colour-parallel on every host core "
+                         "(as the reference runs one world), or one replica world per core")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rollout-steps", type=int, default=64,
                     help="steps of each differentiable rollout (64 in the workload; fewer for profiling)")
@@ -249,6 +254,8 @@ def run_reference_arm(args):
     pyoracle.build()
     scene, kw, desc = WORKLOADS[args.workload]
     n = min(host_cores(), 128)
+    if scene != "batched_worlds" and args.reference_mode == "colour-parallel":
+        return run_reference_colour_parallel(args, scene, kw, desc, n)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(n)
     queue = ctx.Queue()
@@ -283,6 +290,30 @@ def run_reference_arm(args):
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": n, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "timed_steps_per_replica": steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_colour_parallel(args, scene, kw, desc, n):
+    """One world, as the reference steps it: the oracle's colour-parallel loops (collide per
+    contact, prepare and every solver stage per constraint of a colour, the body stages per body;
+    the pair update, the ordered state pass and the overflow colour stay serial) on every host
+    core, timing steps W+1..W+K of the workload within the time budget."""
+    from oracle import pyoracle
+    pyoracle.set_threads(n)
+    r = oracle_run(scene, kw, args.warmup, args.steps, args.reference_seconds)
+    pyoracle.set_threads(1)
+    value = r["steps"] * r["bodies"] * r["substeps"] / r["seconds"]
+    sample = ("one world, colour-parallel on %d host threads (%s), steps %d..%d (bounded to %.0f s)" % (
+        n, cpu_model(), args.warmup + 1, args.warmup + r["steps"], args.reference_seconds))
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * r["seconds"] / r["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene builder, no dataset)",
+        "config": config_block(args, desc), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": n, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timed_steps": r["steps"],
     }
     print(json.dumps(line), flush=True)
 

@@ -58,6 +58,8 @@ int nso_create_revolute(nso_world* w, int body_a, int body_b, const float frame_
                         int enable_spring, float hertz, float damping_ratio, float drag_torque,
                         int collide_connected);
 void nso_step(nso_world* w, float dt, int substeps);
+/* Host threads of the colour-parallel loops (all worlds of the process; default 1). */
+void nso_set_threads(int threads);
 /* Per-body force / torque (n_bodies x 3, id order, either may be NULL) for the next step. */
 void nso_apply_forces(nso_world* w, const float* force, const float* torque);
 uint64_t nso_state_hash(const nso_world* w);

@@ -3,6 +3,9 @@
 // (sleep disabled; CCD only flags fast bodies). Used as the parity checker;
 // the product never links it. Each block cites the reference function it
 // follows; operand order matches the reference so results are bit-identical.
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -242,6 +245,20 @@ bool get_bit(nso_world* w, int c, int b) {
   if (blk >= v.size()) return false;
   return (v[blk] >> (b & 63)) & 1ull;
 }
+// Host threads for the colour-parallel loops (collide per contact, prepare and the solver stages
+// per constraint of a colour, the body stages per body). The reference runs its stages the same
+// way (solver_stages.rs:227-231, collide_pass.rs:209); every such loop touches disjoint data, so
+// any thread count gives the same bits. One thread unless nso_set_threads raises it.
+int g_threads = 1;
+constexpr int kParMin = 64;
+int thread_index() {
+#ifdef _OPENMP
+  return omp_get_thread_num();
+#else
+  return 0;
+#endif
+}
+
 void set_bit(nso_world* w, int c, int b) {
   std::vector<uint64_t>& v = w->color_bits[c];
   size_t blk = (size_t)b >> 6;
@@ -576,7 +593,7 @@ void update_pairs(nso_world* w) {
     return a < b;
   });
   std::vector<uint64_t> keys;
-  auto consider = [&](int a, int b) {
+  auto consider = [&](int a, int b, std::vector<uint64_t>& out) {
     const Shape& A = w->shapes[a];
     const Shape& B = w->shapes[b];
     if (A.is_static && B.is_static) return;
@@ -586,20 +603,29 @@ void update_pairs(nso_world* w) {
     uint64_t k = pair_key(lo, hi);
     if (w->pair_set.count(k)) return;
     if (!should_create_pair(w, lo, hi)) return;
-    keys.push_back(k);
+    out.push_back(k);
   };
-  // small vs small: each pair once (i < j in sweep order)
-  for (size_t i = 0; i < small.size(); ++i) {
-    int a = small[i];
-    float hx = w->fat[a].hi.x;
-    for (size_t j = i + 1; j < small.size(); ++j) {
-      int b = small[j];
-      if (w->fat[b].lo.x > hx) break;
-      consider(a, b);
+  // small vs small: each pair once (i < j in sweep order); the search only reads the world, so
+  // threads collect into their own lists and the keys are sorted below
+  const int ns_ = (int)small.size();
+  std::vector<std::vector<uint64_t>> found(g_threads);
+#pragma omp parallel num_threads(g_threads) if (g_threads > 1 && ns_ >= 1024)
+  {
+    std::vector<uint64_t>& mine = found[thread_index()];
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < ns_; ++i) {
+      int a = small[i];
+      float hx = w->fat[a].hi.x;
+      for (int j = i + 1; j < ns_; ++j) {
+        int b = small[j];
+        if (w->fat[b].lo.x > hx) break;
+        consider(a, b, mine);
+      }
     }
   }
+  for (const std::vector<uint64_t>& f : found) keys.insert(keys.end(), f.begin(), f.end());
   for (int L : large)
-    for (int s : small) consider(L, s);
+    for (int s : small) consider(L, s, keys);
   std::sort(keys.begin(), keys.end());
   keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
   for (int i = 0; i < n; ++i) w->proxy_moved[i] = 0;
@@ -809,6 +835,7 @@ void collide_one(nso_world* w, int cid, std::vector<uint8_t>& bits) {
             m.points[i].persisted = true;
           }
         }
+#pragma omp atomic
         w->recycled++;
         return;
       }
@@ -831,8 +858,10 @@ void collide_one(nso_world* w, int cid, std::vector<uint8_t>& bits) {
 void collide(nso_world* w) {
   w->recycled = 0;
   std::vector<uint8_t> bits(w->contacts.size(), 0);
-  for (size_t i = 0; i < w->contacts.size(); ++i)
-    if (w->contacts[i].contact_id != -1) collide_one(w, (int)i, bits);
+  const int n_ = (int)w->contacts.size();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int i = 0; i < n_; ++i)
+    if (w->contacts[i].contact_id != -1) collide_one(w, i, bits);
   for (size_t i = 0; i < bits.size(); ++i) {
     if (!bits[i]) continue;
     Contact& c = w->contacts[i];
@@ -1055,18 +1084,23 @@ void prepare_all(nso_world* w) {
   prepare_overflow(w, soft, stat);
   float ws = w->def.enable_warm_starting ? 1.0f : 0.0f;
   for (int ci = 0; ci < kOverflowIndex; ++ci) {
-    w->constraints[ci].clear();
-    for (int cid : w->colors[ci].convex) {
-      w->constraints[ci].push_back(prepare_contact(w, cid, soft, stat, ws));
+    const std::vector<int>& ids = w->colors[ci].convex;
+    std::vector<ContactConstraint>& out = w->constraints[ci];
+    out.resize(ids.size());
+    const int n_ = (int)ids.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+    for (int k = 0; k < n_; ++k) out[k] = prepare_contact(w, ids[k], soft, stat, ws);
+    for (int cid : ids)
       if (w->contacts[cid].restitution > 0.0f) w->any_restitution = true;
-    }
   }
 }
 
 // solver_integration.rs:263 integrate_velocities_range
 void integrate_velocities(nso_world* w, float h) {
   V3 g = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
-  for (size_t i = 0; i < w->awake_sims.size(); ++i) {
+  const int n_ = (int)w->awake_sims.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int i = 0; i < n_; ++i) {
     const BodySim& sim = w->awake_sims[i];
     BodyState& st = w->awake_states[i];
     V3 v = st.v, wv = st.w;
@@ -1113,7 +1147,10 @@ void integrate_positions(nso_world* w, float h, float inv_dt) {
   float maxl = w->def.max_linear_speed;
   float maxa = kMaxRotation * inv_dt;
   float maxl2 = maxl * maxl, maxa2 = maxa * maxa;
-  for (BodyState& st : w->awake_states) {
+  const int n_ = (int)w->awake_states.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int i_ = 0; i_ < n_; ++i_) {
+    BodyState& st = w->awake_states[i_];
     V3 v = st.v, wv = st.w;
     v.x = (st.flags & kLockLinX) ? 0.0f : v.x;
     v.y = (st.flags & kLockLinY) ? 0.0f : v.y;
@@ -1140,7 +1177,11 @@ void integrate_positions(nso_world* w, float h, float inv_dt) {
 
 // contact_solver.rs:697 warm_start_contacts_body
 void warm_start_color(nso_world* w, int ci) {
-  for (const ContactConstraint& c : w->constraints[ci]) {
+  auto& list_ = w->constraints[ci];
+  const int n_ = (int)list_.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int k_ = 0; k_ < n_; ++k_) {
+    const ContactConstraint& c = list_[k_];
     const ManifoldConstraint& cm = c.m;
     V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
     float tni = 0.0f;
@@ -1179,7 +1220,11 @@ void push_color(nso_world* w, int ci) {
   float dms = ctx.contact_softness.mass_scale, dis = ctx.contact_softness.impulse_scale;
   float sbr = ctx.static_softness.mass_scale * ctx.static_softness.bias_rate;
   float sms = ctx.static_softness.mass_scale, sis = ctx.static_softness.impulse_scale;
-  for (ContactConstraint& c : w->constraints[ci]) {
+  auto& list_ = w->constraints[ci];
+  const int n_ = (int)list_.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int k_ = 0; k_ < n_; ++k_) {
+    ContactConstraint& c = list_[k_];
     BodyState ba = state_at(w, c.index_a), bb = state_at(w, c.index_b);
     float br = c.is_static ? sbr : dbr, ms = c.is_static ? sms : dms, is = c.is_static ? sis : dis;
     V3 dp = bb.dp - ba.dp;
@@ -1222,7 +1267,11 @@ void push_color(nso_world* w, int ci) {
 void relax_color(nso_world* w, int ci) {
   float inv_h = w->ctx.inv_h;
   float eps = kEps;
-  for (ContactConstraint& c : w->constraints[ci]) {
+  auto& list_ = w->constraints[ci];
+  const int n_ = (int)list_.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int k_ = 0; k_ < n_; ++k_) {
+    ContactConstraint& c = list_[k_];
     BodyState ba = state_at(w, c.index_a), bb = state_at(w, c.index_b);
     bool any_rolling = c.rolling_resistance > 0.0f;
     V3 dp = bb.dp - ba.dp;
@@ -1314,7 +1363,11 @@ void relax_color(nso_world* w, int ci) {
 void restitution_color(nso_world* w, int ci) {
   float inv_h = w->ctx.inv_h;
   float nrt = -w->def.restitution_threshold;
-  for (ContactConstraint& c : w->constraints[ci]) {
+  auto& list_ = w->constraints[ci];
+  const int n_ = (int)list_.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int k_ = 0; k_ < n_; ++k_) {
+    ContactConstraint& c = list_[k_];
     if (c.restitution == 0.0f) continue;
     BodyState ba = state_at(w, c.index_a), bb = state_at(w, c.index_b);
     bool rmask = c.restitution > 0.0f;
@@ -1356,7 +1409,11 @@ void restitution_color(nso_world* w, int ci) {
 
 // contact_solver.rs:1258 store_impulses_body
 void store_color(nso_world* w, int ci) {
-  for (const ContactConstraint& c : w->constraints[ci]) {
+  auto& list_ = w->constraints[ci];
+  const int n_ = (int)list_.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int k_ = 0; k_ < n_; ++k_) {
+    const ContactConstraint& c = list_[k_];
     Contact& ct = w->contacts[c.contact_id];
     if (ct.manifold_count <= 0) continue;
     const ManifoldConstraint& cm = c.m;
@@ -1643,7 +1700,9 @@ void solve_stages(nso_world* w) {
 void finalize(nso_world* w) {
   float dt = w->ctx.dt, inv_dt = w->ctx.inv_dt;
   float spec = speculative_distance();
-  for (size_t i = 0; i < w->awake_sims.size(); ++i) {
+  const int n_ = (int)w->awake_sims.size();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
+  for (int i = 0; i < n_; ++i) {
     BodyState& st = w->awake_states[i];
     BodySim& sim = w->awake_sims[i];
     V3 v = st.v, wv = st.w;
@@ -1670,6 +1729,7 @@ void finalize(nso_world* w) {
     (void)inv_dt;
     if (body.type == 2 && w->def.enable_continuous && max_motion > body.safety_factor * sim.min_extent) {
       sim.flags |= kIsFast;
+#pragma omp atomic
       w->fast_flags_seen++;
     } else {
       sim.center0 = sim.center;
@@ -1720,6 +1780,8 @@ nso_world* nso_create(const nso_world_def* def) {
 }
 
 void nso_destroy(nso_world* w) { delete w; }
+
+void nso_set_threads(int threads) { g_threads = threads < 1 ? 1 : threads; }
 
 // world_runtime.rs:1506 create_body (awake or static set only)
 int nso_create_body(nso_world* w, const nso_body_def* d) {

@@ -89,6 +89,7 @@ def load():
     lib.nso_create.argtypes = [ctypes.POINTER(WorldDef)]
     lib.nso_create.restype = P
     lib.nso_destroy.argtypes = [P]
+    lib.nso_set_threads.argtypes = [ctypes.c_int]
     lib.nso_create_body.argtypes = [P, ctypes.POINTER(BodyDef)]
     lib.nso_create_box.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef)] + [ctypes.c_float] * 3
     lib.nso_create_sphere.argtypes = [P, ctypes.c_int, ctypes.POINTER(ShapeDef), _F3, ctypes.c_float]
@@ -108,6 +109,12 @@ def load():
     lib.nso_apply_forces.argtypes = [P, P, P]
     _lib = lib
     return lib
+
+
+def set_threads(threads):
+    """Host threads of the oracle's colour-parallel loops (every world in the process; default 1).
+    Any count gives the same bits: each parallel loop touches disjoint data."""
+    load().nso_set_threads(int(threads))
 
 
 def _ptr(a):

@@ -36,6 +36,28 @@ def test_reference_golden_hash(name):
     assert _hashes(name, {}, case["steps"])[-1] == case["hash"]
 
 
+@pytest.mark.parametrize("name", ["large_pyramid", "many_pyramids"])
+def test_colour_parallel_oracle_reproduces_golden_hash(name):
+    """The oracle's colour-parallel loops (the reference arm's CPU path) give the same bits on
+    four threads: every parallel loop touches disjoint data."""
+    case = json.load(open(os.path.join(GOLDEN, "reference_hashes.json")))["cases"][name]
+    pyoracle.set_threads(4)
+    try:
+        assert _hashes(name, {}, case["steps"])[-1] == case["hash"]
+    finally:
+        pyoracle.set_threads(1)
+
+
+def test_colour_parallel_oracle_matches_one_thread():
+    kw = {"n": 2000, "seed": 7}
+    one = _hashes("large_pile", kw, 30)
+    pyoracle.set_threads(4)
+    try:
+        assert _hashes("large_pile", kw, 30) == one
+    finally:
+        pyoracle.set_threads(1)
+
+
 def _fixture_cases():
     cases = json.load(open(os.path.join(GOLDEN, "oracle_hashes.json")))["cases"]
     return [pytest.param(c, id="%s-%s" % (c["scene"], "-".join("%s%s" % kv for kv in c["kw"].items()) or "default"))
