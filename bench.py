@@ -550,6 +550,7 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
         return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     plain_ms, taped_ms, vjp_ms, e2e_ms, launches = [], [], [], [], []
+    f64_check = None
     phase = np.zeros(5)
     sampler = None
     grads = None
@@ -597,6 +598,15 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
         tinfo = w.tape_info()
         if tinfo[2]:
             raise SystemExit("bench.py: the adjoint's narrowphase replay missed %d manifolds" % tinfo[2])
+        if timed and rep == args.warmup + args.steps - 1 and rank == 0 and not args.no_cpu_baseline:
+            h0 = time.perf_counter()
+            g64 = w.vjp_f64(dpos=dpos)
+            f64_check = {"host_seconds": time.perf_counter() - h0}
+            for key in ("lin0", "ang0", "mass", "friction"):
+                a_, b_ = np.asarray(g[key], np.float64).ravel(), np.asarray(g64[key]).ravel()
+                rel = np.abs(a_ - b_) / np.maximum(np.abs(b_), 1e-3 * np.abs(b_).max() + 1e-300)
+                f64_check[key] = {"median_rel": float(np.median(rel)), "p99_rel": float(np.quantile(rel, 0.99)),
+                                  "max_rel": float(rel.max()), "frac_within_1e-3": float(np.mean(rel < 1e-3))}
         w.close()
         if timed:
             plain_ms.append(e0.elapsed_time(e1))
@@ -640,6 +650,7 @@ def run_rollout_arm(args, rank, local_rank, world_size, dev, barrier, reduce, uu
                         "adjoint_over_forward": vjp / plain,
                         "recorded_forward_plus_adjoint_over_forward": (taped + vjp) / plain,
                         "checkpoint_substeps": ROLLOUT_CHECKPOINT,
+                        "f64_host_adjoint_check": f64_check,
                         "fd_check": fd},
             "roofline": {"kernel": "k_solve (forward rollout)", "bound": "hbm", "achieved": None,
                          "peak": measured_peak()[0], "unit": "GB/s", "frac": None, "traffic": None,

@@ -237,6 +237,12 @@ int ns_world_tape_info(ns_world* w, int64_t* out);
  * cones are held). Synchronous. */
 int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
                  float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0);
+/* The same vector-Jacobian product with the reverse pass run on the host in f64 (the replay of
+ * the recorded steps still runs on the GPU, bit-identical to the recording): the f64 reference
+ * for ns_world_vjp's f32 device pass. Same arguments, outputs in double; much slower (one CPU
+ * thread). No counterpart in the reference. */
+int ns_world_vjp_f64(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
+                     double* dlin0, double* dang0, double* dmass, double* dfriction, double* dpos0, double* drot0);
 
 /* Diagnostics (no counterpart in the reference): an f64 check, on the host without a GPU, of
  * one local derivative the adjoint uses (which: 0 warm start, 1 push, 2 relax, 3 prepare,

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libnatsel_gpu.so")
 SOURCES = ["natsel_gpu.cu", "nsd_math.cuh", "nsd_geom.cuh", "nsd_types.cuh", "nsd_kernels.cuh", "nsd_solve.cuh",
-           "nsd_ad.cuh", "nsd_adjoint.cuh"]
+           "nsd_ad.cuh", "nsd_adjoint.cuh", "nsd_adjoint_host.h"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

@@ -20,6 +20,7 @@
 #include "../../include/natsel_gpu.h"
 #include "nsd_solve.cuh"
 #include "nsd_adjoint.cuh"
+#include "nsd_adjoint_host.h"
 
 using namespace nsd;
 
@@ -948,6 +949,7 @@ int check_adjoint_scope(ns_world* w) {
 // Device storage of the step tapes of one segment.
 struct TapeSet {
   char* data = nullptr;
+  size_t bytes = 0;
   std::vector<HostStepTape> steps;
 };
 
@@ -965,6 +967,7 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
   size_t o_relax = take(sizeof(float4) * 5 * cap * max_substeps);
   size_t o_fin = take(sizeof(float4) * cap), o_mode = take(cap), o_ops = take(sizeof(CopyOp) * 20);
   NS_CUDA(w, cudaMalloc(&ts->data, per * (size_t)count));
+  ts->bytes = per * (size_t)count;
   ts->steps.resize(count);
   for (int j = 0; j < count; ++j) {
     char* b = ts->data + per * (size_t)j;
@@ -2038,8 +2041,28 @@ int ns_world_tape_info(ns_world* w, int64_t* out) {
   return NS_OK;
 }
 
-int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
-                 float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0) {
+}  // extern "C"
+
+// A copy of a step tape whose pointers point into a host copy of the tape buffer.
+static StepTape rebase_tape(const StepTape& t, const char* dev_base, char* host_base) {
+  auto rb = [&](auto* p) { return (decltype(p))(host_base + ((const char*)p - dev_base)); };
+  StepTape h = t;
+  h.sims = rb(t.sims); h.pre = rb(t.pre); h.post = rb(t.post); h.ctl = rb(t.ctl);
+  h.body = rb(t.body); h.push = rb(t.push); h.relax = rb(t.relax); h.fin = rb(t.fin); h.mode = rb(t.mode);
+  CPlanes& P = h.planes;
+  P.idx = rb(t.planes.idx); P.mass = rb(t.planes.mass); P.ia0 = rb(t.planes.ia0); P.ia1 = rb(t.planes.ia1);
+  P.ib1 = rb(t.planes.ib1); P.n = rb(t.planes.n); P.t1 = rb(t.planes.t1); P.t2 = rb(t.planes.t2);
+  P.ca = rb(t.planes.ca); P.cb = rb(t.planes.cb); P.tm = rb(t.planes.tm); P.fr = rb(t.planes.fr);
+  P.roll = rb(t.planes.roll); P.rm = rb(t.planes.rm); P.pra = rb(t.planes.pra); P.prb = rb(t.planes.prb);
+  P.pimp = rb(t.planes.pimp); P.prest = rb(t.planes.prest);
+  return h;
+}
+
+// The vector-Jacobian product of the recorded rollout: replay each checkpoint segment with the
+// solver tape on, then reverse its steps on the device in f32 (f64 false) or on the host in f64
+// from a copy of the segment's tapes. out: 16 values per body id (lin 3, ang 3, mass, friction,
+// pos 3, rot 4, 0).
+static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::vector<double>& out) {
   if (!w) return NS_ERR_INVALID;
   if (!w->tape || w->tape->steps.empty()) return fail(w, NS_ERR_INVALID, "no recorded steps");
   NS_CUDA(w, cudaSetDevice(w->def.device));
@@ -2063,10 +2086,34 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
   TapeSet ts;
   char* buf = nullptr;
   int st = NS_OK;
+  out.assign((size_t)16 * std::max(nb, 1), 0.0);
   std::vector<float> host_out((size_t)16 * std::max(nb, 1));
+  // the host reverse pass (f64)
+  host_adj::Bufs ha;
+  std::vector<DShape> hshapes;
+  std::vector<Hull> hhulls;
+  std::vector<char> host_tape;
+  host_adj::Consts hc = {};
+  if (f64) {
+    ha.init(n, cap);
+    for (const HostShape& hs : w->shapes) { hshapes.push_back(hs.d); hhulls.push_back(hs.hull); }
+    hc.shapes = hshapes.data(); hc.hulls = hhulls.data(); hc.ssims = w->ssims.data();
+    for (int i = 0; i < nb; ++i) {
+      const HostBody& b = w->bodies[i];
+      if (b.set != 2) continue;
+      int loc = b.local;
+      for (int f = 0; f < 3; ++f) {
+        ha.CQ(loc, f) = seeds_in[0] ? seeds_in[0][3 * i + f] : 0.0;
+        ha.BB(loc, f) = seeds_in[2] ? seeds_in[2][3 * i + f] : 0.0;
+        ha.BB(loc, 4 + f) = seeds_in[3] ? seeds_in[3][3 * i + f] : 0.0;
+      }
+      for (int f = 0; f < 4; ++f) ha.CQ(loc, 4 + f) = seeds_in[1] ? seeds_in[1][4 * i + f] : 0.0;
+    }
+  }
   do {
     if ((st = take_checkpoint(w, &final_state))) break;
     if ((st = alloc_tapes(w, std::max(max_len, 1), max_sub, &ts))) break;
+    if (f64) host_tape.resize(ts.bytes);
     // cotangent buffers and staging
     size_t o = 0;
     auto take = [&](size_t b) { size_t r = o; o += align256(b); return r; };
@@ -2084,15 +2131,17 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
     a.cap = cap; a.n_awake = n;
     float* seed = (float*)(buf + o_seed);
     float* dev_out = (float*)(buf + o_out);
-    const float* src[4] = {dpos, drot, dlin, dang};
     const int width[4] = {3, 4, 3, 3};
     float* dst[4] = {seed, seed + 3 * (size_t)nb, seed + 7 * (size_t)nb, seed + 10 * (size_t)nb};
-    for (int i = 0; i < 4; ++i)
-      if (src[i]) NS_CUDA(w, cudaMemcpyAsync(dst[i], src[i], sizeof(float) * width[i] * (size_t)nb, cudaMemcpyHostToDevice, w->stream));
     int64_t launches = 2;  // the final-state snapshot and the seeds
-    k_adj_seed<<<blocks(nb, 256), 256, 0, w->stream>>>(a, w->body_loc, nb, src[0] ? dst[0] : nullptr,
-                                                        src[1] ? dst[1] : nullptr, src[2] ? dst[2] : nullptr,
-                                                        src[3] ? dst[3] : nullptr);
+    if (!f64) {
+      for (int i = 0; i < 4; ++i)
+        if (seeds_in[i])
+          NS_CUDA(w, cudaMemcpyAsync(dst[i], seeds_in[i], sizeof(float) * width[i] * (size_t)nb, cudaMemcpyHostToDevice, w->stream));
+      k_adj_seed<<<blocks(nb, 256), 256, 0, w->stream>>>(a, w->body_loc, nb, seeds_in[0] ? dst[0] : nullptr,
+                                                          seeds_in[1] ? dst[1] : nullptr, seeds_in[2] ? dst[2] : nullptr,
+                                                          seeds_in[3] ? dst[3] : nullptr);
+    }
     for (int sgi = (int)segs.size() - 1; sgi >= 0 && st == NS_OK; --sgi) {
       int s0 = segs[sgi].first, s1 = segs[sgi].second;
       if (s1 <= s0) continue;
@@ -2116,6 +2165,16 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
         else if (c.overflow_count > 0) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has overflow constraints; the adjoint does not cover them", j);
         else if (c.any_restitution) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has restitution", j);
       }
+      if (st) break;
+      if (f64) {
+        NS_CUDA(w, cudaMemcpy(host_tape.data(), ts.data, ts.bytes, cudaMemcpyDeviceToHost));
+        for (int j = s1 - 1; j >= s0; --j) {
+          StepTape t = rebase_tape(ts.steps[j - s0].dev, ts.data, host_tape.data());
+          StepParams p = make_step_params(w, tp->steps[j].dt, tp->steps[j].substeps);
+          host_adj::step(t, ha, hc, p);
+        }
+        continue;
+      }
       for (int j = s1 - 1; j >= s0 && st == NS_OK; --j) {
         const StepTape& t = ts.steps[j - s0].dev;
         StepParams p = make_step_params(w, tp->steps[j].dt, tp->steps[j].substeps);
@@ -2132,15 +2191,17 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
       }
     }
     if (st) break;
-    k_adj_result<<<blocks(nb, 256), 256, 0, w->stream>>>(a, d, w->body_loc, nb, dev_out);
-    launches += 2;  // the result and the final restore
-    tp->vjp_launches = launches;
-    NS_CUDA(w, cudaMemcpyAsync(host_out.data(), dev_out, sizeof(float) * 16 * (size_t)nb, cudaMemcpyDeviceToHost, w->stream));
     int mismatch = 0;
-    NS_CUDA(w, cudaMemcpyAsync(&mismatch, a.mismatch, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+    if (!f64) {
+      k_adj_result<<<blocks(nb, 256), 256, 0, w->stream>>>(a, d, w->body_loc, nb, dev_out);
+      launches += 2;  // the result and the final restore
+      tp->vjp_launches = launches;
+      NS_CUDA(w, cudaMemcpyAsync(host_out.data(), dev_out, sizeof(float) * 16 * (size_t)nb, cudaMemcpyDeviceToHost, w->stream));
+      NS_CUDA(w, cudaMemcpyAsync(&mismatch, a.mismatch, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+    }
     if ((st = restore_checkpoint(w, final_state))) break;
     NS_CUDA(w, cudaStreamSynchronize(w->stream));
-    tp->replay_mismatch += mismatch;
+    tp->replay_mismatch += f64 ? ha.mismatch : mismatch;
     Control c;
     if ((st = read_control(w, &c))) break;
     if ((st = control_status(w, c))) break;
@@ -2154,16 +2215,68 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
   if (ts.data) cudaFree(ts.data);
   if (buf) cudaFree(buf);
   if (st) return st;
+  if (!f64) {
+    for (size_t i = 0; i < out.size(); ++i) out[i] = host_out[i];
+    return NS_OK;
+  }
+  // results of the host pass (as k_adj_result)
   for (int i = 0; i < nb; ++i) {
-    const float* o = &host_out[(size_t)16 * i];
+    const HostBody& b = w->bodies[i];
+    if (b.set != 2) continue;
+    int loc = b.local;
+    double* o = &out[(size_t)16 * i];
+    for (int f = 0; f < 3; ++f) { o[f] = ha.BB(loc, f); o[3 + f] = ha.BB(loc, 4 + f); o[8 + f] = ha.CQ(loc, f); }
+    for (int f = 0; f < 4; ++f) o[11 + f] = ha.CQ(loc, 4 + f);
+    const DSim& s = w->asims[loc];
+    double im = s.inv_mass;
+    const float* il = &s.inv_inertia_local.cx.x;
+    const float* ii = &s.inertia.cx.x;
+    double dot_ii = 0.0, dot_i = 0.0;
+    for (int f = 0; f < 9; ++f) { dot_ii += ha.PB(loc, pbIinv + f) * il[f]; dot_i += ha.PB(loc, pbInertia + f) * ii[f]; }
+    o[6] = -ha.PB(loc, pbInvMass) * im * im - dot_ii * im + dot_i * im;
+    o[7] = ha.PB(loc, pbFriction);
+  }
+  return NS_OK;
+}
+
+extern "C" {
+
+int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
+                 float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0) {
+  const float* seeds[4] = {dpos, drot, dlin, dang};
+  std::vector<double> o;
+  int st = vjp_run(w, seeds, false, o);
+  if (st) return st;
+  for (int i = 0; i < (int)w->bodies.size(); ++i) {
+    const double* r = &o[(size_t)16 * i];
     for (int f = 0; f < 3; ++f) {
-      if (dlin0) dlin0[3 * i + f] = o[f];
-      if (dang0) dang0[3 * i + f] = o[3 + f];
-      if (dpos0) dpos0[3 * i + f] = o[8 + f];
+      if (dlin0) dlin0[3 * i + f] = (float)r[f];
+      if (dang0) dang0[3 * i + f] = (float)r[3 + f];
+      if (dpos0) dpos0[3 * i + f] = (float)r[8 + f];
     }
-    for (int f = 0; f < 4; ++f) if (drot0) drot0[4 * i + f] = o[11 + f];
-    if (dmass) dmass[i] = o[6];
-    if (dfriction) dfriction[i] = o[7];
+    for (int f = 0; f < 4; ++f) if (drot0) drot0[4 * i + f] = (float)r[11 + f];
+    if (dmass) dmass[i] = (float)r[6];
+    if (dfriction) dfriction[i] = (float)r[7];
+  }
+  return NS_OK;
+}
+
+int ns_world_vjp_f64(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
+                     double* dlin0, double* dang0, double* dmass, double* dfriction, double* dpos0, double* drot0) {
+  const float* seeds[4] = {dpos, drot, dlin, dang};
+  std::vector<double> o;
+  int st = vjp_run(w, seeds, true, o);
+  if (st) return st;
+  for (int i = 0; i < (int)w->bodies.size(); ++i) {
+    const double* r = &o[(size_t)16 * i];
+    for (int f = 0; f < 3; ++f) {
+      if (dlin0) dlin0[3 * i + f] = r[f];
+      if (dang0) dang0[3 * i + f] = r[3 + f];
+      if (dpos0) dpos0[3 * i + f] = r[8 + f];
+    }
+    for (int f = 0; f < 4; ++f) if (drot0) drot0[4 * i + f] = r[11 + f];
+    if (dmass) dmass[i] = r[6];
+    if (dfriction) dfriction[i] = r[7];
   }
   return NS_OK;
 }

@@ -87,6 +87,7 @@ EXPORTED = [
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
     "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
+    "ns_world_vjp_f64",
     "ns_adjoint_selfcheck",
 ]
 
@@ -138,6 +139,7 @@ def load_library(path=LIB_PATH):
     lib.ns_world_tape_free.argtypes = [P]
     lib.ns_world_tape_info.argtypes = [P, P]
     lib.ns_world_vjp.argtypes = [P] * 11
+    lib.ns_world_vjp_f64.argtypes = [P] * 11
     lib.ns_adjoint_selfcheck.argtypes = [ctypes.c_int, ctypes.c_int, P]
     _lib = lib
     return lib
@@ -357,6 +359,24 @@ class World:
         self._check(self._lib.ns_world_vjp(self._w, *[_ptr(a) for a in ins], _ptr(out["lin0"]), _ptr(out["ang0"]),
                                            _ptr(out["mass"]), _ptr(out["friction"]), _ptr(out["pos0"]),
                                            _ptr(out["rot0"])))
+        return out
+
+    def vjp_f64(self, dpos=None, drot=None, dlin=None, dang=None):
+        """vjp() with the reverse pass run on the host in f64 (the reference for vjp's f32 pass)."""
+        n = self.body_count
+        def arr(a, w):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, np.float32)
+            if a.shape != (n, w):
+                raise ValueError(f"cotangent must be n_bodies x {w}")
+            return a
+        ins = [arr(dpos, 3), arr(drot, 4), arr(dlin, 3), arr(dang, 3)]
+        out = dict(lin0=np.zeros((n, 3)), ang0=np.zeros((n, 3)), mass=np.zeros(n), friction=np.zeros(n),
+                   pos0=np.zeros((n, 3)), rot0=np.zeros((n, 4)))
+        self._check(self._lib.ns_world_vjp_f64(self._w, *[_ptr(a) for a in ins], _ptr(out["lin0"]),
+                                               _ptr(out["ang0"]), _ptr(out["mass"]), _ptr(out["friction"]),
+                                               _ptr(out["pos0"]), _ptr(out["rot0"])))
         return out
 
 

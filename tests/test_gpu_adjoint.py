@@ -217,3 +217,58 @@ def test_adjoint_scope_is_enforced():
     with pytest.raises(NsError):
         w.step(0.0, SUBSTEPS)
     w.close()
+
+
+def _f64_agreement(g32, g64, keys):
+    """Relative differences of the f32 device adjoint from the f64 host adjoint, per entry, with a
+    floor of 1e-3 of the kind's largest f64 entry."""
+    out = []
+    for k in keys:
+        a, b = np.asarray(g32[k], np.float64).ravel(), np.asarray(g64[k]).ravel()
+        scale = np.abs(b).max()
+        out.append(np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * scale + 1e-300))
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("scene", ["sliders", "collide", "stack"])
+def test_f32_adjoint_matches_f64_host_adjoint(scene):
+    # the same recorded rollout reversed on the device in f32 and on the host in f64
+    bodies, gf = {"sliders": (SLIDERS, 0.6), "collide": (COLLIDE, 0.05), "stack": (STACK, 0.6)}[scene]
+    w = build(bodies, 8, gf)
+    for _ in range(STEPS):
+        w.step(DT, SUBSTEPS)
+    pos = w.bodies()[0]
+    dpos = np.zeros_like(pos, dtype=np.float32)
+    dpos[1:] = 2.0 * (pos[1:] - targets(bodies))
+    g32, g64 = w.vjp(dpos=dpos), w.vjp_f64(dpos=dpos)
+    w.close()
+    vel = {k: np.concatenate([g64["lin0"].ravel(), g64["ang0"].ravel()]) for k in ("lin0", "ang0")}
+    for k in ("lin0", "ang0", "friction", "mass"):
+        a, b = np.asarray(g32[k], np.float64).ravel(), np.asarray(g64[k]).ravel()
+        scale = np.abs(vel[k]).max() if k in vel else np.abs(b).max()
+        if k == "mass" and scale < 1e-6 * np.abs(vel["lin0"]).max():
+            continue  # the loss does not depend on the masses here (friction-driven sliding)
+        assert np.all(np.abs(a - b) <= 1e-3 * np.abs(b) + 1e-4 * scale), (k, a, b)
+
+
+def test_rollout_f32_adjoint_matches_f64_host_adjoint():
+    # 1024 tumbling cubes, 8 steps: a recomputed comparison can land on the other side of a near
+    # tie in f64, so a few entries take another branch; the rest agree to f32 rounding
+    from natsel_b200 import scenes
+    s = scenes.WORLD_SETTINGS["differentiable_rollout"]
+    w = World(gravity=s["gravity"], enable_continuous=0, enable_sleep=0)
+    info = scenes.differentiable_rollout(w)
+    w.tape_begin(8)
+    for _ in range(8):
+        w.step(DT, SUBSTEPS)
+    p = w.bodies()[0]
+    d = np.zeros_like(p, dtype=np.float32)
+    d[1:] = 2.0 * (p[1:] - info["targets"])
+    g32, g64 = w.vjp(dpos=d), w.vjp_f64(dpos=d)
+    assert w.tape_info()[2] == 0
+    w.close()
+    rel = _f64_agreement(g32, g64, ("lin0", "ang0", "mass", "friction"))
+    assert np.median(rel) < 1e-4
+    # measured: 97.9 % within 1e-3; the rest are bodies downstream (through the contact graph) of
+    # an update whose branch resolves differently in f64
+    assert np.mean(rel < 1e-3) > 0.95, np.sort(rel)[-20:]
