@@ -404,6 +404,10 @@ def run_natsel_arm(args):
     for _ in range(args.warmup):
         world.step(DT, sub)
     world.synchronize()
+    autotune = None
+    if scene == "batched_worlds":
+        # the solver's launch shape for this batch, timed from a copy of its state (unchanged)
+        autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms} for b, g, ms in world.autotune(DT, sub, 3)]
     stream = torch.cuda.ExternalStream(world.stream(), device=dev)  # created by the first step
     launches0 = int(world.solver_counts()[12])
 
@@ -469,6 +473,7 @@ def run_natsel_arm(args):
             "data": "synthetic (seeded scene builder, no dataset)", "config": config_block(args, desc),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": launches,
             "one_world_at_a_time": one_at_a_time,
+            "solver_autotune": autotune,
             "wall_s": wall,
             "phase_ms_mean": {k: float(v) for k, v in zip(["broadphase", "collide", "state_color_prepare", "solve",
                                                           "finalize"], phase.mean(0))},

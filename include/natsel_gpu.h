@@ -204,6 +204,18 @@ int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int cou
  * CUDA context stays usable afterwards. */
 int ns_selftest_barrier_timeout(int device, int timeout_ms);
 
+/* Picks the solver's launch shape for this world by timing (no counterpart in the reference,
+ * whose solver is a CPU worker pool): each candidate -- thread-block clusters of 8 and 16 CTAs,
+ * cooperative grids over half the SMs and of 1 to 4 blocks per SM as far as they fit -- steps the world
+ * for 1 + steps steps of (dt, substeps) from a copy of its current state, timed with CUDA events;
+ * the fastest is kept and the world is put back exactly as it was (every shape gives the same
+ * bits). Per candidate c < max_candidates: blocks_out[c], grid_out[c] (1 cooperative grid, 0
+ * cluster) and ms_out[c] (ms per step, -1 for a cluster that does not fit); any may be NULL.
+ * Returns the number of candidates (>= 1), or minus an NS_ERR_* status (message in
+ * ns_last_error). Refused while a tape records. */
+int ns_world_autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_out, int* grid_out,
+                      float* ms_out, int max_candidates);
+
 /* ---- Adjoint: vector-Jacobian product of a recorded rollout --------------------------------
  * No counterpart in the reference, which has no differentiation; these calls are the
  * differentiable form of World::step (solver_integration.rs:807) built on the same step.

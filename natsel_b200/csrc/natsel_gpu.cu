@@ -1992,6 +1992,107 @@ int ns_selftest_barrier_timeout(int device, int timeout_ms) {
 }
 
 
+static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_out, int* grid_out,
+                    float* ms_out, int max_candidates, int* count) {
+  if (!w) return NS_ERR_INVALID;
+  if (!(dt > 0.0f) || steps < 1) return fail(w, NS_ERR_INVALID, "autotune needs dt > 0 and steps >= 1");
+  if (w->tape && w->tape->recording) return fail(w, NS_ERR_UNSUPPORTED, "autotune while a tape records");
+  if (!w->uploaded) {
+    int st = upload_world(w);
+    if (st) return st;
+  }
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  // candidate launch shapes: thread-block clusters of 8 and 16 CTAs, cooperative grids of 1..4
+  // blocks per SM (as many as can be co-resident)
+  int per_sm = 0;
+  NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true, false>, kSolveThreads, 0));
+  NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  std::vector<std::pair<int, bool>> cand = {{8, false}, {kMaxSolveCluster, false}, {w->sm_count / 2, true}};
+  for (int k = 1; k <= std::min(per_sm, 4); ++k) cand.push_back({k * w->sm_count, true});
+  const int old_blocks = w->solver_blocks;
+  const bool old_grid = w->solver_grid, old_eager = w->eager;
+  AdCheckpoint snap;
+  int st = take_checkpoint(w, &snap);
+  std::vector<float> ms(cand.size(), 0.0f);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!st && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    st = fail(w, NS_ERR_CUDA, "autotune events");
+  for (size_t c = 0; c < cand.size() && !st; ++c) {
+    w->solver_blocks = cand[c].first;
+    w->solver_grid = cand[c].second;
+    if (!w->solver_grid) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.blockDim = dim3(kSolveThreads);
+      cfg.gridDim = dim3(w->solver_blocks);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = w->solver_blocks;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, k_solve<false, false>, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        ms[c] = -1.0f;  // this cluster size does not fit
+        continue;
+      }
+    }
+    if ((st = restore_checkpoint(w, snap))) break;
+    // one untimed step, then `steps` timed ones, eagerly (the graph is captured for one shape)
+    if ((st = enqueue_step(w, dt, substeps))) break;
+    NS_CUDA(w, cudaEventRecord(e0, w->stream));
+    for (int k = 0; k < steps && !st; ++k) st = enqueue_step(w, dt, substeps);
+    if (st) break;
+    NS_CUDA(w, cudaEventRecord(e1, w->stream));
+    NS_CUDA(w, cudaEventSynchronize(e1));
+    float t = 0.0f;
+    NS_CUDA(w, cudaEventElapsedTime(&t, e0, e1));
+    ms[c] = t / (float)steps;
+    Control ctl;
+    if ((st = read_control(w, &ctl))) break;
+    if ((st = control_status(w, ctl))) break;
+  }
+  // keep the fastest shape and put the world back as it was
+  int best = -1;
+  for (size_t c = 0; c < cand.size(); ++c)
+    if (ms[c] > 0.0f && (best < 0 || ms[c] < ms[best])) best = (int)c;
+  if (!st && best < 0) st = fail(w, NS_ERR_CUDA, "no solver launch shape could be timed");
+  if (snap.data) {
+    int st2 = restore_checkpoint(w, snap);
+    cudaStreamSynchronize(w->stream);
+    cudaFree(snap.data);
+    if (!st) st = st2;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  w->eager = old_eager;
+  if (st) {
+    w->solver_blocks = old_blocks;
+    w->solver_grid = old_grid;
+    return st;
+  }
+  w->solver_blocks = cand[best].first;
+  w->solver_grid = cand[best].second;
+  if (w->graph_exec) { cudaGraphExecDestroy(w->graph_exec); w->graph_exec = nullptr; }
+  if (w->graph) { cudaGraphDestroy(w->graph); w->graph = nullptr; }
+  int n = std::min<int>((int)cand.size(), max_candidates);
+  for (int c = 0; c < n; ++c) {
+    if (blocks_out) blocks_out[c] = cand[c].first;
+    if (grid_out) grid_out[c] = cand[c].second ? 1 : 0;
+    if (ms_out) ms_out[c] = ms[c];
+  }
+  *count = (int)cand.size();
+  return NS_OK;
+}
+
+int ns_world_autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_out, int* grid_out,
+                      float* ms_out, int max_candidates) {
+  int count = 0;
+  int st = autotune(w, dt, substeps, steps, blocks_out, grid_out, ms_out, max_candidates, &count);
+  return st ? -st : count;
+}
+
 int ns_world_tape_begin(ns_world* w, int checkpoint_substeps) {
   if (!w) return NS_ERR_INVALID;
   if (checkpoint_substeps < 1) return fail(w, NS_ERR_INVALID, "checkpoint_substeps must be >= 1");

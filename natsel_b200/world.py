@@ -87,7 +87,7 @@ EXPORTED = [
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
     "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
-    "ns_world_vjp_f64",
+    "ns_world_vjp_f64", "ns_world_autotune",
     "ns_adjoint_selfcheck",
 ]
 
@@ -140,6 +140,7 @@ def load_library(path=LIB_PATH):
     lib.ns_world_tape_info.argtypes = [P, P]
     lib.ns_world_vjp.argtypes = [P] * 11
     lib.ns_world_vjp_f64.argtypes = [P] * 11
+    lib.ns_world_autotune.argtypes = [P, ctypes.c_float, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_int]
     lib.ns_adjoint_selfcheck.argtypes = [ctypes.c_int, ctypes.c_int, P]
     _lib = lib
     return lib
@@ -320,6 +321,17 @@ class World:
 
     def stream(self):
         return self._lib.ns_world_stream(self._w)
+
+    def autotune(self, dt=1.0 / 60.0, substeps=4, steps=5):
+        """Time the solver's candidate launch shapes on this world and keep the fastest (the world
+        state is unchanged). Returns [(blocks, cooperative_grid, ms_per_step), ...]."""
+        blocks = np.zeros(8, np.int32)
+        grid = np.zeros(8, np.int32)
+        ms = np.zeros(8, np.float32)
+        r = self._lib.ns_world_autotune(self._w, dt, substeps, steps, _ptr(blocks), _ptr(grid), _ptr(ms), 8)
+        if r < 0:
+            raise NsError(-r, self._lib.ns_last_error(self._w).decode())
+        return [(int(blocks[c]), bool(grid[c]), float(ms[c])) for c in range(min(r, 8))]
 
     # ---- adjoint ---------------------------------------------------------------------------
     def tape_begin(self, checkpoint_substeps=8):

@@ -72,3 +72,34 @@ def test_subworld_rules():
         g.create_revolute(b0, b1, (0,) * 6 + (1,), (0,) * 6 + (1,))
     g.create_box(b1, 0.5, 0.5, 0.5)
     assert list(g.subworld_bodies()) == [0, 1, 2]
+
+
+@pytest.mark.parametrize("batched", [True, False], ids=["batch", "single-world"])
+def test_autotune_keeps_the_world_and_its_trajectory(batched):
+    """ns_world_autotune times the solver's candidate launch shapes from a copy of the world's
+    state and keeps the fastest: the world is left as it was, and the steps after it are
+    bit-identical to those of a world that was never tuned."""
+    def build():
+        g = World(default_world_def(gravity=SETTINGS["gravity"], enable_continuous=0))
+        if batched:
+            scenes.batched_worlds(g, count=96, seed=4)
+        else:
+            scenes.large_pile(g, n=1500, seed=5, spread=8.0, drop=(1.0, 15.0))
+        return g
+    tuned, plain = build(), build()
+    for w in (tuned, plain):
+        for _ in range(5):
+            w.step(DT, 4)
+    before = tuned.state_hash()
+    table = tuned.autotune(DT, 4, steps=3)
+    assert len(table) >= 2 and all(ms > 0 or (not grid and ms == -1.0) for _, grid, ms in table)
+    assert tuned.state_hash() == before
+    chosen = tuned.solver_counts()
+    fastest = min((ms, b, grid) for b, grid, ms in table if ms > 0)
+    assert (int(chosen[13]), bool(chosen[14])) == (fastest[1], fastest[2])
+    for _ in range(10):
+        tuned.step(DT, 4)
+        plain.step(DT, 4)
+        assert tuned.state_hash() == plain.state_hash()
+    tuned.close()
+    plain.close()
