@@ -204,8 +204,8 @@ int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int cou
  * CUDA context stays usable afterwards. */
 int ns_selftest_barrier_timeout(int device, int timeout_ms);
 
-/* Picks the solver's launch shape for this world by timing (no counterpart in the reference,
- * whose solver is a CPU worker pool): each candidate -- thread-block clusters of 8 and 16 CTAs,
+/* Picks the solver's launch shape for this world by timing (replaces the reference's hand-set
+ * CPU worker count, WorldDef::worker_count, src/types/world_def.rs:94): each candidate -- thread-block clusters of 8 and 16 CTAs,
  * cooperative grids over half the SMs and of 1 to 4 blocks per SM as far as they fit -- steps the world
  * for 1 + steps steps of (dt, substeps) from a copy of its current state, timed with CUDA events;
  * the fastest is kept and the world is put back exactly as it was (every shape gives the same
