@@ -365,7 +365,7 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_solve<false, false>,
                            (const void*)k_solve<true, true>,
                            (const void*)k_solve<false, true>,
-                           (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare,
+                           (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare, (const void*)k_warm_slots,
                            (const void*)k_finalize, (const void*)k_state_pass,
                            (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
                            (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
@@ -518,6 +518,7 @@ int upload_world(ns_world* w) {
   ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
   ALLOC(long_segment, int, kLongSegmentCap);
   ALLOC(ctl, Control, 1);
+  ALLOC(bwd, float4, 48 * (size_t)na); ALLOC(bw_mask, uint32_t, na);
   CPlanes& P = d.cp;
   P.cap = cap;
 #define PALLOC(field, T, n) do { P.field = dalloc<T>(w, (n), &st); if (!P.field) return st; } while (0)
@@ -773,6 +774,10 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
     cfg.blockDim = dim3(kSolveThreads);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
+    if (d.n_awake > 0) {
+      NS_CUDA(w, cudaMemsetAsync(d.bw_mask, 0, sizeof(uint32_t) * d.n_awake, s));
+      k_warm_slots<<<4 * w->sm_count, 256, 0, s>>>(d, w->jr); ++nk;
+    }
     if (w->solver_grid) {
       NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
       attr[0].id = cudaLaunchAttributeCooperative;

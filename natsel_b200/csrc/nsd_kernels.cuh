@@ -61,6 +61,11 @@ struct DW {
   // Optional record of each contact's narrowphase outcome (0 none or disjoint, 1 recycled,
   // 2 new manifold, 3 no points), written only while the adjoint replays a step.
   uint8_t* np_mode;
+  // Warm start by body: slot (body, colour c) of bwd holds the velocity change that body's
+  // constraint or joint of colour c applies at the next warm start, (dv, dw) at
+  // 2 * (24 * body + c) + {0, 1}, signed for the body's side; bit c of bw_mask[body] marks the
+  // slot as used this step.
+  float4* bwd; uint32_t* bw_mask;
   int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
 };
 

@@ -26,14 +26,17 @@ __device__ __forceinline__ void cluster_sync_all() {
 // self-test, to wait for arrivals that never come). The wait is bounded: after limit_ns (2 s),
 // 2^26 polls or another block's error it raises NS_ERR_TIMEOUT and returns false, and every
 // block then leaves the kernel at its next barrier.
-__device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index, int missing = 0,
-                                                  unsigned long long limit_ns = 2000000000ull) {
-  __shared__ int ok_s;
+__device__ __forceinline__ void grid_arrive(Control* ctl) {
   __syncthreads();
+  if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(&ctl->barrier_count) : "memory");
+}
+
+__device__ __forceinline__ bool grid_wait(Control* ctl, int& index, int missing = 0,
+                                          unsigned long long limit_ns = 2000000000ull) {
+  __shared__ int ok_s;
   if (threadIdx.x == 0) {
     int target = (index + 1) * (int)gridDim.x + missing;
     int* cnt = &ctl->barrier_count;
-    asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(cnt) : "memory");
     int ok = 1;
     unsigned long long t0;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
@@ -53,6 +56,12 @@ __device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index, int 
   __syncthreads();
   index++;
   return ok_s != 0;
+}
+
+__device__ __forceinline__ bool grid_sync_acq_rel(Control* ctl, int& index, int missing = 0,
+                                                  unsigned long long limit_ns = 2000000000ull) {
+  grid_arrive(ctl);
+  return grid_wait(ctl, index, missing, limit_ns);
 }
 
 // Self-test of the solver's bounded grid barrier: every block arrives, but the barrier also
@@ -88,6 +97,7 @@ struct IVIn {
   M3 inertia;
   V3 v, w;
   Q dq;
+  uint32_t state_flags;
 };
 __device__ __forceinline__ IVIn load_iv(const DW& w, int i) {
   const DSim& sim = w.asims[i];
@@ -101,9 +111,10 @@ __device__ __forceinline__ IVIn load_iv(const DW& w, int i) {
   r.q = sim.q;
   r.inertia = sim.inertia;
   r.v = st.v; r.w = st.w; r.dq = st.dq;
+  r.state_flags = st.flags;
   return r;
 }
-__device__ __forceinline__ void apply_iv(const DW& w, const StepParams& p, int i, const IVIn& sim) {
+__device__ __forceinline__ void integrate_velocity(const StepParams& p, const IVIn& sim, V3& v_out, V3& w_out) {
   float h = p.h;
   V3 v = sim.v, wv = sim.w;
   float ld = 1.0f / (1.0f + h * sim.lin_damp);
@@ -136,9 +147,8 @@ __device__ __forceinline__ void apply_iv(const DW& w, const StepParams& p, int i
     om2 = om2 - solve3(J, b);
     wv = rotate(q, om2);
   }
-  DState& st = w.states[i];
-  st.v = v;
-  st.w = wv;
+  v_out = v;
+  w_out = wv;
 }
 
 // solver_integration.rs:377 integrate_positions_range (the state row is the only input)
@@ -203,9 +213,15 @@ struct CData {
   float prest[4];
 };
 
+// Every field is written (zero where the stage reads nothing), so a CData held across the
+// solver's phase loop carries no value from an earlier constraint. The four point slots are
+// read whatever the point count (the planes hold 4 x cap entries) and the unused ones zeroed
+// afterwards, so no load waits for the index load: one L2 round trip brings the constraint.
 __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d) {
+  const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   d.c = unpack_constraint(__ldg(&P.idx[k]), __ldg(&P.mass[k]), __ldg(&P.ia0[k]), __ldg(&P.ia1[k]),
                           __ldg(&P.ib1[k]), __ldg(&P.n[k]));
+  d.t1 = z; d.t2 = z; d.ca = z; d.cb = z; d.fr = z; d.roll = z; d.rm = z; d.tm = z;
   if (stage == kWarm || stage == kRelax) {
     d.t1 = __ldg(&P.t1[k]); d.t2 = __ldg(&P.t2[k]); d.ca = __ldg(&P.ca[k]);
     d.cb = P.cb[k]; d.fr = P.fr[k]; d.roll = P.roll[k];
@@ -213,53 +229,121 @@ __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, 
   if (stage == kRelax) { d.rm = __ldg(&P.rm[k]); d.tm = __ldg(&P.tm[k]); }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    if (q < d.c.pc) {
-      d.pra[q] = __ldg(&P.pra[q * P.cap + k]);
-      d.prb[q] = __ldg(&P.prb[q * P.cap + k]);
-      d.pimp[q] = P.pimp[q * P.cap + k];
-      if (stage == kRestitution) d.prest[q] = P.prest[q * P.cap + k];
-    }
+    d.pra[q] = __ldg(&P.pra[q * P.cap + k]);
+    d.prb[q] = __ldg(&P.prb[q * P.cap + k]);
+    d.pimp[q] = P.pimp[q * P.cap + k];
+    d.prest[q] = stage == kRestitution ? P.prest[q * P.cap + k] : 0.0f;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (q >= d.c.pc) { d.pra[q] = z; d.prb[q] = z; d.pimp[q] = z; d.prest[q] = 0.0f; }
   }
 }
 
-// contact_solver.rs:697 warm_start_contacts_body
-__device__ void warm_start_constraint(const DW& w, const CData& d) {
-  const CLoad& c = d.c;
-  DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
-  V3 t1 = v3(d.t1.x, d.t1.y, d.t1.z), t2 = v3(d.t2.x, d.t2.y, d.t2.z);
-  V3 center_a = v3(d.ca.x, d.ca.y, d.ca.z), center_b = v3(d.cb.x, d.cb.y, d.cb.z);
-  float twist = d.cb.w;
+// Change of the two bodies' velocities by one warm start: body a gets v - dva, w - dwa and
+// body b v + dvb, w + dvb. It depends on the constraint's planes and impulses only, not on the
+// bodies' velocities, so it can be formed when the impulses are last updated and applied later
+// by each body in colour order with the same operations.
+struct WarmDelta { V3 dva, dwa, dvb, dwb; };
+
+// contact_solver.rs:697 warm_start_contacts_body (the per-body change; ni the points' normal
+// impulses, fr the friction impulses, cbf.w the twist impulse, roll the rolling impulse)
+__device__ __forceinline__ WarmDelta contact_warm_delta(const CLoad& c, float4 t1f, float4 t2f, float4 caf,
+                                                        float4 cbf, float4 fr, float4 roll, const float4* pra,
+                                                        const float4* prb, const float* ni) {
+  V3 t1 = v3(t1f.x, t1f.y, t1f.z), t2 = v3(t2f.x, t2f.y, t2f.z);
+  V3 center_a = v3(caf.x, caf.y, caf.z), center_b = v3(cbf.x, cbf.y, cbf.z);
+  float twist = cbf.w;
   V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
   float tni = 0.0f;
   V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     if (q < c.pc) {
-      float ni = d.pimp[q].x;
-      tni += ni;
-      moa = mul_add(moa, ni, v3(d.pra[q].x, d.pra[q].y, d.pra[q].z));
-      mob = mul_add(mob, ni, v3(d.prb[q].x, d.prb[q].y, d.prb[q].z));
+      tni += ni[q];
+      moa = mul_add(moa, ni[q], v3(pra[q].x, pra[q].y, pra[q].z));
+      mob = mul_add(mob, ni[q], v3(prb[q].x, prb[q].y, prb[q].z));
     }
   }
   V3 n = c.n;
-  V3 fi = d.fr.x * t1;
-  fi = mul_add(fi, d.fr.y, t2);
+  V3 fi = fr.x * t1;
+  fi = mul_add(fi, fr.y, t2);
   V3 lin = mul_add(fi, tni, n);
   V3 twi = twist * n;
   V3 anga = cross(moa, n) + cross(center_a, fi) + twi;
   V3 angb = cross(mob, n) + cross(center_b, fi) + twi;
   if (c.rolling > 0.0f) {
-    V3 ri = v3(d.roll.x, d.roll.y, d.roll.z);
+    V3 ri = v3(roll.x, roll.y, roll.z);
     anga = anga + ri;
     angb = angb + ri;
   }
   li = li + lin; aia = aia + anga; aib = aib + angb;
-  ba.w = ba.w - sym_mv(c.sa, aia);
-  ba.v = ba.v - c.ima * li;
-  bb.w = bb.w + sym_mv(c.sb, aib);
-  bb.v = bb.v + c.imb * li;
-  store_state_vw(w, c.ia, ba);
-  store_state_vw(w, c.ib, bb);
+  WarmDelta r;
+  r.dwa = sym_mv(c.sa, aia);
+  r.dva = c.ima * li;
+  r.dwb = sym_mv(c.sb, aib);
+  r.dvb = c.imb * li;
+  return r;
+}
+
+// Record a warm-start change in the slots of colour `color` of both bodies (a static body, index
+// -1, has none). Body a's change is stored negated: v + (-x) is v - x exactly.
+__device__ __forceinline__ void put_warm_delta(const DW& w, int ia, int ib, int color, const WarmDelta& x) {
+  if (ia >= 0) {
+    float4* s = w.bwd + 2 * (24 * (size_t)ia + color);
+    s[0] = make_float4(-x.dva.x, -x.dva.y, -x.dva.z, 0.0f);
+    s[1] = make_float4(-x.dwa.x, -x.dwa.y, -x.dwa.z, 0.0f);
+  }
+  if (ib >= 0) {
+    float4* s = w.bwd + 2 * (24 * (size_t)ib + color);
+    s[0] = make_float4(x.dvb.x, x.dvb.y, x.dvb.z, 0.0f);
+    s[1] = make_float4(x.dwb.x, x.dwb.y, x.dwb.z, 0.0f);
+  }
+}
+
+__device__ __forceinline__ void mark_warm_slot(const DW& w, int body, int color) {
+  if (body >= 0) atomicOr(&w.bw_mask[body], 1u << color);
+}
+
+// A dynamic body's warm start: the changes of its constraints and joints in colour order (the
+// order the colour phases would apply them; one item per colour). load_warm_slots fetches up
+// to kSlotBatch slots and clears their bits from m; apply_warm_slots adds them in order.
+constexpr int kSlotBatch = 8;
+struct WarmSlots {
+  float4 dv[kSlotBatch], dw[kSlotBatch];
+  int count;
+};
+__device__ __forceinline__ void load_warm_slots(const DW& w, int i, uint32_t& m, WarmSlots& ws) {
+  const float4* row = w.bwd + 48 * (size_t)i;
+  ws.count = 0;
+#pragma unroll
+  for (int q = 0; q < kSlotBatch; ++q) {
+    ws.dv[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    ws.dw[q] = ws.dv[q];
+    if (m != 0u) {
+      int c = __ffs(m) - 1;
+      m &= m - 1u;
+      ws.dv[q] = row[2 * c];
+      ws.dw[q] = row[2 * c + 1];
+      ws.count = q + 1;
+    }
+  }
+}
+__device__ __forceinline__ void apply_warm_slots(const WarmSlots& ws, V3& v, V3& wv) {
+#pragma unroll
+  for (int q = 0; q < kSlotBatch; ++q) {
+    if (q < ws.count) {
+      wv = wv + v3(ws.dw[q].x, ws.dw[q].y, ws.dw[q].z);
+      v = v + v3(ws.dv[q].x, ws.dv[q].y, ws.dv[q].z);
+    }
+  }
+}
+__device__ __forceinline__ void warm_body(const DW& w, int i, uint32_t m, WarmSlots& ws, V3& v, V3& wv) {
+  apply_warm_slots(ws, v, wv);
+  while (m != 0u) {
+    load_warm_slots(w, i, m, ws);
+    apply_warm_slots(ws, v, wv);
+  }
 }
 
 // contact_solver.rs:796 push_contacts_body
@@ -315,7 +399,9 @@ __device__ void push_constraint(const DW& w, const StepParams& p, int k, const C
 }
 
 // contact_solver.rs:927 solve_contacts_body (relax)
-__device__ void relax_constraint(const DW& w, const StepParams& p, int k, const CData& d) {
+// warm_color >= 0: also record the warm-start change of the next substep from the updated
+// impulses in the bodies' slots of that colour.
+__device__ void relax_constraint(const DW& w, const StepParams& p, int k, const CData& d, int warm_color) {
   const CPlanes& P = w.cp;
   const CLoad& c = d.c;
   DState ba = state_at(w, c.ia), bb = state_at(w, c.ib);
@@ -334,6 +420,7 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k, const 
   float lt1 = dot(t1, dv) - d.t1.w;
   float lt2 = dot(t2, dv) - d.t2.w;
   float mi = 0.0f, tni = 0.0f, ttl = 0.0f;
+  float nis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     if (q < c.pc) {
@@ -351,6 +438,7 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k, const 
       imp4.x = ni;
       imp4.y = imp4.y + ni;
       P.pimp[q * P.cap + k] = imp4;
+      nis[q] = ni;
       tni += ni;
       ttl += imp4.z * ni;
       lnv += im * impulse;
@@ -376,6 +464,7 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k, const 
     ba.w = ba.w - sym_mv(c.sa, di);
     bb.w = bb.w + sym_mv(c.sb, di);
     P.roll[k] = make_float4(rimp.x, rimp.y, rimp.z, ro.w);
+    ro = make_float4(rimp.x, rimp.y, rimp.z, ro.w);
   }
   {
     float ts = dot(n, bb.w - ba.w);
@@ -415,6 +504,9 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k, const 
   }
   store_state_vw(w, c.ia, ba);
   store_state_vw(w, c.ib, bb);
+  if (warm_color >= 0)
+    put_warm_delta(w, c.ia, c.ib, warm_color,
+                   contact_warm_delta(c, d.t1, d.t2, caf, cbf, fr, ro, d.pra, d.prb, nis));
 }
 
 // contact_solver.rs:1135 apply_restitution_body
@@ -468,10 +560,10 @@ __device__ void restitution_constraint(const DW& w, const StepParams& p, int k, 
   store_state_vw(w, c.ib, bb);
 }
 
-__device__ __forceinline__ void run_contact(const DW& w, const StepParams& p, int k, int stage, const CData& d) {
-  if (stage == kWarm) warm_start_constraint(w, d);
-  else if (stage == kPush) push_constraint(w, p, k, d);
-  else if (stage == kRelax) relax_constraint(w, p, k, d);
+__device__ __forceinline__ void run_contact(const DW& w, const StepParams& p, int k, int stage, const CData& d,
+                                            int warm_color) {
+  if (stage == kPush) push_constraint(w, p, k, d);
+  else if (stage == kRelax) relax_constraint(w, p, k, d, warm_color);
   else restitution_constraint(w, p, k, d);
 }
 
@@ -765,21 +857,29 @@ __device__ V3 solve_point_constraint(float ma, float mb, M3 ia, M3 ib, V3 ra, V3
   return v3(0, 0, 0);
 }
 
-// revolute_joint.rs:261 warm_start_revolute_joint
-__device__ __noinline__ void warm_start_joint(const DW& w, DJoint& j) {
+// revolute_joint.rs:261 warm_start_revolute_joint, the per-body change (dqa, dqb: the bodies'
+// rotation increments, which no stage between a joint's last update and the next warm start
+// changes)
+__device__ __forceinline__ WarmDelta joint_warm_delta(const DJoint& j, Q dqa, Q dqb) {
   float mA = j.inv_mass_a, mB = j.inv_mass_b;
-  DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
-  V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
-  V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
+  V3 ra = rotate(dqa, j.frame_a.p), rb = rotate(dqb, j.frame_b.p);
   float axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
   V3 ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
   ang = mul_add(ang, axial, j.rotation_axis_z);
-  va = va - mA * j.linear_impulse;
-  wa = wa - mul_mv(j.inv_ia, cross(ra, j.linear_impulse) + ang);
-  vb = vb + mB * j.linear_impulse;
-  wb = wb + mul_mv(j.inv_ib, cross(rb, j.linear_impulse) + ang);
-  if (sa.flags & kDynamicFlag) { sa.v = va; sa.w = wa; }
-  if (sb.flags & kDynamicFlag) { sb.v = vb; sb.w = wb; }
+  WarmDelta r;
+  r.dva = mA * j.linear_impulse;
+  r.dwa = mul_mv(j.inv_ia, cross(ra, j.linear_impulse) + ang);
+  r.dvb = mB * j.linear_impulse;
+  r.dwb = mul_mv(j.inv_ib, cross(rb, j.linear_impulse) + ang);
+  return r;
+}
+
+// The same applied at once (the overflow colour's joints).
+__device__ __noinline__ void warm_start_joint(const DW& w, DJoint& j) {
+  DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+  WarmDelta x = joint_warm_delta(j, sa.dq, sb.dq);
+  if (sa.flags & kDynamicFlag) { sa.v = sa.v - x.dva; sa.w = sa.w - x.dwa; }
+  if (sb.flags & kDynamicFlag) { sb.v = sb.v + x.dvb; sb.w = sb.w + x.dwb; }
   store_state_vw(w, j.index_a, sa);
   store_state_vw(w, j.index_b, sb);
 }
@@ -944,8 +1044,46 @@ __device__ void run_overflow(const DW& w, const StepParams& p, const JointRanges
   }
 }
 
+// Warm start of a step's first substep: every coloured constraint and joint records its change
+// in its bodies' slots and marks them (later substeps' changes are recorded by the relax
+// updates before them). bw_mask is zero at launch.
+__global__ void __launch_bounds__(256) k_warm_slots(DW w, JointRanges jr) {
+  __shared__ int coff[kOverflowIndex + 1];
+  if (threadIdx.x <= kOverflowIndex) coff[threadIdx.x] = w.ctl->color_offset[threadIdx.x];
+  __syncthreads();
+  const int n_col = coff[kOverflowIndex], n_jnt = jr.off[kOverflowIndex];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_col + n_jnt; i += gridDim.x * blockDim.x) {
+    if (i < n_col) {
+      const int k = i;
+      int c = 0;
+      while (coff[c + 1] <= k) ++c;
+      CData d;
+      load_direct(w.cp, k, kWarm, d);
+      float ni[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ni[q] = d.pimp[q].x;
+      put_warm_delta(w, d.c.ia, d.c.ib, c,
+                     contact_warm_delta(d.c, d.t1, d.t2, d.ca, d.cb, d.fr, d.roll, d.pra, d.prb, ni));
+      mark_warm_slot(w, d.c.ia, c);
+      mark_warm_slot(w, d.c.ib, c);
+    } else {
+      const int t = i - n_col;
+      int c = 0;
+      while (jr.off[c + 1] <= t) ++c;
+      const DJoint& j = w.joints[w.joint_list[t]];
+      DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+      put_warm_delta(w, j.index_a, j.index_b, c, joint_warm_delta(j, sa.dq, sb.dq));
+      mark_warm_slot(w, j.index_a, c);
+      mark_warm_slot(w, j.index_b, c);
+    }
+  }
+}
+
 // Phase codes: contact phases stage * 32 + color; the rest as below.
-constexpr int kPhaseIntegrateVelocity = 1000, kPhaseIntegratePosition = 1001, kPhaseOverflow = 2000;
+// kPhaseIntegrateVelocityWarm: integrate velocities, then each body's warm start from its
+// slots; kPhaseBodyWarm: the slots alone (after the overflow colour's warm start).
+constexpr int kPhaseIntegrateVelocity = 1000, kPhaseIntegratePosition = 1001, kPhaseIntegrateVelocityWarm = 1002,
+              kPhaseBodyWarm = 1003, kPhaseOverflow = 2000;
 
 // Record of the solver's inputs kept while the adjoint replays a step (kTape): per substep
 // three body rows (before integrate-velocities, before and after integrate-positions), the
@@ -987,8 +1125,14 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
     int n_ovf = w.ctl->overflow_count;
     bool ovf_work = n_ovf > 0 || jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex];
     int n = 0;
-    phases[n++] = kPhaseIntegrateVelocity;
-    for (int stage = kWarm; stage <= kRelax; ++stage) {
+    if (ovf_work) {
+      phases[n++] = kPhaseIntegrateVelocity;
+      phases[n++] = kPhaseOverflow + kWarm;
+      phases[n++] = kPhaseBodyWarm;
+    } else {
+      phases[n++] = kPhaseIntegrateVelocityWarm;
+    }
+    for (int stage = kPush; stage <= kRelax; ++stage) {
       if (stage == kRelax) phases[n++] = kPhaseIntegratePosition;
       if (ovf_work) phases[n++] = kPhaseOverflow + stage;
       for (int c = 0; c < kOverflowIndex; ++c)
@@ -1009,16 +1153,49 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
   const int main_phases = p.substeps * n_ph;
   const int total_phases = main_phases + (n_rph > 0 ? p.restitution_iterations * n_rph : 0);
   auto phase_at = [&](int s) { return s < main_phases ? phases[s % n_ph] : rphases[(s - main_phases) % n_rph]; };
+  // Items of colour c: t < nj is joint t, t in [nj, total) constraint coff[c] + t - nj, in every
+  // stage (restitution skips the joints), so one thread owns a constraint in all its phases.
+  auto contact_range = [&](int ph, int& nj, int& total) {
+    const int c = ph & 31;
+    nj = jr.off[c + 1] - jr.off[c];
+    total = nj + (coff[c + 1] - coff[c]);
+  };
   const int stride = gridDim.x * blockDim.x;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  // Items go to threads 32 at a time, dealt across the blocks (chunk j to block j % gridDim.x):
+  // a colour with fewer items than the launch has threads occupies every SM with a few warps
+  // instead of filling the first blocks, and a phase's time follows the warps per SM.
+  const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
   int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
     const int sub = s / n_ph;
-    if (ph == kPhaseIntegrateVelocity) {
+    if (ph == kPhaseIntegrateVelocity || ph == kPhaseIntegrateVelocityWarm) {
       for (int i = g; i < w.n_awake; i += stride) {
         if (kTape) tp.body[((size_t)sub * 3) * w.n_awake + i] = w.states[i];
-        apply_iv(w, p, i, load_iv(w, i));
+        IVIn in = load_iv(w, i);
+        uint32_t m = ph == kPhaseIntegrateVelocityWarm ? w.bw_mask[i] : 0u;
+        if ((in.state_flags & kDynamicFlag) == 0u) m = 0u;
+        WarmSlots ws;
+        load_warm_slots(w, i, m, ws);  // in flight while the velocity is integrated
+        V3 v, wv;
+        integrate_velocity(p, in, v, wv);
+        warm_body(w, i, m, ws, v, wv);
+        DState& st = w.states[i];
+        st.v = v;
+        st.w = wv;
+      }
+    } else if (ph == kPhaseBodyWarm) {
+      for (int i = g; i < w.n_awake; i += stride) {
+        uint32_t m = w.bw_mask[i];
+        DState st = w.states[i];
+        if ((st.flags & kDynamicFlag) && m != 0u) {
+          V3 v = st.v, wv = st.w;
+          WarmSlots ws;
+          load_warm_slots(w, i, m, ws);
+          warm_body(w, i, m, ws, v, wv);
+          w.states[i].v = v;
+          w.states[i].w = wv;
+        }
       }
     } else if (ph == kPhaseIntegratePosition) {
       for (int i = g; i < w.n_awake; i += stride) {
@@ -1031,19 +1208,25 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, 
       run_overflow(w, p, jr, ph - kPhaseOverflow);
     } else {
       int stage = ph >> 5, c = ph & 31;
-      int nj = stage == kRestitution ? 0 : jr.off[c + 1] - jr.off[c];
-      int total = nj + (coff[c + 1] - coff[c]);
-      for (int t = g; t < total; t += stride) {
-        if (t < nj) {
-          DJoint& j = w.joints[w.joint_list[jr.off[c] + t]];
-          if (stage == kWarm) warm_start_joint(w, j);
-          else solve_joint(w, p, j, stage == kPush);
-        } else {
-          int k = coff[c] + (t - nj);
-          CData d;
-          load_direct(w.cp, k, stage, d);
-          if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
-          run_contact(w, p, k, stage, d);
+      int nj, total;
+      contact_range(ph, nj, total);
+      const int warm_color = stage == kRelax && s < main_phases && sub + 1 < p.substeps ? c : -1;
+      // The colour's contacts, then its joints: no two items of one colour share a dynamic
+      // body, so their order does not change any result. Each thread keeps its items of the
+      // colour (t = g, g + stride, ...).
+      for (int t = g >= nj ? g : g + ((nj - g + stride - 1) / stride) * stride; t < total; t += stride) {
+        int k = coff[c] + (t - nj);
+        CData d;
+        load_direct(w.cp, k, stage, d);
+        if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
+        run_contact(w, p, k, stage, d, warm_color);
+      }
+      for (int tj = g; stage != kRestitution && tj < nj; tj += stride) {
+        DJoint& j = w.joints[w.joint_list[jr.off[c] + tj]];
+        solve_joint(w, p, j, stage == kPush);
+        if (warm_color >= 0) {
+          DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+          put_warm_delta(w, j.index_a, j.index_b, c, joint_warm_delta(j, sa.dq, sb.dq));
         }
       }
     }
