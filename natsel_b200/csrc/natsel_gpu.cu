@@ -666,7 +666,7 @@ int enqueue_pair_update(ns_world* w) {
                                               d.bp_vals_in, d.bp_vals_out, nsh, 0, w->sort_bits, s));
   NS_CUDA(w, cudaMemsetAsync(d.cells, 0, sizeof(int2) * ((size_t)d.cell_mask + 1), s));
   k_bp_gather<<<blocks(d.n_small, 256), 256, 0, s>>>(d); ++nk;
-  k_bp_query<<<blocks(d.n_small, 128), 128, 0, s>>>(d); ++nk;
+  k_bp_query<<<blocks(d.n_small, kQueryThreads / 32), kQueryThreads, 0, s>>>(d); ++nk;
   k_bp_large<<<blocks(nsh, 256), 256, 0, s>>>(d); ++nk;
   NS_CUDA(w, cub::DeviceScan::ExclusiveSum(w->cub_scan_tmp, w->cub_scan_bytes, d.seg_count, d.seg_off, nsh, s));
   k_bp_scatter<<<4 * w->sm_count, 256, 0, s>>>(d); ++nk;

@@ -246,11 +246,15 @@ __device__ __forceinline__ void axis_cells(float lo, float hi, const DW& w, int*
 // proxy's lies in the grid cells around it. Each overlapping pair with at least one moved
 // proxy is reported once (by the smaller moved shape id when both moved); a proxy met again
 // through a hash collision is skipped by checking its own cell and sub-world (proxies of
-// different sub-worlds never pair).
-__global__ void k_bp_query(DW w) {
+// different sub-worlds never pair). One warp per proxy, lane l < 27 scanning cell
+// (x0 + l / 9, y0 + l / 3 % 3, z0 + l % 3) of the at most 3 x 3 x 3 around it; the pairs are
+// sorted per shape afterwards, so the order they are found in does not matter.
+constexpr int kQueryThreads = 128;
+__global__ void __launch_bounds__(kQueryThreads) k_bp_query(DW w) {
   if (w.ctl->moved_count == 0) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w.n_small) return;
+  const int i = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = (int)(threadIdx.x & 31u);
+  if (i >= w.n_small || lane >= 27) return;
   int mm = w.bp_meta[i];
   if (!(mm & kMetaMoved)) return;
   int m = mm & kMetaId;
@@ -262,27 +266,25 @@ __global__ void k_bp_query(DW w) {
   axis_cells(A.x, A.y, w, &x0, &x1);
   axis_cells(A.z, A.w, w, &y0, &y1);
   axis_cells(Az.x, Az.y, w, &z0, &z1);
-  for (int cx = x0; cx <= x1; ++cx)
-    for (int cy = y0; cy <= y1; ++cy)
-      for (int cz = z0; cz <= z1; ++cz) {
-        int2 r = w.cells[cell_hash(mw, cx, cy, cz) & (uint32_t)w.cell_mask];
-        for (int j = r.x; j < r.y; ++j) {
-          if (j == i) continue;
-          int bm = w.bp_meta[j];
-          int b = bm & kMetaId;
-          if ((bm & kMetaMoved) && b < m) continue;  // the smaller moved proxy of a pair reports it
-          if (m_static && (bm & kMetaStatic)) continue;
-          float4 B = w.bp_xy[j];
-          if (A.y < B.x || A.x > B.y) continue;  // aabb_overlaps (collision/aabb.rs:903), axis by axis
-          if (A.w < B.z || A.z > B.w) continue;
-          float2 Bz = w.bp_z[j];
-          if (Az.y < Bz.x || Az.x > Bz.y) continue;
-          if (grid_coord(B.x, w.inv_cell) != cx || grid_coord(B.z, w.inv_cell) != cy ||
-              grid_coord(Bz.x, w.inv_cell) != cz || w.bp_world[j] != mw)
-            continue;
-          emit_overlapping_pair(w, m, b);
-        }
-      }
+  const int cx = x0 + lane / 9, cy = y0 + (lane / 3) % 3, cz = z0 + lane % 3;
+  if (cx > x1 || cy > y1 || cz > z1) return;
+  int2 r = w.cells[cell_hash(mw, cx, cy, cz) & (uint32_t)w.cell_mask];
+  for (int j = r.x; j < r.y; ++j) {
+    if (j == i) continue;
+    int bm = w.bp_meta[j];
+    int b = bm & kMetaId;
+    if ((bm & kMetaMoved) && b < m) continue;  // the smaller moved proxy of a pair reports it
+    if (m_static && (bm & kMetaStatic)) continue;
+    float4 B = w.bp_xy[j];
+    if (A.y < B.x || A.x > B.y) continue;  // aabb_overlaps (collision/aabb.rs:903), axis by axis
+    if (A.w < B.z || A.z > B.w) continue;
+    float2 Bz = w.bp_z[j];
+    if (Az.y < Bz.x || Az.x > Bz.y) continue;
+    if (grid_coord(B.x, w.inv_cell) != cx || grid_coord(B.z, w.inv_cell) != cy ||
+        grid_coord(Bz.x, w.inv_cell) != cz || w.bp_world[j] != mw)
+      continue;
+    emit_overlapping_pair(w, m, b);
+  }
 }
 
 __global__ void k_bp_large(DW w) {
