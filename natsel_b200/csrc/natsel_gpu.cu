@@ -741,7 +741,7 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   // narrowphase (collide_pass.rs:164)
   NS_CUDA(w, cudaMemsetAsync(d.ctl->collide_count, 0, sizeof(d.ctl->collide_count), s));
   k_collide<<<std::min(blocks(d.cap, kCollideThreads), 16 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
-  k_collide_update<<<std::min(blocks(d.cap, kCollideThreads), 8 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
+  k_collide_update<<<std::min(blocks(d.cap, kCollideUpdateThreads), 32 * w->sm_count), kCollideUpdateThreads, 0, s>>>(d); ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
   if (d.n_worlds == 1) {

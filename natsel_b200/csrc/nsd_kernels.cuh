@@ -660,7 +660,10 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
 
 // Narrowphase, second pass: full updates, kind by kind, so a warp runs one shape
 // combination. Contacts are independent here: the order only changes which warp runs what.
-__global__ void __launch_bounds__(kCollideThreads) k_collide_update(DW w) {
+// Small blocks spread the updates over every SM: a thread keeps ~2 KB of clip polygons on its
+// stack, and fewer warps per SM keep more of it in L1.
+constexpr int kCollideUpdateThreads = 64;
+__global__ void __launch_bounds__(kCollideUpdateThreads) k_collide_update(DW w) {
   __shared__ int start[kPairKinds + 1];
   if (threadIdx.x == 0) {
     int acc = 0;
