@@ -231,7 +231,9 @@ int ns_world_autotune(ns_world* w, float dt, int substeps, int steps, int* block
 int ns_world_tape_begin(ns_world* w, int checkpoint_substeps);
 /* Stops recording; the tape stays for ns_world_vjp. */
 int ns_world_tape_end(ns_world* w);
-/* Releases the tape and its checkpoints. */
+/* Releases the tape and its checkpoints. The checkpoints' device memory (and the VJP's scratch)
+ * stays with the world for the next tape, so repeated rollouts allocate nothing after the first;
+ * ns_world_destroy frees it. */
 int ns_world_tape_free(ns_world* w);
 /* out[8]: recorded steps, checkpoints, narrowphase replays that did not reproduce the
  * recorded manifold (their pose derivatives are left out), VJP calls, recording (0/1),

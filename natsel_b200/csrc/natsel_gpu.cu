@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -72,6 +73,14 @@ struct ns_world {
   std::vector<void*> allocations;
   std::vector<size_t> allocation_bytes;
   struct AdTape* tape = nullptr;   // rollout record for the adjoint (ns_world_tape_begin)
+  // Device buffers kept for reuse by later tapes and VJPs and freed with the world: checkpoint
+  // buffers (with their copy tables, valid for the world's allocation set, which is fixed once
+  // uploaded), the VJP's step tapes and its cotangent buffers.
+  std::vector<char*> ckpt_pool;
+  char* tapes_buf = nullptr; size_t tapes_cap = 0;
+  char* adj_buf = nullptr; size_t adj_cap = 0;
+  // Snapshot layout of the allocations (device table, written once) and its total size.
+  SnapOp* snap_ops = nullptr; size_t snap_bytes = 0;
   void* cub_sort_tmp = nullptr;
   size_t cub_sort_bytes = 0;
   void* cub_scan_tmp = nullptr;
@@ -861,9 +870,7 @@ int read_control(ns_world* w, Control* c) {
 // put back in its final state afterwards.
 struct AdStepRec { float dt; int substeps; };
 struct AdCheckpoint {
-  char* data = nullptr;      // snapshot bytes followed by the two copy tables
-  CopyOp* save = nullptr;
-  CopyOp* load = nullptr;
+  char* data = nullptr;      // snapshot of every allocation (layout in ns_world::snap_ops)
 };
 struct AdTape {
   int every = 8;
@@ -881,42 +888,103 @@ namespace {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Device scratch for checkpoints and the VJP comes from one stream-ordered memory pool per
+// device, shared by all worlds of the process: memory a destroyed world gave back is reused by
+// the next without a cudaMalloc, and up to kPoolKeep bytes stay reserved between uses.
+constexpr uint64_t kPoolKeep = 16ull << 30;
+cudaMemPool_t scratch_pool(int device) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) { cudaGetLastError(); pool = nullptr; }
+  if (pool) {
+    uint64_t keep = kPoolKeep;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  pools[device] = pool;
+  return pool;
+}
+
+int scratch_alloc(ns_world* w, char** p, size_t bytes) {
+  cudaMemPool_t pool = scratch_pool(w->def.device);
+  if (!pool) return fail(w, NS_ERR_CUDA, "no memory pool on device %d", w->def.device);
+  NS_CUDA(w, cudaMallocFromPoolAsync((void**)p, bytes, pool, w->stream));
+  return NS_OK;
+}
+
+void scratch_free(ns_world* w, char* p) {
+  if (p) cudaFreeAsync(p, w->stream);
+}
+
 int take_checkpoint(ns_world* w, AdCheckpoint* ck) {
   if (w->allocation_bytes.size() != w->allocations.size())
     return fail(w, NS_ERR_INVALID, "device allocation table is inconsistent");
-  size_t n = w->allocations.size(), bytes = 0;
-  std::vector<size_t> off(n);
-  for (size_t i = 0; i < n; ++i) { off[i] = bytes; bytes += align256(w->allocation_bytes[i]); }
-  size_t table = align256(n * sizeof(CopyOp));
-  if (!ck->data) {
-    NS_CUDA(w, cudaMalloc(&ck->data, bytes + 2 * table));
-    std::vector<CopyOp> save(n), load(n);
+  const size_t n = w->allocations.size();
+  if (!w->snap_ops) {
+    std::vector<SnapOp> ops(n);
+    size_t bytes = 0;
     for (size_t i = 0; i < n; ++i) {
-      save[i] = {(const char*)w->allocations[i], ck->data + off[i], w->allocation_bytes[i]};
-      load[i] = {ck->data + off[i], (char*)w->allocations[i], w->allocation_bytes[i]};
+      ops[i] = {(char*)w->allocations[i], bytes, w->allocation_bytes[i]};
+      bytes += align256(w->allocation_bytes[i]);
     }
-    ck->save = (CopyOp*)(ck->data + bytes);
-    ck->load = (CopyOp*)(ck->data + bytes + table);
-    NS_CUDA(w, cudaMemcpy(ck->save, save.data(), n * sizeof(CopyOp), cudaMemcpyHostToDevice));
-    NS_CUDA(w, cudaMemcpy(ck->load, load.data(), n * sizeof(CopyOp), cudaMemcpyHostToDevice));
+    char* table = nullptr;
+    int st = scratch_alloc(w, &table, std::max<size_t>(n, 1) * sizeof(SnapOp));
+    if (st) return st;
+    w->snap_ops = (SnapOp*)table;
+    w->snap_bytes = bytes;
+    NS_CUDA(w, cudaMemcpyAsync(w->snap_ops, ops.data(), n * sizeof(SnapOp), cudaMemcpyHostToDevice, w->stream));
+    NS_CUDA(w, cudaStreamSynchronize(w->stream));
   }
-  k_multi_copy<<<4 * w->sm_count, 256, 0, w->stream>>>(ck->save, (int)n);
+  if (!ck->data && !w->ckpt_pool.empty()) {
+    ck->data = w->ckpt_pool.back();
+    w->ckpt_pool.pop_back();
+  }
+  if (!ck->data) {
+    int st = scratch_alloc(w, &ck->data, w->snap_bytes);
+    if (st) return st;
+  }
+  k_snapshot<<<4 * w->sm_count, 256, 0, w->stream>>>(w->snap_ops, (int)n, ck->data, 1);
   NS_CUDA(w, cudaGetLastError());
   return NS_OK;
 }
 
 int restore_checkpoint(ns_world* w, const AdCheckpoint& ck) {
-  k_multi_copy<<<4 * w->sm_count, 256, 0, w->stream>>>(ck.load, (int)w->allocations.size());
+  k_snapshot<<<4 * w->sm_count, 256, 0, w->stream>>>(w->snap_ops, (int)w->allocations.size(), ck.data, 0);
   NS_CUDA(w, cudaGetLastError());
   return NS_OK;
+}
+
+// A checkpoint buffer goes back to the world's pool (the stream must be past its last use).
+void release_checkpoint(ns_world* w, AdCheckpoint* ck) {
+  if (ck->data) w->ckpt_pool.push_back(ck->data);
+  ck->data = nullptr;
 }
 
 void free_tape(ns_world* w) {
   if (!w->tape) return;
   cudaStreamSynchronize(w->stream);
-  for (AdCheckpoint& c : w->tape->ckpt) cudaFree(c.data);
+  for (AdCheckpoint& c : w->tape->ckpt) release_checkpoint(w, &c);
   delete w->tape;
   w->tape = nullptr;
+}
+
+// Device scratch of at least `bytes`, kept in *buf / *cap for later calls.
+int reuse_buffer(ns_world* w, char** buf, size_t* cap, size_t bytes) {
+  if (*cap >= bytes && *buf) return NS_OK;
+  scratch_free(w, *buf);
+  *buf = nullptr;
+  *cap = 0;
+  int st = scratch_alloc(w, buf, bytes);
+  if (st) return st;
+  *cap = bytes;
+  return NS_OK;
 }
 
 int tape_after_step(ns_world* w, float dt, int substeps) {
@@ -971,7 +1039,9 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
   size_t o_push = take(sizeof(float4) * 4 * cap * max_substeps);
   size_t o_relax = take(sizeof(float4) * 5 * cap * max_substeps);
   size_t o_fin = take(sizeof(float4) * cap), o_mode = take(cap), o_ops = take(sizeof(CopyOp) * 20);
-  NS_CUDA(w, cudaMalloc(&ts->data, per * (size_t)count));
+  int st = reuse_buffer(w, &w->tapes_buf, &w->tapes_cap, per * (size_t)count);
+  if (st) return st;
+  ts->data = w->tapes_buf;
   ts->bytes = per * (size_t)count;
   ts->steps.resize(count);
   for (int j = 0; j < count; ++j) {
@@ -1428,6 +1498,11 @@ void ns_world_destroy(ns_world* w) {
     if (w->graph_exec) cudaGraphExecDestroy(w->graph_exec);
     if (w->graph) cudaGraphDestroy(w->graph);
     free_tape(w);
+    for (char* p : w->ckpt_pool) scratch_free(w, p);
+    scratch_free(w, w->tapes_buf);
+    scratch_free(w, w->adj_buf);
+    scratch_free(w, (char*)w->snap_ops);
+    cudaStreamSynchronize(w->stream);
     for (void* p : w->allocations) cudaFree(p);
     if (w->host_ctl) cudaFreeHost(w->host_ctl);
     if (w->host_in) cudaFreeHost(w->host_in);
@@ -2066,7 +2141,7 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
   if (snap.data) {
     int st2 = restore_checkpoint(w, snap);
     cudaStreamSynchronize(w->stream);
-    cudaFree(snap.data);
+    release_checkpoint(w, &snap);
     if (!st) st = st2;
   }
   if (e0) cudaEventDestroy(e0);
@@ -2228,7 +2303,8 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     size_t o_mb = take(sizeof(float) * kMB * (size_t)cap), o_mis = take(sizeof(int));
     size_t o_yrec = take(sizeof(float) * 3 * ad::kRelaxOut * (size_t)cap * max_sub);
     size_t o_seed = take(sizeof(float) * 13 * (size_t)nb), o_out = take(sizeof(float) * 16 * (size_t)nb);
-    if (cudaMalloc(&buf, o) != cudaSuccess) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
+    if (reuse_buffer(w, &w->adj_buf, &w->adj_cap, o) != NS_OK) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
+    buf = w->adj_buf;
     NS_CUDA(w, cudaMemsetAsync(buf, 0, o, w->stream));
     AdjBufs a;
     a.bb = (float*)(buf + o_bb); a.cq = (float*)(buf + o_cq); a.pb = (float*)(buf + o_pb);
@@ -2317,9 +2393,7 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     if (final_state.data) { restore_checkpoint(w, final_state); cudaStreamSynchronize(w->stream); }
   }
   cudaStreamSynchronize(w->stream);
-  if (final_state.data) cudaFree(final_state.data);
-  if (ts.data) cudaFree(ts.data);
-  if (buf) cudaFree(buf);
+  release_checkpoint(w, &final_state);
   if (st) return st;
   if (!f64) {
     for (size_t i = 0; i < out.size(); ++i) out[i] = host_out[i];

@@ -334,7 +334,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
   if (threadIdx.x == 24) coff[24] = t.ctl->color_offset[23];
   __syncthreads();
   const int n = a.n_awake;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  // items dealt 32 at a time across the blocks, as in the forward solver
+  const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
   const int stride = gridDim.x * blockDim.x;
   int bar = 0;
   auto contacts = [&](auto stage_tag, int sub) -> bool {
@@ -351,7 +352,11 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
     for (int i = g; i < n; i += stride) adj_ip(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
     if (!contacts(std::integral_constant<int, kPush>(), sub)) return;
-    if (!contacts(std::integral_constant<int, kWarm>(), sub)) return;
+    // Warm start changes a body's velocity by a constant (v - x), so its reverse leaves the body
+    // cotangents as they are and only reads them: every colour's warm start reverses in one
+    // phase, before integrate-velocities changes those cotangents.
+    for (int k = g; k < coff[kOverflowIndex]; k += stride) adj_contact<kWarm>(t, a, p, n, k, sub);
+    if (!phase_sync<kGrid>(ctl, bar)) return;
     for (int i = g; i < n; i += stride) adj_iv(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
   }
@@ -668,6 +673,21 @@ __global__ void k_multi_copy(const CopyOp* ops, int n_ops) {
     float4* d = (float4*)op.dst;
     for (size_t i = tid; i < n16; i += stride) d[i] = s[i];
     for (size_t i = n16 * 16 + tid; i < op.bytes; i += stride) op.dst[i] = op.src[i];
+  }
+}
+
+// Snapshot of a world's device allocations into one buffer: allocation i lives at base + off.
+// save copies the allocations into the buffer, otherwise the buffer back into them.
+struct SnapOp { char* dev; size_t off; size_t bytes; };
+__global__ void k_snapshot(const SnapOp* ops, int n_ops, char* base, int save) {
+  size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  for (int o = 0; o < n_ops; ++o) {
+    SnapOp op = ops[o];
+    const char* src = save ? op.dev : base + op.off;
+    char* dst = save ? base + op.off : op.dev;
+    size_t n16 = op.bytes / 16;
+    for (size_t i = tid; i < n16; i += stride) ((float4*)dst)[i] = ((const float4*)src)[i];
+    for (size_t i = n16 * 16 + tid; i < op.bytes; i += stride) dst[i] = src[i];
   }
 }
 
