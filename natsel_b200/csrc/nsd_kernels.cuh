@@ -10,6 +10,25 @@
 namespace nsd {
 
 constexpr int kStatePassThreads = 1024;
+
+// Warp-aggregated counters. A counter that every element of a large pass bumps serialises one
+// atomic per element at its L2 slice; here the threads that reach the call together (the
+// active mask) add their total with one atomic. add_converged adds 1 per thread;
+// slot_converged hands each thread a distinct slot of counters[key] (slots within a group in
+// lane order, groups in atomic order: for lists whose order does not matter).
+__device__ __forceinline__ void add_converged(int* counter) {
+  const unsigned am = __activemask();
+  if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(counter, __popc(am));
+}
+__device__ __forceinline__ int slot_converged(int* counters, int key) {
+  const unsigned am = __activemask();
+  const unsigned peers = __match_any_sync(am, key);
+  const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&counters[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
 constexpr int kColorBlock = 1024;
 constexpr int kSolveThreads = 256;   // per CTA of the solver cluster
 constexpr int kMaxSolveCluster = 16;
@@ -608,7 +627,7 @@ __device__ bool collide_recycle(const DW& w, int cid) {
           }
         }
         recycled = true;
-        atomicAdd(&w.ctl->recycled, 1);
+        add_converged(&w.ctl->recycled);
         if (w.np_mode) w.np_mode[cid] = 1;
       }
     }
@@ -652,7 +671,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
     if (!w.contacts[cid].alive) continue;
     if (collide_recycle(w, cid)) {
       int kind = w.contacts[cid].kind;
-      int slot = atomicAdd(&w.ctl->collide_count[kind], 1);
+      int slot = slot_converged(w.ctl->collide_count, kind);
       w.collide_list[(size_t)kind * w.cap + slot] = cid;
     }
   }
@@ -979,21 +998,59 @@ __global__ void __launch_bounds__(kColorBlock) k_color_count(DW w) {
   }
 }
 
-__global__ void k_color_scan(DW w) {
-  int k = threadIdx.x;
+// Exclusive prefix over the partition blocks of each colour's counts, and the colour offsets.
+// One block: thread t owns a run of consecutive partition blocks, sums it per colour, the runs'
+// sums are scanned across the block (warp shuffles, then the warps' totals), and each thread
+// writes its run's prefixes.
+constexpr int kColorScanThreads = 1024;
+__global__ void __launch_bounds__(kColorScanThreads) k_color_scan(DW w) {
+  __shared__ int warp_sum[kColorScanThreads / 32];
   __shared__ int totals[24];
-  if (k < kOverflowIndex) {
-    int run = 0;
-    for (int b = 0; b < w.n_color_blocks; ++b) {
-      int v = w.block_color[b * 24 + k];
-      w.block_color[b * 24 + k] = run;
-      run += v;
-    }
-    totals[k] = run;
-    w.ctl->color_count[k] = run;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int nb = w.n_color_blocks;
+  const int per = (nb + kColorScanThreads - 1) / kColorScanThreads;
+  const int b0 = min(nb, t * per), b1 = min(nb, b0 + per);
+  int own[kOverflowIndex];
+#pragma unroll
+  for (int k = 0; k < kOverflowIndex; ++k) own[k] = 0;
+  for (int b = b0; b < b1; ++b) {
+#pragma unroll
+    for (int k = 0; k < kOverflowIndex; ++k) own[k] += w.block_color[b * 24 + k];
   }
-  __syncthreads();
-  if (k == 0) {
+#pragma unroll
+  for (int k = 0; k < kOverflowIndex; ++k) {
+    int v = own[k], x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int s = warp_sum[lane], z = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      warp_sum[lane] = z - s;  // exclusive prefix of the warps
+      if (lane == 31) totals[k] = z;
+    }
+    __syncthreads();
+    own[k] = warp_sum[warp] + x - v;  // exclusive prefix of this thread's run
+    __syncthreads();
+  }
+  for (int b = b0; b < b1; ++b) {
+#pragma unroll
+    for (int k = 0; k < kOverflowIndex; ++k) {
+      int v = w.block_color[b * 24 + k];
+      w.block_color[b * 24 + k] = own[k];
+      own[k] += v;
+    }
+  }
+  if (t < kOverflowIndex) w.ctl->color_count[t] = totals[t];
+  if (t == 0) {
     int run = 0;
     for (int c = 0; c < kOverflowIndex; ++c) { w.ctl->color_offset[c] = run; run += totals[c]; }
     w.ctl->color_offset[kOverflowIndex] = run;

@@ -1271,7 +1271,7 @@ __global__ void k_finalize(DW w, StepParams p) {
   float max_motion = maxf(maxdp, maxv * dt);
   if (p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
     sim.flags |= kIsFast;
-    atomicAdd(&w.ctl->fast_flags, 1);
+    add_converged(&w.ctl->fast_flags);
   }
   M3 R = matrix_from_quat(sim.q);
   sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
@@ -1302,7 +1302,7 @@ __global__ void k_finalize(DW w, StepParams p) {
       if (!aabb_contains(w.fat[sid], a)) {
         w.fat[sid] = aabb_inflate(a, sh.aabb_margin);
         w.moved[sid] = 1;
-        atomicAdd(&w.ctl->moved_count, 1);
+        add_converged(&w.ctl->moved_count);
       }
     }
   }
