@@ -374,7 +374,8 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_solve<false, false>,
                            (const void*)k_solve<true, true>,
                            (const void*)k_solve<false, true>,
-                           (const void*)k_prepare_overflow, (const void*)k_color_scatter_prepare, (const void*)k_warm_slots,
+                           (const void*)k_prepare_overflow, (const void*)k_color_scatter, (const void*)k_prepare_slots,
+                           (const void*)k_warm_slots,
                            (const void*)k_finalize, (const void*)k_state_pass,
                            (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
                            (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
@@ -527,7 +528,7 @@ int upload_world(ns_world* w) {
   ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
   ALLOC(long_segment, int, kLongSegmentCap);
   ALLOC(ctl, Control, 1);
-  ALLOC(bwd, float4, 48 * (size_t)na); ALLOC(bw_mask, uint32_t, na);
+  ALLOC(bwd, float4, 48 * (size_t)na); ALLOC(bw_mask, uint32_t, na); ALLOC(slot_cid, int, cap);
   CPlanes& P = d.cp;
   P.cap = cap;
 #define PALLOC(field, T, n) do { P.field = dalloc<T>(w, (n), &st); if (!P.field) return st; } while (0)
@@ -765,7 +766,8 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
     NS_CUDA(w, cudaMemcpyAsync(tape->dev.post, d.contacts, sizeof(DContact) * (size_t)d.cap, cudaMemcpyDeviceToDevice, s));
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
   k_color_scan<<<1, kColorScanThreads, 0, s>>>(d); ++nk;
-  k_color_scatter_prepare<<<d.n_color_blocks, kColorBlock, 0, s>>>(d, p); ++nk;
+  k_color_scatter<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
+  k_prepare_slots<<<std::min(blocks(d.cap, kPrepareThreads), 16 * w->sm_count), kPrepareThreads, 0, s>>>(d, p); ++nk;
   k_prepare_overflow<<<std::min(std::max(d.n_worlds, 8), 4096), 128, 0, s>>>(d, p); ++nk;
   if (d.n_joints > 0) {
     k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);

@@ -85,6 +85,7 @@ struct DW {
   // 2 * (24 * body + c) + {0, 1}, signed for the body's side; bit c of bw_mask[body] marks the
   // slot as used this step.
   float4* bwd; uint32_t* bw_mask;
+  int* slot_cid;  // contact id of each coloured constraint slot (this step)
   int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
 };
 
@@ -1162,7 +1163,9 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
   P.rm[slot] = make_float4(rm.yy, rm.yz, rm.zz, 0.0f);
 }
 
-__global__ void __launch_bounds__(kColorBlock) k_color_scatter_prepare(DW w, StepParams p) {
+// Slot of every coloured contact (its colour's offset, the partition block's prefix, its rank in
+// the block); the constraint is prepared by k_prepare_slots in slot order.
+__global__ void __launch_bounds__(kColorBlock) k_color_scatter(DW w) {
   __shared__ int wc[kColorBlock / 32][24];
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
   int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
@@ -1179,7 +1182,16 @@ __global__ void __launch_bounds__(kColorBlock) k_color_scatter_prepare(DW w, Ste
   for (int q = 0; q < warp; ++q) before += wc[q][col];
   int rank = __popc(my_mask & ((1u << lane) - 1u));
   int slot = w.ctl->color_offset[col] + w.block_color[blockIdx.x * 24 + col] + before + rank;
-  prepare_constraint(w, p, cid, slot);
+  w.slot_cid[slot] = cid;
+}
+
+// solver_prepare.rs:269 prepare per constraint slot (small blocks: the arithmetic keeps its
+// registers instead of the 64 a 1024-thread block allows, and the planes are written in order).
+constexpr int kPrepareThreads = 128;
+__global__ void __launch_bounds__(kPrepareThreads) k_prepare_slots(DW w, StepParams p) {
+  const int n = w.ctl->color_offset[kOverflowIndex];
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x)
+    prepare_constraint(w, p, w.slot_cid[slot], slot);
 }
 
 // overflow_contact_solver.rs:92 prepare_overflow_contacts
