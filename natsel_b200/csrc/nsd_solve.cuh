@@ -1112,9 +1112,11 @@ __device__ __forceinline__ void tape_contact(const DW& w, const SolveTape& tp, i
 }
 
 // Persistent solver. kGrid: one cooperative launch over the whole GPU, phases separated by
-// grid_sync_acq_rel; otherwise one thread-block cluster separated by barrier.cluster.
+// grid_sync_acq_rel, compiled for two blocks per SM (128 registers; the batch's colours hold
+// more items than one block per SM has threads); otherwise one thread-block cluster separated
+// by barrier.cluster.
 template <bool kGrid, bool kTape>
-__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(DW w, StepParams p, JointRanges jr, SolveTape tp) {
+__global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, StepParams p, JointRanges jr, SolveTape tp) {
   __shared__ int coff[25];
   __shared__ int phases[3 * 25 + 2];  // one substep
   __shared__ int rphases[25];         // one restitution iteration
