@@ -213,10 +213,8 @@ struct CData {
   float prest[4];
 };
 
-// Every field is written (zero where the stage reads nothing), so a CData held across the
-// solver's phase loop carries no value from an earlier constraint. The four point slots are
-// read whatever the point count (the planes hold 4 x cap entries) and the unused ones zeroed
-// afterwards, so no load waits for the index load: one L2 round trip brings the constraint.
+// Every field is written (zero where the stage reads nothing). Only the manifold's points are
+// read: the cluster's 16 SMs move every phase's constraints from L2, so bytes count.
 __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d) {
   const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   d.c = unpack_constraint(__ldg(&P.idx[k]), __ldg(&P.mass[k]), __ldg(&P.ia0[k]), __ldg(&P.ia1[k]),
@@ -229,14 +227,13 @@ __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, 
   if (stage == kRelax) { d.rm = __ldg(&P.rm[k]); d.tm = __ldg(&P.tm[k]); }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    d.pra[q] = __ldg(&P.pra[q * P.cap + k]);
-    d.prb[q] = __ldg(&P.prb[q * P.cap + k]);
-    d.pimp[q] = P.pimp[q * P.cap + k];
-    d.prest[q] = stage == kRestitution ? P.prest[q * P.cap + k] : 0.0f;
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    if (q >= d.c.pc) { d.pra[q] = z; d.prb[q] = z; d.pimp[q] = z; d.prest[q] = 0.0f; }
+    d.pra[q] = z; d.prb[q] = z; d.pimp[q] = z; d.prest[q] = 0.0f;
+    if (q < d.c.pc) {
+      d.pra[q] = __ldg(&P.pra[q * P.cap + k]);
+      d.prb[q] = __ldg(&P.prb[q * P.cap + k]);
+      d.pimp[q] = P.pimp[q * P.cap + k];
+      if (stage == kRestitution) d.prest[q] = P.prest[q * P.cap + k];
+    }
   }
 }
 
