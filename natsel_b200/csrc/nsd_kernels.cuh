@@ -574,33 +574,54 @@ __device__ bool update_contact(const DW& w, DContact& c, V3 lca, WXf xa, V3 lcb,
 // needs a full manifold update (collide_full).
 __device__ bool collide_recycle(const DW& w, int cid) {
   DContact& c = w.contacts[cid];
-  if (!aabb_overlaps(w.fat[c.shape_a], w.fat[c.shape_b])) {
-    c.flags = (c.flags | cSimDisjoint) & ~cSimTouching;
+  // Every read is issued before the first write, in two dependent rounds (the contact, then
+  // its shapes' fat AABBs and its bodies' poses): the contact and body records are far apart in
+  // memory and mostly come from DRAM, so one round trip per field would dominate the pass.
+  const int shape_a = c.shape_a, shape_b = c.shape_b, enc_a = c.enc_a, enc_b = c.enc_b;
+  const uint32_t flags = c.flags;
+  const int manifold_count = c.manifold_count;
+  const Q cached_rot_a = c.cached_rot_a, cached_rot_b = c.cached_rot_b;
+  const Xf xc = c.cached_rel;
+  const int point_count = c.manifold.point_count;
+  const V3 n = c.manifold.normal;
+  V3 anchor_a[4], anchor_b[4];
+  float base_sep[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    anchor_a[i] = c.manifold.points[i].anchor_a;
+    anchor_b[i] = c.manifold.points[i].anchor_b;
+    base_sep[i] = c.manifold.points[i].base_separation;
+  }
+  const AABB fat_a = w.fat[shape_a], fat_b = w.fat[shape_b];
+  const DSim& sa = sim_of(w, enc_a);
+  const DSim& sb = sim_of(w, enc_b);
+  WXf xa, xb;
+  xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
+  xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
+  const uint32_t flags_a = sa.flags, flags_b = sb.flags;
+  const V3 max_extent_a = sa.max_extent, max_extent_b = sb.max_extent;
+  const Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+  if (!aabb_overlaps(fat_a, fat_b)) {
+    c.flags = (flags | cSimDisjoint) & ~cSimTouching;
     atomicOr(&w.changed_bits[cid >> 5], 1u << (cid & 31));
     if (w.np_mode) w.np_mode[cid] = 0;
     return false;
   }
-  const DSim& sa = sim_of(w, c.enc_a);
-  const DSim& sb = sim_of(w, c.enc_b);
-  bool was_touching = (c.flags & cSimTouching) != 0;
-  WXf xa, xb;
-  xa.p.x = sa.px; xa.p.y = sa.py; xa.p.z = sa.pz; xa.q = sa.q;
-  xb.p.x = sb.px; xb.p.y = sb.py; xb.p.z = sb.pz; xb.q = sb.q;
-  bool is_fast = ((sa.flags | sb.flags) & kIsFast) != 0;
+  bool was_touching = (flags & cSimTouching) != 0;
+  bool is_fast = ((flags_a | flags_b) & kIsFast) != 0;
   float recycle = contact_recycle_distance();
   float spec = speculative_distance();
   float recycle_nt = minf(recycle, spec);
   float tol = was_touching ? recycle : recycle_nt;
   bool recycled = false;
-  if (!is_fast && recycle > 0.0f && (c.flags & cRelativeValid) && (c.flags & cRecycle)) {
+  if (!is_fast && recycle > 0.0f && (flags & cRelativeValid) && (flags & cRecycle)) {
     // collide_pass.rs:606-687 contact recycling
-    float ang_a = dot_quat(xa.q, c.cached_rot_a);
-    float ang_b = dot_quat(xb.q, c.cached_rot_b);
+    float ang_a = dot_quat(xa.q, cached_rot_a);
+    float ang_b = dot_quat(xb.q, cached_rot_b);
     float ang = minf(ang_a * ang_a, ang_b * ang_b);
     Xf x = inv_mul_wxf(xa, xb);
-    Xf xc = c.cached_rel;
-    V3 mea = c.enc_a < -1 ? v3(0, 0, 0) : sa.max_extent;
-    V3 meb = c.enc_b < -1 ? v3(0, 0, 0) : sb.max_extent;
+    V3 mea = enc_a < -1 ? v3(0, 0, 0) : max_extent_a;
+    V3 meb = enc_b < -1 ? v3(0, 0, 0) : max_extent_b;
     V3 me = max3(mea, meb);
     float dsq = distance_sq(x.p, xc.p);
     if (ang > kRecycleAngular && dsq < tol * tol) {
@@ -610,21 +631,22 @@ __device__ bool collide_recycle(const DW& w, int cid) {
       V3 arc = modified_cross(abs3(qr.v), me);
       float arc_sq = 4.0f * length_sq(arc);
       if (arc_sq < slack * slack) {
-        Q dqa = mul_quat(xa.q, conjugate(c.cached_rot_a));
-        Q dqb = mul_quat(xb.q, conjugate(c.cached_rot_b));
+        Q dqa = mul_quat(xa.q, conjugate(cached_rot_a));
+        Q dqb = mul_quat(xb.q, conjugate(cached_rot_b));
         M3 ma = matrix_from_quat(dqa), mb = matrix_from_quat(dqb);
-        Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
         V3 dc = sub_pos(cb, ca);
-        if (c.manifold_count > 0) {
+        if (manifold_count > 0) {
           Manifold& m = c.manifold;
-          V3 n = m.normal;
-          for (int i = 0; i < m.point_count; ++i) {
-            V3 ra = mul_mv(ma, m.points[i].anchor_a);
-            V3 rb = mul_mv(mb, m.points[i].anchor_b);
-            V3 dp = dc + (rb - ra);
-            m.points[i].separation = m.points[i].base_separation + dot(dp, n);
-            m.points[i].normal_velocity = 0.0f;
-            m.points[i].persisted = 1;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (i < point_count) {
+              V3 ra = mul_mv(ma, anchor_a[i]);
+              V3 rb = mul_mv(mb, anchor_b[i]);
+              V3 dp = dc + (rb - ra);
+              m.points[i].separation = base_sep[i] + dot(dp, n);
+              m.points[i].normal_velocity = 0.0f;
+              m.points[i].persisted = 1;
+            }
           }
         }
         recycled = true;
