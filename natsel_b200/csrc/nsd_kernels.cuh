@@ -86,6 +86,7 @@ struct DW {
   // slot as used this step.
   float4* bwd; uint32_t* bw_mask;
   int* slot_cid;  // contact id of each coloured constraint slot (this step)
+  int8_t* slot_color;  // colour of each contact slot for the partition (-1: not coloured)
   int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
 };
 
@@ -1008,6 +1009,7 @@ __global__ void __launch_bounds__(kColorBlock) k_color_count(DW w) {
   __shared__ int wc[kColorBlock / 32][24];
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
   int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
+  if (cid < w.cap) w.slot_color[cid] = (int8_t)col;  // read by k_color_scatter
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = 0; k < kOverflowIndex; ++k) {
     unsigned m = __ballot_sync(0xffffffffu, col == k);
@@ -1190,7 +1192,7 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
 __global__ void __launch_bounds__(kColorBlock) k_color_scatter(DW w) {
   __shared__ int wc[kColorBlock / 32][24];
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
-  int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
+  int col = cid < w.cap ? (int)w.slot_color[cid] : -1;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned my_mask = 0;
   for (int k = 0; k < kOverflowIndex; ++k) {
