@@ -765,7 +765,7 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   if (tape)
     NS_CUDA(w, cudaMemcpyAsync(tape->dev.post, d.contacts, sizeof(DContact) * (size_t)d.cap, cudaMemcpyDeviceToDevice, s));
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
-  k_color_scan<<<1, kColorScanThreads, 0, s>>>(d); ++nk;
+  k_color_scan<<<kOverflowIndex, kColorScanThreads, 0, s>>>(d); ++nk;
   k_color_scatter<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
   k_prepare_slots<<<std::min(blocks(d.cap, kPrepareThreads), 16 * w->sm_count), kPrepareThreads, 0, s>>>(d, p); ++nk;
   k_prepare_overflow<<<std::min(std::max(d.n_worlds, 8), 4096), 128, 0, s>>>(d, p); ++nk;

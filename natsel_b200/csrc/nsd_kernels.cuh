@@ -1023,65 +1023,44 @@ __global__ void __launch_bounds__(kColorBlock) k_color_count(DW w) {
   }
 }
 
-// Exclusive prefix over the partition blocks of each colour's counts, and the colour offsets.
-// One block: thread t owns a run of consecutive partition blocks, sums it per colour, the runs'
-// sums are scanned across the block (warp shuffles, then the warps' totals), and each thread
-// writes its run's prefixes.
+// Exclusive prefix over the partition blocks of each colour's counts: block c scans colour c's
+// column. Thread t owns a run of consecutive partition blocks; the runs' sums are scanned
+// across the block (warp shuffles, then the warps' totals) and each thread writes its run's
+// prefixes. The colour offsets follow from the totals (k_color_scatter).
 constexpr int kColorScanThreads = 1024;
 __global__ void __launch_bounds__(kColorScanThreads) k_color_scan(DW w) {
   __shared__ int warp_sum[kColorScanThreads / 32];
-  __shared__ int totals[24];
+  const int k = blockIdx.x;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int nb = w.n_color_blocks;
   const int per = (nb + kColorScanThreads - 1) / kColorScanThreads;
   const int b0 = min(nb, t * per), b1 = min(nb, b0 + per);
-  int own[kOverflowIndex];
+  int own = 0;
+  for (int b = b0; b < b1; ++b) own += w.block_color[b * 24 + k];
+  int x = own;
 #pragma unroll
-  for (int k = 0; k < kOverflowIndex; ++k) own[k] = 0;
-  for (int b = b0; b < b1; ++b) {
-#pragma unroll
-    for (int k = 0; k < kOverflowIndex; ++k) own[k] += w.block_color[b * 24 + k];
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
-#pragma unroll
-  for (int k = 0; k < kOverflowIndex; ++k) {
-    int v = own[k], x = v;
+  if (lane == 31) warp_sum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int s0 = warp_sum[lane], z = s0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      int y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= o) z += y;
     }
-    if (lane == 31) warp_sum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      int s = warp_sum[lane], z = s;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, z, o);
-        if (lane >= o) z += y;
-      }
-      warp_sum[lane] = z - s;  // exclusive prefix of the warps
-      if (lane == 31) totals[k] = z;
-    }
-    __syncthreads();
-    own[k] = warp_sum[warp] + x - v;  // exclusive prefix of this thread's run
-    __syncthreads();
+    warp_sum[lane] = z - s0;  // exclusive prefix of the warps
+    if (lane == 31) w.ctl->color_count[k] = z;
   }
+  __syncthreads();
+  int run = warp_sum[warp] + x - own;  // exclusive prefix of this thread's run
   for (int b = b0; b < b1; ++b) {
-#pragma unroll
-    for (int k = 0; k < kOverflowIndex; ++k) {
-      int v = w.block_color[b * 24 + k];
-      w.block_color[b * 24 + k] = own[k];
-      own[k] += v;
-    }
-  }
-  if (t < kOverflowIndex) w.ctl->color_count[t] = totals[t];
-  if (t == 0) {
-    int run = 0;
-    for (int c = 0; c < kOverflowIndex; ++c) { w.ctl->color_offset[c] = run; run += totals[c]; }
-    w.ctl->color_offset[kOverflowIndex] = run;
-    w.ctl->color_offset[24] = run;
-    w.ctl->color_count[kOverflowIndex] = w.ctl->overflow_count;
-    w.ctl->any_restitution = 0;
+    int v = w.block_color[b * 24 + k];
+    w.block_color[b * 24 + k] = run;
+    run += v;
   }
 }
 
@@ -1191,6 +1170,18 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
 // the block); the constraint is prepared by k_prepare_slots in slot order.
 __global__ void __launch_bounds__(kColorBlock) k_color_scatter(DW w) {
   __shared__ int wc[kColorBlock / 32][24];
+  __shared__ int offset_s[kOverflowIndex + 1];
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int c = 0; c < kOverflowIndex; ++c) { offset_s[c] = run; run += w.ctl->color_count[c]; }
+    offset_s[kOverflowIndex] = run;
+    if (blockIdx.x == 0) {
+      for (int c = 0; c <= kOverflowIndex; ++c) w.ctl->color_offset[c] = offset_s[c];
+      w.ctl->color_offset[24] = run;
+      w.ctl->color_count[kOverflowIndex] = w.ctl->overflow_count;
+      w.ctl->any_restitution = 0;
+    }
+  }
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
   int col = cid < w.cap ? (int)w.slot_color[cid] : -1;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1205,7 +1196,7 @@ __global__ void __launch_bounds__(kColorBlock) k_color_scatter(DW w) {
   int before = 0;
   for (int q = 0; q < warp; ++q) before += wc[q][col];
   int rank = __popc(my_mask & ((1u << lane) - 1u));
-  int slot = w.ctl->color_offset[col] + w.block_color[blockIdx.x * 24 + col] + before + rank;
+  int slot = offset_s[col] + w.block_color[blockIdx.x * 24 + col] + before + rank;
   w.slot_cid[slot] = cid;
 }
 
