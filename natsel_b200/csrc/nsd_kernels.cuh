@@ -1078,34 +1078,49 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
   const CPlanes& P = w.cp;
   float inv_tau = 1.0f / speculative_distance();
   float ws = p.warm_start;
-  int ia = ct.enc_a >= 0 ? ct.enc_a : -1;
-  int ib = ct.enc_b >= 0 ? ct.enc_b : -1;
+  // The contact's fields, then its bodies' masses, are read before the first plane is written:
+  // with the writes in between, each read would wait for its own trip to DRAM.
+  const int enc_a = ct.enc_a, enc_b = ct.enc_b;
+  const uint32_t flags = ct.flags;
+  const float rolling = ct.rolling, friction = ct.friction, restitution = ct.restitution;
+  const V3 tangent_velocity = ct.tangent_velocity;
+  const Manifold& man = ct.manifold;
+  const V3 n = man.normal;
+  const float twist_impulse = man.twist_impulse;
+  const V3 rolling_impulse = man.rolling_impulse, friction_impulse = man.friction_impulse;
+  const int pc = man.point_count;
+  V3 ra_[4], rb_[4];
+  float sep_[4], nimp_[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    ra_[i] = man.points[i].anchor_a;
+    rb_[i] = man.points[i].anchor_b;
+    sep_[i] = man.points[i].separation;
+    nimp_[i] = man.points[i].normal_impulse;
+  }
+  int ia = enc_a >= 0 ? enc_a : -1;
+  int ib = enc_b >= 0 ? enc_b : -1;
   float ima = 0.0f, imb = 0.0f;
   Sym sa = sym_zero(), sb = sym_zero();
   if (ia >= 0) { ima = w.asims[ia].inv_mass; sa = sym_from(w.asims[ia].inv_inertia_world); }
   if (ib >= 0) { imb = w.asims[ib].inv_mass; sb = sym_from(w.asims[ib].inv_inertia_world); }
-  bool is_static = (ct.flags & cStatic) != 0;
-  float rolling = ct.rolling;
+  bool is_static = (flags & cStatic) != 0;
   Sym inv_iab = sym_add(sa, sb);
   Sym rm = rolling > 0.0f ? sym_invert(inv_iab) : sym_zero();
-  const Manifold& man = ct.manifold;
-  V3 n = man.normal;
   V3 t1 = perp(n);
   V3 t2 = cross(t1, n);
-  float tv1 = dot(ct.tangent_velocity, t1), tv2 = dot(ct.tangent_velocity, t2);
-  float twist = ws * man.twist_impulse;
-  V3 rimp = rolling > 0.0f ? ws * man.rolling_impulse : v3(0, 0, 0);
-  V2 fi = v2(ws * dot(man.friction_impulse, t1), ws * dot(man.friction_impulse, t2));
+  float tv1 = dot(tangent_velocity, t1), tv2 = dot(tangent_velocity, t2);
+  float twist = ws * twist_impulse;
+  V3 rimp = rolling > 0.0f ? ws * rolling_impulse : v3(0, 0, 0);
+  V2 fi = v2(ws * dot(friction_impulse, t1), ws * dot(friction_impulse, t2));
   V3 ca = v3(0, 0, 0), cb = v3(0, 0, 0);
   float tw = 0.0f;
-  int pc = man.point_count;
-  V3 ra_[4], rb_[4];
-  for (int i = 0; i < pc; ++i) {
-    const ManifoldPoint& mp = man.points[i];
-    V3 ra = mp.anchor_a, rb = mp.anchor_b;
-    ra_[i] = ra; rb_[i] = rb;
-    float base_sep = mp.separation - dot(rb - ra, n);
-    float weight = clampf(2.0f - mp.separation * inv_tau, kMinFrictionWeight, 1.0f);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i >= pc) break;
+    V3 ra = ra_[i], rb = rb_[i];
+    float base_sep = sep_[i] - dot(rb - ra, n);
+    float weight = clampf(2.0f - sep_[i] * inv_tau, kMinFrictionWeight, 1.0f);
     ca = ca + weight * ra;
     cb = cb + weight * rb;
     tw += weight;
@@ -1124,19 +1139,23 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
     ca = v3(0, 0, 0); cb = v3(0, 0, 0);
   }
   float rv[4] = {0, 0, 0, 0};
-  if (ct.restitution > 0.0f) {
+  if (restitution > 0.0f) {
     DState s_a = state_at(w, ia), s_b = state_at(w, ib);
-    for (int i = 0; i < pc; ++i) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      if (i >= pc) break;
       V3 vra = s_a.v + cross(s_a.w, ra_[i]);
       V3 vrb = s_b.v + cross(s_b.w, rb_[i]);
       rv[i] = dot(n, vrb - vra);
     }
     atomicOr(&w.ctl->any_restitution, 1);
   }
-  for (int i = 0; i < pc; ++i) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i >= pc) break;
     V3 d = ra_[i] - ca;
     float lever = sqrtf(dot(d, d));
-    P.pimp[i * P.cap + slot] = make_float4(ws * man.points[i].normal_impulse, 0.0f, lever, rv[i]);
+    P.pimp[i * P.cap + slot] = make_float4(ws * nimp_[i], 0.0f, lever, rv[i]);
     P.prest[i * P.cap + slot] = 0.0f;
   }
   V3 rta1 = cross(ca, t1), rta2 = cross(ca, t2), rtb1 = cross(cb, t1), rtb2 = cross(cb, t2);
@@ -1151,7 +1170,7 @@ __device__ void prepare_constraint(const DW& w, const StepParams& p, int cid, in
   float ktw = dot(n, sym_mv(inv_iab, n));
   float twist_mass = ktw > 0.0f ? 1.0f / ktw : 0.0f;
   P.idx[slot] = make_int4(ia, ib, cid, pc | (is_static ? 256 : 0));
-  P.mass[slot] = make_float4(ima, imb, ct.friction, ct.restitution);
+  P.mass[slot] = make_float4(ima, imb, friction, restitution);
   P.ia0[slot] = make_float4(sa.xx, sa.xy, sa.xz, sa.yy);
   P.ia1[slot] = make_float4(sa.yz, sa.zz, sb.xx, sb.xy);
   P.ib1[slot] = make_float4(sb.xz, sb.yy, sb.yz, sb.zz);
