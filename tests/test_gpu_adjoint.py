@@ -184,6 +184,25 @@ def test_checkpoint_interval_does_not_change_gradients():
         np.testing.assert_allclose(g1[k], g2[k], rtol=1e-5, atol=1e-6)
 
 
+def test_reused_scratch_gives_the_same_gradients():
+    """Checkpoint buffers, step tapes and cotangent buffers are reused across VJPs of one world
+    and across worlds (one memory pool per device): the gradients must not change by a bit."""
+    g1 = adjoint(COLLIDE)[0]
+    g2 = adjoint(COLLIDE)[0]  # a fresh world drawing on the memory the first one gave back
+    w = build(COLLIDE, 8)
+    for _ in range(STEPS):
+        w.step(DT, SUBSTEPS)
+    pos = w.bodies()[0]
+    dpos = np.zeros_like(pos, dtype=np.float32)
+    dpos[1:] = 2.0 * (pos[1:] - targets(COLLIDE))
+    g3 = w.vjp(dpos=dpos)
+    g4 = w.vjp(dpos=dpos)  # the same world again, on its kept buffers
+    w.close()
+    for k in g1:
+        for g in (g2, g3, g4):
+            assert np.asarray(g[k]).tobytes() == np.asarray(g1[k]).tobytes(), k
+
+
 def test_vjp_of_velocity_cotangent_is_identity_without_contacts():
     # a free box in flight: final velocity = initial velocity + g t, so dL/dv0 = dL/dv
     w = World(**WORLD)
