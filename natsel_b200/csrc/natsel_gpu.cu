@@ -528,7 +528,7 @@ int upload_world(ns_world* w) {
   ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
   ALLOC(long_segment, int, kLongSegmentCap);
   ALLOC(ctl, Control, 1);
-  ALLOC(bwd, float4, 48 * (size_t)na); ALLOC(bw_mask, uint32_t, na); ALLOC(slot_cid, int, cap); ALLOC(slot_color, int8_t, cap);
+  ALLOC(bwd, float4, 48 * (size_t)na); ALLOC(bw_mask, uint32_t, na); ALLOC(slot_cid, int, cap); ALLOC(slot_state, uint8_t, cap);
   CPlanes& P = d.cp;
   P.cap = cap;
 #define PALLOC(field, T, n) do { P.field = dalloc<T>(w, (n), &st); if (!P.field) return st; } while (0)

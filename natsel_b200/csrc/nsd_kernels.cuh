@@ -29,6 +29,14 @@ __device__ __forceinline__ int slot_converged(int* counters, int key) {
   base = __shfl_sync(peers, base, leader);
   return base + __popc(peers & ((1u << lane) - 1u));
 }
+
+// DW::slot_state: bit 7 alive, bits 0..4 the colour + 1 of a touching contact in colours 0..22.
+constexpr uint8_t kSlotAlive = 0x80;
+__device__ __forceinline__ uint8_t slot_state_of(bool alive, bool touching, int color) {
+  return (uint8_t)((alive ? kSlotAlive : 0) |
+                   (alive && touching && color >= 0 && color < kOverflowIndex ? color + 1 : 0));
+}
+__device__ __forceinline__ int slot_color_of(uint8_t s) { return (s & kSlotAlive) ? (int)(s & 31) - 1 : -1; }
 constexpr int kColorBlock = 1024;
 constexpr int kSolveThreads = 256;   // per CTA of the solver cluster
 constexpr int kMaxSolveCluster = 16;
@@ -86,7 +94,10 @@ struct DW {
   // slot as used this step.
   float4* bwd; uint32_t* bw_mask;
   int* slot_cid;  // contact id of each coloured constraint slot (this step)
-  int8_t* slot_color;  // colour of each contact slot for the partition (-1: not coloured)
+  // One byte per contact slot, kept with the contact: bit 7 alive, bits 0..4 the colour + 1 of a
+  // touching contact in colours 0..22 (0 otherwise). Read by passes over every slot instead of
+  // the 400-byte contact records.
+  uint8_t* slot_state;
   int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
 };
 
@@ -458,6 +469,7 @@ __global__ void k_bp_create(DW w) {
     c.sat = SATCache();
     c.simplex = SimplexCache();
     w.contacts[id] = c;
+    w.slot_state[id] = slot_state_of(true, false, -1);
     hs_insert(w, key);
   }
 }
@@ -692,7 +704,7 @@ __device__ void collide_full(const DW& w, int cid) {
 constexpr int kCollideThreads = 256;
 __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
   for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
-    if (!w.contacts[cid].alive) continue;
+    if (!(w.slot_state[cid] & kSlotAlive)) continue;
     if (collide_recycle(w, cid)) {
       int kind = w.contacts[cid].kind;
       int slot = slot_converged(w.ctl->collide_count, kind);
@@ -862,14 +874,17 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
         c.alive = 0;
         c.color = -1;
         c.local = -1;
+        w.slot_state[st.cid[i]] = slot_state_of(false, false, -1);
       } else if (f & cSimStarted) {
         c.flags = (f & ~cSimStarted) | cTouching;
         c.color = color;
         if (color != kOverflowIndex) c.local = -1;
+        w.slot_state[st.cid[i]] = slot_state_of(true, true, color);
       } else if (f & cSimStopped) {
         c.flags = f & ~(cSimStopped | cTouching);
         c.color = -1;
         c.local = -1;
+        w.slot_state[st.cid[i]] = slot_state_of(true, false, -1);
       }
       w.destroyed[base + i] = destroyed;
     }
@@ -946,6 +961,7 @@ __global__ void k_state_worlds(DW w) {
         c.alive = 0;
         c.color = -1;
         c.local = -1;
+        w.slot_state[cid] = slot_state_of(false, false, -1);
         w.free_stack[base + top++] = cid;  // contact_creation.rs:543: ids go back in id order
         hs_erase(w, pair_key(c.shape_a, c.shape_b));
       } else if (f & cSimStarted) {   // constraint_graph.rs:113 add_contact_to_graph
@@ -968,6 +984,7 @@ __global__ void k_state_worlds(DW w) {
           }
         }
         c.color = color;
+        w.slot_state[cid] = slot_state_of(true, true, color);
         if (color == kOverflowIndex) {
           c.local = ovf;
           olist[ovf++] = cid;
@@ -980,6 +997,7 @@ __global__ void k_state_worlds(DW w) {
         remove(color);
         c.color = -1;
         c.local = -1;
+        w.slot_state[cid] = slot_state_of(true, false, -1);
       }
     }
   }
@@ -1008,8 +1026,7 @@ __device__ __forceinline__ int colored_color(const DContact& c) {
 __global__ void __launch_bounds__(kColorBlock) k_color_count(DW w) {
   __shared__ int wc[kColorBlock / 32][24];
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
-  int col = cid < w.cap ? colored_color(w.contacts[cid]) : -1;
-  if (cid < w.cap) w.slot_color[cid] = (int8_t)col;  // read by k_color_scatter
+  int col = cid < w.cap ? slot_color_of(w.slot_state[cid]) : -1;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = 0; k < kOverflowIndex; ++k) {
     unsigned m = __ballot_sync(0xffffffffu, col == k);
@@ -1202,7 +1219,7 @@ __global__ void __launch_bounds__(kColorBlock) k_color_scatter(DW w) {
     }
   }
   int cid = blockIdx.x * kColorBlock + threadIdx.x;
-  int col = cid < w.cap ? (int)w.slot_color[cid] : -1;
+  int col = cid < w.cap ? slot_color_of(w.slot_state[cid]) : -1;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned my_mask = 0;
   for (int k = 0; k < kOverflowIndex; ++k) {
