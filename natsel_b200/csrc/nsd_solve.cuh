@@ -1,13 +1,16 @@
 // Persistent colored solver (solver_stages.rs:543 solve_constraint_stages) and body
 // finalization (solver_integration.rs:587 finalize_body_range).
 //
-// One persistent launch runs every substep: integrate velocities, then per stage (warm
-// start, push, relax) the overflow color on one thread followed by colors 0..22, each color
-// one phase separated by a barrier over the whole launch (a grid-wide barrier for a
-// cooperative launch over the GPU, or the hardware barrier of one thread-block cluster);
-// then restitution and impulse storage. Every block takes the same path through the phases
-// (the loop bounds are read identically by all of them), so every block reaches every
-// barrier; colors with no work are skipped by all blocks alike.
+// One persistent launch runs every substep: integrate velocities together with each body's
+// warm start (the changes its constraints recorded, applied in colour order; the overflow
+// colour's warm start, when there is overflow work, runs on one thread per world between the
+// two), then per stage (push, relax) the overflow color on one thread followed by colors
+// 0..22, each color one phase separated by a barrier over the whole launch (a grid-wide
+// barrier for a cooperative launch over the GPU, or the hardware barrier of one thread-block
+// cluster), integrate positions between the stages; then restitution and impulse storage.
+// Every block takes the same path through the phases (the loop bounds are read identically
+// by all of them), so every block reaches every barrier; colors with no work are skipped by
+// all blocks alike.
 #pragma once
 #include "nsd_kernels.cuh"
 
