@@ -481,8 +481,11 @@ int upload_world(ns_world* w) {
     }
     d.cell = ext * 1.001f + 1e-3f;
     d.inv_cell = 1.0f / d.cell;
+    // at least twice as many buckets as small proxies: the keys of a 10 000-shape world fit in 16
+    // bits, two passes of the radix sort (proxies met through a hash collision are filtered by
+    // their cell)
     int buckets = 1024;
-    while (buckets < 4 * std::max(d.n_small, 1)) buckets <<= 1;
+    while (buckets < 2 * std::max(d.n_small, 1)) buckets <<= 1;
     d.cell_mask = buckets - 1;
     w->sort_bits = 1;
     while ((1u << w->sort_bits) <= (unsigned)buckets) ++w->sort_bits;
