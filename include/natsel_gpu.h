@@ -27,7 +27,8 @@ enum {
   NS_ERR_CUDA = 2,        /* CUDA runtime error (message in ns_last_error) */
   NS_ERR_CAPACITY = 3,    /* a device capacity (contacts, pairs) was exceeded */
   NS_ERR_TIMEOUT = 4,     /* a bounded grid barrier gave up; the step result is invalid */
-  NS_ERR_NONFINITE = 5,   /* a body state became NaN/Inf */
+  NS_ERR_NONFINITE = 5,   /* finalize found a NaN/Inf velocity, position or rotation (reported by
+                             the next synchronising call; the world stays in error) */
   NS_ERR_UNSUPPORTED = 6  /* feature outside the implemented path (e.g. sleeping) */
 };
 
@@ -121,7 +122,8 @@ int ns_world_step(ns_world* world, float dt, int substeps);
  * does (replaces apply_body_force_to_center body_api.rs:351 and apply_body_torque :366 for
  * every body at once). The arrays are copied before the call returns. */
 int ns_world_apply_forces(ns_world* world, const float* force, const float* torque);
-/* Wait for queued steps and report device-side errors (capacity, barrier timeout). */
+/* Wait for queued steps and report device-side errors (capacity, barrier timeout, non-finite
+ * body state). */
 int ns_world_synchronize(ns_world* world);
 
 /* Readback (synchronises). Arrays are per body in id order:
@@ -163,7 +165,12 @@ int ns_world_solver_counts(ns_world* world, int64_t* counts16);
  * convex_manifold_shapes.rs:21-643). Types: 0 capsule, 3 box hull, 5 sphere; A is
  * the primary type (capsule > sphere, hull > sphere/capsule). geom: box hx,hy,hz;
  * sphere cx,cy,cz,r; capsule c1 xyz, c2 xyz, r. xf = B in A's frame (p xyz, q xyzs).
- * The SAT/simplex caches are read and written back. Runs one device thread per pair. */
+ * The SAT/simplex caches are read and written back. Runs one device thread per pair.
+ * Every job is checked on the host before any GPU work, and a batch with one bad job is
+ * rejected whole with NS_ERR_INVALID: the pair must be one of the six primary-first pairs
+ * above, sat_type 0..8 with sat_hit 0 or 1, a face cache (type 2 or 3) must name a face
+ * 0..5, an edge cache (type 4) an even half-edge 0..22 on both boxes, and the simplex cache
+ * 0..3 vertices whose indices lie inside the shapes (box 8, capsule 2, sphere 1 vertex). */
 typedef struct {
   int32_t type_a, type_b;
   float geom_a[7], geom_b[7];
@@ -189,12 +196,16 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count);
  * compiled into the library (about 1 MiB, held on every GPU that loads the library until the
  * process exits) and so handles at most 4096 pairs per call; larger batches are rejected with
  * NS_ERR_CAPACITY before any GPU work (split them into calls of 4096 or fewer). Inputs and
- * outputs are the caller's host arrays, as for ns_collide_pairs, with identical results. The
- * first call on a device looks up the scratch address there and makes the kernel's first
- * launch on that device: make that first call before any stream capture. All calls on a device
- * share the one scratch area, so calls that overlap on the GPU (from several host threads, for
- * example) race; serialise them. Runs on the calling thread's current device and returns when
- * the results are in the host arrays. */
+ * outputs are the caller's host arrays, as for ns_collide_pairs, with identical results and
+ * the same job checks. The first call on a device sets that device up: it raises the device's
+ * per-thread stack limit to what the narrowphase kernel needs (the CUDA driver may allocate the
+ * larger local-memory reservation then) and, under lazy module loading, makes the library's
+ * module and with it the scratch area resident on the device. That first call may therefore
+ * allocate device memory or fail for lack of it: make it once at start-up, before the host's
+ * own allocator reserves the device and before any stream capture; later calls allocate
+ * nothing. All calls on a device share the one scratch area, so calls that overlap on the GPU
+ * (from several host threads, for example) race; serialise them. Runs on the calling thread's
+ * current device and returns when the results are in the host arrays. */
 int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int count);
 
 /* Diagnostics (no counterpart in the reference): launches the bounded grid barrier of the

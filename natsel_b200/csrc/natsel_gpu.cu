@@ -852,6 +852,8 @@ __global__ void k_gather_bodies(DW d, const int* body_loc, int nb, double* pos, 
 int control_status(ns_world* w, const Control& c) {
   if (c.error == kErrCapacity) return fail(w, NS_ERR_CAPACITY, "device capacity exceeded (contacts or pairs)");
   if (c.error == kErrTimeout) return fail(w, NS_ERR_TIMEOUT, "solver grid barrier timed out");
+  if (c.error == kErrNonFinite)
+    return fail(w, NS_ERR_NONFINITE, "a body velocity, position or rotation became NaN or Inf in finalize");
   if (c.error) return fail(w, c.error, "device error %d", c.error);
   return NS_OK;
 }
@@ -1445,8 +1447,45 @@ extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
   return NS_OK;
 }
 
-namespace {
-}  // namespace
+// Host-side check of a batch narrowphase job before any GPU work: the kernel indexes local
+// arrays with the caller's cache fields (a face plane per SAT face index, a half-edge pair per
+// edge index, simplex vertices per cached index), so every one must lie inside its shape.
+// Pairs follow the reference's primary-type order (contact_creation.rs:88-96).
+static int shape_vertex_count(int type) { return type == kHull ? kHullVertexCount : type == kCapsule ? 2 : 1; }
+
+static int validate_pair_jobs(const ns_pair_job* jobs, int count, const char* who) {
+  for (int i = 0; i < count; ++i) {
+    const ns_pair_job& j = jobs[i];
+    bool pair_ok = (j.type_a == kSphere && j.type_b == kSphere) ||
+                   (j.type_a == kCapsule && (j.type_b == kSphere || j.type_b == kCapsule)) ||
+                   (j.type_a == kHull && (j.type_b == kSphere || j.type_b == kCapsule || j.type_b == kHull));
+    if (!pair_ok)
+      return fail(nullptr, NS_ERR_INVALID, "%s: job %d pairs shape types (%d, %d), not a primary-first pair of "
+                  "0 capsule, 3 box hull, 5 sphere", who, i, j.type_a, j.type_b);
+    if (j.sat_type < kInvalidAxis || j.sat_type > kManualEdgePairAxis || j.sat_hit < 0 || j.sat_hit > 1)
+      return fail(nullptr, NS_ERR_INVALID, "%s: job %d has SAT cache type %d / hit %d", who, i, j.sat_type, j.sat_hit);
+    bool face_a = j.sat_type == kFaceAxisA, face_b = j.sat_type == kFaceAxisB, edge = j.sat_type == kEdgePairAxis;
+    // face caches index a face plane; edge caches index the first half-edge of a twin pair
+    if ((face_a && (j.sat_index_a < 0 || j.sat_index_a >= kHullFaceCount)) ||
+        (face_b && (j.sat_index_b < 0 || j.sat_index_b >= kHullFaceCount)) ||
+        (edge && (j.sat_index_a < 0 || j.sat_index_a >= kHullEdgeCount - 1 || (j.sat_index_a & 1) ||
+                  j.sat_index_b < 0 || j.sat_index_b >= kHullEdgeCount - 1 || (j.sat_index_b & 1))) ||
+        j.sat_index_a < 0 || j.sat_index_a > 255 || j.sat_index_b < 0 || j.sat_index_b > 255)
+      return fail(nullptr, NS_ERR_INVALID, "%s: job %d has SAT cache indices (%d, %d) outside the box for type %d",
+                  who, i, j.sat_index_a, j.sat_index_b, j.sat_type);
+    if (j.simplex_count < 0 || j.simplex_count > 3)
+      return fail(nullptr, NS_ERR_INVALID, "%s: job %d has simplex cache count %d (0..3)", who, i, j.simplex_count);
+    int na = shape_vertex_count(j.type_a), nb = shape_vertex_count(j.type_b);
+    for (int k = 0; k < 4; ++k) {
+      bool used = k < j.simplex_count;
+      int ia = j.simplex_ia[k], ib = j.simplex_ib[k];
+      if (ia < 0 || ia > 255 || ib < 0 || ib > 255 || (used && (ia >= na || ib >= nb)))
+        return fail(nullptr, NS_ERR_INVALID, "%s: job %d simplex vertex %d indexes (%d, %d) of shapes with %d and %d "
+                    "vertices", who, i, k, ia, ib, na, nb);
+    }
+  }
+  return NS_OK;
+}
 
 // Fixed device scratch of ns_collide_pairs_noalloc: the device copies of one call's jobs
 // (first kNoAllocPairs * sizeof(PairJob) bytes) and results (the rest). Every GPU that loads
@@ -1456,10 +1495,11 @@ constexpr size_t kNoAllocJobBytes = (size_t)kNoAllocPairs * sizeof(nsd::PairJob)
 static_assert(kNoAllocJobBytes % 256 == 0, "results must start 256-byte aligned");
 static __device__ __align__(256) unsigned char g_pair_scratch[kNoAllocJobBytes + (size_t)kNoAllocPairs * sizeof(nsd::PairResult)];
 
-// Device address of g_pair_scratch per device, looked up once with that device current (in
-// host code the symbol is only a host-side stand-in, never a device address).
+// In host code g_pair_scratch is only a host-side stand-in, never a device address: each call
+// asks the runtime for the address on the current device. The stack set-up is done once per
+// device (under the mutex).
 constexpr int kNoAllocMaxDevices = 64;
-static unsigned char* g_pair_scratch_addr[kNoAllocMaxDevices];
+static bool g_pair_stack_ready[kNoAllocMaxDevices];
 static std::mutex g_pair_scratch_mutex;
 
 extern "C" {
@@ -1995,7 +2035,9 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count) {
   if (count < 0 || (count > 0 && (!jobs || !results))) return fail(nullptr, NS_ERR_INVALID, "invalid pair batch");
   if (count == 0) return NS_OK;
   {
-    int st0 = ensure_stack(nullptr);
+    int st0 = validate_pair_jobs(jobs, count, "ns_collide_pairs");
+    if (st0) return st0;
+    st0 = ensure_stack(nullptr);
     if (st0) return st0;
   }
   PairJob* dj = nullptr;
@@ -2016,15 +2058,23 @@ int ns_collide_pairs(ns_pair_job* jobs, ns_pair_result* results, int count) {
 }
 
 // See natsel_gpu.h: the batch narrowphase without any device allocation. The first call on a
-// device resolves the scratch address for that device (and is the first launch of the kernel
-// there); everything after that is two copies in, one launch and two copies out, all on the
-// legacy default stream, so each call has finished when it returns.
+// device raises that device's per-thread stack limit to what the narrowphase kernels need (the
+// same set-up ns_collide_pairs and world creation do; the driver may allocate the larger
+// local-memory reservation then) and, with lazy module loading, makes the module and its
+// scratch array resident there. Every call looks the scratch address up again with the device
+// current (cheap), so a reset device or another context never sees a stale address. Then two
+// copies in, one launch and two copies out, all on the legacy default stream, so each call has
+// finished when it returns.
 int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int count) {
   if (count < 0 || (count > 0 && (!jobs || !results))) return fail(nullptr, NS_ERR_INVALID, "invalid pair batch");
   if (count > kNoAllocPairs)
     return fail(nullptr, NS_ERR_CAPACITY, "ns_collide_pairs_noalloc: %d pairs exceed its fixed scratch of %d pairs",
                 count, kNoAllocPairs);
   if (count == 0) return NS_OK;
+  {
+    int st0 = validate_pair_jobs(jobs, count, "ns_collide_pairs_noalloc");
+    if (st0) return st0;
+  }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc: %s", cudaGetErrorString(e));
@@ -2032,15 +2082,15 @@ int ns_collide_pairs_noalloc(ns_pair_job* jobs, ns_pair_result* results, int cou
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_pair_scratch_mutex);
-    if (!g_pair_scratch_addr[dev]) {
-      e = cudaGetSymbolAddress((void**)&g_pair_scratch_addr[dev], g_pair_scratch);
-      if (e != cudaSuccess) {
-        g_pair_scratch_addr[dev] = nullptr;
-        return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc scratch address: %s", cudaGetErrorString(e));
-      }
+    if (!g_pair_stack_ready[dev]) {
+      int st0 = ensure_stack(nullptr);
+      if (st0) return st0;
+      g_pair_stack_ready[dev] = true;
     }
-    base = g_pair_scratch_addr[dev];
   }
+  e = cudaGetSymbolAddress((void**)&base, g_pair_scratch);
+  if (e != cudaSuccess)
+    return fail(nullptr, NS_ERR_CUDA, "ns_collide_pairs_noalloc scratch address: %s", cudaGetErrorString(e));
   // every slot below count is overwritten (jobs by the copy, results by the kernel), so nothing
   // left from an earlier call is read
   PairJob* dj = reinterpret_cast<PairJob*>(base);

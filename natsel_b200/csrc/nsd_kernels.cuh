@@ -46,6 +46,7 @@ constexpr unsigned long long kHsTomb = ~0ull - 1ull;
 // Error codes mirrored from natsel_gpu.h.
 constexpr int kErrCapacity = 3;
 constexpr int kErrTimeout = 4;
+constexpr int kErrNonFinite = 5;
 
 struct DW {
   DSim* asims; DState* states; int n_awake;

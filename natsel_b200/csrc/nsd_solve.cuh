@@ -1277,7 +1277,14 @@ __global__ void k_finalize(DW w, StepParams p) {
   }
   M3 R = matrix_from_quat(sim.q);
   sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
-  if ((sim.flags & kIsFast) == 0) {
+  // solver_integration.rs:626-627 asserts finite velocities here; the device raises
+  // NS_ERR_NONFINITE instead (first error wins) and keeps the body's old fat AABB, so a
+  // non-finite pose never reaches the broadphase grid
+  bool finite = isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(wv.x) && isfinite(wv.y) &&
+                isfinite(wv.z) && isfinite(sim.cx) && isfinite(sim.cy) && isfinite(sim.cz) &&
+                isfinite(sim.q.v.x) && isfinite(sim.q.v.y) && isfinite(sim.q.v.z) && isfinite(sim.q.s);
+  if (!finite) atomicCAS(&w.ctl->error, 0, kErrNonFinite);
+  if (finite && (sim.flags & kIsFast) == 0) {
     WXf xf_;
     xf_.p = tp; xf_.q = sim.q;
     float spec = speculative_distance();

@@ -179,16 +179,36 @@ def jointed_chains(world, chains=2000, links=24, boxes=4000, seed=3, grid=45, sp
     return {"name": "jointed_chains", "dynamic_bodies": chains * links + boxes, "joints": n_joints}
 
 
+def _batch_plan(index, seed):
+    """The seeded draws of batch world ``index``: (kind, N, rng positioned after them)."""
+    rng = np.random.Generator(np.random.PCG64([seed, index]))
+    n = int(np.exp(rng.uniform(np.log(32.0), np.log(512.0))))
+    kind = "pyramid" if rng.uniform() < 0.5 else "drop"
+    return kind, n, rng
+
+
+def _pyramid_base(n):
+    return max(2, int((np.sqrt(8 * n + 1) - 1) / 2))
+
+
+def batch_world_size(index, seed=4):
+    """Dynamic bodies of batch world ``index`` without building it (a pyramid of base b holds
+    b (b + 1) / 2 cubes; a drop holds N bodies)."""
+    kind, n, _ = _batch_plan(index, seed)
+    if kind == "pyramid":
+        b = _pyramid_base(n)
+        return b * (b + 1) // 2
+    return n
+
+
 def batch_world(world, index, seed=4):
     """One world of the batched-worlds workload: N ~ log-uniform(32, 512) bodies, either a box
     pyramid of about N cubes or a random drop of N bodies with the 10 000-body pile's shape mix
     and parameter ranges (dropped from its volume scaled to N at the same density), seeded by
     (seed, index)."""
-    rng = np.random.Generator(np.random.PCG64([seed, index]))
-    n = int(np.exp(rng.uniform(np.log(32.0), np.log(512.0))))
-    if rng.uniform() < 0.5:
-        base = max(2, int((np.sqrt(8 * n + 1) - 1) / 2))
-        info = box_pyramid(world, base=base, seed=int(rng.integers(1 << 30)))
+    kind, n, rng = _batch_plan(index, seed)
+    if kind == "pyramid":
+        info = box_pyramid(world, base=_pyramid_base(n), seed=int(rng.integers(1 << 30)))
         return {"kind": "pyramid", "dynamic_bodies": info["dynamic_bodies"]}
     # the 10 000-body pile's 40 x 60 x 40 m volume scaled to N at the same initial density
     scale = (n / 10000.0) ** (1.0 / 3.0)
@@ -199,16 +219,18 @@ def batch_world(world, index, seed=4):
     return {"kind": "drop", "dynamic_bodies": info["dynamic_bodies"]}
 
 
-def batched_worlds(world, count=4096, seed=4):
-    """``count`` independent worlds (batch_world) in one world object, one sub-world each."""
+def batched_worlds(world, count=4096, seed=4, indices=None):
+    """``count`` independent worlds (batch_world) in one world object, one sub-world each;
+    ``indices`` builds only those worlds of the batch (one rank's share), in that order."""
     total, kinds = 0, []
-    for k in range(count):
+    picks = range(count) if indices is None else indices
+    for k, index in enumerate(picks):
         if k > 0:
             world.begin_subworld()
-        info = batch_world(world, k, seed)
+        info = batch_world(world, int(index), seed)
         total += info["dynamic_bodies"]
         kinds.append(info["kind"])
-    return {"name": "batched_worlds", "worlds": count, "dynamic_bodies": total, "kinds": kinds}
+    return {"name": "batched_worlds", "worlds": len(kinds), "dynamic_bodies": total, "kinds": kinds}
 
 
 PI = F(3.14159265359)  # base/constants.rs:6

@@ -76,14 +76,34 @@ class ShapeDef(ctypes.Structure):
 _F3 = ctypes.c_float * 3
 _F7 = ctypes.c_float * 7
 _lib = None
+_lib_path = None
+
+
+def use_host_native():
+    """Switch this process to an oracle built with -march=native for the host it runs on (the
+    CPU-baseline timing build: -O3 -ffp-contract=off, as the portable build, plus the host's
+    vector extensions, which change no bits without contraction). Must run before the first
+    oracle call. Returns a one-line description of the build that will be used."""
+    global _lib_path
+    if _lib is not None:
+        raise RuntimeError("use_host_native() must run before the oracle is loaded")
+    import tempfile
+    out = os.path.join(tempfile.mkdtemp(prefix="ns_oracle_"), "libns_oracle_native.so")
+    r = subprocess.run(["make", "-s", "-C", HERE, "native", "OUT=" + out], capture_output=True, text=True)
+    if r.returncode != 0 or not os.path.exists(out):
+        build()
+        return "portable -O3 build (the -march=native build failed: %s)" % (r.stderr.strip().splitlines() or ["?"])[-1]
+    _lib_path = out
+    return "-O3 -march=native -ffp-contract=off, built on this host"
 
 
 def load():
     global _lib
     if _lib is not None:
         return _lib
-    build()
-    lib = ctypes.CDLL(LIB_PATH)
+    if _lib_path is None:
+        build()
+    lib = ctypes.CDLL(_lib_path or LIB_PATH)
     P = ctypes.c_void_p
     lib.nso_default_world_def.argtypes = [ctypes.POINTER(WorldDef)]
     lib.nso_create.argtypes = [ctypes.POINTER(WorldDef)]

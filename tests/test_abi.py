@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from conftest import HAS_GPU, ROOT
@@ -59,3 +60,108 @@ def test_sleeping_is_rejected():
     d = nw.default_world_def(enable_sleep=1)
     with pytest.raises(nw.NsError):
         nw.World(d)
+
+
+def _c_layout():
+    """Field offsets and struct sizes of the header's structs, as a C99 compiler lays them out."""
+    import shutil
+    import subprocess
+    import tempfile
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {
+        "ns_world_def": [f[0] for f in nw.WorldDef._fields_],
+        "ns_body_def": [f[0] for f in nw.BodyDef._fields_],
+        "ns_shape_def": [f[0] for f in nw.ShapeDef._fields_],
+    }
+    from natsel_b200 import narrowphase
+    structs["ns_pair_job"] = list(narrowphase.PAIR_JOB_DTYPE.names)
+    structs["ns_pair_result"] = list(narrowphase.PAIR_RESULT_DTYPE.names)
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "natsel_gpu.h"', 'int main(void) {']
+    for s, fields in structs.items():
+        lines.append('  printf("%s size %%zu\\n", sizeof(%s));' % (s, s))
+        for f in fields:
+            lines.append('  printf("%s %s %%zu\\n", offsetof(%s, %s));' % (s, f, s, f))
+    lines += ['  return 0;', '}']
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "layout.c"), os.path.join(d, "layout")
+        open(src, "w").write("\n".join(lines) + "\n")
+        subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I",
+                        os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    layout = {}
+    for line in out.splitlines():
+        s, f, v = line.split()
+        layout[(s, f)] = int(v)
+    return layout
+
+
+def test_header_compiles_as_c99_with_the_mirrored_layouts():
+    from natsel_b200 import narrowphase
+    layout = _c_layout()
+    for name, cls in (("ns_world_def", nw.WorldDef), ("ns_body_def", nw.BodyDef), ("ns_shape_def", nw.ShapeDef)):
+        assert layout[(name, "size")] == ctypes.sizeof(cls)
+        for f in cls._fields_:
+            assert layout[(name, f[0])] == getattr(cls, f[0]).offset, (name, f[0])
+    for name, dt in (("ns_pair_job", narrowphase.PAIR_JOB_DTYPE), ("ns_pair_result", narrowphase.PAIR_RESULT_DTYPE)):
+        assert layout[(name, "size")] == dt.itemsize
+        for f in dt.names:
+            assert layout[(name, f)] == dt.fields[f][1], (name, f)
+
+
+def _bad_jobs():
+    """One valid batch with a single bad job planted in it, for every check the host makes."""
+    import _pairgen
+    from natsel_b200 import narrowphase
+    cases = []
+
+    def plant(idx, **fields):
+        jobs = _pairgen.make_jobs(narrowphase.PAIR_JOB_DTYPE, 12, 3, 1.0)
+        for k, v in fields.items():
+            jobs[idx][k] = v
+        return jobs
+
+    # idx 0 is hull-hull, 1 hull-sphere, 2 hull-capsule, 3 sphere-sphere, 4 capsule-sphere
+    cases.append(("unknown type", plant(3, type_a=7)))
+    cases.append(("secondary type first", plant(3, type_a=5, type_b=0)))
+    cases.append(("sphere with a box", plant(3, type_b=3)))
+    cases.append(("sat type", plant(0, sat_type=9)))
+    cases.append(("sat hit", plant(0, sat_hit=2)))
+    cases.append(("face index", plant(0, sat_type=2, sat_index_a=6)))
+    cases.append(("face b index", plant(0, sat_type=3, sat_index_b=200)))
+    cases.append(("odd edge", plant(0, sat_type=4, sat_index_a=3, sat_index_b=2)))
+    cases.append(("edge past the end", plant(0, sat_type=4, sat_index_a=0, sat_index_b=24)))
+    cases.append(("negative index", plant(0, sat_index_a=-1)))
+    cases.append(("simplex count", plant(1, simplex_count=65535)))
+    cases.append(("simplex count negative", plant(1, simplex_count=-1)))
+    ia = np.array([0, 8, 0, 0], np.int32)
+    cases.append(("simplex vertex of the box", plant(1, simplex_count=2, simplex_ia=ia)))
+    ib = np.array([0, 1, 0, 0], np.int32)
+    cases.append(("simplex vertex of the sphere", plant(1, simplex_count=2, simplex_ib=ib)))
+    ib2 = np.array([2, 0, 0, 0], np.int32)
+    cases.append(("simplex vertex of the capsule", plant(2, simplex_count=1, simplex_ib=ib2)))
+    return cases
+
+
+
+@pytest.mark.parametrize("entry", ["ns_collide_pairs", "ns_collide_pairs_noalloc"])
+def test_bad_pair_jobs_are_rejected_on_the_host_before_any_gpu_work(entry):
+    """Every job is checked before a copy or launch: a batch with one bad job returns
+    NS_ERR_INVALID and leaves the jobs as they were (no device is needed to see it)."""
+    from natsel_b200 import narrowphase
+    lib = nw.load_library()
+    fn = getattr(lib, entry)
+    for what, jobs in _bad_jobs():
+        before = jobs.tobytes()
+        results = np.zeros(len(jobs), narrowphase.PAIR_RESULT_DTYPE)
+        status = fn(jobs.ctypes.data_as(ctypes.c_void_p), results.ctypes.data_as(ctypes.c_void_p), len(jobs))
+        assert status == 1, what
+        assert b"job" in lib.ns_last_error(None), what
+        assert jobs.tobytes() == before and not results.tobytes().strip(b"\0"), what
+    # the untouched batch passes the checks (without a GPU it then fails on the device instead)
+    import _pairgen
+    jobs = _pairgen.make_jobs(narrowphase.PAIR_JOB_DTYPE, 12, 3, 1.0)
+    results = np.zeros(len(jobs), narrowphase.PAIR_RESULT_DTYPE)
+    status = fn(jobs.ctypes.data_as(ctypes.c_void_p), results.ctypes.data_as(ctypes.c_void_p), len(jobs))
+    assert status == (0 if HAS_GPU else 2)

@@ -290,6 +290,25 @@ def test_barrier_timeout_is_reported_and_context_survives():
     _both(lambda w: scenes.box_pyramid(w, base=3), steps=2)
 
 
+def test_nonfinite_state_is_reported():
+    """A NaN force reaches finalize's finite check (the reference asserts finite velocities
+    there, solver_integration.rs:626-627): the next synchronising call reports
+    NS_ERR_NONFINITE. Only the one step with the NaN runs; its bodies keep their old fat AABBs."""
+    g = World(default_world_def(gravity=(0.0, -9.81, 0.0)))
+    scenes.box_pyramid(g, base=4)
+    for _ in range(3):
+        g.step(DT, 4)
+    g.synchronize()
+    f = np.zeros((g.body_count, 3), np.float32)
+    f[g.body_count - 1, 0] = np.nan
+    g.apply_forces(f)
+    g.step(DT, 4)
+    with pytest.raises(NsError) as err:
+        g.synchronize()
+    assert err.value.code == 5 and "NaN" in str(err.value)
+    g.close()
+
+
 # ----- full-size properties -----------------------------------------------------------------
 def test_large_pile_settles():
     """600 steps of the 10 000-body pile (the workload's full length): state stays finite,

@@ -180,3 +180,23 @@ def test_pairs_fixture():
     assert r1.tobytes() == z["res1"].tobytes() and jobs.tobytes() == z["jobs1"].tobytes()
     r2 = pyoracle.collide_pairs(jobs)
     assert r2.tobytes() == z["res2"].tobytes() and jobs.tobytes() == z["jobs2"].tobytes()
+
+
+def test_native_timing_build_keeps_the_golden_hash():
+    """The CPU baselines time an -O3 -march=native build of the oracle made on the timing host;
+    without contraction it must give the same bits (here: many_pyramids, 100 steps, 4 threads)."""
+    import subprocess
+    import sys
+    from conftest import ROOT, TESTS
+    script = (
+        "import sys, json; sys.path[:0] = [%r, %r]\n"
+        "from oracle import pyoracle\n"
+        "desc = pyoracle.use_host_native()\n"
+        "assert 'march=native' in desc, desc\n"
+        "pyoracle.set_threads(4)\n"
+        "from test_oracle_pins import _hashes\n"
+        "case = json.load(open(%r))['cases']['many_pyramids']\n"
+        "assert _hashes('many_pyramids', {}, case['steps'])[-1] == case['hash']\n"
+        "print('native ok')\n" % (ROOT, TESTS, os.path.join(GOLDEN, "reference_hashes.json")))
+    out = subprocess.run([sys.executable, "-c", script], capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0 and "native ok" in out.stdout, out.stdout + out.stderr

@@ -44,3 +44,38 @@ def test_batches_over_the_limit_are_rejected_before_any_work():
     assert err.value.code == 3 and "4096" in str(err.value)
     assert jobs.tobytes() == before
     assert len(narrowphase.collide_pairs_noalloc(jobs[:0].copy())) == 0
+
+
+FIRST_CALL_SCRIPT = r"""
+import sys
+sys.path[:0] = [{root!r}, {tests!r}]
+import numpy as np
+from natsel_b200 import narrowphase
+from oracle import pyoracle
+import _pairgen
+jobs = _pairgen.make_jobs(narrowphase.PAIR_JOB_DTYPE, 3000, 81, 1.2)
+ref = jobs.copy().view(pyoracle.PAIR_JOB_DTYPE)
+got = narrowphase.collide_pairs_noalloc(jobs)        # the first library call of this process
+want = pyoracle.collide_pairs(ref)
+assert got.tobytes() == want.tobytes(), "results differ from the oracle"
+assert jobs.tobytes() == ref.tobytes(), "written-back caches differ from the oracle"
+again = narrowphase.collide_pairs_noalloc(jobs)       # second call, from the written-back caches
+assert again.tobytes() == pyoracle.collide_pairs(ref).tobytes()
+print("first-call ok", int((got["point_count"] > 0).sum()))
+"""
+
+
+def test_first_call_in_a_fresh_process_matches_the_oracle():
+    """A host that cannot allocate makes this its first call into the library, at start-up:
+    the device set-up that call does (stack limit, module load) must leave correct results.
+    Runs in a new process, so nothing else has touched the device before it."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT, TESTS
+    script = FIRST_CALL_SCRIPT.format(root=ROOT, tests=TESTS)
+    out = subprocess.run([sys.executable, "-c", script], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ))
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "first-call ok" in out.stdout
+    assert int(out.stdout.split()[-1]) > 300
