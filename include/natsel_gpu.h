@@ -92,11 +92,36 @@ int ns_create_sphere_shape(ns_world* world, int body, const ns_shape_def* def, c
                            float radius);
 int ns_create_capsule_shape(ns_world* world, int body, const ns_shape_def* def, const float center1[3],
                             const float center2[3], float radius);
-/* frame = position xyz + rotation xyzs, local to each body's origin. */
+/* frame = position xyz + rotation xyzs, local to each body's origin. The joint's softness is the
+ * world's joint_hertz / joint_damping_ratio; max_motor_torque > 0 enables a motor of speed 0
+ * (a drag torque). ns_create_revolute_joint_def takes every field instead. */
 int ns_create_revolute_joint(ns_world* world, int body_a, int body_b, const float frame_a[7],
                              const float frame_b[7], int enable_limit, float lower_angle,
                              float upper_angle, int enable_spring, float hertz, float damping_ratio,
                              float max_motor_torque, int collide_connected);
+
+/* RevoluteJointDef (types/joint_defs.rs:154, with its JointDef base :30; the base's force and
+ * torque thresholds and draw scale belong to joint events and debug draw, outside this path).
+ * The rotation axis is the z axis of the local frames. */
+typedef struct {
+  int body_a, body_b;
+  float local_frame_a[7], local_frame_b[7]; /* position xyz + rotation xyzs */
+  float constraint_hertz;                    /* 60 */
+  float constraint_damping_ratio;            /* 2 */
+  int collide_connected;                     /* 0 */
+  float target_angle;                        /* spring rest angle, radians */
+  int enable_spring;
+  float hertz, damping_ratio;
+  int enable_limit;
+  float lower_angle, upper_angle;
+  int enable_motor;
+  float max_motor_torque, motor_speed;
+} ns_revolute_joint_def;
+/* Defaults of RevoluteJointDef::default (everything off, identity frames, bodies -1). */
+void ns_default_revolute_joint_def(ns_revolute_joint_def* def);
+/* create_revolute_joint (revolute_joint.rs:161) with the whole definition. Returns the joint id
+ * (>= 0) or -1. */
+int ns_create_revolute_joint_def(ns_world* world, const ns_revolute_joint_def* def);
 
 /* Batched worlds (no counterpart in the reference, which steps one world at a time): a world
  * can hold several independent sub-worlds that are stepped together by every ns_world_step.

@@ -1646,6 +1646,37 @@ int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa
                              int enable_limit, float lower, float upper, int enable_spring, float hertz,
                              float damping_ratio, float max_motor_torque, int collide_connected) {
   if (!w || !fa || !fb) return -1;
+  ns_revolute_joint_def d;
+  ns_default_revolute_joint_def(&d);
+  d.body_a = body_a; d.body_b = body_b;
+  memcpy(d.local_frame_a, fa, sizeof(d.local_frame_a));
+  memcpy(d.local_frame_b, fb, sizeof(d.local_frame_b));
+  d.constraint_hertz = w->def.joint_hertz;
+  d.constraint_damping_ratio = w->def.joint_damping_ratio;
+  d.collide_connected = collide_connected;
+  d.enable_spring = enable_spring; d.hertz = hertz; d.damping_ratio = damping_ratio;
+  d.enable_limit = enable_limit; d.lower_angle = lower; d.upper_angle = upper;
+  // a motor with zero speed (a drag torque) whenever a torque is given
+  d.enable_motor = max_motor_torque > 0.0f; d.max_motor_torque = max_motor_torque; d.motor_speed = 0.0f;
+  return ns_create_revolute_joint_def(w, &d);
+}
+
+void ns_default_revolute_joint_def(ns_revolute_joint_def* d) {
+  memset(d, 0, sizeof(*d));
+  d->body_a = d->body_b = -1;
+  d->local_frame_a[6] = 1.0f;
+  d->local_frame_b[6] = 1.0f;
+  d->constraint_hertz = 60.0f;          // joint_defs.rs:54-55
+  d->constraint_damping_ratio = 2.0f;
+}
+
+// revolute_joint.rs:161 create_revolute_joint with the whole RevoluteJointDef
+int ns_create_revolute_joint_def(ns_world* w, const ns_revolute_joint_def* def) {
+  if (!w || !def) return -1;
+  int body_a = def->body_a, body_b = def->body_b;
+  const float* fa = def->local_frame_a;
+  const float* fb = def->local_frame_b;
+  int collide_connected = def->collide_connected;
   if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
   int nb = (int)w->bodies.size();
   if (body_a < 0 || body_b < 0 || body_a >= nb || body_b >= nb || body_a == body_b) { w->err = "invalid joint bodies"; return -1; }
@@ -1663,12 +1694,14 @@ int ns_create_revolute_joint(ns_world* w, int body_a, int body_b, const float fa
   j.enc_a = encode(ba); j.enc_b = encode(bb);
   j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
   j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
-  j.constraint_hertz = w->def.joint_hertz;
-  j.constraint_damping_ratio = w->def.joint_damping_ratio;
+  j.constraint_hertz = def->constraint_hertz;
+  j.constraint_damping_ratio = def->constraint_damping_ratio;
   j.constraint_softness.bias_rate = 0.0f; j.constraint_softness.mass_scale = 1.0f; j.constraint_softness.impulse_scale = 0.0f;
-  j.enable_limit = enable_limit != 0; j.lower_angle = lower; j.upper_angle = upper;
-  j.enable_spring = enable_spring != 0; j.hertz = hertz; j.damping_ratio = damping_ratio;
-  j.max_motor_torque = max_motor_torque; j.enable_motor = max_motor_torque > 0.0f;
+  j.enable_limit = def->enable_limit != 0; j.lower_angle = def->lower_angle; j.upper_angle = def->upper_angle;
+  j.enable_spring = def->enable_spring != 0; j.hertz = def->hertz; j.damping_ratio = def->damping_ratio;
+  j.target_angle = def->target_angle;
+  j.max_motor_torque = def->max_motor_torque; j.enable_motor = def->enable_motor != 0;
+  j.motor_speed = def->motor_speed;
   // constraint_graph.rs:256 assign_joint_color
   uint32_t& ma = w->body_mask[body_a];
   uint32_t& mb = w->body_mask[body_b];

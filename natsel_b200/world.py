@@ -74,6 +74,39 @@ class ShapeDef(ctypes.Structure):
     ]
 
 
+class RevoluteJointDef(ctypes.Structure):
+    """ns_revolute_joint_def (the reference's RevoluteJointDef, types/joint_defs.rs:154)."""
+    _fields_ = [
+        ("body_a", ctypes.c_int), ("body_b", ctypes.c_int),
+        ("local_frame_a", ctypes.c_float * 7), ("local_frame_b", ctypes.c_float * 7),
+        ("constraint_hertz", ctypes.c_float), ("constraint_damping_ratio", ctypes.c_float),
+        ("collide_connected", ctypes.c_int),
+        ("target_angle", ctypes.c_float),
+        ("enable_spring", ctypes.c_int), ("hertz", ctypes.c_float), ("damping_ratio", ctypes.c_float),
+        ("enable_limit", ctypes.c_int), ("lower_angle", ctypes.c_float), ("upper_angle", ctypes.c_float),
+        ("enable_motor", ctypes.c_int), ("max_motor_torque", ctypes.c_float), ("motor_speed", ctypes.c_float),
+    ]
+
+
+def revolute_def(cls, default_hertz, default_zeta, body_a, body_b, frame_a, frame_b, enable_limit, lower, upper,
+                 enable_spring, hertz, damping_ratio, max_motor_torque, collide_connected, enable_motor,
+                 motor_speed, target_angle, constraint_hertz, constraint_damping_ratio):
+    """Fill a revolute joint definition struct (``cls``: this module's or the oracle's mirror)."""
+    d = cls()
+    d.body_a, d.body_b = body_a, body_b
+    d.local_frame_a = (ctypes.c_float * 7)(*frame_a)
+    d.local_frame_b = (ctypes.c_float * 7)(*frame_b)
+    d.constraint_hertz = default_hertz if constraint_hertz is None else constraint_hertz
+    d.constraint_damping_ratio = default_zeta if constraint_damping_ratio is None else constraint_damping_ratio
+    d.collide_connected = int(collide_connected)
+    d.target_angle = target_angle
+    d.enable_spring, d.hertz, d.damping_ratio = int(enable_spring), hertz, damping_ratio
+    d.enable_limit, d.lower_angle, d.upper_angle = int(enable_limit), lower, upper
+    d.enable_motor = int(max_motor_torque > 0.0) if enable_motor is None else int(enable_motor)
+    d.max_motor_torque, d.motor_speed = max_motor_torque, motor_speed
+    return d
+
+
 _F3 = ctypes.c_float * 3
 _F7 = ctypes.c_float * 7
 _lib = None
@@ -81,7 +114,7 @@ _lib = None
 EXPORTED = [
     "ns_default_world_def", "ns_world_create", "ns_world_destroy", "ns_last_error",
     "ns_create_body", "ns_create_box_shape", "ns_create_sphere_shape", "ns_create_capsule_shape",
-    "ns_create_revolute_joint", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
+    "ns_create_revolute_joint", "ns_default_revolute_joint_def", "ns_create_revolute_joint_def", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
     "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
@@ -114,6 +147,9 @@ def load_library(path=LIB_PATH):
     lib.ns_create_revolute_joint.argtypes = [P, ctypes.c_int, ctypes.c_int, _F7, _F7, ctypes.c_int,
                                              ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float,
                                              ctypes.c_float, ctypes.c_float, ctypes.c_int]
+    lib.ns_default_revolute_joint_def.argtypes = [ctypes.POINTER(RevoluteJointDef)]
+    lib.ns_default_revolute_joint_def.restype = None
+    lib.ns_create_revolute_joint_def.argtypes = [P, ctypes.POINTER(RevoluteJointDef)]
     lib.ns_world_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
     lib.ns_world_synchronize.argtypes = [P]
     lib.ns_world_get_bodies.argtypes = [P, P, P, P, P]
@@ -168,6 +204,7 @@ class World:
     def __init__(self, world_def=None, **overrides):
         self._lib = load_library()
         d = world_def if world_def is not None else default_world_def(**overrides)
+        self._def = d
         self._w = self._lib.ns_world_create(ctypes.byref(d))
         if not self._w:
             raise NsError(1, self._lib.ns_last_error(None).decode())
@@ -226,10 +263,22 @@ class World:
 
     def create_revolute(self, body_a, body_b, frame_a, frame_b, enable_limit=False, lower=0.0, upper=0.0,
                         enable_spring=False, hertz=0.0, damping_ratio=0.0, max_motor_torque=0.0,
-                        collide_connected=False):
-        return self._id(self._lib.ns_create_revolute_joint(
-            self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b), int(enable_limit), lower, upper,
-            int(enable_spring), hertz, damping_ratio, max_motor_torque, int(collide_connected)))
+                        collide_connected=False, enable_motor=None, motor_speed=0.0, target_angle=0.0,
+                        constraint_hertz=None, constraint_damping_ratio=None):
+        """A revolute joint. With only the first arguments this is ns_create_revolute_joint (a
+        positive max_motor_torque is a drag motor of speed 0, softness from the world); any of
+        enable_motor, motor_speed, target_angle or the constraint softness goes through
+        ns_create_revolute_joint_def with the whole definition."""
+        if enable_motor is None and motor_speed == 0.0 and target_angle == 0.0 and constraint_hertz is None \
+                and constraint_damping_ratio is None:
+            return self._id(self._lib.ns_create_revolute_joint(
+                self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b), int(enable_limit), lower, upper,
+                int(enable_spring), hertz, damping_ratio, max_motor_torque, int(collide_connected)))
+        d = revolute_def(RevoluteJointDef, self._def.joint_hertz, self._def.joint_damping_ratio, body_a, body_b,
+                         frame_a, frame_b, enable_limit, lower, upper, enable_spring, hertz, damping_ratio,
+                         max_motor_torque, collide_connected, enable_motor, motor_speed, target_angle,
+                         constraint_hertz, constraint_damping_ratio)
+        return self._id(self._lib.ns_create_revolute_joint_def(self._w, ctypes.byref(d)))
 
     # stepping and readback ----------------------------------------------
     def step(self, dt=1.0 / 60.0, substeps=4):

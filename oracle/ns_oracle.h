@@ -57,6 +57,22 @@ int nso_create_revolute(nso_world* w, int body_a, int body_b, const float frame_
                         const float frame_b[7], int enable_limit, float lower, float upper,
                         int enable_spring, float hertz, float damping_ratio, float drag_torque,
                         int collide_connected);
+/* The whole RevoluteJointDef (types/joint_defs.rs:154 with its JointDef base :30); same layout
+ * as the product's ns_revolute_joint_def. */
+typedef struct {
+  int body_a, body_b;
+  float local_frame_a[7], local_frame_b[7];
+  float constraint_hertz, constraint_damping_ratio;
+  int collide_connected;
+  float target_angle;
+  int enable_spring;
+  float hertz, damping_ratio;
+  int enable_limit;
+  float lower_angle, upper_angle;
+  int enable_motor;
+  float max_motor_torque, motor_speed;
+} nso_revolute_def;
+int nso_create_revolute_def(nso_world* w, const nso_revolute_def* def);
 void nso_step(nso_world* w, float dt, int substeps);
 /* Host threads of the colour-parallel loops (all worlds of the process; default 1). */
 void nso_set_threads(int threads);

@@ -1858,12 +1858,31 @@ int nso_create_capsule(nso_world* w, int body, const nso_shape_def* def, const f
   return create_shape(w, body, def, s);
 }
 
+static int add_revolute(nso_world* w, Joint j);
+
 int nso_create_revolute(nso_world* w, int body_a, int body_b, const float fa[7], const float fb[7],
                         int enable_limit, float lower, float upper, int enable_spring, float hertz,
                         float damping_ratio, float drag_torque, int collide_connected) {
   Joint j = make_revolute_joint(body_a, body_b, fa, fb, enable_limit != 0, lower, upper,
                                 enable_spring != 0, hertz, damping_ratio, drag_torque,
                                 collide_connected != 0, w->def.joint_hertz, w->def.joint_damping_ratio);
+  return add_revolute(w, j);
+}
+
+// revolute_joint.rs:161-181 create_revolute_joint: every RevoluteJointDef field is copied
+int nso_create_revolute_def(nso_world* w, const nso_revolute_def* d) {
+  Joint j = make_revolute_joint(d->body_a, d->body_b, d->local_frame_a, d->local_frame_b, d->enable_limit != 0,
+                                d->lower_angle, d->upper_angle, d->enable_spring != 0, d->hertz, d->damping_ratio,
+                                d->max_motor_torque, d->collide_connected != 0, d->constraint_hertz,
+                                d->constraint_damping_ratio);
+  j.enable_motor = d->enable_motor != 0;
+  j.motor_speed = d->motor_speed;
+  j.target_angle = d->target_angle;
+  return add_revolute(w, j);
+}
+
+static int add_revolute(nso_world* w, Joint j) {
+  int body_a = j.body_a, body_b = j.body_b;
   int id = (int)w->joints.size();
   j.id = id;
   // joint.rs:164 create_joint: awake joints go to the graph; bodies' joint counts grow.

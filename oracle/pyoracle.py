@@ -73,6 +73,38 @@ class ShapeDef(ctypes.Structure):
     ]
 
 
+class RevoluteDef(ctypes.Structure):
+    """nso_revolute_def: the reference's RevoluteJointDef (types/joint_defs.rs:154)."""
+    _fields_ = [
+        ("body_a", ctypes.c_int), ("body_b", ctypes.c_int),
+        ("local_frame_a", ctypes.c_float * 7), ("local_frame_b", ctypes.c_float * 7),
+        ("constraint_hertz", ctypes.c_float), ("constraint_damping_ratio", ctypes.c_float),
+        ("collide_connected", ctypes.c_int),
+        ("target_angle", ctypes.c_float),
+        ("enable_spring", ctypes.c_int), ("hertz", ctypes.c_float), ("damping_ratio", ctypes.c_float),
+        ("enable_limit", ctypes.c_int), ("lower_angle", ctypes.c_float), ("upper_angle", ctypes.c_float),
+        ("enable_motor", ctypes.c_int), ("max_motor_torque", ctypes.c_float), ("motor_speed", ctypes.c_float),
+    ]
+
+
+def _revolute_def(default_hertz, default_zeta, body_a, body_b, frame_a, frame_b, enable_limit, lower, upper,
+                  enable_spring, hertz, damping_ratio, max_motor_torque, collide_connected, enable_motor,
+                  motor_speed, target_angle, constraint_hertz, constraint_damping_ratio):
+    d = RevoluteDef()
+    d.body_a, d.body_b = body_a, body_b
+    d.local_frame_a = (ctypes.c_float * 7)(*frame_a)
+    d.local_frame_b = (ctypes.c_float * 7)(*frame_b)
+    d.constraint_hertz = default_hertz if constraint_hertz is None else constraint_hertz
+    d.constraint_damping_ratio = default_zeta if constraint_damping_ratio is None else constraint_damping_ratio
+    d.collide_connected = int(collide_connected)
+    d.target_angle = target_angle
+    d.enable_spring, d.hertz, d.damping_ratio = int(enable_spring), hertz, damping_ratio
+    d.enable_limit, d.lower_angle, d.upper_angle = int(enable_limit), lower, upper
+    d.enable_motor = int(max_motor_torque > 0.0) if enable_motor is None else int(enable_motor)
+    d.max_motor_torque, d.motor_speed = max_motor_torque, motor_speed
+    return d
+
+
 _F3 = ctypes.c_float * 3
 _F7 = ctypes.c_float * 7
 _lib = None
@@ -117,6 +149,7 @@ def load():
     lib.nso_create_revolute.argtypes = [P, ctypes.c_int, ctypes.c_int, _F7, _F7, ctypes.c_int, ctypes.c_float,
                                         ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                         ctypes.c_float, ctypes.c_int]
+    lib.nso_create_revolute_def.argtypes = [P, ctypes.POINTER(RevoluteDef)]
     lib.nso_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
     lib.nso_state_hash.argtypes = [P]
     lib.nso_state_hash.restype = ctypes.c_uint64
@@ -155,6 +188,7 @@ class OracleWorld:
         for k, v in overrides.items():
             if hasattr(d, k):
                 setattr(d, k, v)
+        self._def = d
         self._w = self._lib.nso_create(ctypes.byref(d))
         self.body_types = []
 
@@ -200,10 +234,18 @@ class OracleWorld:
 
     def create_revolute(self, body_a, body_b, frame_a, frame_b, enable_limit=False, lower=0.0, upper=0.0,
                         enable_spring=False, hertz=0.0, damping_ratio=0.0, max_motor_torque=0.0,
-                        collide_connected=False):
-        return self._lib.nso_create_revolute(self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b),
-                                             int(enable_limit), lower, upper, int(enable_spring), hertz,
-                                             damping_ratio, max_motor_torque, int(collide_connected))
+                        collide_connected=False, enable_motor=None, motor_speed=0.0, target_angle=0.0,
+                        constraint_hertz=None, constraint_damping_ratio=None):
+        if enable_motor is None and motor_speed == 0.0 and target_angle == 0.0 and constraint_hertz is None \
+                and constraint_damping_ratio is None:
+            return self._lib.nso_create_revolute(self._w, body_a, body_b, _F7(*frame_a), _F7(*frame_b),
+                                                 int(enable_limit), lower, upper, int(enable_spring), hertz,
+                                                 damping_ratio, max_motor_torque, int(collide_connected))
+        d = _revolute_def(self._def.joint_hertz, self._def.joint_damping_ratio, body_a, body_b, frame_a, frame_b,
+                          enable_limit, lower, upper, enable_spring, hertz, damping_ratio, max_motor_torque,
+                          collide_connected, enable_motor, motor_speed, target_angle, constraint_hertz,
+                          constraint_damping_ratio)
+        return self._lib.nso_create_revolute_def(self._w, ctypes.byref(d))
 
     def step(self, dt=1.0 / 60.0, substeps=4):
         self._lib.nso_step(self._w, dt, substeps)

@@ -290,6 +290,26 @@ def test_barrier_timeout_is_reported_and_context_survives():
     _both(lambda w: scenes.box_pyramid(w, base=3), steps=2)
 
 
+def test_spring_limit_motor_revolute_matches_oracle():
+    """The scene of revolute_joint_tests.rs:21-62 (spring 4 Hz / 0.6, motor 50 N m at 1 rad/s,
+    limit +-0.5 rad, initial spin) built through ns_create_revolute_joint_def: 120 steps equal
+    to the oracle's, bit for bit, every step."""
+    g = World(default_world_def(gravity=(0.0, -10.0, 0.0)))
+    o = pyoracle.OracleWorld(gravity=(0.0, -10.0, 0.0), enable_continuous=True)
+    for w in (g, o):
+        a = w.create_body(type=0, position=(0.0, 3.0, 0.0))
+        b = w.create_body(type=2, position=(1.5, 3.0, 0.0), angular_velocity=(1.0, 0.5, 0.0))
+        w.create_box(b, 0.2, 0.2, 0.2, density=1000.0)
+        w.create_revolute(a, b, (1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0), (-0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0),
+                          enable_spring=True, hertz=4.0, damping_ratio=0.6, enable_motor=True,
+                          max_motor_torque=50.0, motor_speed=1.0, enable_limit=True, lower=-0.5, upper=0.5)
+    for _ in range(120):
+        g.step(DT, 4)
+        o.step(DT, 4)
+        assert g.state_hash() == o.state_hash()
+    g.close()
+
+
 def test_nonfinite_state_is_reported():
     """A NaN force reaches finalize's finite check (the reference asserts finite velocities
     there, solver_integration.rs:626-627): the next synchronising call reports
