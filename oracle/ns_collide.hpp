@@ -21,11 +21,11 @@ struct Hull {
   Plane planes[6];
   // SoA copies padded to a multiple of 8 (hull.rs:231 hull_soa_stride);
   // normals beyond face_count are zero (hull.rs:833-837).
-  float vx[8], vy[8], vz[8];
-  float nx[8], ny[8], nz[8];
-  float edge_cosines[12];  // box hulls never fill these: zero (hull.rs:754)
+  real vx[8], vy[8], vz[8];
+  real nx[8], ny[8], nz[8];
+  real edge_cosines[12];  // box hulls never fill these: zero (hull.rs:754)
   AABB bounds;
-  float volume = 0, surface_area = 0, inner_radius = 0;
+  real volume = 0, surface_area = 0, inner_radius = 0;
   V3 center;
   M3 central_inertia;
 };
@@ -41,19 +41,19 @@ static const uint8_t kBoxEdgeData[24][4] = {
 static const uint8_t kBoxFaceEdges[6] = {0, 8, 16, 20, 19, 21};
 
 // geometry_queries.rs:81
-inline M3 box_inertia(float mass, V3 mn, V3 mx) {
+inline M3 box_inertia(real mass, V3 mn, V3 mx) {
   V3 d = mx - mn;
-  float ixx = mass * (d.y * d.y + d.z * d.z) / 12.0f;
-  float iyy = mass * (d.x * d.x + d.z * d.z) / 12.0f;
-  float izz = mass * (d.x * d.x + d.y * d.y) / 12.0f;
+  real ixx = mass * (d.y * d.y + d.z * d.z) / 12.0f;
+  real iyy = mass * (d.x * d.x + d.z * d.z) / 12.0f;
+  real izz = mass * (d.x * d.x + d.y * d.y) / 12.0f;
   return diag(ixx, iyy, izz);
 }
 
 // hull.rs:754 make_transformed_box_hull with the identity transform
-inline Hull make_box_hull(float hx, float hy, float hz) {
+inline Hull make_box_hull(real hx, real hy, real hz) {
   Hull h;
   Xf t = xf(v3(0, 0, 0), qid());
-  float min_h = 0.2f * linear_slop();
+  real min_h = 0.2f * linear_slop();
   V3 e = max3(v3(min_h, min_h, min_h), v3(hx, hy, hz));
   h.vertex_count = 8; h.edge_count = 24; h.face_count = 6;
   for (int i = 0; i < 8; ++i) h.vertex_edge[i] = kBoxVertexEdges[i];
@@ -100,9 +100,9 @@ inline Hull make_box_hull(float hx, float hy, float hz) {
 // hull.rs:488
 inline int find_hull_support_vertex(const Hull& h, V3 d) {
   int best = -1;
-  float best_dot = -kFltMax;
+  real best_dot = -kFltMax;
   for (int i = 0; i < h.vertex_count; ++i) {
-    float p = d.x * h.vx[i] + d.y * h.vy[i] + d.z * h.vz[i];
+    real p = d.x * h.vx[i] + d.y * h.vy[i] + d.z * h.vz[i];
     if (p > best_dot) { best_dot = p; best = i; }
   }
   return best;
@@ -110,9 +110,9 @@ inline int find_hull_support_vertex(const Hull& h, V3 d) {
 // hull.rs:505
 inline int find_hull_support_face(const Hull& h, V3 d) {
   int best = -1;
-  float best_dot = -kFltMax;
+  real best_dot = -kFltMax;
   for (int i = 0; i < h.face_count; ++i) {
-    float p = dot(h.planes[i].n, d);
+    real p = dot(h.planes[i].n, d);
     if (p > best_dot) { best_dot = p; best = i; }
   }
   return best;
@@ -124,16 +124,16 @@ enum SepFeature : uint8_t {
   kInvalidAxis = 0, kBacksideAxis, kFaceAxisA, kFaceAxisB, kEdgePairAxis, kClosestPointsAxis,
   kManualFaceAxisA, kManualFaceAxisB, kManualEdgePairAxis
 };
-struct SATCache { float separation = 0; uint8_t type = kInvalidAxis, index_a = 0, index_b = 0, hit = 0; };
+struct SATCache { real separation = 0; uint8_t type = kInvalidAxis, index_a = 0, index_b = 0, hit = 0; };
 struct FeaturePair { uint8_t owner1 = 0, index1 = 0, owner2 = 0, index2 = 0; };
-struct LocalPoint { V3 point; float separation; FeaturePair pair; };
+struct LocalPoint { V3 point; real separation; FeaturePair pair; };
 struct LocalManifold {
   V3 normal = {0, 0, 0};
   LocalPoint points[4];
   int point_count = 0;
 };
-struct ClipVertex { V3 position = {0, 0, 0}; float separation = 0; FeaturePair pair; };
-struct SepAxis { V3 normal; float separation; int index_a, index_b; uint8_t kind; };
+struct ClipVertex { V3 position = {0, 0, 0}; real separation = 0; FeaturePair pair; };
+struct SepAxis { V3 normal; real separation; int index_a, index_b; uint8_t kind; };
 struct AxisQuery { SepAxis face_a, face_b, edge; uint8_t separated_feature; };
 
 inline uint32_t make_feature_id(FeaturePair p) {                                   // manifold.rs:58
@@ -154,7 +154,7 @@ inline FeaturePair flip_pair(FeaturePair p) {                                   
 // manifold.rs:117
 inline int find_incident_face(const Hull& h, V3 ref_n, int vertex_index) {
   int min_edge = -1;
-  float min_proj = kFltMax;
+  real min_proj = kFltMax;
   int edge_index = h.vertex_edge[vertex_index];
   int start = edge_index;
   V3 origin = h.points[h.edges[edge_index].origin];
@@ -163,7 +163,7 @@ inline int find_incident_face(const Hull& h, V3 ref_n, int vertex_index) {
     HalfEdge tw = h.edges[e.twin];
     V3 to = h.points[tw.origin];
     V3 axis = normalize(to - origin);
-    float proj = absf(dot(axis, ref_n));
+    real proj = absf(dot(axis, ref_n));
     if (proj < min_proj) { min_edge = edge_index; min_proj = proj; }
     edge_index = tw.next;
     if (edge_index == start) break;
@@ -178,22 +178,22 @@ inline int find_incident_face(const Hull& h, V3 ref_n, int vertex_index) {
 inline int clip_polygon(ClipVertex* out, const ClipVertex* poly, int count, Plane clip, int edge,
                         Plane ref) {
   ClipVertex v1 = poly[count - 1];
-  float d1 = plane_sep(clip, v1.position);
+  real d1 = plane_sep(clip, v1.position);
   int n = 0;
   for (int i = 0; i < count; ++i) {
     ClipVertex v2 = poly[i];
-    float d2 = plane_sep(clip, v2.position);
+    real d2 = plane_sep(clip, v2.position);
     if (d1 <= 0.0f && d2 <= 0.0f) {
       out[n++] = v2;
     } else if (d1 <= 0.0f && d2 > 0.0f) {
-      float f = d1 / (d1 - d2);
+      real f = d1 / (d1 - d2);
       V3 pos = mul_add(v1.position, f, v2.position - v1.position);
       ClipVertex v;
       v.position = pos; v.separation = plane_sep(ref, pos); v.pair = v2.pair;
       v.pair.owner2 = 0; v.pair.index2 = (uint8_t)edge;
       out[n++] = v;
     } else if (d2 <= 0.0f && d1 > 0.0f) {
-      float f = d1 / (d1 - d2);
+      real f = d1 / (d1 - d2);
       V3 pos = mul_add(v1.position, f, v2.position - v1.position);
       ClipVertex v;
       v.position = pos; v.separation = plane_sep(ref, pos); v.pair = v1.pair;
@@ -210,11 +210,11 @@ inline int clip_polygon(ClipVertex* out, const ClipVertex* poly, int count, Plan
 inline int clip_segment(ClipVertex* seg, Plane p) {
   int n = 0;
   ClipVertex a = seg[0], b = seg[1];
-  float d1 = plane_sep(p, a.position), d2 = plane_sep(p, b.position);
+  real d1 = plane_sep(p, a.position), d2 = plane_sep(p, b.position);
   if (d1 <= 0.0f) seg[n++] = a;
   if (d2 <= 0.0f) seg[n++] = b;
   if (d1 * d2 < 0.0f) {
-    float t = d1 / (d1 - d2);
+    real t = d1 / (d1 - d2);
     seg[n].position = (1.0f - t) * a.position + t * b.position;
     seg[n].pair = d1 > 0.0f ? a.pair : b.pair;
     n++;
@@ -243,15 +243,15 @@ inline int clip_segment_to_hull_face(ClipVertex* seg, const Hull& h, int ref_fac
 }
 
 // convex_manifold.rs:198
-inline bool test_edge_candidate_sorted(float a1, float a2, float c, float bound) {
-  float hi = maxf(a1, a2), lo = minf(a1, a2);
+inline bool test_edge_candidate_sorted(real a1, real a2, real c, real bound) {
+  real hi = maxf(a1, a2), lo = minf(a1, a2);
   bool exterior = hi >= bound;
-  float u = lo - c * hi;
+  real u = lo - c * hi;
   bool max_is_interior = u >= 0.0f;
-  float s = 1.0f - c * c;
-  float bound_term = (bound - hi) * (bound + hi);
-  float lhs = u * u;
-  float rhs = bound_term * s;
+  real s = 1.0f - c * c;
+  real bound_term = (bound - hi) * (bound + hi);
+  real lhs = u * u;
+  real rhs = bound_term * s;
   bool max_beats_bound = lhs >= rhs;
   bool nearly_parallel = s < 1e-4f;
   bool interior = max_is_interior && (max_beats_bound || nearly_parallel);
@@ -260,19 +260,19 @@ inline bool test_edge_candidate_sorted(float a1, float a2, float c, float bound)
 
 inline int round_up4(int n) { return (n + 3) & ~3; }
 
-inline void get_face_dots(const Hull& h, V3 d, float* dots) {                     // :227
+inline void get_face_dots(const Hull& h, V3 d, real* dots) {                     // :227
   for (int i = 0; i < h.face_count; ++i) dots[i] = d.x * h.nx[i] + d.y * h.ny[i] + d.z * h.nz[i];
 }
-inline void get_face_plane_separations(const Hull& h, V3 c, float* s) {           // :236
+inline void get_face_plane_separations(const Hull& h, V3 c, real* s) {           // :236
   get_face_dots(h, c, s);
   for (int i = 0; i < h.face_count; ++i) s[i] -= h.planes[i].off;
 }
-inline int filter_edge_candidates(const Hull& h, const float* ps, float bound, int* idx, int count) {
+inline int filter_edge_candidates(const Hull& h, const real* ps, real bound, int* idx, int count) {
   int kept = 0;
   for (int k = 0; k < count; ++k) {
     int i = idx[k];
     int i1 = h.edges[i].face, i2 = h.edges[i + 1].face;
-    float c = h.edge_cosines[i >> 1];
+    real c = h.edge_cosines[i >> 1];
     idx[kept] = i;
     if (test_edge_candidate_sorted(ps[i1], ps[i2], c, bound)) kept++;
   }
@@ -280,31 +280,33 @@ inline int filter_edge_candidates(const Hull& h, const float* ps, float bound, i
 }
 
 // convex_manifold.rs:277 -- the vertex index rides in the low 7 mantissa bits
-inline float get_support_wide(V3 n, const float* vx, const float* vy, const float* vz, int cnt,
-                              float bias, int* vi) {
-  const uint32_t mask = (1u << 7) - 1;
-  float min_value = INFINITY;
+inline real get_support_wide(V3 n, const real* vx, const real* vy, const real* vz, int cnt,
+                              real bias, int* vi) {
+  // an unsigned integer as wide as the scalar carries its bits
+  typedef typename std::conditional<sizeof(real) == 4, uint32_t, uint64_t>::type bits_t;
+  const bits_t mask = (bits_t(1) << 7) - 1;
+  real min_value = INFINITY;
   for (int i = 0; i < cnt; ++i) {
-    float d = n.x * vx[i] + n.y * vy[i] + n.z * vz[i];
-    float value = bias - d;
-    uint32_t bits;
-    std::memcpy(&bits, &value, 4);
-    bits = (bits & ~mask) | ((uint32_t)i & mask);
-    float aug;
-    std::memcpy(&aug, &bits, 4);
+    real d = n.x * vx[i] + n.y * vy[i] + n.z * vz[i];
+    real value = bias - d;
+    bits_t bits;
+    std::memcpy(&bits, &value, sizeof(real));
+    bits = (bits & ~mask) | ((bits_t)i & mask);
+    real aug;
+    std::memcpy(&aug, &bits, sizeof(real));
     if (aug < min_value) min_value = aug;
   }
-  uint32_t mb;
-  std::memcpy(&mb, &min_value, 4);
+  bits_t mb;
+  std::memcpy(&mb, &min_value, sizeof(real));
   int v = (int)(mb & mask);
   *vi = v;
   return n.x * vx[v] + n.y * vy[v] + n.z * vz[v];
 }
 
-inline float get_face_separation(V3 dir, float plane_sep_v, const float* vx, const float* vy,
-                                 const float* vz, int n, V3 center, V3 extents, int* vi) {
-  float bias = dot(dir, center) + 1.0625f * dot(abs3(dir), extents);
-  float support = get_support_wide(dir, vx, vy, vz, n, bias, vi);
+inline real get_face_separation(V3 dir, real plane_sep_v, const real* vx, const real* vy,
+                                 const real* vz, int n, V3 center, V3 extents, int* vi) {
+  real bias = dot(dir, center) + 1.0625f * dot(abs3(dir), extents);
+  real support = get_support_wide(dir, vx, vy, vz, n, bias, vi);
   return plane_sep_v - support;
 }
 
@@ -312,35 +314,35 @@ inline float get_face_separation(V3 dir, float plane_sep_v, const float* vx, con
 inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, bool early) {
   M3 r = matrix_from_quat(xb.q);
   M3 inv_r = transpose(r);
-  float spec = speculative_distance();
+  real spec = speculative_distance();
   AxisQuery res;
   res.face_a = {v3(0, 0, 0), -INFINITY, kNull, kNull, kFaceAxisA};
   res.face_b = {v3(0, 0, 0), -INFINITY, kNull, kNull, kFaceAxisB};
   res.edge = {v3(0, 0, 0), -INFINITY, kNull, kNull, kEdgePairAxis};
   res.separated_feature = kInvalidAxis;
 
-  float dot_a[8], dot_b[8], pd_a[8], pd_b[8];
+  real dot_a[8], dot_b[8], pd_a[8], pd_b[8];
   int eia[16], eib[16];
 
   int wide_vb = round_up4(hb.vertex_count);
   V3 c_b = aabb_center(hb.bounds), h_b = aabb_extents(hb.bounds);
   V3 delta_center = mul_mv(r, hb.center) + xb.p - ha.center;
-  float center_distance = length(delta_center);
-  float radius = ha.inner_radius + hb.inner_radius;
-  float radius_bound = radius - (linear_slop() + 0.001f * (center_distance + radius));
+  real center_distance = length(delta_center);
+  real radius = ha.inner_radius + hb.inner_radius;
+  real radius_bound = radius - (linear_slop() + 0.001f * (center_distance + radius));
 
   get_face_dots(ha, delta_center, dot_a);
   int seed_a = 0;
-  float max_dot_a = dot_a[0];
+  real max_dot_a = dot_a[0];
   for (int i = 1; i < ha.face_count; ++i)
     if (dot_a[i] > max_dot_a) { max_dot_a = dot_a[i]; seed_a = i; }
 
-  float floor_a = -INFINITY, seed_sep_a = -INFINITY;
+  real floor_a = -INFINITY, seed_sep_a = -INFINITY;
   int seed_vb = 0;
   if (early) {
     Plane p = ha.planes[seed_a];
     V3 dir = -mul_mv(inv_r, p.n);
-    float ps = dot(p.n, xb.p) - p.off;
+    real ps = dot(p.n, xb.p) - p.off;
     seed_sep_a = get_face_separation(dir, ps, hb.vx, hb.vy, hb.vz, wide_vb, c_b, h_b, &seed_vb);
     floor_a = minf(seed_sep_a, spec);
   }
@@ -348,10 +350,10 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
     if (dot_a[i] - radius_bound < maxf(floor_a, res.face_a.separation)) continue;
     Plane p = ha.planes[i];
     int vi = seed_vb;
-    float sep = seed_sep_a;
+    real sep = seed_sep_a;
     if (!early || i != seed_a) {
       V3 dir = -mul_mv(inv_r, p.n);
-      float ps = dot(p.n, xb.p) - p.off;
+      real ps = dot(p.n, xb.p) - p.off;
       sep = get_face_separation(dir, ps, hb.vx, hb.vy, hb.vz, wide_vb, c_b, h_b, &vi);
     }
     if (sep > res.face_a.separation) {
@@ -365,16 +367,16 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
   V3 c_a = aabb_center(ha.bounds), h_a = aabb_extents(ha.bounds);
   get_face_dots(hb, -mul_mv(inv_r, delta_center), dot_b);
   int seed_b = 0;
-  float max_dot_b = dot_b[0];
+  real max_dot_b = dot_b[0];
   for (int i = 1; i < hb.face_count; ++i)
     if (dot_b[i] > max_dot_b) { max_dot_b = dot_b[i]; seed_b = i; }
 
-  float floor_b = -INFINITY, seed_sep_b = -INFINITY;
+  real floor_b = -INFINITY, seed_sep_b = -INFINITY;
   int seed_va = 0;
   if (early) {
     Plane p = hb.planes[seed_b];
     V3 dir = -mul_mv(r, p.n);
-    float ps = dot(dir, xb.p) - p.off;
+    real ps = dot(dir, xb.p) - p.off;
     seed_sep_b = get_face_separation(dir, ps, ha.vx, ha.vy, ha.vz, wide_va, c_a, h_a, &seed_va);
     floor_b = maxf(seed_sep_b, res.face_a.separation);
     floor_b = minf(floor_b, spec);
@@ -384,9 +386,9 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
     Plane p = hb.planes[i];
     V3 dir = -mul_mv(r, p.n);
     int vi = seed_va;
-    float sep = seed_sep_b;
+    real sep = seed_sep_b;
     if (!early || i != seed_b) {
-      float ps = dot(dir, xb.p) - p.off;
+      real ps = dot(dir, xb.p) - p.off;
       sep = get_face_separation(dir, ps, ha.vx, ha.vy, ha.vz, wide_va, c_a, h_a, &vi);
     }
     if (sep > res.face_b.separation) {
@@ -397,29 +399,29 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
   }
 
   int na = 0, nb = 0;
-  float max_face_sep = maxf(res.face_a.separation, res.face_b.separation);
-  float bound_slack = radius - radius_bound;
-  float threshold_a = early ? max_face_sep + hb.inner_radius - bound_slack : -INFINITY;
-  float threshold_b = early ? max_face_sep + ha.inner_radius - bound_slack : -INFINITY;
+  real max_face_sep = maxf(res.face_a.separation, res.face_b.separation);
+  real bound_slack = radius - radius_bound;
+  real threshold_a = early ? max_face_sep + hb.inner_radius - bound_slack : -INFINITY;
+  real threshold_b = early ? max_face_sep + ha.inner_radius - bound_slack : -INFINITY;
   V3 center_b_in_a = mul_mv(r, hb.center) + xb.p;
   V3 center_a_in_b = mul_mv(inv_r, ha.center - xb.p);
   get_face_plane_separations(ha, center_b_in_a, pd_a);
   get_face_plane_separations(hb, center_a_in_b, pd_b);
   for (int i = 0; i < ha.edge_count; i += 2) {
     int i1 = ha.edges[i].face, i2 = ha.edges[i + 1].face;
-    float c = ha.edge_cosines[i >> 1];
+    real c = ha.edge_cosines[i >> 1];
     eia[na] = i;
     if (test_edge_candidate_sorted(pd_a[i1], pd_a[i2], c, threshold_a)) na++;
   }
   for (int i = 0; i < hb.edge_count; i += 2) {
     int i1 = hb.edges[i].face, i2 = hb.edges[i + 1].face;
-    float c = hb.edge_cosines[i >> 1];
+    real c = hb.edge_cosines[i >> 1];
     eib[nb] = i;
     if (test_edge_candidate_sorted(pd_b[i1], pd_b[i2], c, threshold_b)) nb++;
   }
 
   if (early && nb * ((na + 3) >> 2) >= 10) {
-    float probe_bound =
+    real probe_bound =
         max_face_sep - (0.1f * linear_slop() + 0.001f * absf(center_distance + radius));
     int vb = res.face_a.index_b != kNull ? res.face_a.index_b : seed_vb;
     V3 probe_b = v3(hb.vx[vb], hb.vy[vb], hb.vz[vb]);
@@ -435,7 +437,7 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
 
   // negative_transform_from_soa (convex_manifold.rs:340): rows of r dotted with the input
   V3 r0 = v3(r.cx.x, r.cy.x, r.cz.x), r1 = v3(r.cx.y, r.cy.y, r.cz.y), r2 = v3(r.cx.z, r.cy.z, r.cz.z);
-  float bfx[8], bfy[8], bfz[8], bwx[8], bwy[8], bwz[8];
+  real bfx[8], bfy[8], bfz[8], bwx[8], bwy[8], bwz[8];
   int wide_fb = round_up4(hb.face_count);
   for (int i = 0; i < wide_fb; ++i) {
     V3 v = v3(hb.nx[i], hb.ny[i], hb.nz[i]);
@@ -449,8 +451,8 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
     bwx[i] = -o.x; bwy[i] = -o.y; bwz[i] = -o.z;
   }
   V3 an0[16], an1[16], ad[16], av0[16];
-  float atol[16];
-  float sq_tol = kParallelEdgeTol * kParallelEdgeTol;
+  real atol[16];
+  real sq_tol = kParallelEdgeTol * kParallelEdgeTol;
   for (int k = 0; k < na; ++k) {
     HalfEdge e = ha.edges[eia[k]], tw = ha.edges[eia[k] + 1];
     an0[k] = ha.planes[e.face].n;
@@ -460,8 +462,8 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
     av0[k] = v3(ha.vx[v0], ha.vy[v0], ha.vz[v0]);
     atol[k] = sq_tol * (ad[k].x * ad[k].x + ad[k].y * ad[k].y + ad[k].z * ad[k].z);
   }
-  float ls = linear_slop();
-  float eps = -ls * ls;
+  real ls = linear_slop();
+  real eps = -ls * ls;
   for (int j = 0; j < nb; ++j) {
     HalfEdge e = hb.edges[eib[j]], tw = hb.edges[eib[j] + 1];
     int f0 = e.face, f1 = tw.face, v0 = e.origin, v1 = tw.origin;
@@ -472,18 +474,18 @@ inline AxisQuery compute_separating_axis(const Hull& ha, const Hull& hb, Xf xb, 
     V3 dc = bv1 - bv0;
     for (int i = 0; i < na; ++i) {
       V3 d = ad[i];
-      float cba = dot(c, d), dba = dot(dn, d);
+      real cba = dot(c, d), dba = dot(dn, d);
       if (cba * dba >= eps) continue;
-      float adc = dot(an0[i], dc), bdc = dot(an1[i], dc);
+      real adc = dot(an0[i], dc), bdc = dot(an1[i], dc);
       if (adc * bdc >= eps || cba * bdc >= eps) continue;
-      float max_cd = maxf(cba * cba, dba * dba);
+      real max_cd = maxf(cba * cba, dba * dba);
       if (max_cd <= atol[i]) continue;
-      float t = -cba / (dba - cba);
+      real t = -cba / (dba - cba);
       V3 n = mul_add(c, t, dn - c);
-      float len2 = dot(n, n);
-      float inv = 1.0f / std::sqrt(len2);
+      real len2 = dot(n, n);
+      real inv = 1.0f / std::sqrt(len2);
       n = inv * n;
-      float sep = -dot(av0[i] + bv0, n);
+      real sep = -dot(av0[i] + bv0, n);
       if (sep > res.edge.separation) {
         res.edge.normal = n; res.edge.separation = sep;
         res.edge.index_a = eia[i]; res.edge.index_b = eib[j];
@@ -502,15 +504,15 @@ inline void reduce_manifold_points(LocalManifold* m, LocalPoint* pts, int count)
     return;
   }
   V3 normal = m->normal;
-  float spec = speculative_distance();
-  float tol_sqr = spec * spec;
-  const float bias = 0.95f;
+  real spec = speculative_distance();
+  real tol_sqr = spec * spec;
+  const real bias = 0.95f;
   int best = kNull;
-  float best_score = -kFltMax;
+  real best_score = -kFltMax;
   V3 sd = arbitrary_perp(normal);
   for (int i = 0; i < count; ++i) {
     if (pts[i].separation > spec) continue;
-    float score = -pts[i].separation + dot(sd, pts[i].point);
+    real score = -pts[i].separation + dot(sd, pts[i].point);
     if (bias * score > best_score) { best = i; best_score = score; }
   }
   if (best == kNull) { m->point_count = 0; return; }
@@ -524,9 +526,9 @@ inline void reduce_manifold_points(LocalManifold* m, LocalPoint* pts, int count)
   for (int i = 0; i < count; ++i) {
     V3 d = pts[i].point - a;
     V3 v = mul_sub(d, dot(d, normal), normal);
-    float dsq = length_sq(v);
-    float sep = maxf(0.0f, -pts[i].separation);
-    float score = dsq + 4.0f * sep * sep;
+    real dsq = length_sq(v);
+    real sep = maxf(0.0f, -pts[i].separation);
+    real score = dsq + 4.0f * sep * sep;
     if (bias * score > best_score) { best_score = score; best = i; }
   }
   if (best_score < tol_sqr) return;
@@ -537,12 +539,12 @@ inline void reduce_manifold_points(LocalManifold* m, LocalPoint* pts, int count)
   V3 b = m->points[1].point;
 
   best_score = tol_sqr; best = kNull;
-  float best_signed = 0.0f;
+  real best_signed = 0.0f;
   V3 ba = b - a;
   for (int i = 0; i < count; ++i) {
     V3 p = pts[i].point;
-    float signed_area = dot(normal, cross(ba, p - a));
-    float score = absf(signed_area);
+    real signed_area = dot(normal, cross(ba, p - a));
+    real score = absf(signed_area);
     if (bias * score >= best_score) { best_score = score; best = i; best_signed = signed_area; }
   }
   if (best == kNull) return;
@@ -553,13 +555,13 @@ inline void reduce_manifold_points(LocalManifold* m, LocalPoint* pts, int count)
   V3 c = m->points[2].point;
 
   best_score = tol_sqr; best = kNull;
-  float sign = best_signed < 0.0f ? -1.0f : 1.0f;
+  real sign = best_signed < 0.0f ? -1.0f : 1.0f;
   for (int i = 0; i < count; ++i) {
     V3 p = pts[i].point;
-    float u1 = sign * dot(normal, cross(p - a, ba));
-    float u2 = sign * dot(normal, cross(p - b, c - b));
-    float u3 = sign * dot(normal, cross(p - c, a - c));
-    float score = maxf(u1, maxf(u2, u3));
+    real u1 = sign * dot(normal, cross(p - a, ba));
+    real u2 = sign * dot(normal, cross(p - b, c - b));
+    real u3 = sign * dot(normal, cross(p - c, a - c));
+    real score = maxf(u1, maxf(u2, u3));
     if (bias * score > best_score) { best_score = score; best = i; }
   }
   if (best != kNull) {
@@ -618,7 +620,7 @@ inline bool build_face_a_contact(LocalManifold* m, const Hull& ha, const Hull& h
   count = min_i(count, 64);
   m->normal = rp.n;
   const ClipVertex* src = use1 ? poly1 : poly2;
-  float min_sep = kFltMax;
+  real min_sep = kFltMax;
   for (int i = 0; i < count; ++i) {
     LocalPoint p;
     p.point = mul_sub(src[i].position, 0.5f * src[i].separation, rp.n);
@@ -674,7 +676,7 @@ inline bool build_edge_contact(LocalManifold* m, const Hull& ha, const Hull& hb,
   V3 normal = q.normal;
   SegResult r = line_distance(pa, e_a, pb, e_b);
   if (!within_segments(r)) { *cache = SATCache(); return false; }
-  float sep = dot(normal, r.p2 - r.p1);
+  real sep = dot(normal, r.p2 - r.p1);
   V3 point = 0.5f * (r.p1 + r.p2);
   m->normal = normal;
   m->point_count = 1;
@@ -692,8 +694,8 @@ inline bool build_edge_contact(LocalManifold* m, const Hull& ha, const Hull& hb,
 inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf xb, SATCache* cache,
                           int* sat_calls_out) {
   m->point_count = 0;
-  float spec = speculative_distance();
-  float ls = linear_slop();
+  real spec = speculative_distance();
+  real ls = linear_slop();
   cache->hit = 0;
   switch (cache->type) {
     case kInvalidAxis: break;
@@ -702,7 +704,7 @@ inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf x
       V3 sd = -inv_rotate(xb.q, p.n);
       int vi = find_hull_support_vertex(hb, sd);
       V3 support = xf_point(xb, hb.points[vi]);
-      float sep = plane_sep(p, support);
+      real sep = plane_sep(p, support);
       if (sep >= spec) { cache->hit = 1; return; }
       SepAxis fq = {p.n, 0.0f, cache->index_a, vi, kFaceAxisA};
       SATCache local;
@@ -715,7 +717,7 @@ inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf x
       V3 sd = -rotate(xb.q, p.n);
       int vi = find_hull_support_vertex(ha, sd);
       V3 support = inv_xf_point(xb, ha.points[vi]);
-      float sep = plane_sep(p, support);
+      real sep = plane_sep(p, support);
       if (sep >= spec) { cache->hit = 1; return; }
       SepAxis fq = {-p.n, 0.0f, vi, cache->index_b, kFaceAxisB};
       SATCache local;
@@ -736,14 +738,14 @@ inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf x
       V3 e_b = qb - pb;
       V3 ub = rotate(xb.q, hb.planes[e2.face].n);
       V3 vb = rotate(xb.q, hb.planes[t2.face].n);
-      float cba = dot(ub, e_a), dba = dot(vb, e_a);
-      float adc = -dot(ua, e_b), bdc = -dot(va, e_b);
+      real cba = dot(ub, e_a), dba = dot(vb, e_a);
+      real adc = -dot(ua, e_b), bdc = -dot(va, e_b);
       if (cba * dba < 0.0f && adc * bdc < 0.0f && cba * bdc > 0.0f) {
-        float sq = kParallelEdgeTol * kParallelEdgeTol;
+        real sq = kParallelEdgeTol * kParallelEdgeTol;
         if (maxf(cba * cba, dba * dba) >= sq * length_sq(e_a)) {
-          float t = cba / (cba - dba);
+          real t = cba / (cba - dba);
           V3 axis = normalize(lerp(ub, vb, t));
-          float sep = dot(axis, qa - qb);
+          real sep = dot(axis, qa - qb);
           if (sep > spec) { cache->hit = 1; return; }
           SepAxis eq = {-axis, 0.0f, cache->index_a, cache->index_b, kEdgePairAxis};
           SATCache local;
@@ -775,8 +777,8 @@ inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf x
   }
   SepAxis eq = aq.edge;
   if (eq.index_a == kNull) return;
-  float face_sep = maxf(aq.face_a.separation, aq.face_b.separation);
-  float clip_sep = cache->separation;
+  real face_sep = maxf(aq.face_a.separation, aq.face_b.separation);
+  real clip_sep = cache->separation;
   if ((m->point_count == 0 && eq.separation > face_sep) || eq.separation > clip_sep + ls) {
     LocalManifold em;
     SATCache ec;
@@ -792,19 +794,19 @@ inline void collide_hulls(LocalManifold* m, const Hull& ha, const Hull& hb, Xf x
 
 // ---------------------------------------------------------------------------
 // Sphere / capsule pairs (convex_manifold_shapes.rs)
-struct Sphere { V3 center; float radius; };
-struct Capsule { V3 c1, c2; float radius; };
+struct Sphere { V3 center; real radius; };
+struct Capsule { V3 c1, c2; real radius; };
 
 inline void collide_spheres(LocalManifold* m, Sphere a, Sphere b, Xf xb) {        // :21
   m->point_count = 0;
   V3 c1 = a.center, c2 = xf_point(xb, b.center);
-  float tr = a.radius + b.radius;
-  float maxd = tr + speculative_distance();
+  real tr = a.radius + b.radius;
+  real maxd = tr + speculative_distance();
   V3 off = c2 - c1;
-  float dsq = length_sq(off);
+  real dsq = length_sq(off);
   if (dsq > maxd * maxd) return;
   V3 n = v3(0.0f, 1.0f, 0.0f);
-  float d = std::sqrt(dsq);
+  real d = std::sqrt(dsq);
   if (d * d > 1000.0f * kMinPositive) n = (1.0f / d) * off;
   V3 point = 0.5f * (mul_sub(mul_add(c1, a.radius, n) + c2, b.radius, n));
   m->normal = n;
@@ -817,14 +819,14 @@ inline void collide_spheres(LocalManifold* m, Sphere a, Sphere b, Xf xb) {      
 inline void collide_capsule_sphere(LocalManifold* m, Capsule a, Sphere b, Xf xb) { // :74
   m->point_count = 0;
   V3 c = xf_point(xb, b.center);
-  float tr = b.radius + a.radius;
-  float maxd = tr + speculative_distance();
+  real tr = b.radius + a.radius;
+  real maxd = tr + speculative_distance();
   V3 cp = point_to_segment(a.c1, a.c2, c);
   V3 off = c - cp;
-  float dsq = length_sq(off);
+  real dsq = length_sq(off);
   if (dsq > maxd * maxd) return;
   V3 n = v3(0.0f, 1.0f, 0.0f);
-  float d = std::sqrt(dsq);
+  real d = std::sqrt(dsq);
   if (d * d > 1000.0f * kMinPositive) n = (1.0f / d) * off;
   V3 point = 0.5f * mul_add(mul_sub(c, b.radius, n) + cp, a.radius, n);
   m->normal = n;
@@ -835,41 +837,41 @@ inline void collide_capsule_sphere(LocalManifold* m, Capsule a, Sphere b, Xf xb)
 }
 
 // GJK (collision/distance.rs)
-struct SimplexCache { float metric = 0; uint16_t count = 0; uint8_t ia[4] = {0, 0, 0, 0}, ib[4] = {0, 0, 0, 0}; };
-struct SVert { V3 wa, wb, w; float a; int ia, ib; };
+struct SimplexCache { real metric = 0; uint16_t count = 0; uint8_t ia[4] = {0, 0, 0, 0}, ib[4] = {0, 0, 0, 0}; };
+struct SVert { V3 wa, wb, w; real a; int ia, ib; };
 struct Simplex { SVert v[4]; int count = 0; };
-struct DistOut { V3 pa, pb, normal; float distance; };
+struct DistOut { V3 pa, pb, normal; real distance; };
 
 inline int point_support(const V3* pts, int n, V3 axis) {                          // :17/:38
   V3 o = pts[0];
   int mi = 0;
-  float mp = 0.0f;
+  real mp = 0.0f;
   for (int i = 1; i < n; ++i) {
-    float p = dot(axis, pts[i] - o);
+    real p = dot(axis, pts[i] - o);
     if (p > mp) { mi = i; mp = p; }
   }
   return mi;
 }
-inline void bary_edge(V3 a, V3 b, float* u, float* v, float* d) {                  // :58
+inline void bary_edge(V3 a, V3 b, real* u, real* v, real* d) {                  // :58
   V3 ab = b - a;
   *d = dot(ab, ab); *u = dot(b, ab); *v = -dot(a, ab);
 }
-inline void bary_tri(V3 a, V3 b, V3 c, float* u, float* v, float* w, float* d) {   // :67
+inline void bary_tri(V3 a, V3 b, V3 c, real* u, real* v, real* w, real* d) {   // :67
   V3 ab = b - a, ac = c - a;
   V3 bxc = cross(b, c), cxa = cross(c, a), axb = cross(a, b), abxac = cross(ab, ac);
   *d = dot(abxac, abxac); *u = dot(bxc, abxac); *v = dot(cxa, abxac); *w = dot(axb, abxac);
 }
-inline void bary_tet(V3 a, V3 b, V3 c, V3 d, float* u, float* v, float* w, float* x, float* dv) {
+inline void bary_tet(V3 a, V3 b, V3 c, V3 d, real* u, real* v, real* w, real* x, real* dv) {
   V3 ab = b - a, ac = c - a, ad = d - a;
-  float divisor = scalar_triple(ab, ac, ad);
-  float sign = divisor < 0.0f ? -1.0f : 1.0f;
+  real divisor = scalar_triple(ab, ac, ad);
+  real sign = divisor < 0.0f ? -1.0f : 1.0f;
   *u = sign * scalar_triple(b, c, d);
   *v = sign * scalar_triple(a, d, c);
   *w = sign * scalar_triple(a, b, d);
   *x = sign * scalar_triple(a, c, b);
   *dv = sign * divisor;
 }
-inline float simplex_metric(const Simplex& s) {                                     // :96
+inline real simplex_metric(const Simplex& s) {                                     // :96
   switch (s.count) {
     case 1: return 0.0f;
     case 2: return distance(s.v[0].w, s.v[1].w);
@@ -880,21 +882,21 @@ inline float simplex_metric(const Simplex& s) {                                 
 }
 inline bool solve2(Simplex& s) {                                                   // :130
   V3 a = s.v[0].w, b = s.v[1].w, ab = b - a;
-  float divisor = dot(ab, ab), u = dot(b, ab), v = -dot(a, ab);
+  real divisor = dot(ab, ab), u = dot(b, ab), v = -dot(a, ab);
   if (v <= 0.0f) { s.count = 1; s.v[0].a = 1.0f; return true; }
   if (u <= 0.0f) { s.count = 1; s.v[0] = s.v[1]; s.v[0].a = 1.0f; return true; }
   if (divisor <= 0.0f) return false;
-  float den = 1.0f / divisor;
+  real den = 1.0f / divisor;
   s.v[0].a = den * u; s.v[1].a = den * v;
   return true;
 }
-inline bool edge_pick(Simplex& s, SVert a, SVert b, float u, float v, float d) {
+inline bool edge_pick(Simplex& s, SVert a, SVert b, real u, real v, real d) {
   s.count = 2; s.v[0] = a; s.v[1] = b;
   if (d <= 0.0f) return false;
   s.v[0].a = u / d; s.v[1].a = v / d;
   return true;
 }
-inline bool tri_pick(Simplex& s, SVert a, SVert b, SVert c, float u, float v, float w, float d) {
+inline bool tri_pick(Simplex& s, SVert a, SVert b, SVert c, real u, real v, real w, real d) {
   s.count = 3; s.v[0] = a; s.v[1] = b; s.v[2] = c;
   if (d <= 0.0f) return false;
   s.v[0].a = u / d; s.v[1].a = v / d; s.v[2].a = w / d;
@@ -902,14 +904,14 @@ inline bool tri_pick(Simplex& s, SVert a, SVert b, SVert c, float u, float v, fl
 }
 inline bool solve3(Simplex& s) {                                                   // :159
   SVert v1 = s.v[0], v2 = s.v[1], v3_ = s.v[2];
-  float ab_u, ab_v, ab_d, bc_u, bc_v, bc_d, ca_u, ca_v, ca_d;
+  real ab_u, ab_v, ab_d, bc_u, bc_v, bc_d, ca_u, ca_v, ca_d;
   bary_edge(v1.w, v2.w, &ab_u, &ab_v, &ab_d);
   bary_edge(v2.w, v3_.w, &bc_u, &bc_v, &bc_d);
   bary_edge(v3_.w, v1.w, &ca_u, &ca_v, &ca_d);
   if (ab_v <= 0.0f && ca_u <= 0.0f) { s.count = 1; s.v[0] = v1; s.v[0].a = 1.0f; return true; }
   if (bc_v <= 0.0f && ab_u <= 0.0f) { s.count = 1; s.v[0] = v2; s.v[0].a = 1.0f; return true; }
   if (ca_v <= 0.0f && bc_u <= 0.0f) { s.count = 1; s.v[0] = v3_; s.v[0].a = 1.0f; return true; }
-  float tu, tv, tw, td;
+  real tu, tv, tw, td;
   bary_tri(v1.w, v2.w, v3_.w, &tu, &tv, &tw, &td);
   if (tw <= 0.0f && ab_u > 0.0f && ab_v > 0.0f) return edge_pick(s, v1, v2, ab_u, ab_v, ab_d);
   if (tu <= 0.0f && bc_u > 0.0f && bc_v > 0.0f) return edge_pick(s, v2, v3_, bc_u, bc_v, bc_d);
@@ -920,7 +922,7 @@ inline bool solve3(Simplex& s) {                                                
 }
 inline bool solve4(Simplex& s) {                                                   // :249
   SVert A = s.v[0], B = s.v[1], C = s.v[2], D = s.v[3];
-  float ab[3], ac[3], ad[3], bc[3], cd[3], db[3];
+  real ab[3], ac[3], ad[3], bc[3], cd[3], db[3];
   bary_edge(A.w, B.w, &ab[0], &ab[1], &ab[2]);
   bary_edge(A.w, C.w, &ac[0], &ac[1], &ac[2]);
   bary_edge(A.w, D.w, &ad[0], &ad[1], &ad[2]);
@@ -931,7 +933,7 @@ inline bool solve4(Simplex& s) {                                                
   if (ab[0] <= 0.0f && db[0] <= 0.0f && bc[1] <= 0.0f) { s.count = 1; s.v[0] = B; s.v[0].a = 1.0f; return true; }
   if (ac[0] <= 0.0f && bc[0] <= 0.0f && cd[1] <= 0.0f) { s.count = 1; s.v[0] = C; s.v[0].a = 1.0f; return true; }
   if (ad[0] <= 0.0f && cd[0] <= 0.0f && db[1] <= 0.0f) { s.count = 1; s.v[0] = D; s.v[0].a = 1.0f; return true; }
-  float acb[4], abd[4], adc[4], bcd[4];
+  real acb[4], abd[4], adc[4], bcd[4];
   bary_tri(A.w, C.w, B.w, &acb[0], &acb[1], &acb[2], &acb[3]);
   bary_tri(A.w, B.w, D.w, &abd[0], &abd[1], &abd[2], &abd[3]);
   bary_tri(A.w, D.w, C.w, &adc[0], &adc[1], &adc[2], &adc[3]);
@@ -942,7 +944,7 @@ inline bool solve4(Simplex& s) {                                                
   if (acb[0] <= 0.0f && bcd[2] <= 0.0f && bc[0] > 0.0f && bc[1] > 0.0f) return edge_pick(s, B, C, bc[0], bc[1], bc[2]);
   if (adc[0] <= 0.0f && bcd[0] <= 0.0f && cd[0] > 0.0f && cd[1] > 0.0f) return edge_pick(s, C, D, cd[0], cd[1], cd[2]);
   if (abd[0] <= 0.0f && bcd[1] <= 0.0f && db[0] > 0.0f && db[1] > 0.0f) return edge_pick(s, D, B, db[0], db[1], db[2]);
-  float tu, tv, tw, tx, td;
+  real tu, tv, tw, tx, td;
   bary_tet(A.w, B.w, C.w, D.w, &tu, &tv, &tw, &tx, &td);
   if (tx < 0.0f && acb[0] > 0.0f && acb[1] > 0.0f && acb[2] > 0.0f) return tri_pick(s, A, C, B, acb[0], acb[1], acb[2], acb[3]);
   if (tw < 0.0f && abd[0] > 0.0f && abd[1] > 0.0f && abd[2] > 0.0f) return tri_pick(s, A, B, D, abd[0], abd[1], abd[2], abd[3]);
@@ -993,7 +995,7 @@ inline DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
     s.v[i].ia = i1; s.v[i].ib = i2; s.v[i].wa = w1; s.v[i].wb = w2; s.v[i].w = w2 - w1; s.v[i].a = 0.0f;
   }
   if (s.count > 0) {
-    float m1 = cache->metric, m2 = simplex_metric(s);
+    real m1 = cache->metric, m2 = simplex_metric(s);
     if (2.0f * m1 < m2 || m2 < 0.5f * m1 || m2 < kEps) s.count = 0;
   }
   if (s.count == 0) {
@@ -1005,7 +1007,7 @@ inline DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
   DistOut out;
   out.pa = out.pb = out.normal = v3(0, 0, 0);
   out.distance = 0;
-  float dsq = kFltMax;
+  real dsq = kFltMax;
   V3 normal = v3(0, 0, 0);
   int it = 0;
   while (it < 32) {
@@ -1023,7 +1025,7 @@ inline DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
       out.distance = 0.0f;
       return out;
     }
-    float old = dsq;
+    real old = dsq;
     V3 cp = closest_on_simplex(s);
     dsq = dot(cp, cp);
     if (dsq >= old) { s = backup; break; }
@@ -1079,9 +1081,9 @@ inline DistOut shape_distance(const V3* pa, int na, const V3* pb, int nb, Xf x, 
 inline void collide_hull_sphere(LocalManifold* m, const Hull& ha, Sphere b, Xf xb, SimplexCache* cache) {
   m->point_count = 0;
   V3 c = xf_point(xb, b.center);
-  float spec = speculative_distance();
+  real spec = speculative_distance();
   DistOut d = shape_distance(ha.points, ha.vertex_count, &c, 1, xf(v3(0, 0, 0), qid()), cache);
-  float ra = 0.0f, rb = b.radius, r = ra + rb;
+  real ra = 0.0f, rb = b.radius, r = ra + rb;
   if (d.distance > r + spec) { *cache = SimplexCache(); return; }
   if (d.distance > 100.0f * kEps) {
     V3 n = normalize(d.pb - d.pa);
@@ -1094,9 +1096,9 @@ inline void collide_hull_sphere(LocalManifold* m, const Hull& ha, Sphere b, Xf x
     m->points[0].pair = FeaturePair();
   } else {
     int best = -1;
-    float best_d = -kFltMax;
+    real best_d = -kFltMax;
     for (int i = 0; i < ha.face_count; ++i) {
-      float dd = plane_sep(ha.planes[i], c);
+      real dd = plane_sep(ha.planes[i], c);
       if (dd > best_d) { best = i; best_d = dd; }
     }
     V3 n = ha.planes[best].n;
@@ -1115,21 +1117,21 @@ inline void collide_capsules(LocalManifold* m, Capsule a, Capsule b, Xf xb) {
   m->point_count = 0;
   V3 a1 = a.c1, a2 = a.c2;
   V3 b1 = xf_point(xb, b.c1), b2 = xf_point(xb, b.c2);
-  float radius = a.radius + b.radius;
-  float maxd = radius + speculative_distance();
+  real radius = a.radius + b.radius;
+  real maxd = radius + speculative_distance();
   SegResult res = segment_distance(a1, a2, b1, b2);
   V3 off = res.p2 - res.p1;
-  float dsq = length_sq(off);
-  float ls = linear_slop();
-  float mind = 0.01f * ls;
+  real dsq = length_sq(off);
+  real ls = linear_slop();
+  real mind = 0.01f * ls;
   if (dsq > maxd * maxd || dsq < mind * mind) return;
   V3 ea, eb;
-  float la = get_length_and_normalize(a2 - a1, &ea);
+  real la = get_length_and_normalize(a2 - a1, &ea);
   if (la < min_capsule_length()) return;
-  float lb = get_length_and_normalize(b2 - b1, &eb);
+  real lb = get_length_and_normalize(b2 - b1, &eb);
   if (lb < min_capsule_length()) return;
-  const float at = 0.05f;
-  float at2 = at * at;
+  const real at = 0.05f;
+  real at2 = at * at;
   V3 axis = cross(ea, eb);
   if (length_sq(axis) < at2) {
     Plane pa0 = plane(-ea, -dot(ea, a.c1));
@@ -1142,14 +1144,14 @@ inline void collide_capsules(LocalManifold* m, Capsule a, Capsule b, Xf xb) {
     if (pc == 2) {
       V3 cp1 = point_to_segment(a1, a2, vb[0].position);
       V3 cp2 = point_to_segment(a1, a2, vb[1].position);
-      float d1 = distance(cp1, vb[0].position);
-      float d2 = distance(cp2, vb[1].position);
+      real d1 = distance(cp1, vb[0].position);
+      real d2 = distance(cp2, vb[1].position);
       if (d1 <= radius && d2 <= radius) {
         if (d1 < mind || d2 < mind) return;
         V3 n1 = (1.0f / d1) * (vb[0].position - cp1);
         V3 n2 = (1.0f / d2) * (vb[1].position - cp2);
         V3 n = normalize(n1 + n2);
-        float ra = a.radius, rb = b.radius;
+        real ra = a.radius, rb = b.radius;
         V3 p1 = 0.5f * mul_sub(mul_add(vb[0].position, ra, n1) + cp1, rb, n);
         V3 p2 = 0.5f * mul_sub(mul_add(vb[1].position, ra, n2) + cp2, rb, n);
         m->normal = n;
@@ -1161,7 +1163,7 @@ inline void collide_capsules(LocalManifold* m, Capsule a, Capsule b, Xf xb) {
     }
   }
   V3 n;
-  float dv = get_length_and_normalize(off, &n);
+  real dv = get_length_and_normalize(off, &n);
   V3 point = 0.5f * mul_sub(mul_add(res.p1, a.radius, n) + res.p2, b.radius, n);
   m->normal = n;
   m->point_count = 1;
@@ -1173,12 +1175,12 @@ inline void collide_capsules(LocalManifold* m, Capsule a, Capsule b, Xf xb) {
 // convex_manifold_shapes.rs:393
 inline SepAxis query_face_hull_capsule(const Hull& h, Capsule c, Xf t) {
   int mf = -1, mv = -1;
-  float ms = -kFltMax;
+  real ms = -kFltMax;
   V3 cpts[2] = {xf_point(t, c.c1), xf_point(t, c.c2)};
   for (int f = 0; f < h.face_count; ++f) {
     Plane p = h.planes[f];
     int vi = point_support(cpts, 2, -p.n);
-    float sep = plane_sep(p, cpts[vi]);
+    real sep = plane_sep(p, cpts[vi]);
     if (sep > ms) { mv = vi; mf = f; ms = sep; }
   }
   SepAxis r = {h.planes[mf].n, ms, mf, mv, kFaceAxisA};
@@ -1187,21 +1189,21 @@ inline SepAxis query_face_hull_capsule(const Hull& h, Capsule c, Xf t) {
 // convex_manifold_shapes.rs:431
 inline SepAxis query_edge_hull_capsule(const Hull& h, Capsule c, Xf t) {
   V3 mn = v3(0, 0, 0);
-  float ms = -kFltMax;
+  real ms = -kFltMax;
   int mia = kNull, mib = kNull;
   V3 pa = xf_point(t, c.c1), qa = xf_point(t, c.c2);
   V3 ea = qa - pa;
-  float sq = kParallelEdgeTol * kParallelEdgeTol;
+  real sq = kParallelEdgeTol * kParallelEdgeTol;
   for (int i = 0; i < h.edge_count; i += 2) {
     HalfEdge e = h.edges[i], tw = h.edges[i + 1];
     V3 qb = h.points[tw.origin];
     V3 ub = h.planes[e.face].n, vb = h.planes[tw.face].n;
-    float cba = dot(ub, ea), dba = dot(vb, ea);
+    real cba = dot(ub, ea), dba = dot(vb, ea);
     if (cba * dba < 0.0f) {
       if (maxf(cba * cba, dba * dba) < sq * length_sq(ea)) continue;
-      float tt = cba / (cba - dba);
+      real tt = cba / (cba - dba);
       V3 axis = normalize(lerp(ub, vb, tt));
-      float sep = dot(axis, qa - qb);
+      real sep = dot(axis, qa - qb);
       if (sep > ms) { mn = axis; ms = sep; mia = 0; mib = i; }
     }
   }
@@ -1217,8 +1219,8 @@ inline bool build_hull_face_capsule(LocalManifold* m, const Hull& ha, Capsule b,
   sb[1].position = xf_point(xb, b.c2); sb[1].separation = 0; sb[1].pair = make_feature_pair(0, 1, 0, 1);
   int pc = clip_segment_to_hull_face(sb, ha, rf);
   if (pc < 2) return false;
-  float d1 = plane_sep(rp, sb[0].position), d2 = plane_sep(rp, sb[1].position);
-  float spec = speculative_distance();
+  real d1 = plane_sep(rp, sb[0].position), d2 = plane_sep(rp, sb[1].position);
+  real spec = speculative_distance();
   if (d1 <= spec || d2 <= spec) {
     V3 n = rp.n;
     V3 p1 = mul_sub(sb[0].position, 0.5f * (d1 + b.radius), n);
@@ -1243,7 +1245,7 @@ inline bool build_hull_capsule_edge(LocalManifold* m, const Hull& ha, Capsule b,
   SegResult r = line_distance(ph, eh, pc, ec);
   if (!within_segments(r)) return false;
   V3 point = 0.5f * (mul_sub(r.p1, b.radius, n) + r.p2);
-  float sep = dot(n, r.p2 - r.p1);
+  real sep = dot(n, r.p2 - r.p1);
   m->normal = n;
   m->point_count = 1;
   m->points[0].point = point;
@@ -1256,20 +1258,20 @@ inline void collide_hull_capsule(LocalManifold* m, const Hull& ha, Capsule b, Xf
   m->point_count = 0;
   V3 cpts[2] = {b.c1, b.c2};
   DistOut d = shape_distance(ha.points, ha.vertex_count, cpts, 2, xb, cache);
-  float spec = speculative_distance();
+  real spec = speculative_distance();
   if (d.distance > b.radius + spec) { *cache = SimplexCache(); return; }
   if (d.distance > 100.0f * kEps) {
     V3 delta = d.normal;
     int rf = find_hull_support_face(ha, delta);
     Plane rp = ha.planes[rf];
-    const float kt = 0.998f;
+    const real kt = 0.998f;
     if (absf(dot(rp.n, delta)) > kt) {
       ClipVertex vb[2];
       vb[0].position = xf_point(xb, b.c1); vb[0].separation = 0; vb[0].pair = make_feature_pair(0, 0, 0, 0);
       vb[1].position = xf_point(xb, b.c2); vb[1].separation = 0; vb[1].pair = make_feature_pair(0, 1, 0, 1);
       int pc = clip_segment_to_hull_face(vb, ha, rf);
       if (pc == 2) {
-        float d1 = plane_sep(rp, vb[0].position), d2 = plane_sep(rp, vb[1].position);
+        real d1 = plane_sep(rp, vb[0].position), d2 = plane_sep(rp, vb[1].position);
         if (d1 <= b.radius + spec || d2 <= b.radius + spec) {
           V3 n = rp.n;
           V3 p1 = mul_sub(vb[0].position, 0.5f * (b.radius + d1), n);
@@ -1294,12 +1296,12 @@ inline void collide_hull_capsule(LocalManifold* m, const Hull& ha, Capsule b, Xf
   if (fq.separation > b.radius) return;
   SepAxis eq = query_edge_hull_capsule(ha, b, xb);
   if (eq.separation > b.radius) return;
-  float face_sep = fq.separation - b.radius;
+  real face_sep = fq.separation - b.radius;
   build_hull_face_capsule(m, ha, b, xb, fq);
   if (m->point_count == 2) face_sep = minf(m->points[0].separation, m->points[1].separation);
   if (eq.index_a == kNull) return;
-  float ls = linear_slop();
-  float edge_sep = eq.separation - b.radius;
+  real ls = linear_slop();
+  real edge_sep = eq.separation - b.radius;
   if (m->point_count == 0 || edge_sep > face_sep + ls) {
     build_hull_capsule_edge(m, ha, b, xb, eq);
   }

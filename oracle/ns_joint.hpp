@@ -7,15 +7,15 @@
 
 namespace nso {
 
-struct JointSoft { float bias_rate, mass_scale, impulse_scale; };
+struct JointSoft { real bias_rate, mass_scale, impulse_scale; };
 
-inline JointSoft joint_make_soft(float hertz, float zeta, float h) {  // solver_integration.rs:72
+inline JointSoft joint_make_soft(real hertz, real zeta, real h) {  // solver_integration.rs:72
   JointSoft s = {0, 0, 0};
   if (hertz == 0.0f) return s;
-  float omega = 2.0f * kPi * hertz;
-  float a1 = 2.0f * zeta + h * omega;
-  float a2 = h * omega * a1;
-  float a3 = 1.0f / (1.0f + a2);
+  real omega = 2.0f * kPi * hertz;
+  real a1 = 2.0f * zeta + h * omega;
+  real a2 = h * omega * a1;
+  real a3 = 1.0f / (1.0f + a2);
   s.bias_rate = omega / a1;
   s.mass_scale = a2 * a3;
   s.impulse_scale = a3;
@@ -26,28 +26,28 @@ struct Joint {
   int id = -1, body_a = -1, body_b = -1, color = -1;
   bool collide_connected = false;
   Xf local_frame_a, local_frame_b;
-  float constraint_hertz = 60.0f, constraint_damping_ratio = 2.0f;
+  real constraint_hertz = 60.0f, constraint_damping_ratio = 2.0f;
   JointSoft constraint_softness = {0.0f, 1.0f, 0.0f};
-  float inv_mass_a = 0, inv_mass_b = 0;
+  real inv_mass_a = 0, inv_mass_b = 0;
   M3 inv_ia, inv_ib;
   bool fixed_rotation = false;
   // RevoluteJointSim (revolute_joint.rs:28)
   V3 linear_impulse = {0, 0, 0};
   V2 perp_impulse = {0, 0};
-  float spring_impulse = 0, motor_impulse = 0, lower_impulse = 0, upper_impulse = 0;
-  float hertz = 0, damping_ratio = 0, max_motor_torque = 0, motor_speed = 0, target_angle = 0;
-  float lower_angle = 0, upper_angle = 0;
+  real spring_impulse = 0, motor_impulse = 0, lower_impulse = 0, upper_impulse = 0;
+  real hertz = 0, damping_ratio = 0, max_motor_torque = 0, motor_speed = 0, target_angle = 0;
+  real lower_angle = 0, upper_angle = 0;
   int index_a = -1, index_b = -1;
   Xf frame_a, frame_b;
   V3 rotation_axis_z, perp_axis_x, perp_axis_y, delta_center;
-  float axial_mass = 0;
+  real axial_mass = 0;
   JointSoft spring_softness = {0, 0, 0};
   bool enable_spring = false, enable_motor = false, enable_limit = false;
 };
 
-inline Joint make_revolute_joint(int a, int b, const float* fa, const float* fb, bool limit, float lower,
-                                 float upper, bool spring, float hertz, float zeta, float drag,
-                                 bool collide, float c_hertz, float c_zeta) {
+inline Joint make_revolute_joint(int a, int b, const float* fa, const float* fb, bool limit, real lower,
+                                 real upper, bool spring, real hertz, real zeta, real drag,
+                                 bool collide, real c_hertz, real c_zeta) {
   Joint j;
   j.body_a = a; j.body_b = b;
   j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
@@ -63,31 +63,31 @@ inline Joint make_revolute_joint(int a, int b, const float* fa, const float* fb,
 }
 
 // revolute_joint.rs:95 solve_point_constraint
-inline V3 solve_point_constraint(float ma, float mb, M3 ia, M3 ib, V3 ra, V3 rb, V3 rhs) {
-  float axy = ra.z * ia.cy.y - ra.y * ia.cz.y;
-  float axz = ra.z * ia.cy.z - ra.y * ia.cz.z;
+inline V3 solve_point_constraint(real ma, real mb, M3 ia, M3 ib, V3 ra, V3 rb, V3 rhs) {
+  real axy = ra.z * ia.cy.y - ra.y * ia.cz.y;
+  real axz = ra.z * ia.cy.z - ra.y * ia.cz.z;
   V3 ay = ra.x * ia.cz - ra.z * ia.cx;
   V3 az = ra.y * ia.cx - ra.x * ia.cy;
-  float bxy = rb.z * ib.cy.y - rb.y * ib.cz.y;
-  float bxz = rb.z * ib.cy.z - rb.y * ib.cz.z;
+  real bxy = rb.z * ib.cy.y - rb.y * ib.cz.y;
+  real bxz = rb.z * ib.cy.z - rb.y * ib.cz.z;
   V3 by = rb.x * ib.cz - rb.z * ib.cx;
   V3 bz = rb.y * ib.cx - rb.x * ib.cy;
-  float m = ma + mb;
-  float kxx = (axy * ra.z - axz * ra.y) + (bxy * rb.z - bxz * rb.y) + m;
-  float kyy = (ay.z * ra.x - ay.x * ra.z) + (by.z * rb.x - by.x * rb.z) + m;
-  float kzz = (az.x * ra.y - az.y * ra.x) + (bz.x * rb.y - bz.y * rb.x) + m;
-  float kxy = (ay.y * ra.z - ay.z * ra.y) + (by.y * rb.z - by.z * rb.y);
-  float kxz = (az.y * ra.z - az.z * ra.y) + (bz.y * rb.z - bz.z * rb.y);
-  float kyz = (az.z * ra.x - az.x * ra.z) + (bz.z * rb.x - bz.x * rb.z);
-  float cxx = kyy * kzz - kyz * kyz;
-  float cyy = kxx * kzz - kxz * kxz;
-  float czz = kxx * kyy - kxy * kxy;
-  float cxy = kxz * kyz - kxy * kzz;
-  float cxz = kxy * kyz - kyy * kxz;
-  float cyz = kxy * kxz - kxx * kyz;
-  float d = kxx * cxx + kxy * cxy + kxz * cxz;
+  real m = ma + mb;
+  real kxx = (axy * ra.z - axz * ra.y) + (bxy * rb.z - bxz * rb.y) + m;
+  real kyy = (ay.z * ra.x - ay.x * ra.z) + (by.z * rb.x - by.x * rb.z) + m;
+  real kzz = (az.x * ra.y - az.y * ra.x) + (bz.x * rb.y - bz.y * rb.x) + m;
+  real kxy = (ay.y * ra.z - ay.z * ra.y) + (by.y * rb.z - by.z * rb.y);
+  real kxz = (az.y * ra.z - az.z * ra.y) + (bz.y * rb.z - bz.z * rb.y);
+  real kyz = (az.z * ra.x - az.x * ra.z) + (bz.z * rb.x - bz.x * rb.z);
+  real cxx = kyy * kzz - kyz * kyz;
+  real cyy = kxx * kzz - kxz * kxz;
+  real czz = kxx * kyy - kxy * kxy;
+  real cxy = kxz * kyz - kxy * kzz;
+  real cxz = kxy * kyz - kyy * kxz;
+  real cyz = kxy * kxz - kxx * kyz;
+  real d = kxx * cxx + kxy * cxy + kxz * cxz;
   if (absf(d) > 1000.0f * kMinPositive) {
-    float inv = 1.0f / d;
+    real inv = 1.0f / d;
     return v3(inv * (cxx * rhs.x + cxy * rhs.y + cxz * rhs.z),
               inv * (cxy * rhs.x + cyy * rhs.y + cyz * rhs.z),
               inv * (cxz * rhs.x + cyz * rhs.y + czz * rhs.z));
@@ -103,10 +103,10 @@ namespace nso {
 
 template <class BodyT, class SimT>
 void prepare_joints(std::vector<Joint>& joints, const std::vector<SimT>& awake, const std::vector<SimT>& stat,
-                    const BodyT* bodies, float h, float inv_h, float warm) {
+                    const BodyT* bodies, real h, real inv_h, real warm) {
   for (Joint& j : joints) {
     // distance_joint_solver.rs:74 prepare_joint
-    float hz = minf(j.constraint_hertz, 0.25f * inv_h);
+    real hz = minf(j.constraint_hertz, 0.25f * inv_h);
     j.constraint_softness = joint_make_soft(hz, j.constraint_damping_ratio, h);
     // revolute_joint.rs:183 prepare_revolute_joint
     const BodyT& ba = bodies[j.body_a];
@@ -125,7 +125,7 @@ void prepare_joints(std::vector<Joint>& joints, const std::vector<SimT>& awake, 
     j.frame_b.p = rotate(sb.transform.q, j.local_frame_b.p - sb.local_center);
     j.delta_center = sub_pos(sb.center, sa.center);
     V3 axis = rotate(j.frame_a.q, v3(0, 0, 1));
-    float k = dot(axis, mul_mv(sum, axis));
+    real k = dot(axis, mul_mv(sum, axis));
     j.axial_mass = k > 0.0f ? 1.0f / k : 0.0f;
     j.rotation_axis_z = axis;
     Q rq = inv_mul_quat(j.frame_a.q, j.frame_b.q);
@@ -150,15 +150,15 @@ StateT joint_state_at(std::vector<StateT>& states, int i) {
 // revolute_joint.rs:261 warm_start_revolute_joint
 template <class StateT>
 void warm_start_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
-                             std::vector<StateT>& states, float h) {
+                             std::vector<StateT>& states, real h) {
   (void)h;
   for (int id : ids) {
     Joint& j = joints[id];
-    float mA = j.inv_mass_a, mB = j.inv_mass_b;
+    real mA = j.inv_mass_a, mB = j.inv_mass_b;
     StateT sa = joint_state_at(states, j.index_a), sb = joint_state_at(states, j.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
     V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
-    float axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
+    real axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
     V3 ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
     ang = mul_add(ang, axial, j.rotation_axis_z);
     va = va - mA * j.linear_impulse;
@@ -175,10 +175,10 @@ void warm_start_joints_color(std::vector<Joint>& joints, const std::vector<int>&
 // revolute_joint.rs:316 solve_revolute_joint
 template <class StateT>
 void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids, std::vector<StateT>& states,
-                        float h, float inv_h, bool use_bias) {
+                        real h, real inv_h, bool use_bias) {
   for (int id : ids) {
     Joint& j = joints[id];
-    float mA = j.inv_mass_a, mB = j.inv_mass_b;
+    real mA = j.inv_mass_a, mB = j.inv_mass_b;
     M3 iA = j.inv_ia, iB = j.inv_ib;
     StateT sa = joint_state_at(states, j.index_a), sb = joint_state_at(states, j.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
@@ -190,57 +190,57 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
     if (!fixed && (j.enable_spring || j.enable_motor || j.enable_limit)) {
       V3 axis = j.rotation_axis_z;
       V3 ga = mul_mv(iA, axis), gb = mul_mv(iB, axis);
-      float k = dot(axis, ga + gb);
-      float acd = dot(wb - wa, axis);
-      float ai = 0.0f;
+      real k = dot(axis, ga + gb);
+      real acd = dot(wb - wa, axis);
+      real ai = 0.0f;
       if (j.enable_spring) {
-        float angle = get_twist_angle(rq);
-        float c = angle - j.target_angle;
-        float bias = j.spring_softness.bias_rate * c;
-        float ms = j.spring_softness.mass_scale, is = j.spring_softness.impulse_scale;
-        float di = -ms * j.axial_mass * (acd + bias) - is * j.spring_impulse;
+        real angle = get_twist_angle(rq);
+        real c = angle - j.target_angle;
+        real bias = j.spring_softness.bias_rate * c;
+        real ms = j.spring_softness.mass_scale, is = j.spring_softness.impulse_scale;
+        real di = -ms * j.axial_mass * (acd + bias) - is * j.spring_impulse;
         j.spring_impulse += di;
         acd += k * di;
         ai += di;
       }
       if (j.enable_motor) {
-        float cdot = acd - j.motor_speed;
-        float old = j.motor_impulse;
-        float mx = j.max_motor_torque * h;
-        float di = clampf(-j.axial_mass * cdot, -mx - old, mx - old);
+        real cdot = acd - j.motor_speed;
+        real old = j.motor_impulse;
+        real mx = j.max_motor_torque * h;
+        real di = clampf(-j.axial_mass * cdot, -mx - old, mx - old);
         j.motor_impulse = old + di;
         acd += k * di;
         ai += di;
       }
       if (j.enable_limit) {
-        float angle = get_twist_angle(rq);
+        real angle = get_twist_angle(rq);
         {
-          float c = angle - j.lower_angle;
-          float bias = 0.0f, ms = 1.0f, is = 0.0f;
+          real c = angle - j.lower_angle;
+          real bias = 0.0f, ms = 1.0f, is = 0.0f;
           if (c > 0.0f) bias = c * inv_h;
           else if (use_bias) {
             bias = j.constraint_softness.bias_rate * c;
             ms = j.constraint_softness.mass_scale;
             is = j.constraint_softness.impulse_scale;
           }
-          float old = j.lower_impulse;
-          float di = maxf(-ms * j.axial_mass * (acd + bias) - is * old, -old);
+          real old = j.lower_impulse;
+          real di = maxf(-ms * j.axial_mass * (acd + bias) - is * old, -old);
           j.lower_impulse = old + di;
           acd += k * di;
           ai += di;
         }
         {
-          float c = j.upper_angle - angle;
-          float bias = 0.0f, ms = 1.0f, is = 0.0f;
+          real c = j.upper_angle - angle;
+          real bias = 0.0f, ms = 1.0f, is = 0.0f;
           if (c > 0.0f) bias = c * inv_h;
           else if (use_bias) {
             bias = j.constraint_softness.bias_rate * c;
             ms = j.constraint_softness.mass_scale;
             is = j.constraint_softness.impulse_scale;
           }
-          float cdot = -acd;
-          float old = j.upper_impulse;
-          float di = maxf(-ms * j.axial_mass * (cdot + bias) - is * old, -old);
+          real cdot = -acd;
+          real old = j.upper_impulse;
+          real di = maxf(-ms * j.axial_mass * (cdot + bias) - is * old, -old);
           j.upper_impulse = old + di;
           ai -= di;
         }
@@ -250,7 +250,7 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
     }
     if (!fixed) {
       V2 bias = v2(0, 0);
-      float ms = 1.0f, is = 0.0f;
+      real ms = 1.0f, is = 0.0f;
       if (use_bias) {
         V2 c = v2(rq.v.x, rq.v.y);
         bias = v2(j.constraint_softness.bias_rate * c.x, j.constraint_softness.bias_rate * c.y);
@@ -262,9 +262,9 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
       j.perp_axis_x = px;
       j.perp_axis_y = py;
       M3 sum = add_mm(iA, iB);
-      float kxx = dot(px, mul_mv(sum, px));
-      float kyy = dot(py, mul_mv(sum, py));
-      float kxy = dot(px, mul_mv(sum, py));
+      real kxx = dot(px, mul_mv(sum, px));
+      real kyy = dot(py, mul_mv(sum, py));
+      real kxy = dot(px, mul_mv(sum, py));
       M2 K;
       K.cx = v2(kxx, kxy);
       K.cy = v2(kxy, kyy);
@@ -282,7 +282,7 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
       V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
       V3 cdot = (vb + cross(wb, rb)) - va - cross(wa, ra);
       V3 bias = v3(0, 0, 0);
-      float ms = 1.0f, is = 0.0f;
+      real ms = 1.0f, is = 0.0f;
       if (use_bias) {
         V3 dca = sa.dp, dcb = sb.dp;
         V3 sep = ((dcb - dca) + (rb - ra)) + j.delta_center;

@@ -10,71 +10,83 @@
 #include <cstdint>
 #include <cfloat>
 #include <cstring>
+#include <type_traits>
 
 namespace nso {
 
-static const float kPi = 3.14159265359f;             // base/constants.rs:6
-static const float kMinPositive = FLT_MIN;           // f32::MIN_POSITIVE
-static const float kEps = FLT_EPSILON;               // f32::EPSILON
-static const float kFltMax = FLT_MAX;
+// The oracle's scalar. The parity build is f32 (the reference's arithmetic, bit for bit); the
+// same sources built with NSO_REAL_F64 give the f64 run the trajectory statistics are checked
+// against (every operation in double; constants keep their f32 literals' values).
+#ifdef NSO_REAL_F64
+typedef double real;
+static const real kMinPositive = DBL_MIN;
+static const real kEps = DBL_EPSILON;
+static const real kFltMax = DBL_MAX;
+#else
+typedef float real;
+static const real kMinPositive = FLT_MIN;           // f32::MIN_POSITIVE
+static const real kEps = FLT_EPSILON;               // f32::EPSILON
+static const real kFltMax = FLT_MAX;
+#endif
+static const real kPi = 3.14159265359f;             // base/constants.rs:6
 static const int kNull = -1;
 static const int kGraphColorCount = 24;              // constants.rs:23
 static const int kOverflowIndex = kGraphColorCount - 1;      // constraint_graph.rs:20
 static const int kDynamicColorCount = kGraphColorCount - 4;  // constraint_graph.rs:23
-static const float kMaxRotation = 0.25f * kPi;       // constants.rs:28
-static const float kRecycleAngular = 0.99240388f;    // constants.rs:29
-static const float kAabbMarginFraction = 0.125f;     // constants.rs:30
-static const float kMinFrictionWeight = 1e-10f;      // constants.rs:26
-static const float kParallelEdgeTol = 0.005f;        // constants.rs:39
+static const real kMaxRotation = 0.25f * kPi;       // constants.rs:28
+static const real kRecycleAngular = 0.99240388f;    // constants.rs:29
+static const real kAabbMarginFraction = 0.125f;     // constants.rs:30
+static const real kMinFrictionWeight = 1e-10f;      // constants.rs:26
+static const real kParallelEdgeTol = 0.005f;        // constants.rs:39
 
 // Length-unit dependent values are computed at run time in the reference
 // (constants.rs:79-121), so they are computed the same way here.
-inline float length_units() { return 1.0f; }
-inline float linear_slop() { return 0.005f * length_units(); }
-inline float speculative_distance() { return 4.0f * linear_slop(); }
-inline float contact_recycle_distance() { return 10.0f * linear_slop(); }
-inline float max_aabb_margin() { return 0.05f * length_units(); }
-inline float huge_value() { return 1.0e5f * length_units(); }
-inline float min_capsule_length() { return linear_slop(); }
+inline real length_units() { return 1.0f; }
+inline real linear_slop() { return 0.005f * length_units(); }
+inline real speculative_distance() { return 4.0f * linear_slop(); }
+inline real contact_recycle_distance() { return 10.0f * linear_slop(); }
+inline real max_aabb_margin() { return 0.05f * length_units(); }
+inline real huge_value() { return 1.0e5f * length_units(); }
+inline real min_capsule_length() { return linear_slop(); }
 
-struct V2 { float x, y; };
-struct V3 { float x, y, z; };
-struct Q { V3 v; float s; };
+struct V2 { real x, y; };
+struct V3 { real x, y, z; };
+struct Q { V3 v; real s; };
 struct M3 { V3 cx, cy, cz; };
 struct M2 { V2 cx, cy; };
 struct Pos { double x, y, z; };
 struct Xf { V3 p; Q q; };
 struct WXf { Pos p; Q q; };
 struct AABB { V3 lo, hi; };
-struct Plane { V3 n; float off; };
+struct Plane { V3 n; real off; };
 
-inline V2 v2(float x, float y) { V2 r = {x, y}; return r; }
-inline V3 v3(float x, float y, float z) { V3 r = {x, y, z}; return r; }
-inline Q quat(V3 v, float s) { Q r = {v, s}; return r; }
+inline V2 v2(real x, real y) { V2 r = {x, y}; return r; }
+inline V3 v3(real x, real y, real z) { V3 r = {x, y, z}; return r; }
+inline Q quat(V3 v, real s) { Q r = {v, s}; return r; }
 inline Q qid() { return quat(v3(0, 0, 0), 1.0f); }
 inline M3 m3(V3 a, V3 b, V3 c) { M3 r = {a, b, c}; return r; }
 inline M3 m3zero() { return m3(v3(0, 0, 0), v3(0, 0, 0), v3(0, 0, 0)); }
 inline Xf xf(V3 p, Q q) { Xf r = {p, q}; return r; }
-inline Plane plane(V3 n, float o) { Plane r = {n, o}; return r; }
+inline Plane plane(V3 n, real o) { Plane r = {n, o}; return r; }
 inline AABB aabb(V3 lo, V3 hi) { AABB r = {lo, hi}; return r; }
 
 // functions.rs:16-60 -- ties return the second operand.
 inline int min_i(int a, int b) { return a < b ? a : b; }
 inline int max_i(int a, int b) { return a > b ? a : b; }
-inline float absf(float a) { return a < 0.0f ? -a : a; }
-inline float minf(float a, float b) { return a < b ? a : b; }
-inline float maxf(float a, float b) { return a > b ? a : b; }
-inline float clampf(float a, float lo, float hi) { return a < lo ? lo : (hi < a ? hi : a); }
+inline real absf(real a) { return a < 0.0f ? -a : a; }
+inline real minf(real a, real b) { return a < b ? a : b; }
+inline real maxf(real a, real b) { return a > b ? a : b; }
+inline real clampf(real a, real lo, real hi) { return a < lo ? lo : (hi < a ? hi : a); }
 
 // functions.rs:68 atan2_approx (polynomial, not libm)
-inline float atan2_approx(float y, float x) {
+inline real atan2_approx(real y, real x) {
   if (x == 0.0f && y == 0.0f) return 0.0f;
-  float ax = absf(x), ay = absf(y);
-  float mx = maxf(ay, ax), mn = minf(ay, ax);
-  float a = mn / mx;
-  float s = a * a, c = s * a, q = s * s;
-  float r = 0.024840285f * q + 0.18681418f;
-  float t = -0.094097948f * q - 0.33213072f;
+  real ax = absf(x), ay = absf(y);
+  real mx = maxf(ay, ax), mn = minf(ay, ax);
+  real a = mn / mx;
+  real s = a * a, c = s * a, q = s * s;
+  real r = 0.024840285f * q + 0.18681418f;
+  real t = -0.094097948f * q - 0.33213072f;
   r = r * s + t;
   r = r * c + a;
   if (ay > ax) r = 1.57079637f - r;
@@ -87,30 +99,30 @@ inline float atan2_approx(float y, float x) {
 inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
-inline V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+inline V3 operator*(real s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
 inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
 
-inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }       // :250
-inline float length(V3 v) { return std::sqrt(dot(v, v)); }                        // :256
-inline float length_sq(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }      // :262
-inline float distance(V3 a, V3 b) { return length(v3(b.x - a.x, b.y - a.y, b.z - a.z)); }
-inline float distance_sq(V3 a, V3 b) {                                            // :274
+inline real dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }       // :250
+inline real length(V3 v) { return std::sqrt(dot(v, v)); }                        // :256
+inline real length_sq(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }      // :262
+inline real distance(V3 a, V3 b) { return length(v3(b.x - a.x, b.y - a.y, b.z - a.z)); }
+inline real distance_sq(V3 a, V3 b) {                                            // :274
   V3 d = v3(b.x - a.x, b.y - a.y, b.z - a.z);
   return d.x * d.x + d.y * d.y + d.z * d.z;
 }
 inline V3 normalize(V3 a) {                                                       // :281
-  float ls = a.x * a.x + a.y * a.y + a.z * a.z;
+  real ls = a.x * a.x + a.y * a.y + a.z * a.z;
   if (ls > 1000.0f * kMinPositive) {
-    float s = 1.0f / std::sqrt(ls);
+    real s = 1.0f / std::sqrt(ls);
     return v3(s * a.x, s * a.y, s * a.z);
   }
   return v3(0, 0, 0);
 }
-inline float get_length_and_normalize(V3 a, V3* out) {                            // :293
-  float ls = a.x * a.x + a.y * a.y + a.z * a.z;
+inline real get_length_and_normalize(V3 a, V3* out) {                            // :293
+  real ls = a.x * a.x + a.y * a.y + a.z * a.z;
   if (ls > 1000.0f * kMinPositive) {
-    float l = std::sqrt(ls);
-    float s = 1.0f / l;
+    real l = std::sqrt(ls);
+    real s = 1.0f / l;
     *out = v3(s * a.x, s * a.y, s * a.z);
     return l;
   }
@@ -122,18 +134,18 @@ inline V3 perp(V3 a) {                                                          
   return normalize(p);
 }
 inline bool is_normalized(V3 a) { return absf(1.0f - dot(a, a)) < 100.0f * kEps; }
-inline V3 mul_add(V3 a, float s, V3 b) { return v3(a.x + s * b.x, a.y + s * b.y, a.z + s * b.z); }  // :322
-inline V3 mul_sub(V3 a, float s, V3 b) { return v3(a.x - s * b.x, a.y - s * b.y, a.z - s * b.z); }  // :328
+inline V3 mul_add(V3 a, real s, V3 b) { return v3(a.x + s * b.x, a.y + s * b.y, a.z + s * b.z); }  // :322
+inline V3 mul_sub(V3 a, real s, V3 b) { return v3(a.x - s * b.x, a.y - s * b.y, a.z - s * b.z); }  // :328
 inline V3 cross(V3 a, V3 b) {                                                     // :333
   return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-inline V3 lerp(V3 a, V3 b, float t) {                                             // :342
+inline V3 lerp(V3 a, V3 b, real t) {                                             // :342
   return v3((1.0f - t) * a.x + t * b.x, (1.0f - t) * a.y + t * b.y, (1.0f - t) * a.z + t * b.z);
 }
-inline V3 blend2(float s, V3 a, float t, V3 b) {                                  // :353
+inline V3 blend2(real s, V3 a, real t, V3 b) {                                  // :353
   return v3(s * a.x + t * b.x, s * a.y + t * b.y, s * a.z + t * b.z);
 }
-inline V3 blend3(float s, V3 a, float t, V3 b, float u, V3 c) {                   // internal_math.rs:249
+inline V3 blend3(real s, V3 a, real t, V3 b, real u, V3 c) {                   // internal_math.rs:249
   return v3(s * a.x + t * b.x + u * c.x, s * a.y + t * b.y + u * c.y, s * a.z + t * b.z + u * c.z);
 }
 inline V3 abs3(V3 a) { return v3(absf(a.x), absf(a.y), absf(a.z)); }
@@ -153,7 +165,7 @@ inline V3 inv_rotate(Q q, V3 v) {
   V3 t3 = cross(q.v, t2);
   return mul_add(v, 2.0f, t3);
 }
-inline float dot_quat(Q a, Q b) { return a.v.x * b.v.x + a.v.y * b.v.y + a.v.z * b.v.z + a.s * b.s; }
+inline real dot_quat(Q a, Q b) { return a.v.x * b.v.x + a.v.y * b.v.y + a.v.z * b.v.z + a.s * b.s; }
 inline Q mul_quat(Q q1, Q q2) {                                                   // :423
   V3 t1 = cross(q1.v, q2.v);
   V3 t2 = mul_add(t1, q1.s, q2.v);
@@ -168,15 +180,15 @@ inline Q inv_mul_quat(Q q1, Q q2) {                                             
 }
 inline Q conjugate(Q q) { return quat(v3(-q.v.x, -q.v.y, -q.v.z), q.s); }
 inline Q normalize_quat(Q q) {                                                    // :450
-  float ls = dot_quat(q, q);
+  real ls = dot_quat(q, q);
   if (ls > 1000.0f * kMinPositive) {
-    float s = 1.0f / std::sqrt(ls);
+    real s = 1.0f / std::sqrt(ls);
     return quat(v3(s * q.v.x, s * q.v.y, s * q.v.z), s * q.s);
   }
   return qid();
 }
-inline float get_twist_angle(Q q) {                                               // :490
-  float twist = q.s < 0.0f ? atan2_approx(-q.v.z, -q.s) : atan2_approx(q.v.z, q.s);
+inline real get_twist_angle(Q q) {                                               // :490
+  real twist = q.s < 0.0f ? atan2_approx(-q.v.z, -q.s) : atan2_approx(q.v.z, q.s);
   return twist * 2.0f;
 }
 
@@ -187,7 +199,7 @@ inline V3 inv_xf_point(Xf t, V3 v) { return inv_rotate(t.q, v - t.p); }
 
 // functions.rs:618-660 world positions (f64)
 inline V3 sub_pos(Pos a, Pos b) {
-  return v3((float)(a.x - b.x), (float)(a.y - b.y), (float)(a.z - b.z));
+  return v3((real)(a.x - b.x), (real)(a.y - b.y), (real)(a.z - b.z));
 }
 inline Pos offset_pos(Pos p, V3 d) {
   Pos r = {p.x + (double)d.x, p.y + (double)d.y, p.z + (double)d.z};
@@ -198,13 +210,13 @@ inline V3 inv_world_point(WXf t, Pos p) { return inv_rotate(t.q, sub_pos(p, t.p)
 inline Xf inv_mul_wxf(WXf a, WXf b) { return xf(inv_world_point(a, b.p), inv_mul_quat(a.q, b.q)); }
 
 // functions.rs:575-603 directed rounding at the f64->f32 boundary
-inline float round_down(double x) {
-  float f = (float)x;
+inline real round_down(double x) {
+  real f = (real)x;
   if ((double)f > x) f = std::nextafter(f, -INFINITY);
   return f;
 }
-inline float round_up(double x) {
-  float f = (float)x;
+inline real round_up(double x) {
+  real f = (real)x;
   if ((double)f < x) f = std::nextafter(f, INFINITY);
   return f;
 }
@@ -216,7 +228,7 @@ inline AABB offset_aabb(AABB b, Pos o) {                                        
 }
 
 // functions.rs:706-832 matrices
-inline float det(M3 m) { return dot(m.cx, cross(m.cy, m.cz)); }
+inline real det(M3 m) { return dot(m.cx, cross(m.cy, m.cz)); }
 inline V3 mul_mv(M3 m, V3 a) {
   return v3(m.cx.x * a.x + m.cy.x * a.y + m.cz.x * a.z,
             m.cx.y * a.x + m.cy.y * a.y + m.cz.y * a.z,
@@ -224,47 +236,47 @@ inline V3 mul_mv(M3 m, V3 a) {
 }
 inline M3 add_mm(M3 a, M3 b) { return m3(a.cx + b.cx, a.cy + b.cy, a.cz + b.cz); }
 inline M3 sub_mm(M3 a, M3 b) { return m3(a.cx - b.cx, a.cy - b.cy, a.cz - b.cz); }
-inline M3 mul_sm(float s, M3 a) { return m3(s * a.cx, s * a.cy, s * a.cz); }
+inline M3 mul_sm(real s, M3 a) { return m3(s * a.cx, s * a.cy, s * a.cz); }
 inline M3 mul_mm(M3 a, M3 b) { return m3(mul_mv(a, b.cx), mul_mv(a, b.cy), mul_mv(a, b.cz)); }
 inline M3 transpose(M3 m) {
   return m3(v3(m.cx.x, m.cy.x, m.cz.x), v3(m.cx.y, m.cy.y, m.cz.y), v3(m.cx.z, m.cy.z, m.cz.z));
 }
 inline M3 invert_matrix(M3 m) {                                                   // :774
-  float d = det(m);
+  real d = det(m);
   if (absf(d) > 1000.0f * kMinPositive) {
-    float inv_d = 1.0f / d;
+    real inv_d = 1.0f / d;
     M3 out = m3(inv_d * cross(m.cy, m.cz), inv_d * cross(m.cz, m.cx), inv_d * cross(m.cx, m.cy));
     return transpose(out);
   }
   return m3zero();
 }
 inline V3 solve3(M3 m, V3 a) {                                                    // :783
-  float d = det(m);
+  real d = det(m);
   if (absf(d) > 1000.0f * kMinPositive) {
-    float inv_d = 1.0f / d;
+    real inv_d = 1.0f / d;
     V3 sx = cross(m.cy, m.cz), sy = cross(m.cz, m.cx), sz = cross(m.cx, m.cy);
     return v3(inv_d * dot(sx, a), inv_d * dot(sy, a), inv_d * dot(sz, a));
   }
   return v3(0, 0, 0);
 }
 inline M3 invert_t(M3 m) {                                                        // :800
-  float d = det(m);
+  real d = det(m);
   if (absf(d) > 1000.0f * kMinPositive) {
-    float inv_d = 1.0f / d;
+    real inv_d = 1.0f / d;
     return m3(inv_d * cross(m.cy, m.cz), inv_d * cross(m.cz, m.cx), inv_d * cross(m.cx, m.cy));
   }
   return m3zero();
 }
 inline M3 abs_m3(M3 m) { return m3(abs3(m.cx), abs3(m.cy), abs3(m.cz)); }
 inline M3 matrix_from_quat(Q q) {                                                 // :821
-  float xx = q.v.x * q.v.x, yy = q.v.y * q.v.y, zz = q.v.z * q.v.z;
-  float xy = q.v.x * q.v.y, xz = q.v.x * q.v.z, xw = q.v.x * q.s;
-  float yz = q.v.y * q.v.z, yw = q.v.y * q.s, zw = q.v.z * q.s;
+  real xx = q.v.x * q.v.x, yy = q.v.y * q.v.y, zz = q.v.z * q.v.z;
+  real xy = q.v.x * q.v.y, xz = q.v.x * q.v.z, xw = q.v.x * q.s;
+  real yz = q.v.y * q.v.z, yw = q.v.y * q.s, zw = q.v.z * q.s;
   return m3(v3(1.0f - 2.0f * (yy + zz), 2.0f * (xy + zw), 2.0f * (xz - yw)),
             v3(2.0f * (xy - zw), 1.0f - 2.0f * (xx + zz), 2.0f * (yz + xw)),
             v3(2.0f * (xz + yw), 2.0f * (yz - xw), 1.0f - 2.0f * (xx + yy)));
 }
-inline M3 diag(float a, float b, float c) {
+inline M3 diag(real a, real b, real c) {
   return m3(v3(a, 0, 0), v3(0, b, 0), v3(0, 0, c));
 }
 inline M3 identity_m3() { return diag(1.0f, 1.0f, 1.0f); }
@@ -278,7 +290,7 @@ inline bool aabb_contains(AABB a, AABB b) {
 }
 inline V3 aabb_center(AABB a) { return 0.5f * (a.hi + a.lo); }
 inline V3 aabb_extents(AABB a) { return 0.5f * (a.hi - a.lo); }
-inline AABB aabb_inflate(AABB a, float e) {
+inline AABB aabb_inflate(AABB a, real e) {
   V3 r = v3(e, e, e);
   return aabb(a.lo - r, a.hi + r);
 }
@@ -299,7 +311,7 @@ inline AABB aabb_transform(Xf t, AABB a) {                                      
 inline Q quat_between_unit_vectors(V3 v1, V3 v2) {
   Q out = quat(v3(0, 0, 0), 0.0f);
   V3 m = lerp(v1, v2, 0.5f);
-  float tol = 100.0f * kEps;
+  real tol = 100.0f * kEps;
   if (length_sq(m) > tol * tol) {
     out.v = cross(v1, m);
     out.s = dot(v1, m);
@@ -314,21 +326,21 @@ inline Q quat_between_unit_vectors(V3 v1, V3 v2) {
   return normalize_quat(out);
 }
 
-struct SegResult { V3 p1, p2; float f1, f2; };
+struct SegResult { V3 p1, p2; real f1, f2; };
 
 inline SegResult line_distance(V3 p1, V3 d1, V3 p2, V3 d2) {                      // :1069
   SegResult r;
-  float a11 = dot(d1, d1), a12 = -dot(d1, d2), a21 = dot(d2, d1), a22 = -dot(d2, d2);
+  real a11 = dot(d1, d1), a12 = -dot(d1, d2), a21 = dot(d2, d1), a22 = -dot(d2, d2);
   V3 w = p1 - p2;
-  float b1 = -dot(d1, w), b2 = -dot(d2, w);
-  float d = a11 * a22 - a12 * a21;
+  real b1 = -dot(d1, w), b2 = -dot(d2, w);
+  real d = a11 * a22 - a12 * a21;
   if (d * d < 1000.0f * kMinPositive) {
-    float s1 = dot(p2 - p1, d1) / dot(d1, d1);
+    real s1 = dot(p2 - p1, d1) / dot(d1, d1);
     r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = p2; r.f2 = 0.0f;
     return r;
   }
-  float s1 = (a22 * b1 - a12 * b2) / d;
-  float s2 = (a11 * b2 - a21 * b1) / d;
+  real s1 = (a22 * b1 - a12 * b2) / d;
+  real s2 = (a11 * b2 - a21 * b1) / d;
   r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = mul_add(p2, s2, d2); r.f2 = s2;
   return r;
 }
@@ -336,21 +348,21 @@ inline SegResult line_distance(V3 p1, V3 d1, V3 p2, V3 d2) {                    
 inline SegResult segment_distance(V3 p1, V3 q1, V3 p2, V3 q2) {                   // :1105
   SegResult r;
   V3 d1 = q1 - p1, d2 = q2 - p2, rr = p1 - p2;
-  float a = dot(d1, d1), b = dot(d1, d2), c = dot(d1, rr), e = dot(d2, d2), f = dot(d2, rr);
+  real a = dot(d1, d1), b = dot(d1, d2), c = dot(d1, rr), e = dot(d2, d2), f = dot(d2, rr);
   if (a < 100.0f * kEps && e < 100.0f * kEps) {
     r.p1 = p1; r.f1 = 0; r.p2 = p2; r.f2 = 0; return r;
   }
   if (a < 100.0f * kEps) {
-    float s2 = clampf(f / e, 0.0f, 1.0f);
+    real s2 = clampf(f / e, 0.0f, 1.0f);
     r.p1 = p1; r.f1 = 0; r.p2 = mul_add(p2, s2, d2); r.f2 = s2; return r;
   }
   if (e < 100.0f * kEps) {
-    float s1 = clampf(-c / a, 0.0f, 1.0f);
+    real s1 = clampf(-c / a, 0.0f, 1.0f);
     r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = p2; r.f2 = 0; return r;
   }
-  float denom = a * e - b * b;
-  float s1 = denom > 1000.0f * kMinPositive ? clampf((b * f - c * e) / denom, 0.0f, 1.0f) : 0.0f;
-  float s2 = (b * s1 + f) / e;
+  real denom = a * e - b * b;
+  real s1 = denom > 1000.0f * kMinPositive ? clampf((b * f - c * e) / denom, 0.0f, 1.0f) : 0.0f;
+  real s2 = (b * s1 + f) / e;
   if (s2 < 0.0f) {
     s1 = clampf(-c / a, 0.0f, 1.0f);
     s2 = 0.0f;
@@ -364,32 +376,32 @@ inline SegResult segment_distance(V3 p1, V3 q1, V3 p2, V3 q2) {                 
 
 inline V3 point_to_segment(V3 a, V3 b, V3 q) {                                    // :1169
   V3 ab = b - a, aq = q - a;
-  float alpha = dot(ab, aq);
+  real alpha = dot(ab, aq);
   if (alpha <= 0.0f) return a;
-  float den = dot(ab, ab);
+  real den = dot(ab, ab);
   if (alpha > den) return b;
   alpha /= den;
   return mul_add(a, alpha, ab);
 }
 
-inline M3 steiner(float mass, V3 o) {                                             // :1189
-  float ixx = mass * (o.y * o.y + o.z * o.z);
-  float iyy = mass * (o.x * o.x + o.z * o.z);
-  float izz = mass * (o.x * o.x + o.y * o.y);
-  float ixy = -mass * o.x * o.y;
-  float ixz = -mass * o.x * o.z;
-  float iyz = -mass * o.y * o.z;
+inline M3 steiner(real mass, V3 o) {                                             // :1189
+  real ixx = mass * (o.y * o.y + o.z * o.z);
+  real iyy = mass * (o.x * o.x + o.z * o.z);
+  real izz = mass * (o.x * o.x + o.y * o.y);
+  real ixy = -mass * o.x * o.y;
+  real ixz = -mass * o.x * o.z;
+  real iyz = -mass * o.y * o.z;
   return m3(v3(ixx, ixy, ixz), v3(ixy, iyy, iyz), v3(ixz, iyz, izz));
 }
 
 // collision/internal_math.rs
-inline float dot2(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
+inline real dot2(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
 inline V2 mul_mv2(M2 m, V2 a) { return v2(m.cx.x * a.x + m.cy.x * a.y, m.cx.y * a.x + m.cy.y * a.y); }
 inline M2 invert2(M2 m) {                                                         // :183
-  float d = m.cx.x * m.cy.y - m.cx.y * m.cy.x;
+  real d = m.cx.x * m.cy.y - m.cx.y * m.cy.x;
   M2 r;
   if (absf(d) > 1000.0f * kMinPositive) {
-    float inv = 1.0f / d;
+    real inv = 1.0f / d;
     r.cx = v2(inv * m.cy.y, -inv * m.cx.y);
     r.cy = v2(-inv * m.cy.x, inv * m.cx.x);
   } else {
@@ -398,9 +410,9 @@ inline M2 invert2(M2 m) {                                                       
   return r;
 }
 inline V2 solve2(M2 m, V2 b) {                                                    // :197
-  float d = m.cx.x * m.cy.y - m.cx.y * m.cy.x;
+  real d = m.cx.x * m.cy.y - m.cx.y * m.cy.x;
   if (d > 1000.0f * kMinPositive) {
-    float inv = 1.0f / d;
+    real inv = 1.0f / d;
     return v2(inv * m.cy.y * b.x - inv * m.cy.x * b.y, -inv * m.cx.y * b.x + inv * m.cx.x * b.y);
   }
   return v2(0, 0);
@@ -411,18 +423,18 @@ inline V3 modified_cross(V3 a, V3 b) {                                          
 inline V3 arbitrary_perp(V3 v) {                                                  // :278
   V3 p;
   if (v.x < -0.5f || v.x > 0.5f) {
-    const float a = 0.67f, b = -0.42f;
+    const real a = 0.67f, b = -0.42f;
     p = v3(a * v.y + b * v.z, -a * v.x, -b * v.x);
   } else if (v.y < -0.5f || v.y > 0.5f) {
-    const float a = 0.67f, c = -0.42f;
+    const real a = 0.67f, c = -0.42f;
     p = v3(a * v.y, -a * v.x + c * v.z, -c * v.y);
   } else {
-    const float a = 0.67f, b = -0.42f;
+    const real a = 0.67f, b = -0.42f;
     p = v3(a * v.z, b * v.z, -a * v.x - b * v.y);
   }
   return normalize(p);
 }
-inline float scalar_triple(V3 a, V3 b, V3 c) {                                    // :299
+inline real scalar_triple(V3 a, V3 b, V3 c) {                                    // :299
   V3 d = v3(b.y * c.z - b.z * c.y, b.z * c.x - b.x * c.z, b.x * c.y - b.y * c.x);
   return a.x * d.x + a.y * d.y + a.z * d.z;
 }
@@ -435,7 +447,7 @@ inline Plane transform_plane(Xf t, Plane p) {                                   
   V3 n = rotate(t.q, p.n);
   return plane(n, p.off + dot(n, t.p));
 }
-inline float plane_sep(Plane p, V3 x) { return dot(p.n, x) - p.off; }            // :362
+inline real plane_sep(Plane p, V3 x) { return dot(p.n, x) - p.off; }            // :362
 inline M3 rotate_inertia(Q q, M3 c) {                                             // :378
   M3 r = matrix_from_quat(q);
   return mul_mm(r, mul_mm(c, transpose(r)));

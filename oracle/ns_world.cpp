@@ -38,14 +38,14 @@ struct BodySim {
   WXf transform;
   Pos center;
   uint32_t flags;
-  float min_extent;
+  real min_extent;
   V3 max_extent;
   Q rotation0;
   Pos center0;
   V3 local_center, force, torque;
-  float inv_mass;
+  real inv_mass;
   M3 inertia, inv_inertia_local, inv_inertia_world;
-  float linear_damping, angular_damping, gravity_scale;
+  real linear_damping, angular_damping, gravity_scale;
   int body_id;
 };
 struct BodyState { V3 v; V3 w; V3 dp; uint32_t flags; Q dq; };
@@ -55,14 +55,14 @@ struct Body {
   int head_shape = -1, shape_count = 0;
   int joint_count = 0;
   uint32_t flags = 0;
-  float sleep_threshold = 0, sleep_time = 0, safety_factor = 0.5f, mass = 0;
+  real sleep_threshold = 0, sleep_time = 0, safety_factor = 0.5f, mass = 0;
 };
 
 struct Shape {
   int id = -1, body_id = -1, next_shape = -1, type = kSphere;
-  float density = 0, aabb_margin = 0;
+  real density = 0, aabb_margin = 0;
   AABB aabb;
-  float friction = 0.6f, restitution = 0, rolling = 0;
+  real friction = 0.6f, restitution = 0, rolling = 0;
   uint64_t category = 1, mask = ~0ull;
   int group = 0;
   Hull hull;
@@ -73,14 +73,14 @@ struct Shape {
 
 struct ManifoldPoint {
   V3 anchor_a, anchor_b;
-  float separation, normal_impulse, total_normal_impulse, normal_velocity, base_separation;
+  real separation, normal_impulse, total_normal_impulse, normal_velocity, base_separation;
   uint32_t feature_id;
   bool persisted;
 };
 struct Manifold {
   ManifoldPoint points[4];
   V3 normal;
-  float twist_impulse;
+  real twist_impulse;
   V3 friction_impulse, rolling_impulse;
   int point_count;
 };
@@ -94,22 +94,22 @@ struct Contact {
   int manifold_count = 0;
   Q cached_rot_a, cached_rot_b;
   Xf cached_rel;
-  float friction = 0, restitution = 0, rolling = 0;
+  real friction = 0, restitution = 0, rolling = 0;
   V3 tangent_velocity = {0, 0, 0};
   SATCache sat;
   SimplexCache simplex;
 };
 
-struct Softness { float bias_rate, mass_scale, impulse_scale; };
+struct Softness { real bias_rate, mass_scale, impulse_scale; };
 
 // solver_integration.rs:72 make_soft
-static Softness make_soft(float hertz, float zeta, float h) {
+static Softness make_soft(real hertz, real zeta, real h) {
   Softness s = {0, 0, 0};
   if (hertz == 0.0f) return s;
-  float omega = 2.0f * kPi * hertz;
-  float a1 = 2.0f * zeta + h * omega;
-  float a2 = h * omega * a1;
-  float a3 = 1.0f / (1.0f + a2);
+  real omega = 2.0f * kPi * hertz;
+  real a1 = 2.0f * zeta + h * omega;
+  real a2 = h * omega * a1;
+  real a3 = 1.0f / (1.0f + a2);
   s.bias_rate = omega / a1;
   s.mass_scale = a2 * a3;
   s.impulse_scale = a3;
@@ -117,7 +117,7 @@ static Softness make_soft(float hertz, float zeta, float h) {
 }
 
 // contact_solver.rs:38-139 symmetric 3x3
-struct Sym { float xx, xy, xz, yy, yz, zz; };
+struct Sym { real xx, xy, xz, yy, yz, zz; };
 static Sym sym_from(M3 m) { Sym s = {m.cx.x, m.cx.y, m.cx.z, m.cy.y, m.cy.z, m.cz.z}; return s; }
 static Sym sym_zero() { Sym s = {0, 0, 0, 0, 0, 0}; return s; }
 static V3 sym_mv(Sym s, V3 a) {
@@ -129,15 +129,15 @@ static Sym sym_add(Sym a, Sym b) {
   return s;
 }
 static Sym sym_invert(Sym m) {
-  float cxx = m.yy * m.zz - m.yz * m.yz;
-  float cxy = m.xz * m.yz - m.xy * m.zz;
-  float cxz = m.xy * m.yz - m.xz * m.yy;
-  float cyy = m.xx * m.zz - m.xz * m.xz;
-  float cyz = m.xy * m.xz - m.xx * m.yz;
-  float czz = m.xx * m.yy - m.xy * m.xy;
-  float d = m.xx * cxx + (m.xy * cxy + m.xz * cxz);
+  real cxx = m.yy * m.zz - m.yz * m.yz;
+  real cxy = m.xz * m.yz - m.xy * m.zz;
+  real cxz = m.xy * m.yz - m.xz * m.yy;
+  real cyy = m.xx * m.zz - m.xz * m.xz;
+  real cyz = m.xy * m.xz - m.xx * m.yz;
+  real czz = m.xx * m.yy - m.xy * m.xy;
+  real d = m.xx * cxx + (m.xy * cxy + m.xz * cxz);
   bool valid = absf(d) > 1000.0f * kMinPositive;
-  float inv = valid ? 1.0f / d : 0.0f;
+  real inv = valid ? 1.0f / d : 0.0f;
   Sym s = {inv * cxx, inv * cxy, inv * cxz, inv * cyy, inv * cyz, inv * czz};
   return s;
 }
@@ -151,40 +151,40 @@ static V3 inv_rotate_wide(Q q, V3 a) {
 
 struct ConstraintPoint {
   V3 r_a, r_b;
-  float base_separation, relative_velocity, normal_impulse, total_normal_impulse,
+  real base_separation, relative_velocity, normal_impulse, total_normal_impulse,
       restitution_impulse, normal_mass, lever_arm;
 };
 struct ManifoldConstraint {
   ConstraintPoint points[4];
   int point_count;
   V3 normal, tangent1, tangent2, center_a, center_b;
-  float twist_mass, twist_impulse;
+  real twist_mass, twist_impulse;
   M2 tangent_mass;
   V2 friction_impulse;
   V3 rolling_impulse;
-  float tangent_velocity1, tangent_velocity2;
+  real tangent_velocity1, tangent_velocity2;
 };
 struct ContactConstraint {
   int contact_id, index_a, index_b;
-  float inv_mass_a, inv_mass_b;
+  real inv_mass_a, inv_mass_b;
   Sym inv_ia, inv_ib, rolling_mass;
   Softness softness;
-  float friction, restitution, rolling_resistance;
+  real friction, restitution, rolling_resistance;
   bool is_static;
   ManifoldConstraint m;  // convex contacts carry exactly one manifold
 };
 struct OverflowConstraint {
   int contact_id, index_a, index_b;
-  float inv_mass_a, inv_mass_b;
+  real inv_mass_a, inv_mass_b;
   M3 inv_ia, inv_ib, rolling_mass;
   Softness softness;
-  float friction, restitution, rolling_resistance;
+  real friction, restitution, rolling_resistance;
   int manifold_count;
   ManifoldConstraint m;
 };
 
 struct StepContext {
-  float dt, inv_dt, h, inv_h;
+  real dt, inv_dt, h, inv_h;
   int sub_step_count;
   Softness contact_softness, static_softness;
   bool enable_warm_starting;
@@ -296,21 +296,21 @@ AABB shape_local_aabb(const Shape& s, Q q) {
   if (s.type == kHull) return aabb_transform(t, s.hull.bounds);
   if (s.type == kSphere) {  // sphere.rs:27
     V3 c = xf_point(t, s.sphere.center);
-    float r = s.sphere.radius;
+    real r = s.sphere.radius;
     V3 e = v3(r, r, r);
     return aabb(c - e, c + e);
   }
   V3 c1 = xf_point(t, s.capsule.c1), c2 = xf_point(t, s.capsule.c2);  // capsule.rs:66
-  float r = s.capsule.radius;
+  real r = s.capsule.radius;
   V3 e = v3(r, r, r);
   return aabb(min3(c1, c2) - e, max3(c1, c2) + e);
 }
 // shape_runtime.rs:420 compute_fat_shape_aabb
-AABB fat_shape_aabb(const Shape& s, WXf t, float extra) {
+AABB fat_shape_aabb(const Shape& s, WXf t, real extra) {
   return offset_aabb(aabb_inflate(shape_local_aabb(s, t.q), extra), t.p);
 }
 
-struct MassData { float mass; V3 center; M3 inertia; };
+struct MassData { real mass; V3 center; M3 inertia; };
 MassData shape_mass(const Shape& s) {
   MassData md;
   if (s.type == kHull) {  // shape_runtime.rs:312
@@ -318,29 +318,29 @@ MassData shape_mass(const Shape& s) {
     md.center = s.hull.center;
     md.inertia = mul_sm(s.density, s.hull.central_inertia);
   } else if (s.type == kSphere) {  // sphere.rs:13
-    float r = s.sphere.radius;
-    float volume = 4.0f / 3.0f * kPi * r * r * r;
-    float mass = volume * s.density;
-    float ixx = 0.4f * mass * r * r;
+    real r = s.sphere.radius;
+    real volume = 4.0f / 3.0f * kPi * r * r * r;
+    real mass = volume * s.density;
+    real ixx = 0.4f * mass * r * r;
     md.mass = mass;
     md.center = s.sphere.center;
     md.inertia = diag(ixx, ixx, ixx);
   } else {  // capsule.rs:27
     V3 c1 = s.capsule.c1, c2 = s.capsule.c2;
-    float r = s.capsule.radius;
-    float h = distance(c1, c2);
-    float cyl_vol = kPi * r * r * h;
-    float cyl_mass = cyl_vol * s.density;
-    float sph_vol = (4.0f / 3.0f) * kPi * r * r * r;
-    float sph_mass = sph_vol * s.density;
+    real r = s.capsule.radius;
+    real h = distance(c1, c2);
+    real cyl_vol = kPi * r * r * h;
+    real cyl_mass = cyl_vol * s.density;
+    real sph_vol = (4.0f / 3.0f) * kPi * r * r * r;
+    real sph_mass = sph_vol * s.density;
     // geometry_queries.rs cylinder_inertia / sphere_inertia
-    float cyl_lateral = cyl_mass * (3.0f * r * r + h * h) / 12.0f;
-    float cyl_axial = 0.5f * cyl_mass * r * r;
+    real cyl_lateral = cyl_mass * (3.0f * r * r + h * h) / 12.0f;
+    real cyl_axial = 0.5f * cyl_mass * r * r;
     M3 cyl = diag(cyl_lateral, cyl_axial, cyl_lateral);
-    float sph_i = 0.4f * sph_mass * r * r;
+    real sph_i = 0.4f * sph_mass * r * r;
     M3 sph = diag(sph_i, sph_i, sph_i);
     M3 inertia = add_mm(cyl, sph);
-    float st = 0.125f * sph_mass * (3.0f * r + 2.0f * h) * h;
+    real st = 0.125f * sph_mass * (3.0f * r + 2.0f * h) * h;
     inertia.cx.x += st;
     inertia.cz.z += st;
     M3 rot = identity_m3();
@@ -356,16 +356,16 @@ MassData shape_mass(const Shape& s) {
   return md;
 }
 
-struct Extent { float min_extent; V3 max_extent; };
+struct Extent { real min_extent; V3 max_extent; };
 Extent shape_extent(const Shape& s, V3 lc) {  // shape_runtime.rs:499
   Extent e;
   if (s.type == kCapsule) {
-    float r = s.capsule.radius;
+    real r = s.capsule.radius;
     e.min_extent = r;
     V3 c1 = s.capsule.c1 - lc, c2 = s.capsule.c2 - lc;
     e.max_extent = max3(abs3(c1), abs3(c2)) + v3(r, r, r);
   } else if (s.type == kSphere) {
-    float r = s.sphere.radius;
+    real r = s.sphere.radius;
     e.min_extent = r;
     e.max_extent = abs3(s.sphere.center - lc) + v3(r, r, r);
   } else {  // hull_queries.rs:101
@@ -382,11 +382,11 @@ void update_isotropic_inertia(nso_world* w, int bi) {
   Body& b = w->bodies[bi];
   BodySim& s = sim_of(w, b);
   M3 I = s.inertia;
-  float mean = (I.cx.x + I.cy.y + I.cz.z) / 3.0f;
-  float dx = I.cx.x - mean, dy = I.cy.y - mean, dz = I.cz.z - mean;
-  float off = I.cy.x * I.cy.x + I.cz.x * I.cz.x + I.cz.y * I.cz.y;
-  float dev = dx * dx + dy * dy + dz * dz + 2.0f * off;
-  float tol = 0.2f;  // world isotropic_inertia_tolerance default (world_runtime.rs:1256)
+  real mean = (I.cx.x + I.cy.y + I.cz.z) / 3.0f;
+  real dx = I.cx.x - mean, dy = I.cy.y - mean, dz = I.cz.z - mean;
+  real off = I.cy.x * I.cy.x + I.cz.x * I.cz.x + I.cz.y * I.cz.y;
+  real dev = dx * dx + dy * dy + dz * dz + 2.0f * off;
+  real tol = 0.2f;  // world isotropic_inertia_tolerance default (world_runtime.rs:1256)
   if (2.0f * dev > 3.0f * tol * tol * mean * mean) b.flags |= kGyroscopic;
   else b.flags &= ~kGyroscopic;
   sync_body_flags(w, bi);
@@ -432,7 +432,7 @@ void update_body_mass(nso_world* w, int bi) {
     M3 I = add_mm(md.inertia, steiner(md.mass, off));
     s.inertia = add_mm(s.inertia, I);
   }
-  float d = det(s.inertia);
+  real d = det(s.inertia);
   if (d > 0.0f) {
     s.inv_inertia_local = invert_t(s.inertia);
     M3 R = matrix_from_quat(s.transform.q);
@@ -459,12 +459,12 @@ void update_body_mass(nso_world* w, int bi) {
 }
 
 // shape_creation.rs:199 compute_shape_margin
-float shape_margin(const Shape& s) {
-  float margin = 0.0f;
+real shape_margin(const Shape& s) {
+  real margin = 0.0f;
   if (s.type == kSphere) margin = s.sphere.radius;
   else if (s.type == kCapsule) margin = 0.5f * distance(s.capsule.c2, s.capsule.c1) + s.capsule.radius;
   else {
-    float mx = 0.0f;
+    real mx = 0.0f;
     for (int i = 0; i < s.hull.vertex_count; ++i)
       mx = maxf(mx, distance_sq(s.hull.points[i], s.hull.center));
     margin = std::sqrt(mx);
@@ -488,10 +488,10 @@ int create_shape(nso_world* w, int bi, const nso_shape_def* def, Shape sh) {
   sh.is_static = b.type == 0;
   // shape_creation.rs:236 update_shape_aabbs at the body's current transform
   const BodySim& s = sim_of(w, b);
-  float spec = speculative_distance();
+  real spec = speculative_distance();
   AABB a = fat_shape_aabb(sh, s.transform, spec);
   sh.aabb = a;
-  float margin = b.type == 0 ? spec : sh.aabb_margin;
+  real margin = b.type == 0 ? spec : sh.aabb_margin;
   w->fat.push_back(aabb_inflate(a, margin));
   // broad_phase.rs:73 -- static proxies are marked only when contact creation is forced,
   // which ShapeDef's default (invoke_contact_creation = true) does.
@@ -566,8 +566,8 @@ void create_contact(nso_world* w, int sa, int sb) {
   if (ba.type == 0 || bb.type == 0) c.flags |= cStatic;
   c.flags |= cSpeculative;  // enable_speculative world + shape defaults
   if ((ba.flags & kEnableRecycling) && (bb.flags & kEnableRecycling)) c.flags |= cRecycle;
-  float ra = A.type == kSphere ? A.sphere.radius : (A.type == kCapsule ? A.capsule.radius : 0.0f);
-  float rb = B.type == kSphere ? B.sphere.radius : (B.type == kCapsule ? B.capsule.radius : 0.0f);
+  real ra = A.type == kSphere ? A.sphere.radius : (A.type == kCapsule ? A.capsule.radius : 0.0f);
+  real rb = B.type == kSphere ? B.sphere.radius : (B.type == kCapsule ? B.capsule.radius : 0.0f);
   c.rolling = maxf(A.rolling, B.rolling) * maxf(ra, rb);
   w->pair_set.insert(pair_key(sa, sb));
   w->contacts[cid] = c;
@@ -584,7 +584,7 @@ void update_pairs(nso_world* w) {
   if (!any) return;
   std::vector<int> small, large;
   for (int i = 0; i < n; ++i) {
-    float wx = w->fat[i].hi.x - w->fat[i].lo.x;
+    real wx = w->fat[i].hi.x - w->fat[i].lo.x;
     if (w->shapes[i].is_static && wx > 8.0f) large.push_back(i);
     else small.push_back(i);
   }
@@ -615,7 +615,7 @@ void update_pairs(nso_world* w) {
 #pragma omp for schedule(dynamic, 64)
     for (int i = 0; i < ns_; ++i) {
       int a = small[i];
-      float hx = w->fat[a].hi.x;
+      real hx = w->fat[a].hi.x;
       for (int j = i + 1; j < ns_; ++j) {
         int b = small[j];
         if (w->fat[b].lo.x > hx) break;
@@ -798,26 +798,26 @@ void collide_one(nso_world* w, int cid, std::vector<uint8_t>& bits) {
   bool was_touching = (c.flags & cSimTouching) != 0;
   WXf xa = sa.transform, xb = sb.transform;
   bool is_fast = ((sa.flags | sb.flags) & kIsFast) != 0;
-  float recycle = contact_recycle_distance();
-  float spec = speculative_distance();
-  float recycle_nt = minf(recycle, spec);
-  float tol = was_touching ? recycle : recycle_nt;
+  real recycle = contact_recycle_distance();
+  real spec = speculative_distance();
+  real recycle_nt = minf(recycle, spec);
+  real tol = was_touching ? recycle : recycle_nt;
   if (!is_fast && recycle > 0.0f && (c.flags & cRelativeValid) && (c.flags & cRecycle)) {
-    float ang_a = dot_quat(xa.q, c.cached_rot_a);
-    float ang_b = dot_quat(xb.q, c.cached_rot_b);
-    float ang = minf(ang_a * ang_a, ang_b * ang_b);
+    real ang_a = dot_quat(xa.q, c.cached_rot_a);
+    real ang_b = dot_quat(xb.q, c.cached_rot_b);
+    real ang = minf(ang_a * ang_a, ang_b * ang_b);
     Xf x = inv_mul_wxf(xa, xb);
     Xf xc = c.cached_rel;
     V3 mea = c.encoded_a < -1 ? v3(0, 0, 0) : sa.max_extent;
     V3 meb = c.encoded_b < -1 ? v3(0, 0, 0) : sb.max_extent;
     V3 me = max3(mea, meb);
-    float dsq = distance_sq(x.p, xc.p);
+    real dsq = distance_sq(x.p, xc.p);
     if (ang > kRecycleAngular && dsq < tol * tol) {
-      float dist = std::sqrt(dsq);
-      float slack = tol - dist;
+      real dist = std::sqrt(dsq);
+      real slack = tol - dist;
       Q qr = inv_mul_quat(xc.q, x.q);
       V3 arc = modified_cross(abs3(qr.v), me);
-      float arc_sq = 4.0f * length_sq(arc);
+      real arc_sq = 4.0f * length_sq(arc);
       if (arc_sq < slack * slack) {
         Q dqa = mul_quat(xa.q, conjugate(c.cached_rot_a));
         Q dqb = mul_quat(xb.q, conjugate(c.cached_rot_b));
@@ -895,8 +895,8 @@ void set_state(nso_world* w, int i, const BodyState& s) {
 }
 
 // contact_solver.rs:445 prepare_contact_constraint
-ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness static_soft, float ws) {
-  float inv_tau = 1.0f / speculative_distance();
+ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness static_soft, real ws) {
+  real inv_tau = 1.0f / speculative_distance();
   const Contact& ct = w->contacts[cid];
   ContactConstraint c;
   std::memset(&c, 0, sizeof(c));
@@ -928,7 +928,7 @@ ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness
   mc.friction_impulse = v2(ws * dot(man.friction_impulse, mc.tangent1), ws * dot(man.friction_impulse, mc.tangent2));
   V3 normal = mc.normal, t1 = mc.tangent1, t2 = mc.tangent2;
   V3 ca = v3(0, 0, 0), cb = v3(0, 0, 0);
-  float tw = 0.0f;
+  real tw = 0.0f;
   for (int i = 0; i < man.point_count; ++i) {
     const ManifoldPoint& mp = man.points[i];
     ConstraintPoint& cp = mc.points[i];
@@ -939,12 +939,12 @@ ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness
     cp.total_normal_impulse = 0.0f;
     cp.relative_velocity = 0.0f;
     cp.restitution_impulse = 0.0f;
-    float weight = clampf(2.0f - mp.separation * inv_tau, kMinFrictionWeight, 1.0f);
+    real weight = clampf(2.0f - mp.separation * inv_tau, kMinFrictionWeight, 1.0f);
     ca = ca + weight * cp.r_a;
     cb = cb + weight * cp.r_b;
     tw += weight;
     V3 rna = cross(cp.r_a, normal), rnb = cross(cp.r_b, normal);
-    float k = c.inv_mass_a + c.inv_mass_b;
+    real k = c.inv_mass_a + c.inv_mass_b;
     k += dot(rna, sym_mv(c.inv_ia, rna));
     k += dot(rnb, sym_mv(c.inv_ib, rnb));
     cp.normal_mass = k > 0.0f ? 1.0f / k : 0.0f;
@@ -965,17 +965,17 @@ ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness
     V3 rtb1 = cross(mc.center_b, t1), rtb2 = cross(mc.center_b, t2);
     V3 ia1 = sym_mv(c.inv_ia, rta1), ia2 = sym_mv(c.inv_ia, rta2);
     V3 ib1 = sym_mv(c.inv_ib, rtb1), ib2 = sym_mv(c.inv_ib, rtb2);
-    float msum = c.inv_mass_a + c.inv_mass_b;
-    float kxx = (msum + dot(rta1, ia1)) + dot(rtb1, ib1);
-    float kyy = (msum + dot(rta2, ia2)) + dot(rtb2, ib2);
-    float kxy = dot(rta1, ia2) + dot(rtb1, ib2);
-    float d = kxx * kyy - kxy * kxy;
+    real msum = c.inv_mass_a + c.inv_mass_b;
+    real kxx = (msum + dot(rta1, ia1)) + dot(rtb1, ib1);
+    real kyy = (msum + dot(rta2, ia2)) + dot(rtb2, ib2);
+    real kxy = dot(rta1, ia2) + dot(rtb1, ib2);
+    real d = kxx * kyy - kxy * kxy;
     bool valid = absf(d) > 1000.0f * kMinPositive && tw > 0.0f;
-    float inv = valid ? 1.0f / d : 0.0f;
+    real inv = valid ? 1.0f / d : 0.0f;
     mc.tangent_mass.cx = v2(inv * kyy, -(inv * kxy));
     mc.tangent_mass.cy = v2(-(inv * kxy), inv * kxx);
   }
-  float ktw = dot(normal, sym_mv(inv_iab, normal));
+  real ktw = dot(normal, sym_mv(inv_iab, normal));
   mc.twist_mass = ktw > 0.0f ? 1.0f / ktw : 0.0f;
   if (ct.restitution > 0.0f) {
     BodyState sa = state_at(w, ia), sb = state_at(w, ib);
@@ -992,8 +992,8 @@ ContactConstraint prepare_contact(nso_world* w, int cid, Softness soft, Softness
 // overflow_contact_solver.rs:92 prepare_overflow_contacts
 void prepare_overflow(nso_world* w, Softness soft, Softness static_soft) {
   w->overflow.clear();
-  float ws = w->def.enable_warm_starting ? 1.0f : 0.0f;
-  float inv_tau = 1.0f / speculative_distance();
+  real ws = w->def.enable_warm_starting ? 1.0f : 0.0f;
+  real inv_tau = 1.0f / speculative_distance();
   for (int cid : w->colors[kOverflowIndex].overflow) {
     Contact& ct = w->contacts[cid];
     OverflowConstraint c;
@@ -1004,7 +1004,7 @@ void prepare_overflow(nso_world* w, Softness soft, Softness static_soft) {
     c.inv_ia = m3zero(); c.inv_ib = m3zero();
     if (ia >= 0) { c.inv_mass_a = w->awake_sims[ia].inv_mass; c.inv_ia = w->awake_sims[ia].inv_inertia_world; }
     if (ib >= 0) { c.inv_mass_b = w->awake_sims[ib].inv_mass; c.inv_ib = w->awake_sims[ib].inv_inertia_world; }
-    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    real mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
     c.rolling_mass = invert_matrix(add_mm(iA, iB));
     c.softness = (ct.flags & cStatic) ? static_soft : soft;
@@ -1026,18 +1026,18 @@ void prepare_overflow(nso_world* w, Softness soft, Softness static_soft) {
       mc.tangent_velocity1 = dot(ct.tangent_velocity, t1);
       mc.tangent_velocity2 = dot(ct.tangent_velocity, t2);
       V3 ca = v3(0, 0, 0), cb = v3(0, 0, 0);
-      float tw = 0.0f;
+      real tw = 0.0f;
       for (int i = 0; i < pc; ++i) {
         ConstraintPoint cp;
         std::memset(&cp, 0, sizeof(cp));
         const ManifoldPoint& mp = man.points[i];
         cp.r_a = mp.anchor_a; cp.r_b = mp.anchor_b;
-        float s = mp.separation;
+        real s = mp.separation;
         cp.base_separation = s - dot(cp.r_b - cp.r_a, n);
         cp.normal_impulse = ws * mp.normal_impulse;
         V3 ra = cp.r_a, rb = cp.r_b;
         V3 rna = cross(ra, n), rnb = cross(rb, n);
-        float k = mA + mB + dot(rna, mul_mv(iA, rna)) + dot(rnb, mul_mv(iB, rnb));
+        real k = mA + mB + dot(rna, mul_mv(iA, rna)) + dot(rnb, mul_mv(iB, rnb));
         cp.normal_mass = k > 0.0f ? 1.0f / k : 0.0f;
         if (sample) {
           V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
@@ -1046,13 +1046,13 @@ void prepare_overflow(nso_world* w, Softness soft, Softness static_soft) {
           cp.relative_velocity = 0.0f;
         }
         man.points[i].normal_velocity = 0.0f;
-        float weight = clampf(2.0f - s * inv_tau, kMinFrictionWeight, 1.0f);
+        real weight = clampf(2.0f - s * inv_tau, kMinFrictionWeight, 1.0f);
         ca = mul_add(ca, weight, ra);
         cb = mul_add(cb, weight, rb);
         tw += weight;
         mc.points[i] = cp;
       }
-      float iw = 1.0f / tw;
+      real iw = 1.0f / tw;
       ca = iw * ca; cb = iw * cb;
       mc.center_a = ca; mc.center_b = cb;
       for (int i = 0; i < pc; ++i) mc.points[i].lever_arm = distance(mc.points[i].r_a, ca);
@@ -1064,7 +1064,7 @@ void prepare_overflow(nso_world* w, Softness soft, Softness static_soft) {
       k.cy.x = k.cx.y;
       mc.tangent_mass = invert2(k);
       mc.friction_impulse = v2(ws * dot(man.friction_impulse, t1), ws * dot(man.friction_impulse, t2));
-      float ktw = dot(n, mul_mv(add_mm(iA, iB), n));
+      real ktw = dot(n, mul_mv(add_mm(iA, iB), n));
       mc.twist_mass = ktw > 0.0f ? 1.0f / ktw : 0.0f;
       mc.twist_impulse = ws * man.twist_impulse;
       mc.rolling_impulse = ws * man.rolling_impulse;
@@ -1078,11 +1078,11 @@ void prepare_all(nso_world* w) {
   w->any_restitution = false;
   prepare_joints(w->joints, w->awake_sims, w->static_sims, w->bodies.data(), w->ctx.h, w->ctx.inv_h,
                  w->def.enable_warm_starting ? 1.0f : 0.0f);
-  float hz = minf(w->def.contact_hertz, 0.125f * w->ctx.inv_h);
+  real hz = minf(w->def.contact_hertz, 0.125f * w->ctx.inv_h);
   Softness soft = make_soft(hz, w->def.contact_damping_ratio, w->ctx.h);
   Softness stat = make_soft(2.0f * hz, 0.5f * w->def.contact_damping_ratio, w->ctx.h);
   prepare_overflow(w, soft, stat);
-  float ws = w->def.enable_warm_starting ? 1.0f : 0.0f;
+  real ws = w->def.enable_warm_starting ? 1.0f : 0.0f;
   for (int ci = 0; ci < kOverflowIndex; ++ci) {
     const std::vector<int>& ids = w->colors[ci].convex;
     std::vector<ContactConstraint>& out = w->constraints[ci];
@@ -1096,7 +1096,7 @@ void prepare_all(nso_world* w) {
 }
 
 // solver_integration.rs:263 integrate_velocities_range
-void integrate_velocities(nso_world* w, float h) {
+void integrate_velocities(nso_world* w, real h) {
   V3 g = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
   const int n_ = (int)w->awake_sims.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
@@ -1104,9 +1104,9 @@ void integrate_velocities(nso_world* w, float h) {
     const BodySim& sim = w->awake_sims[i];
     BodyState& st = w->awake_states[i];
     V3 v = st.v, wv = st.w;
-    float ld = 1.0f / (1.0f + h * sim.linear_damping);
-    float ad = 1.0f / (1.0f + h * sim.angular_damping);
-    float gs = sim.inv_mass > 0.0f ? sim.gravity_scale : 0.0f;
+    real ld = 1.0f / (1.0f + h * sim.linear_damping);
+    real ad = 1.0f / (1.0f + h * sim.angular_damping);
+    real gs = sim.inv_mass > 0.0f ? sim.gravity_scale : 0.0f;
     V3 lvd = blend2(h * sim.inv_mass, sim.force, h * gs, g);
     v = mul_add(lvd, ld, v);
     V3 avd = h * mul_mv(sim.inv_inertia_world, sim.torque);
@@ -1116,13 +1116,13 @@ void integrate_velocities(nso_world* w, float h) {
       Q q = mul_quat(st.dq, q0);
       V3 om1 = inv_rotate(q, wv);
       V3 om2 = om1;
-      float i00 = sim.inertia.cx.x, i01 = sim.inertia.cy.x, i02 = sim.inertia.cz.x;
-      float i11 = sim.inertia.cy.y, i12 = sim.inertia.cz.y, i22 = sim.inertia.cz.z;
+      real i00 = sim.inertia.cx.x, i01 = sim.inertia.cy.x, i02 = sim.inertia.cz.x;
+      real i11 = sim.inertia.cy.y, i12 = sim.inertia.cz.y, i22 = sim.inertia.cz.z;
       {
-        float w1 = om2.x, w2 = om2.y, w3 = om2.z;
-        float iw1 = i00 * w1 + i01 * w2 + i02 * w3;
-        float iw2 = i01 * w1 + i11 * w2 + i12 * w3;
-        float iw3 = i02 * w1 + i12 * w2 + i22 * w3;
+        real w1 = om2.x, w2 = om2.y, w3 = om2.z;
+        real iw1 = i00 * w1 + i01 * w2 + i02 * w3;
+        real iw2 = i01 * w1 + i11 * w2 + i12 * w3;
+        real iw3 = i02 * w1 + i12 * w2 + i22 * w3;
         V3 dw = om2 - om1;
         V3 b = v3(i00 * dw.x + i01 * dw.y + i02 * dw.z + h * (w2 * iw3 - w3 * iw2),
                   i01 * dw.x + i11 * dw.y + i12 * dw.z + h * (w3 * iw1 - w1 * iw3),
@@ -1143,10 +1143,10 @@ void integrate_velocities(nso_world* w, float h) {
 }
 
 // solver_integration.rs:377 integrate_positions_range
-void integrate_positions(nso_world* w, float h, float inv_dt) {
-  float maxl = w->def.max_linear_speed;
-  float maxa = kMaxRotation * inv_dt;
-  float maxl2 = maxl * maxl, maxa2 = maxa * maxa;
+void integrate_positions(nso_world* w, real h, real inv_dt) {
+  real maxl = w->def.max_linear_speed;
+  real maxa = kMaxRotation * inv_dt;
+  real maxl2 = maxl * maxl, maxa2 = maxa * maxa;
   const int n_ = (int)w->awake_states.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
   for (int i_ = 0; i_ < n_; ++i_) {
@@ -1159,12 +1159,12 @@ void integrate_positions(nso_world* w, float h, float inv_dt) {
     wv.y = (st.flags & kLockAngY) ? 0.0f : wv.y;
     wv.z = (st.flags & kLockAngZ) ? 0.0f : wv.z;
     if (dot(v, v) > maxl2) {
-      float ratio = maxl / length(v);
+      real ratio = maxl / length(v);
       v = ratio * v;
       st.flags |= kIsSpeedCapped;
     }
     if (dot(wv, wv) > maxa2 && (st.flags & kAllowFastRotation) == 0) {
-      float ratio = maxa / length(wv);
+      real ratio = maxa / length(wv);
       wv = ratio * wv;
       st.flags |= kIsSpeedCapped;
     }
@@ -1184,7 +1184,7 @@ void warm_start_color(nso_world* w, int ci) {
     const ContactConstraint& c = list_[k_];
     const ManifoldConstraint& cm = c.m;
     V3 li = v3(0, 0, 0), aia = v3(0, 0, 0), aib = v3(0, 0, 0);
-    float tni = 0.0f;
+    real tni = 0.0f;
     V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
     for (int p = 0; p < cm.point_count; ++p) {
       const ConstraintPoint& cp = cm.points[p];
@@ -1214,41 +1214,41 @@ void warm_start_color(nso_world* w, int ci) {
 // contact_solver.rs:796 push_contacts_body
 void push_color(nso_world* w, int ci) {
   const StepContext& ctx = w->ctx;
-  float inv_h = ctx.inv_h;
-  float cs = -w->def.contact_speed;
-  float dbr = ctx.contact_softness.mass_scale * ctx.contact_softness.bias_rate;
-  float dms = ctx.contact_softness.mass_scale, dis = ctx.contact_softness.impulse_scale;
-  float sbr = ctx.static_softness.mass_scale * ctx.static_softness.bias_rate;
-  float sms = ctx.static_softness.mass_scale, sis = ctx.static_softness.impulse_scale;
+  real inv_h = ctx.inv_h;
+  real cs = -w->def.contact_speed;
+  real dbr = ctx.contact_softness.mass_scale * ctx.contact_softness.bias_rate;
+  real dms = ctx.contact_softness.mass_scale, dis = ctx.contact_softness.impulse_scale;
+  real sbr = ctx.static_softness.mass_scale * ctx.static_softness.bias_rate;
+  real sms = ctx.static_softness.mass_scale, sis = ctx.static_softness.impulse_scale;
   auto& list_ = w->constraints[ci];
   const int n_ = (int)list_.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
   for (int k_ = 0; k_ < n_; ++k_) {
     ContactConstraint& c = list_[k_];
     BodyState ba = state_at(w, c.index_a), bb = state_at(w, c.index_b);
-    float br = c.is_static ? sbr : dbr, ms = c.is_static ? sms : dms, is = c.is_static ? sis : dis;
+    real br = c.is_static ? sbr : dbr, ms = c.is_static ? sms : dms, is = c.is_static ? sis : dis;
     V3 dp = bb.dp - ba.dp;
-    float im = c.inv_mass_a + c.inv_mass_b;
+    real im = c.inv_mass_a + c.inv_mass_b;
     ManifoldConstraint& cm = c.m;
     V3 n = cm.normal;
-    float ns = dot(n, dp);
+    real ns = dot(n, dp);
     V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
-    float lnv = dot(n, bb.v - ba.v);
-    float mi = 0.0f;
+    real lnv = dot(n, bb.v - ba.v);
+    real mi = 0.0f;
     for (int p = 0; p < cm.point_count; ++p) {
       ConstraintPoint& cp = cm.points[p];
-      float s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
+      real s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
       bool sep = s > 0.0f;
-      float spec_bias = s * inv_h;
-      float ovl = maxf(br * s, cs);
-      float vb = sep ? spec_bias : ovl;
-      float pms = sep ? 1.0f : ms;
-      float pis = sep ? 0.0f : is;
+      real spec_bias = s * inv_h;
+      real ovl = maxf(br * s, cs);
+      real vb = sep ? spec_bias : ovl;
+      real pms = sep ? 1.0f : ms;
+      real pis = sep ? 0.0f : is;
       V3 ua = cross(cp.r_a, n), ub = cross(cp.r_b, n);
       V3 ga = sym_mv(c.inv_ia, ua), gb = sym_mv(c.inv_ib, ub);
-      float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
-      float neg = cp.normal_mass * (pms * vn + vb) + pis * cp.normal_impulse;
-      float imp = maxf(-neg, -cp.normal_impulse);
+      real vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+      real neg = cp.normal_mass * (pms * vn + vb) + pis * cp.normal_impulse;
+      real imp = maxf(-neg, -cp.normal_impulse);
       cp.normal_impulse = cp.normal_impulse + imp;
       lnv += im * imp;
       mi += imp;
@@ -1265,8 +1265,8 @@ void push_color(nso_world* w, int ci) {
 
 // contact_solver.rs:927 solve_contacts_body (relax)
 void relax_color(nso_world* w, int ci) {
-  float inv_h = w->ctx.inv_h;
-  float eps = kEps;
+  real inv_h = w->ctx.inv_h;
+  real eps = kEps;
   auto& list_ = w->constraints[ci];
   const int n_ = (int)list_.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
@@ -1275,26 +1275,26 @@ void relax_color(nso_world* w, int ci) {
     BodyState ba = state_at(w, c.index_a), bb = state_at(w, c.index_b);
     bool any_rolling = c.rolling_resistance > 0.0f;
     V3 dp = bb.dp - ba.dp;
-    float im = c.inv_mass_a + c.inv_mass_b;
+    real im = c.inv_mass_a + c.inv_mass_b;
     ManifoldConstraint& cm = c.m;
     V3 n = cm.normal;
-    float ns = dot(n, dp);
+    real ns = dot(n, dp);
     V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
     V3 dv = bb.v - ba.v;
-    float lnv = dot(n, dv);
-    float lt1 = dot(cm.tangent1, dv) - cm.tangent_velocity1;
-    float lt2 = dot(cm.tangent2, dv) - cm.tangent_velocity2;
-    float mi = 0.0f, tni = 0.0f, ttl = 0.0f;
+    real lnv = dot(n, dv);
+    real lt1 = dot(cm.tangent1, dv) - cm.tangent_velocity1;
+    real lt2 = dot(cm.tangent2, dv) - cm.tangent_velocity2;
+    real mi = 0.0f, tni = 0.0f, ttl = 0.0f;
     for (int p = 0; p < cm.point_count; ++p) {
       ConstraintPoint& cp = cm.points[p];
-      float s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
-      float vb = maxf(0.0f, s * inv_h);
+      real s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
+      real vb = maxf(0.0f, s * inv_h);
       V3 ua = cross(cp.r_a, n), ub = cross(cp.r_b, n);
       V3 ga = sym_mv(c.inv_ia, ua), gb = sym_mv(c.inv_ib, ub);
-      float vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
-      float neg = cp.normal_mass * (vn + vb);
-      float imp = maxf(-neg, -cp.normal_impulse);
-      float ni = cp.normal_impulse + imp;
+      real vn = lnv + (dot(ub, bb.w) - dot(ua, ba.w));
+      real neg = cp.normal_mass * (vn + vb);
+      real imp = maxf(-neg, -cp.normal_impulse);
+      real ni = cp.normal_impulse + imp;
       cp.normal_impulse = ni;
       cp.total_normal_impulse = cp.total_normal_impulse + ni;
       tni += ni;
@@ -1308,11 +1308,11 @@ void relax_color(nso_world* w, int ci) {
       V3 di = sym_mv(c.rolling_mass, ba.w - bb.w);
       V3 old = cm.rolling_impulse;
       cm.rolling_impulse = old + di;
-      float mx = c.rolling_resistance * tni;
-      float lsq = dot(cm.rolling_impulse, cm.rolling_impulse);
+      real mx = c.rolling_resistance * tni;
+      real lsq = dot(cm.rolling_impulse, cm.rolling_impulse);
       bool mask = lsq > eps + mx * mx;
-      float nrm = mx / (std::sqrt(lsq) + eps);
-      float sc = mask ? nrm : 1.0f;
+      real nrm = mx / (std::sqrt(lsq) + eps);
+      real sc = mask ? nrm : 1.0f;
       V3 scaled = sc * cm.rolling_impulse;
       if (c.rolling_resistance == 0.0f) scaled = v3(0, 0, 0);
       cm.rolling_impulse = scaled;
@@ -1321,10 +1321,10 @@ void relax_color(nso_world* w, int ci) {
       bb.w = bb.w + sym_mv(c.inv_ib, di);
     }
     {
-      float ts = dot(n, bb.w - ba.w);
-      float ml = c.friction * ttl;
-      float old = cm.twist_impulse;
-      float imp = -(cm.twist_mass * ts);
+      real ts = dot(n, bb.w - ba.w);
+      real ml = c.friction * ttl;
+      real old = cm.twist_impulse;
+      real imp = -(cm.twist_mass * ts);
       imp = maxf(-ml - old, minf(imp, ml - old));
       cm.twist_impulse = old + imp;
       ba.w = ba.w - imp * sym_mv(c.inv_ia, n);
@@ -1338,11 +1338,11 @@ void relax_color(nso_world* w, int ci) {
       V2 di = mul_mv2(cm.tangent_mass, vt);
       di = v2(-di.x, -di.y);
       V2 ni = v2(cm.friction_impulse.x + di.x, cm.friction_impulse.y + di.y);
-      float mx = c.friction * tni;
-      float lsq = ni.x * ni.x + ni.y * ni.y;
+      real mx = c.friction * tni;
+      real lsq = ni.x * ni.x + ni.y * ni.y;
       bool mask = lsq > mx * mx;
-      float nrm = mx / (std::sqrt(lsq) + eps);
-      float sc = mask ? nrm : 1.0f;
+      real nrm = mx / (std::sqrt(lsq) + eps);
+      real sc = mask ? nrm : 1.0f;
       ni = v2(sc * ni.x, sc * ni.y);
       di = v2(ni.x - cm.friction_impulse.x, ni.y - cm.friction_impulse.y);
       cm.friction_impulse = ni;
@@ -1361,8 +1361,8 @@ void relax_color(nso_world* w, int ci) {
 
 // contact_solver.rs:1135 apply_restitution_body
 void restitution_color(nso_world* w, int ci) {
-  float inv_h = w->ctx.inv_h;
-  float nrt = -w->def.restitution_threshold;
+  real inv_h = w->ctx.inv_h;
+  real nrt = -w->def.restitution_threshold;
   auto& list_ = w->constraints[ci];
   const int n_ = (int)list_.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
@@ -1374,24 +1374,24 @@ void restitution_color(nso_world* w, int ci) {
     V3 dp = bb.dp - ba.dp;
     ManifoldConstraint& cm = c.m;
     V3 n = cm.normal;
-    float ns = dot(n, dp);
+    real ns = dot(n, dp);
     V3 na = inv_rotate_wide(ba.dq, n), nb = inv_rotate_wide(bb.dq, n);
     for (int p = 0; p < cm.point_count; ++p) {
       ConstraintPoint& cp = cm.points[p];
-      float s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
-      float nm = rmask ? cp.normal_mass : 0.0f;
-      float comp = cp.total_normal_impulse - cp.restitution_impulse;
+      real s = (ns + (dot(nb, cp.r_b) - dot(na, cp.r_a))) + cp.base_separation;
+      real nm = rmask ? cp.normal_mass : 0.0f;
+      real comp = cp.total_normal_impulse - cp.restitution_impulse;
       bool armed = rmask && cp.relative_velocity < nrt && comp > 0.0f;
-      float sb = maxf(0.0f, s * inv_h);
-      float vb = armed ? c.restitution * cp.relative_velocity : sb;
+      real sb = maxf(0.0f, s * inv_h);
+      real vb = armed ? c.restitution * cp.relative_velocity : sb;
       V3 vra = ba.v + cross(ba.w, cp.r_a), vrb = bb.v + cross(bb.w, cp.r_b);
-      float vn = dot(vrb - vra, n);
-      float neg = nm * (vn + vb);
-      float ni = maxf(cp.normal_impulse - neg, 0.0f);
-      float imp = ni - cp.normal_impulse;
-      float app = minf(maxf(-nm * vn, 0.0f), maxf(imp, 0.0f));
-      float allow = c.restitution * (comp + app) - cp.restitution_impulse;
-      float mx = app + maxf(allow, 0.0f);
+      real vn = dot(vrb - vra, n);
+      real neg = nm * (vn + vb);
+      real ni = maxf(cp.normal_impulse - neg, 0.0f);
+      real imp = ni - cp.normal_impulse;
+      real app = minf(maxf(-nm * vn, 0.0f), maxf(imp, 0.0f));
+      real allow = c.restitution * (comp + app) - cp.restitution_impulse;
+      real mx = app + maxf(allow, 0.0f);
       imp = armed ? minf(imp, mx) : imp;
       cp.normal_impulse = cp.normal_impulse + imp;
       cp.restitution_impulse = cp.restitution_impulse + (imp - app);
@@ -1439,7 +1439,7 @@ void warm_start_overflow(nso_world* w) {
     for (int mi = 0; mi < c.manifold_count; ++mi) {
       const ManifoldConstraint& mc = c.m;
       V3 n = mc.normal;
-      float tni = 0.0f;
+      real tni = 0.0f;
       V3 moa = v3(0, 0, 0), mob = v3(0, 0, 0);
       for (int j = 0; j < mc.point_count; ++j) {
         const ConstraintPoint& cp = mc.points[j];
@@ -1469,10 +1469,10 @@ void warm_start_overflow(nso_world* w) {
   }
 }
 void push_overflow(nso_world* w) {
-  float inv_h = w->ctx.inv_h;
-  float cs = w->def.contact_speed;
+  real inv_h = w->ctx.inv_h;
+  real cs = w->def.contact_speed;
   for (OverflowConstraint& c : w->overflow) {
-    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    real mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
     BodyState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
@@ -1486,18 +1486,18 @@ void push_overflow(nso_world* w) {
         ConstraintPoint& cp = mc.points[p];
         V3 ra = cp.r_a, rb = cp.r_b;
         V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
-        float s = dot(ds, n) + cp.base_separation;
-        float vbias, mscale, iscale;
+        real s = dot(ds, n) + cp.base_separation;
+        real vbias, mscale, iscale;
         if (s > 0.0f) { vbias = s * inv_h; mscale = 1.0f; iscale = 0.0f; }
         else {
           vbias = maxf(soft.mass_scale * soft.bias_rate * s, -cs);
           mscale = soft.mass_scale; iscale = soft.impulse_scale;
         }
         V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
-        float vn = dot(vrb - vra, n);
-        float ni0 = cp.normal_impulse;
-        float di = -cp.normal_mass * (mscale * vn + vbias) - iscale * ni0;
-        float ni = maxf(ni0 + di, 0.0f);
+        real vn = dot(vrb - vra, n);
+        real ni0 = cp.normal_impulse;
+        real di = -cp.normal_mass * (mscale * vn + vbias) - iscale * ni0;
+        real ni = maxf(ni0 + di, 0.0f);
         di = ni - ni0;
         cp.normal_impulse = ni;
         V3 P = di * n;
@@ -1512,30 +1512,30 @@ void push_overflow(nso_world* w) {
   }
 }
 void relax_overflow(nso_world* w) {
-  float inv_h = w->ctx.inv_h;
+  real inv_h = w->ctx.inv_h;
   for (OverflowConstraint& c : w->overflow) {
-    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    real mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
     BodyState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
     Q dqa = sa.dq, dqb = sb.dq;
     V3 dp = sb.dp - sa.dp;
-    float fr = c.friction, rr = c.rolling_resistance;
+    real fr = c.friction, rr = c.rolling_resistance;
     for (int mi = 0; mi < c.manifold_count; ++mi) {
       ManifoldConstraint& mc = c.m;
       V3 n = mc.normal;
-      float tni = 0.0f, ttl = 0.0f;
+      real tni = 0.0f, ttl = 0.0f;
       for (int p = 0; p < mc.point_count; ++p) {
         ConstraintPoint& cp = mc.points[p];
         V3 ra = cp.r_a, rb = cp.r_b;
         V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
-        float s = dot(ds, n) + cp.base_separation;
-        float vbias = s > 0.0f ? s * inv_h : 0.0f;
+        real s = dot(ds, n) + cp.base_separation;
+        real vbias = s > 0.0f ? s * inv_h : 0.0f;
         V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
-        float vn = dot(vrb - vra, n);
-        float ni0 = cp.normal_impulse;
-        float di = -cp.normal_mass * (vn + vbias);
-        float ni = maxf(ni0 + di, 0.0f);
+        real vn = dot(vrb - vra, n);
+        real ni0 = cp.normal_impulse;
+        real di = -cp.normal_mass * (vn + vbias);
+        real ni = maxf(ni0 + di, 0.0f);
         di = ni - ni0;
         cp.normal_impulse = ni;
         cp.total_normal_impulse += ni;
@@ -1548,10 +1548,10 @@ void relax_overflow(nso_world* w) {
         wb = wb + mul_mv(iB, cross(rb, P));
       }
       {
-        float ts = dot(n, wb - wa);
-        float mx = fr * ttl;
-        float di = -mc.twist_mass * ts;
-        float old = mc.twist_impulse;
+        real ts = dot(n, wb - wa);
+        real mx = fr * ttl;
+        real di = -mc.twist_mass * ts;
+        real old = mc.twist_impulse;
         mc.twist_impulse = clampf(old + di, -mx, mx);
         di = mc.twist_impulse - old;
         wa = wa - mul_mv(iA, di * n);
@@ -1561,8 +1561,8 @@ void relax_overflow(nso_world* w) {
         V3 di = -mul_mv(c.rolling_mass, wb - wa);
         V3 old = mc.rolling_impulse;
         mc.rolling_impulse = old + di;
-        float mx = rr * tni;
-        float msq = dot(mc.rolling_impulse, mc.rolling_impulse);
+        real mx = rr * tni;
+        real msq = dot(mc.rolling_impulse, mc.rolling_impulse);
         if (msq > mx * mx + kEps) mc.rolling_impulse = (mx / std::sqrt(msq)) * mc.rolling_impulse;
         di = mc.rolling_impulse - old;
         wa = wa - mul_mv(iA, di);
@@ -1576,10 +1576,10 @@ void relax_overflow(nso_world* w) {
         V2 tm = mul_mv2(mc.tangent_mass, vt);
         V2 di = v2(-tm.x, -tm.y);
         V2 ni = v2(mc.friction_impulse.x + di.x, mc.friction_impulse.y + di.y);
-        float mx = fr * tni;
-        float lsq = dot2(ni, ni);
+        real mx = fr * tni;
+        real lsq = dot2(ni, ni);
         if (lsq > mx * mx) {
-          float sc = mx / std::sqrt(lsq);
+          real sc = mx / std::sqrt(lsq);
           ni.x *= sc; ni.y *= sc;
         }
         di = v2(ni.x - mc.friction_impulse.x, ni.y - mc.friction_impulse.y);
@@ -1596,12 +1596,12 @@ void relax_overflow(nso_world* w) {
   }
 }
 void restitution_overflow(nso_world* w) {
-  float thr = w->def.restitution_threshold;
-  float inv_h = w->ctx.inv_h;
+  real thr = w->def.restitution_threshold;
+  real inv_h = w->ctx.inv_h;
   for (OverflowConstraint& c : w->overflow) {
-    float rest = c.restitution;
+    real rest = c.restitution;
     if (rest == 0.0f) continue;
-    float mA = c.inv_mass_a, mB = c.inv_mass_b;
+    real mA = c.inv_mass_a, mB = c.inv_mass_b;
     M3 iA = c.inv_ia, iB = c.inv_ib;
     BodyState sa = state_at(w, c.index_a), sb = state_at(w, c.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
@@ -1613,23 +1613,23 @@ void restitution_overflow(nso_world* w) {
       for (int p = 0; p < mc.point_count; ++p) {
         ConstraintPoint cp = mc.points[p];
         V3 ra = cp.r_a, rb = cp.r_b;
-        float comp = cp.total_normal_impulse - cp.restitution_impulse;
+        real comp = cp.total_normal_impulse - cp.restitution_impulse;
         bool armed = rest > 0.0f && cp.relative_velocity < -thr && comp > 0.0f;
-        float vbias;
+        real vbias;
         if (armed) vbias = rest * cp.relative_velocity;
         else {
           V3 ds = dp + (rotate(dqb, rb) - rotate(dqa, ra));
-          float s = dot(ds, n) + cp.base_separation;
+          real s = dot(ds, n) + cp.base_separation;
           vbias = s > 0.0f ? s * inv_h : 0.0f;
         }
         V3 vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
-        float vn = dot(vrb - vra, n);
-        float imp = -cp.normal_mass * (vn + vbias);
-        float ni = maxf(cp.normal_impulse + imp, 0.0f);
+        real vn = dot(vrb - vra, n);
+        real imp = -cp.normal_mass * (vn + vbias);
+        real ni = maxf(cp.normal_impulse + imp, 0.0f);
         imp = ni - cp.normal_impulse;
-        float app = minf(maxf(-cp.normal_mass * vn, 0.0f), maxf(imp, 0.0f));
+        real app = minf(maxf(-cp.normal_mass * vn, 0.0f), maxf(imp, 0.0f));
         if (armed) {
-          float allow = rest * (comp + app) - cp.restitution_impulse;
+          real allow = rest * (comp + app) - cp.restitution_impulse;
           imp = minf(imp, app + maxf(allow, 0.0f));
         }
         mc.points[p].normal_impulse += imp;
@@ -1698,8 +1698,8 @@ void solve_stages(nso_world* w) {
 
 // solver_integration.rs:587 finalize_body_range (sleep disabled; fast bodies only flagged)
 void finalize(nso_world* w) {
-  float dt = w->ctx.dt, inv_dt = w->ctx.inv_dt;
-  float spec = speculative_distance();
+  real dt = w->ctx.dt, inv_dt = w->ctx.inv_dt;
+  real spec = speculative_distance();
   const int n_ = (int)w->awake_sims.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_threads > 1 && n_ >= kParMin)
   for (int i = 0; i < n_; ++i) {
@@ -1711,9 +1711,9 @@ void finalize(nso_world* w) {
     sim.center = offset_pos(sim.center, st.dp);
     sim.transform.q = normalize_quat(mul_quat(st.dq, sim.transform.q));
     V3 varc = modified_cross(abs3(lom), sim.max_extent);
-    float maxv = length(v) + length(varc);
+    real maxv = length(v) + length(varc);
     V3 rarc = modified_cross(abs3(ldr), sim.max_extent);
-    float maxdp = length(st.dp) + 2.0f * length(rarc);
+    real maxdp = length(st.dp) + 2.0f * length(rarc);
     st.dp = v3(0, 0, 0);
     st.dq = qid();
     sim.transform.p = offset_pos(sim.center, -rotate(sim.transform.q, sim.local_center));
@@ -1725,7 +1725,7 @@ void finalize(nso_world* w) {
     body.flags |= st.flags & kIsSpeedCapped;
     st.flags &= ~kTransient;
     body.sleep_time = 0.0f;
-    float max_motion = maxf(maxdp, maxv * dt);
+    real max_motion = maxf(maxdp, maxv * dt);
     (void)inv_dt;
     if (body.type == 2 && w->def.enable_continuous && max_motion > body.safety_factor * sim.min_extent) {
       sim.flags |= kIsFast;
@@ -1922,12 +1922,12 @@ void nso_step(nso_world* w, float dt, int substeps) {
   c.sub_step_count = substeps < 1 ? 1 : substeps;
   if (dt > 0.0f) {
     c.inv_dt = 1.0f / dt;
-    c.h = dt / (float)c.sub_step_count;
-    c.inv_h = (float)c.sub_step_count * c.inv_dt;
+    c.h = dt / (real)c.sub_step_count;
+    c.inv_h = (real)c.sub_step_count * c.inv_dt;
   } else {
     c.inv_dt = 0.0f; c.h = 0.0f; c.inv_h = 0.0f;
   }
-  float hz = minf(w->def.contact_hertz, 0.125f * c.inv_h);
+  real hz = minf(w->def.contact_hertz, 0.125f * c.inv_h);
   c.contact_softness = make_soft(hz, w->def.contact_damping_ratio, c.h);
   c.static_softness = make_soft(2.0f * hz, 0.5f * w->def.contact_damping_ratio, c.h);
   c.enable_warm_starting = w->def.enable_warm_starting != 0;

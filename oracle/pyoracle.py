@@ -20,10 +20,14 @@ STATIC_BODY = 0
 DYNAMIC_BODY = 2
 
 
+LIB64_PATH = os.path.join(HERE, "libns_oracle64.so")
+
+
 def build(force=False):
-    """Compile libns_oracle.so with g++ (IEEE f32, no contraction)."""
-    if not force and os.path.exists(LIB_PATH):
-        t = os.path.getmtime(LIB_PATH)
+    """Compile libns_oracle.so (IEEE f32, no contraction) and libns_oracle64.so (the same sources
+    in f64) with g++."""
+    if not force and all(os.path.exists(p) for p in (LIB_PATH, LIB64_PATH)):
+        t = min(os.path.getmtime(LIB_PATH), os.path.getmtime(LIB64_PATH))
         if all(os.path.getmtime(os.path.join(HERE, s)) <= t for s in SOURCES):
             return LIB_PATH
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -129,13 +133,27 @@ def use_host_native():
     return "-O3 -march=native -ffp-contract=off, built on this host"
 
 
-def load():
-    global _lib
+_lib64 = None
+
+
+def load(precision="f32"):
+    """The oracle library: "f32" is the parity oracle (the reference's arithmetic), "f64" the
+    same step with every scalar in double (the trajectory-statistics reference)."""
+    global _lib, _lib64
+    if precision == "f64":
+        if _lib64 is None:
+            build()
+            _lib64 = _declare(ctypes.CDLL(LIB64_PATH))
+        return _lib64
     if _lib is not None:
         return _lib
     if _lib_path is None:
         build()
-    lib = ctypes.CDLL(_lib_path or LIB_PATH)
+    _lib = _declare(ctypes.CDLL(_lib_path or LIB_PATH))
+    return _lib
+
+
+def _declare(lib):
     P = ctypes.c_void_p
     lib.nso_default_world_def.argtypes = [ctypes.POINTER(WorldDef)]
     lib.nso_create.argtypes = [ctypes.POINTER(WorldDef)]
@@ -160,7 +178,6 @@ def load():
     lib.nso_counters.argtypes = [P, P]
     lib.nso_collide_pairs.argtypes = [P, P, ctypes.c_int]
     lib.nso_apply_forces.argtypes = [P, P, P]
-    _lib = lib
     return lib
 
 
@@ -178,8 +195,8 @@ class OracleWorld:
     """CPU oracle world with the same scene-building calls as natsel_b200.World."""
 
     def __init__(self, gravity=(0.0, -10.0, 0.0), enable_continuous=True, enable_warm_starting=True,
-                 **overrides):
-        self._lib = load()
+                 precision="f32", **overrides):
+        self._lib = load(precision)
         d = WorldDef()
         self._lib.nso_default_world_def(ctypes.byref(d))
         d.gravity = (ctypes.c_float * 3)(*gravity)

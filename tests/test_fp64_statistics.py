@@ -1,0 +1,111 @@
+"""Long trajectories against an FP64 run of the same scene (the oracle built with every scalar
+in double): the FP32 device step and the FP32 oracle must stay statistically with the FP64
+run, by energy, penetration and resting-contact statistics, since chaos rules out pointwise
+agreement over hundreds of steps of a pile. Before the first contacts the runs still agree
+pointwise, and there the bar is tight.
+
+Tolerances (stated per statistic in ``assert_close``), set from the FP32 oracle against the
+FP64 oracle on the same scenes: energy per unit mass of the bodies on the ground 1 %, mean
+speed 0.05 m/s, median height 1 cm + 1 %, bodies that rolled off the ground's edge 5 (or
+0.5 %), touching contacts 3 %, deepest penetration 5 mm + 25 %, 99th-percentile penetration
+1 mm; over the quasi-static pyramid they are tight everywhere."""
+import numpy as np
+import pytest
+
+from natsel_b200 import scenes
+from oracle import pyoracle
+
+from _stats import mean_stats, trajectory_stats
+
+DT = 1.0 / 60.0
+
+
+def _oracle(name, precision, **kw):
+    w = pyoracle.OracleWorld(precision=precision, **scenes.WORLD_SETTINGS[name])
+    scenes.BUILDERS[name](w, **kw)
+    return w
+
+
+def _gpu(name, **kw):
+    from natsel_b200.world import World, default_world_def
+    s = scenes.WORLD_SETTINGS[name]
+    w = World(default_world_def(gravity=s["gravity"], enable_continuous=int(s["enable_continuous"])))
+    scenes.BUILDERS[name](w, **kw)
+    return w
+
+
+def assert_close(a, b, n_bodies, settled=True):
+    """a: the FP32 run's statistics, b: the FP64 run's."""
+    assert abs(a["energy"] - b["energy"]) <= 0.01 * abs(b["energy"]), (a, b)
+    assert abs(a["median_height"] - b["median_height"]) <= 0.01 + 0.01 * b["median_height"], (a, b)
+    assert abs(a["off_ground"] - b["off_ground"]) <= max(5, 0.005 * n_bodies), (a, b)
+    assert abs(a["touching"] - b["touching"]) <= 0.03 * max(b["touching"], 1), (a, b)
+    assert abs(a["p99_penetration"] - b["p99_penetration"]) <= 1e-3, (a, b)
+    if settled:
+        assert abs(a["speed"] - b["speed"]) <= 0.05, (a, b)
+        # the single deepest of ~10^4 points is an extreme value: a quarter of it plus 5 mm
+        assert abs(a["max_penetration"] - b["max_penetration"]) <= 0.005 + 0.25 * b["max_penetration"], (a, b)
+
+
+def assert_pointwise(a, b):
+    """Before chaos sets in: energy to 1e-5, touching contacts to 0.1 % (a pair grazing at the
+    speculative distance may start touching one step apart), heights to 0.1 mm."""
+    assert abs(a["energy"] - b["energy"]) <= 1e-5 * abs(b["energy"]), (a, b)
+    assert abs(a["touching"] - b["touching"]) <= 1e-3 * b["touching"], (a, b)
+    assert abs(a["median_height"] - b["median_height"]) <= 1e-4, (a, b)
+    assert abs(a["max_penetration"] - b["max_penetration"]) <= 1e-4, (a, b)
+
+
+def _pile_run(fp32, fp64, n_bodies, steps=600, early=40, tail=100):
+    rows32, rows64 = [], []
+    for s in range(1, steps + 1):
+        fp32.step(DT, 4)
+        fp64.step(DT, 4)
+        if s == early:
+            assert_pointwise(trajectory_stats(fp32), trajectory_stats(fp64))
+        if s > steps - tail and s % 10 == 0:
+            rows32.append(trajectory_stats(fp32))
+            rows64.append(trajectory_stats(fp64))
+    assert_close(mean_stats(rows32), mean_stats(rows64), n_bodies)
+
+
+def _pyramid_run(fp32, fp64, steps=1000):
+    for s in range(1, steps + 1):
+        fp32.step(DT, 4)
+        fp64.step(DT, 4)
+        if s % 100 == 0:
+            a, b = trajectory_stats(fp32), trajectory_stats(fp64)
+            assert_pointwise(a, b)
+            assert a["max_penetration"] < 0.005
+
+
+def test_oracle_fp32_pile_stays_with_fp64():
+    """The FP32 oracle against the FP64 oracle: a 2 000-body pile of the 10 000-body pile's shape
+    mix dropped for 600 steps (4 host threads; every thread count gives the same bits)."""
+    pyoracle.load("f32").nso_set_threads(4)
+    pyoracle.load("f64").nso_set_threads(4)
+    try:
+        _pile_run(_oracle("large_pile", "f32", n=2000, seed=7), _oracle("large_pile", "f64", n=2000, seed=7), 2000)
+    finally:
+        pyoracle.load("f32").nso_set_threads(1)
+        pyoracle.load("f64").nso_set_threads(1)
+
+
+@pytest.mark.gpu
+def test_box_pyramid_1000_steps_against_fp64():
+    """Config 1 (210 cubes, 1000 steps): the device's FP32 run and the FP64 run agree on energy,
+    contacts, heights and penetration every 100 steps."""
+    _pyramid_run(_gpu("box_pyramid"), _oracle("box_pyramid", "f64"))
+
+
+@pytest.mark.gpu
+def test_large_pile_600_steps_against_fp64():
+    """Config 2 at full size (10 000 bodies, 600 steps): the device's FP32 run against the FP64
+    run, pointwise at step 40 and by the settled pile's statistics over the last 100 steps."""
+    import os
+    threads = max(1, min(16, os.cpu_count() or 1))
+    pyoracle.load("f64").nso_set_threads(threads)
+    try:
+        _pile_run(_gpu("large_pile"), _oracle("large_pile", "f64"), 10000)
+    finally:
+        pyoracle.load("f64").nso_set_threads(1)
