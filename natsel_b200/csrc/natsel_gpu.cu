@@ -61,6 +61,7 @@ struct ns_world {
   std::vector<DState> states;
   std::vector<HostShape> shapes;
   std::vector<AABB> fat;
+  std::vector<AABB> saabb;  // each shape's bounds at creation (shape.aabb; continuous pass input)
   std::vector<DJoint> joints;
   std::vector<uint32_t> body_mask;
   std::vector<std::vector<int>> joint_partners;  // per body: bodies a joint keeps from colliding
@@ -334,6 +335,7 @@ int create_shape(ns_world* w, int bi, const ns_shape_def* def, HostShape hs) {
   Pos p = {sim.px, sim.py, sim.pz};
   AABB a = offset_aabb(aabb_inflate(shape_local_aabb(hs, sim.q), spec), p);
   w->fat.push_back(aabb_inflate(a, s.is_static ? spec : s.aabb_margin));
+  w->saabb.push_back(a);
   s.hull = s.type == kHull ? sid : -1;
   w->shapes.push_back(hs);
   b.shapes.push_back(sid);
@@ -376,7 +378,7 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_solve<false, true>,
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter, (const void*)k_prepare_slots,
                            (const void*)k_warm_slots,
-                           (const void*)k_finalize, (const void*)k_state_pass,
+                           (const void*)k_finalize, (const void*)k_continuous, (const void*)k_state_pass,
                            (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
                            (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
   for (const void* k : kernels) {
@@ -458,6 +460,20 @@ int upload_world(ns_world* w) {
   }
   d.n_large = (int)large.size();
   d.n_small = nsh - d.n_large;
+  // static shapes per sub-world, for the continuous pass
+  std::vector<int> static_list, static_off(n_worlds + 1, 0);
+  for (int i = 0; i < nsh; ++i)
+    if (dshapes[i].is_static) static_off[dshapes[i].world + 1]++;
+  for (int k = 0; k < n_worlds; ++k) static_off[k + 1] += static_off[k];
+  {
+    std::vector<int> cursor(static_off.begin(), static_off.end() - 1);
+    static_list.resize(static_off[n_worlds]);
+    for (int i = 0; i < nsh; ++i)
+      if (dshapes[i].is_static) static_list[cursor[dshapes[i].world]++] = i;
+  }
+  // the sweep of a body starts at its pose at upload (body_api.rs:221, :533 center0/rotation0)
+  for (DSim& s : w->asims) { s.cx0 = s.cx; s.cy0 = s.cy; s.cz0 = s.cz; s.q0 = s.q; }
+  for (DSim& s : w->ssims) { s.cx0 = s.cx; s.cy0 = s.cy; s.cz0 = s.cz; s.q0 = s.q; }
   std::vector<int> large_off(n_worlds + 1, 0);
   for (int i : large) large_off[dshapes[i].world + 1]++;
   for (int k = 0; k < n_worlds; ++k) large_off[k + 1] += large_off[k];
@@ -526,6 +542,8 @@ int upload_world(ns_world* w) {
   ALLOC(pool_top, int, n_worlds); ALLOC(pool_next, int, n_worlds); ALLOC(ovf_count, int, n_worlds);
   ALLOC(large_off, int, n_worlds + 1);
   ALLOC(large_list, int, large.size());
+  ALLOC(fast_list, int, std::max(na, 1)); ALLOC(static_off, int, n_worlds + 1);
+  ALLOC(static_list, int, std::max<size_t>(static_list.size(), 1)); ALLOC(saabb, AABB, nsh);
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
   ALLOC(block_color, int, (size_t)d.n_color_blocks * 24);
@@ -557,6 +575,9 @@ int upload_world(ns_world* w) {
   if ((st = upload(w, d.world_cbase, world_cbase))) return st;
   if ((st = upload(w, d.world_shape, world_shape))) return st;
   if ((st = upload(w, d.large_off, large_off))) return st;
+  if ((st = upload(w, d.static_off, static_off))) return st;
+  if ((st = upload(w, d.static_list, static_list))) return st;
+  if ((st = upload(w, d.saabb, w->saabb))) return st;
   {
     std::vector<int> zeros(n_worlds, 0);
     if ((st = upload(w, d.pool_top, zeros))) return st;
@@ -815,7 +836,12 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, ev_flags));
   // finalize (solver_integration.rs:435)
+  if (w->def.enable_continuous) NS_CUDA(w, cudaMemsetAsync(&d.ctl->fast_count, 0, sizeof(int), s));
   k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p); ++nk;
+  if (w->def.enable_continuous) {
+    // continuous.rs:337 for the fast bodies finalize queued (solver_integration.rs:540-566)
+    k_continuous<<<blocks(d.n_awake, 64), 64, 0, s>>>(d, p); ++nk;
+  }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, ev_flags));
   NS_CUDA(w, cudaGetLastError());
   w->step_kernels = w->pair_kernels + nk;

@@ -100,6 +100,11 @@ struct DW {
   // the 400-byte contact records.
   uint8_t* slot_state;
   int* long_segment;  // candidate segments of more than kShortSegment keys (this pair update)
+  // Continuous collision: the fast bodies finalize queues (awake indices, this step), the
+  // static shapes of each sub-world (static_list[static_off[w] .. static_off[w + 1])) and each
+  // shape's last bounds (shape.aabb in the reference: the speculative-inflated box finalize
+  // computes, or the swept end box of the continuous pass).
+  int* fast_list; int* static_list; int* static_off; AABB* saabb;
 };
 
 struct JointRanges { int off[25]; };

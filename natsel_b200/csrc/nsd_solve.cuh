@@ -13,6 +13,7 @@
 // all blocks alike.
 #pragma once
 #include "nsd_kernels.cuh"
+#include "nsd_toi.cuh"
 
 namespace nsd {
 
@@ -1242,9 +1243,23 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
   }
 }
 
-// solver_integration.rs:587 finalize_body_range (sleep disabled: bodies never sleep; a fast
-// body is flagged and keeps its previous broadphase bounds, as the reference leaves them
-// to the continuous pass)
+// shape_runtime.rs:370 compute_shape_aabb of a shape under a transform
+__device__ AABB shape_box(const DW& w, const DShape& sh, Xf t) {
+  if (sh.type == kHull) return aabb_transform(t, w.hulls[sh.hull].bounds);  // hull_queries.rs:16
+  if (sh.type == kSphere) {                                                   // sphere.rs:27
+    V3 c = xf_point(t, sh.sphere.center);
+    float r = sh.sphere.radius;
+    V3 e = v3(r, r, r);
+    return aabb(c - e, c + e);
+  }
+  V3 c1 = xf_point(t, sh.capsule.c1), c2 = xf_point(t, sh.capsule.c2);          // capsule.rs:66
+  float r = sh.capsule.radius;
+  V3 e = v3(r, r, r);
+  return aabb(min3(c1, c2) - e, max3(c1, c2) + e);
+}
+
+// solver_integration.rs:587 finalize_body_range (sleep disabled: bodies never sleep). A fast
+// body is queued for the continuous pass, which sets its bounds (solver_integration.rs:540-566).
 __global__ void k_finalize(DW w, StepParams p) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w.n_awake) return;
@@ -1271,19 +1286,24 @@ __global__ void k_finalize(DW w, StepParams p) {
   sim.flags &= ~(kIsFast | kTransient);
   st.flags &= ~kTransient;
   float max_motion = maxf(maxdp, maxv * dt);
-  if (p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
-    sim.flags |= kIsFast;
-    add_converged(&w.ctl->fast_flags);
-  }
-  M3 R = matrix_from_quat(sim.q);
-  sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
   // solver_integration.rs:626-627 asserts finite velocities here; the device raises
   // NS_ERR_NONFINITE instead (first error wins) and keeps the body's old fat AABB, so a
-  // non-finite pose never reaches the broadphase grid
+  // non-finite pose never reaches the broadphase grid or the continuous pass
   bool finite = isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(wv.x) && isfinite(wv.y) &&
                 isfinite(wv.z) && isfinite(sim.cx) && isfinite(sim.cy) && isfinite(sim.cz) &&
                 isfinite(sim.q.v.x) && isfinite(sim.q.v.y) && isfinite(sim.q.v.z) && isfinite(sim.q.s);
   if (!finite) atomicCAS(&w.ctl->error, 0, kErrNonFinite);
+  if (finite && p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
+    sim.flags |= kIsFast;
+    add_converged(&w.ctl->fast_flags);
+    // the continuous pass (k_continuous) sweeps it from (cx0, q0) and updates its bounds
+    w.fast_list[atomicAdd(&w.ctl->fast_count, 1)] = i;
+  } else {
+    sim.cx0 = sim.cx; sim.cy0 = sim.cy; sim.cz0 = sim.cz;
+    sim.q0 = sim.q;
+  }
+  M3 R = matrix_from_quat(sim.q);
+  sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
   if (finite && (sim.flags & kIsFast) == 0) {
     WXf xf_;
     xf_.p = tp; xf_.q = sim.q;
@@ -1292,22 +1312,8 @@ __global__ void k_finalize(DW w, StepParams p) {
       int sid = w.body_shapes[k];
       const DShape& sh = w.shapes[sid];
       // shape_runtime.rs:405-427 compute_fat_shape_aabb
-      Xf lt = xf(v3(0, 0, 0), xf_.q);
-      AABB a;
-      if (sh.type == kHull) {
-        a = aabb_transform(lt, w.hulls[sh.hull].bounds);
-      } else if (sh.type == kSphere) {
-        V3 c = xf_point(lt, sh.sphere.center);
-        float r = sh.sphere.radius;
-        V3 e = v3(r, r, r);
-        a = aabb(c - e, c + e);
-      } else {
-        V3 c1 = xf_point(lt, sh.capsule.c1), c2 = xf_point(lt, sh.capsule.c2);
-        float r = sh.capsule.radius;
-        V3 e = v3(r, r, r);
-        a = aabb(min3(c1, c2) - e, max3(c1, c2) + e);
-      }
-      a = offset_aabb(aabb_inflate(a, spec), xf_.p);
+      AABB a = offset_aabb(aabb_inflate(shape_box(w, sh, xf(v3(0, 0, 0), xf_.q)), spec), xf_.p);
+      w.saabb[sid] = a;
       if (!aabb_contains(w.fat[sid], a)) {
         w.fat[sid] = aabb_inflate(a, sh.aabb_margin);
         w.moved[sid] = 1;
@@ -1317,6 +1323,155 @@ __global__ void k_finalize(DW w, StepParams p) {
   }
   w.states[i] = st;
   w.asims[i] = sim;
+}
+
+// The proxy of a shape (shape_runtime.rs:643 make_shape_proxy) and its centroid
+// (shape_runtime.rs:434 get_shape_centroid), both in the body's frame.
+__device__ void shape_proxy(const DW& w, const DShape& sh, Proxy* p, V3* centroid) {
+  if (sh.type == kHull) {
+    const Hull& h = w.hulls[sh.hull];
+    for (int k = 0; k < kHullVertexCount; ++k) p->pts[k] = h.points[k];
+    p->count = kHullVertexCount;
+    p->radius = 0.0f;
+    *centroid = h.center;
+  } else if (sh.type == kSphere) {
+    p->pts[0] = sh.sphere.center;
+    p->count = 1;
+    p->radius = sh.sphere.radius;
+    *centroid = sh.sphere.center;
+  } else {
+    p->pts[0] = sh.capsule.c1;
+    p->pts[1] = sh.capsule.c2;
+    p->count = 2;
+    p->radius = sh.capsule.radius;
+    *centroid = lerp(sh.capsule.c1, sh.capsule.c2, 0.5f);
+  }
+}
+
+// world_runtime.rs:929 make_relative_sweep: from (center0, rotation0) to the current pose
+__device__ __forceinline__ Sweep sweep_of(const DSim& s, Pos base) {
+  Sweep sw;
+  sw.c1 = sub_pos(Pos{s.cx0, s.cy0, s.cz0}, base);
+  sw.c2 = sub_pos(Pos{s.cx, s.cy, s.cz}, base);
+  sw.q1 = s.q0;
+  sw.q2 = s.q;
+  sw.local_center = s.local_center;
+  return sw;
+}
+
+// continuous.rs:337 solve_continuous for one fast (non-bullet) body: each of its shapes that
+// is fast on its own (continuous.rs:124) is swept against the static shapes of its sub-world
+// whose fat bounds overlap the shape's swept box; the earliest hit moves the body back along
+// its sweep. Only the earliest fraction matters, so the order the static shapes are visited in
+// does not change the result, and fast bodies are independent of one another (they only read
+// static bodies), so one thread per fast body gives the reference's serial pass.
+__device__ void continuous_body(const DW& w, const StepParams& p, int i) {
+  DSim sim = w.asims[i];
+  DState st = w.states[i];
+  const Pos base = {sim.cx0, sim.cy0, sim.cz0};
+  const Sweep sweep = sweep_of(sim, base);
+  const Xf xf1 = xf(sweep.c1 - rotate(sweep.q1, sweep.local_center), sweep.q1);
+  const Xf xf2 = xf(sweep.c2 - rotate(sweep.q2, sweep.local_center), sweep.q2);
+  const float chord = 2.0f * length(inv_mul_quat(sweep.q1, sweep.q2).v);
+  float fraction = 1.0f;
+  for (int k = sim.shape_begin; k < sim.shape_end; ++k) {
+    const int fid = w.body_shapes[k];
+    const DShape& fs = w.shapes[fid];
+    const int s0 = w.static_off[fs.world], s1 = w.static_off[fs.world + 1];
+    Proxy fp;
+    V3 lc;
+    shape_proxy(w, fs, &fp, &lc);
+    AABB box1 = w.saabb[fid];
+    AABB box2 = offset_aabb(shape_box(w, fs, xf2), base);
+    w.saabb[fid] = box2;
+    // continuous.rs:124 is_shape_fast
+    float radius, min_extent;
+    if (fs.type == kSphere) {
+      radius = fs.sphere.radius;
+      min_extent = fs.sphere.radius;
+    } else if (fs.type == kCapsule) {
+      radius = 0.5f * distance(fs.capsule.c1, fs.capsule.c2) + fs.capsule.radius;
+      min_extent = fs.capsule.radius;
+    } else {
+      const Hull& h = w.hulls[fs.hull];
+      V3 far = v3((lc.x - h.bounds.lo.x) > (h.bounds.hi.x - lc.x) ? h.bounds.lo.x : h.bounds.hi.x,
+                  (lc.y - h.bounds.lo.y) > (h.bounds.hi.y - lc.y) ? h.bounds.lo.y : h.bounds.hi.y,
+                  (lc.z - h.bounds.lo.z) > (h.bounds.hi.z - lc.z) ? h.bounds.lo.z : h.bounds.hi.z);
+      radius = distance(far, lc);
+      min_extent = h.inner_radius;
+    }
+    float motion = distance(xf_point(xf1, lc), xf_point(xf2, lc)) + chord * radius;
+    if (!(motion > sim.safety_factor * min_extent)) continue;
+    AABB swept = aabb(min3(box1.lo, box2.lo), max3(box1.hi, box2.hi));
+    for (int t = s0; t < s1; ++t) {
+      const int sid = w.static_list[t];
+      if (!aabb_overlaps(w.fat[sid], swept) || !should_create_pair(w, sid, fid)) continue;
+      const DShape& ss = w.shapes[sid];
+      Proxy sp;
+      V3 unused;
+      shape_proxy(w, ss, &sp, &unused);
+      ToiResult r = time_of_impact(sp, fp, sweep_of(sim_of(w, ss.enc), base), sweep, fraction);
+      if (0.0f < r.fraction && r.fraction < fraction) fraction = r.fraction;
+    }
+  }
+  const float spec = speculative_distance();
+  if (fraction < 1.0f) {
+    // move the body back to the time of impact (continuous.rs:452-470)
+    Q q = nlerp(sweep.q1, sweep.q2, fraction);
+    V3 c = lerp(sweep.c1, sweep.c2, fraction);
+    V3 origin = c - rotate(q, sweep.local_center);
+    Pos tp = offset_pos(base, origin);
+    Pos center = offset_pos(base, c);
+    sim.px = tp.x; sim.py = tp.y; sim.pz = tp.z;
+    sim.q = q;
+    sim.cx = center.x; sim.cy = center.y; sim.cz = center.z;
+    sim.cx0 = center.x; sim.cy0 = center.y; sim.cz0 = center.z;
+    sim.q0 = q;
+    sim.flags |= kHadToi;
+    // the gravity of the time lost (other forces are ignored, as in the reference)
+    float time_loss = (1.0f - fraction) * p.dt;
+    V3 dv = (-time_loss * sim.gravity_scale) * p.gravity;
+    dv.x = (st.flags & kLockLinX) ? 0.0f : dv.x;
+    dv.y = (st.flags & kLockLinY) ? 0.0f : dv.y;
+    dv.z = (st.flags & kLockLinZ) ? 0.0f : dv.z;
+    st.v = st.v + dv;
+    for (int k = sim.shape_begin; k < sim.shape_end; ++k) {
+      const int sid = w.body_shapes[k];
+      const DShape& sh = w.shapes[sid];
+      AABB a = offset_aabb(aabb_inflate(shape_box(w, sh, xf(v3(0, 0, 0), q)), spec), tp);
+      w.saabb[sid] = a;
+      if (!aabb_contains(w.fat[sid], a)) {
+        w.fat[sid] = aabb_inflate(a, sh.aabb_margin);
+        w.moved[sid] = 1;
+        add_converged(&w.ctl->moved_count);
+      }
+    }
+  } else {
+    sim.cx0 = sim.cx; sim.cy0 = sim.cy; sim.cz0 = sim.cz;
+    sim.q0 = sim.q;
+    // the swept end box stands as the shape's bounds (continuous.rs:573-590)
+    for (int k = sim.shape_begin; k < sim.shape_end; ++k) {
+      const int sid = w.body_shapes[k];
+      AABB a = w.saabb[sid];
+      if (!aabb_contains(w.fat[sid], a)) {
+        w.fat[sid] = aabb_inflate(a, w.shapes[sid].aabb_margin);
+        w.moved[sid] = 1;
+        add_converged(&w.ctl->moved_count);
+      }
+    }
+  }
+  // solver_integration.rs:556-564: the world inverse inertia at the final rotation
+  M3 R = matrix_from_quat(sim.q);
+  sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
+  w.states[i] = st;
+  w.asims[i] = sim;
+}
+
+// The continuous pass: one thread per fast body queued by k_finalize this step.
+__global__ void __launch_bounds__(64) k_continuous(DW w, StepParams p) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w.ctl->fast_count) return;
+  continuous_body(w, p, w.fast_list[t]);
 }
 
 }  // namespace nsd

@@ -44,6 +44,8 @@ struct alignas(16) DSim {
   float safety_factor;
   int body_id;
   int shape_begin, shape_end;  // range in the body->shape index table
+  double cx0, cy0, cz0;        // centre and rotation at the start of the sweep (center0,
+  Q q0;                        // rotation0): the last pose finalize accepted without a sweep test
 };
 
 struct alignas(16) DState {
@@ -245,6 +247,7 @@ struct Control {
   int live_contacts;
   int collide_count[6];   // contacts per pair kind queued for a full manifold update
   int long_segments;      // candidate segments handed to the block sort this pair update
+  int fast_count;         // fast bodies queued by finalize for the continuous pass (this step)
 };
 
 }  // namespace nsd

@@ -98,15 +98,18 @@ def _random_quats(rng, n):
 GROUND_HALF_HEIGHT = 5.0
 
 
-def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0, spread=20.0, drop=(1.0, 61.0)):
+def large_pile(world, n=10000, seed=2, ground_half=50.0, restitution=0.0, spread=20.0, drop=(1.0, 61.0),
+               ground_half_height=None):
     """10 000 dynamic bodies (60% boxes, 25% spheres, 15% capsules) dropped from a 40x60x40 m volume.
     ``restitution`` > 0 gives every shape that coefficient (exercises the restitution stage).
-    The ground box is 100 x 10 x 100 m with its top at y = 0: bodies dropped from 61 m arrive
-    at up to 35 m/s (0.58 m per step) and, with continuous collision outside this path, a
-    1 m slab would let the smallest of them pass through in one step."""
+    The ground box is 100 x 10 x 100 m with its top at y = 0 (``ground_half_height`` sets its
+    half thickness): bodies dropped from 61 m arrive at up to 35 m/s (0.58 m per step), so
+    without the continuous pass a 1 m slab would let the smallest of them through in one step;
+    with it (``enable_continuous``), the slab holds them."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    g = world.create_body(type=STATIC, position=(0.0, -GROUND_HALF_HEIGHT, 0.0))
-    world.create_box(g, ground_half, GROUND_HALF_HEIGHT, ground_half, friction=0.6)
+    hy = GROUND_HALF_HEIGHT if ground_half_height is None else float(ground_half_height)
+    g = world.create_body(type=STATIC, position=(0.0, -hy, 0.0))
+    world.create_box(g, ground_half, hy, ground_half, friction=0.6)
     n_box = int(round(0.6 * n))
     n_sph = int(round(0.25 * n))
     kinds = np.array([0] * n_box + [1] * n_sph + [2] * (n - n_box - n_sph))

@@ -112,6 +112,13 @@ typedef struct {
 } nso_pair_result;
 void nso_collide_pairs(nso_pair_job* jobs, nso_pair_result* results, int count);
 
+/* One time-of-impact query (collision/time_of_impact.rs:391). Proxies: up to 8 points (xyz) and
+ * a radius. Sweeps: local_center xyz, c1 xyz, c2 xyz, q1 xyzs, q2 xyzs (17 floats).
+ * out[13]: state (0 unknown, 1 failed, 2 overlapped, 3 hit, 4 separated), fraction, distance,
+ * point xyz, normal xyz, distance / push-back / root iterations. */
+void nso_time_of_impact(const float* points_a, int count_a, float radius_a, const float* points_b, int count_b,
+                        float radius_b, const float* sweep_a, const float* sweep_b, float max_fraction, float* out);
+
 #ifdef __cplusplus
 }
 #endif

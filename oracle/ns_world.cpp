@@ -14,6 +14,7 @@
 
 #include "ns_collide.hpp"
 #include "ns_joint.hpp"
+#include "ns_toi.hpp"
 #include "ns_oracle.h"
 
 namespace nso {
@@ -290,10 +291,9 @@ void sync_body_flags(nso_world* w, int bi) {
   if (b.set_index == 2) w->awake_states[b.local_index].flags = b.flags & ~kTransient;
 }
 
-// shape_runtime.rs:405 compute_shape_aabb in a rotation-only frame
-AABB shape_local_aabb(const Shape& s, Q q) {
-  Xf t = xf(v3(0, 0, 0), q);
-  if (s.type == kHull) return aabb_transform(t, s.hull.bounds);
+// shape_runtime.rs:370 compute_shape_aabb
+AABB shape_aabb_xf(const Shape& s, Xf t) {
+  if (s.type == kHull) return aabb_transform(t, s.hull.bounds);  // hull_queries.rs:16
   if (s.type == kSphere) {  // sphere.rs:27
     V3 c = xf_point(t, s.sphere.center);
     real r = s.sphere.radius;
@@ -305,6 +305,8 @@ AABB shape_local_aabb(const Shape& s, Q q) {
   V3 e = v3(r, r, r);
   return aabb(min3(c1, c2) - e, max3(c1, c2) + e);
 }
+// shape_runtime.rs:405 compute_shape_aabb in a rotation-only frame
+AABB shape_local_aabb(const Shape& s, Q q) { return shape_aabb_xf(s, xf(v3(0, 0, 0), q)); }
 // shape_runtime.rs:420 compute_fat_shape_aabb
 AABB fat_shape_aabb(const Shape& s, WXf t, real extra) {
   return offset_aabb(aabb_inflate(shape_local_aabb(s, t.q), extra), t.p);
@@ -1696,7 +1698,169 @@ void solve_stages(nso_world* w) {
   for (int ci = 0; ci < kOverflowIndex; ++ci) store_color(w, ci);
 }
 
-// solver_integration.rs:587 finalize_body_range (sleep disabled; fast bodies only flagged)
+// ---------------------------------------------------------------------------------------------
+// Continuous collision of fast (non-bullet) bodies against static shapes: continuous.rs:337
+// solve_continuous, run in body order after finalize (solver_integration.rs:540-566).
+
+// shape_runtime.rs:434 get_shape_centroid
+V3 shape_centroid(const Shape& s) {
+  if (s.type == kHull) return s.hull.center;
+  if (s.type == kSphere) return s.sphere.center;
+  return lerp(s.capsule.c1, s.capsule.c2, 0.5f);
+}
+
+// shape_runtime.rs:643 make_shape_proxy
+Proxy shape_proxy(const Shape& s) {
+  Proxy p;
+  if (s.type == kHull) {
+    p.count = s.hull.vertex_count;
+    for (int i = 0; i < p.count; ++i) p.pts[i] = s.hull.points[i];
+    p.radius = 0.0f;
+  } else if (s.type == kSphere) {
+    p.count = 1;
+    p.pts[0] = s.sphere.center;
+    p.radius = s.sphere.radius;
+  } else {
+    p.count = 2;
+    p.pts[0] = s.capsule.c1;
+    p.pts[1] = s.capsule.c2;
+    p.radius = s.capsule.radius;
+  }
+  return p;
+}
+
+// world_runtime.rs:929 make_relative_sweep
+Sweep relative_sweep(const BodySim& b, Pos base) {
+  Sweep s;
+  s.c1 = sub_pos(b.center0, base);
+  s.c2 = sub_pos(b.center, base);
+  s.q1 = b.rotation0;
+  s.q2 = b.transform.q;
+  s.local_center = b.local_center;
+  return s;
+}
+
+// continuous.rs:124 is_shape_fast (convex shapes)
+bool is_shape_fast(const Shape& s, V3 centroid1, V3 centroid2, real rotation_chord, real safety_factor) {
+  real radius;
+  V3 lc = shape_centroid(s);
+  if (s.type == kSphere) {
+    radius = s.sphere.radius;
+  } else if (s.type == kCapsule) {
+    radius = 0.5f * distance(s.capsule.c1, s.capsule.c2) + s.capsule.radius;
+  } else {
+    const AABB& b = s.hull.bounds;  // internal_math.rs:426 farthest_point_on_aabb
+    V3 f = v3((lc.x - b.lo.x) > (b.hi.x - lc.x) ? b.lo.x : b.hi.x, (lc.y - b.lo.y) > (b.hi.y - lc.y) ? b.lo.y : b.hi.y,
+              (lc.z - b.lo.z) > (b.hi.z - lc.z) ? b.lo.z : b.hi.z);
+    radius = distance(f, lc);
+  }
+  // shape_runtime.rs:547 compute_shape_min_extent
+  real min_extent = s.type == kCapsule ? s.capsule.radius : s.type == kSphere ? s.sphere.radius : s.hull.inner_radius;
+  real max_motion = distance(centroid1, centroid2) + rotation_chord * radius;
+  return max_motion > safety_factor * min_extent;
+}
+
+// contact_creation.rs:113 should_bodies_collide (joints without collide_connected)
+bool bodies_collide(nso_world* w, int ia, int ib) {
+  const Body& ba = w->bodies[ia];
+  const Body& bb = w->bodies[ib];
+  if (ba.type != 2 && bb.type != 2) return false;
+  const Body& scan = ba.joint_count < bb.joint_count ? ba : bb;
+  int other = ba.joint_count < bb.joint_count ? bb.id : ba.id;
+  if (scan.id < (int)w->body_joints.size())
+    for (int jid : w->body_joints[scan.id]) {
+      const Joint& j = w->joints[jid];
+      int o = j.body_a == scan.id ? j.body_b : j.body_a;
+      if (!j.collide_connected && o == other) return false;
+    }
+  return true;
+}
+
+// shape_runtime.rs:284 should_shapes_collide
+bool shapes_collide(const Shape& a, const Shape& b) {
+  if (a.group == b.group && a.group != 0) return a.group > 0;
+  return (a.mask & b.category) != 0 && (a.category & b.mask) != 0;
+}
+
+void solve_continuous(nso_world* w, int i) {
+  BodySim& sim = w->awake_sims[i];
+  BodyState& st = w->awake_states[i];
+  Body& body = w->bodies[sim.body_id];
+  Pos base = sim.center0;
+  Sweep sweep = relative_sweep(sim, base);
+  Xf xf1 = xf(sweep.c1 - rotate(sweep.q1, sweep.local_center), sweep.q1);
+  Xf xf2 = xf(sweep.c2 - rotate(sweep.q2, sweep.local_center), sweep.q2);
+  real fraction = 1.0f;
+  real rotation_chord = 2.0f * length(inv_mul_quat(sweep.q1, sweep.q2).v);
+  for (int fid = body.head_shape; fid != -1; fid = w->shapes[fid].next_shape) {
+    Shape& fs = w->shapes[fid];
+    V3 lc = shape_centroid(fs);
+    V3 centroid1 = xf_point(xf1, lc), centroid2 = xf_point(xf2, lc);
+    AABB box1 = fs.aabb;
+    AABB box2 = offset_aabb(shape_aabb_xf(fs, xf2), base);
+    fs.aabb = box2;
+    if (!is_shape_fast(fs, centroid1, centroid2, rotation_chord, body.safety_factor)) continue;
+    AABB swept = aabb(min3(box1.lo, box2.lo), max3(box1.hi, box2.hi));
+    Proxy fp = shape_proxy(fs);
+    // the static tree's proxies whose fat bounds overlap the swept box; only the earliest hit
+    // matters, so the visiting order does not change the result
+    for (int sid = 0; sid < (int)w->shapes.size(); ++sid) {
+      const Shape& ss = w->shapes[sid];
+      if (!ss.is_static || !aabb_overlaps(w->fat[sid], swept)) continue;
+      if (ss.body_id == fs.body_id || !shapes_collide(fs, ss) || !bodies_collide(w, sim.body_id, ss.body_id)) continue;
+      const BodySim& ssim = sim_of(w, w->bodies[ss.body_id]);
+      Proxy sp = shape_proxy(ss);
+      ToiOut o = time_of_impact(sp, fp, relative_sweep(ssim, base), sweep, fraction);
+      if (0.0f < o.fraction && o.fraction < fraction) fraction = o.fraction;
+    }
+  }
+  real spec = speculative_distance();
+  if (fraction < 1.0f) {
+    Q q = nlerp(sweep.q1, sweep.q2, fraction);
+    V3 c = lerp(sweep.c1, sweep.c2, fraction);
+    V3 origin = c - rotate(q, sweep.local_center);
+    WXf t = {offset_pos(base, origin), q};
+    Pos center = offset_pos(base, c);
+    sim.transform = t;
+    sim.center = center;
+    sim.rotation0 = q;
+    sim.center0 = center;
+    sim.flags |= kHadToi;
+    // the gravity lost in the remaining time (other forces ignored, as the reference does)
+    real time_loss = (1.0f - fraction) * w->ctx.dt;
+    V3 g = v3(w->def.gravity[0], w->def.gravity[1], w->def.gravity[2]);
+    V3 dv = (-time_loss * sim.gravity_scale) * g;
+    dv.x = (st.flags & kLockLinX) ? 0.0f : dv.x;
+    dv.y = (st.flags & kLockLinY) ? 0.0f : dv.y;
+    dv.z = (st.flags & kLockLinZ) ? 0.0f : dv.z;
+    st.v = st.v + dv;
+    for (int sid = body.head_shape; sid != -1; sid = w->shapes[sid].next_shape) {
+      Shape& sh = w->shapes[sid];
+      AABB a = fat_shape_aabb(sh, t, spec);
+      sh.aabb = a;
+      if (!aabb_contains(w->fat[sid], a)) {
+        w->fat[sid] = aabb_inflate(a, sh.aabb_margin);
+        w->proxy_moved[sid] = 1;
+      }
+    }
+  } else {
+    sim.rotation0 = sim.transform.q;
+    sim.center0 = sim.center;
+    for (int sid = body.head_shape; sid != -1; sid = w->shapes[sid].next_shape) {
+      Shape& sh = w->shapes[sid];
+      if (!aabb_contains(w->fat[sid], sh.aabb)) {
+        w->fat[sid] = aabb_inflate(sh.aabb, sh.aabb_margin);
+        w->proxy_moved[sid] = 1;
+      }
+    }
+  }
+  // solver_integration.rs:556-564: the world inertia at the (possibly moved back) rotation
+  M3 R = matrix_from_quat(sim.transform.q);
+  sim.inv_inertia_world = mul_mm(mul_mm(R, sim.inv_inertia_local), transpose(R));
+}
+
+// solver_integration.rs:587 finalize_body_range (sleep disabled), then the continuous pass of
+// the fast bodies in body order (solver_integration.rs:540-566)
 void finalize(nso_world* w) {
   real dt = w->ctx.dt, inv_dt = w->ctx.inv_dt;
   real spec = speculative_distance();
@@ -1749,6 +1913,8 @@ void finalize(nso_world* w) {
       }
     }
   }
+  for (int i = 0; i < n_; ++i)
+    if (w->awake_sims[i].flags & kIsFast) solve_continuous(w, i);
 }
 
 }  // namespace
@@ -2029,6 +2195,31 @@ void nso_apply_forces(nso_world* w, const float* force, const float* torque) {
     if (force) s.force = s.force + v3(force[3 * i], force[3 * i + 1], force[3 * i + 2]);
     if (torque) s.torque = s.torque + v3(torque[3 * i], torque[3 * i + 1], torque[3 * i + 2]);
   }
+}
+
+void nso_time_of_impact(const float* pa, int na, float ra, const float* pb, int nb, float rb, const float* sa,
+                        const float* sb, float max_fraction, float* out) {
+  Proxy a, b;
+  a.count = na < 1 ? 1 : (na > 8 ? 8 : na);
+  b.count = nb < 1 ? 1 : (nb > 8 ? 8 : nb);
+  for (int i = 0; i < a.count; ++i) a.pts[i] = v3(pa[3 * i], pa[3 * i + 1], pa[3 * i + 2]);
+  for (int i = 0; i < b.count; ++i) b.pts[i] = v3(pb[3 * i], pb[3 * i + 1], pb[3 * i + 2]);
+  a.radius = ra;
+  b.radius = rb;
+  auto sweep = [](const float* f) {
+    Sweep s;
+    s.local_center = v3(f[0], f[1], f[2]);
+    s.c1 = v3(f[3], f[4], f[5]);
+    s.c2 = v3(f[6], f[7], f[8]);
+    s.q1 = quat(v3(f[9], f[10], f[11]), f[12]);
+    s.q2 = quat(v3(f[13], f[14], f[15]), f[16]);
+    return s;
+  };
+  ToiOut o = time_of_impact(a, b, sweep(sa), sweep(sb), max_fraction);
+  float r[13] = {(float)o.state, (float)o.fraction, (float)o.distance, (float)o.point.x, (float)o.point.y,
+                 (float)o.point.z, (float)o.normal.x, (float)o.normal.y, (float)o.normal.z,
+                 (float)o.distance_iterations, (float)o.push_back_iterations, (float)o.root_iterations, 0.0f};
+  for (int i = 0; i < 13; ++i) out[i] = r[i];
 }
 
 void nso_collide_pairs(nso_pair_job* jobs, nso_pair_result* results, int count) {

@@ -178,7 +178,29 @@ def _declare(lib):
     lib.nso_counters.argtypes = [P, P]
     lib.nso_collide_pairs.argtypes = [P, P, ctypes.c_int]
     lib.nso_apply_forces.argtypes = [P, P, P]
+    lib.nso_time_of_impact.argtypes = [P, ctypes.c_int, ctypes.c_float, P, ctypes.c_int, ctypes.c_float, P, P,
+                                       ctypes.c_float, P]
+    lib.nso_time_of_impact.restype = None
     return lib
+
+
+TOI_STATES = {0: "unknown", 1: "failed", 2: "overlapped", 3: "hit", 4: "separated"}
+
+
+def time_of_impact(points_a, radius_a, points_b, radius_b, sweep_a, sweep_b, max_fraction=1.0, precision="f32"):
+    """collision/time_of_impact.rs:391 on two point proxies and sweeps (local_center, c1, c2, q1,
+    q2 with quaternions as x, y, z, s). Returns a dict of the TOIOutput fields."""
+    pa = np.ascontiguousarray(points_a, np.float32).reshape(-1, 3)
+    pb = np.ascontiguousarray(points_b, np.float32).reshape(-1, 3)
+    sa = np.ascontiguousarray(np.concatenate([np.ravel(x) for x in sweep_a]), np.float32)
+    sb = np.ascontiguousarray(np.concatenate([np.ravel(x) for x in sweep_b]), np.float32)
+    assert sa.size == 17 and sb.size == 17
+    out = np.zeros(13, np.float32)
+    load(precision).nso_time_of_impact(_ptr(pa), len(pa), radius_a, _ptr(pb), len(pb), radius_b, _ptr(sa), _ptr(sb),
+                                       max_fraction, _ptr(out))
+    return {"state": TOI_STATES[int(out[0])], "fraction": out[1], "distance": out[2], "point": out[3:6].copy(),
+            "normal": out[6:9].copy(), "distance_iterations": int(out[9]), "push_back_iterations": int(out[10]),
+            "root_iterations": int(out[11])}
 
 
 def set_threads(threads):
