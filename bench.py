@@ -574,7 +574,7 @@ def step_counts_block(m):
             "joints": float(c[3])}
 
 
-def measure_e2e(ctx, scene, kw, schedule, indices=None):
+def measure_e2e(ctx, scene, kw, schedule, indices=None, warmup=0):
     """The schedule through the public API with host buffers: every step uploads that step's
     external forces and torques (24 B per body, host->device); every timed step also reads the
     whole body state back into pinned host memory (64 B per body). The wall clock of each timed
@@ -591,6 +591,12 @@ def measure_e2e(ctx, scene, kw, schedule, indices=None):
     lin = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     ang = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     done, seconds = 0, 0.0
+    while done < warmup:
+        world.apply_forces(forces[done % 8], torques[done % 8])
+        world.step(DT, sub)
+        done += 1
+    if warmup:
+        world.autotune(DT, sub, 3)  # the same launch-shape choice as the device-timed run
     ctx.barrier()
     for target in schedule:
         while done < target - 1:
@@ -676,16 +682,14 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
     schedule = timed_schedule(length, steps, warmup)
     indices = batch_share(kw, ctx.rank, ctx.world_size) if scene == "batched_worlds" else None
     world, info, sub = build_gpu_world(scene, kw, ctx.local_rank, indices)
-    autotune = None
-    if scene == "batched_worlds":
-        for _ in range(warmup):
-            world.step(DT, sub)
-        # the solver's launch shape for this batch, timed from a copy of its state (unchanged)
-        autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms} for b, g, ms in world.autotune(DT, sub, 3)]
-        schedule = [s_ for s_ in schedule if s_ > warmup] or [warmup + 1]
-        m = measure_device_continue(ctx, world, sub, schedule, warmup, sample_clocks=headline)
-    else:
-        m = measure_device(ctx, world, sub, schedule, sample_clocks=headline)
+    for _ in range(warmup):
+        world.step(DT, sub)
+    # launch shapes for this workload (solver, recycle pass, manifold updates, preparation), each
+    # timed from a copy of the world's state after the warm-up; the world is left unchanged
+    autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms} for b, g, ms in world.autotune(DT, sub, 3)]
+    tune_rows, shapes = world.autotune_table(), world.launch_shapes()
+    schedule = [s_ for s_ in schedule if s_ > warmup] or [warmup + 1]
+    m = measure_device_continue(ctx, world, sub, schedule, warmup, sample_clocks=headline)
     world.close()
     bodies = info["dynamic_bodies"]
     value, total_ms = job_throughput(bodies, sub, len(schedule), float(m["step_ms"].sum()), ctx.reduce)
@@ -705,10 +709,12 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
                                                       "finalize"], m["phase"].mean(0))},
         "step_counts_mean": step_counts_block(m), "dynamic_bodies": bodies,
     }
-    if autotune is not None:
-        rec["solver_autotune"] = autotune
+    rec["solver_autotune"] = autotune
+    rec["autotune"] = {"chosen": shapes, "candidates": tune_rows,
+                       "method": "each candidate steps 1 + 3 steps from a copy of the world after the warm-up, "
+                                 "CUDA events; one kernel at a time, the fastest kept; the world is restored"}
     if headline and not args.no_e2e:
-        rec["e2e"] = measure_e2e(ctx, scene, kw, schedule, indices)
+        rec["e2e"] = measure_e2e(ctx, scene, kw, schedule, indices, warmup)
     if headline and ctx.rank == 0 and ctx.world_size == 1 and not args.no_cpu_baseline and scene == "batched_worlds":
         r = oracle_batch_run(kw, warmup, steps, args.cpu_seconds)
         rec["cpu_baseline"] = {

@@ -40,7 +40,8 @@ typedef struct ns_world ns_world;
 typedef struct {
   float gravity[3];            /* (0,-10,0) */
   int enable_sleep;            /* must be 0: sleeping islands are outside this path */
-  int enable_continuous;       /* fast bodies are only flagged (continuous.rs is outside this path) */
+  int enable_continuous;       /* 1: fast dynamic bodies are swept against static shapes after
+                                  finalize and moved back to the time of impact (continuous.rs:337) */
   int enable_warm_starting;    /* 1 */
   float contact_hertz;         /* 30 */
   float contact_damping_ratio; /* 10 */
@@ -251,6 +252,19 @@ int ns_selftest_barrier_timeout(int device, int timeout_ms);
  * ns_last_error). Refused while a tape records. */
 int ns_world_autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_out, int* grid_out,
                       float* ms_out, int max_candidates);
+/* After the solver's shape, ns_world_autotune tunes, one kernel at a time from the same copy of
+ * the world, the launch shapes of the narrowphase recycle pass (contacts per thread: threads per
+ * block and blocks per SM), the full manifold updates and the constraint preparation, and keeps
+ * the fastest of each (every shape gives the same bits). ns_world_autotune_table lists every
+ * timed candidate of the last call: dimension (0 solver, 1 recycle pass, 2 manifold updates,
+ * 3 preparation), value_a (blocks of the solver launch, or threads per block), value_b (1 for a
+ * cooperative solver grid / 0 for a cluster, or blocks per SM at most) and ms per step (-1 when
+ * a cluster size does not fit). Returns the number of rows (any output may be NULL). */
+int ns_world_autotune_table(const ns_world* w, int* dimension, int* value_a, int* value_b, float* ms,
+                            int max_rows);
+/* out8: solver blocks, cooperative grid (0/1), recycle threads per block, recycle blocks per SM,
+ * update threads, update blocks per SM, prepare threads, prepare blocks per SM. */
+int ns_world_launch_shapes(const ns_world* w, int* out8);
 
 /* ---- Adjoint: vector-Jacobian product of a recorded rollout --------------------------------
  * No counterpart in the reference, which has no differentiation; these calls are the

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -88,6 +89,12 @@ struct ns_world {
   size_t cub_scan_bytes = 0;
   int solver_blocks = 1;           // blocks of the solver launch
   bool solver_grid = true;         // cooperative grid (true) or one thread-block cluster
+  // launch shapes of the grid-stride step kernels (threads per block, blocks per SM at most),
+  // chosen by ns_world_autotune; every shape gives the same bits
+  int recycle_threads = kCollideThreads, recycle_per_sm = 16;       // k_collide
+  int update_threads = kCollideUpdateThreads, update_per_sm = 32;   // k_collide_update
+  int prepare_threads = kPrepareThreads, prepare_per_sm = 16;       // k_prepare_slots
+  std::vector<std::array<float, 4>> tune_rows;  // last autotune: dimension, a, b, ms per step
   int sort_bits = 32;              // key bits of the broadphase sort (bucket index + large flag)
   bool state_shared = false;
   size_t state_smem = 0;
@@ -774,8 +781,11 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
     NS_CUDA(w, cudaMemcpyAsync(tape->dev.pre, d.contacts, sizeof(DContact) * (size_t)d.cap, cudaMemcpyDeviceToDevice, s));
   // narrowphase (collide_pass.rs:164)
   NS_CUDA(w, cudaMemsetAsync(d.ctl->collide_count, 0, sizeof(d.ctl->collide_count), s));
-  k_collide<<<std::min(blocks(d.cap, kCollideThreads), 16 * w->sm_count), kCollideThreads, 0, s>>>(d); ++nk;
-  k_collide_update<<<std::min(blocks(d.cap, kCollideUpdateThreads), 32 * w->sm_count), kCollideUpdateThreads, 0, s>>>(d); ++nk;
+  k_collide<<<std::min(blocks(d.cap, w->recycle_threads), w->recycle_per_sm * w->sm_count), w->recycle_threads, 0, s>>>(d);
+  ++nk;
+  k_collide_update<<<std::min(blocks(d.cap, w->update_threads), w->update_per_sm * w->sm_count), w->update_threads, 0,
+                     s>>>(d);
+  ++nk;
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
   if (d.n_worlds == 1) {
@@ -791,7 +801,9 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   k_color_count<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
   k_color_scan<<<kOverflowIndex, kColorScanThreads, 0, s>>>(d); ++nk;
   k_color_scatter<<<d.n_color_blocks, kColorBlock, 0, s>>>(d); ++nk;
-  k_prepare_slots<<<std::min(blocks(d.cap, kPrepareThreads), 16 * w->sm_count), kPrepareThreads, 0, s>>>(d, p); ++nk;
+  k_prepare_slots<<<std::min(blocks(d.cap, w->prepare_threads), w->prepare_per_sm * w->sm_count), w->prepare_threads, 0,
+                    s>>>(d, p);
+  ++nk;
   k_prepare_overflow<<<std::min(std::max(d.n_worlds, 8), 4096), 128, 0, s>>>(d, p); ++nk;
   if (d.n_joints > 0) {
     k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
@@ -2186,6 +2198,26 @@ int ns_selftest_barrier_timeout(int device, int timeout_ms) {
 }
 
 
+// Times `steps` steps (after one untimed step) from the checkpoint, eagerly with the world's
+// current launch shapes; ms per step, or a negative status.
+static int time_from_checkpoint(ns_world* w, const AdCheckpoint& snap, float dt, int substeps, int steps,
+                                cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  int st = restore_checkpoint(w, snap);
+  if (st) return st;
+  if ((st = enqueue_step(w, dt, substeps))) return st;
+  NS_CUDA(w, cudaEventRecord(e0, w->stream));
+  for (int k = 0; k < steps && !st; ++k) st = enqueue_step(w, dt, substeps);
+  if (st) return st;
+  NS_CUDA(w, cudaEventRecord(e1, w->stream));
+  NS_CUDA(w, cudaEventSynchronize(e1));
+  float t = 0.0f;
+  NS_CUDA(w, cudaEventElapsedTime(&t, e0, e1));
+  *ms = t / (float)steps;
+  Control ctl;
+  if ((st = read_control(w, &ctl))) return st;
+  return control_status(w, ctl);
+}
+
 static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_out, int* grid_out,
                     float* ms_out, int max_candidates, int* count) {
   if (!w) return NS_ERR_INVALID;
@@ -2196,8 +2228,8 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
     if (st) return st;
   }
   NS_CUDA(w, cudaSetDevice(w->def.device));
-  // candidate launch shapes: thread-block clusters of 8 and 16 CTAs, cooperative grids of 1..4
-  // blocks per SM (as many as can be co-resident)
+  // candidate solver launch shapes: thread-block clusters of 8 and 16 CTAs, cooperative grids
+  // over half the SMs and of 1..4 blocks per SM (as many as can be co-resident)
   int per_sm = 0;
   NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true, false>, kSolveThreads, 0));
   NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -2205,6 +2237,9 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
   for (int k = 1; k <= std::min(per_sm, 4); ++k) cand.push_back({k * w->sm_count, true});
   const int old_blocks = w->solver_blocks;
   const bool old_grid = w->solver_grid, old_eager = w->eager;
+  const int old_shapes[6] = {w->recycle_threads, w->recycle_per_sm, w->update_threads, w->update_per_sm,
+                             w->prepare_threads, w->prepare_per_sm};
+  w->tune_rows.clear();
   AdCheckpoint snap;
   int st = take_checkpoint(w, &snap);
   std::vector<float> ms(cand.size(), 0.0f);
@@ -2229,29 +2264,46 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
       if (cudaOccupancyMaxActiveClusters(&clusters, k_solve<false, false>, &cfg) != cudaSuccess || clusters < 1) {
         cudaGetLastError();
         ms[c] = -1.0f;  // this cluster size does not fit
+        w->tune_rows.push_back({0.0f, (float)cand[c].first, 0.0f, -1.0f});
         continue;
       }
     }
-    if ((st = restore_checkpoint(w, snap))) break;
-    // one untimed step, then `steps` timed ones, eagerly (the graph is captured for one shape)
-    if ((st = enqueue_step(w, dt, substeps))) break;
-    NS_CUDA(w, cudaEventRecord(e0, w->stream));
-    for (int k = 0; k < steps && !st; ++k) st = enqueue_step(w, dt, substeps);
-    if (st) break;
-    NS_CUDA(w, cudaEventRecord(e1, w->stream));
-    NS_CUDA(w, cudaEventSynchronize(e1));
-    float t = 0.0f;
-    NS_CUDA(w, cudaEventElapsedTime(&t, e0, e1));
-    ms[c] = t / (float)steps;
-    Control ctl;
-    if ((st = read_control(w, &ctl))) break;
-    if ((st = control_status(w, ctl))) break;
+    st = time_from_checkpoint(w, snap, dt, substeps, steps, e0, e1, &ms[c]);
+    w->tune_rows.push_back({0.0f, (float)cand[c].first, cand[c].second ? 1.0f : 0.0f, ms[c]});
   }
-  // keep the fastest shape and put the world back as it was
+  // keep the fastest solver shape
   int best = -1;
   for (size_t c = 0; c < cand.size(); ++c)
     if (ms[c] > 0.0f && (best < 0 || ms[c] < ms[best])) best = (int)c;
   if (!st && best < 0) st = fail(w, NS_ERR_CUDA, "no solver launch shape could be timed");
+  if (!st) {
+    w->solver_blocks = cand[best].first;
+    w->solver_grid = cand[best].second;
+  }
+  // then, one kernel at a time with the others kept, the launch shapes of the recycle pass, the
+  // full manifold updates and the constraint preparation (threads per block within each
+  // kernel's launch bound, blocks per SM at most); the default stays unless a shape is faster
+  struct Dim { int id; int* threads; int* per_sm; std::vector<std::pair<int, int>> opts; };
+  std::vector<Dim> dims = {
+      {1, &w->recycle_threads, &w->recycle_per_sm, {{256, 16}, {128, 16}, {256, 8}, {256, 32}, {128, 32}}},
+      {2, &w->update_threads, &w->update_per_sm, {{64, 32}, {32, 32}, {64, 16}, {64, 64}, {32, 64}}},
+      {3, &w->prepare_threads, &w->prepare_per_sm, {{128, 16}, {64, 16}, {128, 8}, {128, 32}, {64, 32}}}};
+  for (Dim& dm : dims) {
+    float best_ms = -1.0f;
+    std::pair<int, int> keep = {*dm.threads, *dm.per_sm};
+    for (const auto& o : dm.opts) {
+      if (st) break;
+      *dm.threads = o.first;
+      *dm.per_sm = o.second;
+      float t = -1.0f;
+      st = time_from_checkpoint(w, snap, dt, substeps, steps, e0, e1, &t);
+      w->tune_rows.push_back({(float)dm.id, (float)o.first, (float)o.second, t});
+      if (!st && (best_ms < 0.0f || t < best_ms)) { best_ms = t; keep = o; }
+    }
+    *dm.threads = keep.first;
+    *dm.per_sm = keep.second;
+  }
+  // put the world back as it was
   if (snap.data) {
     int st2 = restore_checkpoint(w, snap);
     cudaStreamSynchronize(w->stream);
@@ -2264,10 +2316,11 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
   if (st) {
     w->solver_blocks = old_blocks;
     w->solver_grid = old_grid;
+    w->recycle_threads = old_shapes[0]; w->recycle_per_sm = old_shapes[1];
+    w->update_threads = old_shapes[2]; w->update_per_sm = old_shapes[3];
+    w->prepare_threads = old_shapes[4]; w->prepare_per_sm = old_shapes[5];
     return st;
   }
-  w->solver_blocks = cand[best].first;
-  w->solver_grid = cand[best].second;
   if (w->graph_exec) { cudaGraphExecDestroy(w->graph_exec); w->graph_exec = nullptr; }
   if (w->graph) { cudaGraphDestroy(w->graph); w->graph = nullptr; }
   int n = std::min<int>((int)cand.size(), max_candidates);
@@ -2285,6 +2338,26 @@ int ns_world_autotune(ns_world* w, float dt, int substeps, int steps, int* block
   int count = 0;
   int st = autotune(w, dt, substeps, steps, blocks_out, grid_out, ms_out, max_candidates, &count);
   return st ? -st : count;
+}
+
+int ns_world_autotune_table(const ns_world* w, int* dimension, int* value_a, int* value_b, float* ms, int max_rows) {
+  if (!w || max_rows < 0) return -NS_ERR_INVALID;
+  int n = std::min<int>((int)w->tune_rows.size(), max_rows);
+  for (int r = 0; r < n; ++r) {
+    if (dimension) dimension[r] = (int)w->tune_rows[r][0];
+    if (value_a) value_a[r] = (int)w->tune_rows[r][1];
+    if (value_b) value_b[r] = (int)w->tune_rows[r][2];
+    if (ms) ms[r] = w->tune_rows[r][3];
+  }
+  return (int)w->tune_rows.size();
+}
+
+int ns_world_launch_shapes(const ns_world* w, int* out8) {
+  if (!w || !out8) return NS_ERR_INVALID;
+  int v[8] = {w->solver_blocks, w->solver_grid ? 1 : 0, w->recycle_threads, w->recycle_per_sm, w->update_threads,
+              w->update_per_sm, w->prepare_threads, w->prepare_per_sm};
+  for (int i = 0; i < 8; ++i) out8[i] = v[i];
+  return NS_OK;
 }
 
 int ns_world_tape_begin(ns_world* w, int checkpoint_substeps) {

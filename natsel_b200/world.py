@@ -120,7 +120,7 @@ EXPORTED = [
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
     "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
-    "ns_world_vjp_f64", "ns_world_autotune",
+    "ns_world_vjp_f64", "ns_world_autotune", "ns_world_autotune_table", "ns_world_launch_shapes",
     "ns_adjoint_selfcheck",
 ]
 
@@ -150,6 +150,8 @@ def load_library(path=LIB_PATH):
     lib.ns_default_revolute_joint_def.argtypes = [ctypes.POINTER(RevoluteJointDef)]
     lib.ns_default_revolute_joint_def.restype = None
     lib.ns_create_revolute_joint_def.argtypes = [P, ctypes.POINTER(RevoluteJointDef)]
+    lib.ns_world_autotune_table.argtypes = [P, P, P, P, P, ctypes.c_int]
+    lib.ns_world_launch_shapes.argtypes = [P, P]
     lib.ns_world_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
     lib.ns_world_synchronize.argtypes = [P]
     lib.ns_world_get_bodies.argtypes = [P, P, P, P, P]
@@ -381,6 +383,29 @@ class World:
         if r < 0:
             raise NsError(-r, self._lib.ns_last_error(self._w).decode())
         return [(int(blocks[c]), bool(grid[c]), float(ms[c])) for c in range(min(r, 8))]
+
+    TUNE_DIMENSIONS = {0: "solver", 1: "recycle_pass", 2: "manifold_updates", 3: "prepare"}
+
+    def autotune_table(self):
+        """Every candidate the last autotune timed: dicts of dimension, a, b, ms_per_step (for the
+        solver a = blocks and b = cooperative grid; otherwise threads per block and blocks per SM)."""
+        n = self._lib.ns_world_autotune_table(self._w, None, None, None, None, 0)
+        if n < 0:
+            raise NsError(-n, "autotune_table")
+        dim, a, b = (np.zeros(max(n, 1), np.int32) for _ in range(3))
+        ms = np.zeros(max(n, 1), np.float32)
+        self._lib.ns_world_autotune_table(self._w, _ptr(dim), _ptr(a), _ptr(b), _ptr(ms), n)
+        return [{"dimension": self.TUNE_DIMENSIONS[int(dim[r])], "a": int(a[r]), "b": int(b[r]),
+                 "ms_per_step": float(ms[r])} for r in range(n)]
+
+    def launch_shapes(self):
+        """The launch shapes in use: solver blocks and grid flag, then threads per block and blocks
+        per SM of the recycle pass, the manifold updates and the preparation."""
+        out = np.zeros(8, np.int32)
+        self._check(self._lib.ns_world_launch_shapes(self._w, _ptr(out)))
+        keys = ["solver_blocks", "solver_grid", "recycle_threads", "recycle_per_sm", "update_threads",
+                "update_per_sm", "prepare_threads", "prepare_per_sm"]
+        return {k: int(v) for k, v in zip(keys, out)}
 
     # ---- adjoint ---------------------------------------------------------------------------
     def tape_begin(self, checkpoint_substeps=8):

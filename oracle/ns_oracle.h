@@ -16,7 +16,7 @@ typedef struct nso_world nso_world;
 typedef struct {
   float gravity[3];
   int enable_sleep;          /* must be 0: sleeping islands are out of scope */
-  int enable_continuous;     /* 1 = flag fast bodies (CCD itself is out of scope) */
+  int enable_continuous;     /* 1 = continuous pass of fast bodies against static shapes */
   int enable_warm_starting;
   float contact_hertz;
   float contact_damping_ratio;

@@ -97,6 +97,16 @@ def test_autotune_keeps_the_world_and_its_trajectory(batched):
     chosen = tuned.solver_counts()
     fastest = min((ms, b, grid) for b, grid, ms in table if ms > 0)
     assert (int(chosen[13]), bool(chosen[14])) == (fastest[1], fastest[2])
+    # the other tuned kernels: every candidate timed, the fastest (or the default on a tie) kept
+    rows = tuned.autotune_table()
+    shapes = tuned.launch_shapes()
+    keys = {"recycle_pass": ("recycle_threads", "recycle_per_sm"), "manifold_updates": ("update_threads", "update_per_sm"),
+            "prepare": ("prepare_threads", "prepare_per_sm")}
+    for dim, (kt, kb) in keys.items():
+        cands = [r for r in rows if r["dimension"] == dim]
+        assert len(cands) == 5 and all(r["ms_per_step"] > 0 for r in cands)
+        best = min(cands, key=lambda r: r["ms_per_step"])
+        assert (shapes[kt], shapes[kb]) == (best["a"], best["b"])
     for _ in range(10):
         tuned.step(DT, 4)
         plain.step(DT, 4)
