@@ -15,8 +15,8 @@ def trajectory_stats(world, gravity=9.81, ground_half=50.0):
     - ``off_ground``: dynamic bodies that left the ground box (fell past its edge);
     - ``touching``: touching contacts (manifolds with at least one point), the resting-contact
       count of a settled pile;
-    - ``max_penetration`` / ``p99_penetration``: the deepest and the 99th-percentile depth over
-      every manifold point (depth = -separation)."""
+    - ``max_penetration`` / ``p999_penetration`` / ``p99_penetration``: the deepest, the
+      99.9th- and the 99th-percentile depth over every manifold point (depth = -separation)."""
     pos, rot, lin, ang = world.bodies()
     dyn = np.array(world.body_types) == 2
     x, y, z = pos[:, 0], pos[:, 1], pos[:, 2]
@@ -34,6 +34,7 @@ def trajectory_stats(world, gravity=9.81, ground_half=50.0):
         "off_ground": int((dyn & ~on).sum()),
         "touching": int((pc > 0).sum()),
         "max_penetration": float(depth.max()),
+        "p999_penetration": float(np.quantile(depth, 0.999)),
         "p99_penetration": float(np.quantile(depth, 0.99)),
     }
 

@@ -7,8 +7,9 @@ pointwise, and there the bar is tight.
 Tolerances (stated per statistic in ``assert_close``), set from the FP32 oracle against the
 FP64 oracle on the same scenes: energy per unit mass of the bodies on the ground 1 %, mean
 speed 0.05 m/s, median height 1 cm + 1 %, bodies that rolled off the ground's edge 5 (or
-0.5 %), touching contacts 3 %, deepest penetration 5 mm + 25 %, 99th-percentile penetration
-1 mm; over the quasi-static pyramid they are tight everywhere."""
+0.5 %), touching contacts 3 %, 99th-percentile penetration 1 mm, 99.9th percentile 3 mm + 15 %,
+the deepest point under 25 cm in both; over the quasi-static pyramid they are tight
+everywhere."""
 import numpy as np
 import pytest
 
@@ -43,8 +44,11 @@ def assert_close(a, b, n_bodies, settled=True):
     assert abs(a["p99_penetration"] - b["p99_penetration"]) <= 1e-3, (a, b)
     if settled:
         assert abs(a["speed"] - b["speed"]) <= 0.05, (a, b)
-        # the single deepest of ~10^4 points is an extreme value: a quarter of it plus 5 mm
-        assert abs(a["max_penetration"] - b["max_penetration"]) <= 0.005 + 0.25 * b["max_penetration"], (a, b)
+        # the 99.9th percentile of ~10^4 points: 3 mm + 15 %; the single deepest point is an
+        # extreme value of a chaotic pile (11 and 16 cm in the 10 000-body pile's FP32 and FP64
+        # runs), held only to a bound
+        assert abs(a["p999_penetration"] - b["p999_penetration"]) <= 0.003 + 0.15 * b["p999_penetration"], (a, b)
+        assert a["max_penetration"] < 0.25 and b["max_penetration"] < 0.25, (a, b)
 
 
 def assert_pointwise(a, b):
