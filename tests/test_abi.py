@@ -165,3 +165,56 @@ def test_bad_pair_jobs_are_rejected_on_the_host_before_any_gpu_work(entry):
     results = np.zeros(len(jobs), narrowphase.PAIR_RESULT_DTYPE)
     status = fn(jobs.ctypes.data_as(ctypes.c_void_p), results.ctypes.data_as(ctypes.c_void_p), len(jobs))
     assert status == (0 if HAS_GPU else 2)
+
+
+def _rust_source():
+    return open(os.path.join(ROOT, "natsel-gpu-sys", "src", "lib.rs")).read()
+
+
+def _c_params(name):
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    m = re.search(r"\b%s\s*\(([^)]*)\)" % name, text)
+    args = [a for a in m.group(1).split(",") if a.strip() and a.strip() != "void"]
+    return len(args)
+
+
+def test_rust_ffi_crate_declares_every_header_function():
+    """natsel-gpu-sys/src/lib.rs (the reference-side binding; cargo is not in this image) declares
+    every function of include/natsel_gpu.h, with the same number of parameters."""
+    src = _rust_source()
+    block = src[src.index('extern "C" {'):]
+    block = block[:block.index("\n}\n")]
+    decls = dict((m.group(1), m.group(2)) for m in re.finditer(r"pub fn (ns_[a-z0-9_]+)\(([^)]*)\)", block, re.S))
+    assert sorted(decls) == declared_functions()
+    for name, params in decls.items():
+        n = len([p for p in params.split(",") if p.strip()])
+        assert n == _c_params(name), name
+
+
+def test_rust_ffi_structs_mirror_the_header_layouts():
+    """Each #[repr(C)] struct of the crate lists the header struct's fields in the same order with
+    types of the same size (checked against the offsets a C99 compiler gives the header)."""
+    src = _rust_source()
+    sizes = {"c_int": 4, "f32": 4, "i32": 4, "u32": 4, "u64": 8, "f64": 8}
+
+    def rust_fields(name):
+        body = re.search(r"pub struct %s \{(.*?)\n\}" % name, src, re.S).group(1)
+        out = []
+        for fname, ftype in re.findall(r"pub (\w+): ([^,\n]+),", body):
+            ftype = ftype.strip()
+            n, base = 1, ftype
+            while base.startswith("["):
+                inner, count = re.match(r"\[(.*); (\d+)\]$", base).groups()
+                n *= int(count)
+                base = inner
+            out.append((fname.rstrip("_") if fname == "type_" else fname, sizes[base] * n, sizes[base]))
+        return out
+
+    layout = _c_layout()
+    for name in ("ns_world_def", "ns_body_def", "ns_shape_def", "ns_pair_job", "ns_pair_result"):
+        off = 0
+        for fname, size, align in rust_fields(name):
+            off = (off + align - 1) // align * align
+            assert layout[(name, fname)] == off, (name, fname)
+            off += size
+        assert (off + 7) // 8 * 8 >= layout[(name, "size")] >= off
