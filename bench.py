@@ -525,6 +525,7 @@ def measure_device(ctx, world, sub, schedule, sample_clocks):
     solve_bytes = np.zeros(k_steps, np.float64)
     launches = np.zeros(k_steps, np.int64)
     counts = np.zeros((k_steps, 4), np.float64)
+    phases = np.zeros(k_steps, np.float64)
     ctx.barrier()
     sampler = ClockSampler(ctx.uuids) if (ctx.rank == 0 and sample_clocks) else None
     wall0 = time.perf_counter()
@@ -548,6 +549,7 @@ def measure_device(ctx, world, sub, schedule, sample_clocks):
             sc = world.solver_counts()
             solve_bytes[k] = solve_launch_bytes(sc, sub)
             launches[k] = int(sc[11])
+            phases[k] = float(sc[15])
             c = world.counters()
             counts[k] = (c[0], c[1], sc[2], sc[5])
     world.synchronize()
@@ -556,20 +558,55 @@ def measure_device(ctx, world, sub, schedule, sample_clocks):
     clocks = sampler.stop() if sampler else None
     step_ms = np.array([s_.elapsed_time(e) for s_, e in zip(starts, ends)])
     return {"step_ms": step_ms, "phase": phase, "solve_bytes": solve_bytes, "launches": launches,
-            "counts": counts, "clocks": clocks, "wall": wall}
+            "counts": counts, "clocks": clocks, "wall": wall, "solve_phases": phases}
 
 
-def roofline_block(m, kernel="k_solve", traffic_file="k_solve_large_pile.json"):
+def latency_floor(ctx, world_kw, substeps=4, solver_blocks=None, steps=60):
+    """The solver's per-phase floor: the time of one dependent phase (the barrier over the launch
+    plus one constraint's load-and-solve chain) measured on a world with one box resting on a
+    ground box, whose launch is 4 phases per substep with one item each. Returns us per phase."""
+    from natsel_b200.world import World, default_world_def
+    kw = dict(world_kw)
+    if solver_blocks is not None:
+        kw["solver_blocks"] = solver_blocks
+    w = World(default_world_def(device=ctx.local_rank, **kw))
+    g = w.create_body(type=0, position=(0.0, -0.5, 0.0))
+    w.create_box(g, 5.0, 0.5, 5.0)
+    b = w.create_body(type=2, position=(0.0, 0.5, 0.0))
+    w.create_box(b, 0.5, 0.5, 0.5)
+    for _ in range(10):
+        w.step(DT, substeps)
+    ms, ph = 0.0, 0
+    for _ in range(steps):
+        w.step(DT, substeps)
+        ms += float(w.phase_times()[3])
+        ph += int(w.solver_counts()[15])
+    w.close()
+    return 1000.0 * ms / max(ph, 1)
+
+
+def roofline_block(m, kernel="k_solve", traffic_file="k_solve_large_pile.json", floor_us=None):
     solve_ms = m["phase"][:, 3]
     achieved = m["solve_bytes"].sum() / (solve_ms.sum() / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
     alg = float(m["solve_bytes"].mean())
     traffic, source = profiled_traffic(alg, traffic_file) if traffic_file else (None, None)
-    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
-            if peak_kind == "measured" else peak_kind,
-            "traffic": traffic, "traffic_source": source,
-            "algorithmic_bytes_per_launch": alg, "launch_ms": float(solve_ms.mean())}
+    rec = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+           if peak_kind == "measured" else peak_kind,
+           "traffic": traffic, "traffic_source": source,
+           "algorithmic_bytes_per_launch": alg, "launch_ms": float(solve_ms.mean())}
+    if floor_us is not None:
+        # the latency roofline the launch actually meets: its dependent phases times the measured
+        # floor of one phase (barrier plus one constraint's chain, one item per phase)
+        ph = float(m["solve_phases"].mean())
+        floor_ms = ph * floor_us / 1000.0
+        rec["latency"] = {"phases_per_launch": ph, "floor_us_per_phase": floor_us, "floor_ms": floor_ms,
+                          "frac": floor_ms / float(solve_ms.mean()),
+                          "us_per_phase": 1000.0 * float(solve_ms.mean()) / ph if ph else None,
+                          "floor_method": "one box resting on a ground box, same solver launch shape: "
+                                          "solve time / its phases (4 per substep, one item each)"}
+    return rec
 
 
 def step_counts_block(m):
@@ -578,7 +615,7 @@ def step_counts_block(m):
             "joints": float(c[3])}
 
 
-def measure_e2e(ctx, scene, kw, schedule, indices=None, warmup=0):
+def measure_e2e(ctx, scene, kw, schedule, indices=None, warmup=0, shapes=None):
     """The schedule through the public API with host buffers: every step uploads that step's
     external forces and torques (24 B per body, host->device); every timed step also reads the
     whole body state back into pinned host memory (64 B per body). The wall clock of each timed
@@ -594,13 +631,13 @@ def measure_e2e(ctx, scene, kw, schedule, indices=None, warmup=0):
     rot = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     lin = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     ang = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    if shapes is not None:
+        world.set_launch_shapes(shapes)  # the same launch shapes as the device-timed run
     done, seconds = 0, 0.0
     while done < warmup:
         world.apply_forces(forces[done % 8], torques[done % 8])
         world.step(DT, sub)
         done += 1
-    if warmup:
-        world.autotune(DT, sub, 3)  # the same launch-shape choice as the device-timed run
     ctx.barrier()
     for target in schedule:
         while done < target - 1:
@@ -685,20 +722,43 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
     length = LENGTHS[scene]
     schedule = timed_schedule(length, steps, warmup)
     indices = batch_share(kw, ctx.rank, ctx.world_size) if scene == "batched_worlds" else None
-    world, info, sub = build_gpu_world(scene, kw, ctx.local_rank, indices)
-    for _ in range(warmup):
-        world.step(DT, sub)
     # launch shapes for this workload (solver, recycle pass, manifold updates, preparation), each
-    # timed from a copy of the world's state after the warm-up; the world is left unchanged
-    autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms} for b, g, ms in world.autotune(DT, sub, 3)]
-    tune_rows, shapes = world.autotune_table(), world.launch_shapes()
+    # timed from a copy of a world's state by the autotuner. A single world is tuned on a copy of
+    # the scene stepped to the middle of its run (the drop's first steps hold few contacts), and
+    # the measured world takes those shapes; a batch is tuned on itself after the warm-up.
+    world, info, sub = build_gpu_world(scene, kw, ctx.local_rank, indices)
+    if scene == "batched_worlds":
+        tune_step = warmup
+        for _ in range(warmup):
+            world.step(DT, sub)
+        autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms}
+                    for b, g, ms in world.autotune(DT, sub, 3)]
+        tune_rows, shapes = world.autotune_table(), world.launch_shapes()
+        done = warmup
+    else:
+        tune_step = length // 2
+        tw, _, _ = build_gpu_world(scene, kw, ctx.local_rank, indices)
+        for _ in range(tune_step):
+            tw.step(DT, sub)
+        autotune = [{"blocks": b, "cooperative_grid": g, "ms_per_step": ms} for b, g, ms in tw.autotune(DT, sub, 3)]
+        tune_rows, shapes = tw.autotune_table(), tw.launch_shapes()
+        tw.close()
+        world.set_launch_shapes(shapes)
+        for _ in range(warmup):
+            world.step(DT, sub)
+        done = warmup
     schedule = [s_ for s_ in schedule if s_ > warmup] or [warmup + 1]
-    m = measure_device_continue(ctx, world, sub, schedule, warmup, sample_clocks=headline)
+    m = measure_device_continue(ctx, world, sub, schedule, done, sample_clocks=headline)
     world.close()
     bodies = info["dynamic_bodies"]
     value, total_ms = job_throughput(bodies, sub, len(schedule), float(m["step_ms"].sum()), ctx.reduce)
     launches = int(ctx.reduce(float(m["launches"].sum()), "sum"))
     traffic_file = "k_solve_large_pile.json" if scene == "large_pile" else None
+    from natsel_b200 import scenes as _scenes
+    s_ = _scenes.WORLD_SETTINGS[scene]
+    floor_us = latency_floor(ctx, {"gravity": s_["gravity"], "enable_continuous": int(s_["enable_continuous"])},
+                             sub, solver_blocks=shapes["solver_blocks"] if shapes["solver_grid"] else
+                             min(shapes["solver_blocks"], 16))
     rec = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ctx.world_size, "steps": len(schedule),
         "warmup": warmup, "ms_per_step": total_ms / len(schedule), "higher_is_better": True,
@@ -707,18 +767,19 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
         "config": config_block(args, desc, schedule, scene) if headline else
         {"workload": "%s: %s" % (scene, desc), "timed_steps": schedule_block(schedule, length),
          "l2": "flushed before each timed step (256 MiB write outside the timed events)"},
-        "roofline": roofline_block(m, traffic_file=traffic_file),
+        "roofline": roofline_block(m, traffic_file=traffic_file, floor_us=floor_us),
         "clocks": m["clocks"], "gpu_launches": launches, "wall_s": m["wall"],
         "phase_ms_mean": {k: float(v) for k, v in zip(["broadphase", "collide", "state_color_prepare", "solve",
                                                       "finalize"], m["phase"].mean(0))},
         "step_counts_mean": step_counts_block(m), "dynamic_bodies": bodies,
     }
     rec["solver_autotune"] = autotune
-    rec["autotune"] = {"chosen": shapes, "candidates": tune_rows,
-                       "method": "each candidate steps 1 + 3 steps from a copy of the world after the warm-up, "
-                                 "CUDA events; one kernel at a time, the fastest kept; the world is restored"}
+    rec["autotune"] = {"chosen": shapes, "candidates": tune_rows, "tuned_at_step": tune_step,
+                       "method": "each candidate steps 1 + 3 steps from a copy of the world's state at the "
+                                 "tuning step, CUDA events; one kernel at a time, the fastest kept; the world "
+                                 "is restored, and the measured world takes the chosen shapes"}
     if headline and not args.no_e2e:
-        rec["e2e"] = measure_e2e(ctx, scene, kw, schedule, indices, warmup)
+        rec["e2e"] = measure_e2e(ctx, scene, kw, schedule, indices, warmup, shapes)
     if headline and ctx.rank == 0 and ctx.world_size == 1 and not args.no_cpu_baseline and scene == "batched_worlds":
         r = oracle_batch_run(kw, warmup, steps, args.cpu_seconds)
         rec["cpu_baseline"] = {

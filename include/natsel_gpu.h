@@ -182,7 +182,8 @@ void* ns_world_stream(ns_world* world);
  * [6] overflow contacts [7] restitution on [8] gyroscopic bodies [9] overflow points
  * [10] overflow static sides [11] library kernel launches per step [12] library kernel
  * launches since creation; [13] blocks of the solver launch [14] 1 when that launch is a
- * cooperative grid, 0 when it is one thread-block cluster; [15] zero. */
+ * cooperative grid, 0 when it is one thread-block cluster; [15] dependent phases of the last
+ * solver launch (each ends at a barrier over the launch). */
 int ns_world_solver_counts(ns_world* world, int64_t* counts16);
 
 /* Batch narrowphase (replaces the per-pair routines collide_hulls_with_scratch
@@ -265,6 +266,12 @@ int ns_world_autotune_table(const ns_world* w, int* dimension, int* value_a, int
 /* out8: solver blocks, cooperative grid (0/1), recycle threads per block, recycle blocks per SM,
  * update threads, update blocks per SM, prepare threads, prepare blocks per SM. */
 int ns_world_launch_shapes(const ns_world* w, int* out8);
+/* Sets the launch shapes (the same 8 values) directly, e.g. ones an earlier autotune chose on a
+ * world of the same kind at a representative step. Threads per block must be multiples of 32
+ * within each kernel's launch bound (256, 64, 128), blocks per SM 1..64, a cluster 1..16 CTAs
+ * that fits, a cooperative grid co-resident; NS_ERR_INVALID otherwise. Uploads the scene if it
+ * is not yet on the device. Every shape gives the same bits. */
+int ns_world_set_launch_shapes(ns_world* w, const int* in8);
 
 /* ---- Adjoint: vector-Jacobian product of a recorded rollout --------------------------------
  * No counterpart in the reference, which has no differentiation; these calls are the

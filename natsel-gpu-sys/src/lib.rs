@@ -174,6 +174,7 @@ extern "C" {
     pub fn ns_world_autotune_table(w: *const ns_world, dimension: *mut c_int, value_a: *mut c_int,
                                    value_b: *mut c_int, ms: *mut f32, max_rows: c_int) -> c_int;
     pub fn ns_world_launch_shapes(w: *const ns_world, out8: *mut c_int) -> c_int;
+    pub fn ns_world_set_launch_shapes(w: *mut ns_world, in8: *const c_int) -> c_int;
 
     pub fn ns_world_tape_begin(w: *mut ns_world, checkpoint_substeps: c_int) -> c_int;
     pub fn ns_world_tape_end(w: *mut ns_world) -> c_int;

@@ -2068,6 +2068,27 @@ int ns_world_solver_counts(ns_world* w, int64_t* out) {
   Control c;
   int st = read_control(w, &c);
   if (st) return st;
+  {
+    // the dependent phases of the last solver launch, listed as k_solve lists them: per substep
+    // integrate velocities (+ the overflow warm start and the body warm start when there is
+    // overflow work), push colours, integrate positions, relax colours; then the restitution
+    // iterations' colours
+    const JointRanges& jr = w->jr;
+    bool ovf_work = c.overflow_count > 0 || jr.off[kOverflowIndex + 1] > jr.off[kOverflowIndex];
+    int64_t n = ovf_work ? 3 : 1, m = 0;
+    for (int stage = 0; stage < 2; ++stage) {
+      if (stage == 1) n++;
+      if (ovf_work) n++;
+      for (int col = 0; col < kOverflowIndex; ++col)
+        if (c.color_offset[col + 1] != c.color_offset[col] || jr.off[col + 1] != jr.off[col]) n++;
+    }
+    if (c.any_restitution && w->def.restitution_iterations > 0) {
+      if (c.overflow_count > 0) m++;
+      for (int col = 0; col < kOverflowIndex; ++col)
+        if (c.color_offset[col + 1] != c.color_offset[col]) m++;
+    }
+    out[15] = (int64_t)w->last_substeps * n + (int64_t)w->def.restitution_iterations * m;
+  }
   int total = c.color_offset[kOverflowIndex];
   std::vector<int4> idx(std::max(total, 1));
   if (total > 0)
@@ -2350,6 +2371,55 @@ int ns_world_autotune_table(const ns_world* w, int* dimension, int* value_a, int
     if (ms) ms[r] = w->tune_rows[r][3];
   }
   return (int)w->tune_rows.size();
+}
+
+int ns_world_set_launch_shapes(ns_world* w, const int* in8) {
+  if (!w || !in8) return NS_ERR_INVALID;
+  if (!w->uploaded) {
+    int st = upload_world(w);
+    if (st) return st;
+  }
+  NS_CUDA(w, cudaSetDevice(w->def.device));
+  const int blocks_ = in8[0], grid = in8[1];
+  auto threads_ok = [](int t, int most) { return t >= 32 && t <= most && t % 32 == 0; };
+  if (!threads_ok(in8[2], kCollideThreads) || !threads_ok(in8[4], kCollideUpdateThreads) ||
+      !threads_ok(in8[6], kPrepareThreads))
+    return fail(w, NS_ERR_INVALID, "threads per block must be a multiple of 32 within the kernel's launch bound");
+  for (int k : {3, 5, 7})
+    if (in8[k] < 1 || in8[k] > 64) return fail(w, NS_ERR_INVALID, "blocks per SM must be in 1..64");
+  if (grid != 0 && grid != 1) return fail(w, NS_ERR_INVALID, "the solver grid flag must be 0 or 1");
+  if (grid) {
+    int per_sm = 0;
+    NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<true, false>, kSolveThreads, 0));
+    if (blocks_ < 1 || blocks_ > per_sm * w->sm_count)
+      return fail(w, NS_ERR_INVALID, "a cooperative solver grid of %d blocks is not co-resident", blocks_);
+  } else {
+    if (blocks_ < 1 || blocks_ > kMaxSolveCluster) return fail(w, NS_ERR_INVALID, "cluster of %d CTAs", blocks_);
+    NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(kSolveThreads);
+    cfg.gridDim = dim3(blocks_);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = blocks_;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_solve<false, false>, &cfg) != cudaSuccess || clusters < 1) {
+      cudaGetLastError();
+      return fail(w, NS_ERR_INVALID, "a cluster of %d CTAs does not fit on this device", blocks_);
+    }
+  }
+  w->solver_blocks = blocks_;
+  w->solver_grid = grid != 0;
+  w->recycle_threads = in8[2]; w->recycle_per_sm = in8[3];
+  w->update_threads = in8[4]; w->update_per_sm = in8[5];
+  w->prepare_threads = in8[6]; w->prepare_per_sm = in8[7];
+  if (w->graph_exec) { cudaGraphExecDestroy(w->graph_exec); w->graph_exec = nullptr; }
+  if (w->graph) { cudaGraphDestroy(w->graph); w->graph = nullptr; }
+  return NS_OK;
 }
 
 int ns_world_launch_shapes(const ns_world* w, int* out8) {

@@ -120,7 +120,7 @@ EXPORTED = [
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
     "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
-    "ns_world_vjp_f64", "ns_world_autotune", "ns_world_autotune_table", "ns_world_launch_shapes",
+    "ns_world_vjp_f64", "ns_world_autotune", "ns_world_autotune_table", "ns_world_launch_shapes", "ns_world_set_launch_shapes",
     "ns_adjoint_selfcheck",
 ]
 
@@ -152,6 +152,7 @@ def load_library(path=LIB_PATH):
     lib.ns_create_revolute_joint_def.argtypes = [P, ctypes.POINTER(RevoluteJointDef)]
     lib.ns_world_autotune_table.argtypes = [P, P, P, P, P, ctypes.c_int]
     lib.ns_world_launch_shapes.argtypes = [P, P]
+    lib.ns_world_set_launch_shapes.argtypes = [P, P]
     lib.ns_world_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
     lib.ns_world_synchronize.argtypes = [P]
     lib.ns_world_get_bodies.argtypes = [P, P, P, P, P]
@@ -406,6 +407,13 @@ class World:
         keys = ["solver_blocks", "solver_grid", "recycle_threads", "recycle_per_sm", "update_threads",
                 "update_per_sm", "prepare_threads", "prepare_per_sm"]
         return {k: int(v) for k, v in zip(keys, out)}
+
+    def set_launch_shapes(self, shapes):
+        """Apply launch shapes (a dict as launch_shapes() returns) chosen elsewhere."""
+        keys = ["solver_blocks", "solver_grid", "recycle_threads", "recycle_per_sm", "update_threads",
+                "update_per_sm", "prepare_threads", "prepare_per_sm"]
+        arr = np.array([int(shapes[k]) for k in keys], np.int32)
+        self._check(self._lib.ns_world_set_launch_shapes(self._w, _ptr(arr)))
 
     # ---- adjoint ---------------------------------------------------------------------------
     def tape_begin(self, checkpoint_substeps=8):

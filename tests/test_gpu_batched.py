@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from natsel_b200 import scenes
-from natsel_b200.world import World, default_world_def
+from natsel_b200.world import NsError, World, default_world_def
 from oracle import pyoracle
 
 pytestmark = pytest.mark.gpu
@@ -107,9 +107,19 @@ def test_autotune_keeps_the_world_and_its_trajectory(batched):
         assert len(cands) == 5 and all(r["ms_per_step"] > 0 for r in cands)
         best = min(cands, key=lambda r: r["ms_per_step"])
         assert (shapes[kt], shapes[kb]) == (best["a"], best["b"])
+    # the same shapes applied to a fresh world of the same scene (ns_world_set_launch_shapes)
+    applied = build()
+    applied.set_launch_shapes(shapes)
+    assert applied.launch_shapes() == shapes
+    for _ in range(5):
+        applied.step(DT, 4)
     for _ in range(10):
         tuned.step(DT, 4)
         plain.step(DT, 4)
-        assert tuned.state_hash() == plain.state_hash()
-    tuned.close()
-    plain.close()
+        applied.step(DT, 4)
+        assert tuned.state_hash() == plain.state_hash() == applied.state_hash()
+    bad = dict(shapes, update_threads=96)  # above k_collide_update's launch bound
+    with pytest.raises(NsError):
+        applied.set_launch_shapes(bad)
+    for w in (tuned, plain, applied):
+        w.close()
