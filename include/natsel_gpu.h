@@ -282,9 +282,9 @@ int ns_world_set_launch_shapes(ns_world* w, const int* in8);
  * substeps have passed since the last checkpoint (steps are whole, so a checkpoint falls on
  * the first step boundary at or after that count). While recording, dt must be > 0 and
  * ns_world_apply_forces is refused. Scope: one world (no sub-worlds) of box bodies with the
- * centre of mass at the body origin, no joints, restitution, rolling resistance or continuous
- * collision (NS_ERR_UNSUPPORTED otherwise); steps that put contacts in the overflow colour are
- * reported by ns_world_vjp as NS_ERR_UNSUPPORTED. */
+ * centre of mass at the body origin, no joints, rolling resistance or continuous collision
+ * (NS_ERR_UNSUPPORTED otherwise); steps that put contacts in the overflow colour are reported
+ * by ns_world_vjp as NS_ERR_UNSUPPORTED, and steps with restitution by ns_world_vjp_f64. */
 int ns_world_tape_begin(ns_world* w, int checkpoint_substeps);
 /* Stops recording; the tape stays for ns_world_vjp. */
 int ns_world_tape_end(ns_world* w);
@@ -308,6 +308,11 @@ int ns_world_tape_info(ns_world* w, int64_t* out);
  * cones are held). Synchronous. */
 int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float* dlin, const float* dang,
                  float* dlin0, float* dang0, float* dmass, float* dfriction, float* dpos0, float* drot0);
+/* drestitution[n_bodies]: the last ns_world_vjp's cotangent of each body's shape restitution
+ * (a contact's coefficient is the larger of its two shapes', world_runtime.rs mix_restitution,
+ * and its cotangent goes to the body whose shape supplied it; zero for bodies no restitution
+ * update reached). NS_ERR_INVALID before the first ns_world_vjp or after bodies were added. */
+int ns_world_vjp_restitution(const ns_world* w, float* drestitution);
 /* The same vector-Jacobian product with the reverse pass run on the host in f64 (the replay of
  * the recorded steps still runs on the GPU, bit-identical to the recording): the f64 reference
  * for ns_world_vjp's f32 device pass. Same arguments, outputs in double; much slower (one CPU
@@ -324,7 +329,8 @@ int ns_world_vjp_f64(ns_world* w, const float* dpos, const float* drot, const fl
  * kind of the box cases (-1 otherwise). which 12..16 instead compare the hand-written reverse
  * sweeps the GPU runs for warm start, push, relax (also their state-and-impulse-only form),
  * integrate positions and integrate velocities (without the gyroscopic step) with the
- * dual-number products. */
+ * dual-number products. which 17 checks restitution like 0..11; which 18 compares the
+ * hand-written reverse of the relative normal velocity prepare samples with the dual numbers. */
 int ns_adjoint_selfcheck(int which, int seed, double* worst);
 
 #ifdef __cplusplus

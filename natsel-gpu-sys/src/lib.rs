@@ -183,6 +183,7 @@ extern "C" {
     pub fn ns_world_vjp(w: *mut ns_world, dpos: *const f32, drot: *const f32, dlin: *const f32, dang: *const f32,
                         dlin0: *mut f32, dang0: *mut f32, dmass: *mut f32, dfriction: *mut f32, dpos0: *mut f32,
                         drot0: *mut f32) -> c_int;
+    pub fn ns_world_vjp_restitution(w: *const ns_world, drestitution: *mut f32) -> c_int;
     pub fn ns_world_vjp_f64(w: *mut ns_world, dpos: *const f32, drot: *const f32, dlin: *const f32,
                             dang: *const f32, dlin0: *mut f64, dang0: *mut f64, dmass: *mut f64,
                             dfriction: *mut f64, dpos0: *mut f64, drot0: *mut f64) -> c_int;
@@ -318,18 +319,19 @@ pub struct Grads {
     pub ang0: Vec<f32>,
     pub mass: Vec<f32>,
     pub friction: Vec<f32>,
+    pub restitution: Vec<f32>,
 }
 
 impl Grads {
     pub fn new(bodies: usize) -> Self {
         Grads { lin0: vec![0.0; 3 * bodies], ang0: vec![0.0; 3 * bodies], mass: vec![0.0; bodies],
-                friction: vec![0.0; bodies] }
+                friction: vec![0.0; bodies], restitution: vec![0.0; bodies] }
     }
 }
 
 /// The rollout tape: records the steps taken through it (checkpoints every
 /// `checkpoint_substeps` substeps) and pulls cotangents of the final state back to the
-/// initial velocities, masses and frictions. Dropping it releases the tape.
+/// initial velocities, masses, frictions and restitutions. Dropping it releases the tape.
 pub struct Tape<'a> {
     gpu: &'a mut GpuWorld,
 }
@@ -350,7 +352,8 @@ impl<'a> Tape<'a> {
             ns_world_vjp(self.gpu.ptr, dpos.as_ptr(), std::ptr::null(), std::ptr::null(), std::ptr::null(),
                          grads.lin0.as_mut_ptr(), grads.ang0.as_mut_ptr(), grads.mass.as_mut_ptr(),
                          grads.friction.as_mut_ptr(), std::ptr::null_mut(), std::ptr::null_mut())
-        }, self.gpu.ptr)
+        }, self.gpu.ptr)?;
+        check(unsafe { ns_world_vjp_restitution(self.gpu.ptr, grads.restitution.as_mut_ptr()) }, self.gpu.ptr)
     }
 }
 

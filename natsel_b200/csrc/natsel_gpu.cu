@@ -75,6 +75,7 @@ struct ns_world {
   std::vector<void*> allocations;
   std::vector<size_t> allocation_bytes;
   struct AdTape* tape = nullptr;   // rollout record for the adjoint (ns_world_tape_begin)
+  std::vector<float> vjp_restitution;  // the last f32 VJP's restitution cotangents, body id order
   // Device buffers kept for reuse by later tapes and VJPs and freed with the world: checkpoint
   // buffers (with their copy tables, valid for the world's allocation set, which is fixed once
   // uploaded), the VJP's step tapes and its cotangent buffers.
@@ -1061,8 +1062,7 @@ int check_adjoint_scope(ns_world* w) {
   if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
   for (const HostShape& hs : w->shapes) {
     if (hs.d.type != kHull) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint covers box shapes only");
-    if (hs.d.restitution != 0.0f || hs.d.rolling != 0.0f)
-      return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover restitution or rolling resistance");
+    if (hs.d.rolling != 0.0f) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover rolling resistance");
   }
   for (const DSim& a : w->asims) {
     if (a.local_center.x != 0.0f || a.local_center.y != 0.0f || a.local_center.z != 0.0f)
@@ -1091,6 +1091,8 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
   size_t o_push = take(sizeof(float4) * 4 * cap * max_substeps);
   size_t o_relax = take(sizeof(float4) * 5 * cap * max_substeps);
   size_t o_fin = take(sizeof(float4) * cap), o_mode = take(cap), o_ops = take(sizeof(CopyOp) * 20);
+  const int rest_its = std::max(w->def.restitution_iterations, 0);
+  size_t o_rest = take(sizeof(float4) * 6 * cap * (size_t)std::max(rest_its, 1));
   int st = reuse_buffer(w, &w->tapes_buf, &w->tapes_cap, per * (size_t)count);
   if (st) return st;
   ts->data = w->tapes_buf;
@@ -1126,8 +1128,11 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
     t.relax = (float4*)(b + o_relax);
     t.fin = (float4*)(b + o_fin);
     t.mode = (uint8_t*)(b + o_mode);
+    t.rest = (float4*)(b + o_rest);
+    t.rest_iterations = rest_its;
     t.substeps = 0;
     h.solve.body = t.body; h.solve.push = t.push; h.solve.relax = t.relax; h.solve.fin = t.fin;
+    h.solve.rest = t.rest;
     h.plane_ops = (CopyOp*)(b + o_ops);
     h.n_plane_ops = (int)ops.size();
     NS_CUDA(w, cudaMemcpy(h.plane_ops, ops.data(), ops.size() * sizeof(CopyOp), cudaMemcpyHostToDevice));
@@ -1481,6 +1486,54 @@ extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
         if (which == 15) ip_fn(in, bp, y.data()); else iv_fn(in, bp, y.data());
         double g = 0.0;
         for (int j = 0; j < ny; ++j) g += yb[j] * y[j].d[0];
+        e = std::max(e, std::fabs(g - hand[i]) / std::max(1.0, std::fabs(g)));
+      }
+      break;
+    }
+    case 17: {  // restitution (dual numbers against central differences)
+      x.assign(kRV, 0.0);
+      for (int i = 0; i < 12; ++i) x[i] = r.range(-1.0, 1.0);
+      for (int i = 0; i < 3; ++i) { x[rvDpA + i] = r.range(-0.01, 0.01); x[rvDpB + i] = r.range(-0.01, 0.01); }
+      for (int b = 0; b < 2; ++b) {
+        double* q = &x[b ? rvDqB : rvDqA];
+        q[0] = r.range(-0.02, 0.02); q[1] = r.range(-0.02, 0.02); q[2] = r.range(-0.02, 0.02);
+        q[3] = std::sqrt(1.0 - q[0] * q[0] - q[1] * q[1] - q[2] * q[2]);
+      }
+      for (int q = 0; q < 4; ++q) {
+        x[rvLam + q] = r.range(0.05, 1.0);
+        x[rvTot + q] = r.range(0.5, 3.0);
+        x[rvRest + q] = r.range(0.0, 0.4);
+      }
+      x[rvIma] = r.range(0.5, 2.0); x[rvImb] = r.range(0.5, 2.0);
+      random_spd(r, &x[rvSa]); random_spd(r, &x[rvSb]);
+      random_unit(r, &x[rvN], 3);
+      x[rvE] = r.range(0.2, 0.9);
+      for (int q = 0; q < 4; ++q) {
+        for (int f = 0; f < 6; ++f) x[rv_point(q, f)] = r.range(-0.5, 0.5);
+        x[rv_point(q, 6)] = r.range(-0.02, 0.01);
+        x[rv_point(q, 7)] = r.range(0.3, 1.0);
+        // even seeds: every point approaches faster than the threshold (the bounce is armed)
+        x[rv_point(q, 8)] = (seed & 1) ? r.range(-4.0, 0.5) : r.range(-4.0, -1.2);
+      }
+      RParams rp = {1 + seed % 4, 240.0f, 1.0f};
+      e = vjp_fd_error(x, kRestOut, [&](const auto& in, auto* y) { restitution_fn(in, rp, y); }, r);
+      break;
+    }
+    case 18: {  // hand-written reverse of the relative normal velocity against the dual numbers
+      x.assign(kRL, 0.0);
+      for (int i = 0; i < kRL; ++i) x[i] = r.range(-1.0, 1.0);
+      random_unit(r, &x[rlN], 3);
+      const double yb = r.range(-1.0, 1.0);
+      std::vector<double> hand(kRL, 0.0);
+      relvel_vjp(x.data(), yb, hand.data());
+      Dual<double, 1> y[1];
+      e = 0.0;
+      for (int i = 0; i < kRL; ++i) {
+        SeedIn<double, 1> in;
+        in.x = x.data();
+        in.dir[0] = i;
+        relvel_fn(in, y);
+        double g = yb * y[0].d[0];
         e = std::max(e, std::fabs(g - hand[i]) / std::max(1.0, std::fabs(g)));
       }
       break;
@@ -2496,6 +2549,7 @@ static StepTape rebase_tape(const StepTape& t, const char* dev_base, char* host_
   StepTape h = t;
   h.sims = rb(t.sims); h.pre = rb(t.pre); h.post = rb(t.post); h.ctl = rb(t.ctl);
   h.body = rb(t.body); h.push = rb(t.push); h.relax = rb(t.relax); h.fin = rb(t.fin); h.mode = rb(t.mode);
+  h.rest = rb(t.rest);
   CPlanes& P = h.planes;
   P.idx = rb(t.planes.idx); P.mass = rb(t.planes.mass); P.ia0 = rb(t.planes.ia0); P.ia1 = rb(t.planes.ia1);
   P.ib1 = rb(t.planes.ib1); P.n = rb(t.planes.n); P.t1 = rb(t.planes.t1); P.t2 = rb(t.planes.t2);
@@ -2568,6 +2622,8 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     size_t o_pb = take(sizeof(float) * kPB * (size_t)n), o_kb = take(sizeof(float) * ad::kCVOwn * (size_t)cap);
     size_t o_mb = take(sizeof(float) * kMB * (size_t)cap), o_mis = take(sizeof(int));
     size_t o_yrec = take(sizeof(float) * 3 * ad::kRelaxOut * (size_t)cap * max_sub);
+    size_t o_tot = take(sizeof(float) * 4 * (size_t)cap), o_restb = take(sizeof(float) * 4 * (size_t)cap);
+    size_t o_rel = take(sizeof(float) * 4 * (size_t)cap);
     size_t o_seed = take(sizeof(float) * 13 * (size_t)nb), o_out = take(sizeof(float) * 16 * (size_t)nb);
     if (reuse_buffer(w, &w->adj_buf, &w->adj_cap, o) != NS_OK) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
     buf = w->adj_buf;
@@ -2576,6 +2632,7 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     a.bb = (float*)(buf + o_bb); a.cq = (float*)(buf + o_cq); a.pb = (float*)(buf + o_pb);
     a.kb = (float*)(buf + o_kb); a.mb = (float*)(buf + o_mb); a.mismatch = (int*)(buf + o_mis);
     a.yrec = (float*)(buf + o_yrec);
+    a.totb = (float*)(buf + o_tot); a.restb = (float*)(buf + o_restb); a.relb = (float*)(buf + o_rel);
     a.cap = cap; a.n_awake = n;
     float* seed = (float*)(buf + o_seed);
     float* dev_out = (float*)(buf + o_out);
@@ -2611,7 +2668,8 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
         const Control& c = ctl[j - s0];
         if (c.error) st = control_status(w, c);
         else if (c.overflow_count > 0) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has overflow constraints; the adjoint does not cover them", j);
-        else if (c.any_restitution) st = fail(w, NS_ERR_UNSUPPORTED, "step %d has restitution", j);
+        else if (c.any_restitution && f64)
+          st = fail(w, NS_ERR_UNSUPPORTED, "step %d has restitution; the f64 reverse pass does not cover it", j);
       }
       if (st) break;
       if (f64) {
@@ -2626,10 +2684,29 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
       for (int j = s1 - 1; j >= s0 && st == NS_OK; --j) {
         const StepTape& t = ts.steps[j - s0].dev;
         StepParams p = make_step_params(w, tp->steps[j].dt, tp->steps[j].substeps);
-        int n_slots = ctl[j - s0].color_offset[kOverflowIndex];
+        const Control& c = ctl[j - s0];
+        int n_slots = c.color_offset[kOverflowIndex];
+        bool rest = n_slots > 0 && c.any_restitution;
         if (n > 0) k_adj_finalize<<<blocks(n, 128), 128, 0, w->stream>>>(t, a, n);
         if (n_slots > 0) k_adj_store<<<blocks(n_slots, 128), 128, 0, w->stream>>>(t, a, n_slots);
+        // the restitution iterations ran after the substeps, colours in order: reverse them
+        if (rest && p.restitution_iterations > 0) {
+          const ad::RParams rp = {0, p.inv_h, p.restitution_threshold};
+          const int per_block = kAdjThreads / 32;
+          for (int it = p.restitution_iterations - 1; it >= 0; --it)
+            for (int col = kOverflowIndex - 1; col >= 0; --col) {
+              int cnt = c.color_offset[col + 1] - c.color_offset[col];
+              if (cnt <= 0) continue;
+              k_adj_restitution<<<blocks(cnt, per_block), kAdjThreads, 0, w->stream>>>(t, a, d, rp, it, col);
+              launches += 1;
+            }
+        }
         if ((st = launch_adj_solve(w, t, a, p))) break;
+        // prepare's relative velocities read the velocities at the step's start
+        if (rest) {
+          k_adj_relvel<<<blocks(n_slots, 128), 128, 0, w->stream>>>(t, a, n_slots);
+          launches += 1;
+        }
         if (n_slots > 0) k_adj_consts<<<blocks(n_slots, 64), 64, 0, w->stream>>>(t, a, p, n_slots);
         if (n_slots > 0) k_adj_prepare<<<blocks(n_slots, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d, p, n_slots);
         if (n > 0) k_adj_inertia<<<blocks(n, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a);
@@ -2704,6 +2781,16 @@ int ns_world_vjp(ns_world* w, const float* dpos, const float* drot, const float*
     if (dmass) dmass[i] = (float)r[6];
     if (dfriction) dfriction[i] = (float)r[7];
   }
+  w->vjp_restitution.assign(w->bodies.size(), 0.0f);
+  for (size_t i = 0; i < w->bodies.size(); ++i) w->vjp_restitution[i] = (float)o[16 * i + 15];
+  return NS_OK;
+}
+
+int ns_world_vjp_restitution(const ns_world* w, float* drestitution) {
+  if (!w || !drestitution) return NS_ERR_INVALID;
+  if (w->vjp_restitution.size() != w->bodies.size())
+    return fail(const_cast<ns_world*>(w), NS_ERR_INVALID, "no ns_world_vjp result for the current bodies");
+  std::copy(w->vjp_restitution.begin(), w->vjp_restitution.end(), drestitution);
   return NS_OK;
 }
 

@@ -463,6 +463,102 @@ NSD_HD void relax_fn(const In& x, const CParams& cp, T* y) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Restitution (nsd_solve.cuh restitution_constraint, contact_solver.rs:1135 apply_restitution_body)
+// has its own input vector: the two bodies' velocities and final position deltas, the points'
+// normal, total normal and restitution impulses, and the constants the update reads.
+enum RV : int {
+  rvVA = 0, rvWA = 3, rvVB = 6, rvWB = 9, rvDpA = 12, rvDpB = 15, rvDqA = 18, rvDqB = 22,
+  rvLam = 26, rvTot = 30, rvRest = 34, rvIma = 38, rvImb = 39, rvSa = 40, rvSb = 46, rvN = 52, rvE = 55,
+  rvPoint = 56,  // + 10 q: ra 0..2, rb 3..5, base separation 6, normal mass 7, relative velocity 8
+  kRV = 96,
+};
+NSD_HD int rv_point(int q, int f) { return rvPoint + 10 * q + f; }
+// Outputs: vA wA vB wB (12), normal impulses (4), total normal impulses (4), restitution impulses (4).
+constexpr int kRestOut = 24;
+struct RParams {
+  int pc;
+  float inv_h, threshold;
+};
+
+// The restitution update of one constraint, restated on a scalar type T (float, double or a dual
+// number). With restitution 0 the update does nothing (the outputs are the inputs).
+template <class T, class In>
+NSD_HD void restitution_fn(const In& x, const RParams& rp, T* y) {
+  TV3<T> va = in3<T>(x, rvVA), wa = in3<T>(x, rvWA), vb = in3<T>(x, rvVB), wb = in3<T>(x, rvWB);
+  for (int q = 0; q < 4; ++q) {
+    y[12 + q] = x(rvLam + q);
+    y[16 + q] = x(rvTot + q);
+    y[20 + q] = x(rvRest + q);
+  }
+  T e = x(rvE);
+  if (val(e) != 0.0f) {
+    T inv_h = T(rp.inv_h);
+    T nrt = T(-rp.threshold);
+    bool rmask = e > T(0.0f);
+    TV3<T> dp = in3<T>(x, rvDpB) - in3<T>(x, rvDpA);
+    TV3<T> n = in3<T>(x, rvN);
+    T ns = dot(n, dp);
+    TQ<T> dqa = in4<T>(x, rvDqA), dqb = in4<T>(x, rvDqB);
+    TV3<T> na = inv_rotate_wide(dqa, n), nb = inv_rotate_wide(dqb, n);
+    T ima = x(rvIma), imb = x(rvImb);
+    TSym<T> sa = in_sym<T>(x, rvSa), sb = in_sym<T>(x, rvSb);
+    for (int q = 0; q < rp.pc; ++q) {
+      TV3<T> ra = in3<T>(x, rv_point(q, 0)), rb = in3<T>(x, rv_point(q, 3));
+      T lam = y[12 + q], tot = y[16 + q], rest = y[20 + q];
+      T relvel = x(rv_point(q, 8));
+      T s = (ns + (dot(nb, rb) - dot(na, ra))) + x(rv_point(q, 6));
+      T nm = rmask ? x(rv_point(q, 7)) : T(0.0f);
+      T comp = tot - rest;
+      bool armed = rmask && relvel < nrt && comp > T(0.0f);
+      T sbias = tmax(T(0.0f), s * inv_h);
+      T vbias = armed ? e * relvel : sbias;
+      TV3<T> vra = va + cross(wa, ra), vrb = vb + cross(wb, rb);
+      T vn = dot(vrb - vra, n);
+      T neg = nm * (vn + vbias);
+      T ni = tmax(lam - neg, T(0.0f));
+      T impulse = ni - lam;
+      T app = tmin(tmax(-nm * vn, T(0.0f)), tmax(impulse, T(0.0f)));
+      T allow = e * (comp + app) - rest;
+      T mx = app + tmax(allow, T(0.0f));
+      impulse = armed ? tmin(impulse, mx) : impulse;
+      y[12 + q] = lam + impulse;
+      y[20 + q] = rest + (impulse - app);
+      y[16 + q] = tot + impulse;
+      TV3<T> P = impulse * n;
+      wa = wa - sym_mv(sa, cross(ra, P));
+      va = va - ima * P;
+      wb = wb + sym_mv(sb, cross(rb, P));
+      vb = vb + imb * P;
+    }
+  }
+  out3(y, 0, va); out3(y, 3, wa); out3(y, 6, vb); out3(y, 9, wb);
+}
+
+// The relative normal velocity prepare samples for restitution at one point (nsd_kernels.cuh
+// prepare_constraint, contact_solver.rs:626-644): n . ((vB + wB x rB) - (vA + wA x rA)), from
+// the bodies' velocities at the step's start, the manifold normal and the point's anchors.
+enum RL : int { rlVA = 0, rlWA = 3, rlVB = 6, rlWB = 9, rlN = 12, rlRa = 15, rlRb = 18, kRL = 21 };
+template <class T, class In>
+NSD_HD void relvel_fn(const In& x, T* y) {
+  TV3<T> vra = in3<T>(x, rlVA) + cross(in3<T>(x, rlWA), in3<T>(x, rlRa));
+  TV3<T> vrb = in3<T>(x, rlVB) + cross(in3<T>(x, rlWB), in3<T>(x, rlRb));
+  y[0] = dot(in3<T>(x, rlN), vrb - vra);
+}
+// Its reverse: xb += yb * d(relvel)/dx. With d = vrb - vra, the normal takes yb d; vA and vB
+// take -/+ yb n; wA and wB take -/+ yb (r x n); rA and rB take -/+ yb (n x w).
+template <class R>
+NSD_HD void relvel_vjp(const R* x, R yb, R* xb) {
+  PlainIn<R> in{x};
+  TV3<R> va = in3<R>(in, rlVA), wa = in3<R>(in, rlWA), vb = in3<R>(in, rlVB), wb = in3<R>(in, rlWB);
+  TV3<R> n = in3<R>(in, rlN), ra = in3<R>(in, rlRa), rb = in3<R>(in, rlRb);
+  TV3<R> d = (vb + cross(wb, rb)) - (va + cross(wa, ra));
+  TV3<R> gwa = cross(ra, n), gwb = cross(rb, n), gra = cross(n, wa), grb = cross(n, wb);
+  R parts[kRL] = {-n.x, -n.y, -n.z, -gwa.x, -gwa.y, -gwa.z, n.x, n.y, n.z, gwb.x, gwb.y, gwb.z,
+                  d.x, d.y, d.z, -gra.x, -gra.y, -gra.z, grb.x, grb.y, grb.z};
+  for (int i = 0; i < kRL; ++i) xb[i] += yb * parts[i];
+}
+
+// ---------------------------------------------------------------------------------------------
 // Hand-derived reverse sweeps of warm start, push and relax (one thread per constraint). Each
 // takes the stage's inputs x (constraint vector layout) and the cotangents ybar of its outputs
 // and adds the vector-Jacobian product into xbar (kCV entries, zeroed by the caller). They are

@@ -37,12 +37,14 @@ struct StepTape {
   float4* relax;     // [substep][5][cap]: the same before relax, then fr.x, fr.y, twist
   float4* fin;       // [cap]: friction impulse x, y and twist after the solve
   uint8_t* mode;     // [cap]: narrowphase 0 none/disjoint, 1 recycled, 2 new manifold, 3 no points
+  float4* rest;      // [iteration][6][cap]: the inputs of each restitution update (SolveTape::rest)
+  int rest_iterations;
   int substeps;
 };
 
 // Cotangent buffers of the reverse pass.
 enum : int {
-  pbInvMass = 0, pbIiw = 1, pbIinv = 10, pbFriction = 19, pbInertia = 20, kPB = 29,
+  pbInvMass = 0, pbIiw = 1, pbIinv = 10, pbFriction = 19, pbInertia = 20, pbRestitution = 29, kPB = 30,
   // contact manifold cotangent: normal, per point 9 (anchor_a, anchor_b, separation,
   // base separation, normal impulse), friction impulse, twist, cached rotations
   mbN = 0, mbPoint = 3, mbFrictionImpulse = 39, mbTwist = 42, mbRotA = 43, mbRotB = 47, kMB = 51,
@@ -55,6 +57,9 @@ struct AdjBufs {
   float* kb;   // [kCVOwn][cap]: constraint entries cvLam.. of each slot
   float* mb;   // [kMB][cap]: manifold state of each contact id
   float* yrec; // [substep][stage][kRelaxOut][cap]: output cotangents each contact update received
+  float* totb; // [4][cap]: the points' total normal impulses (what restitution reads of them)
+  float* restb;  // [4][cap]: the points' restitution impulses
+  float* relb; // [4][cap]: the points' relative normal velocities at prepare
   int* mismatch;  // narrowphase replays that did not reproduce the forward manifold
   int cap, n_awake;
 };
@@ -66,6 +71,10 @@ __device__ __forceinline__ float& CQ(const AdjBufs& a, int i, int f) { return a.
 __device__ __forceinline__ float& PB(const AdjBufs& a, int i, int f) { return a.pb[(size_t)i * kPB + f]; }
 __device__ __forceinline__ float& KB(const AdjBufs& a, int k, int cv) { return a.kb[(size_t)(cv - ad::cvLam) * a.cap + k]; }
 __device__ __forceinline__ float& MB(const AdjBufs& a, int c, int f) { return a.mb[(size_t)f * a.cap + c]; }
+__device__ __forceinline__ void put3(float* x, int at, V3 v) { x[at] = v.x; x[at + 1] = v.y; x[at + 2] = v.z; }
+__device__ __forceinline__ float& TOTB(const AdjBufs& a, int k, int q) { return a.totb[(size_t)q * a.cap + k]; }
+__device__ __forceinline__ float& RESTB(const AdjBufs& a, int k, int q) { return a.restb[(size_t)q * a.cap + k]; }
+__device__ __forceinline__ float& RELB(const AdjBufs& a, int k, int q) { return a.relb[(size_t)q * a.cap + k]; }
 
 // ---------------------------------------------------------------------------------------------
 // Finalize (k_finalize): centre' = centre + dp, q' = normalize(dq q).
@@ -101,6 +110,9 @@ __global__ void k_adj_store(StepTape t, AdjBufs a, int n_slots) {
   int4 idx = t.planes.idx[k];
   int cid = idx.z, pc = idx.w & 255;
   for (int cv = cvLam; cv < kCV; ++cv) KB(a, k, cv) = 0.0f;
+  // the total normal and restitution impulses start from zero at prepare and nothing after the
+  // step reads them: their cotangents start at zero here, as do the relative velocities'
+  for (int q = 0; q < 4; ++q) { TOTB(a, k, q) = 0.0f; RESTB(a, k, q) = 0.0f; RELB(a, k, q) = 0.0f; }
   for (int q = 0; q < pc; ++q) {
     KB(a, k, cvLam + q) = MB(a, cid, mb_point(q, 8));
     MB(a, cid, mb_point(q, 8)) = 0.0f;
@@ -203,6 +215,10 @@ __device__ void adj_contact(const StepTape& t, const AdjBufs& a, const StepParam
     yb[f] = b >= 0 ? BB(a, b, g < 3 ? g : g + 1) : 0.0f;
   }
   for (int q = 0; q < 4; ++q) yb[12 + q] = KB(a, k, cvLam + q);
+  // relax adds each point's new normal impulse to its total (imp.y += ni), which restitution
+  // reads: the total's cotangent joins the new impulse's and passes on unchanged
+  if (Stage == kRelax)
+    for (int q = 0; q < 4; ++q) yb[12 + q] += TOTB(a, k, q);
   yb[16] = KB(a, k, cvFr); yb[17] = KB(a, k, cvFr + 1); yb[18] = KB(a, k, cvTwist);
   for (int i = 0; i < cvIma; ++i) xb[i] = 0.0f;
   if (Stage == kWarm) warm_vjp<float, false>(x, cp, yb, xb);
@@ -322,6 +338,184 @@ __device__ void adj_iv(const StepTape& t, const AdjBufs& a, const StepParams& p,
     for (int f = 0; f < 4; ++f) CQ(a, i, 4 + f) += xb[22 + f];      // rotation at the step start
     for (int f = 0; f < 4; ++f) BB(a, i, 12 + f) += xb[26 + f];     // substep rotation dq
     for (int f = 0; f < 9; ++f) PB(a, i, pbInertia + f) += xb[30 + f];
+  }
+}
+
+// Reverse of one restitution iteration over one colour (the forward runs after the substeps,
+// colours 0..22 per iteration; the reverse runs iterations and colours backwards): one warp per
+// constraint of colour `colour` evaluates ad::restitution_fn on dual numbers, lane l seeding
+// input directions l, l + 32 and l + 64, and contracts the output tangents with the outputs'
+// cotangents. Bodies' velocity cotangents, the impulses' and the total and restitution
+// impulses' are replaced, position deltas' and constants' accumulated; the restitution
+// coefficient's cotangent goes to the shape whose coefficient the contact took
+// (max(e_a, e_b), world_runtime.rs mix_restitution), the relative velocities' to k_adj_relvel.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_restitution(StepTape t, AdjBufs a, DW w, ad::RParams rp0,
+                                                                 int it, int colour) {
+  using namespace ad;
+  __shared__ float xs_s[kAdjThreads / 32][kRV];
+  __shared__ float ys_s[kAdjThreads / 32][kRestOut];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c0 = t.ctl->color_offset[colour], c1 = t.ctl->color_offset[colour + 1];
+  const int k = c0 + blockIdx.x * (kAdjThreads / 32) + warp;
+  if (k >= c1) return;
+  const CPlanes& P = t.planes;
+  const float e = P.mass[k].w;
+  if (!(e > 0.0f)) return;  // the forward update changed nothing (and recorded no inputs)
+  const int4 idx = P.idx[k];
+  const int ia = idx.x, ib = idx.y, cid = idx.z, cap = a.cap, n = a.n_awake;
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  const float4* rows = t.rest + (size_t)it * 6 * cap;
+  if (lane == 0) {
+    for (int r = 0; r < 4; ++r) {
+      float4 v = rows[(size_t)r * cap + k];
+      xs[3 * r] = v.x; xs[3 * r + 1] = v.y; xs[3 * r + 2] = v.z;
+      xs[rvLam + r] = v.w;
+    }
+    float4 tot = rows[4 * (size_t)cap + k], rest = rows[5 * (size_t)cap + k];
+    xs[rvTot] = tot.x; xs[rvTot + 1] = tot.y; xs[rvTot + 2] = tot.z; xs[rvTot + 3] = tot.w;
+    xs[rvRest] = rest.x; xs[rvRest + 1] = rest.y; xs[rvRest + 2] = rest.z; xs[rvRest + 3] = rest.w;
+    // the position deltas restitution sees: after the last substep's integrate positions
+    for (int side = 0; side < 2; ++side) {
+      int b = side == 0 ? ia : ib;
+      V3 dp = v3(0, 0, 0);
+      Q dq = qid();
+      if (b >= 0) {
+        const DState& st = t.body[((size_t)(t.substeps - 1) * 3 + 2) * n + b];
+        dp = st.dp;
+        dq = st.dq;
+      }
+      int at = side == 0 ? rvDpA : rvDpB, aq = side == 0 ? rvDqA : rvDqB;
+      xs[at] = dp.x; xs[at + 1] = dp.y; xs[at + 2] = dp.z;
+      xs[aq] = dq.v.x; xs[aq + 1] = dq.v.y; xs[aq + 2] = dq.v.z; xs[aq + 3] = dq.s;
+    }
+    float4 m = P.mass[k], a0 = P.ia0[k], a1 = P.ia1[k], b1 = P.ib1[k], nn = P.n[k];
+    xs[rvIma] = m.x; xs[rvImb] = m.y; xs[rvE] = m.w;
+    xs[rvSa] = a0.x; xs[rvSa + 1] = a0.y; xs[rvSa + 2] = a0.z; xs[rvSa + 3] = a0.w; xs[rvSa + 4] = a1.x;
+    xs[rvSa + 5] = a1.y;
+    xs[rvSb] = a1.z; xs[rvSb + 1] = a1.w; xs[rvSb + 2] = b1.x; xs[rvSb + 3] = b1.y; xs[rvSb + 4] = b1.z;
+    xs[rvSb + 5] = b1.w;
+    xs[rvN] = nn.x; xs[rvN + 1] = nn.y; xs[rvN + 2] = nn.z;
+    for (int q = 0; q < 4; ++q) {
+      float4 ra = P.pra[(size_t)q * cap + k], rbv = P.prb[(size_t)q * cap + k], im = P.pimp[(size_t)q * cap + k];
+      xs[rv_point(q, 0)] = ra.x; xs[rv_point(q, 1)] = ra.y; xs[rv_point(q, 2)] = ra.z; xs[rv_point(q, 6)] = ra.w;
+      xs[rv_point(q, 3)] = rbv.x; xs[rv_point(q, 4)] = rbv.y; xs[rv_point(q, 5)] = rbv.z; xs[rv_point(q, 7)] = rbv.w;
+      xs[rv_point(q, 8)] = im.w;
+      xs[rv_point(q, 9)] = 0.0f;
+    }
+  }
+  if (lane < 12) {
+    int b = lane < 6 ? ia : ib;
+    int g = lane % 6;
+    ys[lane] = b >= 0 ? BB(a, b, g < 3 ? g : g + 1) : 0.0f;
+  } else if (lane < 16) {
+    ys[lane] = KB(a, k, cvLam + lane - 12);
+  } else if (lane < 20) {
+    ys[lane] = TOTB(a, k, lane - 16);
+  } else if (lane < 24) {
+    ys[lane] = RESTB(a, k, lane - 20);
+  }
+  __syncwarp();
+  RParams rp = rp0;
+  rp.pc = idx.w & 255;
+  SeedIn<float, 3> in;
+  in.x = xs;
+  in.dir[0] = lane;
+  in.dir[1] = lane + 32;
+  in.dir[2] = lane + 64;
+  Dual<float, 3> y[kRestOut];
+  restitution_fn(in, rp, y);
+  float xb[3];
+  for (int kk = 0; kk < 3; ++kk) {
+    float acc = 0.0f;
+    for (int j = 0; j < kRestOut; ++j) acc += ys[j] * y[j].d[kk];
+    xb[kk] = acc;
+  }
+  __syncwarp();
+  for (int kk = 0; kk < 3; ++kk) {
+    const int d = in.dir[kk];
+    const float v = xb[kk];
+    if (d < 12) {
+      int b = d < 6 ? ia : ib;
+      int g = d % 6;
+      if (b >= 0) BB(a, b, g < 3 ? g : g + 1) = v;
+    } else if (d < rvDpB) {
+      if (ia >= 0) BB(a, ia, 8 + d - rvDpA) += v;
+    } else if (d < rvDqA) {
+      if (ib >= 0) BB(a, ib, 8 + d - rvDpB) += v;
+    } else if (d < rvDqB) {
+      if (ia >= 0) BB(a, ia, 12 + d - rvDqA) += v;
+    } else if (d < rvLam) {
+      if (ib >= 0) BB(a, ib, 12 + d - rvDqB) += v;
+    } else if (d < rvTot) {
+      KB(a, k, cvLam + d - rvLam) = v;
+    } else if (d < rvRest) {
+      TOTB(a, k, d - rvTot) = v;
+    } else if (d < rvIma) {
+      RESTB(a, k, d - rvRest) = v;
+    } else if (d == rvIma) {
+      KB(a, k, cvIma) += v;
+    } else if (d == rvImb) {
+      KB(a, k, cvImb) += v;
+    } else if (d < rvSb) {
+      KB(a, k, cvSa + d - rvSa) += v;
+    } else if (d < rvN) {
+      KB(a, k, cvSb + d - rvSb) += v;
+    } else if (d < rvE) {
+      KB(a, k, cvN + d - rvN) += v;
+    } else if (d == rvE) {
+      // e = max(e_a, e_b): the cotangent goes to the shape that supplied it
+      const DContact& c = t.post[cid];
+      float ea = w.shapes[c.shape_a].restitution, eb = w.shapes[c.shape_b].restitution;
+      int body = ea > eb ? ia : ib;
+      if (body >= 0 && v != 0.0f) atomicAdd(&PB(a, body, pbRestitution), v);
+    } else {
+      int q = (d - rvPoint) / 10, f = (d - rvPoint) % 10;
+      // anchors, base separation and normal mass share the constraint layout's point entries
+      if (f < 8) KB(a, k, cv_point(q, f)) += v;
+      else if (f == 8) RELB(a, k, q) += v;
+    }
+  }
+}
+
+// Reverse of the relative normal velocities prepare records for restitution (one thread per
+// slot; ad::relvel_vjp): runs after the reverse solve, when the bodies' velocity cotangents are
+// those of the step's start, whose velocities prepare read. The normal's and anchors' cotangents
+// go to the contact's manifold, the velocities' to the bodies (atomics: a body has slots in
+// every colour).
+__global__ void k_adj_relvel(StepTape t, AdjBufs a, int n_slots) {
+  using namespace ad;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_slots) return;
+  const int4 idx = t.planes.idx[k];
+  if (!(t.planes.mass[k].w > 0.0f)) return;  // prepare sampled no velocity
+  const int ia = idx.x, ib = idx.y, cid = idx.z, pc = idx.w & 255;
+  const Manifold& m = t.post[cid].manifold;
+  float x[kRL];
+  for (int f = 0; f < 12; ++f) x[f] = 0.0f;
+  if (ia >= 0) { const DState& s = t.body[ia]; put3(x, rlVA, s.v); put3(x, rlWA, s.w); }
+  if (ib >= 0) { const DState& s = t.body[ib]; put3(x, rlVB, s.v); put3(x, rlWB, s.w); }
+  put3(x, rlN, m.normal);
+  float acc[kRL];
+  for (int f = 0; f < 15; ++f) acc[f] = 0.0f;
+  for (int q = 0; q < pc; ++q) {
+    float g = RELB(a, k, q);
+    if (g == 0.0f) continue;
+    put3(x, rlRa, m.points[q].anchor_a);
+    put3(x, rlRb, m.points[q].anchor_b);
+    float xb[kRL];
+    for (int f = 0; f < kRL; ++f) xb[f] = 0.0f;
+    relvel_vjp(x, g, xb);
+    for (int f = 0; f < 15; ++f) acc[f] += xb[f];
+    for (int f = 0; f < 3; ++f) {
+      MB(a, cid, mb_point(q, f)) += xb[rlRa + f];
+      MB(a, cid, mb_point(q, 3 + f)) += xb[rlRb + f];
+    }
+  }
+  for (int f = 0; f < 3; ++f) {
+    MB(a, cid, mbN + f) += acc[rlN + f];
+    if (ia >= 0) { atomicAdd(&BB(a, ia, f), acc[rlVA + f]); atomicAdd(&BB(a, ia, 4 + f), acc[rlWA + f]); }
+    if (ib >= 0) { atomicAdd(&BB(a, ib, f), acc[rlVB + f]); atomicAdd(&BB(a, ib, 4 + f), acc[rlWB + f]); }
   }
 }
 
@@ -635,7 +829,7 @@ __global__ void k_adj_seed(AdjBufs a, const int* body_loc, int nb, const float* 
     for (int f = 0; f < 4; ++f) CQ(a, loc, 4 + f) = drot ? drot[4 * i + f] : 0.0f;
   }
 }
-// out per body id: lin 3 | ang 3 | mass | friction | pos 3 | rot 4  (16 floats)
+// out per body id: lin 3 | ang 3 | mass | friction | pos 3 | rot 4 | restitution  (16 floats)
 __global__ void k_adj_result(AdjBufs a, const DW w, const int* body_loc, int nb, float* out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
     float* o = out + (size_t)16 * i;
@@ -646,6 +840,7 @@ __global__ void k_adj_result(AdjBufs a, const DW w, const int* body_loc, int nb,
     }
     for (int f = 0; f < 3; ++f) { o[f] = BB(a, loc, f); o[3 + f] = BB(a, loc, 4 + f); o[8 + f] = CQ(a, loc, f); }
     for (int f = 0; f < 4; ++f) o[11 + f] = CQ(a, loc, 4 + f);
+    o[15] = PB(a, loc, pbRestitution);
     // inv_mass = 1/m and the local inverse inertia scale as 1/m
     const DSim& s = w.asims[loc];
     float im = s.inv_mass;
@@ -658,7 +853,6 @@ __global__ void k_adj_result(AdjBufs a, const DW w, const int* body_loc, int nb,
     for (int f = 0; f < 9; ++f) dot_i += PB(a, loc, pbInertia + f) * ii[f];
     o[6] = -PB(a, loc, pbInvMass) * im * im - dot_ii * im + dot_i * im;
     o[7] = PB(a, loc, pbFriction);
-    o[15] = 0.0f;
   }
 }
 

@@ -1101,7 +1101,29 @@ struct SolveTape {
   float4* push;    // [substep][4][cap]: vA|l0, wA|l1, vB|l2, wB|l3
   float4* relax;   // [substep][5][cap]: the same, then fr.x, fr.y, twist
   float4* fin;     // [cap]
+  float4* rest;    // [iteration][6][cap]: vA|l0, wA|l1, vB|l2, wB|l3, the points' total normal
+                   // impulses, their restitution impulses (before each restitution update)
 };
+
+__device__ __forceinline__ void tape_restitution(const DW& w, const SolveTape& tp, int it, int k, const CData& d) {
+  const int cap = w.cp.cap;
+  DState ba = state_at(w, d.c.ia), bb = state_at(w, d.c.ib);
+  float l[4], tot[4], rest[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    bool on = q < d.c.pc;
+    l[q] = on ? d.pimp[q].x : 0.0f;
+    tot[q] = on ? d.pimp[q].y : 0.0f;
+    rest[q] = on ? d.prest[q] : 0.0f;
+  }
+  float4* rows = tp.rest + (size_t)it * 6 * cap;
+  rows[k] = make_float4(ba.v.x, ba.v.y, ba.v.z, l[0]);
+  rows[(size_t)cap + k] = make_float4(ba.w.x, ba.w.y, ba.w.z, l[1]);
+  rows[2 * (size_t)cap + k] = make_float4(bb.v.x, bb.v.y, bb.v.z, l[2]);
+  rows[3 * (size_t)cap + k] = make_float4(bb.w.x, bb.w.y, bb.w.z, l[3]);
+  rows[4 * (size_t)cap + k] = make_float4(tot[0], tot[1], tot[2], tot[3]);
+  rows[5 * (size_t)cap + k] = make_float4(rest[0], rest[1], rest[2], rest[3]);
+}
 
 __device__ __forceinline__ void tape_contact(const DW& w, const SolveTape& tp, int sub, int stage, int k,
                                              const CData& d) {
@@ -1249,6 +1271,8 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
         CData d;
         load_direct(w.cp, k, stage, d, (!kGrid && t == t0) ? sidx[c * kSolveThreads + threadIdx.x] : __ldg(&w.cp.idx[k]));
         if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
+        if (kTape && stage == kRestitution && tp.rest && d.c.restitution > 0.0f)
+          tape_restitution(w, tp, (s - main_phases) / n_rph, k, d);
         run_contact(w, p, k, stage, d, warm_color);
       }
       for (int tj = g; stage != kRestitution && tj < nj; tj += stride) {

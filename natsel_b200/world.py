@@ -120,7 +120,7 @@ EXPORTED = [
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
     "ns_world_begin_subworld", "ns_world_subworld_count", "ns_world_subworld_bodies", "ns_world_subworld_hashes",
     "ns_world_tape_begin", "ns_world_tape_end", "ns_world_tape_free", "ns_world_tape_info", "ns_world_vjp",
-    "ns_world_vjp_f64", "ns_world_autotune", "ns_world_autotune_table", "ns_world_launch_shapes", "ns_world_set_launch_shapes",
+    "ns_world_vjp_f64", "ns_world_vjp_restitution", "ns_world_autotune", "ns_world_autotune_table", "ns_world_launch_shapes", "ns_world_set_launch_shapes",
     "ns_adjoint_selfcheck",
 ]
 
@@ -179,6 +179,7 @@ def load_library(path=LIB_PATH):
     lib.ns_world_tape_info.argtypes = [P, P]
     lib.ns_world_vjp.argtypes = [P] * 11
     lib.ns_world_vjp_f64.argtypes = [P] * 11
+    lib.ns_world_vjp_restitution.argtypes = [P, P]
     lib.ns_world_autotune.argtypes = [P, ctypes.c_float, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_int]
     lib.ns_adjoint_selfcheck.argtypes = [ctypes.c_int, ctypes.c_int, P]
     _lib = lib
@@ -436,8 +437,8 @@ class World:
     def vjp(self, dpos=None, drot=None, dlin=None, dang=None):
         """Pull cotangents of the final state (body id order) back to the tape's start.
 
-        Returns a dict of float32 arrays: lin0, ang0 (n x 3), mass, friction (n), pos0 (n x 3),
-        rot0 (n x 4)."""
+        Returns a dict of float32 arrays: lin0, ang0 (n x 3), mass, friction, restitution (n),
+        pos0 (n x 3), rot0 (n x 4)."""
         n = self.body_count
         def arr(a, w):
             if a is None:
@@ -453,6 +454,8 @@ class World:
         self._check(self._lib.ns_world_vjp(self._w, *[_ptr(a) for a in ins], _ptr(out["lin0"]), _ptr(out["ang0"]),
                                            _ptr(out["mass"]), _ptr(out["friction"]), _ptr(out["pos0"]),
                                            _ptr(out["rot0"])))
+        out["restitution"] = np.zeros(n, np.float32)
+        self._check(self._lib.ns_world_vjp_restitution(self._w, _ptr(out["restitution"])))
         return out
 
     def vjp_f64(self, dpos=None, drot=None, dlin=None, dang=None):
@@ -477,7 +480,8 @@ class World:
 ADJOINT_CHECKS = ["warm_start", "push", "relax", "prepare", "integrate_velocities", "integrate_positions",
                   "finalize_rotation", "inverse_inertia", "recycle", "box_face", "box_any", "box_edge",
                   "warm_start_reverse_sweep", "push_reverse_sweep", "relax_reverse_sweep",
-                  "integrate_positions_reverse_sweep", "integrate_velocities_reverse_sweep"]
+                  "integrate_positions_reverse_sweep", "integrate_velocities_reverse_sweep", "restitution",
+                  "relative_velocity_reverse_sweep"]
 
 
 def adjoint_selfcheck(which, seed):

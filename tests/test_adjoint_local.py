@@ -1,12 +1,12 @@
 """The adjoint's local derivatives, checked in f64 on the host (no GPU).
 
 The reverse stages of ns_world_vjp rest on a dual-number restatement of each forward function
-(warm start, push, relax, prepare, the body stages, recycled separations and box-box
-manifolds). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random inputs and
+(warm start, push, relax, prepare, the body stages, recycled separations, box-box
+manifolds and restitution). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random inputs and
 compares its vector-Jacobian product, direction by direction, with central differences of the
 same function; and it compares the hand-derived reverse sweeps the solver stages run on the
-GPU (warm start, push, relax, integrate positions and velocities) with the dual-number
-products, which they must reproduce to rounding.
+GPU (warm start, push, relax, integrate positions and velocities, the relative normal velocity
+restitution samples) with the dual-number products, which they must reproduce to rounding.
 """
 import pytest
 
@@ -40,3 +40,17 @@ def test_reverse_sweeps_match_dual_numbers(which):
     for seed in range(16):
         worst, _ = adjoint_selfcheck(which, seed)
         assert 0.0 <= worst < 1e-12, (ADJOINT_CHECKS[which], seed, worst)
+
+
+def test_restitution_vjp_matches_central_differences():
+    """The restitution update (contact_solver.rs:1135 apply_restitution_body) on one to four
+    points; even seeds arm every point's bounce (relative velocity below the threshold)."""
+    for seed in range(24):
+        worst, _ = adjoint_selfcheck(17, seed)
+        assert 0.0 <= worst < 1e-6, (seed, worst)
+
+
+def test_relative_velocity_reverse_sweep_matches_dual_numbers():
+    for seed in range(16):
+        worst, _ = adjoint_selfcheck(18, seed)
+        assert 0.0 <= worst < 1e-12, (seed, worst)

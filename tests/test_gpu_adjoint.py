@@ -2,7 +2,8 @@
 differences of the forward step, and the tape's bookkeeping.
 
 The scenes keep one contact set over the horizon (boxes sliding and spinning on the ground, a
-box running into a lighter one, a box sliding on another). Contact solves still have kinks (an
+box running into a lighter one, a box sliding on another, boxes bouncing off the ground and off
+each other with restitution). Contact solves still have kinks (an
 impulse meeting its clamp at zero, a corner point unloading); where one falls inside the
 difference interval the central difference does not converge, and below h ~ 1e-3 the f32
 rounding of the trajectory dominates it. So each entry is differenced at h and 2 h, and the
@@ -36,15 +37,26 @@ STACK = [
     ((0.0, 0.498, 0.0), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1000.0, 0.8),
     ((0.05, 1.394, 0.02), (0.4, 0.4, 0.4), (1.2, 0.0, 0.2), (0.0, 0.4, 0.0), 600.0, 0.4),
 ]
+# an optional seventh field is the shape's restitution. Boxes 5 mm above the ground land in the
+# first step faster than the restitution threshold and bounce (contact_solver.rs:1135
+# apply_restitution_body); then a box running into another, both with restitution
+BOUNCE = [
+    ((0.0, 0.505, 0.0), (0.5, 0.5, 0.5), (1.0, -3.0, 0.3), (0.0, 0.3, 0.0), 1000.0, 0.5, 0.5),
+    ((3.0, 0.405, 1.0), (0.4, 0.4, 0.4), (-0.5, -2.5, 0.0), (0.0, 0.0, 0.2), 700.0, 0.6, 0.8),
+]
+COLLIDE_BOUNCE = [
+    ((-1.2, 0.498, 0.0), (0.5, 0.5, 0.5), (3.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1000.0, 0.5, 0.6),
+    ((0.0, 0.398, 0.05), (0.4, 0.4, 0.4), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 500.0, 0.5, 0.3),
+]
 
 
 def build(bodies, checkpoint=None, ground_friction=0.6):
     w = World(**WORLD)
     g = w.create_body(type=STATIC_BODY, position=(0.0, -0.5, 0.0))
     w.create_box(g, 20.0, 0.5, 20.0, friction=ground_friction)
-    for pos, he, v, om, rho, mu in bodies:
+    for pos, he, v, om, rho, mu, *rest in bodies:
         b = w.create_body(type=DYNAMIC_BODY, position=pos, linear_velocity=v, angular_velocity=om, enable_sleep=False)
-        w.create_box(b, *he, density=rho, friction=mu)
+        w.create_box(b, *he, density=rho, friction=mu, restitution=rest[0] if rest else 0.0)
     if checkpoint is not None:
         w.tape_begin(checkpoint)
     return w
@@ -104,11 +116,13 @@ def check(bodies, ground_friction=0.6):
     assert info[2] == 0, "narrowphase replay did not reproduce a recorded manifold"
     assert h0 == h1, "the adjoint must leave the world in its final state"
     rows = []  # kind, adjoint, fd(h), fd(2 h)
-    for i, (pos, he, v, om, rho, mu) in enumerate(bodies):
+    for i, (pos, he, v, om, rho, mu, *rest) in enumerate(bodies):
         vol = 8.0 * he[0] * he[1] * he[2]
         entries = [("velocity", g["lin0"][i + 1, c], 2, c, 1e-3) for c in range(3)]
         entries += [("velocity", g["ang0"][i + 1, c], 3, c, 1e-3) for c in range(3)]
         entries += [("mass", g["mass"][i + 1] * vol, 4, 0, 1e-3 * rho), ("friction", g["friction"][i + 1], 5, 0, 1e-3)]
+        if rest:
+            entries.append(("restitution", g["restitution"][i + 1], 6, 0, 1e-3))
         for kind, a, field, c, h in entries:
             rows.append((kind, float(a), fd(bodies, i, field, c, h, ground_friction),
                          fd(bodies, i, field, c, 2 * h, ground_friction)))
@@ -147,6 +161,24 @@ def test_colliding_boxes_gradients_match_finite_differences():
 def test_box_on_box_gradients_match_finite_differences():
     rows, checked = check(STACK)
     assert checked_count(checked, "velocity") >= 2
+
+
+def test_bouncing_boxes_gradients_match_finite_differences():
+    rows, checked = check(BOUNCE)
+    assert checked_count(checked, "restitution") >= 2
+    assert checked_count(checked, "velocity") >= 4
+    # the bounce is what the restitution gradient measures: both boxes rise after landing
+    w = build(BOUNCE)
+    for _ in range(2):
+        w.step(DT, SUBSTEPS)
+    assert (w.bodies()[2][1:, 1] > 0.5).all()
+    w.close()
+
+
+def test_colliding_bouncing_boxes_gradients_match_finite_differences():
+    rows, checked = check(COLLIDE_BOUNCE, ground_friction=0.05)
+    assert checked_count(checked, "velocity") >= 2
+    assert checked_count(checked, "restitution") >= 1
 
 
 def test_spinning_box_rotation_gradient_matches_finite_differences():
@@ -235,6 +267,13 @@ def test_adjoint_scope_is_enforced():
         w.apply_forces(force=np.zeros((4, 3), np.float32))
     with pytest.raises(NsError):
         w.step(0.0, SUBSTEPS)
+    w.close()
+    # restitution has an f32 device reverse only
+    w = build(BOUNCE, checkpoint=8)
+    w.step(DT, SUBSTEPS)
+    with pytest.raises(NsError) as e:
+        w.vjp_f64(dpos=np.ones((3, 3), np.float32))
+    assert e.value.code == 6 and "restitution" in str(e.value)
     w.close()
 
 
