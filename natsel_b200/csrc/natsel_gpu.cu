@@ -625,10 +625,6 @@ int upload_world(ns_world* w) {
   // the kernel's static shared memory counts against the same 48 KB default, so the limit is
   // always raised to what this launch needs
   NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
-  // the cluster solver stages its index planes in dynamic shared memory (any shape may be chosen
-  // later by the autotuner, so the attribute is set for every world)
-  NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveIdxBytes));
-  NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveIdxBytes));
   // solver launch shape. solver_blocks 0: one cluster of the largest size that fits (16 CTAs on
   // B200) for a single world, a cooperative grid over every SM for a batch of sub-worlds; 1..16: one thread-block cluster of that many CTAs (non-portable sizes above 8); above
   // 16: a cooperative grid of that many blocks, capped at what fits co-resident. On the
@@ -645,7 +641,6 @@ int upload_world(ns_world* w) {
       for (int cs = want; cs >= 1; --cs) {
         cudaLaunchConfig_t cfg = {};
         cfg.blockDim = dim3(kSolveThreads);
-        cfg.dynamicSmemBytes = kSolveIdxBytes;  // the cluster solver's staged index planes
         cfg.gridDim = dim3(cs);
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -825,7 +820,6 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(w->solver_blocks);
     cfg.blockDim = dim3(kSolveThreads);
-    cfg.dynamicSmemBytes = kSolveIdxBytes;  // the cluster solver's staged index planes
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     if (d.n_awake > 0) {
@@ -836,7 +830,6 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
       NS_CUDA(w, cudaMemsetAsync(&d.ctl->barrier_count, 0, sizeof(int), s));
       attr[0].id = cudaLaunchAttributeCooperative;
       attr[0].val.cooperative = 1;
-      cfg.dynamicSmemBytes = 0;
     } else {
       attr[0].id = cudaLaunchAttributeClusterDimension;
       attr[0].val.clusterDim.x = w->solver_blocks;
@@ -2333,7 +2326,6 @@ static int autotune(ns_world* w, float dt, int substeps, int steps, int* blocks_
     if (!w->solver_grid) {
       cudaLaunchConfig_t cfg = {};
       cfg.blockDim = dim3(kSolveThreads);
-      cfg.dynamicSmemBytes = kSolveIdxBytes;  // the cluster solver's staged index planes
       cfg.gridDim = dim3(w->solver_blocks);
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -2459,7 +2451,6 @@ int ns_world_set_launch_shapes(ns_world* w, const int* in8) {
     NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(kSolveThreads);
-    cfg.dynamicSmemBytes = kSolveIdxBytes;  // the cluster solver's staged index planes
     cfg.gridDim = dim3(blocks_);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

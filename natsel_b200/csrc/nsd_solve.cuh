@@ -218,12 +218,10 @@ struct CData {
 };
 
 // Every field is written (zero where the stage reads nothing). Only the manifold's points are
-// read: the cluster's 16 SMs move every phase's constraints from L2, so bytes count. The index
-// plane (bodies and point count) may come from the caller (the solver keeps it in shared
-// memory), so the body-state and point loads need not wait for an L2 round trip.
-__device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d, int4 idx) {
+// read: the cluster's 16 SMs move every phase's constraints from L2, so bytes count.
+__device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d) {
   const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  d.c = unpack_constraint(idx, __ldg(&P.mass[k]), __ldg(&P.ia0[k]), __ldg(&P.ia1[k]),
+  d.c = unpack_constraint(__ldg(&P.idx[k]), __ldg(&P.mass[k]), __ldg(&P.ia0[k]), __ldg(&P.ia1[k]),
                           __ldg(&P.ib1[k]), __ldg(&P.n[k]));
   d.t1 = z; d.t2 = z; d.ca = z; d.cb = z; d.fr = z; d.roll = z; d.rm = z; d.tm = z;
   if (stage == kWarm || stage == kRelax) {
@@ -241,10 +239,6 @@ __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, 
       if (stage == kRestitution) d.prest[q] = P.prest[q * P.cap + k];
     }
   }
-}
-
-__device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, CData& d) {
-  load_direct(P, k, stage, d, __ldg(&P.idx[k]));
 }
 
 // Change of the two bodies' velocities by one warm start: body a gets v - dva, w - dwa and
@@ -1144,16 +1138,8 @@ __device__ __forceinline__ void tape_contact(const DW& w, const SolveTape& tp, i
 // grid_sync_acq_rel, compiled for two blocks per SM (128 registers; the batch's colours hold
 // more items than one block per SM has threads); otherwise one thread-block cluster separated
 // by barrier.cluster.
-// The cluster launch (kGrid false) stages, for each colour, the index plane of the first
-// constraint each thread owns in shared memory before the first phase (kSolveIdxBytes of dynamic
-// shared memory; the plane is written by prepare and only read here), so a colour phase starts
-// its body-state loads from shared memory; further constraints of a thread in one colour read the
-// plane from global memory.
-constexpr size_t kSolveIdxBytes = (size_t)kOverflowIndex * kSolveThreads * sizeof(int4);
-
 template <bool kGrid, bool kTape>
 __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, StepParams p, JointRanges jr, SolveTape tp) {
-  extern __shared__ int4 sidx[];  // [colour][thread], cluster launch only
   __shared__ int coff[25];
   __shared__ int phases[3 * 25 + 2];  // one substep
   __shared__ int rphases[25];         // one restitution iteration
@@ -1204,18 +1190,6 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
   // a colour with fewer items than the launch has threads occupies every SM with a few warps
   // instead of filling the first blocks, and a phase's time follows the warps per SM.
   const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
-  // the first contact item of this thread in colour c (items below nj are the colour's joints)
-  auto first_item = [&](int c) {
-    const int nj = jr.off[c + 1] - jr.off[c];
-    return g >= nj ? g : g + ((nj - g + stride - 1) / stride) * stride;
-  };
-  if (!kGrid) {
-    for (int c = 0; c < kOverflowIndex; ++c) {
-      const int nj = jr.off[c + 1] - jr.off[c], total = nj + (coff[c + 1] - coff[c]);
-      const int t0 = first_item(c);
-      sidx[c * kSolveThreads + threadIdx.x] = t0 < total ? __ldg(&w.cp.idx[coff[c] + (t0 - nj)]) : make_int4(0, 0, 0, 0);
-    }
-  }
   int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
@@ -1265,11 +1239,10 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
       // The colour's contacts, then its joints: no two items of one colour share a dynamic
       // body, so their order does not change any result. Each thread keeps its items of the
       // colour (t = g, g + stride, ...).
-      const int t0 = first_item(c);
-      for (int t = t0; t < total; t += stride) {
+      for (int t = g >= nj ? g : g + ((nj - g + stride - 1) / stride) * stride; t < total; t += stride) {
         int k = coff[c] + (t - nj);
         CData d;
-        load_direct(w.cp, k, stage, d, (!kGrid && t == t0) ? sidx[c * kSolveThreads + threadIdx.x] : __ldg(&w.cp.idx[k]));
+        load_direct(w.cp, k, stage, d);
         if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
         if (kTape && stage == kRestitution && tp.rest && d.c.restitution > 0.0f)
           tape_restitution(w, tp, (s - main_phases) / n_rph, k, d);
