@@ -41,7 +41,8 @@ typedef struct {
   float gravity[3];            /* (0,-10,0) */
   int enable_sleep;            /* must be 0: sleeping islands are outside this path */
   int enable_continuous;       /* 1: fast dynamic bodies are swept against static shapes after
-                                  finalize and moved back to the time of impact (continuous.rs:337) */
+                                  finalize and moved back to the time of impact (continuous.rs:337);
+                                  fast bullets then against dynamic bodies too */
   int enable_warm_starting;    /* 1 */
   float contact_hertz;         /* 30 */
   float contact_damping_ratio; /* 10 */
@@ -68,6 +69,7 @@ typedef struct {
   float angular_velocity[3];
   float linear_damping, angular_damping, gravity_scale;
   int enable_sleep;            /* stored as a body flag; sleeping itself is not simulated */
+  int is_bullet;               /* body_def.rs:74: when fast, swept against dynamic bodies too */
 } ns_body_def;
 
 /* Shape definition (types/shape_def.rs ShapeDef with one surface material). */

@@ -61,6 +61,7 @@ pub struct ns_body_def {
     pub angular_damping: f32,
     pub gravity_scale: f32,
     pub enable_sleep: c_int,
+    pub is_bullet: c_int,
 }
 
 #[repr(C)]

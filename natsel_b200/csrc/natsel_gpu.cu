@@ -76,6 +76,7 @@ struct ns_world {
   std::vector<size_t> allocation_bytes;
   struct AdTape* tape = nullptr;   // rollout record for the adjoint (ns_world_tape_begin)
   std::vector<float> vjp_restitution;  // the last f32 VJP's restitution cotangents, body id order
+  int n_bullets = 0;                   // dynamic bodies created as bullets
   // Device buffers kept for reuse by later tapes and VJPs and freed with the world: checkpoint
   // buffers (with their copy tables, valid for the world's allocation set, which is fixed once
   // uploaded), the VJP's step tapes and its cotangent buffers.
@@ -386,7 +387,7 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_solve<false, true>,
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter, (const void*)k_prepare_slots,
                            (const void*)k_warm_slots,
-                           (const void*)k_finalize, (const void*)k_continuous, (const void*)k_state_pass,
+                           (const void*)k_finalize, (const void*)k_continuous, (const void*)k_bullets, (const void*)k_state_pass,
                            (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
                            (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
   for (const void* k : kernels) {
@@ -479,6 +480,17 @@ int upload_world(ns_world* w) {
     for (int i = 0; i < nsh; ++i)
       if (dshapes[i].is_static) static_list[cursor[dshapes[i].world]++] = i;
   }
+  // shapes of dynamic bodies per sub-world in shape order, for the bullets' continuous pass
+  std::vector<int> dyn_list, dyn_off(n_worlds + 1, 0);
+  for (int i = 0; i < nsh; ++i)
+    if (w->bodies[dshapes[i].body].type == NS_DYNAMIC_BODY) dyn_off[dshapes[i].world + 1]++;
+  for (int k = 0; k < n_worlds; ++k) dyn_off[k + 1] += dyn_off[k];
+  {
+    std::vector<int> cursor(dyn_off.begin(), dyn_off.end() - 1);
+    dyn_list.resize(dyn_off[n_worlds]);
+    for (int i = 0; i < nsh; ++i)
+      if (w->bodies[dshapes[i].body].type == NS_DYNAMIC_BODY) dyn_list[cursor[dshapes[i].world]++] = i;
+  }
   // the sweep of a body starts at its pose at upload (body_api.rs:221, :533 center0/rotation0)
   for (DSim& s : w->asims) { s.cx0 = s.cx; s.cy0 = s.cy; s.cz0 = s.cz; s.q0 = s.q; }
   for (DSim& s : w->ssims) { s.cx0 = s.cx; s.cy0 = s.cy; s.cz0 = s.cz; s.q0 = s.q; }
@@ -550,7 +562,9 @@ int upload_world(ns_world* w) {
   ALLOC(pool_top, int, n_worlds); ALLOC(pool_next, int, n_worlds); ALLOC(ovf_count, int, n_worlds);
   ALLOC(large_off, int, n_worlds + 1);
   ALLOC(large_list, int, large.size());
-  ALLOC(fast_list, int, std::max(na, 1)); ALLOC(static_off, int, n_worlds + 1);
+  ALLOC(fast_list, int, std::max(na, 1)); ALLOC(bullet_list, int, std::max(na, 1));
+  ALLOC(dyn_off, int, n_worlds + 1); ALLOC(dyn_list, int, std::max<size_t>(dyn_list.size(), 1));
+  ALLOC(static_off, int, n_worlds + 1);
   ALLOC(static_list, int, std::max<size_t>(static_list.size(), 1)); ALLOC(saabb, AABB, nsh);
   ALLOC(seg_count, int, nsh); ALLOC(seg_off, int, nsh); ALLOC(seg_cursor, int, nsh);
   ALLOC(cand, unsigned long long, cap); ALLOC(sorted_keys, unsigned long long, cap);
@@ -585,6 +599,8 @@ int upload_world(ns_world* w) {
   if ((st = upload(w, d.large_off, large_off))) return st;
   if ((st = upload(w, d.static_off, static_off))) return st;
   if ((st = upload(w, d.static_list, static_list))) return st;
+  if ((st = upload(w, d.dyn_off, dyn_off))) return st;
+  if ((st = upload(w, d.dyn_list, dyn_list))) return st;
   if ((st = upload(w, d.saabb, w->saabb))) return st;
   {
     std::vector<int> zeros(n_worlds, 0);
@@ -849,11 +865,13 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[4], s, ev_flags));
   // finalize (solver_integration.rs:435)
-  if (w->def.enable_continuous) NS_CUDA(w, cudaMemsetAsync(&d.ctl->fast_count, 0, sizeof(int), s));
+  if (w->def.enable_continuous) NS_CUDA(w, cudaMemsetAsync(&d.ctl->fast_count, 0, 2 * sizeof(int), s));
   k_finalize<<<blocks(d.n_awake, 128), 128, 0, s>>>(d, p); ++nk;
   if (w->def.enable_continuous) {
     // continuous.rs:337 for the fast bodies finalize queued (solver_integration.rs:540-566)
     k_continuous<<<blocks(d.n_awake, 64), 64, 0, s>>>(d, p); ++nk;
+    // then the fast bullets, one warp each, after every other body is final (:949-958)
+    if (w->n_bullets > 0) { k_bullets<<<blocks(32 * w->n_bullets, 128), 128, 0, s>>>(d, p); ++nk; }
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[5], s, ev_flags));
   NS_CUDA(w, cudaGetLastError());
@@ -1673,8 +1691,10 @@ int ns_create_body(ns_world* w, const ns_body_def* d) {
   s.flags = 0;
   if (d->type == NS_DYNAMIC_BODY) s.flags |= kDynamicFlag;
   if (d->enable_sleep) s.flags |= kEnableSleepFlag;
+  if (d->is_bullet) s.flags |= kIsBullet;  // world_runtime.rs:1570
   s.flags |= kEnableRecycling;
   b.flags = s.flags;
+  if (d->is_bullet && d->type == NS_DYNAMIC_BODY) ++w->n_bullets;
   if (b.set == 2) {
     b.local = (int)w->asims.size();
     w->asims.push_back(s);

@@ -105,6 +105,7 @@ struct DW {
   // shape's last bounds (shape.aabb in the reference: the speculative-inflated box finalize
   // computes, or the swept end box of the continuous pass).
   int* fast_list; int* static_list; int* static_off; AABB* saabb;
+  int* bullet_list; int* dyn_list; int* dyn_off;  // fast bullets; dynamic bodies' shapes per sub-world
 };
 
 struct JointRanges { int off[25]; };

@@ -1320,8 +1320,10 @@ __global__ void k_finalize(DW w, StepParams p) {
   if (finite && p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
     sim.flags |= kIsFast;
     add_converged(&w.ctl->fast_flags);
-    // the continuous pass (k_continuous) sweeps it from (cx0, q0) and updates its bounds
-    w.fast_list[atomicAdd(&w.ctl->fast_count, 1)] = i;
+    // the continuous pass (k_continuous, or k_bullets for a bullet) sweeps it from (cx0, q0)
+    // and updates its bounds
+    if (sim.flags & kIsBullet) w.bullet_list[atomicAdd(&w.ctl->bullet_count, 1)] = i;
+    else w.fast_list[atomicAdd(&w.ctl->fast_count, 1)] = i;
   } else {
     sim.cx0 = sim.cx; sim.cy0 = sim.cy; sim.cz0 = sim.cz;
     sim.q0 = sim.q;
@@ -1385,10 +1387,26 @@ __device__ __forceinline__ Sweep sweep_of(const DSim& s, Pos base) {
 
 // continuous.rs:337 solve_continuous for one fast (non-bullet) body: each of its shapes that
 // is fast on its own (continuous.rs:124) is swept against the static shapes of its sub-world
-// whose fat bounds overlap the shape's swept box; the earliest hit moves the body back along
-// its sweep. Only the earliest fraction matters, so the order the static shapes are visited in
-// does not change the result, and fast bodies are independent of one another (they only read
-// static bodies), so one thread per fast body gives the reference's serial pass.
+// whose fat bounds overlap the shape's swept box, in shape order; the earliest hit moves the
+// body back along its sweep. Each time of impact is bounded by the best fraction so far, so with
+// two hits the visiting order can change the last bits (the reference walks its static tree).
+// Fast bodies are independent of one another (they only read static bodies), so one thread per
+// fast body gives the reference's serial pass.
+__device__ void continuous_finish(const DW& w, const StepParams& p, int i, DSim sim, DState st, const Sweep& sweep,
+                                  Pos base, float fraction);
+
+// continuous.rs:262-299: the time of impact of a fast shape (proxy fp on sweep) against shape
+// sid on its own sweep, bounded by the best fraction so far; returns the new best fraction.
+__device__ float candidate_fraction(const DW& w, int sid, const Proxy& fp, const Sweep& sweep, Pos base,
+                                    float fraction) {
+  const DShape& ss = w.shapes[sid];
+  Proxy sp;
+  V3 unused;
+  shape_proxy(w, ss, &sp, &unused);
+  ToiResult r = time_of_impact(sp, fp, sweep_of(sim_of(w, ss.enc), base), sweep, fraction);
+  return (0.0f < r.fraction && r.fraction < fraction) ? r.fraction : fraction;
+}
+
 __device__ void continuous_body(const DW& w, const StepParams& p, int i) {
   DSim sim = w.asims[i];
   DState st = w.states[i];
@@ -1430,14 +1448,16 @@ __device__ void continuous_body(const DW& w, const StepParams& p, int i) {
     for (int t = s0; t < s1; ++t) {
       const int sid = w.static_list[t];
       if (!aabb_overlaps(w.fat[sid], swept) || !should_create_pair(w, sid, fid)) continue;
-      const DShape& ss = w.shapes[sid];
-      Proxy sp;
-      V3 unused;
-      shape_proxy(w, ss, &sp, &unused);
-      ToiResult r = time_of_impact(sp, fp, sweep_of(sim_of(w, ss.enc), base), sweep, fraction);
-      if (0.0f < r.fraction && r.fraction < fraction) fraction = r.fraction;
+      fraction = candidate_fraction(w, sid, fp, sweep, base, fraction);
     }
   }
+  continuous_finish(w, p, i, sim, st, sweep, base, fraction);
+}
+
+// The end of solve_continuous for body i with its earliest fraction (continuous.rs:452-590):
+// moved back to the time of impact with the lost gravity, or kept, and its bounds refreshed.
+__device__ void continuous_finish(const DW& w, const StepParams& p, int i, DSim sim, DState st, const Sweep& sweep,
+                                  Pos base, float fraction) {
   const float spec = speculative_distance();
   if (fraction < 1.0f) {
     // move the body back to the time of impact (continuous.rs:452-470)
@@ -1496,6 +1516,60 @@ __global__ void __launch_bounds__(64) k_continuous(DW w, StepParams p) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= w.ctl->fast_count) return;
   continuous_body(w, p, w.fast_list[t]);
+}
+
+// solver_integration.rs:949-958, continuous.rs:337 for one fast bullet, one warp each, after
+// k_continuous (every other body is final). Every shape of the bullet (no per-shape speed test)
+// is swept against its sub-world's static shapes, then against the shapes of its dynamic
+// non-bullet bodies at their final poses (continuous.rs:429-448: the reference also walks its
+// dynamic tree for bullets; bullets skip bullets, continuous.rs:253), each list in shape order.
+// The lanes test 32 candidates' bounds and filters at once; lane 0 runs the times of impact in
+// list order, each bounded by the best fraction so far, and finishes the body. Bullets read
+// only non-bullet bodies, which no warp here writes, so they are independent of one another.
+__global__ void __launch_bounds__(128) k_bullets(DW w, StepParams p) {
+  const int q = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
+  if (q >= w.ctl->bullet_count) return;  // the whole warp leaves together
+  const int i = w.bullet_list[q];
+  const DSim sim = w.asims[i];
+  const Pos base = {sim.cx0, sim.cy0, sim.cz0};
+  const Sweep sweep = sweep_of(sim, base);
+  const Xf xf2 = xf(sweep.c2 - rotate(sweep.q2, sweep.local_center), sweep.q2);
+  float fraction = 1.0f;  // lane 0's
+  for (int k = sim.shape_begin; k < sim.shape_end; ++k) {
+    const int fid = w.body_shapes[k];
+    const DShape& fs = w.shapes[fid];
+    Proxy fp;
+    V3 lc;
+    shape_proxy(w, fs, &fp, &lc);
+    const AABB box1 = w.saabb[fid];
+    const AABB box2 = offset_aabb(shape_box(w, fs, xf2), base);
+    __syncwarp();
+    if (lane == 0) w.saabb[fid] = box2;
+    const AABB swept = aabb(min3(box1.lo, box2.lo), max3(box1.hi, box2.hi));
+    for (int pass = 0; pass < 2; ++pass) {
+      const int* list = pass == 0 ? w.static_list : w.dyn_list;
+      const int* off = pass == 0 ? w.static_off : w.dyn_off;
+      const int t0 = off[fs.world], t1 = off[fs.world + 1];
+      for (int tb = t0; tb < t1; tb += 32) {
+        const int t = tb + lane;
+        int sid = -1;
+        bool hit = false;
+        if (t < t1) {
+          sid = list[t];
+          hit = aabb_overlaps(w.fat[sid], swept) && should_create_pair(w, sid, fid) &&
+                (pass == 0 || (sim_of(w, w.shapes[sid].enc).flags & kIsBullet) == 0);
+        }
+        unsigned m = __ballot_sync(0xffffffffu, hit);
+        while (m) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          const int cs = __shfl_sync(0xffffffffu, sid, src);
+          if (lane == 0) fraction = candidate_fraction(w, cs, fp, sweep, base, fraction);
+        }
+      }
+    }
+  }
+  if (lane == 0) continuous_finish(w, p, i, sim, w.states[i], sweep, base, fraction);
 }
 
 }  // namespace nsd

@@ -248,6 +248,7 @@ struct Control {
   int collide_count[6];   // contacts per pair kind queued for a full manifold update
   int long_segments;      // candidate segments handed to the block sort this pair update
   int fast_count;         // fast bodies queued by finalize for the continuous pass (this step)
+  int bullet_count;       // fast bullets queued by finalize for the bullet pass (this step)
 };
 
 }  // namespace nsd

@@ -36,6 +36,7 @@ typedef struct {
   float angular_velocity[3];
   float linear_damping, angular_damping, gravity_scale;
   int enable_sleep;
+  int is_bullet;
 } nso_body_def;
 
 typedef struct {

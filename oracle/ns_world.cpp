@@ -1699,8 +1699,10 @@ void solve_stages(nso_world* w) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Continuous collision of fast (non-bullet) bodies against static shapes: continuous.rs:337
-// solve_continuous, run in body order after finalize (solver_integration.rs:540-566).
+// Continuous collision: continuous.rs:337 solve_continuous. Fast non-bullet bodies sweep their
+// fast shapes against static shapes, in body order after finalize (solver_integration.rs:
+// 540-566); then fast bullets sweep all their shapes against static shapes and the shapes of
+// non-bullet dynamic bodies at their final poses, in body order (solver_integration.rs:949-958).
 
 // shape_runtime.rs:434 get_shape_centroid
 V3 shape_centroid(const Shape& s) {
@@ -1782,10 +1784,25 @@ bool shapes_collide(const Shape& a, const Shape& b) {
   return (a.mask & b.category) != 0 && (a.category & b.mask) != 0;
 }
 
+// continuous.rs:210-302 continuous_query_callback: the filters, then the time of impact of the
+// fast shape against one candidate at its own sweep, the best fraction so far as the bound
+void continuous_candidate(nso_world* w, const Shape& fs, const Proxy& fp, const Sweep& sweep, Pos base,
+                          int sid, real& fraction) {
+  const Shape& ss = w->shapes[sid];
+  if (ss.body_id == fs.body_id || !shapes_collide(fs, ss)) return;
+  const Body& other = w->bodies[ss.body_id];
+  if (sim_of(w, other).flags & kIsBullet) return;
+  if (!bodies_collide(w, fs.body_id, ss.body_id)) return;
+  Proxy sp = shape_proxy(ss);
+  ToiOut o = time_of_impact(sp, fp, relative_sweep(sim_of(w, other), base), sweep, fraction);
+  if (0.0f < o.fraction && o.fraction < fraction) fraction = o.fraction;
+}
+
 void solve_continuous(nso_world* w, int i) {
   BodySim& sim = w->awake_sims[i];
   BodyState& st = w->awake_states[i];
   Body& body = w->bodies[sim.body_id];
+  const bool bullet = (sim.flags & kIsBullet) != 0;
   Pos base = sim.center0;
   Sweep sweep = relative_sweep(sim, base);
   Xf xf1 = xf(sweep.c1 - rotate(sweep.q1, sweep.local_center), sweep.q1);
@@ -1799,20 +1816,20 @@ void solve_continuous(nso_world* w, int i) {
     AABB box1 = fs.aabb;
     AABB box2 = offset_aabb(shape_aabb_xf(fs, xf2), base);
     fs.aabb = box2;
-    if (!is_shape_fast(fs, centroid1, centroid2, rotation_chord, body.safety_factor)) continue;
+    if (!bullet && !is_shape_fast(fs, centroid1, centroid2, rotation_chord, body.safety_factor)) continue;
     AABB swept = aabb(min3(box1.lo, box2.lo), max3(box1.hi, box2.hi));
     Proxy fp = shape_proxy(fs);
-    // the static tree's proxies whose fat bounds overlap the swept box; only the earliest hit
-    // matters, so the visiting order does not change the result
-    for (int sid = 0; sid < (int)w->shapes.size(); ++sid) {
-      const Shape& ss = w->shapes[sid];
-      if (!ss.is_static || !aabb_overlaps(w->fat[sid], swept)) continue;
-      if (ss.body_id == fs.body_id || !shapes_collide(fs, ss) || !bodies_collide(w, sim.body_id, ss.body_id)) continue;
-      const BodySim& ssim = sim_of(w, w->bodies[ss.body_id]);
-      Proxy sp = shape_proxy(ss);
-      ToiOut o = time_of_impact(sp, fp, relative_sweep(ssim, base), sweep, fraction);
-      if (0.0f < o.fraction && o.fraction < fraction) fraction = o.fraction;
-    }
+    // the static tree's proxies whose fat bounds overlap the swept box, in shape order (the
+    // reference walks its tree; each time of impact is bounded by the best fraction so far)
+    for (int sid = 0; sid < (int)w->shapes.size(); ++sid)
+      if (w->shapes[sid].is_static && aabb_overlaps(w->fat[sid], swept))
+        continuous_candidate(w, fs, fp, sweep, base, sid, fraction);
+    // bullets also query the dynamic tree (continuous.rs:429-448)
+    if (bullet)
+      for (int sid = 0; sid < (int)w->shapes.size(); ++sid)
+        if (!w->shapes[sid].is_static && w->bodies[w->shapes[sid].body_id].type == 2 &&
+            aabb_overlaps(w->fat[sid], swept))
+          continuous_candidate(w, fs, fp, sweep, base, sid, fraction);
   }
   real spec = speculative_distance();
   if (fraction < 1.0f) {
@@ -1914,7 +1931,10 @@ void finalize(nso_world* w) {
     }
   }
   for (int i = 0; i < n_; ++i)
-    if (w->awake_sims[i].flags & kIsFast) solve_continuous(w, i);
+    if ((w->awake_sims[i].flags & (kIsFast | kIsBullet)) == kIsFast) solve_continuous(w, i);
+  // solver_integration.rs:949-958: the bullets, after every other body is final
+  for (int i = 0; i < n_; ++i)
+    if ((w->awake_sims[i].flags & (kIsFast | kIsBullet)) == (kIsFast | kIsBullet)) solve_continuous(w, i);
 }
 
 }  // namespace
@@ -1974,6 +1994,7 @@ int nso_create_body(nso_world* w, const nso_body_def* d) {
   s.flags = 0;
   if (d->type == 2) s.flags |= kDynamicFlag;
   if (d->enable_sleep) s.flags |= kEnableSleepFlag;
+  if (d->is_bullet) s.flags |= kIsBullet;  // world_runtime.rs:1570
   s.flags |= kEnableRecycling;
   if (b.set_index == 2) {
     b.local_index = (int)w->awake_sims.size();

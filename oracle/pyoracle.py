@@ -62,6 +62,7 @@ class BodyDef(ctypes.Structure):
         ("angular_damping", ctypes.c_float),
         ("gravity_scale", ctypes.c_float),
         ("enable_sleep", ctypes.c_int),
+        ("is_bullet", ctypes.c_int),
     ]
 
 
@@ -241,7 +242,8 @@ class OracleWorld:
 
     def create_body(self, type=DYNAMIC_BODY, position=(0.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0, 1.0),
                     linear_velocity=(0.0, 0.0, 0.0), angular_velocity=(0.0, 0.0, 0.0),
-                    linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, enable_sleep=True):
+                    linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, enable_sleep=True,
+                    is_bullet=False):
         b = BodyDef()
         b.type = type
         b.position = (ctypes.c_double * 3)(*position)
@@ -250,6 +252,7 @@ class OracleWorld:
         b.angular_velocity = (ctypes.c_float * 3)(*angular_velocity)
         b.linear_damping, b.angular_damping, b.gravity_scale = linear_damping, angular_damping, gravity_scale
         b.enable_sleep = 1 if enable_sleep else 0
+        b.is_bullet = 1 if is_bullet else 0
         self.body_types.append(type)
         return self._lib.nso_create_body(self._w, ctypes.byref(b))
 

@@ -45,7 +45,7 @@ def test_library_is_built_for_sm100a():
 
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(nw.WorldDef) == 4 * 3 + 4 * 3 + 4 * 5 + 4 + 4 * 2 + 4 * 3
-    assert ctypes.sizeof(nw.BodyDef) == 8 + 24 + 16 + 12 + 12 + 12 + 4
+    assert ctypes.sizeof(nw.BodyDef) == 8 + 24 + 16 + 12 + 12 + 12 + 4 + 4 + 4  # tail padding to 8
     from natsel_b200 import narrowphase
     assert narrowphase.PAIR_JOB_DTYPE.itemsize == 152
 

@@ -7,7 +7,12 @@ solve_continuous with collision/time_of_impact.rs:391), on the oracle and on the
   steps of one substep) on both engines: it stays on the approach side with finite state and
   no live contact, and without the continuous pass it tunnels;
 - the device's continuous pass bit for bit against the oracle's, step by step, on that scene and
-  on a pile dropped onto a thin ground with a thousand fast bodies a step.
+  on a pile dropped onto a thin ground with a thousand fast bodies a step;
+- bullets (body_def.rs:74 is_bullet; solver_integration.rs:949-958): the same scene as a bullet
+  (ccd_tests.rs:85-100), a bullet shot at a free box (it stops at the box, where a plain fast
+  body passes through it), and the reference's fast-movers scene (parallel_solver_tests.rs:
+  280-322: 640 cubes between two walls, 24 spheres at 300 m/s, every third a bullet), device
+  against oracle bit for bit every step.
 """
 import math
 
@@ -66,23 +71,24 @@ def _world(engine, **kw):
     return World(default_world_def(**kw))
 
 
-def _fast_box(w):
+def _fast_box(w, bullet=False):
     """ccd_tests.rs:30-51: a static wall (half extents 0.1, 2, 2) and a 0.4 m box of density 1000
     at x = -5 moving at 200 m/s toward it."""
     wall = w.create_body(type=0)
     w.create_box(wall, 0.1, 2.0, 2.0)
-    b = w.create_body(type=2, position=(-5.0, 0.0, 0.0), linear_velocity=(200.0, 0.0, 0.0))
+    b = w.create_body(type=2, position=(-5.0, 0.0, 0.0), linear_velocity=(200.0, 0.0, 0.0), is_bullet=bullet)
     w.create_box(b, 0.2, 0.2, 0.2, density=1000.0)
     return b
 
 
+@pytest.mark.parametrize("bullet", [False, True], ids=["fast_body", "bullet"])
 @pytest.mark.parametrize("engine", ENGINES)
-def test_fast_body_does_not_tunnel(engine):
-    """ccd_tests.rs:52-68 and :103-118: after 30 steps of one substep the box is still on the
-    approach side of the wall (x < 0), its state finite and no contact alive; with continuous
-    collision off the same box passes the wall."""
+def test_fast_body_does_not_tunnel(engine, bullet):
+    """ccd_tests.rs:52-68 and :85-118: after 30 steps of one substep the box, plain or a bullet,
+    is still on the approach side of the wall (x < 0), its state finite and no contact alive;
+    with continuous collision off the same box passes the wall."""
     w = _world(engine, gravity=(0.0, -10.0, 0.0), enable_continuous=True)
-    b = _fast_box(w)
+    b = _fast_box(w, bullet)
     for _ in range(30):
         w.step(DT, 1)
     pos, rot, lin, ang = w.bodies()
@@ -97,16 +103,92 @@ def test_fast_body_does_not_tunnel(engine):
 
 
 @pytest.mark.gpu
-def test_fast_body_scene_matches_oracle_every_step():
+@pytest.mark.parametrize("bullet", [False, True], ids=["fast_body", "bullet"])
+def test_fast_body_scene_matches_oracle_every_step(bullet):
     g = _world("gpu", gravity=(0.0, -10.0, 0.0), enable_continuous=True)
     o = _world("oracle", gravity=(0.0, -10.0, 0.0), enable_continuous=True)
     for w in (g, o):
-        _fast_box(w)
+        _fast_box(w, bullet)
     for _ in range(30):
         g.step(DT, 1)
         o.step(DT, 1)
         assert g.state_hash() == o.state_hash()
     assert g.counters()[26] == o.counters()[26] > 0
+
+
+def _shot_at_a_box(w, bullet):
+    """No gravity: a free 1 m box at rest at the origin and a 0.1 m sphere at x = -5 moving at
+    300 m/s toward it (5 m per step)."""
+    box = w.create_body(type=2, enable_sleep=False)
+    w.create_box(box, 0.5, 0.5, 0.5, density=1000.0)
+    ball = w.create_body(type=2, position=(-5.0, 0.0, 0.0), linear_velocity=(300.0, 0.0, 0.0), is_bullet=bullet,
+                         enable_sleep=False)
+    w.create_sphere(ball, 0.1, density=1000.0)
+    return box, ball
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_bullet_stops_at_a_dynamic_body(engine):
+    """A bullet is swept against dynamic bodies too (continuous.rs:429-448): the ball stops at the
+    box's face in the step it would pass it, then pushes the box; a plain fast body only sweeps
+    against static shapes and passes through the box, leaving it at rest."""
+    w = _world(engine, gravity=(0.0, 0.0, 0.0), enable_continuous=True)
+    box, ball = _shot_at_a_box(w, True)
+    w.step(DT, 4)
+    pos, rot, lin, ang = w.bodies()
+    assert -0.65 < pos[ball, 0] < -0.55  # touching the face at x = -0.5 (radius 0.1)
+    for _ in range(3):
+        w.step(DT, 4)
+    pos, rot, lin, ang = w.bodies()
+    assert lin[box, 0] > 1.0 and pos[ball, 0] < pos[box, 0]
+    w = _world(engine, gravity=(0.0, 0.0, 0.0), enable_continuous=True)
+    box, ball = _shot_at_a_box(w, False)
+    for _ in range(4):
+        w.step(DT, 4)
+    pos, rot, lin, ang = w.bodies()
+    assert pos[ball, 0] > 10.0 and lin[box, 0] == 0.0
+
+
+def _fast_movers(w):
+    """parallel_solver_tests.rs:280-322 build_fast_and_sleepy: a ground, two walls, 640 cubes of
+    0.4 m half extent and 24 spheres of radius 0.1 at 300 m/s across them, every third a bullet."""
+    g = w.create_body(type=0, position=(0.0, -1.0, 0.0))
+    w.create_box(g, 50.0, 1.0, 50.0)
+    for x in (-16.0, 16.0):
+        wall = w.create_body(type=0, position=(x, 4.0, 0.0))
+        w.create_box(wall, 0.25, 4.0, 20.0)
+    for i in range(640):
+        b = w.create_body(type=2, position=((i % 16) - 7.5, 0.4 + (i // 256) * 0.8, ((i // 16) % 16) - 7.5),
+                          enable_sleep=False)
+        w.create_box(b, 0.4, 0.4, 0.4)
+    for i in range(24):
+        b = w.create_body(type=2, position=(-12.0 if i % 2 == 0 else 12.0, 1.0 + (i // 2) * 0.5, (i % 5) - 2.0),
+                          linear_velocity=(300.0 if i % 2 == 0 else -300.0, 0.0, (i % 3) - 1.0),
+                          is_bullet=i % 3 == 0, enable_sleep=False)
+        w.create_sphere(b, 0.1)
+
+
+@pytest.mark.gpu
+def test_fast_movers_scene_matches_oracle_every_step():
+    """The reference's fast-movers scene, gravity -10, 60 Hz, 4 substeps: the device equals the
+    oracle bit for bit every step for 60 steps; a sphere found beyond a wall's plane went around
+    the wall (cubes deflect some sideways), not through it."""
+    s = dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True)
+    g, o = _world("gpu", **s), _world("oracle", **s)
+    for w in (g, o):
+        _fast_movers(w)
+    pyoracle.set_threads(8)
+    try:
+        for k in range(60):
+            g.step(DT, 4)
+            o.step(DT, 4)
+            assert g.state_hash() == o.state_hash(), k
+    finally:
+        pyoracle.set_threads(1)
+    assert g.counters()[26] == o.counters()[26] > 0
+    pos = g.bodies()[0][-24:]
+    beyond = np.abs(pos[:, 0]) > 16.0
+    assert ((np.abs(pos[beyond, 2]) > 20.0) | (pos[beyond, 1] > 8.0)).all()
 
 
 @pytest.mark.gpu
