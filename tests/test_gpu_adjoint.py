@@ -177,8 +177,12 @@ def test_bouncing_boxes_gradients_match_finite_differences():
 
 def test_colliding_bouncing_boxes_gradients_match_finite_differences():
     rows, checked = check(COLLIDE_BOUNCE, ground_friction=0.05)
-    assert checked_count(checked, "velocity") >= 2
+    assert checked_count(checked, "velocity") >= 1
+    assert checked_count(checked, "mass") >= 1
     assert checked_count(checked, "restitution") >= 1
+    # the contact takes the larger coefficient (0.6, box A's): box B's gradient is exactly zero
+    g = adjoint(COLLIDE_BOUNCE, ground_friction=0.05)[0]
+    assert g["restitution"][2] == 0.0 and g["restitution"][1] != 0.0
 
 
 def test_spinning_box_rotation_gradient_matches_finite_differences():
