@@ -332,7 +332,10 @@ int ns_world_vjp_f64(ns_world* w, const float* dpos, const float* drot, const fl
  * sweeps the GPU runs for warm start, push, relax (also their state-and-impulse-only form),
  * integrate positions and integrate velocities (without the gyroscopic step) with the
  * dual-number products. which 17 checks restitution like 0..11; which 18 compares the
- * hand-written reverse of the relative normal velocity prepare samples with the dual numbers. */
+ * hand-written reverse of the relative normal velocity prepare samples with the dual numbers.
+ * which 19..23 check the manifolds of sphere-sphere, capsule-sphere, capsule-capsule,
+ * box-sphere and box-capsule pairs like 9..11; worst[1] = the point count (19..21) or the
+ * replayed path (22, 23: 2 GJK point, 3 GJK face, 4 face, 5 edge pair). */
 int ns_adjoint_selfcheck(int which, int seed, double* worst);
 
 #ifdef __cplusplus

@@ -1071,10 +1071,8 @@ int check_adjoint_scope(ns_world* w) {
   if (w->sub_body_begin.size() > 1) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint takes a single world");
   if (!w->joints.empty()) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover joints");
   if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
-  for (const HostShape& hs : w->shapes) {
-    if (hs.d.type != kHull) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint covers box shapes only");
+  for (const HostShape& hs : w->shapes)
     if (hs.d.rolling != 0.0f) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover rolling resistance");
-  }
   for (const DSim& a : w->asims) {
     if (a.local_center.x != 0.0f || a.local_center.y != 0.0f || a.local_center.z != 0.0f)
       return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs each body's centre of mass at its origin");
@@ -1547,6 +1545,69 @@ extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
         double g = yb * y[0].d[0];
         e = std::max(e, std::fabs(g - hand[i]) / std::max(1.0, std::fabs(g)));
       }
+      break;
+    }
+    case 19: case 20: case 21: case 22: case 23: {
+      // manifolds of sphere-sphere (19), capsule-sphere (20), capsule-capsule (21), box-sphere
+      // (22) and box-capsule (23) at random touching poses; worst[1] = the point count (19..21)
+      // or the replayed path (22, 23)
+      DShape A, B;
+      std::memset(&A, 0, sizeof(A));
+      std::memset(&B, 0, sizeof(B));
+      Hull box = make_box_hull(0.6f, 0.4f, 0.5f);
+      const Sphere sa = {v3(0, 0, 0), 0.5f}, sb = {v3(0, 0, 0), 0.3f};
+      const Capsule capa = {v3(-0.5f, 0, 0), v3(0.5f, 0, 0), 0.3f}, capb = {v3(-0.4f, 0, 0), v3(0.4f, 0, 0), 0.2f};
+      A.type = which == 19 ? kSphere : (which <= 21 ? kCapsule : kHull);
+      B.type = (which == 19 || which == 20 || which == 22) ? kSphere : kCapsule;
+      A.sphere = sa; A.capsule = capa;
+      B.sphere = sb; B.capsule = capb;
+      const Hull* ha = A.type == kHull ? &box : nullptr;
+      // box-capsule cycles through its four paths by seed; the others take what comes
+      const int want = which == 23 ? kRoundGjk + seed % 4 : (which == 22 ? (seed % 4 == 3 ? kRoundDeepFace : kRoundGjk) : -1);
+      Pos ca = {0.0, 0.0, 0.0}, cb = {0.0, 0.0, 0.0};
+      double qa[4], qb[4];
+      RoundCase rc;
+      rc.path = kRoundNone;
+      for (int attempt = 0; attempt < 4000; ++attempt) {
+        for (int i = 0; i < 3; ++i) qa[i] = r.range(-0.3, 0.3);
+        qa[3] = 1.0;
+        // near-parallel capsules on even seeds (the two-point branch)
+        double tilt = (which == 21 && (seed & 1) == 0) ? 0.02 : 1.0;
+        for (int i = 0; i < 3; ++i) qb[i] = r.range(-tilt, tilt);
+        qb[3] = 1.0;
+        if (which == 21 && (seed & 1) == 0)  // B turned like A plus a little
+          for (int i = 0; i < 3; ++i) qb[i] += qa[i];
+        double la = std::sqrt(qa[0] * qa[0] + qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]);
+        double lb = std::sqrt(qb[0] * qb[0] + qb[1] * qb[1] + qb[2] * qb[2] + qb[3] * qb[3]);
+        for (int i = 0; i < 4; ++i) { qa[i] /= la; qb[i] /= lb; }
+        double reach = which == 19 ? 0.81 : (which == 20 ? 1.05 : 1.0);
+        double dir[3];
+        random_unit(r, dir, 3);
+        double rad = which <= 21 ? r.range(0.3, reach) : r.range(0.0, 1.1);
+        cb = {rad * dir[0], rad * dir[1], rad * dir[2]};
+        Q fqa = {v3((float)qa[0], (float)qa[1], (float)qa[2]), (float)qa[3]};
+        Q fqb = {v3((float)qb[0], (float)qb[1], (float)qb[2]), (float)qb[3]};
+        WXf wa = {ca, fqa}, wb = {cb, fqb};
+        rc = round_case(A, B, ha, inv_mul_wxf(wa, wb), SimplexCache());
+        if (rc.path == kRoundNone || (want >= 0 && rc.path != want)) continue;
+        std::vector<double> xt(kFI, 0.0);
+        const float fa[4] = {fqa.v.x, fqa.v.y, fqa.v.z, fqa.s}, fb[4] = {fqb.v.x, fqb.v.y, fqb.v.z, fqb.s};
+        for (int i = 0; i < 4; ++i) { xt[fiQa + i] = fa[i]; xt[fiQb + i] = fb[i]; }
+        ad::PlainIn<double> in{xt.data()};
+        double y[kFO];
+        if (narrow_round_fn(in, ca, cb, A, B, ha, rc, y) < 1) { rc.path = kRoundNone; continue; }
+        x = xt;
+        break;
+      }
+      if (rc.path == kRoundNone) return fail(nullptr, NS_ERR_INVALID, "no touching pose found");
+      int pc;
+      {
+        ad::PlainIn<double> in{x.data()};
+        double y[kFO];
+        pc = narrow_round_fn(in, ca, cb, A, B, ha, rc, y);
+      }
+      worst[1] = which <= 21 ? (double)pc : (double)rc.path;
+      e = vjp_fd_error(x, 3 + 7 * pc, [&](const auto& in, auto* y) { narrow_round_fn(in, ca, cb, A, B, ha, rc, y); }, r);
       break;
     }
     default:

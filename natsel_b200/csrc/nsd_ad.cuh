@@ -1583,5 +1583,428 @@ NSD_HD int narrow_box_fn(const In& x, const Pos& ca, const Pos& cb, const Hull& 
   return lm.point_count;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Manifolds of the pairs with a sphere or a capsule (nsd_geom.cuh collide_spheres,
+// collide_capsule_sphere, collide_capsules, collide_hull_sphere, collide_hull_capsule;
+// convex_manifold_shapes.rs:21-643), replayed along the branch the forward step took. The box
+// pairs make discrete choices the value parts alone cannot repeat (the GJK simplex, the SAT
+// face and edge): round_case runs the forward's own f32 routines on the same poses and cache and
+// records them, and the restatement follows the record. Inside a branch, GJK's closest points
+// are the barycentric projection of the origin onto its final simplex (distance.rs:58-67 and
+// :496), whose derivatives are exact; the sphere and capsule pairs take their comparisons on the
+// value parts like the box builders.
+enum : int {
+  kRoundNone = 0,      // no manifold
+  kRoundDirect = 1,    // sphere-sphere, capsule-sphere, capsule-capsule
+  kRoundGjk = 2,       // box pair, one point from the GJK closest points
+  kRoundGjkFace = 3,   // box-capsule, the capsule clipped to the face the GJK normal picks
+  kRoundDeepFace = 4,  // box-sphere with the centre inside; box-capsule SAT face
+  kRoundDeepEdge = 5,  // box-capsule SAT edge pair
+};
+struct RoundCase {
+  int path, face, edge;
+  SimplexCache simplex;  // the GJK simplex after the forward's distance query
+};
+
+// The forward's choices for one pair (A the higher shape type), from the f32 routines.
+NSD_HD RoundCase round_case(const DShape& A, const DShape& B, const Hull* ha, Xf xb, SimplexCache cache) {
+  RoundCase rc;
+  rc.path = kRoundNone; rc.face = -1; rc.edge = -1;
+  rc.simplex = SimplexCache();
+  if (A.type != kHull) { rc.path = kRoundDirect; return rc; }
+  const float spec = speculative_distance();
+  if (B.type == kSphere) {
+    V3 c = xf_point(xb, B.sphere.center);
+    DistOut d = shape_distance(ha->points, kHullVertexCount, &c, 1, xf(v3(0, 0, 0), qid()), &cache);
+    float r = 0.0f + B.sphere.radius;
+    if (d.distance > r + spec) return rc;
+    if (d.distance > 100.0f * kEps) { rc.path = kRoundGjk; rc.simplex = cache; return rc; }
+    float best_d = -kFltMax;
+    for (int i = 0; i < kHullFaceCount; ++i) {
+      float dd = plane_sep(ha->planes[i], c);
+      if (dd > best_d) { rc.face = i; best_d = dd; }
+    }
+    rc.path = kRoundDeepFace;
+    return rc;
+  }
+  const Capsule cap = B.capsule;
+  V3 cpts[2] = {cap.c1, cap.c2};
+  DistOut d = shape_distance(ha->points, kHullVertexCount, cpts, 2, xb, &cache);
+  if (d.distance > cap.radius + spec) return rc;
+  if (d.distance > 100.0f * kEps) {
+    rc.simplex = cache;
+    rc.path = kRoundGjk;
+    int rf = find_hull_support_face(*ha, d.normal);
+    Plane rp = ha->planes[rf];
+    if (absf(dot(rp.n, d.normal)) > 0.998f) {
+      ClipVertex vb[2];
+      vb[0].position = xf_point(xb, cap.c1); vb[0].separation = 0; vb[0].pair = make_feature_pair(0, 0, 0, 0);
+      vb[1].position = xf_point(xb, cap.c2); vb[1].separation = 0; vb[1].pair = make_feature_pair(0, 1, 0, 1);
+      if (clip_segment_to_hull_face(vb, *ha, rf) == 2) {
+        float d1 = plane_sep(rp, vb[0].position), d2 = plane_sep(rp, vb[1].position);
+        if (d1 <= cap.radius + spec || d2 <= cap.radius + spec) { rc.path = kRoundGjkFace; rc.face = rf; }
+      }
+    }
+    return rc;
+  }
+  SepAxis fq = query_face_hull_capsule(*ha, cap, xb);
+  if (fq.separation > cap.radius) return rc;
+  SepAxis eq = query_edge_hull_capsule(*ha, cap, xb);
+  if (eq.separation > cap.radius) return rc;
+  LocalManifold lm;
+  lm.point_count = 0;
+  float face_sep = fq.separation - cap.radius;
+  build_hull_face_capsule(&lm, *ha, cap, xb, fq);
+  if (lm.point_count == 2) { face_sep = minf(lm.points[0].separation, lm.points[1].separation); rc.path = kRoundDeepFace; }
+  rc.face = fq.index_a;
+  if (eq.index_a == kNull) return rc;
+  float edge_sep = eq.separation - cap.radius;
+  if (lm.point_count == 0 || edge_sep > face_sep + linear_slop()) {
+    if (build_hull_capsule_edge(&lm, *ha, cap, xb, eq)) { rc.path = kRoundDeepEdge; rc.edge = eq.index_b; }
+  }
+  return rc;
+}
+
+template <class T> struct TSegResult { TV3<T> p1, p2; T f1, f2; };
+
+// nsd_math.cuh point_to_segment (functions.rs:1169)
+template <class T>
+NSD_HD TV3<T> t_point_to_segment(const TV3<T>& a, const TV3<T>& b, const TV3<T>& q) {
+  TV3<T> ab = b - a, aq = q - a;
+  T alpha = dot(ab, aq);
+  if (alpha <= T(0.0f)) return a;
+  T den = dot(ab, ab);
+  if (alpha > den) return b;
+  alpha = alpha / den;
+  return mul_add(a, alpha, ab);
+}
+// nsd_math.cuh segment_distance (functions.rs:1105)
+template <class T>
+NSD_HD TSegResult<T> t_segment_distance(const TV3<T>& p1, const TV3<T>& q1, const TV3<T>& p2, const TV3<T>& q2) {
+  TSegResult<T> r;
+  TV3<T> d1 = q1 - p1, d2 = q2 - p2, rr = p1 - p2;
+  T a = dot(d1, d1), b = dot(d1, d2), c = dot(d1, rr), e = dot(d2, d2), f = dot(d2, rr);
+  const T small = T(100.0f * kEps), zero = T(0.0f), one = T(1.0f);
+  if (a < small && e < small) { r.p1 = p1; r.f1 = zero; r.p2 = p2; r.f2 = zero; return r; }
+  if (a < small) {
+    T s2 = tclamp(f / e, zero, one);
+    r.p1 = p1; r.f1 = zero; r.p2 = mul_add(p2, s2, d2); r.f2 = s2; return r;
+  }
+  if (e < small) {
+    T s1 = tclamp(-c / a, zero, one);
+    r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = p2; r.f2 = zero; return r;
+  }
+  T denom = a * e - b * b;
+  T s1 = denom > T(1000.0f * kMinPositive) ? tclamp((b * f - c * e) / denom, zero, one) : zero;
+  T s2 = (b * s1 + f) / e;
+  if (s2 < zero) {
+    s1 = tclamp(-c / a, zero, one);
+    s2 = zero;
+  } else if (s2 > one) {
+    s1 = tclamp((b - c) / a, zero, one);
+    s2 = one;
+  }
+  r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = mul_add(p2, s2, d2); r.f2 = s2;
+  return r;
+}
+// nsd_math.cuh line_distance (functions.rs:1069)
+template <class T>
+NSD_HD TSegResult<T> t_line_distance(const TV3<T>& p1, const TV3<T>& d1, const TV3<T>& p2, const TV3<T>& d2) {
+  TSegResult<T> r;
+  T a11 = dot(d1, d1), a12 = -dot(d1, d2), a21 = dot(d2, d1), a22 = -dot(d2, d2);
+  TV3<T> w = p1 - p2;
+  T b1 = -dot(d1, w), b2 = -dot(d2, w);
+  T d = a11 * a22 - a12 * a21;
+  if (d * d < T(1000.0f * kMinPositive)) {
+    T s1 = dot(p2 - p1, d1) / dot(d1, d1);
+    r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = p2; r.f2 = T(0.0f);
+    return r;
+  }
+  T s1 = (a22 * b1 - a12 * b2) / d;
+  T s2 = (a11 * b2 - a21 * b1) / d;
+  r.p1 = mul_add(p1, s1, d1); r.f1 = s1; r.p2 = mul_add(p2, s2, d2); r.f2 = s2;
+  return r;
+}
+// nsd_math.cuh get_length_and_normalize (functions.rs:293)
+template <class T>
+NSD_HD T t_length_and_normalize(const TV3<T>& a, TV3<T>* out) {
+  T ls = a.x * a.x + a.y * a.y + a.z * a.z;
+  if (ls > T(1000.0f * kMinPositive)) {
+    T l = tsqrt(ls);
+    T s = T(1.0f) / l;
+    *out = tv3<T>(s * a.x, s * a.y, s * a.z);
+    return l;
+  }
+  *out = tzero3<T>();
+  return T(0.0f);
+}
+// nsd_geom.cuh clip_segment (convex_manifold.rs:127) against a constant plane
+template <class T>
+NSD_HD int t_clip_segment(TClipVertex<T>* seg, const Plane& pf) {
+  const TPlane<T> p = tplane<T>(pf);
+  int n = 0;
+  TClipVertex<T> a = seg[0], b = seg[1];
+  T d1 = plane_sep(p, a.position), d2 = plane_sep(p, b.position);
+  if (d1 <= T(0.0f)) seg[n++] = a;
+  if (d2 <= T(0.0f)) seg[n++] = b;
+  if (d1 * d2 < T(0.0f)) {
+    T t = d1 / (d1 - d2);
+    seg[n].position = (T(1.0f) - t) * a.position + t * b.position;
+    seg[n].pair = d1 > T(0.0f) ? a.pair : b.pair;
+    n++;
+  }
+  return n;
+}
+// nsd_geom.cuh clip_segment_to_hull_face (convex_manifold.rs:163): the side planes are the box's
+template <class T>
+NSD_HD int t_clip_segment_to_hull_face(TClipVertex<T>* seg, const Hull& h, int ref_face) {
+  Plane rp = h.planes[ref_face];
+  int start = box_face_edge(ref_face);
+  int ei = start;
+  for (;;) {
+    HalfEdge e = box_edge(ei);
+    int ni = e.next;
+    HalfEdge nx = box_edge(ni);
+    V3 p1 = h.points[e.origin], p2 = h.points[nx.origin];
+    V3 tangent = nsd::normalize(p2 - p1);
+    V3 binormal = nsd::cross(tangent, rp.n);
+    if (t_clip_segment(seg, plane_from_normal_point(binormal, p1)) < 2) return 0;
+    ei = ni;
+    if (ei == start) break;
+  }
+  return 2;
+}
+// The GJK closest points on the final simplex (count 1..3): vertex i pairs point ia[i] of A
+// (constant, A's frame) with point ib[i] of B (already in A's frame).
+template <class T>
+NSD_HD void t_gjk_witness(const SimplexCache& sc, const V3* pa, const TV3<T>* pb, TV3<T>* wa, TV3<T>* wb) {
+  TV3<T> A[3], B[3], W[3];
+  const int n = sc.count < 3 ? sc.count : 3;
+  for (int i = 0; i < n; ++i) {
+    A[i] = tv3<T>(pa[sc.ia[i]]);
+    B[i] = pb[sc.ib[i]];
+    W[i] = B[i] - A[i];
+  }
+  if (n <= 1) { *wa = A[0]; *wb = B[0]; return; }
+  if (n == 2) {
+    TV3<T> ab = W[1] - W[0];
+    T d = dot(ab, ab), u = dot(W[1], ab), v = -dot(W[0], ab);
+    T l0 = u / d, l1 = v / d;
+    *wa = blend2(l0, A[0], l1, A[1]);
+    *wb = blend2(l0, B[0], l1, B[1]);
+    return;
+  }
+  TV3<T> ab = W[1] - W[0], ac = W[2] - W[0];
+  TV3<T> bxc = cross(W[1], W[2]), cxa = cross(W[2], W[0]), axb = cross(W[0], W[1]), n3 = cross(ab, ac);
+  T d = dot(n3, n3), u = dot(bxc, n3), v = dot(cxa, n3), w = dot(axb, n3);
+  T l0 = u / d, l1 = v / d, l2 = w / d;
+  *wa = blend2(l0, A[0], l1, A[1]) + l2 * A[2];
+  *wb = blend2(l0, B[0], l1, B[1]) + l2 * B[2];
+}
+
+template <class T>
+NSD_HD void t_collide_spheres(TLocalManifold<T>* m, Sphere a, Sphere b, const TXf<T>& xb) {
+  TV3<T> c1 = tv3<T>(a.center), c2 = xf_point(xb, tv3<T>(b.center));
+  float tr = a.radius + b.radius;
+  float maxd = tr + speculative_distance();
+  TV3<T> off = c2 - c1;
+  T dsq = length_sq(off);
+  if (dsq > T(maxd * maxd)) return;
+  TV3<T> n = tv3<T>(T(0.0f), T(1.0f), T(0.0f));
+  T d = tsqrt(dsq);
+  if (d * d > T(1000.0f * kMinPositive)) n = (T(1.0f) / d) * off;
+  m->normal = n;
+  m->point_count = 1;
+  m->points[0].point = T(0.5f) * (mul_sub(mul_add(c1, T(a.radius), n) + c2, T(b.radius), n));
+  m->points[0].separation = d - T(tr);
+  m->points[0].pair = FeaturePair();
+}
+template <class T>
+NSD_HD void t_collide_capsule_sphere(TLocalManifold<T>* m, Capsule a, Sphere b, const TXf<T>& xb) {
+  TV3<T> c = xf_point(xb, tv3<T>(b.center));
+  float tr = b.radius + a.radius;
+  float maxd = tr + speculative_distance();
+  TV3<T> cp = t_point_to_segment(tv3<T>(a.c1), tv3<T>(a.c2), c);
+  TV3<T> off = c - cp;
+  T dsq = length_sq(off);
+  if (dsq > T(maxd * maxd)) return;
+  TV3<T> n = tv3<T>(T(0.0f), T(1.0f), T(0.0f));
+  T d = tsqrt(dsq);
+  if (d * d > T(1000.0f * kMinPositive)) n = (T(1.0f) / d) * off;
+  m->normal = n;
+  m->point_count = 1;
+  m->points[0].point = T(0.5f) * mul_add(mul_sub(c, T(b.radius), n) + cp, T(a.radius), n);
+  m->points[0].separation = d - T(tr);
+  m->points[0].pair = FeaturePair();
+}
+template <class T>
+NSD_HD void t_collide_capsules(TLocalManifold<T>* m, Capsule a, Capsule b, const TXf<T>& xb) {
+  TV3<T> a1 = tv3<T>(a.c1), a2 = tv3<T>(a.c2);
+  TV3<T> b1 = xf_point(xb, tv3<T>(b.c1)), b2 = xf_point(xb, tv3<T>(b.c2));
+  float radius = a.radius + b.radius;
+  float maxd = radius + speculative_distance();
+  TSegResult<T> res = t_segment_distance(a1, a2, b1, b2);
+  TV3<T> off = res.p2 - res.p1;
+  T dsq = length_sq(off);
+  float mind = 0.01f * linear_slop();
+  if (dsq > T(maxd * maxd) || dsq < T(mind * mind)) return;
+  V3 ea;
+  float la = get_length_and_normalize(a.c2 - a.c1, &ea);
+  if (la < min_capsule_length()) return;
+  TV3<T> eb;
+  T lb = t_length_and_normalize(b2 - b1, &eb);
+  if (lb < T(min_capsule_length())) return;
+  TV3<T> axis = cross(tv3<T>(ea), eb);
+  if (length_sq(axis) < T(0.05f * 0.05f)) {
+    Plane pa0 = plane(-ea, -nsd::dot(ea, a.c1));
+    Plane pa1 = plane(ea, nsd::dot(ea, a.c2));
+    TClipVertex<T> vb[2];
+    vb[0].position = b1; vb[0].separation = T(0.0f); vb[0].pair = make_feature_pair(0, 0, 0, 0);
+    vb[1].position = b2; vb[1].separation = T(0.0f); vb[1].pair = make_feature_pair(0, 1, 0, 1);
+    int pc = t_clip_segment(vb, pa0);
+    if (pc == 2) pc = t_clip_segment(vb, pa1);
+    if (pc == 2) {
+      TV3<T> cp1 = t_point_to_segment(a1, a2, vb[0].position);
+      TV3<T> cp2 = t_point_to_segment(a1, a2, vb[1].position);
+      T d1 = length(vb[0].position - cp1), d2 = length(vb[1].position - cp2);
+      if (d1 <= T(radius) && d2 <= T(radius)) {
+        if (d1 < T(mind) || d2 < T(mind)) return;
+        TV3<T> n1 = (T(1.0f) / d1) * (vb[0].position - cp1);
+        TV3<T> n2 = (T(1.0f) / d2) * (vb[1].position - cp2);
+        TV3<T> n = normalize(n1 + n2);
+        T ra = T(a.radius), rb = T(b.radius);
+        m->normal = n;
+        m->point_count = 2;
+        m->points[0].point = T(0.5f) * mul_sub(mul_add(vb[0].position, ra, n1) + cp1, rb, n);
+        m->points[0].separation = d1 - T(radius);
+        m->points[0].pair = vb[0].pair;
+        m->points[1].point = T(0.5f) * mul_sub(mul_add(vb[1].position, ra, n2) + cp2, rb, n);
+        m->points[1].separation = d2 - T(radius);
+        m->points[1].pair = vb[1].pair;
+        return;
+      }
+    }
+  }
+  TV3<T> n;
+  T dv = t_length_and_normalize(off, &n);
+  m->normal = n;
+  m->point_count = 1;
+  m->points[0].point = T(0.5f) * mul_sub(mul_add(res.p1, T(a.radius), n) + res.p2, T(b.radius), n);
+  m->points[0].separation = dv - T(radius);
+  m->points[0].pair = FeaturePair();
+}
+template <class T>
+NSD_HD void t_hull_sphere(TLocalManifold<T>* m, const Hull& ha, Sphere b, const TXf<T>& xb, const RoundCase& rc) {
+  TV3<T> c = xf_point(xb, tv3<T>(b.center));
+  const T rb = T(b.radius), r = T(0.0f + b.radius);
+  TV3<T> n, pa;
+  T sep;
+  if (rc.path == kRoundGjk) {
+    TV3<T> wb;
+    t_gjk_witness(rc.simplex, ha.points, &c, &pa, &wb);
+    n = normalize(wb - pa);
+    sep = length(wb - pa) - r;
+  } else {
+    pa = c;  // the centre is inside: GJK's witness points coincide with it
+    n = tv3<T>(ha.planes[rc.face].n);
+    sep = plane_sep(tplane<T>(ha.planes[rc.face]), c) - r;
+  }
+  TV3<T> ca = mul_add(c, T(0.0f) - dot(c - pa, n), n);
+  TV3<T> cb = mul_sub(c, rb, n);
+  m->normal = n;
+  m->point_count = 1;
+  m->points[0].point = lerp(ca, cb, T(0.5f));
+  m->points[0].separation = sep;
+  m->points[0].pair = FeaturePair();
+}
+template <class T>
+NSD_HD void t_hull_capsule(TLocalManifold<T>* m, const Hull& ha, Capsule b, const TXf<T>& xb, const RoundCase& rc) {
+  const T br = T(b.radius);
+  TV3<T> q1 = xf_point(xb, tv3<T>(b.c1)), q2 = xf_point(xb, tv3<T>(b.c2));
+  if (rc.path == kRoundGjk) {
+    TM3<T> mt = matrix_from_quat(xb.q);
+    TV3<T> cpts[2] = {mul_mv(mt, tv3<T>(b.c1)) + xb.p, mul_mv(mt, tv3<T>(b.c2)) + xb.p};
+    TV3<T> pa, pb;
+    t_gjk_witness(rc.simplex, ha.points, cpts, &pa, &pb);
+    TV3<T> delta = normalize(pb - pa);
+    m->normal = delta;
+    m->point_count = 1;
+    m->points[0].point = T(0.5f) * (mul_sub(pa, br, delta) + pb);
+    m->points[0].separation = length(pb - pa) - br;
+    m->points[0].pair = FeaturePair();
+    return;
+  }
+  if (rc.path == kRoundGjkFace || rc.path == kRoundDeepFace) {
+    TClipVertex<T> vb[2];
+    vb[0].position = q1; vb[0].separation = T(0.0f); vb[0].pair = make_feature_pair(0, 0, 0, 0);
+    vb[1].position = q2; vb[1].separation = T(0.0f); vb[1].pair = make_feature_pair(0, 1, 0, 1);
+    if (t_clip_segment_to_hull_face(vb, ha, rc.face) != 2) return;
+    TPlane<T> rp = tplane<T>(ha.planes[rc.face]);
+    T d1 = plane_sep(rp, vb[0].position), d2 = plane_sep(rp, vb[1].position);
+    TV3<T> n = rp.n;
+    m->normal = n;
+    m->point_count = 2;
+    // the two builders sum the half-depths in opposite orders
+    T h1 = rc.path == kRoundGjkFace ? T(0.5f) * (br + d1) : T(0.5f) * (d1 + br);
+    T h2 = rc.path == kRoundGjkFace ? T(0.5f) * (br + d2) : T(0.5f) * (d2 + br);
+    m->points[0].point = mul_sub(vb[0].position, h1, n);
+    m->points[0].separation = d1 - br;
+    m->points[0].pair = vb[0].pair;
+    m->points[1].point = mul_sub(vb[1].position, h2, n);
+    m->points[1].separation = d2 - br;
+    m->points[1].pair = vb[1].pair;
+    return;
+  }
+  // the SAT edge pair: the capsule's axis against box edge rc.edge (query_edge_hull_capsule)
+  TV3<T> ec = q2 - q1;
+  HalfEdge e = box_edge(rc.edge), tw = box_edge(rc.edge + 1);
+  TV3<T> ub = tv3<T>(ha.planes[e.face].n), vb = tv3<T>(ha.planes[tw.face].n);
+  T cba = dot(ub, ec), dba = dot(vb, ec);
+  T tt = cba / (cba - dba);
+  TV3<T> n = normalize(lerp(ub, vb, tt));
+  HalfEdge e2 = box_edge(rc.edge);
+  HalfEdge t2 = box_edge(e2.twin);
+  TV3<T> ph = tv3<T>(ha.points[e2.origin]), qh = tv3<T>(ha.points[t2.origin]);
+  TSegResult<T> r = t_line_distance(ph, qh - ph, q1, ec);
+  m->normal = n;
+  m->point_count = 1;
+  m->points[0].point = T(0.5f) * (mul_sub(r.p1, br, n) + r.p2);
+  m->points[0].separation = dot(n, r.p2 - r.p1) - br;
+  m->points[0].pair = make_feature_pair(0, 0, 1, rc.edge);
+}
+
+// The manifold of a pair with a sphere or a capsule followed by update_contact's world
+// transform; same inputs and outputs as narrow_box_fn. Returns the point count, or -1 when the
+// replay makes no manifold.
+template <class T, class In>
+NSD_HD int narrow_round_fn(const In& x, const Pos& ca, const Pos& cb, const DShape& A, const DShape& B, const Hull* ha,
+                           const RoundCase& rc, T* y, uint32_t* ids = nullptr) {
+  if (rc.path == kRoundNone) return -1;
+  TQ<T> qa = in4<T>(x, fiQa), qb = in4<T>(x, fiQb);
+  TV3<T> d = sub_pos_t(cb, ca, in3<T>(x, fiCb), in3<T>(x, fiCa));
+  TXf<T> xb;
+  xb.p = inv_rotate(qa, d);
+  xb.q = inv_mul_quat(qa, qb);
+  TLocalManifold<T> lm;
+  lm.point_count = 0;
+  if (A.type == kSphere) t_collide_spheres(&lm, A.sphere, B.sphere, xb);
+  else if (A.type == kCapsule && B.type == kSphere) t_collide_capsule_sphere(&lm, A.capsule, B.sphere, xb);
+  else if (A.type == kCapsule) t_collide_capsules(&lm, A.capsule, B.capsule, xb);
+  else if (B.type == kSphere) t_hull_sphere(&lm, *ha, B.sphere, xb, rc);
+  else t_hull_capsule(&lm, *ha, B.capsule, xb, rc);
+  if (lm.point_count == 0) return -1;
+  TM3<T> ma = matrix_from_quat(qa);
+  TV3<T> dab = sub_pos_t(ca, cb, in3<T>(x, fiCa), in3<T>(x, fiCb));
+  out3(y, 0, mul_mv(ma, lm.normal));
+  for (int i = 0; i < lm.point_count; ++i) {
+    TV3<T> aa = mul_mv(ma, lm.points[i].point);
+    out3(y, 3 + 7 * i, aa);
+    out3(y, 3 + 7 * i + 3, aa + dab);
+    y[3 + 7 * i + 6] = lm.points[i].separation;
+    if (ids) ids[i] = make_feature_id(lm.points[i].pair);
+  }
+  return lm.point_count;
+}
+
 }  // namespace ad
 }  // namespace nsd

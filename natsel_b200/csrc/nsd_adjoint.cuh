@@ -710,13 +710,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_narrow(StepTape t, AdjBufs 
       xs[fiQb] = sb.q.v.x; xs[fiQb + 1] = sb.q.v.y; xs[fiQb + 2] = sb.q.v.z; xs[fiQb + 3] = sb.q.s;
     }
     __syncwarp();
-    NarrowCase nc = {post.sat.type, post.sat.index_a, post.sat.index_b, post.sat.hit};
     SeedIn<float, 1> in;
     in.x = xs;
     in.dir[0] = lane < kFI ? lane : -1;
     Dual<float, 1> y[kFO];
     uint32_t ids[4];
-    int got = narrow_box_fn(in, pa, pb, w.hulls[A.hull], w.hulls[B.hull], nc, y, ids);
+    int got;
+    if (A.type == kHull && B.type == kHull) {
+      NarrowCase nc = {post.sat.type, post.sat.index_a, post.sat.index_b, post.sat.hit};
+      got = narrow_box_fn(in, pa, pb, w.hulls[A.hull], w.hulls[B.hull], nc, y, ids);
+    } else {
+      // the forward's choices from its own poses and GJK cache (every lane alike)
+      const Hull* ha = A.type == kHull ? &w.hulls[A.hull] : nullptr;
+      WXf wa = {pa, sa.q}, wb = {pb, sb.q};
+      RoundCase rc = round_case(A, B, ha, inv_mul_wxf(wa, wb), pre.simplex);
+      got = narrow_round_fn(in, pa, pb, A, B, ha, rc, y, ids);
+    }
     bool same = got == pc;
     for (int q = 0; same && q < pc; ++q) same = ids[q] == post.manifold.points[q].feature_id;
     if (!same) {

@@ -373,6 +373,13 @@ inline void narrow(const StepTape& t, Bufs& a, const Consts& cs) {
       Pos pa = {sa.px, sa.py, sa.pz}, pb = {sb.px, sb.py, sb.pz};
       double xs[kFI] = {0, 0, 0, sa.q.v.x, sa.q.v.y, sa.q.v.z, sa.q.s, 0, 0, 0, sb.q.v.x, sb.q.v.y, sb.q.v.z, sb.q.s};
       NarrowCase nc = {post.sat.type, post.sat.index_a, post.sat.index_b, post.sat.hit};
+      const bool boxes = A.type == kHull && B.type == kHull;
+      const Hull* ha = A.type == kHull ? &cs.hulls[A.hull] : nullptr;
+      RoundCase rc = {};
+      if (!boxes) {
+        WXf wa = {pa, sa.q}, wb = {pb, sb.q};
+        rc = round_case(A, B, ha, inv_mul_wxf(wa, wb), pre.simplex);
+      }
       bool same = true;
       double g[kFI];
       for (int d = 0; d < kFI && same; ++d) {
@@ -381,7 +388,8 @@ inline void narrow(const StepTape& t, Bufs& a, const Consts& cs) {
         in.dir[0] = d;
         Dual<double, 1> y[kFO];
         uint32_t ids[4];
-        int got = narrow_box_fn(in, pa, pb, cs.hulls[A.hull], cs.hulls[B.hull], nc, y, ids);
+        int got = boxes ? narrow_box_fn(in, pa, pb, cs.hulls[A.hull], cs.hulls[B.hull], nc, y, ids)
+                        : narrow_round_fn(in, pa, pb, A, B, ha, rc, y, ids);
         same = got == pc;
         for (int q = 0; same && q < pc; ++q) same = ids[q] == post.manifold.points[q].feature_id;
         double acc = 0.0;

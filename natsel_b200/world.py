@@ -484,7 +484,8 @@ ADJOINT_CHECKS = ["warm_start", "push", "relax", "prepare", "integrate_velocitie
                   "finalize_rotation", "inverse_inertia", "recycle", "box_face", "box_any", "box_edge",
                   "warm_start_reverse_sweep", "push_reverse_sweep", "relax_reverse_sweep",
                   "integrate_positions_reverse_sweep", "integrate_velocities_reverse_sweep", "restitution",
-                  "relative_velocity_reverse_sweep"]
+                  "relative_velocity_reverse_sweep", "sphere_sphere", "capsule_sphere", "capsule_capsule",
+                  "box_sphere", "box_capsule"]
 
 
 def adjoint_selfcheck(which, seed):

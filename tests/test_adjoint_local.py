@@ -1,8 +1,8 @@
 """The adjoint's local derivatives, checked in f64 on the host (no GPU).
 
 The reverse stages of ns_world_vjp rest on a dual-number restatement of each forward function
-(warm start, push, relax, prepare, the body stages, recycled separations, box-box
-manifolds and restitution). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random inputs and
+(warm start, push, relax, prepare, the body stages, recycled separations, the manifolds of
+every shape pair and restitution). ns_adjoint_selfcheck evaluates that restatement in f64 at seeded random inputs and
 compares its vector-Jacobian product, direction by direction, with central differences of the
 same function; and it compares the hand-derived reverse sweeps the solver stages run on the
 GPU (warm start, push, relax, integrate positions and velocities, the relative normal velocity
@@ -54,3 +54,21 @@ def test_relative_velocity_reverse_sweep_matches_dual_numbers():
     for seed in range(16):
         worst, _ = adjoint_selfcheck(18, seed)
         assert 0.0 <= worst < 1e-12, (seed, worst)
+
+
+@pytest.mark.parametrize("which", range(19, 24), ids=ADJOINT_CHECKS[19:24])
+def test_round_manifold_vjp_matches_central_differences(which):
+    """Sphere and capsule pairs: the dual-number manifold replay against central differences at
+    random touching poses, with the two-point capsule branch and every box-sphere and box-capsule
+    path exercised."""
+    seen = set()
+    for seed in range(16):
+        worst, kind = adjoint_selfcheck(which, seed)
+        assert 0.0 <= worst < 1e-6, (ADJOINT_CHECKS[which], seed, worst, kind)
+        seen.add(int(kind))
+    if which == 21:
+        assert seen == {1, 2}, seen  # one- and two-point manifolds
+    if which == 22:
+        assert seen == {2, 4}, seen  # distance path and the centre inside the box
+    if which == 23:
+        assert seen == {2, 3, 4, 5}, seen

@@ -3,7 +3,7 @@ differences of the forward step, and the tape's bookkeeping.
 
 The scenes keep one contact set over the horizon (boxes sliding and spinning on the ground, a
 box running into a lighter one, a box sliding on another, boxes bouncing off the ground and off
-each other with restitution). Contact solves still have kinks (an
+each other with restitution, spheres and capsules sliding, rolling and colliding). Contact solves still have kinks (an
 impulse meeting its clamp at zero, a corner point unloading); where one falls inside the
 difference interval the central difference does not converge, and below h ~ 1e-3 the f32
 rounding of the trajectory dominates it. So each entry is differenced at h and 2 h, and the
@@ -50,13 +50,51 @@ COLLIDE_BOUNCE = [
 ]
 
 
+# round shapes: ("sphere", r), ("capsule", half length, r) along x, ("capsule_z", half length, r)
+# along z. Spheres sliding into rolling and a capsule sliding and spinning on the ground
+# (box-sphere, box-capsule); a sphere into a sphere, a sphere into a capsule and a capsule into a
+# crossing capsule on slippery ground
+ROUND = [
+    ((0.0, 0.298, 0.0), ("sphere", 0.3), (2.0, 0.0, 0.5), (0.0, 0.0, 0.0), 1000.0, 0.6),
+    ((3.0, 0.198, 1.0), ("capsule", 0.4, 0.2), (-1.5, 0.0, 0.3), (0.0, 0.5, 0.0), 800.0, 0.5),
+    ((-3.0, 0.248, -2.0), ("sphere", 0.25), (0.5, 0.0, 1.8), (0.0, 0.0, 0.0), 1200.0, 0.7),
+]
+ROUND_COLLIDE = [
+    ((-1.2, 0.298, 0.0), ("sphere", 0.3), (3.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1000.0, 0.5),
+    ((0.0, 0.248, 0.05), ("sphere", 0.25), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 500.0, 0.5),
+    ((-1.3, 0.248, 3.1), ("sphere", 0.25), (3.0, 0.0, 0.0), (0.0, 0.0, 0.0), 900.0, 0.5),
+    ((0.0, 0.198, 3.0), ("capsule_z", 0.4, 0.2), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 600.0, 0.5),
+    ((-1.4, 0.198, -3.1), ("capsule", 0.3, 0.2), (3.0, 0.0, 0.0), (0.0, 0.0, 0.0), 900.0, 0.5),
+    ((0.0, 0.198, -3.0), ("capsule_z", 0.4, 0.2), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 600.0, 0.5),
+]
+
+
+def make_shape(w, b, he, **kw):
+    if he[0] == "sphere":
+        w.create_sphere(b, he[1], **kw)
+    elif he[0] == "capsule":
+        w.create_capsule(b, (-he[1], 0.0, 0.0), (he[1], 0.0, 0.0), he[2], **kw)
+    elif he[0] == "capsule_z":
+        w.create_capsule(b, (0.0, 0.0, -he[1]), (0.0, 0.0, he[1]), he[2], **kw)
+    else:
+        w.create_box(b, *he, **kw)
+
+
+def volume(he):
+    if he[0] == "sphere":
+        return 4.0 / 3.0 * np.pi * he[1] ** 3
+    if he[0] in ("capsule", "capsule_z"):
+        return np.pi * he[2] ** 2 * 2.0 * he[1] + 4.0 / 3.0 * np.pi * he[2] ** 3
+    return 8.0 * he[0] * he[1] * he[2]
+
+
 def build(bodies, checkpoint=None, ground_friction=0.6):
     w = World(**WORLD)
     g = w.create_body(type=STATIC_BODY, position=(0.0, -0.5, 0.0))
     w.create_box(g, 20.0, 0.5, 20.0, friction=ground_friction)
     for pos, he, v, om, rho, mu, *rest in bodies:
         b = w.create_body(type=DYNAMIC_BODY, position=pos, linear_velocity=v, angular_velocity=om, enable_sleep=False)
-        w.create_box(b, *he, density=rho, friction=mu, restitution=rest[0] if rest else 0.0)
+        make_shape(w, b, he, density=rho, friction=mu, restitution=rest[0] if rest else 0.0)
     if checkpoint is not None:
         w.tape_begin(checkpoint)
     return w
@@ -117,7 +155,7 @@ def check(bodies, ground_friction=0.6):
     assert h0 == h1, "the adjoint must leave the world in its final state"
     rows = []  # kind, adjoint, fd(h), fd(2 h)
     for i, (pos, he, v, om, rho, mu, *rest) in enumerate(bodies):
-        vol = 8.0 * he[0] * he[1] * he[2]
+        vol = volume(he)
         entries = [("velocity", g["lin0"][i + 1, c], 2, c, 1e-3) for c in range(3)]
         entries += [("velocity", g["ang0"][i + 1, c], 3, c, 1e-3) for c in range(3)]
         entries += [("mass", g["mass"][i + 1] * vol, 4, 0, 1e-3 * rho), ("friction", g["friction"][i + 1], 5, 0, 1e-3)]
@@ -183,6 +221,18 @@ def test_colliding_bouncing_boxes_gradients_match_finite_differences():
     # the contact takes the larger coefficient (0.6, box A's): box B's gradient is exactly zero
     g = adjoint(COLLIDE_BOUNCE, ground_friction=0.05)[0]
     assert g["restitution"][2] == 0.0 and g["restitution"][1] != 0.0
+
+
+def test_round_shapes_on_the_ground_gradients_match_finite_differences():
+    rows, checked = check(ROUND)
+    assert checked_count(checked, "velocity") >= 4
+    assert checked_count(checked, "friction") >= 2
+
+
+def test_round_shape_collisions_gradients_match_finite_differences():
+    rows, checked = check(ROUND_COLLIDE, ground_friction=0.05)
+    assert checked_count(checked, "velocity") >= 3
+    assert checked_count(checked, "mass") >= 2
 
 
 def test_spinning_box_rotation_gradient_matches_finite_differences():
@@ -259,13 +309,15 @@ def test_vjp_of_velocity_cotangent_is_identity_without_contacts():
 
 
 def test_adjoint_scope_is_enforced():
-    w = World(**WORLD)
-    b = w.create_body(type=DYNAMIC_BODY, position=(0.0, 1.0, 0.0), enable_sleep=False)
-    w.create_sphere(b, 0.5)
-    with pytest.raises(NsError) as e:
-        w.tape_begin(8)
-    assert e.value.code == 6
-    w.close()
+    # rolling resistance, and a centre of mass away from the body origin, are refused
+    for kw in (dict(rolling_resistance=0.1), dict(center=(0.3, 0.0, 0.0))):
+        w = World(**WORLD)
+        b = w.create_body(type=DYNAMIC_BODY, position=(0.0, 1.0, 0.0), enable_sleep=False)
+        w.create_sphere(b, 0.5, **kw)
+        with pytest.raises(NsError) as e:
+            w.tape_begin(8)
+        assert e.value.code == 6
+        w.close()
     w = build(SLIDERS, checkpoint=8)
     with pytest.raises(NsError):
         w.apply_forces(force=np.zeros((4, 3), np.float32))
@@ -292,10 +344,11 @@ def _f64_agreement(g32, g64, keys):
     return np.concatenate(out)
 
 
-@pytest.mark.parametrize("scene", ["sliders", "collide", "stack"])
+@pytest.mark.parametrize("scene", ["sliders", "collide", "stack", "round", "round_collide"])
 def test_f32_adjoint_matches_f64_host_adjoint(scene):
     # the same recorded rollout reversed on the device in f32 and on the host in f64
-    bodies, gf = {"sliders": (SLIDERS, 0.6), "collide": (COLLIDE, 0.05), "stack": (STACK, 0.6)}[scene]
+    bodies, gf = {"sliders": (SLIDERS, 0.6), "collide": (COLLIDE, 0.05), "stack": (STACK, 0.6),
+                  "round": (ROUND, 0.6), "round_collide": (ROUND_COLLIDE, 0.05)}[scene]
     w = build(bodies, 8, gf)
     for _ in range(STEPS):
         w.step(DT, SUBSTEPS)
