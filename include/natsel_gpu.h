@@ -336,7 +336,8 @@ int ns_world_vjp_f64(ns_world* w, const float* dpos, const float* drot, const fl
  * hand-written reverse of the relative normal velocity prepare samples with the dual numbers.
  * which 19..23 check the manifolds of sphere-sphere, capsule-sphere, capsule-capsule,
  * box-sphere and box-capsule pairs like 9..11; worst[1] = the point count (19..21) or the
- * replayed path (22, 23: 2 GJK point, 3 GJK face, 4 face, 5 edge pair). */
+ * replayed path (22, 23: 2 GJK point, 3 GJK face, 4 face, 5 edge pair). which 24..26 check the
+ * revolute joint's solve, warm start and prepare like 0..8. */
 int ns_adjoint_selfcheck(int which, int seed, double* worst);
 
 #ifdef __cplusplus

@@ -825,6 +825,9 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   if (d.n_joints > 0) {
     k_prepare_joints<<<blocks(d.n_joints, 128), 128, 0, s>>>(d, p);
     ++nk;
+    if (tape)
+      NS_CUDA(w, cudaMemcpyAsync(tape->dev.joints, d.joints, sizeof(DJoint) * (size_t)d.n_joints,
+                                 cudaMemcpyDeviceToDevice, s));
   }
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[3], s, ev_flags));
   if (tape) {
@@ -1065,11 +1068,12 @@ int tape_after_step(ns_world* w, float dt, int substeps) {
   return NS_OK;
 }
 
-// The adjoint covers one world of boxes without joints, restitution, rolling resistance or
-// continuous collision.
+// The adjoint covers one world of boxes, spheres and capsules with revolute joints, without
+// rolling resistance, continuous collision, or joints in the overflow colour.
 int check_adjoint_scope(ns_world* w) {
   if (w->sub_body_begin.size() > 1) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint takes a single world");
-  if (!w->joints.empty()) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover joints");
+  if (w->jr.off[kOverflowIndex + 1] > w->jr.off[kOverflowIndex])
+    return fail(w, NS_ERR_UNSUPPORTED, "joints in the overflow colour; the adjoint does not cover them");
   if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
   for (const HostShape& hs : w->shapes)
     if (hs.d.rolling != 0.0f) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover rolling resistance");
@@ -1102,6 +1106,9 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
   size_t o_fin = take(sizeof(float4) * cap), o_mode = take(cap), o_ops = take(sizeof(CopyOp) * 20);
   const int rest_its = std::max(w->def.restitution_iterations, 0);
   size_t o_rest = take(sizeof(float4) * 6 * cap * (size_t)std::max(rest_its, 1));
+  const size_t nj = (size_t)std::max(d.n_joints, 1);
+  size_t o_joints = take(sizeof(DJoint) * nj);
+  size_t o_jrow = take(sizeof(float4) * 2 * 6 * nj * max_substeps), o_jwarm = take(sizeof(float4) * 4 * nj * max_substeps);
   int st = reuse_buffer(w, &w->tapes_buf, &w->tapes_cap, per * (size_t)count);
   if (st) return st;
   ts->data = w->tapes_buf;
@@ -1139,9 +1146,15 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
     t.mode = (uint8_t*)(b + o_mode);
     t.rest = (float4*)(b + o_rest);
     t.rest_iterations = rest_its;
+    t.joints = (DJoint*)(b + o_joints);
+    t.joint = (float4*)(b + o_jrow);
+    t.jwarm = (float4*)(b + o_jwarm);
+    t.n_joints = d.n_joints;
     t.substeps = 0;
     h.solve.body = t.body; h.solve.push = t.push; h.solve.relax = t.relax; h.solve.fin = t.fin;
     h.solve.rest = t.rest;
+    h.solve.joint = d.n_joints > 0 ? t.joint : nullptr;
+    h.solve.jwarm = d.n_joints > 0 ? t.jwarm : nullptr;
     h.plane_ops = (CopyOp*)(b + o_ops);
     h.n_plane_ops = (int)ops.size();
     NS_CUDA(w, cudaMemcpy(h.plane_ops, ops.data(), ops.size() * sizeof(CopyOp), cudaMemcpyHostToDevice));
@@ -1608,6 +1621,83 @@ extern "C" int ns_adjoint_selfcheck(int which, int seed, double* worst) {
       }
       worst[1] = which <= 21 ? (double)pc : (double)rc.path;
       e = vjp_fd_error(x, 3 + 7 * pc, [&](const auto& in, auto* y) { narrow_round_fn(in, ca, cb, A, B, ha, rc, y); }, r);
+      break;
+    }
+    case 24: case 25: case 26: {
+      // revolute joint: the solve (24; even seeds push with bias, odd relax; the spring, motor
+      // and limit rows by seed), its warm start (25) and its prepare (26)
+      auto rand_quat = [&](double* q, double tilt) {
+        for (int i = 0; i < 3; ++i) q[i] = r.range(-tilt, tilt);
+        q[3] = 1.0;
+        double l = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + 1.0);
+        for (int i = 0; i < 4; ++i) q[i] /= l;
+      };
+      auto rand_m3 = [&](double* m) {  // symmetric positive definite, columns cx cy cz
+        double s6[6];
+        random_spd(r, s6);
+        const int at[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int i = 0; i < 9; ++i) m[i] = s6[at[i]];
+      };
+      if (which == 26) {
+        x.assign(kJPI, 0.0);
+        rand_quat(&x[jpQa], 0.6);
+        rand_quat(&x[jpQb], 0.6);
+        x[jpIma] = r.range(0.5, 2.0); x[jpImb] = r.range(0.5, 2.0);
+        rand_m3(&x[jpIA]); rand_m3(&x[jpIB]);
+        Xf lfa = xf(v3((float)r.range(-0.5, 0.5), (float)r.range(-0.5, 0.5), (float)r.range(-0.5, 0.5)), qid());
+        Xf lfb = xf(v3((float)r.range(-0.5, 0.5), (float)r.range(-0.5, 0.5), (float)r.range(-0.5, 0.5)),
+                    quat(v3(0.0f, (float)std::sin(0.3), 0.0f), (float)std::cos(0.3)));
+        Pos ca = {r.range(-2, 2), r.range(0, 3), r.range(-2, 2)}, cb = {r.range(-2, 2), r.range(0, 3), r.range(-2, 2)};
+        e = vjp_fd_error(x, kJPO, [&](const auto& in, auto* y) {
+          joint_prepare_fn(in, lfa, lfb, v3(0, 0, 0), v3(0, 0, 0), ca, cb, y);
+        }, r);
+        break;
+      }
+      x.assign(kJX, 0.0);
+      for (int i = 0; i < 12; ++i) x[i] = r.range(-1.0, 1.0);
+      for (int i = 0; i < 3; ++i) { x[jxDpA + i] = r.range(-0.01, 0.01); x[jxDpB + i] = r.range(-0.01, 0.01); }
+      rand_quat(&x[jxDqA], 0.02);
+      rand_quat(&x[jxDqB], 0.02);
+      for (int i = 0; i < 3; ++i) x[jxLin + i] = r.range(-0.5, 0.5);
+      x[jxPerp] = r.range(-0.2, 0.2); x[jxPerp + 1] = r.range(-0.2, 0.2);
+      x[jxSpring] = r.range(-0.1, 0.1); x[jxMotor] = r.range(-0.05, 0.05);
+      x[jxLower] = r.range(0.0, 0.2); x[jxUpper] = r.range(0.0, 0.2);
+      for (int i = 0; i < 3; ++i) { x[jxPx + i] = r.range(-0.5, 0.5); x[jxPy + i] = r.range(-0.5, 0.5); }
+      x[jxIma] = r.range(0.5, 2.0); x[jxImb] = r.range(0.5, 2.0);
+      rand_m3(&x[jxIA]); rand_m3(&x[jxIB]);
+      rand_quat(&x[jxFqA], 0.5);
+      rand_quat(&x[jxFqB], 0.5);
+      for (int i = 0; i < 3; ++i) { x[jxFpA + i] = r.range(-0.5, 0.5); x[jxFpB + i] = r.range(-0.5, 0.5); x[jxDc + i] = r.range(-1.0, 1.0); }
+      {
+        // the axis and axial mass as prepare makes them
+        ad::PlainIn<double> in{x.data()};
+        ad::TQ<double> fq = ad::in4<double>(in, jxFqA);
+        ad::TV3<double> axis = ad::rotate(fq, ad::tv3<double>(0.0, 0.0, 1.0));
+        ad::TM3<double> ia = ad::in_m3<double>(in, jxIA), ib = ad::in_m3<double>(in, jxIB);
+        ad::TM3<double> sum = ad::tm3<double>(ia.cx + ib.cx, ia.cy + ib.cy, ia.cz + ib.cz);
+        x[jxAxis] = axis.x; x[jxAxis + 1] = axis.y; x[jxAxis + 2] = axis.z;
+        x[jxAxial] = 1.0 / ad::dot(axis, ad::mul_mv(sum, axis));
+      }
+      if (which == 25) {
+        e = vjp_fd_error(x, 12, [&](const auto& in, auto* y) { joint_warm_fn(in, y); }, r);
+        break;
+      }
+      JParams jp;
+      jp.use_bias = (seed & 1) == 0;
+      jp.fixed = false;
+      jp.spring = seed % 3 == 0;
+      jp.motor = seed % 3 == 1;
+      jp.limit = seed % 3 != 1;
+      jp.cs = make_soft(60.0f, 2.0f, h);
+      jp.ss = make_soft(2.0f, 0.3f, h);
+      jp.target = (float)r.range(-0.3, 0.3);
+      jp.lower = (float)r.range(-0.6, 0.0);
+      jp.upper = (float)r.range(0.0, 0.6);
+      if (seed % 6 == 2) { jp.lower = 0.4f; jp.upper = 0.8f; }  // the angle below the lower limit
+      jp.motor_speed = (float)r.range(-1.0, 1.0);
+      jp.max_torque_h = (seed % 4 == 1) ? 1e-3f : 10.0f * h;  // odd motors clamp
+      jp.inv_h = 1.0f / h;
+      e = vjp_fd_error(x, kJSolveOut, [&](const auto& in, auto* y) { joint_solve_fn(in, jp, y); }, r);
       break;
     }
     default:
@@ -2622,6 +2712,7 @@ static StepTape rebase_tape(const StepTape& t, const char* dev_base, char* host_
   h.sims = rb(t.sims); h.pre = rb(t.pre); h.post = rb(t.post); h.ctl = rb(t.ctl);
   h.body = rb(t.body); h.push = rb(t.push); h.relax = rb(t.relax); h.fin = rb(t.fin); h.mode = rb(t.mode);
   h.rest = rb(t.rest);
+  h.joints = rb(t.joints); h.joint = rb(t.joint); h.jwarm = rb(t.jwarm);
   CPlanes& P = h.planes;
   P.idx = rb(t.planes.idx); P.mass = rb(t.planes.mass); P.ia0 = rb(t.planes.ia0); P.ia1 = rb(t.planes.ia1);
   P.ib1 = rb(t.planes.ib1); P.n = rb(t.planes.n); P.t1 = rb(t.planes.t1); P.t2 = rb(t.planes.t2);
@@ -2640,6 +2731,7 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
   if (!w->tape || w->tape->steps.empty()) return fail(w, NS_ERR_INVALID, "no recorded steps");
   NS_CUDA(w, cudaSetDevice(w->def.device));
   AdTape* tp = w->tape;
+  if (f64 && w->dw.n_joints > 0) return fail(w, NS_ERR_UNSUPPORTED, "the f64 reverse pass does not cover joints");
   tp->recording = false;
   tp->vjp_calls++;
   const DW& d = w->dw;
@@ -2696,6 +2788,8 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     size_t o_yrec = take(sizeof(float) * 3 * ad::kRelaxOut * (size_t)cap * max_sub);
     size_t o_tot = take(sizeof(float) * 4 * (size_t)cap), o_restb = take(sizeof(float) * 4 * (size_t)cap);
     size_t o_rel = take(sizeof(float) * 4 * (size_t)cap);
+    const size_t nj = (size_t)std::max(d.n_joints, 1);
+    size_t o_jb = take(sizeof(float) * ad::kJState * nj), o_jc = take(sizeof(float) * ad::kJConst * nj);
     size_t o_seed = take(sizeof(float) * 13 * (size_t)nb), o_out = take(sizeof(float) * 16 * (size_t)nb);
     if (reuse_buffer(w, &w->adj_buf, &w->adj_cap, o) != NS_OK) { st = fail(w, NS_ERR_CUDA, "adjoint buffers (%zu bytes)", o); break; }
     buf = w->adj_buf;
@@ -2705,6 +2799,8 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     a.kb = (float*)(buf + o_kb); a.mb = (float*)(buf + o_mb); a.mismatch = (int*)(buf + o_mis);
     a.yrec = (float*)(buf + o_yrec);
     a.totb = (float*)(buf + o_tot); a.restb = (float*)(buf + o_restb); a.relb = (float*)(buf + o_rel);
+    a.jb = (float*)(buf + o_jb); a.jc = (float*)(buf + o_jc);
+    a.joint_list = d.joint_list; a.jr = w->jr; a.n_joints = d.n_joints;
     a.cap = cap; a.n_awake = n;
     float* seed = (float*)(buf + o_seed);
     float* dev_out = (float*)(buf + o_out);
@@ -2781,6 +2877,10 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
         }
         if (n_slots > 0) k_adj_consts<<<blocks(n_slots, 64), 64, 0, w->stream>>>(t, a, p, n_slots);
         if (n_slots > 0) k_adj_prepare<<<blocks(n_slots, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d, p, n_slots);
+        if (d.n_joints > 0) {
+          k_adj_joint_prepare<<<blocks(d.n_joints, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d, p);
+          launches += 1;
+        }
         if (n > 0) k_adj_inertia<<<blocks(n, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a);
         k_adj_narrow<<<blocks(cap, kAdjThreads / 32), kAdjThreads, 0, w->stream>>>(t, a, d);
         NS_CUDA(w, cudaGetLastError());

@@ -2006,5 +2006,267 @@ NSD_HD int narrow_round_fn(const In& x, const Pos& ca, const Pos& cb, const DSha
   return lm.point_count;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Revolute joints (nsd_solve.cuh solve_joint and joint_warm_delta, nsd_kernels.cuh
+// k_prepare_joints; revolute_joint.rs:183-553). The joint vector holds the bodies' velocities,
+// position and rotation increments, the joint's impulses and perp axes (the warm start reads the
+// axes the last solve wrote; the solve recomputes them) and the prepared constants.
+enum JX : int {
+  jxVA = 0, jxWA = 3, jxVB = 6, jxWB = 9, jxDpA = 12, jxDpB = 15, jxDqA = 18, jxDqB = 22,
+  jxLin = 26, jxPerp = 29, jxSpring = 31, jxMotor = 32, jxLower = 33, jxUpper = 34,
+  jxPx = 35, jxPy = 38,
+  jxIma = 41, jxImb = 42, jxIA = 43, jxIB = 52, jxFqA = 61, jxFqB = 65, jxFpA = 69, jxFpB = 72,
+  jxAxis = 75, jxAxial = 78, jxDc = 79, kJX = 82,
+};
+// Solve outputs: velocities 0..11, impulses 12..20 (jxLin..jxUpper order), perp axes 21..26.
+constexpr int kJSolveOut = 27;
+// The joint's carried state (impulses and perp axes: jxLin..jxPy + 2) and its constants
+// (jxIma..kJX).
+constexpr int kJState = jxIma - jxLin, kJConst = kJX - jxIma;
+struct JParams {
+  bool use_bias, fixed, spring, motor, limit;
+  Softness cs, ss;  // constraint and spring softness
+  float target, lower, upper, motor_speed, max_torque_h, inv_h;
+};
+
+// nsd_math.cuh atan2_approx (functions.rs:68) and get_twist_angle (:490)
+template <class T>
+NSD_HD T t_atan2_approx(const T& y, const T& x) {
+  if (x == T(0.0f) && y == T(0.0f)) return T(0.0f);
+  T ax = tabs(x), ay = tabs(y);
+  T mx = tmax(ay, ax), mn = tmin(ay, ax);
+  T a = mn / mx;
+  T s = a * a, c = s * a, q = s * s;
+  T r = T(0.024840285f) * q + T(0.18681418f);
+  T t = T(-0.094097948f) * q - T(0.33213072f);
+  r = r * s + t;
+  r = r * c + a;
+  if (ay > ax) r = T(1.57079637f) - r;
+  if (x < T(0.0f)) r = T(3.14159274f) - r;
+  if (y < T(0.0f)) r = -r;
+  return r;
+}
+template <class T>
+NSD_HD T t_twist_angle(const TQ<T>& q) {
+  T twist = q.s < T(0.0f) ? t_atan2_approx(-q.v.z, -q.s) : t_atan2_approx(q.v.z, q.s);
+  return twist * T(2.0f);
+}
+// nsd_solve.cuh solve_point_constraint (revolute_joint.rs:95)
+template <class T>
+NSD_HD TV3<T> t_solve_point_constraint(const T& ma, const T& mb, const TM3<T>& ia, const TM3<T>& ib, const TV3<T>& ra,
+                                       const TV3<T>& rb, const TV3<T>& rhs) {
+  T axy = ra.z * ia.cy.y - ra.y * ia.cz.y;
+  T axz = ra.z * ia.cy.z - ra.y * ia.cz.z;
+  TV3<T> ay = ra.x * ia.cz - ra.z * ia.cx;
+  TV3<T> az = ra.y * ia.cx - ra.x * ia.cy;
+  T bxy = rb.z * ib.cy.y - rb.y * ib.cz.y;
+  T bxz = rb.z * ib.cy.z - rb.y * ib.cz.z;
+  TV3<T> by = rb.x * ib.cz - rb.z * ib.cx;
+  TV3<T> bz = rb.y * ib.cx - rb.x * ib.cy;
+  T m = ma + mb;
+  T kxx = (axy * ra.z - axz * ra.y) + (bxy * rb.z - bxz * rb.y) + m;
+  T kyy = (ay.z * ra.x - ay.x * ra.z) + (by.z * rb.x - by.x * rb.z) + m;
+  T kzz = (az.x * ra.y - az.y * ra.x) + (bz.x * rb.y - bz.y * rb.x) + m;
+  T kxy = (ay.y * ra.z - ay.z * ra.y) + (by.y * rb.z - by.z * rb.y);
+  T kxz = (az.y * ra.z - az.z * ra.y) + (bz.y * rb.z - bz.z * rb.y);
+  T kyz = (az.z * ra.x - az.x * ra.z) + (bz.z * rb.x - bz.x * rb.z);
+  T cxx = kyy * kzz - kyz * kyz;
+  T cyy = kxx * kzz - kxz * kxz;
+  T czz = kxx * kyy - kxy * kxy;
+  T cxy = kxz * kyz - kxy * kzz;
+  T cxz = kxy * kyz - kyy * kxz;
+  T cyz = kxy * kxz - kxx * kyz;
+  T d = kxx * cxx + kxy * cxy + kxz * cxz;
+  if (tabs(d) > T(1000.0f * kMinPositive)) {
+    T inv = T(1.0f) / d;
+    return tv3<T>(inv * (cxx * rhs.x + cxy * rhs.y + cxz * rhs.z), inv * (cxy * rhs.x + cyy * rhs.y + cyz * rhs.z),
+                  inv * (cxz * rhs.x + cyz * rhs.y + czz * rhs.z));
+  }
+  return tzero3<T>();
+}
+template <class T, class In> NSD_HD TM3<T> in_m3(const In& x, int i) {
+  return tm3<T>(in3<T>(x, i), in3<T>(x, i + 3), in3<T>(x, i + 6));
+}
+template <class T> NSD_HD TQ<T> tq(const Q& q) { return tquat<T>(tv3<T>(q.v), T(q.s)); }
+template <class T> NSD_HD TV3<T> half_perp(const TQ<T>& qa, const TQ<T>& rq, int axis) {
+  TV3<T> e = tv3<T>(T(axis == 0 ? 1.0f : 0.0f), T(axis == 1 ? 1.0f : 0.0f), T(0.0f));
+  return T(0.5f) * rotate(qa, rq.s * e + cross(rq.v, e));
+}
+
+// solve_joint (revolute_joint.rs:316): spring, motor and limits on the axial row, the two
+// perpendicular angular rows, then the point constraint.
+template <class T, class In>
+NSD_HD void joint_solve_fn(const In& x, const JParams& jp, T* y) {
+  T mA = x(jxIma), mB = x(jxImb);
+  TM3<T> iA = in_m3<T>(x, jxIA), iB = in_m3<T>(x, jxIB);
+  TV3<T> va = in3<T>(x, jxVA), wa = in3<T>(x, jxWA), vb = in3<T>(x, jxVB), wb = in3<T>(x, jxWB);
+  TQ<T> dqa = in4<T>(x, jxDqA), dqb = in4<T>(x, jxDqB);
+  TQ<T> qa = mul_quat(dqa, in4<T>(x, jxFqA));
+  TQ<T> qb = mul_quat(dqb, in4<T>(x, jxFqB));
+  if (dot_quat(qa, qb) < T(0.0f)) qb = tquat<T>(tv3<T>(-qb.v.x, -qb.v.y, -qb.v.z), -qb.s);
+  TQ<T> rq = inv_mul_quat(qa, qb);
+  TV3<T> lin = in3<T>(x, jxLin);
+  T p0 = x(jxPerp), p1 = x(jxPerp + 1);
+  T spring = x(jxSpring), motor = x(jxMotor), lower = x(jxLower), upper = x(jxUpper);
+  TV3<T> px = in3<T>(x, jxPx), py = in3<T>(x, jxPy);
+  const T zero = T(0.0f), one = T(1.0f);
+  if (!jp.fixed && (jp.spring || jp.motor || jp.limit)) {
+    TV3<T> axis = in3<T>(x, jxAxis);
+    T axial = x(jxAxial);
+    TV3<T> ga = mul_mv(iA, axis), gb = mul_mv(iB, axis);
+    T k = dot(axis, ga + gb);
+    T acd = dot(wb - wa, axis);
+    T ai = zero;
+    if (jp.spring) {
+      T angle = t_twist_angle(rq);
+      T c = angle - T(jp.target);
+      T bias = T(jp.ss.bias_rate) * c;
+      T ms = T(jp.ss.mass_scale), is = T(jp.ss.impulse_scale);
+      T di = -ms * axial * (acd + bias) - is * spring;
+      spring = spring + di;
+      acd = acd + k * di;
+      ai = ai + di;
+    }
+    if (jp.motor) {
+      T cdot = acd - T(jp.motor_speed);
+      T old = motor;
+      T mx = T(jp.max_torque_h);
+      T di = tclamp(-axial * cdot, -mx - old, mx - old);
+      motor = old + di;
+      acd = acd + k * di;
+      ai = ai + di;
+    }
+    if (jp.limit) {
+      T angle = t_twist_angle(rq);
+      {
+        T c = angle - T(jp.lower);
+        T bias = zero, ms = one, is = zero;
+        if (c > zero) bias = c * T(jp.inv_h);
+        else if (jp.use_bias) { bias = T(jp.cs.bias_rate) * c; ms = T(jp.cs.mass_scale); is = T(jp.cs.impulse_scale); }
+        T old = lower;
+        T di = tmax(-ms * axial * (acd + bias) - is * old, -old);
+        lower = old + di;
+        acd = acd + k * di;
+        ai = ai + di;
+      }
+      {
+        T c = T(jp.upper) - angle;
+        T bias = zero, ms = one, is = zero;
+        if (c > zero) bias = c * T(jp.inv_h);
+        else if (jp.use_bias) { bias = T(jp.cs.bias_rate) * c; ms = T(jp.cs.mass_scale); is = T(jp.cs.impulse_scale); }
+        T cdot = -acd;
+        T old = upper;
+        T di = tmax(-ms * axial * (cdot + bias) - is * old, -old);
+        upper = old + di;
+        ai = ai - di;
+      }
+    }
+    wa = wa - ai * ga;
+    wb = wb + ai * gb;
+  }
+  if (!jp.fixed) {
+    T bx = zero, by = zero, ms = one, is = zero;
+    if (jp.use_bias) {
+      bx = T(jp.cs.bias_rate) * rq.v.x;
+      by = T(jp.cs.bias_rate) * rq.v.y;
+      ms = T(jp.cs.mass_scale);
+      is = T(jp.cs.impulse_scale);
+    }
+    px = half_perp(qa, rq, 0);
+    py = half_perp(qa, rq, 1);
+    TM3<T> sum = tm3<T>(iA.cx + iB.cx, iA.cy + iB.cy, iA.cz + iB.cz);
+    T kxx = dot(px, mul_mv(sum, px));
+    T kyy = dot(py, mul_mv(sum, py));
+    T kxy = dot(px, mul_mv(sum, py));
+    TV3<T> wr = wb - wa;
+    T rx = dot(wr, px) + bx, ry = dot(wr, py) + by;
+    T sx = zero, sy = zero;
+    T d = kxx * kyy - kxy * kxy;
+    if (d > T(1000.0f * kMinPositive)) {
+      T inv = one / d;
+      sx = inv * kyy * rx - inv * kxy * ry;
+      sy = -inv * kxy * rx + inv * kxx * ry;
+    }
+    T dix = (-ms) * sx - is * p0, diy = (-ms) * sy - is * p1;
+    p0 = p0 + dix;
+    p1 = p1 + diy;
+    TV3<T> ang = dix * px + diy * py;
+    wa = wa - mul_mv(iA, ang);
+    wb = wb + mul_mv(iB, ang);
+  }
+  {
+    TV3<T> ra = rotate(dqa, in3<T>(x, jxFpA)), rb = rotate(dqb, in3<T>(x, jxFpB));
+    TV3<T> cdot = (vb + cross(wb, rb)) - va - cross(wa, ra);
+    TV3<T> bias = tzero3<T>();
+    T ms = one, is = zero;
+    if (jp.use_bias) {
+      TV3<T> sep = ((in3<T>(x, jxDpB) - in3<T>(x, jxDpA)) + (rb - ra)) + in3<T>(x, jxDc);
+      bias = T(jp.cs.bias_rate) * sep;
+      ms = T(jp.cs.mass_scale);
+      is = T(jp.cs.impulse_scale);
+    }
+    TV3<T> b = t_solve_point_constraint(mA, mB, iA, iB, ra, rb, cdot + bias);
+    TV3<T> imp = (-ms) * b - is * lin;
+    lin = lin + imp;
+    va = va - mA * imp;
+    wa = wa - mul_mv(iA, cross(ra, imp));
+    vb = vb + mB * imp;
+    wb = wb + mul_mv(iB, cross(rb, imp));
+  }
+  out3(y, 0, va); out3(y, 3, wa); out3(y, 6, vb); out3(y, 9, wb);
+  out3(y, 12, lin);
+  y[15] = p0; y[16] = p1; y[17] = spring; y[18] = motor; y[19] = lower; y[20] = upper;
+  out3(y, 21, px); out3(y, 24, py);
+}
+
+// joint_warm_delta (revolute_joint.rs:261): outputs dva 0..2, dwa 3..5, dvb 6..8, dwb 9..11
+// (body A takes v - dva, w - dwa; body B v + dvb, w + dwb).
+template <class T, class In>
+NSD_HD void joint_warm_fn(const In& x, T* y) {
+  T mA = x(jxIma), mB = x(jxImb);
+  TM3<T> iA = in_m3<T>(x, jxIA), iB = in_m3<T>(x, jxIB);
+  TV3<T> ra = rotate(in4<T>(x, jxDqA), in3<T>(x, jxFpA)), rb = rotate(in4<T>(x, jxDqB), in3<T>(x, jxFpB));
+  T axial = ((x(jxSpring) + x(jxMotor)) + x(jxLower)) - x(jxUpper);
+  TV3<T> ang = x(jxPerp) * in3<T>(x, jxPx) + x(jxPerp + 1) * in3<T>(x, jxPy);
+  ang = mul_add(ang, axial, in3<T>(x, jxAxis));
+  TV3<T> lin = in3<T>(x, jxLin);
+  out3(y, 0, mA * lin);
+  out3(y, 3, mul_mv(iA, cross(ra, lin) + ang));
+  out3(y, 6, mB * lin);
+  out3(y, 9, mul_mv(iB, cross(rb, lin) + ang));
+}
+
+// k_prepare_joints (revolute_joint.rs:183, distance_joint_solver.rs:74): the constants and the
+// prepare's perp axes from the bodies' poses, inverse masses and world inverse inertias. Inputs:
+// qa 0..3, qb 4..7, tangents of centre A 8..10 and B 11..13, inverse masses 14, 15, inverse
+// inertias 16..24, 25..33. Outputs: the joint vector from jxPx on (perp axes, then constants).
+enum JPI : int { jpQa = 0, jpQb = 4, jpCa = 8, jpCb = 11, jpIma = 14, jpImb = 15, jpIA = 16, jpIB = 25, kJPI = 34 };
+constexpr int kJPO = kJX - jxPx;
+template <class T, class In>
+NSD_HD void joint_prepare_fn(const In& x, const Xf& lfa, const Xf& lfb, V3 lca, V3 lcb, const Pos& ca, const Pos& cb,
+                             T* y) {
+  TQ<T> qa = in4<T>(x, jpQa), qb = in4<T>(x, jpQb);
+  TM3<T> iA = in_m3<T>(x, jpIA), iB = in_m3<T>(x, jpIB);
+  TQ<T> fqa = mul_quat(qa, tq<T>(lfa.q)), fqb = mul_quat(qb, tq<T>(lfb.q));
+  TV3<T> fpa = rotate(qa, tv3<T>(lfa.p - lca)), fpb = rotate(qb, tv3<T>(lfb.p - lcb));
+  TV3<T> dc = sub_pos_t(cb, ca, in3<T>(x, jpCb), in3<T>(x, jpCa));
+  TV3<T> axis = rotate(fqa, tv3<T>(T(0.0f), T(0.0f), T(1.0f)));
+  TM3<T> sum = tm3<T>(iA.cx + iB.cx, iA.cy + iB.cy, iA.cz + iB.cz);
+  T k = dot(axis, mul_mv(sum, axis));
+  T axial = k > T(0.0f) ? T(1.0f) / k : T(0.0f);
+  TQ<T> rq = inv_mul_quat(fqa, fqb);
+  // output i holds joint-vector entry jxPx + i
+  out3(y, jxPx - jxPx, half_perp(fqa, rq, 0));
+  out3(y, jxPy - jxPx, half_perp(fqa, rq, 1));
+  y[jxIma - jxPx] = x(jpIma);
+  y[jxImb - jxPx] = x(jpImb);
+  for (int i = 0; i < 9; ++i) { y[jxIA - jxPx + i] = x(jpIA + i); y[jxIB - jxPx + i] = x(jpIB + i); }
+  out4(y, jxFqA - jxPx, fqa); out4(y, jxFqB - jxPx, fqb);
+  out3(y, jxFpA - jxPx, fpa); out3(y, jxFpB - jxPx, fpb);
+  out3(y, jxAxis - jxPx, axis);
+  y[jxAxial - jxPx] = axial;
+  out3(y, jxDc - jxPx, dc);
+}
+
 }  // namespace ad
 }  // namespace nsd

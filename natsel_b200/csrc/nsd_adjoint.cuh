@@ -38,6 +38,10 @@ struct StepTape {
   float4* fin;       // [cap]: friction impulse x, y and twist after the solve
   uint8_t* mode;     // [cap]: narrowphase 0 none/disjoint, 1 recycled, 2 new manifold, 3 no points
   float4* rest;      // [iteration][6][cap]: the inputs of each restitution update (SolveTape::rest)
+  DJoint* joints;    // [n_joints] after prepare
+  float4* joint;     // [substep][2][6][n_joints]: each joint solve's inputs (SolveTape::joint)
+  float4* jwarm;     // [substep][4][n_joints]: the state each relax leaves for the next warm start
+  int n_joints;
   int rest_iterations;
   int substeps;
 };
@@ -61,7 +65,11 @@ struct AdjBufs {
   float* restb;  // [4][cap]: the points' restitution impulses
   float* relb; // [4][cap]: the points' relative normal velocities at prepare
   int* mismatch;  // narrowphase replays that did not reproduce the forward manifold
-  int cap, n_awake;
+  float* jb;     // [n_joints][kJState]: the joints' impulses and perp axes
+  float* jc;     // [n_joints][kJConst]: the joints' prepared constants (this step)
+  const int* joint_list;  // joints by colour (world constant)
+  JointRanges jr;
+  int cap, n_awake, n_joints;
 };
 
 constexpr int kAdjThreads = 256;
@@ -72,6 +80,8 @@ __device__ __forceinline__ float& PB(const AdjBufs& a, int i, int f) { return a.
 __device__ __forceinline__ float& KB(const AdjBufs& a, int k, int cv) { return a.kb[(size_t)(cv - ad::cvLam) * a.cap + k]; }
 __device__ __forceinline__ float& MB(const AdjBufs& a, int c, int f) { return a.mb[(size_t)f * a.cap + c]; }
 __device__ __forceinline__ void put3(float* x, int at, V3 v) { x[at] = v.x; x[at + 1] = v.y; x[at + 2] = v.z; }
+__device__ __forceinline__ float& JB(const AdjBufs& a, int j, int f) { return a.jb[(size_t)j * ad::kJState + f]; }
+__device__ __forceinline__ float& JC(const AdjBufs& a, int j, int f) { return a.jc[(size_t)j * ad::kJConst + f]; }
 __device__ __forceinline__ float& TOTB(const AdjBufs& a, int k, int q) { return a.totb[(size_t)q * a.cap + k]; }
 __device__ __forceinline__ float& RESTB(const AdjBufs& a, int k, int q) { return a.restb[(size_t)q * a.cap + k]; }
 __device__ __forceinline__ float& RELB(const AdjBufs& a, int k, int q) { return a.relb[(size_t)q * a.cap + k]; }
@@ -519,11 +529,196 @@ __global__ void k_adj_relvel(StepTape t, AdjBufs a, int n_slots) {
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Revolute joints: one warp per joint evaluates the restatement (nsd_ad.cuh joint_solve_fn,
+// joint_warm_fn, joint_prepare_fn) on dual numbers, lane l seeding input directions l, l + 32
+// and l + 64, and contracts the output tangents with the outputs' cotangents.
+
+__device__ ad::JParams joint_params(const DJoint& j, const StepParams& p, bool use_bias) {
+  ad::JParams jp;
+  jp.use_bias = use_bias;
+  jp.fixed = j.fixed_rotation != 0;
+  jp.spring = j.enable_spring != 0;
+  jp.motor = j.enable_motor != 0;
+  jp.limit = j.enable_limit != 0;
+  jp.cs = j.constraint_softness;
+  jp.ss = j.spring_softness;
+  jp.target = j.target_angle;
+  jp.lower = j.lower_angle;
+  jp.upper = j.upper_angle;
+  jp.motor_speed = j.motor_speed;
+  jp.max_torque_h = j.max_motor_torque * p.h;
+  jp.inv_h = p.inv_h;
+  return jp;
+}
+// The prepared constants of the joint vector (jxIma on)
+__device__ void joint_consts(const DJoint& j, float* x) {
+  using namespace ad;
+  x[jxIma] = j.inv_mass_a;
+  x[jxImb] = j.inv_mass_b;
+  put3(x, jxIA, j.inv_ia.cx); put3(x, jxIA + 3, j.inv_ia.cy); put3(x, jxIA + 6, j.inv_ia.cz);
+  put3(x, jxIB, j.inv_ib.cx); put3(x, jxIB + 3, j.inv_ib.cy); put3(x, jxIB + 6, j.inv_ib.cz);
+  put3(x, jxFqA, j.frame_a.q.v); x[jxFqA + 3] = j.frame_a.q.s;
+  put3(x, jxFqB, j.frame_b.q.v); x[jxFqB + 3] = j.frame_b.q.s;
+  put3(x, jxFpA, j.frame_a.p);
+  put3(x, jxFpB, j.frame_b.p);
+  put3(x, jxAxis, j.rotation_axis_z);
+  x[jxAxial] = j.axial_mass;
+  put3(x, jxDc, j.delta_center);
+}
+// A body's position and rotation increments from body row `row` of substep `sub` (identity for
+// a static body)
+__device__ void joint_body_deltas(const StepTape& t, int n, int sub, int row, int b, float* x, int at_dp, int at_dq) {
+  V3 dp = v3(0, 0, 0);
+  Q dq = qid();
+  if (b >= 0) {
+    const DState& st = t.body[((size_t)sub * 3 + row) * n + b];
+    dp = st.dp;
+    dq = st.dq;
+  }
+  put3(x, at_dp, dp);
+  put3(x, at_dq, dq.v);
+  x[at_dq + 3] = dq.s;
+}
+
+// Reverse of one joint's push (use_bias) or relax solve at substep sub (one warp). Velocities'
+// and impulses' cotangents are replaced (the solve updates them), the perp axes' too (the solve
+// recomputes them), position and rotation increments' and the constants' accumulated.
+__device__ void adj_joint_solve(const StepTape& t, const AdjBufs& a, const StepParams& p, int stage, int sub, int ji,
+                                int lane, float* xs, float* ys) {
+  using namespace ad;
+  const DJoint& j = t.joints[ji];
+  const int ia = j.index_a, ib = j.index_b, n = a.n_awake;
+  const size_t nj = (size_t)a.n_joints;
+  if (lane == 0) {
+    const float4* rows = t.joint + (size_t)(sub * 2 + (stage == kRelax ? 1 : 0)) * 6 * nj;
+    float4 r[6];
+    for (int q = 0; q < 6; ++q) r[q] = rows[q * nj + ji];
+    xs[jxVA] = r[0].x; xs[jxVA + 1] = r[0].y; xs[jxVA + 2] = r[0].z; xs[jxLin] = r[0].w;
+    xs[jxWA] = r[1].x; xs[jxWA + 1] = r[1].y; xs[jxWA + 2] = r[1].z; xs[jxLin + 1] = r[1].w;
+    xs[jxVB] = r[2].x; xs[jxVB + 1] = r[2].y; xs[jxVB + 2] = r[2].z; xs[jxLin + 2] = r[2].w;
+    xs[jxWB] = r[3].x; xs[jxWB + 1] = r[3].y; xs[jxWB + 2] = r[3].z; xs[jxPerp] = r[3].w;
+    xs[jxPerp + 1] = r[4].x; xs[jxSpring] = r[4].y; xs[jxMotor] = r[4].z; xs[jxLower] = r[4].w;
+    xs[jxUpper] = r[5].x;
+    const int row = stage == kRelax ? 2 : 1;  // push after integrate velocities, relax after positions
+    joint_body_deltas(t, n, sub, row, ia, xs, jxDpA, jxDqA);
+    joint_body_deltas(t, n, sub, row, ib, xs, jxDpB, jxDqB);
+    // the solve recomputes the perp axes (unless the rotation is fixed, when nothing reads them)
+    put3(xs, jxPx, j.perp_axis_x);
+    put3(xs, jxPy, j.perp_axis_y);
+    joint_consts(j, xs);
+  }
+  if (lane < 12) {
+    const int b = lane < 6 ? ia : ib, g = lane % 6;
+    ys[lane] = b >= 0 ? BB(a, b, g < 3 ? g : g + 1) : 0.0f;
+  } else if (lane < kJSolveOut) {
+    ys[lane] = JB(a, ji, lane - 12);
+  }
+  __syncwarp();
+  const JParams jp = joint_params(j, p, stage == kPush);
+  SeedIn<float, 3> in;
+  in.x = xs;
+  for (int kk = 0; kk < 3; ++kk) in.dir[kk] = lane + 32 * kk < kJX ? lane + 32 * kk : -1;
+  Dual<float, 3> y[kJSolveOut];
+  joint_solve_fn(in, jp, y);
+  float xb[3];
+  for (int kk = 0; kk < 3; ++kk) {
+    float acc = 0.0f;
+    for (int q = 0; q < kJSolveOut; ++q) acc += ys[q] * y[q].d[kk];
+    xb[kk] = acc;
+  }
+  __syncwarp();
+  for (int kk = 0; kk < 3; ++kk) {
+    const int d = in.dir[kk];
+    if (d < 0) continue;
+    const float v = xb[kk];
+    if (d < jxDpA) {
+      const int b = d < 6 ? ia : ib, g = d % 6;
+      if (b >= 0) BB(a, b, g < 3 ? g : g + 1) = v;
+    } else if (d < jxDpB) {
+      if (ia >= 0) BB(a, ia, 8 + d - jxDpA) += v;
+    } else if (d < jxDqA) {
+      if (ib >= 0) BB(a, ib, 8 + d - jxDpB) += v;
+    } else if (d < jxDqB) {
+      if (ia >= 0) BB(a, ia, 12 + d - jxDqA) += v;
+    } else if (d < jxLin) {
+      if (ib >= 0) BB(a, ib, 12 + d - jxDqB) += v;
+    } else if (d < jxIma) {
+      JB(a, ji, d - jxLin) = v;
+    } else {
+      JC(a, ji, d - jxIma) += v;
+    }
+  }
+}
+
+// Reverse of one joint's part of the warm start of substep sub (one warp): the change it made
+// to its bodies' velocities depends on the impulses and perp axes the previous relax left (or
+// prepare, for the first substep), the rotation increments and the constants. The bodies'
+// velocity cotangents are only read; several joints share a body in this phase, so its rotation
+// increments' cotangents are added atomically.
+__device__ void adj_joint_warm(const StepTape& t, const AdjBufs& a, int sub, int ji, int lane, float* xs, float* ys) {
+  using namespace ad;
+  const DJoint& j = t.joints[ji];
+  const int ia = j.index_a, ib = j.index_b, n = a.n_awake;
+  const size_t nj = (size_t)a.n_joints;
+  if (lane == 0) {
+    for (int f = 0; f < jxDpA; ++f) xs[f] = 0.0f;
+    if (sub == 0) {
+      put3(xs, jxLin, j.linear_impulse);
+      xs[jxPerp] = j.perp_impulse.x; xs[jxPerp + 1] = j.perp_impulse.y;
+      xs[jxSpring] = j.spring_impulse; xs[jxMotor] = j.motor_impulse;
+      xs[jxLower] = j.lower_impulse; xs[jxUpper] = j.upper_impulse;
+      put3(xs, jxPx, j.perp_axis_x);
+      put3(xs, jxPy, j.perp_axis_y);
+    } else {
+      const float4* rows = t.jwarm + (size_t)(sub - 1) * 4 * nj;
+      float4 r0 = rows[ji], r1 = rows[nj + ji], r2 = rows[2 * nj + ji], r3 = rows[3 * nj + ji];
+      xs[jxLin] = r0.x; xs[jxLin + 1] = r0.y; xs[jxLin + 2] = r0.z; xs[jxPerp] = r0.w;
+      xs[jxPerp + 1] = r1.x; xs[jxSpring] = r1.y; xs[jxMotor] = r1.z; xs[jxLower] = r1.w;
+      xs[jxUpper] = r2.x; xs[jxPx] = r2.y; xs[jxPx + 1] = r2.z; xs[jxPx + 2] = r2.w;
+      xs[jxPy] = r3.x; xs[jxPy + 1] = r3.y; xs[jxPy + 2] = r3.z;
+    }
+    joint_body_deltas(t, n, sub, 0, ia, xs, jxDpA, jxDqA);
+    joint_body_deltas(t, n, sub, 0, ib, xs, jxDpB, jxDqB);
+    joint_consts(j, xs);
+  }
+  // body A took v - dva, w - dwa; body B v + dvb, w + dwb (dynamic bodies only)
+  if (lane < 12) {
+    const int b = lane < 6 ? ia : ib, g = lane % 6;
+    const float sgn = lane < 6 ? -1.0f : 1.0f;
+    ys[lane] = b >= 0 ? sgn * BB(a, b, g < 3 ? g : g + 1) : 0.0f;
+  }
+  __syncwarp();
+  SeedIn<float, 3> in;
+  in.x = xs;
+  for (int kk = 0; kk < 3; ++kk) in.dir[kk] = lane + 32 * kk < kJX ? lane + 32 * kk : -1;
+  Dual<float, 3> y[12];
+  joint_warm_fn(in, y);
+  for (int kk = 0; kk < 3; ++kk) {
+    const int d = in.dir[kk];
+    if (d < jxDqA) continue;  // velocities and position increments: not read
+    float v = 0.0f;
+    for (int q = 0; q < 12; ++q) v += ys[q] * y[q].d[kk];
+    if (d < jxDqB) {
+      if (ia >= 0) atomicAdd(&BB(a, ia, 12 + d - jxDqA), v);
+    } else if (d < jxLin) {
+      if (ib >= 0) atomicAdd(&BB(a, ib, 12 + d - jxDqB), v);
+    } else if (d < jxIma) {
+      JB(a, ji, d - jxLin) += v;
+    } else {
+      JC(a, ji, d - jxIma) += v;
+    }
+  }
+  __syncwarp();
+}
+
 // Reverse of the solver stages of one step: a persistent launch over the same barriers as the
 // forward solver, phases in reverse order, one thread per constraint or body.
 template <bool kGrid>
 __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBufs a, StepParams p, Control* ctl) {
   __shared__ int coff[25];
+  __shared__ float jxs[kAdjThreads / 32][ad::kJX];
+  __shared__ float jys[kAdjThreads / 32][ad::kJSolveOut];
   if (threadIdx.x < 24) coff[threadIdx.x] = t.ctl->color_offset[threadIdx.x];
   if (threadIdx.x == 24) coff[24] = t.ctl->color_offset[23];
   __syncthreads();
@@ -531,12 +726,18 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
   // items dealt 32 at a time across the blocks, as in the forward solver
   const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
   const int stride = gridDim.x * blockDim.x;
+  // joints: one warp each
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wg = blockIdx.x * (blockDim.x >> 5) + wib, wstride = gridDim.x * (blockDim.x >> 5);
   int bar = 0;
   auto contacts = [&](auto stage_tag, int sub) -> bool {
     constexpr int Stage = decltype(stage_tag)::value;
     for (int c = kOverflowIndex - 1; c >= 0; --c) {
-      if (coff[c + 1] == coff[c]) continue;
+      const int j0 = a.jr.off[c], j1 = a.jr.off[c + 1];
+      if (coff[c + 1] == coff[c] && j1 == j0) continue;
       for (int k = coff[c] + g; k < coff[c + 1]; k += stride) adj_contact<Stage>(t, a, p, n, k, sub);
+      for (int q = j0 + wg; q < j1; q += wstride)
+        adj_joint_solve(t, a, p, Stage, sub, a.joint_list[q], lane, jxs[wib], jys[wib]);
       if (!phase_sync<kGrid>(ctl, bar)) return false;
     }
     return true;
@@ -550,6 +751,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
     // cotangents as they are and only reads them: every colour's warm start reverses in one
     // phase, before integrate-velocities changes those cotangents.
     for (int k = g; k < coff[kOverflowIndex]; k += stride) adj_contact<kWarm>(t, a, p, n, k, sub);
+    for (int q = wg; q < a.n_joints; q += wstride) adj_joint_warm(t, a, sub, q, lane, jxs[wib], jys[wib]);
     if (!phase_sync<kGrid>(ctl, bar)) return;
     for (int i = g; i < n; i += stride) adj_iv(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
@@ -636,6 +838,69 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_prepare(StepTape t, AdjBufs
       }
     }
   }
+}
+
+// Reverse of the joints' prepare (one warp per joint): the constants' and the prepared perp axes'
+// cotangents -> the bodies' rotations and centres, inverse masses and world inverse inertias.
+// Then the joint's cotangents are made those of the previous step's end: the impulses carry
+// over (prepare keeps them, or zeroes them without warm starting), the perp axes and the
+// constants start afresh.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_joint_prepare(StepTape t, AdjBufs a, DW w, StepParams p) {
+  using namespace ad;
+  __shared__ float xs_s[kAdjThreads / 32][kJPI];
+  __shared__ float ys_s[kAdjThreads / 32][kJPO];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ji = blockIdx.x * (kAdjThreads / 32) + warp;
+  if (ji >= a.n_joints) return;
+  float* xs = xs_s[warp];
+  float* ys = ys_s[warp];
+  const DJoint& j = t.joints[ji];
+  auto sim_for = [&](int enc) -> const DSim& { return enc >= 0 ? t.sims[enc] : w.ssims[-enc - 2]; };
+  const DSim& sa = sim_for(j.enc_a);
+  const DSim& sb = sim_for(j.enc_b);
+  if (lane == 0) {
+    xs[jpQa] = sa.q.v.x; xs[jpQa + 1] = sa.q.v.y; xs[jpQa + 2] = sa.q.v.z; xs[jpQa + 3] = sa.q.s;
+    xs[jpQb] = sb.q.v.x; xs[jpQb + 1] = sb.q.v.y; xs[jpQb + 2] = sb.q.v.z; xs[jpQb + 3] = sb.q.s;
+    for (int f = 0; f < 6; ++f) xs[jpCa + f] = 0.0f;
+    xs[jpIma] = sa.inv_mass;
+    xs[jpImb] = sb.inv_mass;
+    put3(xs, jpIA, sa.inv_inertia_world.cx); put3(xs, jpIA + 3, sa.inv_inertia_world.cy);
+    put3(xs, jpIA + 6, sa.inv_inertia_world.cz);
+    put3(xs, jpIB, sb.inv_inertia_world.cx); put3(xs, jpIB + 3, sb.inv_inertia_world.cy);
+    put3(xs, jpIB + 6, sb.inv_inertia_world.cz);
+  }
+  for (int f = lane; f < kJPO; f += 32) ys[f] = f < 6 ? JB(a, ji, jxPx - jxLin + f) : JC(a, ji, f - 6);
+  __syncwarp();
+  SeedIn<float, 2> in;
+  in.x = xs;
+  in.dir[0] = lane;
+  in.dir[1] = lane + 32 < kJPI ? lane + 32 : -1;
+  Dual<float, 2> y[kJPO];
+  const Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
+  joint_prepare_fn(in, j.local_frame_a, j.local_frame_b, sa.local_center, sb.local_center, ca, cb, y);
+  const int ia = j.enc_a >= 0 ? j.enc_a : -1, ib = j.enc_b >= 0 ? j.enc_b : -1;
+  for (int kk = 0; kk < 2; ++kk) {
+    const int d = in.dir[kk];
+    if (d < 0) continue;
+    float v = 0.0f;
+    for (int q = 0; q < kJPO; ++q) v += ys[q] * y[q].d[kk];
+    if (v == 0.0f) continue;
+    if (d < jpQb) { if (ia >= 0) atomicAdd(&CQ(a, ia, 4 + d - jpQa), v); }
+    else if (d < jpCa) { if (ib >= 0) atomicAdd(&CQ(a, ib, 4 + d - jpQb), v); }
+    else if (d < jpCb) { if (ia >= 0) atomicAdd(&CQ(a, ia, d - jpCa), v); }
+    else if (d < jpIma) { if (ib >= 0) atomicAdd(&CQ(a, ib, d - jpCb), v); }
+    else if (d == jpIma) { if (ia >= 0) atomicAdd(&PB(a, ia, pbInvMass), v); }
+    else if (d == jpImb) { if (ib >= 0) atomicAdd(&PB(a, ib, pbInvMass), v); }
+    else if (d < jpIB) { if (ia >= 0) atomicAdd(&PB(a, ia, pbIiw + d - jpIA), v); }
+    else { if (ib >= 0) atomicAdd(&PB(a, ib, pbIiw + d - jpIB), v); }
+  }
+  __syncwarp();
+  // the previous step's end: impulses carry over unless prepare zeroed them
+  for (int f = lane; f < kJState; f += 32) {
+    const bool impulse = f < jxPx - jxLin;
+    if (!impulse || p.warm_start == 0.0f) JB(a, ji, f) = 0.0f;
+  }
+  for (int f = lane; f < kJConst; f += 32) JC(a, ji, f) = 0.0f;
 }
 
 // Reverse of the inverse world inertia of finalize (one warp per body, lanes 0..12).

@@ -1097,7 +1097,34 @@ struct SolveTape {
   float4* fin;     // [cap]
   float4* rest;    // [iteration][6][cap]: vA|l0, wA|l1, vB|l2, wB|l3, the points' total normal
                    // impulses, their restitution impulses (before each restitution update)
+  float4* joint;   // [substep][push, relax][6][n_joints]: vA|lin.x, wA|lin.y, vB|lin.z, wB|perp.x,
+                   // perp.y spring motor lower, upper (before each joint solve)
+  float4* jwarm;   // [substep][4][n_joints]: the state the next substep's warm start reads, after
+                   // relax: lin|perp.x, perp.y spring motor lower, upper|px, py|0
 };
+
+// A revolute joint's inputs before a push or relax solve (the adjoint replays it)
+__device__ __forceinline__ void tape_joint(const DW& w, const SolveTape& tp, int sub, int stage, int ji,
+                                           const DJoint& j) {
+  const size_t nj = (size_t)w.n_joints;
+  const DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
+  float4* rows = tp.joint + (size_t)(sub * 2 + (stage == kRelax ? 1 : 0)) * 6 * nj;
+  rows[ji] = make_float4(sa.v.x, sa.v.y, sa.v.z, j.linear_impulse.x);
+  rows[nj + ji] = make_float4(sa.w.x, sa.w.y, sa.w.z, j.linear_impulse.y);
+  rows[2 * nj + ji] = make_float4(sb.v.x, sb.v.y, sb.v.z, j.linear_impulse.z);
+  rows[3 * nj + ji] = make_float4(sb.w.x, sb.w.y, sb.w.z, j.perp_impulse.x);
+  rows[4 * nj + ji] = make_float4(j.perp_impulse.y, j.spring_impulse, j.motor_impulse, j.lower_impulse);
+  rows[5 * nj + ji] = make_float4(j.upper_impulse, 0.0f, 0.0f, 0.0f);
+}
+// A joint's state after a relax solve, which the warm start of the next substep reads
+__device__ __forceinline__ void tape_joint_warm(const DW& w, const SolveTape& tp, int sub, int ji, const DJoint& j) {
+  const size_t nj = (size_t)w.n_joints;
+  float4* rows = tp.jwarm + (size_t)sub * 4 * nj;
+  rows[ji] = make_float4(j.linear_impulse.x, j.linear_impulse.y, j.linear_impulse.z, j.perp_impulse.x);
+  rows[nj + ji] = make_float4(j.perp_impulse.y, j.spring_impulse, j.motor_impulse, j.lower_impulse);
+  rows[2 * nj + ji] = make_float4(j.upper_impulse, j.perp_axis_x.x, j.perp_axis_x.y, j.perp_axis_x.z);
+  rows[3 * nj + ji] = make_float4(j.perp_axis_y.x, j.perp_axis_y.y, j.perp_axis_y.z, 0.0f);
+}
 
 __device__ __forceinline__ void tape_restitution(const DW& w, const SolveTape& tp, int it, int k, const CData& d) {
   const int cap = w.cp.cap;
@@ -1249,8 +1276,11 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
         run_contact(w, p, k, stage, d, warm_color);
       }
       for (int tj = g; stage != kRestitution && tj < nj; tj += stride) {
-        DJoint& j = w.joints[w.joint_list[jr.off[c] + tj]];
+        const int ji = w.joint_list[jr.off[c] + tj];
+        DJoint& j = w.joints[ji];
+        if (kTape && tp.joint && s < main_phases) tape_joint(w, tp, sub, stage, ji, j);
         solve_joint(w, p, j, stage == kPush);
+        if (kTape && tp.joint && warm_color >= 0) tape_joint_warm(w, tp, sub, ji, j);
         if (warm_color >= 0) {
           DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
           put_warm_delta(w, j.index_a, j.index_b, c, joint_warm_delta(j, sa.dq, sb.dq));

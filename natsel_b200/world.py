@@ -485,7 +485,7 @@ ADJOINT_CHECKS = ["warm_start", "push", "relax", "prepare", "integrate_velocitie
                   "warm_start_reverse_sweep", "push_reverse_sweep", "relax_reverse_sweep",
                   "integrate_positions_reverse_sweep", "integrate_velocities_reverse_sweep", "restitution",
                   "relative_velocity_reverse_sweep", "sphere_sphere", "capsule_sphere", "capsule_capsule",
-                  "box_sphere", "box_capsule"]
+                  "box_sphere", "box_capsule", "joint_solve", "joint_warm_start", "joint_prepare"]
 
 
 def adjoint_selfcheck(which, seed):

@@ -72,3 +72,12 @@ def test_round_manifold_vjp_matches_central_differences(which):
         assert seen == {2, 4}, seen  # distance path and the centre inside the box
     if which == 23:
         assert seen == {2, 3, 4, 5}, seen
+
+
+@pytest.mark.parametrize("which", [24, 25, 26], ids=["joint_solve", "joint_warm_start", "joint_prepare"])
+def test_joint_vjp_matches_central_differences(which):
+    """Revolute joints (revolute_joint.rs:183-553): the solve with and without bias, with the
+    spring, the motor (clamped and not) and the limits in turn; the warm start; the prepare."""
+    for seed in range(12):
+        worst, _ = adjoint_selfcheck(which, seed)
+        assert 0.0 <= worst < 1e-6, (which, seed, worst)

@@ -3,7 +3,8 @@ differences of the forward step, and the tape's bookkeeping.
 
 The scenes keep one contact set over the horizon (boxes sliding and spinning on the ground, a
 box running into a lighter one, a box sliding on another, boxes bouncing off the ground and off
-each other with restitution, spheres and capsules sliding, rolling and colliding). Contact solves still have kinks (an
+each other with restitution, spheres and capsules sliding, rolling and colliding, a jointed double
+pendulum with a motor, limits and a spring, a hinged panel dragged along the ground). Contact solves still have kinks (an
 impulse meeting its clamp at zero, a corner point unloading); where one falls inside the
 difference interval the central difference does not converge, and below h ~ 1e-3 the f32
 rounding of the trajectory dominates it. So each entry is differenced at h and 2 h, and the
@@ -69,6 +70,28 @@ ROUND_COLLIDE = [
 ]
 
 
+# revolute joints: a double pendulum hanging from a static anchor (a motor and limits on the top
+# hinge, a spring on the lower one), and a panel hinged about a vertical axis to a box, both
+# sliding on the ground (joint and contact rows in the same colours)
+ID7 = (0.0, 0.0, 0.0, 1.0)
+UP = (-np.sqrt(0.5), 0.0, 0.0, np.sqrt(0.5))  # frame rotation taking the hinge axis z to y
+PENDULUM = [
+    ((0.0, 3.0, 0.0), (0.1, 0.1, 0.1), None, None, 0.0, 0.6),
+    ((0.0, 2.4, 0.0), (0.15, 0.5, 0.15), (1.2, 0.0, 0.3), (0.0, 0.0, 2.0), 1000.0, 0.6),
+    ((0.0, 1.5, 0.0), (0.15, 0.4, 0.15), (2.6, 0.0, 0.5), (0.0, 0.0, 1.0), 700.0, 0.6),
+    ("joint", 0, 1, (0.0, 0.0, 0.0) + ID7, (0.0, 0.6, 0.0) + ID7,
+     dict(enable_limit=True, lower=-1.2, upper=1.2, enable_motor=True, max_motor_torque=50.0, motor_speed=1.0)),
+    ("joint", 1, 2, (0.0, -0.5, 0.0) + ID7, (0.0, 0.4, 0.0) + ID7,
+     dict(enable_spring=True, hertz=2.0, damping_ratio=0.3)),
+]
+HINGED = [
+    ((0.0, 0.498, 0.0), (0.5, 0.5, 0.5), (1.5, 0.0, 0.0), (0.0, 0.5, 0.0), 1000.0, 0.6),
+    ((1.2, 0.398, 0.0), (0.6, 0.4, 0.1), (1.5, 0.0, 0.3), (0.0, 0.0, 0.0), 500.0, 0.5),
+    ("joint", 0, 1, (0.55, 0.0, 0.0) + UP, (-0.65, 0.1, 0.0) + UP,
+     dict(enable_spring=True, hertz=1.5, damping_ratio=0.5)),
+]
+
+
 def make_shape(w, b, he, **kw):
     if he[0] == "sphere":
         w.create_sphere(b, he[1], **kw)
@@ -88,20 +111,38 @@ def volume(he):
     return 8.0 * he[0] * he[1] * he[2]
 
 
+def body_rows(scene):
+    """A scene lists bodies (a None velocity makes a static anchor) and then joints:
+    ("joint", body index a, body index b, frame a, frame b, keyword arguments of create_revolute)."""
+    return [b for b in scene if b[0] != "joint"]
+
+
 def build(bodies, checkpoint=None, ground_friction=0.6):
     w = World(**WORLD)
     g = w.create_body(type=STATIC_BODY, position=(0.0, -0.5, 0.0))
     w.create_box(g, 20.0, 0.5, 20.0, friction=ground_friction)
-    for pos, he, v, om, rho, mu, *rest in bodies:
-        b = w.create_body(type=DYNAMIC_BODY, position=pos, linear_velocity=v, angular_velocity=om, enable_sleep=False)
-        make_shape(w, b, he, density=rho, friction=mu, restitution=rest[0] if rest else 0.0)
+    ids = []
+    for row in bodies:
+        if row[0] == "joint":
+            _, ia, ib, fa, fb, kw = row
+            w.create_revolute(ids[ia], ids[ib], fa, fb, **kw)
+            continue
+        pos, he, v, om, rho, mu, *rest = row
+        if v is None:
+            b = w.create_body(type=STATIC_BODY, position=pos)
+            make_shape(w, b, he, friction=mu)
+        else:
+            b = w.create_body(type=DYNAMIC_BODY, position=pos, linear_velocity=v, angular_velocity=om,
+                              enable_sleep=False)
+            make_shape(w, b, he, density=rho, friction=mu, restitution=rest[0] if rest else 0.0)
+        ids.append(b)
     if checkpoint is not None:
         w.tape_begin(checkpoint)
     return w
 
 
 def targets(bodies):
-    return np.array([[p[0] + 1.0, p[1], p[2] - 0.5] for p, *_ in bodies])
+    return np.array([[p[0] + 1.0, p[1], p[2] - 0.5] for p, *_ in body_rows(bodies)])
 
 
 def loss(bodies, steps=STEPS, ground_friction=0.6):
@@ -156,7 +197,9 @@ def check(bodies, ground_friction=0.6, h_scale=1.0):
     assert info[2] == 0, "narrowphase replay did not reproduce a recorded manifold"
     assert h0 == h1, "the adjoint must leave the world in its final state"
     rows = []  # kind, adjoint, fd(h), fd(2 h)
-    for i, (pos, he, v, om, rho, mu, *rest) in enumerate(bodies):
+    for i, (pos, he, v, om, rho, mu, *rest) in enumerate(body_rows(bodies)):
+        if v is None:
+            continue  # a static anchor
         vol = volume(he)
         entries = [("velocity", g["lin0"][i + 1, c], 2, c, 1e-3) for c in range(3)]
         entries += [("velocity", g["ang0"][i + 1, c], 3, c, 1e-3) for c in range(3)]
@@ -241,6 +284,18 @@ def test_round_shape_collisions_gradients_match_finite_differences():
         w.step(DT, SUBSTEPS)
     assert (np.abs(w.bodies()[2][[2, 4, 6], 0]) > 0.1).all()
     w.close()
+
+
+def test_jointed_pendulum_gradients_match_finite_differences():
+    rows, checked = check(PENDULUM)
+    assert checked_count(checked, "velocity") >= 4
+    assert checked_count(checked, "mass") >= 1
+
+
+def test_hinged_bodies_on_the_ground_gradients_match_finite_differences():
+    rows, checked = check(HINGED)
+    assert checked_count(checked, "velocity") >= 3
+    assert checked_count(checked, "friction") >= 1
 
 
 def test_spinning_box_rotation_gradient_matches_finite_differences():
@@ -331,6 +386,13 @@ def test_adjoint_scope_is_enforced():
         w.apply_forces(force=np.zeros((4, 3), np.float32))
     with pytest.raises(NsError):
         w.step(0.0, SUBSTEPS)
+    w.close()
+    # joints have an f32 device reverse only
+    w = build(PENDULUM, checkpoint=8)
+    w.step(DT, SUBSTEPS)
+    with pytest.raises(NsError) as e:
+        w.vjp_f64(dpos=np.ones((4, 3), np.float32))
+    assert e.value.code == 6 and "joints" in str(e.value)
     w.close()
     # restitution has an f32 device reverse only
     w = build(BOUNCE, checkpoint=8)
