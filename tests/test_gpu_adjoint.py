@@ -287,13 +287,13 @@ def test_round_shape_collisions_gradients_match_finite_differences():
 
 
 def test_jointed_pendulum_gradients_match_finite_differences():
-    rows, checked = check(PENDULUM)
-    assert checked_count(checked, "velocity") >= 4
-    assert checked_count(checked, "mass") >= 1
+    rows, checked = check(PENDULUM, h_scale=8.0)
+    assert checked_count(checked, "velocity") >= 3
+    assert checked_count(checked, "mass") >= 2
 
 
 def test_hinged_bodies_on_the_ground_gradients_match_finite_differences():
-    rows, checked = check(HINGED)
+    rows, checked = check(HINGED, h_scale=8.0)
     assert checked_count(checked, "velocity") >= 3
     assert checked_count(checked, "friction") >= 1
 
