@@ -388,8 +388,10 @@ int ensure_stack(ns_world* w) {
                            (const void*)k_prepare_overflow, (const void*)k_color_scatter, (const void*)k_prepare_slots,
                            (const void*)k_warm_slots,
                            (const void*)k_finalize, (const void*)k_continuous, (const void*)k_bullets, (const void*)k_state_pass,
-                           (const void*)k_adj_solve<true>, (const void*)k_adj_solve<false>,
-                           (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts};
+                           (const void*)k_adj_solve<true, false>, (const void*)k_adj_solve<false, false>,
+                           (const void*)k_adj_solve<true, true>, (const void*)k_adj_solve<false, true>,
+                           (const void*)k_adj_narrow, (const void*)k_adj_prepare, (const void*)k_adj_consts,
+                           (const void*)k_adj_restitution, (const void*)k_adj_joint_prepare};
   for (const void* k : kernels) {
     cudaError_t e = cudaFuncGetAttributes(&a, k);
     if (e != cudaSuccess) return fail(w, NS_ERR_CUDA, "cudaFuncGetAttributes: %s", cudaGetErrorString(e));
@@ -1165,7 +1167,8 @@ int alloc_tapes(ns_world* w, int count, int max_substeps, TapeSet* ts) {
 // The reverse solve runs on the forward solver's launch shape (one thread-block cluster, or a
 // cooperative grid when the world uses one): its phases are bounded by the barrier and one
 // warp's latency chain, and a grid over every SM measured 2.4x slower on the 1024-box rollout.
-int launch_adj_solve(ns_world* w, const StepTape& t, const AdjBufs& a, const StepParams& p) {
+template <bool kJoints>
+int launch_adj_solve_t(ns_world* w, const StepTape& t, const AdjBufs& a, const StepParams& p) {
   cudaLaunchConfig_t cfg = {};
   cfg.blockDim = dim3(kAdjThreads);
   cfg.stream = w->stream;
@@ -1173,13 +1176,13 @@ int launch_adj_solve(ns_world* w, const StepTape& t, const AdjBufs& a, const Ste
   int blocks = w->solver_blocks;
   if (w->solver_grid) {
     int per_sm = 0;
-    NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve<true>, kAdjThreads, 0));
+    NS_CUDA(w, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve<true, kJoints>, kAdjThreads, 0));
     blocks = std::max(1, std::min(blocks, per_sm * w->sm_count));
     NS_CUDA(w, cudaMemsetAsync(&w->dw.ctl->barrier_count, 0, sizeof(int), w->stream));
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
   } else {
-    NS_CUDA(w, cudaFuncSetAttribute(k_adj_solve<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    NS_CUDA(w, cudaFuncSetAttribute(k_adj_solve<false, kJoints>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = blocks;
     attr[0].val.clusterDim.y = 1;
@@ -1188,9 +1191,12 @@ int launch_adj_solve(ns_world* w, const StepTape& t, const AdjBufs& a, const Ste
   cfg.gridDim = dim3(blocks);
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<true>, t, a, p, w->dw.ctl));
-  else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<false>, t, a, p, w->dw.ctl));
+  if (w->solver_grid) NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<true, kJoints>, t, a, p, w->dw.ctl));
+  else NS_CUDA(w, cudaLaunchKernelEx(&cfg, k_adj_solve<false, kJoints>, t, a, p, w->dw.ctl));
   return NS_OK;
+}
+int launch_adj_solve(ns_world* w, const StepTape& t, const AdjBufs& a, const StepParams& p) {
+  return a.n_joints > 0 ? launch_adj_solve_t<true>(w, t, a, p) : launch_adj_solve_t<false>(w, t, a, p);
 }
 
 // Host check of the adjoint's local derivatives in f64: for each input direction i the
@@ -2798,7 +2804,10 @@ static int vjp_run(ns_world* w, const float* const seeds_in[4], bool f64, std::v
     a.bb = (float*)(buf + o_bb); a.cq = (float*)(buf + o_cq); a.pb = (float*)(buf + o_pb);
     a.kb = (float*)(buf + o_kb); a.mb = (float*)(buf + o_mb); a.mismatch = (int*)(buf + o_mis);
     a.yrec = (float*)(buf + o_yrec);
-    a.totb = (float*)(buf + o_tot); a.restb = (float*)(buf + o_restb); a.relb = (float*)(buf + o_rel);
+    bool any_rest = false;
+    for (const HostShape& hs : w->shapes) any_rest = any_rest || hs.d.restitution > 0.0f;
+    a.totb = any_rest ? (float*)(buf + o_tot) : nullptr;
+    a.restb = (float*)(buf + o_restb); a.relb = (float*)(buf + o_rel);
     a.jb = (float*)(buf + o_jb); a.jc = (float*)(buf + o_jc);
     a.joint_list = d.joint_list; a.jr = w->jr; a.n_joints = d.n_joints;
     a.cap = cap; a.n_awake = n;

@@ -61,7 +61,8 @@ struct AdjBufs {
   float* kb;   // [kCVOwn][cap]: constraint entries cvLam.. of each slot
   float* mb;   // [kMB][cap]: manifold state of each contact id
   float* yrec; // [substep][stage][kRelaxOut][cap]: output cotangents each contact update received
-  float* totb; // [4][cap]: the points' total normal impulses (what restitution reads of them)
+  float* totb; // [4][cap]: the points' total normal impulses (what restitution reads of them);
+               // null when no shape has restitution
   float* restb;  // [4][cap]: the points' restitution impulses
   float* relb; // [4][cap]: the points' relative normal velocities at prepare
   int* mismatch;  // narrowphase replays that did not reproduce the forward manifold
@@ -122,7 +123,8 @@ __global__ void k_adj_store(StepTape t, AdjBufs a, int n_slots) {
   for (int cv = cvLam; cv < kCV; ++cv) KB(a, k, cv) = 0.0f;
   // the total normal and restitution impulses start from zero at prepare and nothing after the
   // step reads them: their cotangents start at zero here, as do the relative velocities'
-  for (int q = 0; q < 4; ++q) { TOTB(a, k, q) = 0.0f; RESTB(a, k, q) = 0.0f; RELB(a, k, q) = 0.0f; }
+  if (a.totb)
+    for (int q = 0; q < 4; ++q) { TOTB(a, k, q) = 0.0f; RESTB(a, k, q) = 0.0f; RELB(a, k, q) = 0.0f; }
   for (int q = 0; q < pc; ++q) {
     KB(a, k, cvLam + q) = MB(a, cid, mb_point(q, 8));
     MB(a, cid, mb_point(q, 8)) = 0.0f;
@@ -227,7 +229,7 @@ __device__ void adj_contact(const StepTape& t, const AdjBufs& a, const StepParam
   for (int q = 0; q < 4; ++q) yb[12 + q] = KB(a, k, cvLam + q);
   // relax adds each point's new normal impulse to its total (imp.y += ni), which restitution
   // reads: the total's cotangent joins the new impulse's and passes on unchanged
-  if (Stage == kRelax)
+  if (Stage == kRelax && a.totb)
     for (int q = 0; q < 4; ++q) yb[12 + q] += TOTB(a, k, q);
   yb[16] = KB(a, k, cvFr); yb[17] = KB(a, k, cvFr + 1); yb[18] = KB(a, k, cvTwist);
   for (int i = 0; i < cvIma; ++i) xb[i] = 0.0f;
@@ -584,8 +586,8 @@ __device__ void joint_body_deltas(const StepTape& t, int n, int sub, int row, in
 // Reverse of one joint's push (use_bias) or relax solve at substep sub (one warp). Velocities'
 // and impulses' cotangents are replaced (the solve updates them), the perp axes' too (the solve
 // recomputes them), position and rotation increments' and the constants' accumulated.
-__device__ void adj_joint_solve(const StepTape& t, const AdjBufs& a, const StepParams& p, int stage, int sub, int ji,
-                                int lane, float* xs, float* ys) {
+__device__ __noinline__ void adj_joint_solve(const StepTape& t, const AdjBufs& a, const StepParams& p, int stage,
+                                             int sub, int ji, int lane, float* xs, float* ys) {
   using namespace ad;
   const DJoint& j = t.joints[ji];
   const int ia = j.index_a, ib = j.index_b, n = a.n_awake;
@@ -656,7 +658,8 @@ __device__ void adj_joint_solve(const StepTape& t, const AdjBufs& a, const StepP
 // prepare, for the first substep), the rotation increments and the constants. The bodies'
 // velocity cotangents are only read; several joints share a body in this phase, so its rotation
 // increments' cotangents are added atomically.
-__device__ void adj_joint_warm(const StepTape& t, const AdjBufs& a, int sub, int ji, int lane, float* xs, float* ys) {
+__device__ __noinline__ void adj_joint_warm(const StepTape& t, const AdjBufs& a, int sub, int ji, int lane, float* xs,
+                                            float* ys) {
   using namespace ad;
   const DJoint& j = t.joints[ji];
   const int ia = j.index_a, ib = j.index_b, n = a.n_awake;
@@ -713,12 +716,14 @@ __device__ void adj_joint_warm(const StepTape& t, const AdjBufs& a, int sub, int
 }
 
 // Reverse of the solver stages of one step: a persistent launch over the same barriers as the
-// forward solver, phases in reverse order, one thread per constraint or body.
-template <bool kGrid>
+// forward solver, phases in reverse order, one thread per constraint or body (one warp per
+// joint). The joints' reverse is compiled only into the kJoints variant: its dual-number frames
+// would otherwise raise every world's stack frame and registers (880 -> 1376 bytes).
+template <bool kGrid, bool kJoints>
 __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBufs a, StepParams p, Control* ctl) {
   __shared__ int coff[25];
-  __shared__ float jxs[kAdjThreads / 32][ad::kJX];
-  __shared__ float jys[kAdjThreads / 32][ad::kJSolveOut];
+  __shared__ float jxs[kJoints ? kAdjThreads / 32 : 1][ad::kJX];
+  __shared__ float jys[kJoints ? kAdjThreads / 32 : 1][ad::kJSolveOut];
   if (threadIdx.x < 24) coff[threadIdx.x] = t.ctl->color_offset[threadIdx.x];
   if (threadIdx.x == 24) coff[24] = t.ctl->color_offset[23];
   __syncthreads();
@@ -736,8 +741,9 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
       const int j0 = a.jr.off[c], j1 = a.jr.off[c + 1];
       if (coff[c + 1] == coff[c] && j1 == j0) continue;
       for (int k = coff[c] + g; k < coff[c + 1]; k += stride) adj_contact<Stage>(t, a, p, n, k, sub);
-      for (int q = j0 + wg; q < j1; q += wstride)
-        adj_joint_solve(t, a, p, Stage, sub, a.joint_list[q], lane, jxs[wib], jys[wib]);
+      if (kJoints)
+        for (int q = j0 + wg; q < j1; q += wstride)
+          adj_joint_solve(t, a, p, Stage, sub, a.joint_list[q], lane, jxs[wib], jys[wib]);
       if (!phase_sync<kGrid>(ctl, bar)) return false;
     }
     return true;
@@ -751,7 +757,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) k_adj_solve(StepTape t, AdjBuf
     // cotangents as they are and only reads them: every colour's warm start reverses in one
     // phase, before integrate-velocities changes those cotangents.
     for (int k = g; k < coff[kOverflowIndex]; k += stride) adj_contact<kWarm>(t, a, p, n, k, sub);
-    for (int q = wg; q < a.n_joints; q += wstride) adj_joint_warm(t, a, sub, q, lane, jxs[wib], jys[wib]);
+    if (kJoints)
+      for (int q = wg; q < a.n_joints; q += wstride) adj_joint_warm(t, a, sub, q, lane, jxs[wib], jys[wib]);
     if (!phase_sync<kGrid>(ctl, bar)) return;
     for (int i = g; i < n; i += stride) adj_iv(t, a, p, n, i, sub);
     if (!phase_sync<kGrid>(ctl, bar)) return;
