@@ -62,7 +62,8 @@ typedef struct {
 
 /* Body definition (types/body_def.rs BodyDef). */
 typedef struct {
-  int type;                    /* NS_STATIC_BODY or NS_DYNAMIC_BODY */
+  int type;                    /* NS_STATIC_BODY, NS_KINEMATIC_BODY (moves at its own velocity,
+                                  zero mass, collides with dynamic bodies only) or NS_DYNAMIC_BODY */
   double position[3];
   float rotation[4];           /* x, y, z, s */
   float linear_velocity[3];

@@ -229,7 +229,17 @@ void update_mass(ns_world* w, int bi) {
   s.max_extent = v3(0, 0, 0);
   if (b.shapes.empty()) return;
   if (b.type != NS_DYNAMIC_BODY) {
+    // body_api.rs:670-689: static and kinematic sims have zero mass; a kinematic body keeps its
+    // shapes' extents about its origin (contact recycling reads them)
     s.cx = s.px; s.cy = s.py; s.cz = s.pz;
+    if (b.type == NS_KINEMATIC_BODY)
+      for (int sid : b.shapes) {
+        float mn;
+        V3 mx;
+        shape_extent(w->shapes[sid], v3(0, 0, 0), &mn, &mx);
+        s.min_extent = minf(s.min_extent, mn);
+        s.max_extent = max3(s.max_extent, mx);
+      }
     return;
   }
   std::vector<MassData> masses;
@@ -482,16 +492,19 @@ int upload_world(ns_world* w) {
     for (int i = 0; i < nsh; ++i)
       if (dshapes[i].is_static) static_list[cursor[dshapes[i].world]++] = i;
   }
-  // shapes of dynamic bodies per sub-world in shape order, for the bullets' continuous pass
+  // shapes of moving bodies per sub-world for the bullets' continuous pass: the kinematic
+  // bodies' in shape order, then the dynamic bodies' (the reference queries its kinematic tree,
+  // then its dynamic tree, continuous.rs:429-448)
   std::vector<int> dyn_list, dyn_off(n_worlds + 1, 0);
   for (int i = 0; i < nsh; ++i)
-    if (w->bodies[dshapes[i].body].type == NS_DYNAMIC_BODY) dyn_off[dshapes[i].world + 1]++;
+    if (w->bodies[dshapes[i].body].type != NS_STATIC_BODY) dyn_off[dshapes[i].world + 1]++;
   for (int k = 0; k < n_worlds; ++k) dyn_off[k + 1] += dyn_off[k];
   {
     std::vector<int> cursor(dyn_off.begin(), dyn_off.end() - 1);
     dyn_list.resize(dyn_off[n_worlds]);
-    for (int i = 0; i < nsh; ++i)
-      if (w->bodies[dshapes[i].body].type == NS_DYNAMIC_BODY) dyn_list[cursor[dshapes[i].world]++] = i;
+    for (int type : {NS_KINEMATIC_BODY, NS_DYNAMIC_BODY})
+      for (int i = 0; i < nsh; ++i)
+        if (w->bodies[dshapes[i].body].type == type) dyn_list[cursor[dshapes[i].world]++] = i;
   }
   // the sweep of a body starts at its pose at upload (body_api.rs:221, :533 center0/rotation0)
   for (DSim& s : w->asims) { s.cx0 = s.cx; s.cy0 = s.cy; s.cz0 = s.cz; s.q0 = s.q; }
@@ -548,7 +561,7 @@ int upload_world(ns_world* w) {
 #define ALLOC(field, T, n) do { d.field = dalloc<T>(w, (n), &st); if (!d.field) return st; } while (0)
   ALLOC(asims, DSim, na); ALLOC(states, DState, na); ALLOC(ssims, DSim, ns);
   ALLOC(shapes, DShape, nsh); ALLOC(hulls, Hull, nsh); ALLOC(fat, AABB, nsh); ALLOC(moved, int, nsh);
-  ALLOC(body_shapes, int, body_shapes.size()); ALLOC(body_mask, uint32_t, nb);
+  ALLOC(body_shapes, int, body_shapes.size()); ALLOC(body_mask, uint32_t, nb); ALLOC(body_dyn, uint8_t, nb);
   ALLOC(body_joint_off, int, nb + 1); ALLOC(body_joint_other, int, jother.size());
   ALLOC(contacts, DContact, cap); ALLOC(free_stack, int, cap);
   ALLOC(hs, unsigned long long, hs_size);
@@ -593,6 +606,11 @@ int upload_world(ns_world* w) {
   if ((st = upload(w, d.fat, w->fat))) return st;
   if ((st = upload(w, d.body_shapes, body_shapes))) return st;
   if ((st = upload(w, d.body_mask, w->body_mask))) return st;
+  {
+    std::vector<uint8_t> dyn(w->bodies.size());
+    for (size_t i = 0; i < w->bodies.size(); ++i) dyn[i] = w->bodies[i].type == NS_DYNAMIC_BODY ? 1 : 0;
+    if ((st = upload(w, d.body_dyn, dyn))) return st;
+  }
   if ((st = upload(w, d.body_joint_off, joff))) return st;
   if ((st = upload(w, d.body_joint_other, jother))) return st;
   if ((st = upload(w, d.large_list, large))) return st;
@@ -1077,6 +1095,8 @@ int check_adjoint_scope(ns_world* w) {
   if (w->jr.off[kOverflowIndex + 1] > w->jr.off[kOverflowIndex])
     return fail(w, NS_ERR_UNSUPPORTED, "joints in the overflow colour; the adjoint does not cover them");
   if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
+  for (const HostBody& b : w->bodies)
+    if (b.type == NS_KINEMATIC_BODY) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover kinematic bodies");
   for (const HostShape& hs : w->shapes)
     if (hs.d.rolling != 0.0f) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover rolling resistance");
   for (const DSim& a : w->asims) {
@@ -1829,7 +1849,10 @@ const char* ns_last_error(const ns_world* w) { return w ? w->err.c_str() : g_cre
 int ns_create_body(ns_world* w, const ns_body_def* d) {
   if (!w || !d) return -1;
   if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
-  if (d->type != NS_STATIC_BODY && d->type != NS_DYNAMIC_BODY) { w->err = "only static and dynamic bodies are supported"; return -1; }
+  if (d->type != NS_STATIC_BODY && d->type != NS_KINEMATIC_BODY && d->type != NS_DYNAMIC_BODY) {
+    w->err = "body type must be NS_STATIC_BODY, NS_KINEMATIC_BODY or NS_DYNAMIC_BODY";
+    return -1;
+  }
   int id = (int)w->bodies.size();
   HostBody b;
   b.type = d->type;

@@ -54,6 +54,7 @@ struct DW {
   DShape* shapes; Hull* hulls; AABB* fat; int* moved; int n_shapes;
   int* body_shapes;                 // shape ids grouped per awake body (DSim shape range)
   uint32_t* body_mask; int n_bodies;
+  uint8_t* body_dyn;  // [body id] 1 for a dynamic body (kinematic and static bodies are not)
   int* body_joint_off; int* body_joint_other;  // joint partners with collision disabled
   DContact* contacts; int cap;
   int* free_stack;
@@ -223,7 +224,8 @@ __device__ bool should_create_pair(const DW& w, int a, int b) {
   } else if (!((A.mask & B.category) != 0 && (A.category & B.mask) != 0)) {
     return false;
   }
-  if (A.is_static && B.is_static) return false;  // contact_creation.rs:113 should_bodies_collide
+  // contact_creation.rs:113 should_bodies_collide: at least one dynamic body
+  if (!w.body_dyn[A.body] && !w.body_dyn[B.body]) return false;
   for (int j = w.body_joint_off[A.body]; j < w.body_joint_off[A.body + 1]; ++j)
     if (w.body_joint_other[j] == B.body) return false;
   return true;
@@ -866,7 +868,7 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
       st.flags[i] = c.flags;
       st.ba[i] = c.body_a;
       st.bb[i] = c.body_b;
-      st.info[i] = (c.color + 1) | ((c.enc_a >= 0) << 8) | ((c.enc_b >= 0) << 9);
+      st.info[i] = (c.color + 1) | ((int)w.body_dyn[c.body_a] << 8) | ((int)w.body_dyn[c.body_b] << 9);
     }
     __syncthreads();
     if (t == 0) ovf_s = use_shared ? state_walk(w, smask, st, n, ovf_s) : state_walk(w, w.body_mask, st, n, ovf_s);
@@ -975,7 +977,7 @@ __global__ void k_state_worlds(DW w) {
         hs_erase(w, pair_key(c.shape_a, c.shape_b));
       } else if (f & cSimStarted) {   // constraint_graph.rs:113 add_contact_to_graph
         c.flags = (f & ~cSimStarted) | cTouching;
-        bool dyn_a = c.enc_a >= 0, dyn_b = c.enc_b >= 0;
+        bool dyn_a = w.body_dyn[c.body_a] != 0, dyn_b = w.body_dyn[c.body_b] != 0;
         int color = kOverflowIndex;
         if (dyn_a && dyn_b) {
           uint32_t avail = ~(w.body_mask[c.body_a] | w.body_mask[c.body_b]) & ((1u << kDynamicColorCount) - 1u);

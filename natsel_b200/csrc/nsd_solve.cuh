@@ -302,6 +302,11 @@ __device__ __forceinline__ void put_warm_delta(const DW& w, int ia, int ib, int 
   }
 }
 
+// The solver index of a dynamic body, -1 for a static or kinematic one
+__device__ __forceinline__ int dynamic_index(const DW& w, int i) {
+  return i >= 0 && (w.states[i].flags & kDynamicFlag) ? i : -1;
+}
+
 __device__ __forceinline__ void mark_warm_slot(const DW& w, int body, int color) {
   if (body >= 0) atomicOr(&w.bw_mask[body], 1u << color);
 }
@@ -505,8 +510,8 @@ __device__ void relax_constraint(const DW& w, const StepParams& p, int k, const 
   }
   store_state_vw(w, c.ia, ba);
   store_state_vw(w, c.ib, bb);
-  if (warm_color >= 0)
-    put_warm_delta(w, c.ia, c.ib, warm_color,
+  if (warm_color >= 0)  // only a dynamic body takes a warm start (kinematic bodies share colours)
+    put_warm_delta(w, (ba.flags & kDynamicFlag) ? c.ia : -1, (bb.flags & kDynamicFlag) ? c.ib : -1, warm_color,
                    contact_warm_delta(c, d.t1, d.t2, caf, cbf, fr, ro, d.pra, d.prb, nis));
 }
 
@@ -1063,19 +1068,23 @@ __global__ void __launch_bounds__(256) k_warm_slots(DW w, JointRanges jr) {
       float ni[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) ni[q] = d.pimp[q].x;
-      put_warm_delta(w, d.c.ia, d.c.ib, c,
+      // only a dynamic body takes a warm start (a kinematic body may have several constraints
+      // in one colour)
+      const int ia = dynamic_index(w, d.c.ia), ib = dynamic_index(w, d.c.ib);
+      put_warm_delta(w, ia, ib, c,
                      contact_warm_delta(d.c, d.t1, d.t2, d.ca, d.cb, d.fr, d.roll, d.pra, d.prb, ni));
-      mark_warm_slot(w, d.c.ia, c);
-      mark_warm_slot(w, d.c.ib, c);
+      mark_warm_slot(w, ia, c);
+      mark_warm_slot(w, ib, c);
     } else {
       const int t = i - n_col;
       int c = 0;
       while (jr.off[c + 1] <= t) ++c;
       const DJoint& j = w.joints[w.joint_list[t]];
       DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
-      put_warm_delta(w, j.index_a, j.index_b, c, joint_warm_delta(j, sa.dq, sb.dq));
-      mark_warm_slot(w, j.index_a, c);
-      mark_warm_slot(w, j.index_b, c);
+      const int ia = (sa.flags & kDynamicFlag) ? j.index_a : -1, ib = (sb.flags & kDynamicFlag) ? j.index_b : -1;
+      put_warm_delta(w, ia, ib, c, joint_warm_delta(j, sa.dq, sb.dq));
+      mark_warm_slot(w, ia, c);
+      mark_warm_slot(w, ib, c);
     }
   }
 }
@@ -1283,7 +1292,8 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
         if (kTape && tp.joint && warm_color >= 0) tape_joint_warm(w, tp, sub, ji, j);
         if (warm_color >= 0) {
           DState sa = state_at(w, j.index_a), sb = state_at(w, j.index_b);
-          put_warm_delta(w, j.index_a, j.index_b, c, joint_warm_delta(j, sa.dq, sb.dq));
+          put_warm_delta(w, (sa.flags & kDynamicFlag) ? j.index_a : -1, (sb.flags & kDynamicFlag) ? j.index_b : -1, c,
+                         joint_warm_delta(j, sa.dq, sb.dq));
         }
       }
     }
@@ -1347,7 +1357,7 @@ __global__ void k_finalize(DW w, StepParams p) {
                 isfinite(wv.z) && isfinite(sim.cx) && isfinite(sim.cy) && isfinite(sim.cz) &&
                 isfinite(sim.q.v.x) && isfinite(sim.q.v.y) && isfinite(sim.q.v.z) && isfinite(sim.q.s);
   if (!finite) atomicCAS(&w.ctl->error, 0, kErrNonFinite);
-  if (finite && p.enable_continuous && max_motion > sim.safety_factor * sim.min_extent) {
+  if (finite && p.enable_continuous && (sim.flags & kDynamicFlag) && max_motion > sim.safety_factor * sim.min_extent) {
     sim.flags |= kIsFast;
     add_converged(&w.ctl->fast_flags);
     // the continuous pass (k_continuous, or k_bullets for a bullet) sweeps it from (cx0, q0)
@@ -1550,9 +1560,10 @@ __global__ void __launch_bounds__(64) k_continuous(DW w, StepParams p) {
 
 // solver_integration.rs:949-958, continuous.rs:337 for one fast bullet, one warp each, after
 // k_continuous (every other body is final). Every shape of the bullet (no per-shape speed test)
-// is swept against its sub-world's static shapes, then against the shapes of its dynamic
-// non-bullet bodies at their final poses (continuous.rs:429-448: the reference also walks its
-// dynamic tree for bullets; bullets skip bullets, continuous.rs:253), each list in shape order.
+// is swept against its sub-world's static shapes, then against the shapes of its kinematic and
+// dynamic non-bullet bodies at their final poses (continuous.rs:429-448: the reference also walks
+// its kinematic and dynamic trees for bullets; bullets skip bullets, continuous.rs:253), each
+// list in shape order.
 // The lanes test 32 candidates' bounds and filters at once; lane 0 runs the times of impact in
 // list order, each bounded by the best fraction so far, and finishes the body. Bullets read
 // only non-bullet bodies, which no warp here writes, so they are independent of one another.

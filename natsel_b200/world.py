@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnatsel_gpu.so")
 
 STATIC_BODY = 0
+KINEMATIC_BODY = 1
 DYNAMIC_BODY = 2
 
 

@@ -409,8 +409,15 @@ void update_body_mass(nso_world* w, int bi) {
   s.max_extent = v3(0, 0, 0);
   if (b.head_shape == -1) return;
   if (b.type != 2) {
+    // body_api.rs:670-689: zero mass; a kinematic body keeps its shapes' extents about its origin
     s.center = s.transform.p;
     s.center0 = s.center;
+    if (b.type == 1)
+      for (int sid = b.head_shape; sid != -1; sid = w->shapes[sid].next_shape) {
+        Extent e = shape_extent(w->shapes[sid], v3(0, 0, 0));
+        s.min_extent = minf(s.min_extent, e.min_extent);
+        s.max_extent = max3(s.max_extent, e.max_extent);
+      }
     return;
   }
   std::vector<MassData> masses;
@@ -1824,12 +1831,12 @@ void solve_continuous(nso_world* w, int i) {
     for (int sid = 0; sid < (int)w->shapes.size(); ++sid)
       if (w->shapes[sid].is_static && aabb_overlaps(w->fat[sid], swept))
         continuous_candidate(w, fs, fp, sweep, base, sid, fraction);
-    // bullets also query the dynamic tree (continuous.rs:429-448)
+    // bullets also query the kinematic tree, then the dynamic tree (continuous.rs:429-448)
     if (bullet)
-      for (int sid = 0; sid < (int)w->shapes.size(); ++sid)
-        if (!w->shapes[sid].is_static && w->bodies[w->shapes[sid].body_id].type == 2 &&
-            aabb_overlaps(w->fat[sid], swept))
-          continuous_candidate(w, fs, fp, sweep, base, sid, fraction);
+      for (int type = 1; type <= 2; ++type)
+        for (int sid = 0; sid < (int)w->shapes.size(); ++sid)
+          if (w->bodies[w->shapes[sid].body_id].type == type && aabb_overlaps(w->fat[sid], swept))
+            continuous_candidate(w, fs, fp, sweep, base, sid, fraction);
   }
   real spec = speculative_distance();
   if (fraction < 1.0f) {

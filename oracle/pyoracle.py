@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "libns_oracle.so")
 SOURCES = ["ns_world.cpp", "ns_math.hpp", "ns_collide.hpp", "ns_joint.hpp", "ns_oracle.h"]
 
 STATIC_BODY = 0
+KINEMATIC_BODY = 1
 DYNAMIC_BODY = 2
 
 
