@@ -286,9 +286,10 @@ int ns_world_set_launch_shapes(ns_world* w, const int* in8);
  * the first step boundary at or after that count). While recording, dt must be > 0 and
  * ns_world_apply_forces is refused. Scope: one world (no sub-worlds) of box, sphere and
  * capsule bodies with the centre of mass at the body origin and revolute joints (none in the
- * overflow colour), without rolling resistance or continuous collision (NS_ERR_UNSUPPORTED
- * otherwise); steps that put contacts in the overflow colour are reported by ns_world_vjp as
- * NS_ERR_UNSUPPORTED, and steps with restitution, or worlds with joints, by ns_world_vjp_f64. */
+ * overflow colour), without kinematic bodies, rolling resistance or continuous collision
+ * (NS_ERR_UNSUPPORTED otherwise); steps that put contacts in the overflow colour are reported
+ * by ns_world_vjp as NS_ERR_UNSUPPORTED, and steps with restitution, or worlds with joints, by
+ * ns_world_vjp_f64. */
 int ns_world_tape_begin(ns_world* w, int checkpoint_substeps);
 /* Stops recording; the tape stays for ns_world_vjp. */
 int ns_world_tape_end(ns_world* w);
