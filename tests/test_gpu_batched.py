@@ -123,3 +123,27 @@ def test_autotune_keeps_the_world_and_its_trajectory(batched):
         applied.set_launch_shapes(bad)
     for w in (tuned, plain, applied):
         w.close()
+
+
+def test_batch_with_kinematic_bodies_and_bullets_matches_each_world_alone():
+    """Sub-worlds with continuous collision on: kinematic platforms, a spinning paddle and a
+    kinematic wall hit by a bullet; the reference's fast-movers scene with bullets among cubes;
+    a pyramid. The bullet pass and the kinematic rules stay inside each sub-world."""
+    from test_continuous import _fast_movers
+    from test_kinematic import _mixed
+    settings = dict(gravity=(0.0, -9.81, 0.0), enable_continuous=True)
+    builders = [_mixed, _fast_movers, lambda w: scenes.BUILDERS["box_pyramid"](w, base=4), _mixed]
+    g = World(default_world_def(gravity=settings["gravity"], enable_continuous=1))
+    for k, build in enumerate(builders):
+        if k:
+            g.begin_subworld()
+        build(g)
+    for _ in range(30):
+        g.step(DT, 4)
+    got = g.subworld_hashes()
+    for k, build in enumerate(builders):
+        o = pyoracle.OracleWorld(**settings)
+        build(o)
+        for _ in range(30):
+            o.step(DT, 4)
+        assert int(got[k]) == o.state_hash(), "sub-world %d differs" % k
