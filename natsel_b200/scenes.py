@@ -29,6 +29,25 @@ def _f(x):
     return float(np.float32(x))
 
 
+def joint_grid(world, n=100):
+    """scenes.rs:49 create_joint_grid (default world: gravity -10): an n x n grid of 0.4 m spheres
+    (the first row static) in the xy plane, each joined to its upper and left neighbours by a
+    spherical joint with the default definition (a point constraint); the spheres' filters keep
+    them from colliding with one another."""
+    ids = []
+    for k in range(n):
+        for i in range(n):
+            b = world.create_body(type=STATIC if i == 0 else DYNAMIC, position=(float(k), float(-i), 0.0),
+                                  enable_sleep=False)
+            world.create_sphere(b, 0.4, category_bits=2, mask_bits=0xFFFFFFFFFFFFFFFD)
+            if i > 0:
+                world.create_spherical(ids[-1], b, (0.0, -0.5, 0.0, 0.0, 0.0, 0.0, 1.0), (0.0, 0.5, 0.0, 0.0, 0.0, 0.0, 1.0))
+            if k > 0:
+                world.create_spherical(ids[-n], b, (0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0), (-0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0))
+            ids.append(b)
+    return {"name": "joint_grid", "dynamic_bodies": n * (n - 1)}
+
+
 def large_pyramid(world, base_count=100):
     """scenes.rs:105 create_large_pyramid (default world: gravity -10)."""
     g = world.create_body(type=STATIC, position=(0.0, -1.0, 0.0))
@@ -365,6 +384,7 @@ WORLD_SETTINGS = {
     # reference World does by default; the other synthetic scenes keep it off (their bodies never
     # move fast enough to need it: the batched worlds' drops are short and sit on a 10 m ground).
     "large_pyramid": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
+    "joint_grid": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
     "many_pyramids": dict(gravity=(0.0, -10.0, 0.0), enable_continuous=True),
     "box_pyramid": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
     "large_pile": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=True),
@@ -375,10 +395,11 @@ WORLD_SETTINGS = {
     "differentiable_rollout": dict(gravity=(0.0, -9.81, 0.0), enable_continuous=False),
 }
 
-SUBSTEPS = {"large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8,
+SUBSTEPS = {"joint_grid": 4, "large_pyramid": 4, "many_pyramids": 4, "box_pyramid": 4, "large_pile": 4, "jointed_chains": 8,
             "overflow_pile": 4, "restitution_ball": 4, "batched_worlds": 4, "differentiable_rollout": 4}
 
 BUILDERS = {
+    "joint_grid": joint_grid,
     "large_pyramid": large_pyramid,
     "many_pyramids": many_pyramids,
     "box_pyramid": box_pyramid,

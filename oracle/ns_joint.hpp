@@ -1,6 +1,6 @@
-// Oracle revolute joint rows. TEST INFRASTRUCTURE ONLY (the parity checker).
-// Restates simulation/revolute_joint.rs and the joint dispatch of
-// simulation/distance_joint_solver.rs:74-346 for the revolute type.
+// Oracle joint rows. TEST INFRASTRUCTURE ONLY (the parity checker).
+// Restates simulation/revolute_joint.rs, simulation/spherical_joint.rs and the joint dispatch of
+// simulation/distance_joint_solver.rs:74-346 for those two types.
 #pragma once
 #include <vector>
 #include "ns_math.hpp"
@@ -43,7 +43,51 @@ struct Joint {
   real axial_mass = 0;
   JointSoft spring_softness = {0, 0, 0};
   bool enable_spring = false, enable_motor = false, enable_limit = false;
+  // SphericalJointSim (spherical_joint.rs:40): type 1. lower_impulse / upper_impulse hold the
+  // twist limit impulses; the spring and motor impulses are vectors.
+  int type = 0;
+  bool enable_cone_limit = false, enable_twist_limit = false;
+  real cone_angle = 0, lower_twist_angle = 0, upper_twist_angle = 0;
+  Q target_rotation = {{0, 0, 0}, 1};
+  V3 motor_velocity = {0, 0, 0}, spring_impulse3 = {0, 0, 0}, motor_impulse3 = {0, 0, 0};
+  real swing_impulse = 0, swing_mass = 0, twist_mass = 0;
+  V3 swing_axis = {0, 0, 0}, twist_jacobian = {0, 0, 0};
+  M3 rotation_mass = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 };
+
+// spherical_joint.rs:119 create_spherical_joint
+inline Joint make_spherical_joint(int a, int b, const float* fa, const float* fb, bool collide, real c_hertz,
+                                  real c_zeta, bool spring, real hertz, real zeta, Q target, bool cone,
+                                  real cone_angle, bool twist, real lower, real upper, bool motor,
+                                  real max_torque, V3 motor_velocity) {
+  Joint j;
+  j.type = 1;
+  j.body_a = a; j.body_b = b;
+  j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
+  j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
+  j.collide_connected = collide;
+  j.constraint_hertz = c_hertz; j.constraint_damping_ratio = c_zeta;
+  j.enable_spring = spring; j.hertz = hertz; j.damping_ratio = zeta; j.target_rotation = target;
+  j.enable_cone_limit = cone; j.cone_angle = cone_angle;
+  j.enable_twist_limit = twist; j.lower_twist_angle = lower; j.upper_twist_angle = upper;
+  j.enable_motor = motor; j.max_motor_torque = max_torque; j.motor_velocity = motor_velocity;
+  j.inv_ia = m3zero(); j.inv_ib = m3zero();
+  return j;
+}
+
+// internal_math.rs:328 delta_quat_to_rotation
+inline V3 delta_quat_to_rotation(Q q, Q target) {
+  Q s = dot_quat(q, target) < 0.0f ? quat(v3(-q.v.x, -q.v.y, -q.v.z), -q.s) : q;
+  Q diff = quat(target.v - s.v, target.s - s.s);
+  Q product = mul_quat(diff, conjugate(s));
+  return 2.0f * product.v;
+}
+// functions.rs:502 get_swing_angle
+inline real get_swing_angle(Q q) {
+  real x = std::sqrt(q.v.z * q.v.z + q.s * q.s);
+  real y = std::sqrt(q.v.x * q.v.x + q.v.y * q.v.y);
+  return 2.0f * atan2_approx(y, x);
+}
 
 inline Joint make_revolute_joint(int a, int b, const float* fa, const float* fb, bool limit, real lower,
                                  real upper, bool spring, real hertz, real zeta, real drag,
@@ -101,6 +145,35 @@ inline V3 solve_point_constraint(real ma, real mb, M3 ia, M3 ib, V3 ra, V3 rb, V
 // does not depend on the world's private types.
 namespace nso {
 
+// spherical_joint.rs:183-230: the spherical joint's part of prepare (after the common frames)
+inline void prepare_spherical(Joint& j, M3 inv_inertia_sum, real h, real warm) {
+  V3 cone_axis = rotate(j.frame_a.q, v3(0, 0, 1));
+  V3 twist_axis = rotate(j.frame_b.q, v3(0, 0, 1));
+  if (j.enable_cone_limit) {
+    V3 swing_axis = normalize(cross(cone_axis, twist_axis));
+    real k = dot(swing_axis, mul_mv(inv_inertia_sum, swing_axis));
+    j.swing_mass = k > 0.0f ? 1.0f / k : 0.0f;
+    j.swing_axis = swing_axis;
+  }
+  if (j.enable_twist_limit) {
+    Q rel_q = inv_mul_quat(j.frame_a.q, j.frame_b.q);
+    real tan_half = std::sqrt((rel_q.v.x * rel_q.v.x + rel_q.v.y * rel_q.v.y) /
+                              (rel_q.v.z * rel_q.v.z + rel_q.s * rel_q.s));
+    V3 swing_axis = normalize(cross(cone_axis, twist_axis));
+    V3 perp_axis = cross(swing_axis, cone_axis);
+    V3 jac = mul_add(cone_axis, tan_half, perp_axis);
+    real k = dot(jac, mul_mv(inv_inertia_sum, jac));
+    j.twist_mass = k > 0.0f ? 1.0f / k : 0.0f;
+    j.twist_jacobian = jac;
+  }
+  j.rotation_mass = !j.fixed_rotation ? invert_matrix(inv_inertia_sum) : m3zero();
+  j.spring_softness = joint_make_soft(j.hertz, j.damping_ratio, h);
+  if (warm == 0.0f) {
+    j.linear_impulse = v3(0, 0, 0); j.motor_impulse3 = v3(0, 0, 0); j.spring_impulse3 = v3(0, 0, 0);
+    j.swing_impulse = 0; j.lower_impulse = 0; j.upper_impulse = 0;
+  }
+}
+
 template <class BodyT, class SimT>
 void prepare_joints(std::vector<Joint>& joints, const std::vector<SimT>& awake, const std::vector<SimT>& stat,
                     const BodyT* bodies, real h, real inv_h, real warm) {
@@ -124,6 +197,10 @@ void prepare_joints(std::vector<Joint>& joints, const std::vector<SimT>& awake, 
     j.frame_b.q = mul_quat(sb.transform.q, j.local_frame_b.q);
     j.frame_b.p = rotate(sb.transform.q, j.local_frame_b.p - sb.local_center);
     j.delta_center = sub_pos(sb.center, sa.center);
+    if (j.type == 1) {
+      prepare_spherical(j, sum, h, warm);
+      continue;
+    }
     V3 axis = rotate(j.frame_a.q, v3(0, 0, 1));
     real k = dot(axis, mul_mv(sum, axis));
     j.axial_mass = k > 0.0f ? 1.0f / k : 0.0f;
@@ -147,6 +224,84 @@ StateT joint_state_at(std::vector<StateT>& states, int i) {
   return s;
 }
 
+// spherical_joint.rs:315-438: the spring, motor, twist limit and cone limit rows of
+// solve_spherical_joint (the point constraint is shared with the revolute joint)
+inline void solve_spherical_angular(Joint& j, Q qa, Q qb, M3 iA, M3 iB, real h, real inv_h, bool use_bias, V3& wa,
+                                    V3& wb) {
+  Q rel_q = inv_mul_quat(qa, qb);
+  if (j.fixed_rotation || !(j.enable_spring || j.enable_motor || j.enable_twist_limit || j.enable_cone_limit)) return;
+  M3 sum = add_mm(iA, iB);
+  V3 cdot = wb - wa;
+  V3 ang = v3(0, 0, 0);
+  if (j.enable_spring) {
+    V3 dr = delta_quat_to_rotation(rel_q, j.target_rotation);
+    V3 c = -(rotate(qa, dr));
+    V3 bias = j.spring_softness.bias_rate * c;
+    real ms = j.spring_softness.mass_scale, is = j.spring_softness.impulse_scale;
+    V3 imp = (-ms) * mul_mv(j.rotation_mass, cdot + bias) - is * j.spring_impulse3;
+    j.spring_impulse3 = j.spring_impulse3 + imp;
+    cdot = cdot + mul_mv(sum, imp);
+    ang = ang + imp;
+  }
+  if (j.enable_motor) {
+    V3 lambda = -(mul_mv(j.rotation_mass, cdot - j.motor_velocity));
+    V3 next = j.motor_impulse3 + lambda;
+    real len = length(next);
+    real mx = j.max_motor_torque * h;
+    if (len > mx) next = (mx / len) * next;
+    lambda = next - j.motor_impulse3;
+    j.motor_impulse3 = next;
+    cdot = cdot + mul_mv(sum, lambda);
+    ang = ang + lambda;
+  }
+  auto limit_terms = [&](real c, real& bias, real& ms, real& is) {
+    bias = 0.0f; ms = 1.0f; is = 0.0f;
+    if (c > 0.0f) bias = c * inv_h;
+    else if (use_bias) {
+      bias = j.constraint_softness.bias_rate * c;
+      ms = j.constraint_softness.mass_scale;
+      is = j.constraint_softness.impulse_scale;
+    }
+  };
+  if (j.enable_twist_limit) {
+    real twist = get_twist_angle(rel_q);
+    V3 jac = j.twist_jacobian;
+    V3 resp = mul_mv(sum, jac);
+    {
+      real bias, ms, is;
+      limit_terms(twist - j.lower_twist_angle, bias, ms, is);
+      real tcd = dot(cdot, jac);
+      real old = j.lower_impulse;
+      real di = maxf(-ms * j.twist_mass * (tcd + bias) - is * old, -old);
+      j.lower_impulse = old + di;
+      cdot = mul_add(cdot, di, resp);
+      ang = mul_add(ang, di, jac);
+    }
+    {
+      real bias, ms, is;
+      limit_terms(j.upper_twist_angle - twist, bias, ms, is);
+      real tcd = -dot(cdot, jac);
+      real old = j.upper_impulse;
+      real di = maxf(-ms * j.twist_mass * (tcd + bias) - is * old, -old);
+      j.upper_impulse = old + di;
+      cdot = cdot - di * resp;
+      ang = ang - di * jac;
+    }
+  }
+  if (j.enable_cone_limit) {
+    real swing = get_swing_angle(rel_q);
+    real bias, ms, is;
+    limit_terms(j.cone_angle - swing, bias, ms, is);
+    real scd = -dot(cdot, j.swing_axis);
+    real old = j.swing_impulse;
+    real di = maxf(-ms * j.swing_mass * (scd + bias) - is * old, -old);
+    j.swing_impulse = old + di;
+    ang = ang - di * j.swing_axis;
+  }
+  wa = wa - mul_mv(iA, ang);
+  wb = wb + mul_mv(iB, ang);
+}
+
 // revolute_joint.rs:261 warm_start_revolute_joint
 template <class StateT>
 void warm_start_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
@@ -158,9 +313,16 @@ void warm_start_joints_color(std::vector<Joint>& joints, const std::vector<int>&
     StateT sa = joint_state_at(states, j.index_a), sb = joint_state_at(states, j.index_b);
     V3 va = sa.v, wa = sa.w, vb = sb.v, wb = sb.w;
     V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
-    real axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
-    V3 ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
-    ang = mul_add(ang, axial, j.rotation_axis_z);
+    V3 ang;
+    if (j.type == 1) {  // spherical_joint.rs:233 warm_start_spherical_joint
+      ang = j.spring_impulse3 + j.motor_impulse3;
+      ang = ang - j.swing_impulse * j.swing_axis;
+      ang = mul_add(ang, j.lower_impulse - j.upper_impulse, j.twist_jacobian);
+    } else {
+      real axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
+      ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
+      ang = mul_add(ang, axial, j.rotation_axis_z);
+    }
     va = va - mA * j.linear_impulse;
     wa = wa - mul_mv(j.inv_ia, cross(ra, j.linear_impulse) + ang);
     vb = vb + mB * j.linear_impulse;
@@ -185,6 +347,9 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
     bool fixed = j.fixed_rotation;
     Q qa = mul_quat(sa.dq, j.frame_a.q);
     Q qb = mul_quat(sb.dq, j.frame_b.q);
+    if (j.type == 1) {
+      solve_spherical_angular(j, qa, qb, iA, iB, h, inv_h, use_bias, wa, wb);
+    } else {
     if (dot_quat(qa, qb) < 0.0f) qb = quat(v3(-qb.v.x, -qb.v.y, -qb.v.z), -qb.s);
     Q rq = inv_mul_quat(qa, qb);
     if (!fixed && (j.enable_spring || j.enable_motor || j.enable_limit)) {
@@ -278,6 +443,7 @@ void solve_joints_color(std::vector<Joint>& joints, const std::vector<int>& ids,
       wa = wa - mul_mv(iA, ang);
       wb = wb + mul_mv(iB, ang);
     }
+    }  // revolute
     {
       V3 ra = rotate(sa.dq, j.frame_a.p), rb = rotate(sb.dq, j.frame_b.p);
       V3 cdot = (vb + cross(wb, rb)) - va - cross(wa, ra);

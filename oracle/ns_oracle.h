@@ -74,6 +74,25 @@ typedef struct {
   float max_motor_torque, motor_speed;
 } nso_revolute_def;
 int nso_create_revolute_def(nso_world* w, const nso_revolute_def* def);
+/* SphericalJointDef (types/joint_defs.rs:169 with its JointDef base :30); same layout as the
+ * product's ns_spherical_joint_def. */
+typedef struct {
+  int body_a, body_b;
+  float local_frame_a[7], local_frame_b[7];
+  float constraint_hertz, constraint_damping_ratio;
+  int collide_connected;
+  int enable_spring;
+  float hertz, damping_ratio;
+  float target_rotation[4];
+  int enable_cone_limit;
+  float cone_angle;
+  int enable_twist_limit;
+  float lower_twist_angle, upper_twist_angle;
+  int enable_motor;
+  float max_motor_torque;
+  float motor_velocity[3];
+} nso_spherical_def;
+int nso_create_spherical_def(nso_world* w, const nso_spherical_def* def);
 void nso_step(nso_world* w, float dt, int substeps);
 /* Host threads of the colour-parallel loops (all worlds of the process; default 1). */
 void nso_set_threads(int threads);

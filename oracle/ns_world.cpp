@@ -2075,6 +2075,17 @@ int nso_create_revolute_def(nso_world* w, const nso_revolute_def* d) {
   return add_revolute(w, j);
 }
 
+int nso_create_spherical_def(nso_world* w, const nso_spherical_def* d) {
+  const float* t = d->target_rotation;
+  Joint j = make_spherical_joint(d->body_a, d->body_b, d->local_frame_a, d->local_frame_b, d->collide_connected != 0,
+                                 d->constraint_hertz, d->constraint_damping_ratio, d->enable_spring != 0, d->hertz,
+                                 d->damping_ratio, quat(v3(t[0], t[1], t[2]), t[3]), d->enable_cone_limit != 0,
+                                 d->cone_angle, d->enable_twist_limit != 0, d->lower_twist_angle,
+                                 d->upper_twist_angle, d->enable_motor != 0, d->max_motor_torque,
+                                 v3(d->motor_velocity[0], d->motor_velocity[1], d->motor_velocity[2]));
+  return add_revolute(w, j);
+}
+
 static int add_revolute(nso_world* w, Joint j) {
   int body_a = j.body_a, body_b = j.body_b;
   int id = (int)w->joints.size();

@@ -93,6 +93,44 @@ class RevoluteDef(ctypes.Structure):
     ]
 
 
+class SphericalDef(ctypes.Structure):
+    """nso_spherical_def: the reference's SphericalJointDef (types/joint_defs.rs:169)."""
+    _fields_ = [
+        ("body_a", ctypes.c_int), ("body_b", ctypes.c_int),
+        ("local_frame_a", ctypes.c_float * 7), ("local_frame_b", ctypes.c_float * 7),
+        ("constraint_hertz", ctypes.c_float), ("constraint_damping_ratio", ctypes.c_float),
+        ("collide_connected", ctypes.c_int),
+        ("enable_spring", ctypes.c_int), ("hertz", ctypes.c_float), ("damping_ratio", ctypes.c_float),
+        ("target_rotation", ctypes.c_float * 4),
+        ("enable_cone_limit", ctypes.c_int), ("cone_angle", ctypes.c_float),
+        ("enable_twist_limit", ctypes.c_int), ("lower_twist_angle", ctypes.c_float),
+        ("upper_twist_angle", ctypes.c_float),
+        ("enable_motor", ctypes.c_int), ("max_motor_torque", ctypes.c_float), ("motor_velocity", ctypes.c_float * 3),
+    ]
+
+
+def fill_spherical_def(d, default_hertz, default_zeta, body_a, body_b, frame_a, frame_b, collide_connected=False,
+                       enable_spring=False, hertz=0.0, damping_ratio=0.0, target_rotation=(0.0, 0.0, 0.0, 1.0),
+                       enable_cone_limit=False, cone_angle=0.0, enable_twist_limit=False, lower_twist_angle=0.0,
+                       upper_twist_angle=0.0, enable_motor=False, max_motor_torque=0.0,
+                       motor_velocity=(0.0, 0.0, 0.0), constraint_hertz=None, constraint_damping_ratio=None):
+    """Fill a spherical joint definition (the oracle's or the product's mirror struct)."""
+    d.body_a, d.body_b = body_a, body_b
+    d.local_frame_a = (ctypes.c_float * 7)(*frame_a)
+    d.local_frame_b = (ctypes.c_float * 7)(*frame_b)
+    d.constraint_hertz = default_hertz if constraint_hertz is None else constraint_hertz
+    d.constraint_damping_ratio = default_zeta if constraint_damping_ratio is None else constraint_damping_ratio
+    d.collide_connected = int(collide_connected)
+    d.enable_spring, d.hertz, d.damping_ratio = int(enable_spring), hertz, damping_ratio
+    d.target_rotation = (ctypes.c_float * 4)(*target_rotation)
+    d.enable_cone_limit, d.cone_angle = int(enable_cone_limit), cone_angle
+    d.enable_twist_limit = int(enable_twist_limit)
+    d.lower_twist_angle, d.upper_twist_angle = lower_twist_angle, upper_twist_angle
+    d.enable_motor, d.max_motor_torque = int(enable_motor), max_motor_torque
+    d.motor_velocity = (ctypes.c_float * 3)(*motor_velocity)
+    return d
+
+
 def _revolute_def(default_hertz, default_zeta, body_a, body_b, frame_a, frame_b, enable_limit, lower, upper,
                   enable_spring, hertz, damping_ratio, max_motor_torque, collide_connected, enable_motor,
                   motor_speed, target_angle, constraint_hertz, constraint_damping_ratio):
@@ -170,6 +208,7 @@ def _declare(lib):
                                         ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                         ctypes.c_float, ctypes.c_int]
     lib.nso_create_revolute_def.argtypes = [P, ctypes.POINTER(RevoluteDef)]
+    lib.nso_create_spherical_def.argtypes = [P, ctypes.POINTER(SphericalDef)]
     lib.nso_step.argtypes = [P, ctypes.c_float, ctypes.c_int]
     lib.nso_state_hash.argtypes = [P]
     lib.nso_state_hash.restype = ctypes.c_uint64
@@ -289,6 +328,12 @@ class OracleWorld:
                           collide_connected, enable_motor, motor_speed, target_angle, constraint_hertz,
                           constraint_damping_ratio)
         return self._lib.nso_create_revolute_def(self._w, ctypes.byref(d))
+
+    def create_spherical(self, body_a, body_b, frame_a, frame_b, **kw):
+        """A spherical joint (spherical_joint.rs:119); keywords as fill_spherical_def."""
+        d = fill_spherical_def(SphericalDef(), self._def.joint_hertz, self._def.joint_damping_ratio, body_a, body_b,
+                               frame_a, frame_b, **kw)
+        return self._lib.nso_create_spherical_def(self._w, ctypes.byref(d))
 
     def step(self, dt=1.0 / 60.0, substeps=4):
         self._lib.nso_step(self._w, dt, substeps)

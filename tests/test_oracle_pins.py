@@ -29,14 +29,14 @@ def _hashes(name, kw, steps):
     return out
 
 
-@pytest.mark.parametrize("name", ["large_pyramid", "many_pyramids"])
+@pytest.mark.parametrize("name", ["large_pyramid", "many_pyramids", "joint_grid"])
 def test_reference_golden_hash(name):
     """Tools/Benchmarks/reference-hashes.json: state hash after N steps of the benchmark scene."""
     case = json.load(open(os.path.join(GOLDEN, "reference_hashes.json")))["cases"][name]
     assert _hashes(name, {}, case["steps"])[-1] == case["hash"]
 
 
-@pytest.mark.parametrize("name", ["large_pyramid", "many_pyramids"])
+@pytest.mark.parametrize("name", ["large_pyramid", "many_pyramids", "joint_grid"])
 def test_colour_parallel_oracle_reproduces_golden_hash(name):
     """The oracle's colour-parallel loops (the reference arm's CPU path) give the same bits on
     four threads: every parallel loop touches disjoint data."""
