@@ -127,6 +127,31 @@ void ns_default_revolute_joint_def(ns_revolute_joint_def* def);
  * (>= 0) or -1. */
 int ns_create_revolute_joint_def(ns_world* world, const ns_revolute_joint_def* def);
 
+/* SphericalJointDef (types/joint_defs.rs:169, with its JointDef base :30): a ball-and-socket joint
+ * at the frames' origins; the cone limit bounds the angle between the frames' z axes, the twist
+ * limit the rotation about body B's z axis, the spring pulls the relative rotation to
+ * target_rotation and the motor drives the relative angular velocity to motor_velocity. */
+typedef struct {
+  int body_a, body_b;
+  float local_frame_a[7], local_frame_b[7]; /* position xyz + rotation xyzs */
+  float constraint_hertz;                    /* 60 */
+  float constraint_damping_ratio;            /* 2 */
+  int collide_connected;                     /* 0 */
+  int enable_spring;
+  float hertz, damping_ratio;
+  float target_rotation[4];                  /* xyzs, identity */
+  int enable_cone_limit;
+  float cone_angle;
+  int enable_twist_limit;
+  float lower_twist_angle, upper_twist_angle;
+  int enable_motor;
+  float max_motor_torque;
+  float motor_velocity[3];
+} ns_spherical_joint_def;
+void ns_default_spherical_joint_def(ns_spherical_joint_def* def);
+/* spherical_joint.rs:119 create_spherical_joint. Returns the joint id (>= 0) or -1. */
+int ns_create_spherical_joint_def(ns_world* world, const ns_spherical_joint_def* def);
+
 /* Batched worlds (no counterpart in the reference, which steps one world at a time): a world
  * can hold several independent sub-worlds that are stepped together by every ns_world_step.
  * Sub-world 0 exists from creation; ns_world_begin_subworld starts the next one and returns

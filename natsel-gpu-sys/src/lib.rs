@@ -100,6 +100,30 @@ pub struct ns_revolute_joint_def {
 
 #[repr(C)]
 #[derive(Clone, Copy, Debug, Default)]
+pub struct ns_spherical_joint_def {
+    pub body_a: c_int,
+    pub body_b: c_int,
+    pub local_frame_a: [f32; 7],
+    pub local_frame_b: [f32; 7],
+    pub constraint_hertz: f32,
+    pub constraint_damping_ratio: f32,
+    pub collide_connected: c_int,
+    pub enable_spring: c_int,
+    pub hertz: f32,
+    pub damping_ratio: f32,
+    pub target_rotation: [f32; 4],
+    pub enable_cone_limit: c_int,
+    pub cone_angle: f32,
+    pub enable_twist_limit: c_int,
+    pub lower_twist_angle: f32,
+    pub upper_twist_angle: f32,
+    pub enable_motor: c_int,
+    pub max_motor_torque: f32,
+    pub motor_velocity: [f32; 3],
+}
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
 pub struct ns_pair_job {
     pub type_a: i32,
     pub type_b: i32,
@@ -145,6 +169,8 @@ extern "C" {
                                     collide_connected: c_int) -> c_int;
     pub fn ns_default_revolute_joint_def(def: *mut ns_revolute_joint_def);
     pub fn ns_create_revolute_joint_def(world: *mut ns_world, def: *const ns_revolute_joint_def) -> c_int;
+    pub fn ns_default_spherical_joint_def(def: *mut ns_spherical_joint_def);
+    pub fn ns_create_spherical_joint_def(world: *mut ns_world, def: *const ns_spherical_joint_def) -> c_int;
 
     pub fn ns_world_begin_subworld(world: *mut ns_world) -> c_int;
     pub fn ns_world_subworld_count(world: *const ns_world) -> c_int;
@@ -261,6 +287,10 @@ impl GpuWorld {
 
     pub fn create_revolute(&mut self, def: &ns_revolute_joint_def) -> Result<i32, NsError> {
         self.id(unsafe { ns_create_revolute_joint_def(self.ptr, def) })
+    }
+
+    pub fn create_spherical(&mut self, def: &ns_spherical_joint_def) -> Result<i32, NsError> {
+        self.id(unsafe { ns_create_spherical_joint_def(self.ptr, def) })
     }
 
     /// The per-step external forces and torques (3 floats per body, body id order).

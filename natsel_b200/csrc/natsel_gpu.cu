@@ -1094,6 +1094,8 @@ int check_adjoint_scope(ns_world* w) {
   if (w->sub_body_begin.size() > 1) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint takes a single world");
   if (w->jr.off[kOverflowIndex + 1] > w->jr.off[kOverflowIndex])
     return fail(w, NS_ERR_UNSUPPORTED, "joints in the overflow colour; the adjoint does not cover them");
+  for (const DJoint& j : w->joints)
+    if (j.type != kJointRevolute) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint covers revolute joints only");
   if (w->def.enable_continuous) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint needs enable_continuous = 0");
   for (const HostBody& b : w->bodies)
     if (b.type == NS_KINEMATIC_BODY) return fail(w, NS_ERR_UNSUPPORTED, "the adjoint does not cover kinematic bodies");
@@ -1961,13 +1963,67 @@ void ns_default_revolute_joint_def(ns_revolute_joint_def* d) {
   d->constraint_damping_ratio = 2.0f;
 }
 
+static int add_joint(ns_world* w, DJoint j, int collide_connected);
+
 // revolute_joint.rs:161 create_revolute_joint with the whole RevoluteJointDef
 int ns_create_revolute_joint_def(ns_world* w, const ns_revolute_joint_def* def) {
   if (!w || !def) return -1;
-  int body_a = def->body_a, body_b = def->body_b;
+  DJoint j;
+  memset(&j, 0, sizeof(j));
+  j.type = kJointRevolute;
+  j.body_a = def->body_a; j.body_b = def->body_b;
   const float* fa = def->local_frame_a;
   const float* fb = def->local_frame_b;
-  int collide_connected = def->collide_connected;
+  j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
+  j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
+  j.constraint_hertz = def->constraint_hertz;
+  j.constraint_damping_ratio = def->constraint_damping_ratio;
+  j.enable_limit = def->enable_limit != 0; j.lower_angle = def->lower_angle; j.upper_angle = def->upper_angle;
+  j.enable_spring = def->enable_spring != 0; j.hertz = def->hertz; j.damping_ratio = def->damping_ratio;
+  j.target_angle = def->target_angle;
+  j.max_motor_torque = def->max_motor_torque; j.enable_motor = def->enable_motor != 0;
+  j.motor_speed = def->motor_speed;
+  return add_joint(w, j, def->collide_connected);
+}
+
+void ns_default_spherical_joint_def(ns_spherical_joint_def* d) {
+  memset(d, 0, sizeof(*d));
+  d->body_a = d->body_b = -1;
+  d->local_frame_a[6] = 1.0f;
+  d->local_frame_b[6] = 1.0f;
+  d->constraint_hertz = 60.0f;          // joint_defs.rs:54-55
+  d->constraint_damping_ratio = 2.0f;
+  d->target_rotation[3] = 1.0f;         // joint_defs.rs:185-203
+}
+
+// spherical_joint.rs:119 create_spherical_joint
+int ns_create_spherical_joint_def(ns_world* w, const ns_spherical_joint_def* def) {
+  if (!w || !def) return -1;
+  DJoint j;
+  memset(&j, 0, sizeof(j));
+  j.type = kJointSpherical;
+  j.body_a = def->body_a; j.body_b = def->body_b;
+  const float* fa = def->local_frame_a;
+  const float* fb = def->local_frame_b;
+  j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
+  j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
+  j.constraint_hertz = def->constraint_hertz;
+  j.constraint_damping_ratio = def->constraint_damping_ratio;
+  j.enable_spring = def->enable_spring != 0; j.hertz = def->hertz; j.damping_ratio = def->damping_ratio;
+  const float* t = def->target_rotation;
+  j.target_rotation = quat(v3(t[0], t[1], t[2]), t[3]);
+  j.enable_cone_limit = def->enable_cone_limit != 0; j.cone_angle = def->cone_angle;
+  j.enable_twist_limit = def->enable_twist_limit != 0;
+  j.lower_twist_angle = def->lower_twist_angle; j.upper_twist_angle = def->upper_twist_angle;
+  j.enable_motor = def->enable_motor != 0; j.max_motor_torque = def->max_motor_torque;
+  j.motor_velocity = v3(def->motor_velocity[0], def->motor_velocity[1], def->motor_velocity[2]);
+  return add_joint(w, j, def->collide_connected);
+}
+
+// joint.rs:164 create_joint: checks, the graph colour (constraint_graph.rs:256) and the bodies'
+// joint bookkeeping, for any joint type
+static int add_joint(ns_world* w, DJoint j, int collide_connected) {
+  const int body_a = j.body_a, body_b = j.body_b;
   if (w->uploaded) { w->err = "scene changes after the first step are not supported"; return -1; }
   int nb = (int)w->bodies.size();
   if (body_a < 0 || body_b < 0 || body_a >= nb || body_b >= nb || body_a == body_b) { w->err = "invalid joint bodies"; return -1; }
@@ -1978,21 +2034,9 @@ int ns_create_revolute_joint_def(ns_world* w, const ns_revolute_joint_def* def) 
     w->err = "joint bodies must belong to the newest sub-world";
     return -1;
   }
-  DJoint j;
-  memset(&j, 0, sizeof(j));
-  j.body_a = body_a; j.body_b = body_b;
   j.world = ba.world;
   j.enc_a = encode(ba); j.enc_b = encode(bb);
-  j.local_frame_a = xf(v3(fa[0], fa[1], fa[2]), quat(v3(fa[3], fa[4], fa[5]), fa[6]));
-  j.local_frame_b = xf(v3(fb[0], fb[1], fb[2]), quat(v3(fb[3], fb[4], fb[5]), fb[6]));
-  j.constraint_hertz = def->constraint_hertz;
-  j.constraint_damping_ratio = def->constraint_damping_ratio;
   j.constraint_softness.bias_rate = 0.0f; j.constraint_softness.mass_scale = 1.0f; j.constraint_softness.impulse_scale = 0.0f;
-  j.enable_limit = def->enable_limit != 0; j.lower_angle = def->lower_angle; j.upper_angle = def->upper_angle;
-  j.enable_spring = def->enable_spring != 0; j.hertz = def->hertz; j.damping_ratio = def->damping_ratio;
-  j.target_angle = def->target_angle;
-  j.max_motor_torque = def->max_motor_torque; j.enable_motor = def->enable_motor != 0;
-  j.motor_speed = def->motor_speed;
   // constraint_graph.rs:256 assign_joint_color
   uint32_t& ma = w->body_mask[body_a];
   uint32_t& mb = w->body_mask[body_b];

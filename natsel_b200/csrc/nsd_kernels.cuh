@@ -1363,6 +1363,36 @@ __global__ void k_prepare_joints(DW w, StepParams p) {
   j.frame_b.p = rotate(sb.q, j.local_frame_b.p - sb.local_center);
   Pos ca = {sa.cx, sa.cy, sa.cz}, cb = {sb.cx, sb.cy, sb.cz};
   j.delta_center = sub_pos(cb, ca);
+  if (j.type == kJointSpherical) {
+    // spherical_joint.rs:183-230
+    V3 cone_axis = rotate(j.frame_a.q, v3(0, 0, 1));
+    V3 twist_axis = rotate(j.frame_b.q, v3(0, 0, 1));
+    if (j.enable_cone_limit) {
+      V3 swing_axis = normalize(cross(cone_axis, twist_axis));
+      float k = dot(swing_axis, mul_mv(sum, swing_axis));
+      j.swing_mass = k > 0.0f ? 1.0f / k : 0.0f;
+      j.swing_axis = swing_axis;
+    }
+    if (j.enable_twist_limit) {
+      Q rel_q = inv_mul_quat(j.frame_a.q, j.frame_b.q);
+      float tan_half = sqrtf((rel_q.v.x * rel_q.v.x + rel_q.v.y * rel_q.v.y) /
+                             (rel_q.v.z * rel_q.v.z + rel_q.s * rel_q.s));
+      V3 swing_axis = normalize(cross(cone_axis, twist_axis));
+      V3 perp_axis = cross(swing_axis, cone_axis);
+      V3 jac = mul_add(cone_axis, tan_half, perp_axis);
+      float k = dot(jac, mul_mv(sum, jac));
+      j.twist_mass = k > 0.0f ? 1.0f / k : 0.0f;
+      j.twist_jacobian = jac;
+    }
+    j.rotation_mass = !j.fixed_rotation ? invert_matrix(sum) : m3zero();
+    j.spring_softness = make_soft(j.hertz, j.damping_ratio, p.h);
+    if (p.warm_start == 0.0f) {
+      j.linear_impulse = v3(0, 0, 0); j.motor_impulse3 = v3(0, 0, 0); j.spring_impulse3 = v3(0, 0, 0);
+      j.swing_impulse = 0; j.lower_impulse = 0; j.upper_impulse = 0;
+    }
+    w.joints[i] = j;
+    return;
+  }
   V3 axis = rotate(j.frame_a.q, v3(0, 0, 1));
   float k = dot(axis, mul_mv(sum, axis));
   j.axial_mass = k > 0.0f ? 1.0f / k : 0.0f;

@@ -176,6 +176,18 @@ NSD_HD Q normalize_quat(Q q) {                                                  
   }
   return qid();
 }
+// internal_math.rs:328 delta_quat_to_rotation
+NSD_HD V3 delta_quat_to_rotation(Q q, Q target) {
+  Q s = dot_quat(q, target) < 0.0f ? quat(v3(-q.v.x, -q.v.y, -q.v.z), -q.s) : q;
+  Q diff = quat(target.v - s.v, target.s - s.s);
+  Q product = mul_quat(diff, conjugate(s));
+  return 2.0f * product.v;
+}
+NSD_HD float get_swing_angle(Q q) {                                               // :502
+  float x = sqrtf(q.v.z * q.v.z + q.s * q.s);
+  float y = sqrtf(q.v.x * q.v.x + q.v.y * q.v.y);
+  return 2.0f * atan2_approx(y, x);
+}
 NSD_HD float get_twist_angle(Q q) {                                               // :490
   float twist = q.s < 0.0f ? atan2_approx(-q.v.z, -q.s) : atan2_approx(q.v.z, q.s);
   return twist * 2.0f;

@@ -869,9 +869,16 @@ __device__ V3 solve_point_constraint(float ma, float mb, M3 ia, M3 ib, V3 ra, V3
 __device__ __forceinline__ WarmDelta joint_warm_delta(const DJoint& j, Q dqa, Q dqb) {
   float mA = j.inv_mass_a, mB = j.inv_mass_b;
   V3 ra = rotate(dqa, j.frame_a.p), rb = rotate(dqb, j.frame_b.p);
-  float axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
-  V3 ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
-  ang = mul_add(ang, axial, j.rotation_axis_z);
+  V3 ang;
+  if (j.type == kJointSpherical) {  // spherical_joint.rs:233 warm_start_spherical_joint
+    ang = j.spring_impulse3 + j.motor_impulse3;
+    ang = ang - j.swing_impulse * j.swing_axis;
+    ang = mul_add(ang, j.lower_impulse - j.upper_impulse, j.twist_jacobian);
+  } else {
+    float axial = j.spring_impulse + j.motor_impulse + j.lower_impulse - j.upper_impulse;
+    ang = j.perp_impulse.x * j.perp_axis_x + j.perp_impulse.y * j.perp_axis_y;
+    ang = mul_add(ang, axial, j.rotation_axis_z);
+  }
   WarmDelta r;
   r.dva = mA * j.linear_impulse;
   r.dwa = mul_mv(j.inv_ia, cross(ra, j.linear_impulse) + ang);
@@ -890,6 +897,83 @@ __device__ __noinline__ void warm_start_joint(const DW& w, DJoint& j) {
   store_state_vw(w, j.index_b, sb);
 }
 
+// spherical_joint.rs:315-438: the spring, motor, twist limit and cone limit rows of
+// solve_spherical_joint (its point constraint is the revolute joint's)
+__device__ void spherical_angular(DJoint& j, const StepParams& p, Q qa, Q qb, M3 iA, M3 iB, bool use_bias, V3& wa,
+                                  V3& wb) {
+  Q rel_q = inv_mul_quat(qa, qb);
+  if (j.fixed_rotation || !(j.enable_spring || j.enable_motor || j.enable_twist_limit || j.enable_cone_limit)) return;
+  M3 sum = add_mm(iA, iB);
+  V3 cdot = wb - wa;
+  V3 ang = v3(0, 0, 0);
+  if (j.enable_spring) {
+    V3 dr = delta_quat_to_rotation(rel_q, j.target_rotation);
+    V3 c = -(rotate(qa, dr));
+    V3 bias = j.spring_softness.bias_rate * c;
+    float ms = j.spring_softness.mass_scale, is = j.spring_softness.impulse_scale;
+    V3 imp = (-ms) * mul_mv(j.rotation_mass, cdot + bias) - is * j.spring_impulse3;
+    j.spring_impulse3 = j.spring_impulse3 + imp;
+    cdot = cdot + mul_mv(sum, imp);
+    ang = ang + imp;
+  }
+  if (j.enable_motor) {
+    V3 lambda = -(mul_mv(j.rotation_mass, cdot - j.motor_velocity));
+    V3 next = j.motor_impulse3 + lambda;
+    float len = length(next);
+    float mx = j.max_motor_torque * p.h;
+    if (len > mx) next = (mx / len) * next;
+    lambda = next - j.motor_impulse3;
+    j.motor_impulse3 = next;
+    cdot = cdot + mul_mv(sum, lambda);
+    ang = ang + lambda;
+  }
+  if (j.enable_twist_limit) {
+    float twist = get_twist_angle(rel_q);
+    V3 jac = j.twist_jacobian;
+    V3 resp = mul_mv(sum, jac);
+    for (int side = 0; side < 2; ++side) {
+      float c = side == 0 ? twist - j.lower_twist_angle : j.upper_twist_angle - twist;
+      float bias = 0.0f, ms = 1.0f, is = 0.0f;
+      if (c > 0.0f) bias = c * p.inv_h;
+      else if (use_bias) {
+        bias = j.constraint_softness.bias_rate * c;
+        ms = j.constraint_softness.mass_scale;
+        is = j.constraint_softness.impulse_scale;
+      }
+      float tcd = side == 0 ? dot(cdot, jac) : -dot(cdot, jac);
+      float& imp = side == 0 ? j.lower_impulse : j.upper_impulse;
+      float old = imp;
+      float di = maxf(-ms * j.twist_mass * (tcd + bias) - is * old, -old);
+      imp = old + di;
+      if (side == 0) {
+        cdot = mul_add(cdot, di, resp);
+        ang = mul_add(ang, di, jac);
+      } else {
+        cdot = cdot - di * resp;
+        ang = ang - di * jac;
+      }
+    }
+  }
+  if (j.enable_cone_limit) {
+    float swing = get_swing_angle(rel_q);
+    float c = j.cone_angle - swing;
+    float bias = 0.0f, ms = 1.0f, is = 0.0f;
+    if (c > 0.0f) bias = c * p.inv_h;
+    else if (use_bias) {
+      bias = j.constraint_softness.bias_rate * c;
+      ms = j.constraint_softness.mass_scale;
+      is = j.constraint_softness.impulse_scale;
+    }
+    float scd = -dot(cdot, j.swing_axis);
+    float old = j.swing_impulse;
+    float di = maxf(-ms * j.swing_mass * (scd + bias) - is * old, -old);
+    j.swing_impulse = old + di;
+    ang = ang - di * j.swing_axis;
+  }
+  wa = wa - mul_mv(iA, ang);
+  wb = wb + mul_mv(iB, ang);
+}
+
 // revolute_joint.rs:316 solve_revolute_joint
 __device__ __noinline__ void solve_joint(const DW& w, const StepParams& p, DJoint& j, bool use_bias) {
   float mA = j.inv_mass_a, mB = j.inv_mass_b;
@@ -899,6 +983,10 @@ __device__ __noinline__ void solve_joint(const DW& w, const StepParams& p, DJoin
   bool fixed = j.fixed_rotation != 0;
   Q qa = mul_quat(sa.dq, j.frame_a.q);
   Q qb = mul_quat(sb.dq, j.frame_b.q);
+  if (j.type == kJointSpherical) {
+    spherical_angular(j, p, qa, qb, iA, iB, use_bias, wa, wb);
+    fixed = true;  // the revolute rows below do not apply
+  }
   if (dot_quat(qa, qb) < 0.0f) qb = quat(v3(-qb.v.x, -qb.v.y, -qb.v.z), -qb.s);
   Q rq = inv_mul_quat(qa, qb);
   if (!fixed && (j.enable_spring || j.enable_motor || j.enable_limit)) {

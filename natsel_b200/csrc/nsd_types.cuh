@@ -213,7 +213,18 @@ struct DJoint {
   Xf frame_a, frame_b;
   V3 rotation_axis_z, perp_axis_x, perp_axis_y, delta_center;
   float axial_mass;
+  // kJointSpherical (spherical_joint.rs:40 SphericalJointSim): lower_impulse / upper_impulse hold
+  // the twist limit impulses, the spring and motor impulses are vectors
+  int type;
+  int enable_cone_limit, enable_twist_limit;
+  float cone_angle, lower_twist_angle, upper_twist_angle;
+  Q target_rotation;
+  V3 motor_velocity, spring_impulse3, motor_impulse3;
+  float swing_impulse, swing_mass, twist_mass;
+  V3 swing_axis, twist_jacobian;
+  M3 rotation_mass;
 };
+enum : int { kJointRevolute = 0, kJointSpherical = 1 };
 
 // Per-step scalars (solver_integration.rs:1024 StepContext plus world settings).
 struct StepParams {

@@ -76,6 +76,22 @@ class ShapeDef(ctypes.Structure):
     ]
 
 
+class SphericalJointDef(ctypes.Structure):
+    """ns_spherical_joint_def (the reference's SphericalJointDef, types/joint_defs.rs:169)."""
+    _fields_ = [
+        ("body_a", ctypes.c_int), ("body_b", ctypes.c_int),
+        ("local_frame_a", ctypes.c_float * 7), ("local_frame_b", ctypes.c_float * 7),
+        ("constraint_hertz", ctypes.c_float), ("constraint_damping_ratio", ctypes.c_float),
+        ("collide_connected", ctypes.c_int),
+        ("enable_spring", ctypes.c_int), ("hertz", ctypes.c_float), ("damping_ratio", ctypes.c_float),
+        ("target_rotation", ctypes.c_float * 4),
+        ("enable_cone_limit", ctypes.c_int), ("cone_angle", ctypes.c_float),
+        ("enable_twist_limit", ctypes.c_int), ("lower_twist_angle", ctypes.c_float),
+        ("upper_twist_angle", ctypes.c_float),
+        ("enable_motor", ctypes.c_int), ("max_motor_torque", ctypes.c_float), ("motor_velocity", ctypes.c_float * 3),
+    ]
+
+
 class RevoluteJointDef(ctypes.Structure):
     """ns_revolute_joint_def (the reference's RevoluteJointDef, types/joint_defs.rs:154)."""
     _fields_ = [
@@ -116,7 +132,8 @@ _lib = None
 EXPORTED = [
     "ns_default_world_def", "ns_world_create", "ns_world_destroy", "ns_last_error",
     "ns_create_body", "ns_create_box_shape", "ns_create_sphere_shape", "ns_create_capsule_shape",
-    "ns_create_revolute_joint", "ns_default_revolute_joint_def", "ns_create_revolute_joint_def", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
+    "ns_create_revolute_joint", "ns_default_revolute_joint_def", "ns_create_revolute_joint_def",
+    "ns_default_spherical_joint_def", "ns_create_spherical_joint_def", "ns_world_step", "ns_world_synchronize", "ns_world_get_bodies",
     "ns_world_body_count", "ns_world_state_hash", "ns_world_contact_capacity", "ns_world_get_contacts",
     "ns_world_counters", "ns_world_phase_times", "ns_world_stream", "ns_world_solver_counts",
     "ns_collide_pairs", "ns_selftest_barrier_timeout", "ns_world_apply_forces", "ns_collide_pairs_noalloc",
@@ -152,6 +169,9 @@ def load_library(path=LIB_PATH):
     lib.ns_default_revolute_joint_def.argtypes = [ctypes.POINTER(RevoluteJointDef)]
     lib.ns_default_revolute_joint_def.restype = None
     lib.ns_create_revolute_joint_def.argtypes = [P, ctypes.POINTER(RevoluteJointDef)]
+    lib.ns_default_spherical_joint_def.argtypes = [ctypes.POINTER(SphericalJointDef)]
+    lib.ns_default_spherical_joint_def.restype = None
+    lib.ns_create_spherical_joint_def.argtypes = [P, ctypes.POINTER(SphericalJointDef)]
     lib.ns_world_autotune_table.argtypes = [P, P, P, P, P, ctypes.c_int]
     lib.ns_world_launch_shapes.argtypes = [P, P]
     lib.ns_world_set_launch_shapes.argtypes = [P, P]
@@ -287,6 +307,31 @@ class World:
                          max_motor_torque, collide_connected, enable_motor, motor_speed, target_angle,
                          constraint_hertz, constraint_damping_ratio)
         return self._id(self._lib.ns_create_revolute_joint_def(self._w, ctypes.byref(d)))
+
+    def create_spherical(self, body_a, body_b, frame_a, frame_b, collide_connected=False, enable_spring=False,
+                         hertz=0.0, damping_ratio=0.0, target_rotation=(0.0, 0.0, 0.0, 1.0), enable_cone_limit=False,
+                         cone_angle=0.0, enable_twist_limit=False, lower_twist_angle=0.0, upper_twist_angle=0.0,
+                         enable_motor=False, max_motor_torque=0.0, motor_velocity=(0.0, 0.0, 0.0),
+                         constraint_hertz=None, constraint_damping_ratio=None):
+        """A spherical joint (ns_create_spherical_joint_def; spherical_joint.rs:119). The
+        constraint softness defaults to the world's joint softness."""
+        d = SphericalJointDef()
+        self._lib.ns_default_spherical_joint_def(ctypes.byref(d))
+        d.body_a, d.body_b = body_a, body_b
+        d.local_frame_a = (ctypes.c_float * 7)(*frame_a)
+        d.local_frame_b = (ctypes.c_float * 7)(*frame_b)
+        d.constraint_hertz = self._def.joint_hertz if constraint_hertz is None else constraint_hertz
+        d.constraint_damping_ratio = (self._def.joint_damping_ratio if constraint_damping_ratio is None
+                                      else constraint_damping_ratio)
+        d.collide_connected = int(collide_connected)
+        d.enable_spring, d.hertz, d.damping_ratio = int(enable_spring), hertz, damping_ratio
+        d.target_rotation = (ctypes.c_float * 4)(*target_rotation)
+        d.enable_cone_limit, d.cone_angle = int(enable_cone_limit), cone_angle
+        d.enable_twist_limit = int(enable_twist_limit)
+        d.lower_twist_angle, d.upper_twist_angle = lower_twist_angle, upper_twist_angle
+        d.enable_motor, d.max_motor_torque = int(enable_motor), max_motor_torque
+        d.motor_velocity = (ctypes.c_float * 3)(*motor_velocity)
+        return self._id(self._lib.ns_create_spherical_joint_def(self._w, ctypes.byref(d)))
 
     # stepping and readback ----------------------------------------------
     def step(self, dt=1.0 / 60.0, substeps=4):
