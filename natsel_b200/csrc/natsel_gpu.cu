@@ -2029,7 +2029,6 @@ static int add_joint(ns_world* w, DJoint j, int collide_connected) {
   if (body_a < 0 || body_b < 0 || body_a >= nb || body_b >= nb || body_a == body_b) { w->err = "invalid joint bodies"; return -1; }
   HostBody& ba = w->bodies[body_a];
   HostBody& bb = w->bodies[body_b];
-  if (ba.type != NS_DYNAMIC_BODY && bb.type != NS_DYNAMIC_BODY) { w->err = "a joint needs a dynamic body"; return -1; }
   if (ba.world != bb.world || ba.world != (int)w->sub_body_begin.size() - 1) {
     w->err = "joint bodies must belong to the newest sub-world";
     return -1;
@@ -2041,7 +2040,9 @@ static int add_joint(ns_world* w, DJoint j, int collide_connected) {
   uint32_t& ma = w->body_mask[body_a];
   uint32_t& mb = w->body_mask[body_b];
   int color = kOverflowIndex;
-  if (ba.type == NS_DYNAMIC_BODY && bb.type == NS_DYNAMIC_BODY) {
+  if (ba.type != NS_DYNAMIC_BODY && bb.type != NS_DYNAMIC_BODY) {
+    color = -1;  // joint.rs:251-262: not attached to a dynamic body, kept in the static set, never solved
+  } else if (ba.type == NS_DYNAMIC_BODY && bb.type == NS_DYNAMIC_BODY) {
     uint32_t avail = ~(ma | mb) & ((1u << kDynamicColorCount) - 1u);
     if (avail) { color = __builtin_ctz(avail); ma |= 1u << color; mb |= 1u << color; }
   } else {

@@ -2113,8 +2113,10 @@ static int add_revolute(nso_world* w, Joint j) {
     for (int i = kOverflowIndex - 1; i >= 1; --i)
       if (!get_bit(w, i, body_b)) { set_bit(w, i, body_b); color = i; break; }
   }
+  // joint.rs:251-262: a joint not attached to a dynamic body stays in the static set, unsolved
+  if (ba.type != 2 && bb.type != 2) color = -1;
   j.color = color;
-  w->colors[color].joints.push_back(id);
+  if (color >= 0) w->colors[color].joints.push_back(id);
   w->joints.push_back(j);
   return id;
 }
