@@ -241,6 +241,66 @@ __device__ __forceinline__ void load_direct(const CPlanes& P, int k, int stage, 
   }
 }
 
+// A constraint's planes staged in shared memory ahead of its phase: one column per lane of the
+// block's first warp, rows idx, mass, ia0, ia1, ib1, n, t1, t2, ca, cb, fr, roll, rm, tm, then
+// pra, prb and pimp of the four points (all four are copied: the point count is in idx).
+constexpr int kStageRows = 26;
+typedef float4 StageBuf[kStageRows][32];
+__device__ __forceinline__ void cp_async16(float4* smem, const void* gmem) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+// Issue the copies of constraint k for the given stage (push or relax). The planes other than
+// the impulses are constant during the launch and the impulses are written only by the thread
+// that owns the constraint (this one), in earlier phases.
+__device__ __forceinline__ void stage_constraint(const CPlanes& P, int k, int stage, StageBuf& b, int lane) {
+  cp_async16(&b[0][lane], &P.idx[k]);
+  cp_async16(&b[1][lane], &P.mass[k]);
+  cp_async16(&b[2][lane], &P.ia0[k]);
+  cp_async16(&b[3][lane], &P.ia1[k]);
+  cp_async16(&b[4][lane], &P.ib1[k]);
+  cp_async16(&b[5][lane], &P.n[k]);
+  if (stage == kRelax) {
+    cp_async16(&b[6][lane], &P.t1[k]);
+    cp_async16(&b[7][lane], &P.t2[k]);
+    cp_async16(&b[8][lane], &P.ca[k]);
+    cp_async16(&b[9][lane], &P.cb[k]);
+    cp_async16(&b[10][lane], &P.fr[k]);
+    cp_async16(&b[11][lane], &P.roll[k]);
+    cp_async16(&b[12][lane], &P.rm[k]);
+    cp_async16(&b[13][lane], &P.tm[k]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    cp_async16(&b[14 + q][lane], &P.pra[q * P.cap + k]);
+    cp_async16(&b[18 + q][lane], &P.prb[q * P.cap + k]);
+    cp_async16(&b[22 + q][lane], &P.pimp[q * P.cap + k]);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// load_direct's result (push or relax) from the staged copy.
+__device__ __forceinline__ void load_staged(const StageBuf& b, int lane, int stage, CData& d) {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float4 i4 = b[0][lane];
+  int4 idx = make_int4(__float_as_int(i4.x), __float_as_int(i4.y), __float_as_int(i4.z), __float_as_int(i4.w));
+  d.c = unpack_constraint(idx, b[1][lane], b[2][lane], b[3][lane], b[4][lane], b[5][lane]);
+  d.t1 = z; d.t2 = z; d.ca = z; d.cb = z; d.fr = z; d.roll = z; d.rm = z; d.tm = z;
+  if (stage == kRelax) {
+    d.t1 = b[6][lane]; d.t2 = b[7][lane]; d.ca = b[8][lane]; d.cb = b[9][lane];
+    d.fr = b[10][lane]; d.roll = b[11][lane]; d.rm = b[12][lane]; d.tm = b[13][lane];
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    d.pra[q] = z; d.prb[q] = z; d.pimp[q] = z; d.prest[q] = 0.0f;
+    if (q < d.c.pc) {
+      d.pra[q] = b[14 + q][lane];
+      d.prb[q] = b[18 + q][lane];
+      d.pimp[q] = b[22 + q][lane];
+    }
+  }
+}
+
 // Change of the two bodies' velocities by one warm start: body a gets v - dva, w - dwa and
 // body b v + dvb, w + dvb. It depends on the constraint's planes and impulses only, not on the
 // bodies' velocities, so it can be formed when the impulses are last updated and applied later
@@ -1314,6 +1374,11 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
   // a colour with fewer items than the launch has threads occupies every SM with a few warps
   // instead of filling the first blocks, and a phase's time follows the warps per SM.
   const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
+  // A contact colour small enough that only the blocks' first warps hold items (one chunk of 32
+  // per block) has its constraints staged in shared memory while the phase before it ends, so
+  // after the barrier only the body states are fetched.
+  __shared__ StageBuf stage_buf;
+  bool staged = false;
   int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
@@ -1366,7 +1431,8 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
       for (int t = g >= nj ? g : g + ((nj - g + stride - 1) / stride) * stride; t < total; t += stride) {
         int k = coff[c] + (t - nj);
         CData d;
-        load_direct(w.cp, k, stage, d);
+        if (staged && t == g) load_staged(stage_buf, (int)threadIdx.x, stage, d);
+        else load_direct(w.cp, k, stage, d);
         if (kTape && (stage == kPush || stage == kRelax) && s < main_phases) tape_contact(w, tp, sub, stage, k, d);
         if (kTape && stage == kRestitution && tp.rest && d.c.restitution > 0.0f)
           tape_restitution(w, tp, (s - main_phases) / n_rph, k, d);
@@ -1385,7 +1451,23 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
         }
       }
     }
-    if (!phase_sync<kGrid>(w.ctl, bar)) return;
+    staged = false;
+    if (s + 1 < total_phases) {
+      const int nph = phase_at(s + 1);
+      const int nstage = nph >> 5;
+      if (nph < kPhaseIntegrateVelocity && (nstage == kPush || nstage == kRelax)) {
+        int nj2, total2;
+        contact_range(nph, nj2, total2);
+        if (nj2 == 0 && total2 <= 32 * (int)gridDim.x && threadIdx.x < 32 && g < total2) {
+          stage_constraint(w.cp, coff[nph & 31] + g, nstage, stage_buf, (int)threadIdx.x);
+          staged = true;
+        }
+      }
+    }
+    if (!phase_sync<kGrid>(w.ctl, bar)) {
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      return;
+    }
   }
   // store impulses (contact_solver.rs:1258; overflow_contact_solver.rs:688)
   for (int wi = g; wi < w.n_worlds; wi += stride) store_overflow(w, w.world_cbase[wi], w.ovf_count[wi]);
