@@ -96,6 +96,9 @@ def parse_args(argv=None):
                     help="steps of each differentiable rollout (64 in the workload; fewer for profiling)")
     ap.add_argument("--no-subrecords", action="store_true",
                     help="skip the batched-worlds, jointed-chains and differentiable-rollout sub-records")
+    ap.add_argument("--shapes", default=None,
+                    help="launch shapes as JSON (the keys of World.launch_shapes()) instead of the autotuner's "
+                         "choice, for profiling a fixed configuration")
     ap.add_argument("--sub-steps", type=int, default=10,
                     help="timed steps of each sampled sub-record (batched worlds, jointed chains)")
     return ap.parse_args(argv)
@@ -735,6 +738,13 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
                     for b, g, ms in world.autotune(DT, sub, 3)]
         tune_rows, shapes = world.autotune_table(), world.launch_shapes()
         done = warmup
+    elif args.shapes and headline:
+        tune_step, autotune, tune_rows = None, None, None
+        shapes = dict(world.launch_shapes(), **json.loads(args.shapes))
+        world.set_launch_shapes(shapes)
+        for _ in range(warmup):
+            world.step(DT, sub)
+        done = warmup
     else:
         tune_step = length // 2
         tw, _, _ = build_gpu_world(scene, kw, ctx.local_rank, indices)
@@ -777,7 +787,8 @@ def measure_plain(args, ctx, scene, kw, desc, steps, warmup, headline):
     rec["autotune"] = {"chosen": shapes, "candidates": tune_rows, "tuned_at_step": tune_step,
                        "method": "each candidate steps 1 + 3 steps from a copy of the world's state at the "
                                  "tuning step, CUDA events; one kernel at a time, the fastest kept; the world "
-                                 "is restored, and the measured world takes the chosen shapes"}
+                                 "is restored, and the measured world takes the chosen shapes"
+                                 if autotune is not None else "fixed by --shapes"}
     if headline and not args.no_e2e:
         rec["e2e"] = measure_e2e(ctx, scene, kw, schedule, indices, warmup, shapes)
     if headline and ctx.rank == 0 and ctx.world_size == 1 and not args.no_cpu_baseline and scene == "batched_worlds":

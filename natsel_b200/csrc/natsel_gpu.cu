@@ -98,7 +98,7 @@ struct ns_world {
   int prepare_threads = kPrepareThreads, prepare_per_sm = 16;       // k_prepare_slots
   std::vector<std::array<float, 4>> tune_rows;  // last autotune: dimension, a, b, ms per step
   int sort_bits = 32;              // key bits of the broadphase sort (bucket index + large flag)
-  bool state_shared = false;
+  int state_mode = 0;
   size_t state_smem = 0;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -651,13 +651,15 @@ int upload_world(ns_world* w) {
   w->allocations.push_back(w->cub_scan_tmp);
   w->allocation_bytes.push_back(std::max<size_t>(w->cub_scan_bytes, 16));
   // state pass: staged change chunks always live in shared memory; every body's color
-  // mask joins them there when it fits
+  // mask joins them there when it fits, and with it a per-body word for the parallel rounds
+  // when that fits too (state_mode 2; 1: masks only, serial walk; 0: masks in global memory)
   int max_smem = 0;
   NS_CUDA(w, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, w->def.device));
   size_t stage_bytes = (size_t)kStateChunk * 5 * sizeof(int);
   size_t need = stage_bytes + (size_t)nb * sizeof(uint32_t);
-  w->state_shared = need + 16 * 1024 <= (size_t)max_smem;
-  w->state_smem = w->state_shared ? need : stage_bytes;
+  size_t need2 = need + (size_t)nb * sizeof(int);
+  w->state_mode = need2 + 16 * 1024 <= (size_t)max_smem ? 2 : need + 16 * 1024 <= (size_t)max_smem ? 1 : 0;
+  w->state_smem = w->state_mode == 2 ? need2 : w->state_mode == 1 ? need : stage_bytes;
   // the kernel's static shared memory counts against the same 48 KB default, so the limit is
   // always raised to what this launch needs
   NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
@@ -826,7 +828,7 @@ int enqueue_step(ns_world* w, float dt, int substeps, const HostStepTape* tape =
   NS_CUDA(w, cudaEventRecordWithFlags(w->ev[2], s, ev_flags));
   // state pass, colors, prepare (collide_pass.rs:386, solver_prepare.rs:269)
   if (d.n_worlds == 1) {
-    k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_shared ? 1 : 0); ++nk;
+    k_state_pass<<<1, kStatePassThreads, w->state_smem, s>>>(d, w->state_mode); ++nk;
   } else {
     NS_CUDA(w, cudaMemsetAsync(&d.ctl->changed_count, 0, sizeof(int), s));
     NS_CUDA(w, cudaMemsetAsync(&d.ctl->overflow_count, 0, sizeof(int), s));

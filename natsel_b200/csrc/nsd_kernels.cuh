@@ -4,6 +4,7 @@
 // Each kernel cites the reference stage it replaces; arithmetic keeps the
 // reference operand order so results match the reference bit for bit.
 #pragma once
+#include <climits>
 #include <cub/cub.cuh>
 #include "nsd_types.cuh"
 
@@ -824,6 +825,106 @@ __device__ int state_walk(const DW& w, MaskT mask, const StateStage& st, int n, 
   return ovf;
 }
 
+// The same transitions with the whole block, in rounds: a change is applied once it is the
+// lowest-numbered change still pending on each of its dynamic bodies (minp[body], kept in shared
+// memory), so every body's mask sees its changes in id order, as in state_walk, and changes on
+// disjoint bodies run together. Static and kinematic bodies never hold colour bits, so only
+// dynamic bodies order the changes. Edits of the overflow list depend on the order of all of
+// them, so the rounds only mark them (bit 26 append, bit 27 remove) and one thread applies them
+// in id order afterwards. Bit 25 marks an applied change. Returns the new overflow count.
+constexpr int kStateDone = 1 << 25, kStateOvfAppend = 1 << 26, kStateOvfRemove = 1 << 27;
+__device__ int state_walk_rounds(const DW& w, uint32_t* mask, int* minp, const StateStage& st, int n, int ovf) {
+  const int t = threadIdx.x;
+  for (;;) {
+    int pending = 0;
+    for (int i = t; i < n; i += kStatePassThreads) {
+      int info = st.info[i];
+      if (info & kStateDone) continue;
+      pending = 1;
+      if ((info >> 8) & 1) atomicMin(&minp[st.ba[i]], i);
+      if ((info >> 9) & 1) atomicMin(&minp[st.bb[i]], i);
+    }
+    if (!__syncthreads_or(pending)) break;
+    for (int i = t; i < n; i += kStatePassThreads) {
+      int info = st.info[i];
+      if (info & kStateDone) continue;
+      const bool dyn_a = (info >> 8) & 1, dyn_b = (info >> 9) & 1;
+      const int a = st.ba[i], b = st.bb[i];
+      if ((dyn_a && minp[a] != i) || (dyn_b && minp[b] != i)) continue;
+      uint32_t f = st.flags[i];
+      int old_color = (info & 255) - 1;
+      int new_color = old_color, destroyed = 0, ovf_op = 0;
+      auto remove = [&](int color) {  // constraint_graph.rs:200
+        if (color != kOverflowIndex) {
+          if (dyn_a) mask[a] &= ~(1u << color);
+          if (dyn_b) mask[b] &= ~(1u << color);
+        } else {
+          ovf_op = kStateOvfRemove;
+        }
+      };
+      if (f == 0) {
+      } else if (f & cSimDisjoint) {
+        if (old_color != -1) remove(old_color);
+        new_color = -1;
+        destroyed = 1;
+      } else if (f & cSimStarted) {
+        int color = kOverflowIndex;
+        if (dyn_a && dyn_b) {
+          uint32_t avail = ~(mask[a] | mask[b]) & ((1u << kDynamicColorCount) - 1u);
+          if (avail) {
+            color = __ffs(avail) - 1;
+            mask[a] |= 1u << color;
+            mask[b] |= 1u << color;
+          }
+        } else {
+          int d = dyn_a ? a : b;
+          uint32_t avail = ~mask[d] & (((1u << kOverflowIndex) - 1u) & ~1u);  // colors 22..1
+          if (avail) {
+            color = 31 - __clz(avail);
+            mask[d] |= 1u << color;
+          }
+        }
+        new_color = color;
+        if (color == kOverflowIndex) ovf_op = kStateOvfAppend;
+      } else if (f & cSimStopped) {
+        remove(old_color);
+        new_color = -1;
+      }
+      st.info[i] = (info & 0xffff) | ((new_color + 1) << 16) | (destroyed << 24) | kStateDone | ovf_op;
+    }
+    __syncthreads();
+    for (int i = t; i < n; i += kStatePassThreads) {
+      minp[st.ba[i]] = INT_MAX;
+      minp[st.bb[i]] = INT_MAX;
+    }
+    __syncthreads();
+  }
+  __shared__ int ovf_s2;
+  if (t == 0) {
+    for (int i = 0; i < n; ++i) {
+      int info = st.info[i];
+      int cid = st.cid[i];
+      if (info & kStateOvfRemove) {
+        int local = w.contacts[cid].local;
+        int last = ovf - 1;
+        if (local != last) {
+          int moved = w.overflow_list[last];
+          w.overflow_list[local] = moved;
+          w.contacts[moved].local = local;
+        }
+        ovf = last;
+      } else if (info & kStateOvfAppend) {
+        w.contacts[cid].local = ovf;
+        w.overflow_list[ovf] = cid;
+        ovf++;
+      }
+    }
+    ovf_s2 = ovf;
+  }
+  __syncthreads();
+  return ovf_s2;
+}
+
 __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_shared) {
   extern __shared__ uint32_t dyn_smem[];
   typedef cub::BlockScan<int, kStatePassThreads> Scan;
@@ -856,8 +957,12 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
   st.ba = st.info + kStateChunk;
   st.bb = st.ba + kStateChunk;
   uint32_t* smask = (uint32_t*)(st.bb + kStateChunk);
+  int* minp = (int*)(smask + w.n_bodies);  // use_shared == 2: the rounds' per-body minimum
   if (use_shared) {
     for (int b = t; b < w.n_bodies; b += kStatePassThreads) smask[b] = w.body_mask[b];
+  }
+  if (use_shared == 2) {
+    for (int b = t; b < w.n_bodies; b += kStatePassThreads) minp[b] = INT_MAX;
   }
   for (int base = 0; base < total; base += kStateChunk) {
     int n = min(kStateChunk, total - base);
@@ -871,7 +976,12 @@ __global__ void __launch_bounds__(kStatePassThreads) k_state_pass(DW w, int use_
       st.info[i] = (c.color + 1) | ((int)w.body_dyn[c.body_a] << 8) | ((int)w.body_dyn[c.body_b] << 9);
     }
     __syncthreads();
-    if (t == 0) ovf_s = use_shared ? state_walk(w, smask, st, n, ovf_s) : state_walk(w, w.body_mask, st, n, ovf_s);
+    if (use_shared == 2) {
+      int o = state_walk_rounds(w, smask, minp, st, n, ovf_s);
+      if (t == 0) ovf_s = o;
+    } else if (t == 0) {
+      ovf_s = use_shared ? state_walk(w, smask, st, n, ovf_s) : state_walk(w, w.body_mask, st, n, ovf_s);
+    }
     __syncthreads();
     for (int i = t; i < n; i += kStatePassThreads) {
       DContact& c = w.contacts[st.cid[i]];
