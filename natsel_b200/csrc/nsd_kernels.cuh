@@ -725,6 +725,8 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
 
 // Narrowphase, second pass: full updates, kind by kind, so a warp runs one shape
 // combination. Contacts are independent here: the order only changes which warp runs what.
+// The kinds go from the costliest (hull-hull) to the cheapest (sphere-sphere), so the last
+// blocks to start are the short ones and the launch does not wait on a tail of hull pairs.
 // Small blocks spread the updates over every SM: a thread keeps ~2 KB of clip polygons on its
 // stack, and fewer warps per SM keep more of it in L1. The minimum of one block per SM lets the
 // compiler keep the manifold routines in 213 registers without spills (it targets 168 with
@@ -732,16 +734,16 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
 constexpr int kCollideUpdateThreads = 64;
 __global__ void __launch_bounds__(kCollideUpdateThreads, 1) k_collide_update(DW w) {
   __shared__ int start[kPairKinds + 1];
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0) {  // start[r]: first item of the r-th kind in cost order (kind 5 - r)
     int acc = 0;
-    for (int k = 0; k < kPairKinds; ++k) { start[k] = acc; acc += w.ctl->collide_count[k]; }
+    for (int r = 0; r < kPairKinds; ++r) { start[r] = acc; acc += w.ctl->collide_count[kPairKinds - 1 - r]; }
     start[kPairKinds] = acc;
   }
   __syncthreads();
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < start[kPairKinds]; t += gridDim.x * blockDim.x) {
-    int k = 0;
-    while (t >= start[k + 1]) ++k;
-    collide_full(w, w.collide_list[(size_t)k * w.cap + (t - start[k])]);
+    int r = 0;
+    while (t >= start[r + 1]) ++r;
+    collide_full(w, w.collide_list[(size_t)(kPairKinds - 1 - r) * w.cap + (t - start[r])]);
   }
 }
 
