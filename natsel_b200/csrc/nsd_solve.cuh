@@ -1374,9 +1374,9 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
   // a colour with fewer items than the launch has threads occupies every SM with a few warps
   // instead of filling the first blocks, and a phase's time follows the warps per SM.
   const int g = (((int)threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + ((int)threadIdx.x & 31);
-  // A contact colour small enough that only the blocks' first warps hold items (one chunk of 32
-  // per block) has its constraints staged in shared memory while the phase before it ends, so
-  // after the barrier only the body states are fetched.
+  // The contact that a thread of a block's first warp holds in the next phase (when the phase's
+  // items are at most one per thread) is staged in shared memory while the phase before it
+  // ends, so after the barrier only the body states are fetched.
   __shared__ StageBuf stage_buf;
   bool staged = false;
   int bar = 0;
@@ -1458,8 +1458,10 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
       if (nph < kPhaseIntegrateVelocity && (nstage == kPush || nstage == kRelax)) {
         int nj2, total2;
         contact_range(nph, nj2, total2);
-        if (nj2 == 0 && total2 <= 32 * (int)gridDim.x && threadIdx.x < 32 && g < total2) {
-          stage_constraint(w.cp, coff[nph & 31] + g, nstage, stage_buf, (int)threadIdx.x);
+        // the contacts follow the colour's joints (items nj2..total2-1); a thread's first
+        // contact of the colour is item g when g >= nj2, and its only one when total2 <= stride
+        if (total2 <= stride && threadIdx.x < 32 && g >= nj2 && g < total2) {
+          stage_constraint(w.cp, coff[nph & 31] + (g - nj2), nstage, stage_buf, (int)threadIdx.x);
           staged = true;
         }
       }
