@@ -106,7 +106,9 @@ def parse_args(argv=None):
 
 def timed_schedule(length, steps, warmup):
     """1-based numbers of the K timed steps: every stride-th step from W + 1, with stride =
-    max(1, (length - W) // K), so the K steps cover the workload's whole run."""
+    max(1, (length - W) // K), so the K steps cover the workload's whole run (K is capped at the
+    length - W steps the run has after the warm-up)."""
+    steps = max(1, min(steps, length - warmup))
     stride = max(1, (length - warmup) // steps)
     return [warmup + 1 + k * stride for k in range(steps)]
 

@@ -103,3 +103,12 @@ def test_partition_is_balanced_and_deterministic():
         loads = share_loads(sizes, shares)
         # greedy longest-first packing: within the largest item of the best possible split
         assert max(loads) - min(loads) <= max(sizes)
+
+
+def test_timed_schedule_spreads_over_the_run_and_stays_inside_it():
+    """K timed steps every (length - W) // K steps from W + 1; K is capped at the steps the run
+    has after the warm-up, so no timed step lies beyond the workload's length."""
+    assert bench.timed_schedule(600, 20, 5) == [6 + 29 * k for k in range(20)]
+    full = bench.timed_schedule(600, 600, 3)
+    assert full == list(range(4, 601))
+    assert bench.timed_schedule(1000, 10, 3)[-1] <= 1000
