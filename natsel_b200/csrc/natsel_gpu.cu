@@ -572,7 +572,7 @@ int upload_world(ns_world* w) {
   ALLOC(bp_vals_in, int, nsh); ALLOC(bp_vals_out, int, nsh);
   ALLOC(bp_xy, float4, nsh); ALLOC(bp_z, float2, nsh); ALLOC(bp_meta, int, nsh);
   ALLOC(cells, int2, (size_t)d.cell_mask + 1); ALLOC(bp_world, int, nsh);
-  ALLOC(collide_list, int, (size_t)kPairKinds * cap);
+  ALLOC(collide_list, int, (size_t)kCollideQueues * cap);
   ALLOC(world_cbase, int, n_worlds + 1); ALLOC(world_shape, int, n_worlds + 1);
   ALLOC(pool_top, int, n_worlds); ALLOC(pool_next, int, n_worlds); ALLOC(ovf_count, int, n_worlds);
   ALLOC(large_off, int, n_worlds + 1);

@@ -418,6 +418,9 @@ __global__ void __launch_bounds__(1024) k_bp_segsort_long(DW w) {
 // Six pair kinds, A being the primary shape: sphere-sphere, capsule-sphere, capsule-capsule,
 // hull-sphere, hull-capsule, hull-hull.
 constexpr int kPairKinds = 6;
+// Queues of the narrowphase's update pass: kinds 0..4, and the hull pairs (kind 5) split by the
+// type of their SAT cache, so the lanes of a warp mostly take the same path through it.
+constexpr int kCollideQueues = 11;
 __device__ __forceinline__ int pair_kind(int ta, int tb) {
   if (ta == kSphere) return 0;
   if (ta == kCapsule) return tb == kSphere ? 1 : 2;
@@ -716,34 +719,35 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
   for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
     if (!(w.slot_state[cid] & kSlotAlive)) continue;
     if (collide_recycle(w, cid)) {
-      int kind = w.contacts[cid].kind;
-      int slot = slot_converged(w.ctl->collide_count, kind);
-      w.collide_list[(size_t)kind * w.cap + slot] = cid;
+      const DContact& c = w.contacts[cid];
+      int q = c.kind < kPairKinds - 1 ? c.kind : kPairKinds - 1 + min((int)c.sat.type, 5);
+      int slot = slot_converged(w.ctl->collide_count, q);
+      w.collide_list[(size_t)q * w.cap + slot] = cid;
     }
   }
 }
 
 // Narrowphase, second pass: full updates, kind by kind, so a warp runs one shape
 // combination. Contacts are independent here: the order only changes which warp runs what.
-// The kinds go from the costliest (hull-hull) to the cheapest (sphere-sphere), so the last
-// blocks to start are the short ones and the launch does not wait on a tail of hull pairs.
+// The queues go from the costliest (the hull pairs) to the cheapest (sphere-sphere), so the
+// last blocks to start are the short ones and the launch does not wait on a tail of hull pairs.
 // Small blocks spread the updates over every SM: a thread keeps ~2 KB of clip polygons on its
 // stack, and fewer warps per SM keep more of it in L1. The minimum of one block per SM lets the
 // compiler keep the manifold routines in 213 registers without spills (it targets 168 with
 // spills otherwise).
 constexpr int kCollideUpdateThreads = 64;
 __global__ void __launch_bounds__(kCollideUpdateThreads, 1) k_collide_update(DW w) {
-  __shared__ int start[kPairKinds + 1];
-  if (threadIdx.x == 0) {  // start[r]: first item of the r-th kind in cost order (kind 5 - r)
+  __shared__ int start[kCollideQueues + 1];
+  if (threadIdx.x == 0) {  // start[r]: first item of the r-th queue in cost order (queue 10 - r)
     int acc = 0;
-    for (int r = 0; r < kPairKinds; ++r) { start[r] = acc; acc += w.ctl->collide_count[kPairKinds - 1 - r]; }
-    start[kPairKinds] = acc;
+    for (int r = 0; r < kCollideQueues; ++r) { start[r] = acc; acc += w.ctl->collide_count[kCollideQueues - 1 - r]; }
+    start[kCollideQueues] = acc;
   }
   __syncthreads();
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < start[kPairKinds]; t += gridDim.x * blockDim.x) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < start[kCollideQueues]; t += gridDim.x * blockDim.x) {
     int r = 0;
     while (t >= start[r + 1]) ++r;
-    collide_full(w, w.collide_list[(size_t)(kPairKinds - 1 - r) * w.cap + (t - start[r])]);
+    collide_full(w, w.collide_list[(size_t)(kCollideQueues - 1 - r) * w.cap + (t - start[r])]);
   }
 }
 

@@ -256,7 +256,8 @@ struct Control {
   int color_count[24];    // constraints per color (colors 0..22)
   int color_offset[25];
   int live_contacts;
-  int collide_count[6];   // contacts per pair kind queued for a full manifold update
+  int collide_count[11];  // contacts queued for a full manifold update: pair kinds 0..4, then the
+                          // hull pairs by the type of their SAT cache (0..5)
   int long_segments;      // candidate segments handed to the block sort this pair update
   int fast_count;         // fast bodies queued by finalize for the continuous pass (this step)
   int bullet_count;       // fast bullets queued by finalize for the bullet pass (this step)
