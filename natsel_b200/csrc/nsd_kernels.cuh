@@ -418,9 +418,15 @@ __global__ void __launch_bounds__(1024) k_bp_segsort_long(DW w) {
 // Six pair kinds, A being the primary shape: sphere-sphere, capsule-sphere, capsule-capsule,
 // hull-sphere, hull-capsule, hull-hull.
 constexpr int kPairKinds = 6;
-// Queues of the narrowphase's update pass: kinds 0..4, and the hull pairs (kind 5) split by the
-// type of their SAT cache, so the lanes of a warp mostly take the same path through it.
-constexpr int kCollideQueues = 11;
+// Queues of the narrowphase's update pass: kinds 0..2, the GJK pairs (kinds 3, 4) split by the
+// size of their simplex cache and the hull pairs (kind 5) by the type of their SAT cache, so the
+// lanes of a warp mostly take the same path through the update.
+constexpr int kCollideQueues = 17;
+__device__ __forceinline__ int collide_queue(const DContact& c) {
+  if (c.kind < 3) return c.kind;
+  if (c.kind < 5) return 3 + 4 * (c.kind - 3) + min((int)c.simplex.count, 3);
+  return 11 + min((int)c.sat.type, 5);
+}
 __device__ __forceinline__ int pair_kind(int ta, int tb) {
   if (ta == kSphere) return 0;
   if (ta == kCapsule) return tb == kSphere ? 1 : 2;
@@ -719,8 +725,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
   for (int cid = blockIdx.x * blockDim.x + threadIdx.x; cid < w.cap; cid += gridDim.x * blockDim.x) {
     if (!(w.slot_state[cid] & kSlotAlive)) continue;
     if (collide_recycle(w, cid)) {
-      const DContact& c = w.contacts[cid];
-      int q = c.kind < kPairKinds - 1 ? c.kind : kPairKinds - 1 + min((int)c.sat.type, 5);
+      int q = collide_queue(w.contacts[cid]);
       int slot = slot_converged(w.ctl->collide_count, q);
       w.collide_list[(size_t)q * w.cap + slot] = cid;
     }
@@ -738,7 +743,7 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide(DW w) {
 constexpr int kCollideUpdateThreads = 64;
 __global__ void __launch_bounds__(kCollideUpdateThreads, 1) k_collide_update(DW w) {
   __shared__ int start[kCollideQueues + 1];
-  if (threadIdx.x == 0) {  // start[r]: first item of the r-th queue in cost order (queue 10 - r)
+  if (threadIdx.x == 0) {  // start[r]: first item of the r-th queue in cost order (queue 16 - r)
     int acc = 0;
     for (int r = 0; r < kCollideQueues; ++r) { start[r] = acc; acc += w.ctl->collide_count[kCollideQueues - 1 - r]; }
     start[kCollideQueues] = acc;

@@ -256,8 +256,9 @@ struct Control {
   int color_count[24];    // constraints per color (colors 0..22)
   int color_offset[25];
   int live_contacts;
-  int collide_count[11];  // contacts queued for a full manifold update: pair kinds 0..4, then the
-                          // hull pairs by the type of their SAT cache (0..5)
+  int collide_count[17];  // contacts queued for a full manifold update: pair kinds 0..2, the
+                          // hull-sphere and hull-capsule pairs by their simplex cache's size
+                          // (0..3), then the hull pairs by the type of their SAT cache (0..5)
   int long_segments;      // candidate segments handed to the block sort this pair update
   int fast_count;         // fast bodies queued by finalize for the continuous pass (this step)
   int bullet_count;       // fast bullets queued by finalize for the bullet pass (this step)
