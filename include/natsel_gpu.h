@@ -53,10 +53,11 @@ typedef struct {
   float joint_hertz;           /* 60 (JointDef default, joint_defs.rs:44) */
   float joint_damping_ratio;   /* 2 */
   int contact_capacity;        /* 0 = automatic (8 per shape + 4096) */
-  int solver_blocks;           /* solver launch: 0 = automatic (one 16-CTA cluster on B200 for one
-                                  world, a grid over every SM for sub-worlds); 1..16 =
-                                  one thread-block cluster of that many CTAs; > 16 = cooperative grid
-                                  of that many blocks (capped at what fits co-resident) */
+  int solver_blocks;           /* solver launch: 0 = automatic (a grid over every SM for sub-worlds
+                                  or a world of 2048 awake bodies or more, else one 16-CTA cluster
+                                  on B200); 1..16 = one thread-block cluster of that many CTAs;
+                                  > 16 = cooperative grid of that many blocks (capped at what fits
+                                  co-resident) */
   int device;                  /* CUDA device ordinal */
 } ns_world_def;
 

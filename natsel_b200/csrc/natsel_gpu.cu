@@ -663,15 +663,18 @@ int upload_world(ns_world* w) {
   // the kernel's static shared memory counts against the same 48 KB default, so the limit is
   // always raised to what this launch needs
   NS_CUDA(w, cudaFuncSetAttribute(k_state_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->state_smem));
-  // solver launch shape. solver_blocks 0: one cluster of the largest size that fits (16 CTAs on
-  // B200) for a single world, a cooperative grid over every SM for a batch of sub-worlds; 1..16: one thread-block cluster of that many CTAs (non-portable sizes above 8); above
-  // 16: a cooperative grid of that many blocks, capped at what fits co-resident. On the
-  // 10 000-body pile the 16-CTA cluster is about 4 % faster than grids of 32 to 148 blocks: a
-  // colour phase is bounded by one thread's latency chain, not by the number of SMs.
+  // solver launch shape. solver_blocks 0: a cooperative grid over every SM for a batch of
+  // sub-worlds or a world of kGridSolveBodies awake bodies or more, else one cluster of the
+  // largest size that fits (16 CTAs on B200); 1..16: one thread-block cluster of that many CTAs
+  // (non-portable sizes above 8); above 16: a cooperative grid of that many blocks, capped at
+  // what fits co-resident. A colour phase costs about what one constraint's chain costs: the
+  // cluster's barrier is the cheaper (0.3 against 1.2 us), the grid stages every colour of up to
+  // 32 items per block in shared memory (on the 10 000-body pile: 0.61 against 0.68 ms per step).
   {
-    // a batch of sub-worlds has many constraints per colour phase: spread it over every SM
+    constexpr int kGridSolveBodies = 2048;
     int want = w->def.solver_blocks > 0 ? w->def.solver_blocks
-               : (n_worlds > 1 ? std::max(w->sm_count, kMaxSolveCluster + 1) : kMaxSolveCluster);
+               : ((n_worlds > 1 || na >= kGridSolveBodies) ? std::max(w->sm_count, kMaxSolveCluster + 1)
+                                                           : kMaxSolveCluster);
     if (want >= 1 && want <= kMaxSolveCluster) {
       NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
       NS_CUDA(w, cudaFuncSetAttribute(k_solve<false, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));

@@ -258,6 +258,20 @@ def test_solver_launch_shapes_match_oracle(solver_blocks):
     assert g.solver_counts()[14] == (1 if solver_blocks > 16 else 0)
 
 
+@pytest.mark.parametrize("n", [3000, 500])
+def test_default_solver_shape_follows_world_size(n):
+    """solver_blocks 0: a cooperative grid over every SM for a world of 2 048 awake bodies or more
+    (it stages each colour's constraints in shared memory), the 16-CTA cluster below (its barrier
+    is the cheaper); the same bits either way."""
+    g, _ = gpu_world("large_pile", n=n, seed=5)
+    o, _ = oracle_world("large_pile", n=n, seed=5)
+    for _ in range(30):
+        g.step(DT, 4)
+        o.step(DT, 4)
+    assert g.state_hash() == o.state_hash()
+    assert g.solver_counts()[14] == (1 if n >= 2048 else 0)
+
+
 def test_eager_path_matches_oracle(monkeypatch):
     """Without a CUDA graph (the fallback when stream capture is refused) the step is the same."""
     monkeypatch.setenv("NATSEL_EAGER", "1")
