@@ -420,12 +420,13 @@ __global__ void __launch_bounds__(1024) k_bp_segsort_long(DW w) {
 constexpr int kPairKinds = 6;
 // Queues of the narrowphase's update pass: kinds 0..2, the GJK pairs (kinds 3, 4) split by the
 // size of their simplex cache and the hull pairs (kind 5) by the type of their SAT cache, so the
-// lanes of a warp mostly take the same path through the update.
+// lanes of a warp mostly take the same path through the update. Within a kind the pairs without
+// a cache (new pairs: a full SAT or GJK from scratch) get the highest queue, run first.
 constexpr int kCollideQueues = 17;
 __device__ __forceinline__ int collide_queue(const DContact& c) {
   if (c.kind < 3) return c.kind;
-  if (c.kind < 5) return 3 + 4 * (c.kind - 3) + min((int)c.simplex.count, 3);
-  return 11 + min((int)c.sat.type, 5);
+  if (c.kind < 5) return 3 + 4 * (c.kind - 3) + 3 - min((int)c.simplex.count, 3);
+  return 11 + 5 - min((int)c.sat.type, 5);
 }
 __device__ __forceinline__ int pair_kind(int ta, int tb) {
   if (ta == kSphere) return 0;
