@@ -1379,6 +1379,10 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
   // ends, so after the barrier only the body states are fetched.
   __shared__ StageBuf stage_buf;
   bool staged = false;
+  // The warm-start slots a body uses are marked by k_warm_slots before the launch and do not
+  // change during it: the mask of the thread's first body is read once, so the integrate-velocity
+  // phases can issue the slot loads without waiting for it.
+  const uint32_t first_mask = g < w.n_awake ? w.bw_mask[g] : 0u;
   int bar = 0;
   for (int s = 0; s < total_phases; ++s) {
     int ph = phase_at(s);
@@ -1387,8 +1391,7 @@ __global__ void __launch_bounds__(kSolveThreads, kGrid ? 2 : 1) k_solve(DW w, St
       for (int i = g; i < w.n_awake; i += stride) {
         if (kTape) tp.body[((size_t)sub * 3) * w.n_awake + i] = w.states[i];
         IVIn in = load_iv(w, i);
-        uint32_t m = ph == kPhaseIntegrateVelocityWarm ? w.bw_mask[i] : 0u;
-        if ((in.state_flags & kDynamicFlag) == 0u) m = 0u;
+        uint32_t m = ph == kPhaseIntegrateVelocityWarm ? (i == g ? first_mask : w.bw_mask[i]) : 0u;
         WarmSlots ws;
         load_warm_slots(w, i, m, ws);  // in flight while the velocity is integrated
         V3 v, wv;
